@@ -1,0 +1,220 @@
+/*
+ * pgxc.h -- C ABI of libpgxc, the B200 (sm_100a) exchange-correlation grid
+ * quadrature that replaces ParaGauss's per-SCF-cycle numerical XC build.
+ *
+ * Drop-in seam (ParaGauss source, paths relative to the project root):
+ *   modules/xc_hamiltonian.f90:1124  call calc_xcks(ham_xc_arr, "orbitals")   (LDA, XC="VWN")
+ *   modules/xc_hamiltonian.f90:1130  call calc_xcks_nl(ham_xc_arr)             (GGA, XC="PBE")
+ * Both calls become one pgxc_build() plus a status check.  pgxc_create() is
+ * called where xc_setup() runs (modules/xc_hamiltonian.f90:328-577), once per
+ * geometry, and pgxc_destroy() where xc_close() runs.
+ *
+ * Conventions (all fixed by the reference; see the per-function comments):
+ *   - lengths in bohr; arrays are the Fortran arrays passed by address, so
+ *     "(n, m) column-major" means element (i, j) at [i + n*j];
+ *   - basis order = unique atom -> l -> independent function -> radial
+ *     function (modules/orbitalprojection_module.f90:30-45), radial functions
+ *     = N_uncontracted primitives first, then contractions
+ *     (modules/orbital_module.f90:1899-1930);
+ *   - C1 only (one irrep, one partner); ispin 1 or 2.
+ *
+ * Error convention: every entry returns PGXC_OK (0) or a negative PGXC_E*
+ * code; nothing aborts and no C++ exception crosses the ABI.  There is no CPU
+ * fallback: without a usable CUDA device the calls fail with PGXC_ENODEV.
+ */
+#ifndef PGXC_H
+#define PGXC_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define PGXC_OK          0
+#define PGXC_EINVAL     -1   /* bad argument, shape or size                 */
+#define PGXC_ENOTSUP    -2   /* valid in ParaGauss but not in this library  */
+#define PGXC_ENOMEM     -3   /* device allocation failed                    */
+#define PGXC_ECUDA      -4   /* CUDA runtime error                          */
+#define PGXC_ETIMEOUT   -5   /* a bounded device wait ran out               */
+#define PGXC_ENONFINITE -6   /* NaN/Inf in an input or a result             */
+#define PGXC_ENODEV     -7   /* no CUDA device / extension unusable         */
+
+/* ---- functional ids: the two XC keywords on the path ----------------- */
+/* XC="VWN": Slater exchange + VWN5 correlation (modules/xc_cntrl.f90:460-465) */
+#define PGXC_XC_VWN 1
+/* XC="PBE": Slater + PW92 + PBE-X enhancement + PBE-C H (xc_cntrl.f90:652-670) */
+#define PGXC_XC_PBE 2
+
+/* ---- precision modes ------------------------------------------------- */
+#define PGXC_PREC_FP64        0  /* FP64 everywhere: the drop-in              */
+#define PGXC_PREC_MIXED_BF16  1  /* FP32 basis, split-BF16x3 tensor-core GEMMs */
+#define PGXC_PREC_MIXED_TF32  2  /* FP32 basis, split-TF32x3 tensor-core GEMMs */
+
+/* Geometry: unique_atoms(:)%position(1:3,1) in bohr, atom-major xyz triplets. */
+typedef struct pgxc_geometry {
+  int32_t natoms;
+  const double* coords;          /* [natoms*3] */
+} pgxc_geometry;
+
+/*
+ * Orbital basis: one "shell" per (unique atom, l), in the reference order
+ * (atom ascending, l ascending).  Mirrors unique_atom_basis_type
+ * (modules/unique_atom_module.f90:143-168): exponents, norms (the legacy
+ * norms of unique_atom_basis_norm_ob, :426-444, passed as the reference holds
+ * them), N_uncontracted_fcts and contractions(N_exponents, N_contracted_fcts).
+ */
+typedef struct pgxc_basis {
+  int32_t nshells;
+  const int32_t* shell_atom;     /* [nshells] 0-based atom index            */
+  const int32_t* shell_l;        /* [nshells] 0..3                          */
+  const int32_t* shell_nexp;     /* [nshells] N_exponents                   */
+  const int32_t* shell_nunc;     /* [nshells] N_uncontracted_fcts           */
+  const int32_t* shell_ncontr;   /* [nshells] N_contracted_fcts             */
+  const double* exponents;       /* [sum nexp]                              */
+  const double* norms;           /* [sum nexp]                              */
+  const double* contractions;    /* [sum nexp*ncontr], per shell (nexp,ncontr) column-major */
+  /*
+   * C1 symmetry adaptation (unique_atom_symadapt_type%m/%c of irrep 1,
+   * partner 1): independent function i of angular momentum l is
+   * sum_m sa_coef_l[i*(2l+1)+m] * Y_lm, m in the solid-harmonic order of
+   * modules/solid_harmonics_module.f90:369-482 (p = z, x, y).  Blocks for
+   * l = 0..sa_lmax are concatenated.  NULL means the identity.
+   */
+  const double* sa_coef;
+  int32_t sa_lmax;
+} pgxc_basis;
+
+/*
+ * Integration grid: grdpts(npts,4) of modules/grid_module.f90:3045-3164,
+ * column-major x, y, z, w.  With weights_are_raw = 0 the weights are already
+ * Becke-scaled (what mkgrid delivers).  With weights_are_raw = 1, column 4
+ * holds the one-centre weights w_ang*w_rad*4*pi (grid_main_calc,
+ * :425-432) and point_atom the host atom of each point; pgxc_create then
+ * multiplies in the Becke partition weight on the device (becke0, :2442-2497).
+ */
+typedef struct pgxc_grid {
+  int64_t npts;
+  const double* grdpts;          /* [npts*4] column-major                   */
+  int32_t weights_are_raw;
+  const int32_t* point_atom;     /* [npts], required when weights_are_raw   */
+} pgxc_grid;
+
+typedef struct pgxc_options {
+  int32_t functional;            /* PGXC_XC_VWN | PGXC_XC_PBE               */
+  int32_t ispin;                 /* 1 or 2                                  */
+  int32_t precision;             /* PGXC_PREC_*                             */
+  int32_t batch_points;          /* screening batch, 0 -> 128 (machineparameters_veclen) */
+  double  screen_threshold;      /* 0 -> reference behaviour (only alpha*r^2 < 50) */
+  int32_t device;                /* CUDA ordinal, -1 -> current device      */
+  int64_t max_chunk_points;      /* 0 -> sized from free HBM                */
+} pgxc_options;
+
+/* Per-phase device times of the last build, milliseconds (CUDA events). */
+typedef struct pgxc_timings {
+  double h2d_ms;
+  double basis_ms;
+  double density_ms;
+  double functional_ms;
+  double potential_ms;
+  double d2h_ms;
+  double total_ms;
+  int64_t kernel_launches;
+} pgxc_timings;
+
+typedef struct pgxc_ctx pgxc_ctx;
+
+/* Fill *opt with defaults (VWN, ispin 1, FP64, 128, no screening, device -1). */
+void pgxc_default_options(pgxc_options* opt);
+
+/*
+ * Per-geometry set-up; replaces the allocation part of xc_setup
+ * (modules/xc_hamiltonian.f90:328-577) and, with weights_are_raw, the
+ * Becke weighting of mkgrid (modules/grid_module.f90:3130-3137).
+ * Copies geometry, basis and grid to device memory owned by *out.
+ */
+int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas,
+                const pgxc_grid* grid, const pgxc_options* opt,
+                pgxc_ctx** out);
+
+/* Number of orbital basis functions (irrep dimension in C1). */
+int pgxc_nbas(const pgxc_ctx* ctx, int32_t* nbas);
+
+/*
+ * One XC build; replaces calc_xcks (modules/xc_hamiltonian.f90:812-1036)
+ * and calc_xcks_nl (:1280-1580) for n_irrep = 1, partners = 1.
+ *   C   : eigvec_occ(1)%m(nbas, nocc, ispin), column-major
+ *         (modules/occupied_levels_module.f90:112-117)
+ *   occ : occ_num_occ(1)%m(nocc, ispin), column-major
+ *   ham_xc_arr : packed upper triangle, element (k,j), k<=j, of spin s at
+ *         ham_xc_arr[s + ispin*(j*(j+1)/2 + k)] (0-based), ACCUMULATED (+=)
+ *         exactly like tristore (:1018-1034) and :1559-1566;
+ *         xc_length must equal ispin*nbas*(nbas+1)/2.
+ *   exc, nel : the build's E_xc and integrated charge are ADDED to *exc and
+ *         *nel (exc_int / charge_int of :936-949, :1408-1423).
+ *   timings may be NULL.
+ * Synchronous: the outputs are valid on return.
+ */
+int pgxc_build(pgxc_ctx* ctx, const double* C, const double* occ,
+               int32_t nbas, int32_t nocc, int32_t ispin,
+               double* ham_xc_arr, int64_t xc_length,
+               double* exc, double* nel, pgxc_timings* timings);
+
+/*
+ * Same build with every operand already in device memory of the context's
+ * device (for callers that keep C on the GPU).  d_exc_nel receives
+ * {E_xc, N_el} (overwritten, not accumulated); d_ham_xc_arr is overwritten
+ * with the packed matrix of this build.  Runs on the context's stream and
+ * synchronises before returning.
+ */
+int pgxc_build_device(pgxc_ctx* ctx, const double* d_C, const double* d_occ,
+                      int32_t nbas, int32_t nocc, int32_t ispin,
+                      double* d_ham_xc_arr, int64_t xc_length,
+                      double* d_exc_nel, pgxc_timings* timings);
+
+/* Copy of the grid weights the context integrates with (Becke-scaled). */
+int pgxc_grid_weights(const pgxc_ctx* ctx, double* w_out, int64_t npts);
+
+/*
+ * Basis functions and gradients on arbitrary points; replaces
+ * orbital_calculate (modules/orbital_module.f90:1934-2299) with
+ * calculate_orbs_and_grads_v3 (:2421-2619).
+ *   pts   : (npts, 3) column-major
+ *   phi   : (npts, nbas) column-major      (orbs_ob(1)%o(:,:,1))
+ *   grads : (npts, 3, nbas) column-major or NULL (orbs_grads(1)%o(:,:,:,1))
+ */
+int pgxc_orbital_calculate(pgxc_ctx* ctx, int64_t npts, const double* pts,
+                           double* phi, double* grads);
+
+/*
+ * Point-wise functional, FP64, on the device; replaces xc_functionals
+ * (modules/xc_func.f90:187-899) for the two keywords.
+ *   rho : (n, ispin); gam : (n, 2*ispin-1) or NULL for VWN
+ *   f   : (n); fr : (n, ispin); fg : (n, 2*ispin-1) or NULL for VWN
+ */
+int pgxc_xc_functionals(int32_t functional, int32_t ispin, int64_t n,
+                        const double* rho, const double* gam,
+                        double* f, double* fr, double* fg);
+
+/*
+ * Becke partition weights on the device; replaces atomicweight2/becke0
+ * (modules/grid_module.f90:2264-2497, autodiff/becke_step_func.f90:84-124)
+ * with art = 0 (WEIGHT_GRADS default, :371-372).
+ *   pts : (npts, 3) column-major; point_atom : host atom per point;
+ *   w_out : partition weight of the host atom at each point.
+ */
+int pgxc_becke_weights(const pgxc_geometry* geo, int64_t npts,
+                       const double* pts, const int32_t* point_atom,
+                       double* w_out);
+
+const char* pgxc_last_error(const pgxc_ctx* ctx);   /* ctx may be NULL */
+const char* pgxc_strerror(int status);
+
+void pgxc_destroy(pgxc_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PGXC_H */

@@ -1,0 +1,146 @@
+"""ctypes binding of the FP64 CPU oracle (liboracle.so) -- TEST INFRASTRUCTURE.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module; the product (libpgxc) never does.
+"""
+import ctypes as ct
+import glob
+import os
+import subprocess
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(os.path.dirname(HERE), "paragauss-gpl_b200"))
+from pgxc import abi  # noqa: E402
+
+_LIB = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def _openblas_path():
+    libs = os.path.join(os.path.dirname(np.__file__), os.pardir, "numpy.libs")
+    hits = sorted(glob.glob(os.path.join(libs, "libscipy_openblas64_*.so")))
+    return os.path.abspath(hits[0]) if hits else None
+
+
+def lib():
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    path = os.path.join(HERE, "liboracle.so")
+    if not os.path.exists(path):
+        build()
+    L = ct.CDLL(path)
+    P = ct.POINTER
+    L.oracle_set_blas.argtypes = [ct.c_char_p]
+    L.oracle_max_threads.restype = ct.c_int
+    L.oracle_nbas.argtypes = [P(abi.Geometry), P(abi.Basis)]
+    L.oracle_nbas.restype = ct.c_int64
+    L.oracle_orbitals.argtypes = [P(abi.Geometry), P(abi.Basis), ct.c_int64, abi._f64p, abi._f64p, abi._f64p]
+    L.oracle_functionals.argtypes = [ct.c_int32, ct.c_int32, ct.c_int64, abi._f64p, abi._f64p, abi._f64p,
+                                     abi._f64p, abi._f64p]
+    L.oracle_becke.argtypes = [P(abi.Geometry), ct.c_int64, abi._f64p, abi._i32p, abi._f64p, ct.c_int32]
+    L.oracle_xc_build.argtypes = [P(abi.Geometry), P(abi.Basis), P(abi.Grid), ct.c_int32, ct.c_int32,
+                                  abi._f64p, abi._f64p, ct.c_int32, ct.c_int32, abi._f64p, ct.c_int64,
+                                  abi._f64p, abi._f64p, ct.c_int32, ct.c_int32, ct.c_int64, ct.c_int64]
+    L.oracle_overlap.argtypes = [P(abi.Geometry), P(abi.Basis), P(abi.Grid), abi._f64p, ct.c_int32]
+    blas = _openblas_path()
+    if blas:
+        L.oracle_set_blas(blas.encode())
+    _LIB = L
+    return L
+
+
+def max_threads():
+    return lib().oracle_max_threads()
+
+
+def orbitals(case, pts, grads=True):
+    m = abi.Marshalled(case)
+    pts = np.ascontiguousarray(np.asarray(pts, dtype=np.float64).T).reshape(-1)
+    n = len(pts) // 3
+    phi = np.zeros(n * case.nbas)
+    gr = np.zeros(n * 3 * case.nbas) if grads else None
+    st = lib().oracle_orbitals(ct.byref(m.geometry), ct.byref(m.basis), n, abi.f64p(pts), abi.f64p(phi),
+                               abi.f64p(gr))
+    assert st == 0, st
+    phi = phi.reshape(case.nbas, n).T
+    if grads:
+        gr = gr.reshape(case.nbas, 3, n).transpose(2, 1, 0)
+    return phi, gr
+
+
+def functionals(xc, ispin, rho, gam=None):
+    """rho (n, ispin), gam (n, 2ispin-1) -> f (n), fr (n, ispin), fg (n, 2ispin-1)."""
+    xcid = abi.XC_IDS[xc] if isinstance(xc, str) else xc
+    rho = np.asarray(rho, dtype=np.float64).reshape(len(rho), -1)
+    n = rho.shape[0]
+    ng = 2 * ispin - 1
+    r = np.ascontiguousarray(rho.T).reshape(-1)
+    g = np.ascontiguousarray(np.asarray(gam, dtype=np.float64).reshape(n, -1).T).reshape(-1) if gam is not None \
+        else np.zeros(n * ng)
+    f = np.zeros(n)
+    fr = np.zeros(n * ispin)
+    fg = np.zeros(n * ng)
+    st = lib().oracle_functionals(xcid, ispin, n, abi.f64p(r), abi.f64p(g), abi.f64p(f), abi.f64p(fr),
+                                  abi.f64p(fg))
+    assert st == 0, st
+    return f, fr.reshape(ispin, n).T, fg.reshape(ng, n).T
+
+
+def becke(case, nthreads=0):
+    m = abi.Marshalled(case, weighted=False)
+    pts = np.ascontiguousarray(case.grid_xyz.T).reshape(-1)
+    w = np.zeros(case.npts)
+    st = lib().oracle_becke(ct.byref(m.geometry), case.npts, abi.f64p(pts), abi.i32p(m._keep[-1]), abi.f64p(w),
+                            nthreads)
+    assert st == 0, st
+    return w
+
+
+def weight_case(case, nthreads=0):
+    """Fill case.grid_w = raw weight * Becke partition weight (mkgrid :3135)."""
+    case.grid_w = case.grid_wraw * becke(case, nthreads)
+    return case
+
+
+def xc_build(case, vla=128, nthreads=0, pt_range=None):
+    """Returns (ham_xc_arr, exc, nel) of one build on the weighted grid."""
+    assert case.grid_w is not None
+    m = abi.Marshalled(case)
+    C = case.c_fortran()
+    occ = case.occ_fortran()
+    ham = np.zeros(case.xc_length)
+    exc = ct.c_double(0.0)
+    nel = ct.c_double(0.0)
+    lo, hi = pt_range if pt_range else (0, case.npts)
+    st = lib().oracle_xc_build(ct.byref(m.geometry), ct.byref(m.basis), ct.byref(m.grid),
+                               abi.XC_IDS[case.functional], case.ispin, abi.f64p(C), abi.f64p(occ), case.nbas,
+                               case.nocc, abi.f64p(ham), case.xc_length, ct.byref(exc), ct.byref(nel), vla,
+                               nthreads, lo, hi)
+    assert st == 0, st
+    return ham, exc.value, nel.value
+
+
+def overlap(case, nthreads=0):
+    m = abi.Marshalled(case)
+    S = np.zeros(case.nbas * case.nbas)
+    st = lib().oracle_overlap(ct.byref(m.geometry), ct.byref(m.basis), ct.byref(m.grid), abi.f64p(S), nthreads)
+    assert st == 0, st
+    return S.reshape(case.nbas, case.nbas)
+
+
+def unpack(ham, nbas, ispin=1, s=0):
+    """Packed (j outer, k<=j inner, spin stride ispin) -> full symmetric matrix."""
+    jj = np.repeat(np.arange(nbas), np.arange(1, nbas + 1))
+    kk = np.concatenate([np.arange(j + 1) for j in range(nbas)])
+    vals = ham[s::ispin][: len(jj)]
+    V = np.zeros((nbas, nbas))
+    V[kk, jj] = vals
+    V[jj, kk] = vals
+    return V

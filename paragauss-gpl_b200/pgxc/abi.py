@@ -1,0 +1,128 @@
+"""ctypes mirrors of the plain-data structs in include/pgxc.h.
+
+The same layouts describe a case to libpgxc (the product) and, in the tests,
+to the CPU oracle, so one marshalling routine serves both.
+"""
+import ctypes as ct
+
+import numpy as np
+
+PGXC_OK = 0
+PGXC_EINVAL = -1
+PGXC_ENOTSUP = -2
+PGXC_ENOMEM = -3
+PGXC_ECUDA = -4
+PGXC_ETIMEOUT = -5
+PGXC_ENONFINITE = -6
+PGXC_ENODEV = -7
+
+XC_VWN = 1
+XC_PBE = 2
+XC_IDS = {"VWN": XC_VWN, "PBE": XC_PBE}
+
+PREC_FP64 = 0
+PREC_MIXED_BF16 = 1
+PREC_MIXED_TF32 = 2
+PREC_IDS = {"fp64": PREC_FP64, "bf16x3": PREC_MIXED_BF16, "tf32x3": PREC_MIXED_TF32}
+
+_i32p = ct.POINTER(ct.c_int32)
+_f64p = ct.POINTER(ct.c_double)
+
+
+class Geometry(ct.Structure):
+    _fields_ = [("natoms", ct.c_int32), ("coords", _f64p)]
+
+
+class Basis(ct.Structure):
+    _fields_ = [
+        ("nshells", ct.c_int32),
+        ("shell_atom", _i32p),
+        ("shell_l", _i32p),
+        ("shell_nexp", _i32p),
+        ("shell_nunc", _i32p),
+        ("shell_ncontr", _i32p),
+        ("exponents", _f64p),
+        ("norms", _f64p),
+        ("contractions", _f64p),
+        ("sa_coef", _f64p),
+        ("sa_lmax", ct.c_int32),
+    ]
+
+
+class Grid(ct.Structure):
+    _fields_ = [
+        ("npts", ct.c_int64),
+        ("grdpts", _f64p),
+        ("weights_are_raw", ct.c_int32),
+        ("point_atom", _i32p),
+    ]
+
+
+class Options(ct.Structure):
+    _fields_ = [
+        ("functional", ct.c_int32),
+        ("ispin", ct.c_int32),
+        ("precision", ct.c_int32),
+        ("batch_points", ct.c_int32),
+        ("screen_threshold", ct.c_double),
+        ("device", ct.c_int32),
+        ("max_chunk_points", ct.c_int64),
+    ]
+
+
+class Timings(ct.Structure):
+    _fields_ = [
+        ("h2d_ms", ct.c_double),
+        ("basis_ms", ct.c_double),
+        ("density_ms", ct.c_double),
+        ("functional_ms", ct.c_double),
+        ("potential_ms", ct.c_double),
+        ("d2h_ms", ct.c_double),
+        ("total_ms", ct.c_double),
+        ("kernel_launches", ct.c_int64),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+def f64p(a):
+    """Pointer to a C-contiguous float64 array (or NULL for None)."""
+    if a is None:
+        return ct.cast(None, _f64p)
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_f64p)
+
+
+def i32p(a):
+    if a is None:
+        return ct.cast(None, _i32p)
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_i32p)
+
+
+class Marshalled:
+    """Keeps the numpy buffers alive while the C structs point into them."""
+
+    def __init__(self, case, weighted=True):
+        self._keep = []
+        c = case
+        coords = np.ascontiguousarray(c.coords, dtype=np.float64).reshape(-1)
+        self._keep.append(coords)
+        self.geometry = Geometry(len(c.coords), f64p(coords))
+        arrs = [np.ascontiguousarray(a, dtype=np.int32) for a in
+                (c.shell_atom, c.shell_l, c.shell_nexp, c.shell_nunc, c.shell_ncontr)]
+        flt = [np.ascontiguousarray(a, dtype=np.float64) for a in
+               (c.exponents, c.norms, c.contractions)]
+        sa = None if c.sa_coef is None else np.ascontiguousarray(c.sa_coef, dtype=np.float64)
+        self._keep += arrs + flt + [sa]
+        self.basis = Basis(len(c.shell_l), *[i32p(a) for a in arrs], *[f64p(a) for a in flt],
+                           f64p(sa), int(c.sa_lmax))
+        w = c.grid_w if (weighted and c.grid_w is not None) else c.grid_wraw
+        grd = np.concatenate([c.grid_xyz[:, 0], c.grid_xyz[:, 1], c.grid_xyz[:, 2], w])
+        grd = np.ascontiguousarray(grd, dtype=np.float64)
+        pa = np.ascontiguousarray(c.point_atom, dtype=np.int32)
+        self._keep += [grd, pa]
+        raw = 0 if (weighted and c.grid_w is not None) else 1
+        self.grid = Grid(len(w), f64p(grd), raw, i32p(pa))
+        self.weights_are_raw = raw
