@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""XC-build benchmark: grid points per second of one exchange-correlation build.
+
+Workload (the metric's configuration): a seeded 60-atom C/H cluster (30 C,
+30 H in a 12 Angstrom cube, d_min 1.1 Angstrom), C 4s3p1d / H 2s1p spherical
+Gaussians (690 functions, exponents log-uniform in [0.05, 1e4]), 75 radial x
+300 angular points per atom, PBE, 210 doubly occupied orbitals.  One step is
+one full XC build (basis, density, functional, V_xc) over the whole grid.
+
+  value : grid points/s with C already resident in HBM (pgxc_build_device)
+  e2e   : grid points/s through pgxc_build with host buffers: C/occ copied
+          host->device and the packed V_xc + E_xc/N_el read back every step
+
+`--impl reference` times the CPU path of the reference algorithm instead
+(the FP64 oracle port, all host threads, bounded sample per step).
+With torchrun (N > 1) the grid is split into contiguous point ranges, one per
+GPU, and the packed V_xc plus {E_xc, N_el} are summed with an NCCL
+all-reduce: the reduction ParaGauss does with MPI_Reduce in xc_sndrcv.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "paragauss-gpl_b200"))
+
+METRIC = "XC-build grid pts/s (mixed vs FP64 on B200 at |dExc|<1e-6 Eh; CPU ref beside)"
+UNIT = "grid_points/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="pgxc", choices=["pgxc", "reference"])
+    p.add_argument("--precision", default=None, help="fp64 | bf16x3 | tf32x3 (default: the headline path)")
+    p.add_argument("--config", type=int, default=2)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--compare-fp64", action="store_true", default=True)
+    return p.parse_args()
+
+
+def headline_precision():
+    return "fp64"
+
+
+# ---------------------------------------------------------------------------
+def workload_desc(case):
+    return (f"{case.name}: {len(case.coords)} atoms, {case.nbas} spherical fns (l<=2), "
+            f"{case.npts} grid pts ({case.meta['nrad']} radial x {case.meta['nang']}-class angular per atom), "
+            f"nocc={case.nocc}, {case.functional}")
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except Exception:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        try:
+            for line in open(self.f.name):
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+                    rows.append(parts)
+        except Exception:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = np.array([float(r[1]) for r in rows])
+        mx = float(rows[0][2])
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        busy = sm[sm > 0.5 * mx] if np.any(sm > 0.5 * mx) else sm
+        return {"sm_mhz": float(np.median(busy)), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+def cuda_timer(torch, fn, steps):
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    for _ in range(steps):
+        fn()
+    t1.record()
+    torch.cuda.synchronize()
+    return t0.elapsed_time(t1)
+
+
+def fp64_peak_tflops(torch):
+    """cuBLAS DGEMM throughput measured now: the FP64 tensor-pipe reference."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    best = 1e30
+    for _ in range(3):
+        best = min(best, cuda_timer(torch, lambda: torch.matmul(a, b), 1))
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def shard(case, rank, world):
+    """Contiguous 64-aligned point range of this rank (xc_sndrcv partition analogue)."""
+    if world == 1:
+        return case
+    from pgxc import cases as C
+    n = case.npts
+    per = -(-n // world)
+    per = -(-per // 64) * 64
+    lo, hi = min(rank * per, n), min((rank + 1) * per, n)
+    sub = C.Case(**{**case.__dict__})
+    sub.grid_xyz = case.grid_xyz[lo:hi]
+    sub.grid_wraw = case.grid_wraw[lo:hi]
+    sub.point_atom = case.point_atom[lo:hi]
+    sub.grid_w = None if case.grid_w is None else case.grid_w[lo:hi]
+    return sub
+
+
+def algorithmic_flops(case):
+    n, N = case.nbas, case.npts
+    x = 2.0 * N * n * n
+    v = 2.0 * N * n * n if case.functional == "PBE" else 1.0 * N * n * n
+    return x, v
+
+
+def cpu_baseline(case, weights, seconds):
+    """Oracle port on host cores over a bounded sample of the workload: whole
+    builds (or a contiguous prefix of the grid) repeated to ~`seconds`."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    c = case
+    c.grid_w = weights
+    threads = O.max_threads()
+    pilot = min(c.npts, 65536)
+    O.xc_build(c, pt_range=(0, min(c.npts, 4096)))  # thread start-up
+    t = time.perf_counter()
+    O.xc_build(c, pt_range=(0, pilot))
+    rate = pilot / max(time.perf_counter() - t, 1e-6)
+    n = int(min(c.npts, max(pilot, rate * seconds)))
+    n = max(128, n // 128 * 128)
+    reps = max(1, int(round(seconds / (n / rate))))
+    t = time.perf_counter()
+    for _ in range(reps):
+        O.xc_build(c, pt_range=(0, n))
+    dt = time.perf_counter() - t
+    what = "the whole grid" if n == c.npts else f"the first {n} of {c.npts} grid points"
+    return {"value": reps * n / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{reps} build(s) over {what} (128-point batches), {threads} OpenMP threads, "
+                      f"OpenBLAS DGEMM; FP64 oracle restating the reference CPU path",
+            "seconds": dt}
+
+
+# ---------------------------------------------------------------------------
+def run_reference(args):
+    from pgxc import cases
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    case = cases.config(args.config)
+    threads = O.max_threads()
+    # bounded sample per step: ~10 s of CPU work
+    n_probe = min(case.npts, 2048)
+    sub = shard(case, 0, 1)
+    sub.grid_w = None
+    probe = cases.Case(**{**case.__dict__})
+    probe.grid_xyz = case.grid_xyz[:n_probe]
+    probe.grid_wraw = case.grid_wraw[:n_probe]
+    probe.point_atom = case.point_atom[:n_probe]
+    O.weight_case(probe)
+    t = time.perf_counter()
+    O.xc_build(probe)
+    rate = n_probe / max(time.perf_counter() - t, 1e-6)
+    total_budget = 150.0
+    per_step = max(2.0, min(12.0, total_budget / max(1, args.steps + args.warmup)))
+    n = int(min(case.npts, max(n_probe, rate * per_step)))
+    n = max(128, n // 128 * 128)
+    samp = cases.Case(**{**case.__dict__})
+    samp.grid_xyz = case.grid_xyz[:n]
+    samp.grid_wraw = case.grid_wraw[:n]
+    samp.point_atom = case.point_atom[:n]
+    O.weight_case(samp)
+    for _ in range(args.warmup):
+        O.xc_build(samp)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        O.xc_build(samp)
+    dt = (time.perf_counter() - t) / args.steps
+    value = n / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": workload_desc(case), "precision": "fp64", "path": "CPU"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"first {n} of {case.npts} grid points per step (contiguous 128-point "
+                                   f"batches), {threads} OpenMP threads, OpenBLAS DGEMM; the Fortran reference "
+                                   f"cannot be compiled here, so the FP64 oracle port restating it is timed"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+    from pgxc import cases, lib
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    prec = args.precision or headline_precision()
+    case = cases.config(args.config)
+    sub = shard(case, rank, world)
+    ctx = lib.Context(sub, precision=prec, weighted=False, device=local)
+    weights = ctx.grid_weights()
+    nb, nocc = case.nbas, case.nocc
+    dC = torch.from_numpy(case.c_fortran()).cuda()
+    docc = torch.from_numpy(case.occ_fortran()).cuda()
+    dham = torch.zeros(case.xc_length, dtype=torch.float64, device="cuda")
+    dsum = torch.zeros(2, dtype=torch.float64, device="cuda")
+    last_tm = {}
+
+    def step():
+        last_tm.update(ctx.build_device(dC.data_ptr(), docc.data_ptr(), dham.data_ptr(), dsum.data_ptr()))
+        if world > 1:
+            dist.all_reduce(dham)
+            dist.all_reduce(dsum)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        ms = cuda_timer(torch, step, args.steps)
+    clocks = clk.summary()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    per_step = ms / args.steps
+    value = case.npts / (per_step * 1e-3)
+    exc, nel = dsum.tolist()
+
+    # end to end through the host-buffer C ABI call
+    C_host = torch.from_numpy(case.c_fortran()).pin_memory()
+    occ_host = torch.from_numpy(case.occ_fortran()).pin_memory()
+    ham_host = np.zeros(case.xc_length)
+
+    def e2e_step():
+        ham_host[:] = 0.0
+        h, e, q = ctx.build(C=C_host.numpy(), occ=occ_host.numpy(), ham=ham_host)
+        if world > 1:
+            th = torch.from_numpy(h).cuda()
+            dist.all_reduce(th)
+            h[:] = th.cpu().numpy()
+        return e
+
+    for _ in range(2):
+        e2e_step()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    ms_e = cuda_timer(torch, e2e_step, args.steps)
+    t = torch.tensor([ms_e], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_e = float(t.item())
+    e2e_value = case.npts / (ms_e / args.steps * 1e-3)
+    h2d = (nb * nocc + nocc) * 8
+    d2h = (case.xc_length + 2) * 8
+
+    # roofline of the dominant contraction kernel (per-launch averages from the library's events)
+    fx, fv = algorithmic_flops(sub)
+    xs, vs = last_tm["xgemm_ms"], last_tm["vgemm_ms"]
+    if xs >= vs:
+        kname, kflops, kms = "density contraction X = phi P (+ fused rho, grad rho)", fx, xs
+    else:
+        kname, kflops, kms = "potential contraction V += phi^T Z", fv, vs
+    roof = None
+    if rank == 0:
+        if prec == "fp64":
+            peak = fp64_peak_tflops(torch)
+            peak_src = "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor pipe); not in MEASURED_PEAKS.json"
+        else:
+            mp = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+            peak = mp["bf16_tflops"]
+            peak_src = "MEASURED_PEAKS.json bf16_tflops (burst) of measured"
+        achieved = kflops / (kms * 1e-3) / 1e12
+        traffic = None
+        tf = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tf):
+            traffic = json.load(open(tf)).get(f"{prec}:{case.functional}")
+        roof = {"bound": "tensor", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
+                "kernel_ms_per_build": kms, "flops_per_build": kflops,
+                "phase_ms": {k: last_tm[k] for k in ("basis_ms", "density_ms", "functional_ms", "potential_ms")}}
+
+    out = None
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(args.warmup, 3), "ms_per_step": per_step, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "f32+" + prec, "data": "synthetic",
+            "config": {"workload": workload_desc(case), "precision": prec,
+                       "parallelism": f"grid split over {world} GPU(s), NCCL all-reduce of packed V_xc",
+                       "l2": "no flush: each build streams several GB of basis/Z data (inputs larger than L2)"},
+            "xc_builds_per_s": 1e3 / per_step, "E_xc": exc, "N_el": nel,
+            "roofline": roof,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": ms_e / args.steps},
+            "gpu_launches": int(last_tm["kernel_launches"]) * args.steps,
+            "clocks": clocks,
+        }
+    if world > 1:
+        dist.barrier()
+    ctx.close()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(case, weights, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

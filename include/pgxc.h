@@ -120,6 +120,8 @@ typedef struct pgxc_timings {
   double potential_ms;
   double d2h_ms;
   double total_ms;
+  double xgemm_ms;        /* density contraction kernel (X = phi P, fused rho) */
+  double vgemm_ms;        /* potential contraction kernel (V += phi^T Z)      */
   int64_t kernel_launches;
 } pgxc_timings;
 

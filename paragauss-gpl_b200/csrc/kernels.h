@@ -1,0 +1,79 @@
+// kernels.h -- host-side launch interface between the C ABI and the kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "pgxc_common.cuh"
+#include "xc_functional.cuh"
+
+namespace pgxc {
+
+// Device pointers and sizes of one context, passed to every launcher.
+struct BuildArgs {
+  // basis
+  const DevShell* shells = nullptr;
+  int nshells = 0;
+  const double* atoms = nullptr;
+  const double* exps = nullptr;
+  const double* norms = nullptr;
+  const double* contr = nullptr;
+  DevSA sa;
+  XcConst xc;
+  // grid (SoA, whole grid)
+  const double* px = nullptr;
+  const double* py = nullptr;
+  const double* pz = nullptr;
+  const double* w = nullptr;
+  // chunk work arrays, [function][ldp]
+  int64_t ldp = 0;      // points per chunk (multiple of 64)
+  double* phi = nullptr;
+  double* gx = nullptr;
+  double* gy = nullptr;
+  double* gz = nullptr;
+  double* Z = nullptr;
+  // per-point arrays [ldp]
+  double* rho = nullptr;
+  double* grx = nullptr;
+  double* gry = nullptr;
+  double* grz = nullptr;
+  double* A = nullptr;
+  double* Bx = nullptr;
+  double* By = nullptr;
+  double* Bz = nullptr;
+  double* partial = nullptr;  // 2 per functional block
+  double* acc = nullptr;      // {E, cE, N, cN}
+  // density matrix
+  int64_t ldc = 0;            // nbas padded to 64
+  double* C = nullptr;        // [nocc_pad][ldc]
+  double* Cocc = nullptr;
+  const double* occ = nullptr;
+  double* P = nullptr;        // [ldc][ldc]
+  // potential tiles
+  int nt = 0;                 // ldc / 64
+  int ntiles = 0;             // nt (nt + 1) / 2
+  int nsplit = 0;
+  int64_t kspan = 0;          // points per split (multiple of 16)
+  const int2* tiles = nullptr;
+  const int* tile_of = nullptr;
+  double* vpart = nullptr;    // [nsplit][ntiles][64*64]
+};
+
+void launch_basis_f64(const BuildArgs& a, int64_t p0, int64_t nvalid, bool grad, cudaStream_t st);
+void launch_basis_points_f64(const BuildArgs& a, const double* px, const double* py, const double* pz, int64_t n,
+                             int64_t ld, double* phi, double* gx, double* gy, double* gz, cudaStream_t st);
+void launch_pmat_f64(const BuildArgs& a, int64_t kpad, cudaStream_t st);
+void launch_density_f64(const BuildArgs& a, bool gga, cudaStream_t st);
+void launch_functional_f64(const BuildArgs& a, int64_t p0, int64_t nvalid, bool gga, cudaStream_t st);
+void launch_zbuild_f64(const BuildArgs& a, bool gga, cudaStream_t st);
+void launch_vpot_f64(const BuildArgs& a, bool gga, cudaStream_t st);
+void launch_pack(const BuildArgs& a, int64_t nbas, int ispin, int spin, double* ham, cudaStream_t st);
+
+// point-wise functional and Becke weights (standalone entry points)
+void launch_xc_points(int functional, int64_t n, const double* rho, const double* gam, double* f, double* fr,
+                      double* fg, cudaStream_t st);
+void launch_becke(const double* atoms, double* dist, int natm, const double* px, const double* py, const double* pz,
+                  const int* owner, int64_t n, double* w, cudaStream_t st);
+void launch_scale_inplace(double* x, const double* s, int64_t n, cudaStream_t st);
+
+}  // namespace pgxc

@@ -1,0 +1,665 @@
+// pgxc_api.cu -- the C ABI of libpgxc (include/pgxc.h).
+//
+// One context per geometry (pgxc_create, where ParaGauss runs xc_setup),
+// one pgxc_build per SCF cycle (in place of calc_xcks / calc_xcks_nl).
+// Everything is computed on the device; a missing or unusable CUDA device is
+// an error (PGXC_ENODEV), never a CPU fallback.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+#include "mixed.h"
+#include "pgxc_common.cuh"
+
+using namespace pgxc;
+
+struct pgxc_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[8] = {};
+  cudaEvent_t kev[4] = {};
+  std::string err;
+  pgxc_options opt;
+  int natm = 0;
+  int64_t nbas = 0, npts = 0;
+  int lmax = 0;
+  BuildArgs a;
+  std::vector<void*> allocs;
+  // host copies needed later
+  std::vector<DevShell> shells;
+  // device buffers not in BuildArgs
+  double* d_ham = nullptr;
+  double* d_dist = nullptr;
+  int nocc_cap = 0;
+  int64_t chunk = 0;
+  double* h_ham = nullptr;      // pinned staging for the packed matrix
+  double* h_acc = nullptr;      // pinned {E, cE, N, cN}
+  MixedState* mixed = nullptr;  // tensor-core mixed-precision path
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+int set_err(pgxc_ctx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  g_err = msg;
+  return code;
+}
+
+#define CUDA_TRY(ctx, call)                                                                     \
+  do {                                                                                          \
+    cudaError_t e_ = (call);                                                                    \
+    if (e_ != cudaSuccess)                                                                      \
+      return set_err(ctx, e_ == cudaErrorMemoryAllocation ? PGXC_ENOMEM : PGXC_ECUDA,           \
+                     std::string(#call " failed: ") + cudaGetErrorString(e_));                  \
+  } while (0)
+
+template <typename T>
+int dalloc(pgxc_ctx* c, T** p, size_t n) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
+  if (e != cudaSuccess)
+    return set_err(c, PGXC_ENOMEM, std::string("cudaMalloc of ") + std::to_string(n * sizeof(T)) +
+                                       " bytes failed: " + cudaGetErrorString(e));
+  c->allocs.push_back(q);
+  *p = (T*)q;
+  return PGXC_OK;
+}
+
+int check_device(pgxc_ctx* c, int want) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) return set_err(c, PGXC_ENODEV, "no CUDA device available");
+  int dev = want;
+  if (dev < 0) {
+    if (cudaGetDevice(&dev) != cudaSuccess) return set_err(c, PGXC_ENODEV, "cudaGetDevice failed");
+  }
+  if (dev >= n) return set_err(c, PGXC_EINVAL, "device ordinal out of range");
+  cudaDeviceProp prop;
+  if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) return set_err(c, PGXC_ENODEV, "device query failed");
+  if (prop.major != 10) return set_err(c, PGXC_ENODEV, "libpgxc is built for sm_100a (B200) only");
+  if (c) c->device = dev;
+  return PGXC_OK;
+}
+
+bool all_finite(const double* p, int64_t n) {
+  for (int64_t i = 0; i < n; ++i)
+    if (!std::isfinite(p[i])) return false;
+  return true;
+}
+
+}  // namespace
+
+extern "C" {
+
+void pgxc_default_options(pgxc_options* o) {
+  if (!o) return;
+  o->functional = PGXC_XC_VWN;
+  o->ispin = 1;
+  o->precision = PGXC_PREC_FP64;
+  o->batch_points = 128;
+  o->screen_threshold = 0.0;
+  o->device = -1;
+  o->max_chunk_points = 0;
+}
+
+const char* pgxc_last_error(const pgxc_ctx* ctx) { return ctx ? ctx->err.c_str() : g_err.c_str(); }
+
+const char* pgxc_strerror(int s) {
+  switch (s) {
+    case PGXC_OK: return "ok";
+    case PGXC_EINVAL: return "invalid argument";
+    case PGXC_ENOTSUP: return "not supported";
+    case PGXC_ENOMEM: return "out of device memory";
+    case PGXC_ECUDA: return "CUDA error";
+    case PGXC_ETIMEOUT: return "device wait timed out";
+    case PGXC_ENONFINITE: return "non-finite value";
+    case PGXC_ENODEV: return "no usable CUDA device";
+    default: return "unknown status";
+  }
+}
+
+void pgxc_destroy(pgxc_ctx* c) {
+  if (!c) return;
+  if (c->device >= 0) cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->mixed) mixed_destroy(c->mixed);
+  for (void* p : c->allocs) cudaFree(p);
+  if (c->h_ham) cudaFreeHost(c->h_ham);
+  if (c->h_acc) cudaFreeHost(c->h_acc);
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : c->kev)
+    if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+int pgxc_nbas(const pgxc_ctx* c, int32_t* nbas) {
+  if (!c || !nbas) return PGXC_EINVAL;
+  *nbas = (int32_t)c->nbas;
+  return PGXC_OK;
+}
+
+static int validate_basis(pgxc_ctx* c, const pgxc_geometry* geo, const pgxc_basis* b, std::vector<DevShell>& out,
+                          int64_t& nbas, int& lmax, int64_t& nexp_tot, int64_t& ncon_tot) {
+  if (!geo || !b || geo->natoms <= 0 || !geo->coords || b->nshells <= 0)
+    return set_err(c, PGXC_EINVAL, "empty geometry or basis");
+  if (!b->shell_atom || !b->shell_l || !b->shell_nexp || !b->shell_nunc || !b->shell_ncontr || !b->exponents ||
+      !b->norms || !b->contractions)
+    return set_err(c, PGXC_EINVAL, "basis arrays must not be NULL");
+  int last_atom = -1, last_l = -1;
+  nbas = 0;
+  lmax = 0;
+  nexp_tot = 0;
+  ncon_tot = 0;
+  for (int s = 0; s < b->nshells; ++s) {
+    DevShell S{};
+    S.atom = b->shell_atom[s];
+    S.l = b->shell_l[s];
+    S.nexp = b->shell_nexp[s];
+    S.nunc = b->shell_nunc[s];
+    S.ncontr = b->shell_ncontr[s];
+    if (S.atom < 0 || S.atom >= geo->natoms) return set_err(c, PGXC_EINVAL, "shell atom index out of range");
+    if (S.l < 0) return set_err(c, PGXC_EINVAL, "negative l");
+    if (S.l > kMaxL) return set_err(c, PGXC_ENOTSUP, "l > 3 is not supported");
+    if (S.nexp <= 0 || S.nunc < 0 || S.ncontr < 0 || S.nunc > S.nexp)
+      return set_err(c, PGXC_EINVAL, "bad shell exponent/contraction counts");
+    if (S.atom < last_atom || (S.atom == last_atom && S.l <= last_l))
+      return set_err(c, PGXC_EINVAL, "shells must be ordered by atom, then l (orbitalprojection order)");
+    last_atom = S.atom;
+    last_l = S.l;
+    S.nrad = S.nunc + S.ncontr;
+    S.exp_off = (int)nexp_tot;
+    S.con_off = (int)ncon_tot;
+    S.f0 = (int)nbas;
+    double mn = 1e300;
+    for (int e = 0; e < S.nexp; ++e) {
+      const double a = b->exponents[nexp_tot + e];
+      if (!(a > 0.0) || !std::isfinite(a)) return set_err(c, PGXC_EINVAL, "exponents must be positive and finite");
+      mn = std::min(mn, a);
+    }
+    S.min_exp = mn;
+    nexp_tot += S.nexp;
+    ncon_tot += (int64_t)S.nexp * S.ncontr;
+    nbas += (int64_t)(2 * S.l + 1) * S.nrad;
+    lmax = std::max(lmax, S.l);
+    out.push_back(S);
+  }
+  if (!all_finite(b->norms, nexp_tot) || !all_finite(b->contractions, ncon_tot) ||
+      !all_finite(geo->coords, 3 * (int64_t)geo->natoms))
+    return set_err(c, PGXC_ENONFINITE, "non-finite basis or geometry input");
+  if (nbas == 0) return set_err(c, PGXC_EINVAL, "basis has no functions");
+  return PGXC_OK;
+}
+
+int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid* grid, const pgxc_options* opt,
+                pgxc_ctx** out) {
+  if (!out) return set_err(nullptr, PGXC_EINVAL, "out is NULL");
+  *out = nullptr;
+  pgxc_ctx* c = new (std::nothrow) pgxc_ctx();
+  if (!c) return set_err(nullptr, PGXC_ENOMEM, "host allocation failed");
+  pgxc_options o;
+  pgxc_default_options(&o);
+  if (opt) o = *opt;
+  if (o.batch_points <= 0) o.batch_points = 128;
+  c->opt = o;
+  auto fail = [&](int st) {
+    g_err = c->err;
+    pgxc_destroy(c);
+    return st;
+  };
+  if (o.functional != PGXC_XC_VWN && o.functional != PGXC_XC_PBE)
+    return fail(set_err(c, PGXC_EINVAL, "unknown functional id"));
+  if (o.ispin != 1 && o.ispin != 2) return fail(set_err(c, PGXC_EINVAL, "ispin must be 1 or 2"));
+  if (o.ispin == 2) return fail(set_err(c, PGXC_ENOTSUP, "open-shell (ispin=2) builds are not implemented yet"));
+  if (o.precision < PGXC_PREC_FP64 || o.precision > PGXC_PREC_MIXED_TF32)
+    return fail(set_err(c, PGXC_EINVAL, "unknown precision mode"));
+  if (!grid || grid->npts <= 0 || !grid->grdpts) return fail(set_err(c, PGXC_EINVAL, "empty grid"));
+  if (grid->weights_are_raw && !grid->point_atom)
+    return fail(set_err(c, PGXC_EINVAL, "raw weights need point_atom"));
+  int64_t nexp_tot, ncon_tot;
+  int st = validate_basis(c, geo, bas, c->shells, c->nbas, c->lmax, nexp_tot, ncon_tot);
+  if (st) return fail(st);
+  if (!all_finite(grid->grdpts, 4 * grid->npts)) return fail(set_err(c, PGXC_ENONFINITE, "non-finite grid input"));
+  if (grid->weights_are_raw)
+    for (int64_t i = 0; i < grid->npts; ++i)
+      if (grid->point_atom[i] < 0 || grid->point_atom[i] >= geo->natoms)
+        return fail(set_err(c, PGXC_EINVAL, "point_atom out of range"));
+  st = check_device(c, o.device);
+  if (st) return fail(st);
+  if (cudaSetDevice(c->device) != cudaSuccess) return fail(set_err(c, PGXC_ECUDA, "cudaSetDevice failed"));
+  CUDA_TRY(c, cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  for (auto& e : c->ev) CUDA_TRY(c, cudaEventCreate(&e));
+  for (auto& e : c->kev) CUDA_TRY(c, cudaEventCreate(&e));
+  c->natm = geo->natoms;
+  c->npts = grid->npts;
+  BuildArgs& a = c->a;
+  a.nshells = (int)c->shells.size();
+  a.xc = make_xc_const();
+  // symmetry adaptation table
+  std::memset(&a.sa, 0, sizeof(a.sa));
+  a.sa.identity = 1;
+  if (bas->sa_coef) {
+    if (bas->sa_lmax < c->lmax) return fail(set_err(c, PGXC_EINVAL, "sa_coef must cover every l of the basis"));
+    int64_t off = 0;
+    for (int l = 0; l <= std::min(bas->sa_lmax, kMaxL); ++l) {
+      const int n = 2 * l + 1;
+      for (int i = 0; i < n; ++i)
+        for (int m = 0; m < n; ++m) {
+          const double v = bas->sa_coef[off + i * n + m];
+          a.sa.c[l][i][m] = v;
+          if (v != (i == m ? 1.0 : 0.0)) a.sa.identity = 0;
+        }
+      off += n * n;
+    }
+  }
+  // basis and geometry
+  DevShell* dsh;
+  double *datoms, *dexps, *dnorms, *dcontr;
+  if ((st = dalloc(c, &dsh, c->shells.size())) || (st = dalloc(c, &datoms, 3 * (size_t)c->natm)) ||
+      (st = dalloc(c, &dexps, nexp_tot)) || (st = dalloc(c, &dnorms, nexp_tot)) ||
+      (st = dalloc(c, &dcontr, std::max<int64_t>(ncon_tot, 1))))
+    return fail(st);
+  CUDA_TRY(c, cudaMemcpy(dsh, c->shells.data(), c->shells.size() * sizeof(DevShell), cudaMemcpyHostToDevice));
+  CUDA_TRY(c, cudaMemcpy(datoms, geo->coords, 3 * sizeof(double) * c->natm, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, cudaMemcpy(dexps, bas->exponents, sizeof(double) * nexp_tot, cudaMemcpyHostToDevice));
+  CUDA_TRY(c, cudaMemcpy(dnorms, bas->norms, sizeof(double) * nexp_tot, cudaMemcpyHostToDevice));
+  if (ncon_tot) CUDA_TRY(c, cudaMemcpy(dcontr, bas->contractions, sizeof(double) * ncon_tot, cudaMemcpyHostToDevice));
+  a.shells = dsh;
+  a.atoms = datoms;
+  a.exps = dexps;
+  a.norms = dnorms;
+  a.contr = dcontr;
+  // grid, SoA
+  const int64_t n = c->npts;
+  double* dgrid;
+  if ((st = dalloc(c, &dgrid, 4 * (size_t)n))) return fail(st);
+  CUDA_TRY(c, cudaMemcpy(dgrid, grid->grdpts, 4 * sizeof(double) * n, cudaMemcpyHostToDevice));
+  a.px = dgrid;
+  a.py = dgrid + n;
+  a.pz = dgrid + 2 * n;
+  a.w = dgrid + 3 * n;
+  if (grid->weights_are_raw) {
+    // w <- w_raw * Becke partition weight of the host atom (mkgrid :3135-3137)
+    int* downer;
+    double* dbecke;
+    if ((st = dalloc(c, &downer, n)) || (st = dalloc(c, &dbecke, n)) ||
+        (st = dalloc(c, &c->d_dist, (size_t)c->natm * c->natm)))
+      return fail(st);
+    CUDA_TRY(c, cudaMemcpy(downer, grid->point_atom, sizeof(int) * n, cudaMemcpyHostToDevice));
+    launch_becke(datoms, c->d_dist, c->natm, a.px, a.py, a.pz, downer, n, dbecke, c->stream);
+    CUDA_TRY(c, cudaGetLastError());
+    launch_scale_inplace(dgrid + 3 * n, dbecke, n, c->stream);
+    CUDA_TRY(c, cudaStreamSynchronize(c->stream));
+  }
+  // chunk sizing
+  a.ldc = round_up(c->nbas, kTile);
+  const bool gga = o.functional == PGXC_XC_PBE;
+  size_t freeb = 0, totb = 0;
+  CUDA_TRY(c, cudaMemGetInfo(&freeb, &totb));
+  const int64_t arrays = gga ? 5 : 2;
+  const int64_t per_pt = a.ldc * 8 * arrays + 8 * 10;
+  int64_t chunk = (int64_t)(0.30 * (double)freeb) / per_pt;
+  chunk = std::min<int64_t>(chunk, 1 << 19);
+  if (o.max_chunk_points > 0) chunk = std::min<int64_t>(chunk, o.max_chunk_points);
+  chunk = std::min<int64_t>(chunk, round_up(n, 64));
+  chunk = std::max<int64_t>(64, chunk / 64 * 64);
+  c->chunk = chunk;
+  a.ldp = chunk;
+  if (o.precision == PGXC_PREC_FP64) {
+    if ((st = dalloc(c, &a.phi, (size_t)a.ldc * chunk)) || (st = dalloc(c, &a.Z, (size_t)a.ldc * chunk)))
+      return fail(st);
+    if (gga && ((st = dalloc(c, &a.gx, (size_t)a.ldc * chunk)) || (st = dalloc(c, &a.gy, (size_t)a.ldc * chunk)) ||
+                (st = dalloc(c, &a.gz, (size_t)a.ldc * chunk))))
+      return fail(st);
+    // rows nbas..ldc-1 stay zero for ever (the basis kernel never writes them)
+    CUDA_TRY(c, cudaMemset(a.phi, 0, sizeof(double) * a.ldc * chunk));
+    if (gga) {
+      CUDA_TRY(c, cudaMemset(a.gx, 0, sizeof(double) * a.ldc * chunk));
+      CUDA_TRY(c, cudaMemset(a.gy, 0, sizeof(double) * a.ldc * chunk));
+      CUDA_TRY(c, cudaMemset(a.gz, 0, sizeof(double) * a.ldc * chunk));
+    }
+  }
+  double* pp;
+  if ((st = dalloc(c, &pp, 8 * (size_t)chunk))) return fail(st);
+  a.rho = pp; a.grx = pp + chunk; a.gry = pp + 2 * chunk; a.grz = pp + 3 * chunk;
+  a.A = pp + 4 * chunk; a.Bx = pp + 5 * chunk; a.By = pp + 6 * chunk; a.Bz = pp + 7 * chunk;
+  if ((st = dalloc(c, &a.partial, 2 * (size_t)((chunk + 255) / 256) + 2)) || (st = dalloc(c, &a.acc, 4)))
+    return fail(st);
+  if ((st = dalloc(c, &a.P, (size_t)a.ldc * a.ldc))) return fail(st);
+  // potential tiles: upper triangle of 64x64 tiles, split over points
+  a.nt = (int)(a.ldc / kTile);
+  a.ntiles = a.nt * (a.nt + 1) / 2;
+  {
+    std::vector<int2> tl;
+    std::vector<int> tof((size_t)a.nt * a.nt, -1);
+    for (int I = 0; I < a.nt; ++I)
+      for (int J = I; J < a.nt; ++J) {
+        tof[(size_t)I * a.nt + J] = (int)tl.size();
+        tl.push_back(make_int2(I, J));
+      }
+    int2* dtl;
+    int* dtof;
+    if ((st = dalloc(c, &dtl, tl.size())) || (st = dalloc(c, &dtof, tof.size()))) return fail(st);
+    CUDA_TRY(c, cudaMemcpy(dtl, tl.data(), tl.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    CUDA_TRY(c, cudaMemcpy(dtof, tof.data(), tof.size() * sizeof(int), cudaMemcpyHostToDevice));
+    a.tiles = dtl;
+    a.tile_of = dtof;
+  }
+  {
+    int ns = (int)std::max<int64_t>(1, (2 * 148 + a.ntiles - 1) / a.ntiles);
+    ns = (int)std::min<int64_t>(ns, std::max<int64_t>(1, chunk / 256));
+    while (chunk % (16LL * ns) != 0 && ns > 1) --ns;
+    a.nsplit = ns;
+    a.kspan = chunk / ns;
+  }
+  if ((st = dalloc(c, &a.vpart, (size_t)a.nsplit * a.ntiles * kTile * kTile))) return fail(st);
+  if ((st = dalloc(c, &c->d_ham, (size_t)o.ispin * c->nbas * (c->nbas + 1) / 2))) return fail(st);
+  CUDA_TRY(c, cudaMallocHost(&c->h_ham, sizeof(double) * o.ispin * c->nbas * (c->nbas + 1) / 2));
+  CUDA_TRY(c, cudaMallocHost(&c->h_acc, sizeof(double) * 4));
+  if (o.precision != PGXC_PREC_FP64) {
+    st = mixed_create(&c->mixed, a, c->nbas, gga, o.precision, c->err);
+    if (st) return fail(st);
+  }
+  *out = c;
+  return PGXC_OK;
+}
+
+// Ensure C / occ buffers for nocc orbitals.
+static int ensure_occ(pgxc_ctx* c, int nocc) {
+  const int kpad = (int)round_up(std::max(nocc, 1), 16);
+  if (kpad <= c->nocc_cap) return PGXC_OK;
+  BuildArgs& a = c->a;
+  double *C, *Cocc, *occ;
+  int st;
+  if ((st = dalloc(c, &C, (size_t)kpad * a.ldc)) || (st = dalloc(c, &Cocc, (size_t)kpad * a.ldc)) ||
+      (st = dalloc(c, &occ, kpad)))
+    return st;
+  a.C = C;
+  a.Cocc = Cocc;
+  a.occ = occ;
+  c->nocc_cap = kpad;
+  return PGXC_OK;
+}
+
+// The device part of a build; C / occ already in a.C / a.occ (padded).
+static int run_build(pgxc_ctx* c, int nocc, pgxc_timings* tm) {
+  BuildArgs& a = c->a;
+  cudaStream_t s = c->stream;
+  const bool gga = c->opt.functional == PGXC_XC_PBE;
+  const int64_t kpad = round_up(std::max(nocc, 1), 16);
+  float t_basis = 0, t_dens = 0, t_func = 0, t_pot = 0, t_x = 0, t_v = 0;
+  int64_t launches = 0;
+  CUDA_TRY(c, cudaMemsetAsync(a.acc, 0, 4 * sizeof(double), s));
+  CUDA_TRY(c, cudaMemsetAsync(a.vpart, 0, sizeof(double) * a.nsplit * a.ntiles * kTile * kTile, s));
+  CUDA_TRY(c, cudaEventRecord(c->ev[1], s));
+  launch_pmat_f64(a, kpad, s);
+  launches += 2;
+  if (c->mixed) launches += mixed_prepare(c->mixed, a, s);
+  CUDA_TRY(c, cudaGetLastError());
+  CUDA_TRY(c, cudaEventRecord(c->ev[2], s));
+  float ms;
+  CUDA_TRY(c, cudaEventSynchronize(c->ev[2]));
+  CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev[1], c->ev[2]));
+  t_dens += ms;
+  for (int64_t p0 = 0; p0 < c->npts; p0 += c->chunk) {
+    const int64_t nv = std::min<int64_t>(c->chunk, c->npts - p0);
+    CUDA_TRY(c, cudaEventRecord(c->ev[3], s));
+    if (c->mixed) launches += mixed_basis(c->mixed, a, p0, nv, gga, s);
+    else { launch_basis_f64(a, p0, nv, gga, s); launches += 1; }
+    CUDA_TRY(c, cudaEventRecord(c->ev[4], s));
+    CUDA_TRY(c, cudaEventRecord(c->kev[0], s));
+    if (c->mixed) launches += mixed_density(c->mixed, a, gga, s);
+    else { launch_density_f64(a, gga, s); launches += 1; }
+    CUDA_TRY(c, cudaEventRecord(c->kev[1], s));
+    CUDA_TRY(c, cudaEventRecord(c->ev[5], s));
+    launch_functional_f64(a, p0, nv, gga, s);
+    launches += 2;
+    CUDA_TRY(c, cudaEventRecord(c->ev[6], s));
+    if (c->mixed) {
+      launches += mixed_potential(c->mixed, a, gga, s, c->kev[2], c->kev[3]);
+    } else {
+      launch_zbuild_f64(a, gga, s);
+      CUDA_TRY(c, cudaEventRecord(c->kev[2], s));
+      launch_vpot_f64(a, gga, s);
+      CUDA_TRY(c, cudaEventRecord(c->kev[3], s));
+      launches += 2;
+    }
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaEventRecord(c->ev[7], s));
+    CUDA_TRY(c, cudaEventSynchronize(c->ev[7]));
+    CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev[3], c->ev[4])); t_basis += ms;
+    CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev[4], c->ev[5])); t_dens += ms;
+    CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev[5], c->ev[6])); t_func += ms;
+    CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev[6], c->ev[7])); t_pot += ms;
+    CUDA_TRY(c, cudaEventElapsedTime(&ms, c->kev[0], c->kev[1])); t_x += ms;
+    CUDA_TRY(c, cudaEventElapsedTime(&ms, c->kev[2], c->kev[3])); t_v += ms;
+  }
+  CUDA_TRY(c, cudaEventRecord(c->ev[3], s));
+  if (c->mixed) launches += mixed_pack(c->mixed, a, c->nbas, c->opt.ispin, 0, c->d_ham, s);
+  else { launch_pack(a, c->nbas, c->opt.ispin, 0, c->d_ham, s); launches += 1; }
+  CUDA_TRY(c, cudaGetLastError());
+  CUDA_TRY(c, cudaEventRecord(c->ev[4], s));
+  CUDA_TRY(c, cudaEventSynchronize(c->ev[4]));
+  CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev[3], c->ev[4]));
+  t_pot += ms;
+  if (tm) {
+    tm->basis_ms = t_basis;
+    tm->density_ms = t_dens;
+    tm->functional_ms = t_func;
+    tm->potential_ms = t_pot;
+    tm->xgemm_ms = t_x;
+    tm->vgemm_ms = t_v;
+    tm->kernel_launches = launches;
+  }
+  return PGXC_OK;
+}
+
+static int check_build_args(pgxc_ctx* c, int32_t nbas, int32_t nocc, int32_t ispin, int64_t xc_length) {
+  if (nbas != c->nbas) return set_err(c, PGXC_EINVAL, "nbas does not match the context's basis");
+  if (ispin != c->opt.ispin) return set_err(c, PGXC_EINVAL, "ispin does not match the context");
+  if (nocc < 0) return set_err(c, PGXC_EINVAL, "nocc < 0");
+  if (xc_length != (int64_t)ispin * nbas * (nbas + 1) / 2)
+    return set_err(c, PGXC_EINVAL, "xc_length must be ispin*nbas*(nbas+1)/2");
+  return PGXC_OK;
+}
+
+int pgxc_build(pgxc_ctx* c, const double* C, const double* occ, int32_t nbas, int32_t nocc, int32_t ispin,
+               double* ham, int64_t xc_length, double* exc, double* nel, pgxc_timings* tm) {
+  if (!c) return set_err(nullptr, PGXC_EINVAL, "ctx is NULL");
+  int st = check_build_args(c, nbas, nocc, ispin, xc_length);
+  if (st) return st;
+  if (!ham || !exc || !nel || (nocc > 0 && (!C || !occ))) return set_err(c, PGXC_EINVAL, "NULL output/input");
+  if (!all_finite(C, (int64_t)nbas * nocc * ispin) || !all_finite(occ, (int64_t)nocc * ispin))
+    return set_err(c, PGXC_ENONFINITE, "non-finite C or occ");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  if ((st = ensure_occ(c, nocc))) return st;
+  BuildArgs& a = c->a;
+  cudaStream_t s = c->stream;
+  const int64_t kpad = round_up(std::max(nocc, 1), 16);
+  CUDA_TRY(c, cudaEventRecord(c->ev[0], s));
+  CUDA_TRY(c, cudaMemsetAsync(a.C, 0, sizeof(double) * kpad * a.ldc, s));
+  CUDA_TRY(c, cudaMemsetAsync((double*)a.occ, 0, sizeof(double) * kpad, s));
+  if (nocc > 0) {
+    CUDA_TRY(c, cudaMemcpy2DAsync(a.C, sizeof(double) * a.ldc, C, sizeof(double) * nbas, sizeof(double) * nbas, nocc,
+                                  cudaMemcpyHostToDevice, s));
+    CUDA_TRY(c, cudaMemcpyAsync((double*)a.occ, occ, sizeof(double) * nocc, cudaMemcpyHostToDevice, s));
+  }
+  CUDA_TRY(c, cudaEventRecord(c->ev[1], s));
+  CUDA_TRY(c, cudaEventSynchronize(c->ev[1]));
+  float h2d = 0;
+  CUDA_TRY(c, cudaEventElapsedTime(&h2d, c->ev[0], c->ev[1]));
+  pgxc_timings local{};
+  if ((st = run_build(c, nocc, &local))) return st;
+  // D2H of the packed matrix and the two sums
+  cudaEvent_t e0 = c->ev[5], e1 = c->ev[6];
+  CUDA_TRY(c, cudaEventRecord(e0, s));
+  CUDA_TRY(c, cudaMemcpyAsync(c->h_ham, c->d_ham, sizeof(double) * xc_length, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaMemcpyAsync(c->h_acc, a.acc, sizeof(double) * 4, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaEventRecord(e1, s));
+  CUDA_TRY(c, cudaEventSynchronize(e1));
+  float d2h = 0, tot = 0;
+  CUDA_TRY(c, cudaEventElapsedTime(&d2h, e0, e1));
+  CUDA_TRY(c, cudaEventElapsedTime(&tot, c->ev[0], e1));
+  if (!std::isfinite(c->h_acc[0]) || !std::isfinite(c->h_acc[2]))
+    return set_err(c, PGXC_ENONFINITE, "non-finite E_xc or N_el");
+  for (int64_t i = 0; i < xc_length; ++i) ham[i] += c->h_ham[i];
+  *exc += c->h_acc[0];
+  *nel += c->h_acc[2];
+  if (tm) {
+    *tm = local;
+    tm->h2d_ms = h2d;
+    tm->d2h_ms = d2h;
+    tm->total_ms = tot;
+  }
+  return PGXC_OK;
+}
+
+int pgxc_build_device(pgxc_ctx* c, const double* d_C, const double* d_occ, int32_t nbas, int32_t nocc, int32_t ispin,
+                      double* d_ham, int64_t xc_length, double* d_exc_nel, pgxc_timings* tm) {
+  if (!c) return set_err(nullptr, PGXC_EINVAL, "ctx is NULL");
+  int st = check_build_args(c, nbas, nocc, ispin, xc_length);
+  if (st) return st;
+  if (!d_ham || !d_exc_nel || (nocc > 0 && (!d_C || !d_occ))) return set_err(c, PGXC_EINVAL, "NULL pointer");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  if ((st = ensure_occ(c, nocc))) return st;
+  BuildArgs& a = c->a;
+  cudaStream_t s = c->stream;
+  const int64_t kpad = round_up(std::max(nocc, 1), 16);
+  CUDA_TRY(c, cudaEventRecord(c->ev[0], s));
+  CUDA_TRY(c, cudaMemsetAsync(a.C, 0, sizeof(double) * kpad * a.ldc, s));
+  CUDA_TRY(c, cudaMemsetAsync((double*)a.occ, 0, sizeof(double) * kpad, s));
+  if (nocc > 0) {
+    CUDA_TRY(c, cudaMemcpy2DAsync(a.C, sizeof(double) * a.ldc, d_C, sizeof(double) * nbas, sizeof(double) * nbas,
+                                  nocc, cudaMemcpyDeviceToDevice, s));
+    CUDA_TRY(c, cudaMemcpyAsync((double*)a.occ, d_occ, sizeof(double) * nocc, cudaMemcpyDeviceToDevice, s));
+  }
+  pgxc_timings local{};
+  if ((st = run_build(c, nocc, &local))) return st;
+  CUDA_TRY(c, cudaMemcpyAsync(d_ham, c->d_ham, sizeof(double) * xc_length, cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(c, cudaMemcpyAsync(d_exc_nel, a.acc, sizeof(double), cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(c, cudaMemcpyAsync(d_exc_nel + 1, a.acc + 2, sizeof(double), cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(c, cudaEventRecord(c->ev[1], s));
+  CUDA_TRY(c, cudaEventSynchronize(c->ev[1]));
+  float tot = 0;
+  CUDA_TRY(c, cudaEventElapsedTime(&tot, c->ev[0], c->ev[1]));
+  if (tm) {
+    *tm = local;
+    tm->total_ms = tot;
+  }
+  return PGXC_OK;
+}
+
+int pgxc_grid_weights(const pgxc_ctx* cc, double* w_out, int64_t npts) {
+  pgxc_ctx* c = const_cast<pgxc_ctx*>(cc);
+  if (!c || !w_out) return set_err(c, PGXC_EINVAL, "NULL argument");
+  if (npts != c->npts) return set_err(c, PGXC_EINVAL, "npts mismatch");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  CUDA_TRY(c, cudaMemcpy(w_out, c->a.w, sizeof(double) * npts, cudaMemcpyDeviceToHost));
+  return PGXC_OK;
+}
+
+int pgxc_orbital_calculate(pgxc_ctx* c, int64_t npts, const double* pts, double* phi, double* grads) {
+  if (!c || !pts || !phi || npts < 0) return set_err(c, PGXC_EINVAL, "bad arguments");
+  if (npts == 0) return PGXC_OK;
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  const int64_t nb = c->nbas;
+  double *dp, *dphi, *dg = nullptr;
+  // temporary buffers: owned by this call
+  CUDA_TRY(c, cudaMalloc(&dp, sizeof(double) * 3 * npts));
+  cudaError_t e = cudaMalloc(&dphi, sizeof(double) * nb * npts);
+  if (e == cudaSuccess && grads) e = cudaMalloc(&dg, sizeof(double) * 3 * nb * npts);
+  int st = PGXC_OK;
+  if (e != cudaSuccess) st = set_err(c, PGXC_ENOMEM, "cudaMalloc failed in pgxc_orbital_calculate");
+  if (!st) {
+    cudaMemcpyAsync(dp, pts, sizeof(double) * 3 * npts, cudaMemcpyHostToDevice, c->stream);
+    launch_basis_points_f64(c->a, dp, dp + npts, dp + 2 * npts, npts, npts, dphi, grads ? dg : nullptr,
+                            grads ? dg + nb * npts : nullptr, grads ? dg + 2 * nb * npts : nullptr, c->stream);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) st = set_err(c, PGXC_ECUDA, std::string("basis kernel: ") + cudaGetErrorString(e));
+  }
+  if (!st) {
+    // device layout [f][p] is already phi(npts, nbas) column-major
+    cudaMemcpy(phi, dphi, sizeof(double) * nb * npts, cudaMemcpyDeviceToHost);
+    if (grads) {
+      // device [c][f][p] -> Fortran (npts, 3, nbas): element (p, c, f) at p + npts*(c + 3 f)
+      std::vector<double> tmp((size_t)3 * nb * npts);
+      cudaMemcpy(tmp.data(), dg, sizeof(double) * 3 * nb * npts, cudaMemcpyDeviceToHost);
+      for (int cc2 = 0; cc2 < 3; ++cc2)
+        for (int64_t f = 0; f < nb; ++f)
+          std::memcpy(grads + npts * (cc2 + 3 * f), tmp.data() + (cc2 * nb + f) * npts, sizeof(double) * npts);
+    }
+  }
+  cudaFree(dp);
+  cudaFree(dphi);
+  if (dg) cudaFree(dg);
+  return st;
+}
+
+int pgxc_xc_functionals(int32_t functional, int32_t ispin, int64_t n, const double* rho, const double* gam, double* f,
+                        double* fr, double* fg) {
+  if (functional != PGXC_XC_VWN && functional != PGXC_XC_PBE) return set_err(nullptr, PGXC_EINVAL, "functional");
+  if (ispin != 1) return set_err(nullptr, PGXC_ENOTSUP, "only ispin=1 point functionals are implemented");
+  if (n < 0 || !rho || !f || !fr) return set_err(nullptr, PGXC_EINVAL, "bad arguments");
+  const bool gga = functional == PGXC_XC_PBE;
+  if (gga && (!gam || !fg)) return set_err(nullptr, PGXC_EINVAL, "PBE needs gam and fg");
+  if (n == 0) return PGXC_OK;
+  int st = check_device(nullptr, -1);
+  if (st) return st;
+  double* d;
+  if (cudaMalloc(&d, sizeof(double) * 5 * n) != cudaSuccess) return set_err(nullptr, PGXC_ENOMEM, "cudaMalloc");
+  cudaMemcpy(d, rho, sizeof(double) * n, cudaMemcpyHostToDevice);
+  if (gga) cudaMemcpy(d + n, gam, sizeof(double) * n, cudaMemcpyHostToDevice);
+  launch_xc_points(functional, n, d, d + n, d + 2 * n, d + 3 * n, d + 4 * n, 0);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) {
+    cudaMemcpy(f, d + 2 * n, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(fr, d + 3 * n, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    if (gga) cudaMemcpy(fg, d + 4 * n, sizeof(double) * n, cudaMemcpyDeviceToHost);
+  }
+  cudaFree(d);
+  if (e != cudaSuccess) return set_err(nullptr, PGXC_ECUDA, cudaGetErrorString(e));
+  return PGXC_OK;
+}
+
+int pgxc_becke_weights(const pgxc_geometry* geo, int64_t npts, const double* pts, const int32_t* point_atom,
+                       double* w_out) {
+  if (!geo || geo->natoms <= 0 || !geo->coords || npts < 0 || !pts || !point_atom || !w_out)
+    return set_err(nullptr, PGXC_EINVAL, "bad arguments");
+  for (int64_t i = 0; i < npts; ++i)
+    if (point_atom[i] < 0 || point_atom[i] >= geo->natoms) return set_err(nullptr, PGXC_EINVAL, "point_atom range");
+  if (npts == 0) return PGXC_OK;
+  int st = check_device(nullptr, -1);
+  if (st) return st;
+  const int natm = geo->natoms;
+  double *d, *datoms, *ddist;
+  int* downer;
+  if (cudaMalloc(&d, sizeof(double) * 4 * npts) != cudaSuccess) return set_err(nullptr, PGXC_ENOMEM, "cudaMalloc");
+  cudaMalloc(&datoms, sizeof(double) * 3 * natm);
+  cudaMalloc(&ddist, sizeof(double) * natm * natm);
+  cudaMalloc(&downer, sizeof(int) * npts);
+  cudaMemcpy(d, pts, sizeof(double) * 3 * npts, cudaMemcpyHostToDevice);
+  cudaMemcpy(datoms, geo->coords, sizeof(double) * 3 * natm, cudaMemcpyHostToDevice);
+  cudaMemcpy(downer, point_atom, sizeof(int) * npts, cudaMemcpyHostToDevice);
+  launch_becke(datoms, ddist, natm, d, d + npts, d + 2 * npts, downer, npts, d + 3 * npts, 0);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) cudaMemcpy(w_out, d + 3 * npts, sizeof(double) * npts, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  cudaFree(datoms);
+  cudaFree(ddist);
+  cudaFree(downer);
+  if (e != cudaSuccess) return set_err(nullptr, PGXC_ECUDA, cudaGetErrorString(e));
+  return PGXC_OK;
+}
+
+}  // extern "C"

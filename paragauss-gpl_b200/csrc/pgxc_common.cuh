@@ -1,0 +1,44 @@
+// pgxc_common.cuh -- shared device-side definitions of libpgxc.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/pgxc.h"
+
+namespace pgxc {
+
+// Maximum angular momentum handled by the basis kernels (f functions).
+constexpr int kMaxL = 3;
+// Radial functions evaluated per pass of the basis kernel; shells with more
+// radial functions are processed in several passes.
+constexpr int kRadGroup = 8;
+
+// One (atom, l) shell of the orbital basis, device copy.
+struct DevShell {
+  int atom;
+  int l;
+  int nexp;
+  int nunc;
+  int ncontr;
+  int nrad;      // nunc + ncontr
+  int exp_off;   // into exponents / norms
+  int con_off;   // into contractions (nexp x ncontr column-major)
+  int f0;        // first basis function
+  int pad_;
+  double min_exp;  // smallest exponent: bounds the shell's spatial extent
+};
+
+// Symmetry adaptation: independent function i of shell l is
+// sum_m sa[l][i][m] Y_lm; identity when sa_identity is set.
+struct DevSA {
+  double c[kMaxL + 1][2 * kMaxL + 1][2 * kMaxL + 1];
+  int identity;
+};
+
+// Tile size of the potential/density-matrix blocking (functions).
+constexpr int kTile = 64;
+
+inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
+
+}  // namespace pgxc

@@ -79,6 +79,8 @@ class Timings(ct.Structure):
         ("potential_ms", ct.c_double),
         ("d2h_ms", ct.c_double),
         ("total_ms", ct.c_double),
+        ("xgemm_ms", ct.c_double),
+        ("vgemm_ms", ct.c_double),
         ("kernel_launches", ct.c_int64),
     ]
 

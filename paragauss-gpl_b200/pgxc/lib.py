@@ -1,0 +1,166 @@
+"""ctypes binding of libpgxc.so (the product).
+
+Loading fails loudly when the library is missing: there is no CPU fallback.
+"""
+import ctypes as ct
+import os
+
+import numpy as np
+
+from . import abi
+
+PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG, "libpgxc.so")
+_LIB = None
+
+
+class PgxcError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"pgxc status {status}: {msg}")
+        self.status = status
+
+
+def lib():
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with __graft_entry__.build() "
+                          "(nvcc, sm_100a); there is no CPU fallback")
+    L = ct.CDLL(LIB_PATH)
+    P = ct.POINTER
+    vp = ct.c_void_p
+    L.pgxc_default_options.argtypes = [P(abi.Options)]
+    L.pgxc_create.argtypes = [P(abi.Geometry), P(abi.Basis), P(abi.Grid), P(abi.Options), P(vp)]
+    L.pgxc_nbas.argtypes = [vp, P(ct.c_int32)]
+    L.pgxc_build.argtypes = [vp, abi._f64p, abi._f64p, ct.c_int32, ct.c_int32, ct.c_int32, abi._f64p, ct.c_int64,
+                             P(ct.c_double), P(ct.c_double), P(abi.Timings)]
+    L.pgxc_build_device.argtypes = [vp, vp, vp, ct.c_int32, ct.c_int32, ct.c_int32, vp, ct.c_int64, vp,
+                                    P(abi.Timings)]
+    L.pgxc_grid_weights.argtypes = [vp, abi._f64p, ct.c_int64]
+    L.pgxc_orbital_calculate.argtypes = [vp, ct.c_int64, abi._f64p, abi._f64p, abi._f64p]
+    L.pgxc_xc_functionals.argtypes = [ct.c_int32, ct.c_int32, ct.c_int64, abi._f64p, abi._f64p, abi._f64p,
+                                      abi._f64p, abi._f64p]
+    L.pgxc_becke_weights.argtypes = [P(abi.Geometry), ct.c_int64, abi._f64p, abi._i32p, abi._f64p]
+    L.pgxc_last_error.argtypes = [vp]
+    L.pgxc_last_error.restype = ct.c_char_p
+    L.pgxc_strerror.argtypes = [ct.c_int]
+    L.pgxc_strerror.restype = ct.c_char_p
+    L.pgxc_destroy.argtypes = [vp]
+    _LIB = L
+    return L
+
+
+def _check(st, ctx=None):
+    if st != 0:
+        msg = lib().pgxc_last_error(ctx)
+        raise PgxcError(st, (msg or b"").decode())
+
+
+class Context:
+    """One geometry: pgxc_create ... pgxc_destroy."""
+
+    def __init__(self, case, precision="fp64", weighted=True, device=-1, max_chunk_points=0,
+                 screen_threshold=0.0, batch_points=128):
+        L = lib()
+        self.case = case
+        self._m = abi.Marshalled(case, weighted=weighted)
+        o = abi.Options()
+        L.pgxc_default_options(ct.byref(o))
+        o.functional = abi.XC_IDS[case.functional]
+        o.ispin = case.ispin
+        o.precision = abi.PREC_IDS[precision]
+        o.device = device
+        o.max_chunk_points = max_chunk_points
+        o.screen_threshold = screen_threshold
+        o.batch_points = batch_points
+        self.opt = o
+        h = ct.c_void_p()
+        st = L.pgxc_create(ct.byref(self._m.geometry), ct.byref(self._m.basis), ct.byref(self._m.grid),
+                           ct.byref(o), ct.byref(h))
+        _check(st)
+        self.h = h
+        nb = ct.c_int32()
+        _check(L.pgxc_nbas(h, ct.byref(nb)), h)
+        self.nbas = nb.value
+
+    def build(self, C=None, occ=None, ham=None, timings=False):
+        """Returns (ham_xc_arr, exc, nel[, timings dict]); ham is accumulated into when given."""
+        c = self.case
+        Cf = c.c_fortran() if C is None else np.ascontiguousarray(C, dtype=np.float64).reshape(-1)
+        of = c.occ_fortran() if occ is None else np.ascontiguousarray(occ, dtype=np.float64).reshape(-1)
+        if ham is None:
+            ham = np.zeros(c.xc_length)
+        exc = ct.c_double(0.0)
+        nel = ct.c_double(0.0)
+        tm = abi.Timings()
+        st = lib().pgxc_build(self.h, abi.f64p(Cf), abi.f64p(of), c.nbas, c.nocc, c.ispin, abi.f64p(ham),
+                              c.xc_length, ct.byref(exc), ct.byref(nel), ct.byref(tm))
+        _check(st, self.h)
+        if timings:
+            return ham, exc.value, nel.value, tm.as_dict()
+        return ham, exc.value, nel.value
+
+    def build_device(self, d_C, d_occ, d_ham, d_exc_nel):
+        """Device-pointer build (ints); returns the timings dict."""
+        c = self.case
+        tm = abi.Timings()
+        st = lib().pgxc_build_device(self.h, d_C, d_occ, c.nbas, c.nocc, c.ispin, d_ham, c.xc_length, d_exc_nel,
+                                     ct.byref(tm))
+        _check(st, self.h)
+        return tm.as_dict()
+
+    def grid_weights(self):
+        w = np.zeros(self.case.npts)
+        _check(lib().pgxc_grid_weights(self.h, abi.f64p(w), len(w)), self.h)
+        return w
+
+    def orbitals(self, pts, grads=True):
+        pts = np.asarray(pts, dtype=np.float64)
+        n = len(pts)
+        p = np.ascontiguousarray(pts.T).reshape(-1)
+        phi = np.zeros(n * self.nbas)
+        gr = np.zeros(n * 3 * self.nbas) if grads else None
+        _check(lib().pgxc_orbital_calculate(self.h, n, abi.f64p(p), abi.f64p(phi), abi.f64p(gr)), self.h)
+        phi = phi.reshape(self.nbas, n).T
+        if grads:
+            gr = gr.reshape(self.nbas, 3, n).transpose(2, 1, 0)
+        return phi, gr
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().pgxc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def xc_functionals(xc, rho, gam=None):
+    rho = np.ascontiguousarray(rho, dtype=np.float64)
+    n = len(rho)
+    g = np.ascontiguousarray(gam, dtype=np.float64) if gam is not None else None
+    f = np.zeros(n)
+    fr = np.zeros(n)
+    fg = np.zeros(n) if g is not None else None
+    _check(lib().pgxc_xc_functionals(abi.XC_IDS[xc], 1, n, abi.f64p(rho), abi.f64p(g), abi.f64p(f), abi.f64p(fr),
+                                     abi.f64p(fg)))
+    return f, fr, fg
+
+
+def becke_weights(case):
+    m = abi.Marshalled(case, weighted=False)
+    pts = np.ascontiguousarray(case.grid_xyz.T).reshape(-1)
+    owner = np.ascontiguousarray(case.point_atom, dtype=np.int32)
+    w = np.zeros(case.npts)
+    _check(lib().pgxc_becke_weights(ct.byref(m.geometry), case.npts, abi.f64p(pts), abi.i32p(owner), abi.f64p(w)))
+    return w
