@@ -210,6 +210,33 @@ int pgxc_becke_weights(const pgxc_geometry* geo, int64_t npts,
                        const double* pts, const int32_t* point_atom,
                        double* w_out);
 
+/*
+ * Allocation-free Becke weights.  No counterpart in the reference: this is an
+ * extra entry for callers that cannot let a library allocate device memory
+ * (a driver whose device arrays all come from its own pool or OpenACC /
+ * CUDA Fortran data regions, or a process that reserved the whole device).
+ * Same result as pgxc_becke_weights, but every argument is device memory:
+ *   d_coords (natoms*3), d_pts (npts,3) column-major, d_point_atom (npts),
+ *   d_w_out (npts).
+ * The only scratch, the natoms x natoms distance matrix, lives in a fixed
+ * device array inside the library (PGXC_NOALLOC_MAX_ATOMS^2 doubles, 2 MiB,
+ * present on every GPU that loads the library until the process exits);
+ * natoms above PGXC_NOALLOC_MAX_ATOMS is rejected with PGXC_EINVAL.  It makes
+ * no cudaMalloc/cudaFree call.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  Work is queued on `stream` (a cudaStream_t, NULL for
+ * the legacy default stream) and the call returns without waiting: the
+ * weights are valid once that stream is synchronised.  All calls on a device
+ * share the scratch array, which keeps the last call's contents (each call
+ * rewrites every entry it reads): calls that overlap on the GPU race.
+ * Errors are reported through pgxc_last_error(NULL).
+ */
+#define PGXC_NOALLOC_MAX_ATOMS 512
+int pgxc_becke_weights_noalloc(int32_t natoms, const double* d_coords,
+                               int64_t npts, const double* d_pts,
+                               const int32_t* d_point_atom, double* d_w_out,
+                               void* stream);
+
 const char* pgxc_last_error(const pgxc_ctx* ctx);   /* ctx may be NULL */
 const char* pgxc_strerror(int status);
 

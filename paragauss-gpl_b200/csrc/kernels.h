@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 #include <cuda_runtime.h>
 
 #include "pgxc_common.cuh"
@@ -74,6 +75,9 @@ void launch_xc_points(int functional, int64_t n, const double* rho, const double
                       double* fg, cudaStream_t st);
 void launch_becke(const double* atoms, double* dist, int natm, const double* px, const double* py, const double* pz,
                   const int* owner, int64_t n, double* w, cudaStream_t st);
+// message returned by pgxc_last_error(NULL)
+void set_global_error(const std::string& msg);
+
 void launch_scale_inplace(double* x, const double* s, int64_t n, cudaStream_t st);
 
 }  // namespace pgxc

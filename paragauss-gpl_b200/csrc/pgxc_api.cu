@@ -98,6 +98,8 @@ bool all_finite(const double* p, int64_t n) {
 
 }  // namespace
 
+void pgxc::set_global_error(const std::string& msg) { g_err = msg; }
+
 extern "C" {
 
 void pgxc_default_options(pgxc_options* o) {
