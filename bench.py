@@ -40,7 +40,7 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="pgxc", choices=["pgxc", "reference"])
-    p.add_argument("--precision", default=None, help="fp64 | bf16x3 | tf32x3 (default: the headline path)")
+    p.add_argument("--precision", default=None, help="fp64 | mixed (default: the headline path)")
     p.add_argument("--config", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)

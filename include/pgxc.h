@@ -48,9 +48,11 @@ extern "C" {
 #define PGXC_XC_PBE 2
 
 /* ---- precision modes ------------------------------------------------- */
-#define PGXC_PREC_FP64        0  /* FP64 everywhere: the drop-in              */
-#define PGXC_PREC_MIXED_BF16  1  /* FP32 basis, split-BF16x3 tensor-core GEMMs */
-#define PGXC_PREC_MIXED_TF32  2  /* FP32 basis, split-TF32x3 tensor-core GEMMs */
+#define PGXC_PREC_FP64        0  /* FP64 everywhere (FP64 tensor pipe): the drop-in */
+/* FP32 basis; both contractions on the INT8 tensor cores with an Ozaki split
+   (4 signed 7-bit digits per operand, exact INT32 accumulation); FP64
+   functional and grid sums */
+#define PGXC_PREC_MIXED_INT8  1
 
 /* Geometry: unique_atoms(:)%position(1:3,1) in bohr, atom-major xyz triplets. */
 typedef struct pgxc_geometry {

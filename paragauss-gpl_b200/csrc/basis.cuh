@@ -16,12 +16,12 @@
 
 namespace pgxc {
 
-// Y[l*l + m] and dY[c][l*l + m], c = x, y, z, for l <= L.
-template <int L>
-__device__ __forceinline__ void solid_harmonics(double x, double y, double z, double* Y, double (*dY)[16]) {
-  const double r2 = x * x + y * y + z * z;
-  Y[0] = 1.0;
-  dY[0][0] = dY[1][0] = dY[2][0] = 0.0;
+// Y[l*l + m] and dY[c][l*l + m], c = x, y, z, for l <= L, in real type R.
+template <int L, typename R>
+__device__ __forceinline__ void solid_harmonics(R x, R y, R z, R* Y, R (*dY)[16]) {
+  const R r2 = x * x + y * y + z * z;
+  Y[0] = R(1);
+  dY[0][0] = dY[1][0] = dY[2][0] = R(0);
   if (L == 0) return;
   Y[1] = z; Y[2] = x; Y[3] = y;
   dY[0][1] = 0; dY[1][1] = 0; dY[2][1] = 1;
@@ -30,54 +30,54 @@ __device__ __forceinline__ void solid_harmonics(double x, double y, double z, do
 #pragma unroll
   for (int l = 2; l <= L; ++l) {
     const int o = l * l, o1 = (l - 1) * (l - 1), o2 = (l - 2) * (l - 2);
-    const double lr = l, l1r = l - 1, ll1r = 2 * l - 1;
-    const double dr2[3] = {2 * x, 2 * y, 2 * z};
+    const R lr = R(l), l1r = R(l - 1), ll1r = R(2 * l - 1);
+    const R dr2[3] = {R(2) * x, R(2) * y, R(2) * z};
     // m index 0
     {
-      const double p1 = Y[o1], p2 = Y[o2];
+      const R p1 = Y[o1], p2 = Y[o2];
       Y[o] = (ll1r * z * p1 - l1r * r2 * p2) / lr;
 #pragma unroll
       for (int c = 0; c < 3; ++c)
-        dY[c][o] = (ll1r * ((c == 2 ? p1 : 0.0) + z * dY[c][o1]) - l1r * (dr2[c] * p2 + r2 * dY[c][o2])) / lr;
+        dY[c][o] = (ll1r * ((c == 2 ? p1 : R(0)) + z * dY[c][o1]) - l1r * (dr2[c] * p2 + r2 * dY[c][o2])) / lr;
     }
 #pragma unroll
     for (int im = 1; im <= l - 2; ++im) {
-      const double sim = (double)(im * im);
-      const double rlm = 1.0 / sqrt(lr * lr - sim);
-      const double rl1m = sqrt(l1r * l1r - sim);
-      const double a = ll1r * z * rlm;
-      const double b = rl1m * r2 * rlm;
+      const R sim = (R)(im * im);
+      const R rlm = R(1) / sqrt(lr * lr - sim);
+      const R rl1m = sqrt(l1r * l1r - sim);
+      const R a = ll1r * z * rlm;
+      const R b = rl1m * r2 * rlm;
 #pragma unroll
       for (int mm = 2 * im - 1; mm <= 2 * im; ++mm) {
-        const double p1 = Y[o1 + mm], p2 = Y[o2 + mm];
+        const R p1 = Y[o1 + mm], p2 = Y[o2 + mm];
         Y[o + mm] = a * p1 - b * p2;
 #pragma unroll
         for (int c = 0; c < 3; ++c)
-          dY[c][o + mm] = (c == 2 ? ll1r * rlm * p1 : 0.0) + a * dY[c][o1 + mm] - rl1m * dr2[c] * rlm * p2 -
+          dY[c][o + mm] = (c == 2 ? ll1r * rlm * p1 : R(0)) + a * dY[c][o1 + mm] - rl1m * dr2[c] * rlm * p2 -
                           b * dY[c][o2 + mm];
       }
     }
     {
       const int im = l - 1;
-      const double rlm = 1.0 / sqrt(lr * lr - (double)(im * im));
-      const double a = ll1r * z * rlm;
+      const R rlm = R(1) / sqrt(lr * lr - (R)(im * im));
+      const R a = ll1r * z * rlm;
 #pragma unroll
       for (int mm = 2 * im - 1; mm <= 2 * im; ++mm) {
-        const double p1 = Y[o1 + mm];
+        const R p1 = Y[o1 + mm];
         Y[o + mm] = a * p1;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) dY[c][o + mm] = (c == 2 ? ll1r * rlm * p1 : 0.0) + a * dY[c][o1 + mm];
+        for (int c = 0; c < 3; ++c) dY[c][o + mm] = (c == 2 ? ll1r * rlm * p1 : R(0)) + a * dY[c][o1 + mm];
       }
     }
     {
-      const double rll = sqrt(ll1r / (2 * lr));
-      const double q2 = Y[o1 + 2 * l - 3], q1 = Y[o1 + 2 * l - 2];
+      const R rll = sqrt(ll1r / (R(2) * lr));
+      const R q2 = Y[o1 + 2 * l - 3], q1 = Y[o1 + 2 * l - 2];
       Y[o + 2 * l - 1] = (x * q2 - y * q1) * rll;
       Y[o + 2 * l] = (y * q2 + x * q1) * rll;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const double g2 = dY[c][o1 + 2 * l - 3], g1 = dY[c][o1 + 2 * l - 2];
-        const double dx = (c == 0), dy = (c == 1);
+        const R g2 = dY[c][o1 + 2 * l - 3], g1 = dY[c][o1 + 2 * l - 2];
+        const R dx = R(c == 0), dy = R(c == 1);
         dY[c][o + 2 * l - 1] = (dx * q2 + x * g2 - dy * q1 - y * g1) * rll;
         dY[c][o + 2 * l] = (dy * q2 + y * g2 + dx * q1 + x * g1) * rll;
       }
@@ -85,25 +85,45 @@ __device__ __forceinline__ void solid_harmonics(double x, double y, double z, do
   }
 }
 
-// Output element types: FP64 for the drop-in path, FP32 for the mixed path.
-template <typename T>
-__device__ __forceinline__ T cvt_out(double v) { return (T)v; }
+// One normalised primitive norm*exp(-alpha r^2), zero where alpha r^2 >= 50
+// (radial0/radial1, modules/orbital_module.f90:1823-1854).  In FP32 the
+// exponent alpha*r^2 (up to 50) would carry an absolute rounding error of
+// up to 50 * 2^-24 into exp; it is therefore formed in FP64 from the FP64 r^2
+// and split as 2^-t = 2^-k * 2^-f (k integer, |f| <= 1/2) before exp2f.
+__device__ __forceinline__ double prim_value(double alpha, double norm, double r2, double) {
+  const double ar2 = alpha * r2;
+  return ar2 < 50.0 ? norm * exp(-ar2) : 0.0;
+}
+__device__ __forceinline__ float prim_value(float, float norm, float, double ar2) {
+  if (!(ar2 < 50.0)) return 0.f;
+  const double t = ar2 * 1.4426950408889634;  // log2(e)
+  const double k = rint(t);
+  return norm * ldexpf(exp2f(-(float)(t - k)), -(int)k);
+}
 
 // Evaluate one shell at one point and store its (2l+1)*nrad functions (and
-// gradients when GRAD) at column p of the [function][ld] arrays.
-template <int L, bool GRAD, typename T>
-__device__ __forceinline__ void shell_at_point(const DevShell& S, const DevSA& sa, double x, double y, double z,
+// gradients when GRAD) at column p of the [function][ld] arrays.  R is the
+// arithmetic type (FP64 for the drop-in path, FP32 for the mixed path), T the
+// stored type.  With R = float, r2d is the FP64 r^2 used for the exponent.
+//
+// With STATS (all 32 lanes of the warp active, one point each), the largest
+// |phi| of this point is folded into *ptmax and the largest |phi| of each
+// function over the warp's points into fnmax[f] (shared memory, as the bit
+// pattern of a non-negative double, which orders like the value).
+template <int L, bool GRAD, typename T, typename R = double, bool STATS = false>
+__device__ __forceinline__ void shell_at_point(const DevShell& S, const DevSA& sa, R x, R y, R z,
                                                const double* __restrict__ exps, const double* __restrict__ norms,
                                                const double* __restrict__ contr, bool valid, int64_t p, int64_t ld,
                                                T* __restrict__ phi, T* __restrict__ gx, T* __restrict__ gy,
-                                               T* __restrict__ gz) {
+                                               T* __restrict__ gz, double r2d = 0.0, double* ptmax = nullptr,
+                                               unsigned long long* fnmax = nullptr) {
   constexpr int NY = (L + 1) * (L + 1);
-  double Y[16];
-  double dY[3][16];
-  solid_harmonics<L>(x, y, z, Y, dY);
-  const double r2 = x * x + y * y + z * z;
+  R Y[16];
+  R dY[3][16];
+  solid_harmonics<L, R>(x, y, z, Y, dY);
+  const R r2 = x * x + y * y + z * z;
   // symmetry-adapted harmonics of this l
-  double Ys[2 * L + 1], dYs[3][2 * L + 1];
+  R Ys[2 * L + 1], dYs[3][2 * L + 1];
 #pragma unroll
   for (int i = 0; i < 2 * L + 1; ++i) {
     if (sa.identity) {
@@ -111,10 +131,10 @@ __device__ __forceinline__ void shell_at_point(const DevShell& S, const DevSA& s
 #pragma unroll
       for (int c = 0; c < 3; ++c) dYs[c][i] = dY[c][L * L + i];
     } else {
-      double v = 0, g0 = 0, g1 = 0, g2 = 0;
+      R v = 0, g0 = 0, g1 = 0, g2 = 0;
 #pragma unroll
       for (int m = 0; m < 2 * L + 1; ++m) {
-        const double cf = sa.c[L][i][m];
+        const R cf = (R)sa.c[L][i][m];
         v += cf * Y[L * L + m];
         g0 += cf * dY[0][L * L + m];
         g1 += cf * dY[1][L * L + m];
@@ -128,24 +148,23 @@ __device__ __forceinline__ void shell_at_point(const DevShell& S, const DevSA& s
   const double* nr = norms + S.exp_off;
   const double* cc = contr + S.con_off;
   for (int r0 = 0; r0 < S.nrad; r0 += kRadGroup) {
-    double R[kRadGroup], dR[kRadGroup];
+    R Rr[kRadGroup], dR[kRadGroup];
 #pragma unroll
-    for (int r = 0; r < kRadGroup; ++r) { R[r] = 0.0; dR[r] = 0.0; }
+    for (int r = 0; r < kRadGroup; ++r) { Rr[r] = R(0); dR[r] = R(0); }
     if (valid) {
       for (int e = 0; e < S.nexp; ++e) {
-        const double alpha = __ldg(ex + e);
-        const double ar2 = alpha * r2;
-        double v = 0.0;
-        if (ar2 < 50.0) v = __ldg(nr + e) * exp(-ar2);
-        const double dv = (-2.0 * alpha) * v;
+        const double alpha_d = __ldg(ex + e);
+        const R alpha = (R)alpha_d;
+        const R v = prim_value(alpha, (R)__ldg(nr + e), r2, alpha_d * r2d);
+        const R dv = (R(-2) * alpha) * v;
 #pragma unroll
         for (int r = 0; r < kRadGroup; ++r) {
           const int rr = r0 + r;
           if (rr < S.nrad) {
-            double cf;
-            if (rr < S.nunc) cf = (e == rr) ? 1.0 : 0.0;
-            else cf = __ldg(cc + e + (int64_t)S.nexp * (rr - S.nunc));
-            R[r] += cf * v;
+            R cf;
+            if (rr < S.nunc) cf = (e == rr) ? R(1) : R(0);
+            else cf = (R)__ldg(cc + e + (int64_t)S.nexp * (rr - S.nunc));
+            Rr[r] += cf * v;
             dR[r] += cf * dv;
           }
         }
@@ -158,12 +177,19 @@ __device__ __forceinline__ void shell_at_point(const DevShell& S, const DevSA& s
         const int rr = r0 + r;
         if (rr < S.nrad) {
           const int64_t f = S.f0 + (int64_t)i * S.nrad + rr;
-          phi[f * ld + p] = cvt_out<T>(Ys[i] * R[r]);
+          phi[f * ld + p] = (T)(Ys[i] * Rr[r]);
+          if (STATS) {
+            double a = fabs((double)(Ys[i] * Rr[r]));
+            *ptmax = fmax(*ptmax, a);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
+            if ((threadIdx.x & 31) == 0) atomicMax(fnmax + f, (unsigned long long)__double_as_longlong(a));
+          }
           if (GRAD) {
-            const double h = Ys[i] * dR[r];
-            gx[f * ld + p] = cvt_out<T>(x * h + dYs[0][i] * R[r]);
-            gy[f * ld + p] = cvt_out<T>(y * h + dYs[1][i] * R[r]);
-            gz[f * ld + p] = cvt_out<T>(z * h + dYs[2][i] * R[r]);
+            const R h = Ys[i] * dR[r];
+            gx[f * ld + p] = (T)(x * h + dYs[0][i] * Rr[r]);
+            gy[f * ld + p] = (T)(y * h + dYs[1][i] * Rr[r]);
+            gz[f * ld + p] = (T)(z * h + dYs[2][i] * Rr[r]);
           }
         }
       }

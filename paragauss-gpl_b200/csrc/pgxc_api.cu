@@ -223,7 +223,7 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
     return fail(set_err(c, PGXC_EINVAL, "unknown functional id"));
   if (o.ispin != 1 && o.ispin != 2) return fail(set_err(c, PGXC_EINVAL, "ispin must be 1 or 2"));
   if (o.ispin == 2) return fail(set_err(c, PGXC_ENOTSUP, "open-shell (ispin=2) builds are not implemented yet"));
-  if (o.precision < PGXC_PREC_FP64 || o.precision > PGXC_PREC_MIXED_TF32)
+  if (o.precision != PGXC_PREC_FP64 && o.precision != PGXC_PREC_MIXED_INT8)
     return fail(set_err(c, PGXC_EINVAL, "unknown precision mode"));
   if (!grid || grid->npts <= 0 || !grid->grdpts) return fail(set_err(c, PGXC_EINVAL, "empty grid"));
   if (grid->weights_are_raw && !grid->point_atom)
@@ -303,18 +303,28 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
     launch_scale_inplace(dgrid + 3 * n, dbecke, n, c->stream);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   }
-  // chunk sizing
+  // potential tiles of the FP64 path and their split over points
   a.ldc = round_up(c->nbas, kTile);
+  a.nt = (int)(a.ldc / kTile);
+  a.ntiles = a.nt * (a.nt + 1) / 2;
+  const int ns64 = (int)std::min<int64_t>(8, std::max<int64_t>(1, (2 * 148 + a.ntiles - 1) / a.ntiles));
+  // chunk sizing: balanced chunks of at most max_chunk points, each a
+  // multiple of 128 * ns64 (CTA rows of both paths, 16-point K slabs per split)
   const bool gga = o.functional == PGXC_XC_PBE;
   size_t freeb = 0, totb = 0;
   CUDA_TRY(c, cudaMemGetInfo(&freeb, &totb));
   const int64_t arrays = gga ? 5 : 2;
-  const int64_t per_pt = a.ldc * 8 * arrays + 8 * 10;
-  int64_t chunk = (int64_t)(0.30 * (double)freeb) / per_pt;
-  chunk = std::min<int64_t>(chunk, 1 << 19);
-  if (o.max_chunk_points > 0) chunk = std::min<int64_t>(chunk, o.max_chunk_points);
-  chunk = std::min<int64_t>(chunk, round_up(n, 64));
-  chunk = std::max<int64_t>(64, chunk / 64 * 64);
+  // FP64 path: phi (+ 3 gradients) and Z in FP64; mixed path: the same in FP64
+  // plus three 5-byte operand tile sets
+  const int64_t row_bytes = o.precision == PGXC_PREC_FP64 ? a.ldc * 8 : round_up(c->nbas, mixed_row_align()) * 8;
+  const int64_t per_pt = row_bytes * arrays + (o.precision == PGXC_PREC_FP64 ? 0 : round_up(c->nbas, mixed_row_align()) * 15) + 8 * 10;
+  const int64_t align = 128LL * ns64;
+  int64_t max_chunk = (int64_t)(0.30 * (double)freeb) / per_pt;
+  max_chunk = std::min<int64_t>(max_chunk, 1 << 19);
+  if (o.max_chunk_points > 0) max_chunk = std::min<int64_t>(max_chunk, o.max_chunk_points);
+  max_chunk = std::max<int64_t>(align, max_chunk / align * align);
+  const int64_t nchunks = (n + max_chunk - 1) / max_chunk;
+  const int64_t chunk = round_up((n + nchunks - 1) / nchunks, align);
   c->chunk = chunk;
   a.ldp = chunk;
   if (o.precision == PGXC_PREC_FP64) {
@@ -339,8 +349,6 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
     return fail(st);
   if ((st = dalloc(c, &a.P, (size_t)a.ldc * a.ldc))) return fail(st);
   // potential tiles: upper triangle of 64x64 tiles, split over points
-  a.nt = (int)(a.ldc / kTile);
-  a.ntiles = a.nt * (a.nt + 1) / 2;
   {
     std::vector<int2> tl;
     std::vector<int> tof((size_t)a.nt * a.nt, -1);
@@ -357,13 +365,8 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
     a.tiles = dtl;
     a.tile_of = dtof;
   }
-  {
-    int ns = (int)std::max<int64_t>(1, (2 * 148 + a.ntiles - 1) / a.ntiles);
-    ns = (int)std::min<int64_t>(ns, std::max<int64_t>(1, chunk / 256));
-    while (chunk % (16LL * ns) != 0 && ns > 1) --ns;
-    a.nsplit = ns;
-    a.kspan = chunk / ns;
-  }
+  a.nsplit = ns64;
+  a.kspan = chunk / ns64;
   if ((st = dalloc(c, &a.vpart, (size_t)a.nsplit * a.ntiles * kTile * kTile))) return fail(st);
   if ((st = dalloc(c, &c->d_ham, (size_t)o.ispin * c->nbas * (c->nbas + 1) / 2))) return fail(st);
   CUDA_TRY(c, cudaMallocHost(&c->h_ham, sizeof(double) * o.ispin * c->nbas * (c->nbas + 1) / 2));
@@ -404,9 +407,12 @@ static int run_build(pgxc_ctx* c, int nocc, pgxc_timings* tm) {
   CUDA_TRY(c, cudaMemsetAsync(a.acc, 0, 4 * sizeof(double), s));
   CUDA_TRY(c, cudaMemsetAsync(a.vpart, 0, sizeof(double) * a.nsplit * a.ntiles * kTile * kTile, s));
   CUDA_TRY(c, cudaEventRecord(c->ev[1], s));
-  launch_pmat_f64(a, kpad, s);
-  launches += 2;
-  if (c->mixed) launches += mixed_prepare(c->mixed, a, s);
+  if (c->mixed) {
+    launches += mixed_prepare(c->mixed, a, nocc, s);
+  } else {
+    launch_pmat_f64(a, kpad, s);
+    launches += 2;
+  }
   CUDA_TRY(c, cudaGetLastError());
   CUDA_TRY(c, cudaEventRecord(c->ev[2], s));
   float ms;
@@ -454,6 +460,11 @@ static int run_build(pgxc_ctx* c, int nocc, pgxc_timings* tm) {
   CUDA_TRY(c, cudaEventSynchronize(c->ev[4]));
   CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev[3], c->ev[4]));
   t_pot += ms;
+  if (c->mixed) {
+    int flag = 0;
+    if (mixed_error_flag(c->mixed, s, &flag) != PGXC_OK) return set_err(c, PGXC_ECUDA, "error-flag read failed");
+    if (flag) return set_err(c, PGXC_ETIMEOUT, "a bounded tensor-core pipeline wait ran out");
+  }
   if (tm) {
     tm->basis_ms = t_basis;
     tm->density_ms = t_dens;

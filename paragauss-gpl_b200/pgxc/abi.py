@@ -21,9 +21,8 @@ XC_PBE = 2
 XC_IDS = {"VWN": XC_VWN, "PBE": XC_PBE}
 
 PREC_FP64 = 0
-PREC_MIXED_BF16 = 1
-PREC_MIXED_TF32 = 2
-PREC_IDS = {"fp64": PREC_FP64, "bf16x3": PREC_MIXED_BF16, "tf32x3": PREC_MIXED_TF32}
+PREC_MIXED_INT8 = 1
+PREC_IDS = {"fp64": PREC_FP64, "mixed": PREC_MIXED_INT8}
 
 _i32p = ct.POINTER(ct.c_int32)
 _f64p = ct.POINTER(ct.c_double)
