@@ -44,7 +44,10 @@ def parse():
     p.add_argument("--config", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
-    p.add_argument("--compare-fp64", action="store_true", default=True)
+    p.add_argument("--max-chunk-points", type=int, default=0,
+                   help="cap on grid points per device chunk (0: sized from free HBM)")
+    p.add_argument("--profile", action="store_true",
+                   help="one build only (for ncu): no warm-up loop, e2e, CPU baseline or peak probe")
     return p.parse_args()
 
 
@@ -254,7 +257,13 @@ def main():
     prec = args.precision or headline_precision()
     case = cases.config(args.config)
     sub = shard(case, rank, world)
-    ctx = lib.Context(sub, precision=prec, weighted=False, device=local)
+    ctx = lib.Context(sub, precision=prec, weighted=False, device=local, max_chunk_points=args.max_chunk_points)
+    if args.profile:
+        d = ctx.build(timings=True)
+        print(json.dumps({"profile": True, "precision": prec, "E_xc": d[1], "N_el": d[2], "timings": d[3]}),
+              flush=True)
+        ctx.close()
+        return
     weights = ctx.grid_weights()
     nb, nocc = case.nbas, case.nocc
     dC = torch.from_numpy(case.c_fortran()).cuda()

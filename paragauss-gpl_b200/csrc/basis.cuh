@@ -105,18 +105,13 @@ __device__ __forceinline__ float prim_value(float, float norm, float, double ar2
 // gradients when GRAD) at column p of the [function][ld] arrays.  R is the
 // arithmetic type (FP64 for the drop-in path, FP32 for the mixed path), T the
 // stored type.  With R = float, r2d is the FP64 r^2 used for the exponent.
-//
-// With STATS (all 32 lanes of the warp active, one point each), the largest
-// |phi| of this point is folded into *ptmax and the largest |phi| of each
-// function over the warp's points into fnmax[f] (shared memory, as the bit
-// pattern of a non-negative double, which orders like the value).
-template <int L, bool GRAD, typename T, typename R = double, bool STATS = false>
+// exps/norms/contr may point to shared memory (plain loads).
+template <int L, bool GRAD, typename T, typename R = double>
 __device__ __forceinline__ void shell_at_point(const DevShell& S, const DevSA& sa, R x, R y, R z,
-                                               const double* __restrict__ exps, const double* __restrict__ norms,
-                                               const double* __restrict__ contr, bool valid, int64_t p, int64_t ld,
+                                               const double* exps, const double* norms, const double* contr,
+                                               bool valid, int64_t p, int64_t ld,
                                                T* __restrict__ phi, T* __restrict__ gx, T* __restrict__ gy,
-                                               T* __restrict__ gz, double r2d = 0.0, double* ptmax = nullptr,
-                                               unsigned long long* fnmax = nullptr) {
+                                               T* __restrict__ gz, double r2d = 0.0) {
   constexpr int NY = (L + 1) * (L + 1);
   R Y[16];
   R dY[3][16];
@@ -153,9 +148,9 @@ __device__ __forceinline__ void shell_at_point(const DevShell& S, const DevSA& s
     for (int r = 0; r < kRadGroup; ++r) { Rr[r] = R(0); dR[r] = R(0); }
     if (valid) {
       for (int e = 0; e < S.nexp; ++e) {
-        const double alpha_d = __ldg(ex + e);
+        const double alpha_d = ex[e];
         const R alpha = (R)alpha_d;
-        const R v = prim_value(alpha, (R)__ldg(nr + e), r2, alpha_d * r2d);
+        const R v = prim_value(alpha, (R)nr[e], r2, alpha_d * r2d);
         const R dv = (R(-2) * alpha) * v;
 #pragma unroll
         for (int r = 0; r < kRadGroup; ++r) {
@@ -163,7 +158,7 @@ __device__ __forceinline__ void shell_at_point(const DevShell& S, const DevSA& s
           if (rr < S.nrad) {
             R cf;
             if (rr < S.nunc) cf = (e == rr) ? R(1) : R(0);
-            else cf = (R)__ldg(cc + e + (int64_t)S.nexp * (rr - S.nunc));
+            else cf = (R)cc[e + (int64_t)S.nexp * (rr - S.nunc)];
             Rr[r] += cf * v;
             dR[r] += cf * dv;
           }
@@ -178,13 +173,6 @@ __device__ __forceinline__ void shell_at_point(const DevShell& S, const DevSA& s
         if (rr < S.nrad) {
           const int64_t f = S.f0 + (int64_t)i * S.nrad + rr;
           phi[f * ld + p] = (T)(Ys[i] * Rr[r]);
-          if (STATS) {
-            double a = fabs((double)(Ys[i] * Rr[r]));
-            *ptmax = fmax(*ptmax, a);
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) a = fmax(a, __shfl_xor_sync(0xffffffffu, a, o));
-            if ((threadIdx.x & 31) == 0) atomicMax(fnmax + f, (unsigned long long)__double_as_longlong(a));
-          }
           if (GRAD) {
             const R h = Ys[i] * dR[r];
             gx[f * ld + p] = (T)(x * h + dYs[0][i] * Rr[r]);
@@ -195,6 +183,50 @@ __device__ __forceinline__ void shell_at_point(const DevShell& S, const DevSA& s
       }
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// K1: basis functions of the shells of one angular momentum L on a chunk of
+// points.  grid = (chunk/128, shells of this L), block = 128 points; the
+// shell's exponents, norms and contraction matrix are staged in shared
+// memory first (global memory for shells larger than the staging area).
+// ---------------------------------------------------------------------------
+constexpr int kStagePrim = 64;
+constexpr int kStageCon = 512;
+
+template <int L, bool GRAD, typename T>
+__global__ void __launch_bounds__(128) k_basis_l(const DevShell* __restrict__ shells, const int* __restrict__ ids,
+                                                 const double* __restrict__ atoms, const double* __restrict__ exps,
+                                                 const double* __restrict__ norms, const double* __restrict__ contr,
+                                                 DevSA sa, const double* __restrict__ px, const double* __restrict__ py,
+                                                 const double* __restrict__ pz, int64_t p0, int64_t nvalid, int64_t ld,
+                                                 T* __restrict__ phi, T* __restrict__ gx, T* __restrict__ gy,
+                                                 T* __restrict__ gz) {
+  __shared__ double s_exp[kStagePrim], s_nrm[kStagePrim], s_con[kStageCon];
+  DevShell S = shells[ids[blockIdx.y]];
+  const double *e_src = exps + S.exp_off, *n_src = norms + S.exp_off, *c_src = contr + S.con_off;
+  const bool staged = S.nexp <= kStagePrim && S.nexp * S.ncontr <= kStageCon;
+  if (staged) {
+    for (int i = threadIdx.x; i < S.nexp; i += blockDim.x) {
+      s_exp[i] = e_src[i];
+      s_nrm[i] = n_src[i];
+    }
+    for (int i = threadIdx.x; i < S.nexp * S.ncontr; i += blockDim.x) s_con[i] = c_src[i];
+    __syncthreads();
+    S.exp_off = 0;
+    S.con_off = 0;
+  }
+  const int64_t p = (int64_t)blockIdx.x * 128 + threadIdx.x;
+  if (p >= ld) return;
+  const bool valid = p < nvalid;
+  double x = 0, y = 0, z = 0;
+  if (valid) {
+    x = px[p0 + p] - atoms[3 * S.atom];
+    y = py[p0 + p] - atoms[3 * S.atom + 1];
+    z = pz[p0 + p] - atoms[3 * S.atom + 2];
+  }
+  shell_at_point<L, GRAD, T, double>(S, sa, x, y, z, staged ? s_exp : exps, staged ? s_nrm : norms,
+                                     staged ? s_con : contr, valid, p, ld, phi, gx, gy, gz);
 }
 
 }  // namespace pgxc

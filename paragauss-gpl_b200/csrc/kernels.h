@@ -15,6 +15,8 @@ struct BuildArgs {
   // basis
   const DevShell* shells = nullptr;
   int nshells = 0;
+  const int* shl[kMaxL + 1] = {};  // shell indices of each angular momentum
+  int nshl[kMaxL + 1] = {};
   const double* atoms = nullptr;
   const double* exps = nullptr;
   const double* norms = nullptr;
@@ -61,6 +63,9 @@ struct BuildArgs {
 };
 
 void launch_basis_f64(const BuildArgs& a, int64_t p0, int64_t nvalid, bool grad, cudaStream_t st);
+// basis values (and gradients) of every shell at points [p0, p0+ld) of (px,py,pz), FP64, [f][ld] layout
+void launch_basis(const BuildArgs& a, const double* px, const double* py, const double* pz, int64_t p0,
+                  int64_t nvalid, int64_t ld, double* phi, double* gx, double* gy, double* gz, cudaStream_t st);
 void launch_basis_points_f64(const BuildArgs& a, const double* px, const double* py, const double* pz, int64_t n,
                              int64_t ld, double* phi, double* gx, double* gy, double* gz, cudaStream_t st);
 void launch_pmat_f64(const BuildArgs& a, int64_t kpad, cudaStream_t st);

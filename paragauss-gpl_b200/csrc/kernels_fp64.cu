@@ -27,54 +27,38 @@
 namespace pgxc {
 
 // ---------------------------------------------------------------------------
-// K1: basis functions.  grid = (ceil(ld/128), nshells), block = 128 points.
+// K1: basis functions, one launch per angular momentum (k_basis_l, basis.cuh)
 // ---------------------------------------------------------------------------
-template <typename T, bool GRAD>
-__global__ void __launch_bounds__(128) k_basis(const DevShell* __restrict__ shells, const double* __restrict__ atoms,
-                                               const double* __restrict__ exps, const double* __restrict__ norms,
-                                               const double* __restrict__ contr, DevSA sa,
-                                               const double* __restrict__ px, const double* __restrict__ py,
-                                               const double* __restrict__ pz, int64_t p0, int64_t nvalid,
-                                               int64_t ld, T* __restrict__ phi, T* __restrict__ gx,
-                                               T* __restrict__ gy, T* __restrict__ gz) {
-  const int64_t p = (int64_t)blockIdx.x * 128 + threadIdx.x;
-  if (p >= ld) return;
-  const DevShell S = shells[blockIdx.y];
-  const bool valid = p < nvalid;
-  double x = 0, y = 0, z = 0;
-  if (valid) {
-    x = px[p0 + p] - atoms[3 * S.atom];
-    y = py[p0 + p] - atoms[3 * S.atom + 1];
-    z = pz[p0 + p] - atoms[3 * S.atom + 2];
-  }
-  switch (S.l) {
-    case 0: shell_at_point<0, GRAD, T>(S, sa, x, y, z, exps, norms, contr, valid, p, ld, phi, gx, gy, gz); break;
-    case 1: shell_at_point<1, GRAD, T>(S, sa, x, y, z, exps, norms, contr, valid, p, ld, phi, gx, gy, gz); break;
-    case 2: shell_at_point<2, GRAD, T>(S, sa, x, y, z, exps, norms, contr, valid, p, ld, phi, gx, gy, gz); break;
-    default: shell_at_point<3, GRAD, T>(S, sa, x, y, z, exps, norms, contr, valid, p, ld, phi, gx, gy, gz); break;
-  }
+template <int L>
+static void launch_basis_one_l(const BuildArgs& a, const double* px, const double* py, const double* pz, int64_t p0,
+                               int64_t nvalid, int64_t ld, double* phi, double* gx, double* gy, double* gz,
+                               cudaStream_t st) {
+  if (a.nshl[L] == 0) return;
+  dim3 grid((unsigned)((ld + 127) / 128), (unsigned)a.nshl[L]);
+  if (gx)
+    k_basis_l<L, true, double><<<grid, 128, 0, st>>>(a.shells, a.shl[L], a.atoms, a.exps, a.norms, a.contr, a.sa, px,
+                                                     py, pz, p0, nvalid, ld, phi, gx, gy, gz);
+  else
+    k_basis_l<L, false, double><<<grid, 128, 0, st>>>(a.shells, a.shl[L], a.atoms, a.exps, a.norms, a.contr, a.sa,
+                                                      px, py, pz, p0, nvalid, ld, phi, nullptr, nullptr, nullptr);
+}
+
+void launch_basis(const BuildArgs& a, const double* px, const double* py, const double* pz, int64_t p0,
+                  int64_t nvalid, int64_t ld, double* phi, double* gx, double* gy, double* gz, cudaStream_t st) {
+  launch_basis_one_l<0>(a, px, py, pz, p0, nvalid, ld, phi, gx, gy, gz, st);
+  launch_basis_one_l<1>(a, px, py, pz, p0, nvalid, ld, phi, gx, gy, gz, st);
+  launch_basis_one_l<2>(a, px, py, pz, p0, nvalid, ld, phi, gx, gy, gz, st);
+  launch_basis_one_l<3>(a, px, py, pz, p0, nvalid, ld, phi, gx, gy, gz, st);
 }
 
 void launch_basis_f64(const BuildArgs& a, int64_t p0, int64_t nvalid, bool grad, cudaStream_t st) {
-  dim3 grid((unsigned)((a.ldp + 127) / 128), (unsigned)a.nshells);
-  if (grad)
-    k_basis<double, true><<<grid, 128, 0, st>>>(a.shells, a.atoms, a.exps, a.norms, a.contr, a.sa, a.px, a.py, a.pz,
-                                                p0, nvalid, a.ldp, a.phi, a.gx, a.gy, a.gz);
-  else
-    k_basis<double, false><<<grid, 128, 0, st>>>(a.shells, a.atoms, a.exps, a.norms, a.contr, a.sa, a.px, a.py,
-                                                 a.pz, p0, nvalid, a.ldp, a.phi, nullptr, nullptr, nullptr);
+  launch_basis(a, a.px, a.py, a.pz, p0, nvalid, a.ldp, a.phi, grad ? a.gx : nullptr, a.gy, a.gz, st);
 }
 
-// basis on arbitrary points (pgxc_orbital_calculate): same kernel, caller arrays
+// basis on arbitrary points (pgxc_orbital_calculate): same kernels, caller arrays
 void launch_basis_points_f64(const BuildArgs& a, const double* px, const double* py, const double* pz, int64_t n,
                              int64_t ld, double* phi, double* gx, double* gy, double* gz, cudaStream_t st) {
-  dim3 grid((unsigned)((ld + 127) / 128), (unsigned)a.nshells);
-  if (gx)
-    k_basis<double, true><<<grid, 128, 0, st>>>(a.shells, a.atoms, a.exps, a.norms, a.contr, a.sa, px, py, pz, 0, n,
-                                                ld, phi, gx, gy, gz);
-  else
-    k_basis<double, false><<<grid, 128, 0, st>>>(a.shells, a.atoms, a.exps, a.norms, a.contr, a.sa, px, py, pz, 0,
-                                                 n, ld, phi, nullptr, nullptr, nullptr);
+  launch_basis(a, px, py, pz, 0, n, ld, phi, gx, gy, gz, st);
 }
 
 // ---------------------------------------------------------------------------

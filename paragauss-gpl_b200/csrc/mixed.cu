@@ -23,7 +23,8 @@
 //   * functional in FP64, E_xc and N_el in FP64 with Kahan compensation;
 //   * ham = Z^T phi on the integer tensor cores, FP64 partial tiles.
 //
-// Kernels: k_mx_basis (values + scale maxima), k_oz_quant_* (operand tiles),
+// Kernels: basis (k_basis_l, shared with the FP64 path), k_oz_quant_* (scales and
+// operand tiles),
 // k_oz_density (tcgen05), k_oz_zbuild, k_oz_vpot (tcgen05), k_oz_pack.
 // Tiles are 128 x 96: five 96-column INT32 accumulators fill 480 of the 512
 // TMEM columns.
@@ -33,7 +34,7 @@
 
 #include <cuda_runtime.h>
 
-#include "basis.cuh"
+#include "kernels.h"
 #include "mixed.h"
 #include "tc.cuh"
 
@@ -50,7 +51,7 @@ constexpr int kBlkA = kRowsA * 32;   // one slice of a 128-row x 32-byte K block
 constexpr int kBlkB = kRowsB * 32;
 constexpr int kOpA = kSlices * kBlkA;
 constexpr int kOpB = kSlices * kBlkB;
-constexpr int kStages = 4;           // bulk-copy ring depth
+constexpr int kStages = 5;           // bulk-copy ring depth
 constexpr int kKStep = 32;           // K elements per int8 MMA
 constexpr int kAlignFn = 384;        // functions padded to lcm(128, 96)
 
@@ -118,50 +119,6 @@ cudaError_t mx_alloc(MixedState* m, T** p, size_t n) {
   return e;
 }
 
-// ---------------------------------------------------------------------------
-// K1m: basis values and gradients in FP64 for one 128-point block, all
-// shells, plus the operand scales: per point, the largest |phi| (thread-
-// local); per function, the largest |phi| over the chunk (warp max -> shared
-// atomicMax -> one global atomicMax per function and block).
-// ---------------------------------------------------------------------------
-template <bool GRAD>
-__global__ void __launch_bounds__(128) k_mx_basis(const DevShell* __restrict__ shells, int nshells,
-                                                  const double* __restrict__ atoms, const double* __restrict__ exps,
-                                                  const double* __restrict__ norms, const double* __restrict__ contr,
-                                                  DevSA sa, const double* __restrict__ px,
-                                                  const double* __restrict__ py, const double* __restrict__ pz,
-                                                  int64_t p0, int64_t nvalid, int64_t ld, int nbas,
-                                                  double* __restrict__ phi, double* __restrict__ gx,
-                                                  double* __restrict__ gy, double* __restrict__ gz,
-                                                  int* __restrict__ e_pt, unsigned long long* __restrict__ fmax) {
-  extern __shared__ unsigned long long sfmax[];
-  for (int f = threadIdx.x; f < nbas; f += blockDim.x) sfmax[f] = 0ull;
-  __syncthreads();
-  const int64_t p = (int64_t)blockIdx.x * 128 + threadIdx.x;
-  const bool valid = p < nvalid;
-  const double qx = valid ? px[p0 + p] : 0.0, qy = valid ? py[p0 + p] : 0.0, qz = valid ? pz[p0 + p] : 0.0;
-  double ptmax = 0.0;
-  for (int s = 0; s < nshells; ++s) {
-    const DevShell S = shells[s];
-    double x = 0, y = 0, z = 0;
-    if (valid) {
-      x = qx - atoms[3 * S.atom];
-      y = qy - atoms[3 * S.atom + 1];
-      z = qz - atoms[3 * S.atom + 2];
-    }
-    switch (S.l) {
-      case 0: shell_at_point<0, GRAD, double, double, true>(S, sa, x, y, z, exps, norms, contr, valid, p, ld, phi, gx, gy, gz, 0.0, &ptmax, sfmax); break;
-      case 1: shell_at_point<1, GRAD, double, double, true>(S, sa, x, y, z, exps, norms, contr, valid, p, ld, phi, gx, gy, gz, 0.0, &ptmax, sfmax); break;
-      case 2: shell_at_point<2, GRAD, double, double, true>(S, sa, x, y, z, exps, norms, contr, valid, p, ld, phi, gx, gy, gz, 0.0, &ptmax, sfmax); break;
-      default: shell_at_point<3, GRAD, double, double, true>(S, sa, x, y, z, exps, norms, contr, valid, p, ld, phi, gx, gy, gz, 0.0, &ptmax, sfmax); break;
-    }
-  }
-  e_pt[p] = scale_exp(ptmax);
-  __syncthreads();
-  for (int f = threadIdx.x; f < nbas; f += blockDim.x)
-    if (sfmax[f]) atomicMax(fmax + f, sfmax[f]);
-}
-
 __global__ void k_oz_fexp(const unsigned long long* __restrict__ mx, int64_t n, int* __restrict__ e) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) e[i] = scale_exp(__longlong_as_double((long long)mx[i]));
@@ -194,25 +151,39 @@ __device__ __forceinline__ void store_row(int8_t* dst, int t, int h, const int8_
     *reinterpret_cast<uint4*>(dst + s * (ROWS * 32) + blk_off(t, h * 16)) = *reinterpret_cast<const uint4*>(d[s]);
 }
 
-// rows = points, K = functions: element (p, f) = phi[f][p], per-point scale
-__global__ void __launch_bounds__(128) k_oz_quant_pts(const double* __restrict__ phi, int64_t ldp,
-                                                      const int* __restrict__ e_pt, int nks,
-                                                      int8_t* __restrict__ out) {
-  const int pb = blockIdx.x, kb = blockIdx.y, t = threadIdx.x;
+// rows = points, K = functions: element (p, f) = phi[f][p].  One block per
+// 128 points: the per-point scale (largest |phi| over all functions) is found
+// first, then every K block of the 128 rows is quantized.
+__global__ void __launch_bounds__(128) k_oz_quant_pts(const double* __restrict__ phi, int64_t ldp, int64_t nbas,
+                                                      int nks, int* __restrict__ e_pt, int8_t* __restrict__ out) {
+  const int pb = blockIdx.x, t = threadIdx.x;
   const int64_t p = (int64_t)pb * 128 + t;
-  const int e = e_pt[p];
-  int8_t* dst = out + ((int64_t)pb * nks + kb) * kOpA;
+  double m8[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int64_t f = 0;
+  for (; f + 8 <= nbas; f += 8) {
 #pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    alignas(16) int8_t d[kSlices][16];
+    for (int j = 0; j < 8; ++j) m8[j] = fmax(m8[j], fabs(phi[(f + j) * ldp + p]));
+  }
+  for (; f < nbas; ++f) m8[0] = fmax(m8[0], fabs(phi[f * ldp + p]));
+  double mx = 0.0;
 #pragma unroll
-    for (int k = 0; k < 16; ++k) {
-      int8_t q[kSlices];
-      digits(phi[(int64_t)(kb * 32 + h * 16 + k) * ldp + p], e, q);
+  for (int j = 0; j < 8; ++j) mx = fmax(mx, m8[j]);
+  const int e = scale_exp(mx);
+  e_pt[p] = e;
+  for (int kb = 0; kb < nks; ++kb) {
+    int8_t* dst = out + ((int64_t)pb * nks + kb) * kOpA;
 #pragma unroll
-      for (int s = 0; s < kSlices; ++s) d[s][k] = q[s];
+    for (int h = 0; h < 2; ++h) {
+      alignas(16) int8_t d[kSlices][16];
+#pragma unroll
+      for (int k = 0; k < 16; ++k) {
+        int8_t q[kSlices];
+        digits(phi[(int64_t)(kb * 32 + h * 16 + k) * ldp + p], e, q);
+#pragma unroll
+        for (int s = 0; s < kSlices; ++s) d[s][k] = q[s];
+      }
+      store_row<128>(dst, t, h, d);
     }
-    store_row<128>(dst, t, h, d);
   }
 }
 
@@ -305,8 +276,9 @@ __device__ __forceinline__ void oz_mma_step(uint32_t tbase, const int8_t* a, con
   }
 }
 
-// this thread's row of the kGroups accumulators, columns c0..c0+15:
-// x = sum_g 2^(-12-7g) D_g
+// this thread's row of the kGroups accumulators, columns c0..c0+15, combined
+// exactly in 64-bit integers: x = sum_g D_g 2^(28-7g) = 2^40 * sum_g 2^(-12-7g) D_g
+// (|D_0| < 2^31, so |x| < 2^60), then converted once to FP64.
 __device__ __forceinline__ void oz_read16(uint32_t trow, int c0, double (&x)[16]) {
   float v[kGroups][16];
 #pragma unroll
@@ -314,12 +286,19 @@ __device__ __forceinline__ void oz_read16(uint32_t trow, int c0, double (&x)[16]
   tc::tmem_ld_wait();
 #pragma unroll
   for (int j = 0; j < 16; ++j) {
-    double acc = 0.0;
+    long long acc = 0;
 #pragma unroll
-    for (int g = kGroups - 1; g >= 0; --g) acc += ldexp((double)__float_as_int(v[g][j]), -12 - 7 * g);
-    x[j] = acc;
+    for (int g = 0; g < kGroups; ++g) acc += (long long)__float_as_int(v[g][j]) << (7 * (kGroups - 1 - g));
+    x[j] = (double)acc;
   }
 }
+
+// 2^e built from the bit pattern; exponents below the normal range give
+// 2^-1022 (every such term is below 2^-960 in magnitude)
+__device__ __forceinline__ double pow2(int e) {
+  return __longlong_as_double((long long)(max(e, -1022) + 1023) << 52);
+}
+constexpr int kCombShift = -12 - 7 * (kGroups - 1);  // x * 2^kCombShift = sum_g 2^(-12-7g) D_g
 
 // ---------------------------------------------------------------------------
 // G1: density.  CTA = 128 points (TMEM lane = point).  For each 96-wide tile
@@ -394,6 +373,7 @@ __global__ void __launch_bounds__(kDensThreads, 1)
     const int64_t p = (int64_t)pb * 128 + row;
     const uint32_t trow = tbase + ((uint32_t)((warp & 3) * 32) << 16);
     const int ea = e_pt[p];
+    const double rs = pow2(ea + kCombShift);  // row scale, applied once per term
     for (int nb = 0; nb < nnb; ++nb) {
       if (!tc::mbar_wait(&S.acc_full, nb & 1)) {
         ok = false;
@@ -419,7 +399,7 @@ __global__ void __launch_bounds__(kDensThreads, 1)
           }
 #pragma unroll
           for (int j = 0; j < 8; ++j) {
-            const double X = ldexp(x[hh + j], ea + __ldg(e_P + nu0 + j));
+            const double X = x[hh + j] * (rs * pow2(__ldg(e_P + nu0 + j)));
             r_acc += X * v[j];
             if (GGA) {
               g_acc[0] += X * w0[j];
@@ -467,25 +447,38 @@ __global__ void __launch_bounds__(256) k_oz_zbuild(int64_t ldp, const double* __
                                                    const double* __restrict__ gz, const double* __restrict__ A,
                                                    const double* __restrict__ Bx, const double* __restrict__ By,
                                                    const double* __restrict__ Bz, double* __restrict__ Z,
-                                                   unsigned long long* __restrict__ zmax) {
+                                                   unsigned long long* __restrict__ zmax,
+                                                   unsigned long long* __restrict__ fmax_) {
   const int64_t f = blockIdx.y;
   const int64_t base = f * ldp;
-  double mx = 0.0;
+  double mz = 0.0, mf = 0.0;
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < ldp; p += (int64_t)gridDim.x * blockDim.x) {
-    double z = A[p] * phi[base + p];
+    const double v = phi[base + p];
+    double z = A[p] * v;
     if (GGA) z += Bx[p] * gx[base + p] + By[p] * gy[base + p] + Bz[p] * gz[base + p];
     Z[base + p] = z;
-    mx = fmax(mx, fabs(z));
+    mz = fmax(mz, fabs(z));
+    mf = fmax(mf, fabs(v));
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-  __shared__ double red[8];
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+  for (int o = 16; o > 0; o >>= 1) {
+    mz = fmax(mz, __shfl_xor_sync(0xffffffffu, mz, o));
+    mf = fmax(mf, __shfl_xor_sync(0xffffffffu, mf, o));
+  }
+  __shared__ double red[2][8];
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = mz;
+    red[1][threadIdx.x >> 5] = mf;
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double m = 0.0;
-    for (int i = 0; i < 8; ++i) m = fmax(m, red[i]);
-    if (m > 0.0) atomicMax(zmax + f, (unsigned long long)__double_as_longlong(m));
+    double a = 0.0, b = 0.0;
+    for (int i = 0; i < 8; ++i) {
+      a = fmax(a, red[0][i]);
+      b = fmax(b, red[1][i]);
+    }
+    if (a > 0.0) atomicMax(zmax + f, (unsigned long long)__double_as_longlong(a));
+    if (b > 0.0) atomicMax(fmax_ + f, (unsigned long long)__double_as_longlong(b));
   }
 }
 
@@ -561,7 +554,7 @@ __global__ void __launch_bounds__(kVThreads, 1)
         double x[16];
         oz_read16(trow, c0, x);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) out[c0 + j] += ldexp(x[j], ea + __ldg(e_fn + tj * kRowsB + c0 + j));
+        for (int j = 0; j < 16; ++j) out[c0 + j] += x[j] * pow2(ea + kCombShift + __ldg(e_fn + tj * kRowsB + c0 + j));
       }
     }
   }
@@ -657,12 +650,9 @@ int mixed_create(MixedState** out, const BuildArgs& a, int64_t nbas, bool gga, i
   m->nsplit = (nks + m->ks_per_split - 1) / m->ks_per_split;
   if ((e = mx_alloc(m, &m->vpart, (size_t)m->nsplit * m->ntiles * kRowsA * kRowsB))) return fail(e, "cudaMalloc");
   const int smem = (int)sizeof(OzSmem) + 1024;
-  const int smem_basis = (int)(m->nbas * sizeof(unsigned long long));
   if ((e = cudaFuncSetAttribute(k_oz_density<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) ||
       (e = cudaFuncSetAttribute(k_oz_density<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) ||
-      (e = cudaFuncSetAttribute(k_oz_vpot, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) ||
-      (e = cudaFuncSetAttribute(k_mx_basis<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_basis)) ||
-      (e = cudaFuncSetAttribute(k_mx_basis<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_basis)))
+      (e = cudaFuncSetAttribute(k_oz_vpot, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)))
     return fail(e, "cudaFuncSetAttribute");
   *out = m;
   return PGXC_OK;
@@ -693,20 +683,10 @@ int mixed_prepare(MixedState* m, const BuildArgs& a, int nocc, cudaStream_t st) 
 }
 
 int mixed_basis(MixedState* m, const BuildArgs& a, int64_t p0, int64_t nvalid, bool gga, cudaStream_t st) {
-  cudaMemsetAsync(m->fmax, 0, sizeof(unsigned long long) * m->ldk, st);
-  const int smem = (int)(m->nbas * sizeof(unsigned long long));
-  const unsigned nb = (unsigned)(m->ldp / 128);
-  if (gga)
-    k_mx_basis<true><<<nb, 128, smem, st>>>(a.shells, a.nshells, a.atoms, a.exps, a.norms, a.contr, a.sa, a.px, a.py,
-                                            a.pz, p0, nvalid, m->ldp, (int)m->nbas, m->phi, m->gx, m->gy, m->gz,
-                                            m->e_pt, m->fmax);
-  else
-    k_mx_basis<false><<<nb, 128, smem, st>>>(a.shells, a.nshells, a.atoms, a.exps, a.norms, a.contr, a.sa, a.px,
-                                             a.py, a.pz, p0, nvalid, m->ldp, (int)m->nbas, m->phi, nullptr, nullptr,
-                                             nullptr, m->e_pt, m->fmax);
+  launch_basis(a, a.px, a.py, a.pz, p0, nvalid, m->ldp, m->phi, gga ? m->gx : nullptr, m->gy, m->gz, st);
   const int nksf = (int)(m->ldk / kKStep);
-  k_oz_quant_pts<<<dim3(nb, (unsigned)nksf), 128, 0, st>>>(m->phi, m->ldp, m->e_pt, nksf, m->tA1);
-  return 2;
+  k_oz_quant_pts<<<(unsigned)(m->ldp / 128), 128, 0, st>>>(m->phi, m->ldp, m->nbas, nksf, m->e_pt, m->tA1);
+  return 5;
 }
 
 int mixed_density(MixedState* m, const BuildArgs& a, bool gga, cudaStream_t st) {
@@ -725,12 +705,14 @@ int mixed_density(MixedState* m, const BuildArgs& a, bool gga, cudaStream_t st) 
 
 int mixed_potential(MixedState* m, const BuildArgs& a, bool gga, cudaStream_t st, cudaEvent_t k0, cudaEvent_t k1) {
   cudaMemsetAsync(m->zmax, 0, sizeof(unsigned long long) * m->ldk, st);
+  cudaMemsetAsync(m->fmax, 0, sizeof(unsigned long long) * m->ldk, st);
   dim3 gz((unsigned)std::min<int64_t>(64, (m->ldp + 255) / 256), (unsigned)m->nbas);
   if (gga)
-    k_oz_zbuild<true><<<gz, 256, 0, st>>>(m->ldp, m->phi, m->gx, m->gy, m->gz, a.A, a.Bx, a.By, a.Bz, m->Z, m->zmax);
+    k_oz_zbuild<true><<<gz, 256, 0, st>>>(m->ldp, m->phi, m->gx, m->gy, m->gz, a.A, a.Bx, a.By, a.Bz, m->Z, m->zmax,
+                                          m->fmax);
   else
     k_oz_zbuild<false><<<gz, 256, 0, st>>>(m->ldp, m->phi, nullptr, nullptr, nullptr, a.A, nullptr, nullptr, nullptr,
-                                           m->Z, m->zmax);
+                                           m->Z, m->zmax, m->fmax);
   const unsigned ne = (unsigned)((m->ldk + 255) / 256);
   k_oz_fexp<<<ne, 256, 0, st>>>(m->zmax, m->ldk, m->e_Z);
   k_oz_fexp<<<ne, 256, 0, st>>>(m->fmax, m->ldk, m->e_fn);

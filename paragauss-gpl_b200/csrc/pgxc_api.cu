@@ -277,6 +277,17 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
   CUDA_TRY(c, cudaMemcpy(dnorms, bas->norms, sizeof(double) * nexp_tot, cudaMemcpyHostToDevice));
   if (ncon_tot) CUDA_TRY(c, cudaMemcpy(dcontr, bas->contractions, sizeof(double) * ncon_tot, cudaMemcpyHostToDevice));
   a.shells = dsh;
+  {
+    std::vector<int> ids[kMaxL + 1];
+    for (int i = 0; i < (int)c->shells.size(); ++i) ids[c->shells[i].l].push_back(i);
+    for (int l = 0; l <= kMaxL; ++l) {
+      a.nshl[l] = (int)ids[l].size();
+      int* d = nullptr;
+      if ((st = dalloc(c, &d, std::max<size_t>(ids[l].size(), 1)))) return fail(st);
+      if (!ids[l].empty()) CUDA_TRY(c, cudaMemcpy(d, ids[l].data(), ids[l].size() * sizeof(int), cudaMemcpyHostToDevice));
+      a.shl[l] = d;
+    }
+  }
   a.atoms = datoms;
   a.exps = dexps;
   a.norms = dnorms;
@@ -423,7 +434,7 @@ static int run_build(pgxc_ctx* c, int nocc, pgxc_timings* tm) {
     const int64_t nv = std::min<int64_t>(c->chunk, c->npts - p0);
     CUDA_TRY(c, cudaEventRecord(c->ev[3], s));
     if (c->mixed) launches += mixed_basis(c->mixed, a, p0, nv, gga, s);
-    else { launch_basis_f64(a, p0, nv, gga, s); launches += 1; }
+    else { launch_basis_f64(a, p0, nv, gga, s); launches += 4; }
     CUDA_TRY(c, cudaEventRecord(c->ev[4], s));
     CUDA_TRY(c, cudaEventRecord(c->kev[0], s));
     if (c->mixed) launches += mixed_density(c->mixed, a, gga, s);
