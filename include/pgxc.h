@@ -107,8 +107,14 @@ typedef struct pgxc_options {
   int32_t functional;            /* PGXC_XC_VWN | PGXC_XC_PBE               */
   int32_t ispin;                 /* 1 or 2                                  */
   int32_t precision;             /* PGXC_PREC_*                             */
-  int32_t batch_points;          /* screening batch, 0 -> 128 (machineparameters_veclen) */
-  double  screen_threshold;      /* 0 -> reference behaviour (only alpha*r^2 < 50) */
+  int32_t batch_points;          /* points per tile, 0 -> 128 (machineparameters_veclen); only 128 */
+  double  screen_threshold;      /* per-tile screening of basis functions:
+                                  *   0  -> drop only functions that are exactly zero on
+                                  *         the tile by the reference's alpha*r^2 < 50 rule
+                                  *         (results as unscreened, up to rounding);
+                                  *   >0 -> also drop functions whose |phi|, |grad phi|
+                                  *         bound stays below the threshold on the tile;
+                                  *   <0 -> no screening (dense layout) */
   int32_t device;                /* CUDA ordinal, -1 -> current device      */
   int64_t max_chunk_points;      /* 0 -> sized from free HBM                */
 } pgxc_options;
@@ -129,7 +135,7 @@ typedef struct pgxc_timings {
 
 typedef struct pgxc_ctx pgxc_ctx;
 
-/* Fill *opt with defaults (VWN, ispin 1, FP64, 128, no screening, device -1). */
+/* Fill *opt with defaults (VWN, ispin 1, FP64, 128, exact screening 0.0, device -1). */
 void pgxc_default_options(pgxc_options* opt);
 
 /*
@@ -144,6 +150,15 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas,
 
 /* Number of orbital basis functions (irrep dimension in C1). */
 int pgxc_nbas(const pgxc_ctx* ctx, int32_t* nbas);
+
+/*
+ * Screening plan of a context created with screen_threshold >= 0 (library
+ * extension, no reference counterpart): 128-point tiles, padded slots, listed
+ * (tile, function) pairs and sum over tiles of (listed functions)^2.
+ * PGXC_EINVAL for a dense-layout context.
+ */
+int pgxc_screen_stats(const pgxc_ctx* ctx, int64_t* ntiles, int64_t* nslots,
+                      int64_t* nlisted, double* sum_n2);
 
 /*
  * One XC build; replaces calc_xcks (modules/xc_hamiltonian.f90:812-1036)

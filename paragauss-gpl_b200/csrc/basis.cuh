@@ -10,6 +10,7 @@
 //   calculate_orbs_and_grads_v3 modules/orbital_module.f90:2421-2619
 //     (phi = Y R, grad phi = (r - R_A) Y R' + grad(Y) R; function order
 //     independent function -> radial function).
+// All arithmetic is FP64 in both precision modes.
 #pragma once
 
 #include "pgxc_common.cuh"
@@ -86,39 +87,31 @@ __device__ __forceinline__ void solid_harmonics(R x, R y, R z, R* Y, R (*dY)[16]
 }
 
 // One normalised primitive norm*exp(-alpha r^2), zero where alpha r^2 >= 50
-// (radial0/radial1, modules/orbital_module.f90:1823-1854).  In FP32 the
-// exponent alpha*r^2 (up to 50) would carry an absolute rounding error of
-// up to 50 * 2^-24 into exp; it is therefore formed in FP64 from the FP64 r^2
-// and split as 2^-t = 2^-k * 2^-f (k integer, |f| <= 1/2) before exp2f.
-__device__ __forceinline__ double prim_value(double alpha, double norm, double r2, double) {
+// (radial0/radial1, modules/orbital_module.f90:1823-1854).
+__device__ __forceinline__ double prim_value(double alpha, double norm, double r2) {
   const double ar2 = alpha * r2;
   return ar2 < 50.0 ? norm * exp(-ar2) : 0.0;
 }
-__device__ __forceinline__ float prim_value(float, float norm, float, double ar2) {
-  if (!(ar2 < 50.0)) return 0.f;
-  const double t = ar2 * 1.4426950408889634;  // log2(e)
-  const double k = rint(t);
-  return norm * ldexpf(exp2f(-(float)(t - k)), -(int)k);
-}
 
-// Evaluate one shell at one point and store its (2l+1)*nrad functions (and
-// gradients when GRAD) at column p of the [function][ld] arrays.  R is the
-// arithmetic type (FP64 for the drop-in path, FP32 for the mixed path), T the
-// stored type.  With R = float, r2d is the FP64 r^2 used for the exponent.
+// Evaluate the selected radial functions of one shell at one point.  The
+// selected radial indices are the set bits of `mask` (nsel of them, in
+// increasing order); selected function k of independent function i is stored
+// at row base + i*nsel + k, column p of the [row][ld] arrays.  The dense
+// layout is mask = all nrad bits, base = S.f0 (row = function index); the
+// screened layout is the tile's significant radial functions and their slot.
 // exps/norms/contr may point to shared memory (plain loads).
-template <int L, bool GRAD, typename T, typename R = double>
-__device__ __forceinline__ void shell_at_point(const DevShell& S, const DevSA& sa, R x, R y, R z,
+template <int L, bool GRAD>
+__device__ __forceinline__ void shell_at_point(const DevShell& S, const DevSA& sa, double x, double y, double z,
                                                const double* exps, const double* norms, const double* contr,
-                                               bool valid, int64_t p, int64_t ld,
-                                               T* __restrict__ phi, T* __restrict__ gx, T* __restrict__ gy,
-                                               T* __restrict__ gz, double r2d = 0.0) {
-  constexpr int NY = (L + 1) * (L + 1);
-  R Y[16];
-  R dY[3][16];
-  solid_harmonics<L, R>(x, y, z, Y, dY);
-  const R r2 = x * x + y * y + z * z;
+                                               bool valid, uint64_t mask, int64_t base, int nsel, int64_t p,
+                                               int64_t ld, double* __restrict__ phi, double* __restrict__ gx,
+                                               double* __restrict__ gy, double* __restrict__ gz) {
+  double Y[16];
+  double dY[3][16];
+  solid_harmonics<L, double>(x, y, z, Y, dY);
+  const double r2 = x * x + y * y + z * z;
   // symmetry-adapted harmonics of this l
-  R Ys[2 * L + 1], dYs[3][2 * L + 1];
+  double Ys[2 * L + 1], dYs[3][2 * L + 1];
 #pragma unroll
   for (int i = 0; i < 2 * L + 1; ++i) {
     if (sa.identity) {
@@ -126,10 +119,10 @@ __device__ __forceinline__ void shell_at_point(const DevShell& S, const DevSA& s
 #pragma unroll
       for (int c = 0; c < 3; ++c) dYs[c][i] = dY[c][L * L + i];
     } else {
-      R v = 0, g0 = 0, g1 = 0, g2 = 0;
+      double v = 0, g0 = 0, g1 = 0, g2 = 0;
 #pragma unroll
       for (int m = 0; m < 2 * L + 1; ++m) {
-        const R cf = (R)sa.c[L][i][m];
+        const double cf = sa.c[L][i][m];
         v += cf * Y[L * L + m];
         g0 += cf * dY[0][L * L + m];
         g1 += cf * dY[1][L * L + m];
@@ -138,27 +131,35 @@ __device__ __forceinline__ void shell_at_point(const DevShell& S, const DevSA& s
       Ys[i] = v; dYs[0][i] = g0; dYs[1][i] = g1; dYs[2][i] = g2;
     }
   }
-  (void)NY;
   const double* ex = exps + S.exp_off;
   const double* nr = norms + S.exp_off;
   const double* cc = contr + S.con_off;
-  for (int r0 = 0; r0 < S.nrad; r0 += kRadGroup) {
-    R Rr[kRadGroup], dR[kRadGroup];
+  uint64_t rem = mask;
+  for (int k0 = 0; k0 < nsel; k0 += kRadGroup) {
+    int rr[kRadGroup];
 #pragma unroll
-    for (int r = 0; r < kRadGroup; ++r) { Rr[r] = R(0); dR[r] = R(0); }
+    for (int r = 0; r < kRadGroup; ++r) {
+      if (k0 + r < nsel) {
+        rr[r] = __ffsll((long long)rem) - 1;
+        rem &= rem - 1;
+      } else {
+        rr[r] = -1;
+      }
+    }
+    double Rr[kRadGroup], dR[kRadGroup];
+#pragma unroll
+    for (int r = 0; r < kRadGroup; ++r) { Rr[r] = 0.0; dR[r] = 0.0; }
     if (valid) {
       for (int e = 0; e < S.nexp; ++e) {
-        const double alpha_d = ex[e];
-        const R alpha = (R)alpha_d;
-        const R v = prim_value(alpha, (R)nr[e], r2, alpha_d * r2d);
-        const R dv = (R(-2) * alpha) * v;
+        const double alpha = ex[e];
+        const double v = prim_value(alpha, nr[e], r2);
+        const double dv = (-2.0 * alpha) * v;
 #pragma unroll
         for (int r = 0; r < kRadGroup; ++r) {
-          const int rr = r0 + r;
-          if (rr < S.nrad) {
-            R cf;
-            if (rr < S.nunc) cf = (e == rr) ? R(1) : R(0);
-            else cf = (R)cc[e + (int64_t)S.nexp * (rr - S.nunc)];
+          if (rr[r] >= 0) {
+            double cf;
+            if (rr[r] < S.nunc) cf = (e == rr[r]) ? 1.0 : 0.0;
+            else cf = cc[e + (int64_t)S.nexp * (rr[r] - S.nunc)];
             Rr[r] += cf * v;
             dR[r] += cf * dv;
           }
@@ -169,15 +170,14 @@ __device__ __forceinline__ void shell_at_point(const DevShell& S, const DevSA& s
     for (int i = 0; i < 2 * L + 1; ++i) {
 #pragma unroll
       for (int r = 0; r < kRadGroup; ++r) {
-        const int rr = r0 + r;
-        if (rr < S.nrad) {
-          const int64_t f = S.f0 + (int64_t)i * S.nrad + rr;
-          phi[f * ld + p] = (T)(Ys[i] * Rr[r]);
+        if (rr[r] >= 0) {
+          const int64_t f = base + (int64_t)i * nsel + k0 + r;
+          phi[f * ld + p] = Ys[i] * Rr[r];
           if (GRAD) {
-            const R h = Ys[i] * dR[r];
-            gx[f * ld + p] = (T)(x * h + dYs[0][i] * Rr[r]);
-            gy[f * ld + p] = (T)(y * h + dYs[1][i] * Rr[r]);
-            gz[f * ld + p] = (T)(z * h + dYs[2][i] * Rr[r]);
+            const double h = Ys[i] * dR[r];
+            gx[f * ld + p] = x * h + dYs[0][i] * Rr[r];
+            gy[f * ld + p] = y * h + dYs[1][i] * Rr[r];
+            gz[f * ld + p] = z * h + dYs[2][i] * Rr[r];
           }
         }
       }
@@ -185,37 +185,47 @@ __device__ __forceinline__ void shell_at_point(const DevShell& S, const DevSA& s
   }
 }
 
-// ---------------------------------------------------------------------------
-// K1: basis functions of the shells of one angular momentum L on a chunk of
-// points.  grid = (chunk/128, shells of this L), block = 128 points; the
-// shell's exponents, norms and contraction matrix are staged in shared
-// memory first (global memory for shells larger than the staging area).
-// ---------------------------------------------------------------------------
+// Stage one shell's exponents, norms and contraction matrix in shared memory
+// (when they fit); returns the pointers to use.
 constexpr int kStagePrim = 64;
 constexpr int kStageCon = 512;
+struct ShellStage {
+  double e[kStagePrim], n[kStagePrim], c[kStageCon];
+};
+__device__ __forceinline__ bool stage_shell(ShellStage& st, DevShell& S, const double* exps, const double* norms,
+                                            const double* contr) {
+  const bool staged = S.nexp <= kStagePrim && S.nexp * S.ncontr <= kStageCon;
+  if (staged) {
+    const double *e_src = exps + S.exp_off, *n_src = norms + S.exp_off, *c_src = contr + S.con_off;
+    for (int i = threadIdx.x; i < S.nexp; i += blockDim.x) {
+      st.e[i] = e_src[i];
+      st.n[i] = n_src[i];
+    }
+    for (int i = threadIdx.x; i < S.nexp * S.ncontr; i += blockDim.x) st.c[i] = c_src[i];
+    S.exp_off = 0;
+    S.con_off = 0;
+  }
+  __syncthreads();
+  return staged;
+}
 
-template <int L, bool GRAD, typename T>
+__host__ __device__ constexpr uint64_t all_radial(int nrad) { return nrad >= 64 ? ~0ull : ((1ull << nrad) - 1); }
+
+// ---------------------------------------------------------------------------
+// K1 (dense): basis functions of the shells of one angular momentum L on a
+// chunk of points.  grid = (chunk/128, shells of this L), block = 128 points.
+// ---------------------------------------------------------------------------
+template <int L, bool GRAD>
 __global__ void __launch_bounds__(128) k_basis_l(const DevShell* __restrict__ shells, const int* __restrict__ ids,
                                                  const double* __restrict__ atoms, const double* __restrict__ exps,
                                                  const double* __restrict__ norms, const double* __restrict__ contr,
                                                  DevSA sa, const double* __restrict__ px, const double* __restrict__ py,
                                                  const double* __restrict__ pz, int64_t p0, int64_t nvalid, int64_t ld,
-                                                 T* __restrict__ phi, T* __restrict__ gx, T* __restrict__ gy,
-                                                 T* __restrict__ gz) {
-  __shared__ double s_exp[kStagePrim], s_nrm[kStagePrim], s_con[kStageCon];
+                                                 double* __restrict__ phi, double* __restrict__ gx,
+                                                 double* __restrict__ gy, double* __restrict__ gz) {
+  __shared__ ShellStage st;
   DevShell S = shells[ids[blockIdx.y]];
-  const double *e_src = exps + S.exp_off, *n_src = norms + S.exp_off, *c_src = contr + S.con_off;
-  const bool staged = S.nexp <= kStagePrim && S.nexp * S.ncontr <= kStageCon;
-  if (staged) {
-    for (int i = threadIdx.x; i < S.nexp; i += blockDim.x) {
-      s_exp[i] = e_src[i];
-      s_nrm[i] = n_src[i];
-    }
-    for (int i = threadIdx.x; i < S.nexp * S.ncontr; i += blockDim.x) s_con[i] = c_src[i];
-    __syncthreads();
-    S.exp_off = 0;
-    S.con_off = 0;
-  }
+  const bool staged = stage_shell(st, S, exps, norms, contr);
   const int64_t p = (int64_t)blockIdx.x * 128 + threadIdx.x;
   if (p >= ld) return;
   const bool valid = p < nvalid;
@@ -225,8 +235,44 @@ __global__ void __launch_bounds__(128) k_basis_l(const DevShell* __restrict__ sh
     y = py[p0 + p] - atoms[3 * S.atom + 1];
     z = pz[p0 + p] - atoms[3 * S.atom + 2];
   }
-  shell_at_point<L, GRAD, T, double>(S, sa, x, y, z, staged ? s_exp : exps, staged ? s_nrm : norms,
-                                     staged ? s_con : contr, valid, p, ld, phi, gx, gy, gz);
+  shell_at_point<L, GRAD>(S, sa, x, y, z, staged ? st.e : exps, staged ? st.n : norms, staged ? st.c : contr, valid,
+                          all_radial(S.nrad), S.f0, S.nrad, p, ld, phi, gx, gy, gz);
+}
+
+// ---------------------------------------------------------------------------
+// K1 (screened): one block per work item = the significant radial functions
+// of one shell on the 128 points of one tile.  Rows are slots of the chunk's
+// compact [slot][128] arrays (slot - s0).
+// ---------------------------------------------------------------------------
+struct BasisItem {
+  int tile;                 // global tile index
+  int shell;
+  int64_t slot;             // global slot of the shell's first significant function
+  int nsig;                 // popcount(mask)
+  int pad_;
+  unsigned long long mask;  // significant radial functions of the shell
+};
+
+template <int L, bool GRAD>
+__global__ void __launch_bounds__(128) k_basis_items(const BasisItem* __restrict__ items,
+                                                     const DevShell* __restrict__ shells,
+                                                     const double* __restrict__ atoms, const double* __restrict__ exps,
+                                                     const double* __restrict__ norms,
+                                                     const double* __restrict__ contr, DevSA sa,
+                                                     const double* __restrict__ qx, const double* __restrict__ qy,
+                                                     const double* __restrict__ qz, int64_t s0,
+                                                     double* __restrict__ phi, double* __restrict__ gx,
+                                                     double* __restrict__ gy, double* __restrict__ gz) {
+  __shared__ ShellStage st;
+  const BasisItem it = items[blockIdx.x];
+  DevShell S = shells[it.shell];
+  const bool staged = stage_shell(st, S, exps, norms, contr);
+  const int64_t q = (int64_t)it.tile * 128 + threadIdx.x;
+  const double x = qx[q] - atoms[3 * S.atom];
+  const double y = qy[q] - atoms[3 * S.atom + 1];
+  const double z = qz[q] - atoms[3 * S.atom + 2];
+  shell_at_point<L, GRAD>(S, sa, x, y, z, staged ? st.e : exps, staged ? st.n : norms, staged ? st.c : contr, true,
+                          it.mask, it.slot - s0, it.nsig, threadIdx.x, 128, phi, gx, gy, gz);
 }
 
 }  // namespace pgxc

@@ -17,6 +17,7 @@
 #include "kernels.h"
 #include "mixed.h"
 #include "pgxc_common.cuh"
+#include "screened.h"
 
 using namespace pgxc;
 
@@ -41,7 +42,8 @@ struct pgxc_ctx {
   int64_t chunk = 0;
   double* h_ham = nullptr;      // pinned staging for the packed matrix
   double* h_acc = nullptr;      // pinned {E, cE, N, cN}
-  MixedState* mixed = nullptr;  // tensor-core mixed-precision path
+  MixedState* mixed = nullptr;  // tensor-core mixed-precision path (dense)
+  ScreenPlan* screen = nullptr; // screened (tile-sparse) build, when screen_threshold >= 0
 };
 
 namespace {
@@ -134,6 +136,7 @@ void pgxc_destroy(pgxc_ctx* c) {
   if (c->device >= 0) cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->mixed) mixed_destroy(c->mixed);
+  if (c->screen) screen_destroy(c->screen);
   for (void* p : c->allocs) cudaFree(p);
   if (c->h_ham) cudaFreeHost(c->h_ham);
   if (c->h_acc) cudaFreeHost(c->h_acc);
@@ -143,6 +146,13 @@ void pgxc_destroy(pgxc_ctx* c) {
     if (e) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
+}
+
+int pgxc_screen_stats(const pgxc_ctx* c, int64_t* ntiles, int64_t* nslots, int64_t* nlisted, double* sum_n2) {
+  if (!c) return set_err(nullptr, PGXC_EINVAL, "ctx is NULL");
+  if (!c->screen) return set_err(const_cast<pgxc_ctx*>(c), PGXC_EINVAL, "context has no screening plan");
+  screen_stats(c->screen, ntiles, nslots, nlisted, sum_n2, nullptr);
+  return PGXC_OK;
 }
 
 int pgxc_nbas(const pgxc_ctx* c, int32_t* nbas) {
@@ -175,6 +185,7 @@ static int validate_basis(pgxc_ctx* c, const pgxc_geometry* geo, const pgxc_basi
     if (S.l > kMaxL) return set_err(c, PGXC_ENOTSUP, "l > 3 is not supported");
     if (S.nexp <= 0 || S.nunc < 0 || S.ncontr < 0 || S.nunc > S.nexp)
       return set_err(c, PGXC_EINVAL, "bad shell exponent/contraction counts");
+    if (S.nunc + S.ncontr > 64) return set_err(c, PGXC_ENOTSUP, "more than 64 radial functions in one shell");
     if (S.atom < last_atom || (S.atom == last_atom && S.l <= last_l))
       return set_err(c, PGXC_EINVAL, "shells must be ordered by atom, then l (orbitalprojection order)");
     last_atom = S.atom;
@@ -314,14 +325,41 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
     launch_scale_inplace(dgrid + 3 * n, dbecke, n, c->stream);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   }
-  // potential tiles of the FP64 path and their split over points
   a.ldc = round_up(c->nbas, kTile);
+  const bool gga = o.functional == PGXC_XC_PBE;
+  if (o.screen_threshold >= 0.0) {
+    // screened build: per-tile significant-function lists; only P, the
+    // accumulators and the packed matrix are shared with the dense layout
+    if ((st = dalloc(c, &a.acc, 4)) || (st = dalloc(c, &a.P, (size_t)a.ldc * a.ldc))) return fail(st);
+    if ((st = dalloc(c, &c->d_ham, (size_t)o.ispin * c->nbas * (c->nbas + 1) / 2))) return fail(st);
+    CUDA_TRY(c, cudaMallocHost(&c->h_ham, sizeof(double) * o.ispin * c->nbas * (c->nbas + 1) / 2));
+    CUDA_TRY(c, cudaMallocHost(&c->h_acc, sizeof(double) * 4));
+    ScreenInput in;
+    in.shells = &c->shells;
+    in.atoms = geo->coords;
+    in.natm = c->natm;
+    in.nbas = c->nbas;
+    in.grdpts = grid->grdpts;
+    in.npts = n;
+    in.exps = bas->exponents;
+    in.norms = bas->norms;
+    in.contr = bas->contractions;
+    in.threshold = o.screen_threshold;
+    in.gga = gga;
+    in.precision = o.precision;
+    in.max_chunk_points = o.max_chunk_points;
+    std::string e;
+    st = screen_create(&c->screen, in, a, c->stream, e);
+    if (st) return fail(set_err(c, st, e));
+    *out = c;
+    return PGXC_OK;
+  }
+  // potential tiles of the FP64 path and their split over points
   a.nt = (int)(a.ldc / kTile);
   a.ntiles = a.nt * (a.nt + 1) / 2;
   const int ns64 = (int)std::min<int64_t>(8, std::max<int64_t>(1, (2 * 148 + a.ntiles - 1) / a.ntiles));
   // chunk sizing: balanced chunks of at most max_chunk points, each a
   // multiple of 128 * ns64 (CTA rows of both paths, 16-point K slabs per split)
-  const bool gga = o.functional == PGXC_XC_PBE;
   size_t freeb = 0, totb = 0;
   CUDA_TRY(c, cudaMemGetInfo(&freeb, &totb));
   const int64_t arrays = gga ? 5 : 2;
@@ -413,6 +451,29 @@ static int run_build(pgxc_ctx* c, int nocc, pgxc_timings* tm) {
   cudaStream_t s = c->stream;
   const bool gga = c->opt.functional == PGXC_XC_PBE;
   const int64_t kpad = round_up(std::max(nocc, 1), 16);
+  if (c->screen) {
+    CUDA_TRY(c, cudaMemsetAsync(a.acc, 0, 4 * sizeof(double), s));
+    CUDA_TRY(c, cudaEventRecord(c->ev[1], s));
+    launch_pmat_f64(a, kpad, s);
+    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, cudaEventRecord(c->ev[2], s));
+    ScreenTimes T;
+    std::string e;
+    const int st = screen_run(c->screen, a, s, c->d_ham, c->opt.ispin, 0, &T, e);
+    if (st) return set_err(c, st, e);
+    float ms = 0;
+    CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev[1], c->ev[2]));
+    if (tm) {
+      tm->basis_ms = T.basis;
+      tm->density_ms = T.density + ms;
+      tm->functional_ms = T.functional;
+      tm->potential_ms = T.potential;
+      tm->xgemm_ms = T.x;
+      tm->vgemm_ms = T.v;
+      tm->kernel_launches = T.launches + 2;
+    }
+    return PGXC_OK;
+  }
   float t_basis = 0, t_dens = 0, t_func = 0, t_pot = 0, t_x = 0, t_v = 0;
   int64_t launches = 0;
   CUDA_TRY(c, cudaMemsetAsync(a.acc, 0, 4 * sizeof(double), s));

@@ -1,0 +1,845 @@
+// screened.cu -- planning and FP64 kernels of the screened (tile-sparse) XC build.
+//
+// Per geometry (screen_create):
+//   Morton order of the grid, tiles of 128 points (padded with weight-0 copies);
+//   k_tile_atom_d2    smallest squared distance of each tile to each atom;
+//   host plan         per tile the listed functions (slots, padded to 32), the
+//                     basis work items (tile, shell, radial mask) and chunks.
+// Per build (screen_run), per chunk of tiles:
+//   k_basis_items     phi, grad phi of listed functions only     [K1]
+//   k_pad_zero        zero rows of padding slots
+//   k_sdensity        X = phi_t P[S_t, S_t] on DMMA, P gathered by cp.async,
+//                     fused rho, grad rho                          [K3]
+//   k_functional      (kernels_fp64.cu)                            [K2]
+//   k_szbuild         Z = A phi (+ B . grad phi)
+//   k_svpot           H[S_t, S_t] += Z_t^T phi_t on DMMA, scatter-added into
+//                     the full matrix with FP64 atomics            [K4]
+// then k_spack packs V (LDA: H; GGA: H + H^T, the symmetrisation of
+// modules/xc_hamiltonian.f90:1559-1566) into the tristore order.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <type_traits>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "basis.cuh"
+#include "dgemm.cuh"
+#include "kernels.h"
+#include "screened.h"
+#include "screened_mixed.h"
+
+namespace pgxc {
+
+constexpr int kSlotAlign = 32;   // slots per tile are padded to this (INT8 K step)
+constexpr int64_t kSlack = 128;  // zero rows after the last slot of a chunk
+
+struct ScreenPlan {
+  int64_t ntiles = 0, nslots = 0, nlisted = 0;
+  double sum_n2 = 0.0;
+  int max_n = 0;
+  bool gga = false;
+  int64_t nbas = 0;
+  // device, whole grid
+  double *qx = nullptr, *qy = nullptr, *qz = nullptr, *qw = nullptr;  // Morton-ordered points [ntiles*128]
+  int64_t* tso = nullptr;   // [ntiles+1] first slot of each tile
+  int* slot_fn = nullptr;   // [nslots] function of each slot, -1 for padding
+  int* slot_tile = nullptr; // [nslots]
+  BasisItem* items[kMaxL + 1] = {};
+  // host copies of the partition
+  std::vector<int64_t> h_tso;
+  std::vector<int64_t> chunk_t0;                   // chunk c covers tiles [chunk_t0[c], chunk_t0[c+1])
+  std::vector<int64_t> item_off[kMaxL + 1];        // items of chunk c: [item_off[L][c], item_off[L][c+1])
+  int64_t chunk_slots = 0, chunk_tiles = 0;        // buffer capacities
+  // device, per chunk
+  double *phi = nullptr, *gx = nullptr, *gy = nullptr, *gz = nullptr, *Z = nullptr;
+  double* pt = nullptr;      // 8 point arrays of chunk_tiles*128
+  double* partial = nullptr;
+  double* V = nullptr;       // [nbas][nbas]
+  ScreenMixed* mixed = nullptr;
+  cudaEvent_t ev[10] = {};
+  std::vector<void*> allocs;
+};
+
+namespace {
+
+template <typename T>
+cudaError_t sp_alloc(ScreenPlan* sp, T** p, size_t n) {
+  void* q = nullptr;
+  cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
+  if (e == cudaSuccess) {
+    sp->allocs.push_back(q);
+    *p = (T*)q;
+  }
+  return e;
+}
+
+// ---------------------------------------------------------------------------
+// planning kernels
+// ---------------------------------------------------------------------------
+__global__ void k_gather_points(const int64_t* __restrict__ perm, int64_t nq, const double* __restrict__ px,
+                                const double* __restrict__ py, const double* __restrict__ pz,
+                                const double* __restrict__ w, double* __restrict__ qx, double* __restrict__ qy,
+                                double* __restrict__ qz, double* __restrict__ qw) {
+  const int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= nq) return;
+  int64_t i = perm[q];
+  double wt = 0.0;
+  if (i >= 0) wt = w[i];
+  else i = perm[q & ~(int64_t)127];  // padding: a weight-0 copy of the tile's first point
+  qx[q] = px[i];
+  qy[q] = py[i];
+  qz[q] = pz[i];
+  qw[q] = wt;
+}
+
+// d2[t][a] = min over the tile's points of |r - R_a|^2, rounded down to float
+__global__ void __launch_bounds__(128) k_tile_atom_d2(const double* __restrict__ qx, const double* __restrict__ qy,
+                                                      const double* __restrict__ qz, const double* __restrict__ atoms,
+                                                      int natm, float* __restrict__ d2) {
+  __shared__ float red[4];
+  const int64_t t = blockIdx.x;
+  const int64_t q = t * 128 + threadIdx.x;
+  const double x = qx[q], y = qy[q], z = qz[q];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int a = 0; a < natm; ++a) {
+    const double dx = x - atoms[3 * a], dy = y - atoms[3 * a + 1], dz = z - atoms[3 * a + 2];
+    float f = __double2float_rd(dx * dx + dy * dy + dz * dz);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) f = fminf(f, __shfl_xor_sync(0xffffffffu, f, o));
+    if (lane == 0) red[warp] = f;
+    __syncthreads();
+    if (threadIdx.x == 0) d2[t * natm + a] = fminf(fminf(red[0], red[1]), fminf(red[2], red[3]));
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// FP64 kernels
+// ---------------------------------------------------------------------------
+template <bool GGA>
+__global__ void k_pad_zero(const int* __restrict__ slot_fn, int64_t nslots, double* __restrict__ phi,
+                           double* __restrict__ gx, double* __restrict__ gy, double* __restrict__ gz) {
+  const int64_t total = nslots * 128;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    if (slot_fn[e >> 7] >= 0) continue;
+    phi[e] = 0.0;
+    if (GGA) {
+      gx[e] = 0.0;
+      gy[e] = 0.0;
+      gz[e] = 0.0;
+    }
+  }
+}
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool pred) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  const int sz = pred ? 8 : 0;  // 0: fill with zeros
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+
+// B slab of the density GEMM: element (k, n) = P[fn(k0+k)][fn(n0+n)], zero
+// where a slot is padding or n0+n >= n_valid.
+__device__ __forceinline__ void load_gslab(double* s, const double* __restrict__ P, int64_t ldc,
+                                           const int* __restrict__ sfn, int nvalid, int n0, int k0) {
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int c = t + i * kGemmThreads;
+    const int k = c >> 6, nn = c & 63;
+    const int fk = sfn[k0 + k];
+    const int col = n0 + nn;
+    const int fn = col < nvalid ? sfn[col] : -1;
+    const bool ok = fk >= 0 && fn >= 0;
+    cp_async8(s + OpTile<false, 64>::idx(nn, k), ok ? P + (int64_t)fk * ldc + fn : P, ok);
+  }
+}
+
+// K3 (screened): CTA = (tile, half of its 128 points); loops over 64-wide
+// blocks of the tile's slots.  The tile's slot -> function list is kept in
+// shared memory after the GEMM stages.
+template <bool GGA>
+__global__ void __launch_bounds__(kGemmThreads) k_sdensity(const double* __restrict__ phi,
+                                                          const double* __restrict__ gx,
+                                                          const double* __restrict__ gy,
+                                                          const double* __restrict__ gz,
+                                                          const int64_t* __restrict__ tso, int64_t t0, int64_t s0,
+                                                          const int* __restrict__ slot_fn,
+                                                          const double* __restrict__ P, int64_t ldc,
+                                                          double* __restrict__ rho, double* __restrict__ grx,
+                                                          double* __restrict__ gry, double* __restrict__ grz) {
+  extern __shared__ double smem[];
+  constexpr int EA = OpTile<false, 64>::kElems, EB = OpTile<false, 64>::kElems;
+  double* sA = smem;
+  double* sB = smem + kStages * EA;
+  int* sfn = reinterpret_cast<int*>(smem + kStages * (EA + EB));
+  const int64_t t = t0 + blockIdx.x;
+  const int64_t sb = tso[t] - s0;
+  const int n = (int)(tso[t + 1] - tso[t]);
+  const int m0 = blockIdx.y * 64;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) sfn[i] = slot_fn[tso[t] + i];
+  __syncthreads();
+  const double* A = phi + sb * 128;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm0 = (warp >> 1) * 32, wn0 = (warp & 1) * 32;
+  const int fr = lane >> 2, fk = lane & 3;
+  const int nslab = n / kBK;
+  double rp[4][2] = {}, gp[3][4][2] = {};
+  for (int n0 = 0; n0 < n; n0 += 64) {
+    Acc acc;
+    acc.zero();
+#pragma unroll
+    for (int s = 0; s < kStages - 1; ++s) {
+      if (s < nslab) {
+        load_slab<false>(sA + s * EA, A, 128, m0, (int64_t)s * kBK);
+        load_gslab(sB + s * EB, P, ldc, sfn, n, n0, s * kBK);
+      }
+      cp_async_commit();
+    }
+    for (int it = 0; it < nslab; ++it) {
+      cp_async_wait<kStages - 2>();
+      __syncthreads();
+      {
+        const int nx = it + kStages - 1;
+        if (nx < nslab) {
+          const int st = nx % kStages;
+          load_slab<false>(sA + st * EA, A, 128, m0, (int64_t)nx * kBK);
+          load_gslab(sB + st * EB, P, ldc, sfn, n, n0, nx * kBK);
+        }
+        cp_async_commit();
+      }
+      const double* a_s = sA + (it % kStages) * EA;
+      const double* b_s = sB + (it % kStages) * EB;
+#pragma unroll
+      for (int kk = 0; kk < kBK; kk += 4) {
+        double af[4], bf[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) af[i] = a_s[OpTile<false, 64>::idx(wm0 + i * 8 + fr, kk + fk)];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) bf[j] = b_s[OpTile<false, 64>::idx(wn0 + j * 8 + fr, kk + fk)];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) dmma(acc.v[i][j], af[i], bf[j]);
+      }
+    }
+    cp_async_wait<0>();
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int r = m0 + wm0 + i * 8 + (lane >> 2);
+#pragma unroll
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int c = n0 + wn0 + j * 8 + 2 * (lane & 3) + e;
+          if (c < n) {
+            const double x = acc.v[i][j][e];
+            const int64_t o = (sb + c) * 128 + r;
+            rp[i][e] += x * phi[o];
+            if (GGA) {
+              gp[0][i][e] += x * gx[o];
+              gp[1][i][e] += x * gy[o];
+              gp[2][i][e] += x * gz[o];
+            }
+          }
+        }
+    }
+  }
+  // reduce the 4 lanes of a row, then the two column-warps through smem
+  double* red = smem;  // [2 warps-n][4 quantities][64 rows]
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    double v[4];
+    v[0] = rp[i][0] + rp[i][1];
+    if (GGA) {
+      v[1] = gp[0][i][0] + gp[0][i][1];
+      v[2] = gp[1][i][0] + gp[1][i][1];
+      v[3] = gp[2][i][0] + gp[2][i][1];
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (q > 0 && !GGA) break;
+      v[q] += __shfl_xor_sync(0xffffffffu, v[q], 1);
+      v[q] += __shfl_xor_sync(0xffffffffu, v[q], 2);
+      if ((lane & 3) == 0) red[((warp & 1) * 4 + q) * 64 + wm0 + i * 8 + (lane >> 2)] = v[q];
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < 64) {
+    const int r = threadIdx.x;
+    const int64_t o = (int64_t)blockIdx.x * 128 + m0 + r;
+    rho[o] = red[0 * 64 + r] + red[4 * 64 + r];
+    if (GGA) {
+      grx[o] = 2.0 * (red[1 * 64 + r] + red[5 * 64 + r]);
+      gry[o] = 2.0 * (red[2 * 64 + r] + red[6 * 64 + r]);
+      grz[o] = 2.0 * (red[3 * 64 + r] + red[7 * 64 + r]);
+    }
+  }
+}
+
+// Z[s][p] = A[p] phi[s][p] (+ B[p] . grad phi[s][p]) over the chunk's slots
+template <bool GGA>
+__global__ void k_szbuild(int64_t nslots, const int* __restrict__ slot_tile, int64_t t0,
+                          const double* __restrict__ phi, const double* __restrict__ gx,
+                          const double* __restrict__ gy, const double* __restrict__ gz,
+                          const double* __restrict__ A, const double* __restrict__ Bx,
+                          const double* __restrict__ By, const double* __restrict__ Bz, double* __restrict__ Z) {
+  const int64_t total = nslots * 128;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = ((int64_t)slot_tile[e >> 7] - t0) * 128 + (e & 127);
+    double z = A[p] * phi[e];
+    if (GGA) z += Bx[p] * gx[e] + By[p] * gy[e] + Bz[p] * gz[e];
+    Z[e] = z;
+  }
+}
+
+// (I, J) of pair q of the tile's 64-blocks: all nb^2 (GGA) or I <= J (LDA)
+__device__ __forceinline__ void pair_of(int q, int nb, bool all, int& I, int& J) {
+  if (all) {
+    I = q / nb;
+    J = q % nb;
+    return;
+  }
+  I = 0;
+  while (q >= nb - I) {
+    q -= nb - I;
+    ++I;
+  }
+  J = I + q;
+}
+
+// K4 (screened): H[fn_i][fn_j] += sum_p Z[i][p] phi[j][p] for the slots i, j
+// of one tile; LDA keeps fn_i <= fn_j only (H is symmetric).
+template <bool GGA>
+__global__ void __launch_bounds__(kGemmThreads) k_svpot(const double* __restrict__ phi, const double* __restrict__ Z,
+                                                       const int64_t* __restrict__ tso, int64_t t0, int64_t s0,
+                                                       const int* __restrict__ slot_fn, double* __restrict__ V,
+                                                       int64_t ldv) {
+  extern __shared__ double smem[];
+  constexpr int kGemmDoubles = kStages * (OpTile<true, 64>::kElems + OpTile<true, 64>::kElems);
+  int* sfn = reinterpret_cast<int*>(smem + kGemmDoubles);
+  const int64_t t = t0 + blockIdx.x;
+  const int64_t sb = tso[t] - s0;
+  const int n = (int)(tso[t + 1] - tso[t]);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) sfn[i] = slot_fn[tso[t] + i];
+  __syncthreads();
+  const int nb = (n + 63) / 64;
+  const int npairs = GGA ? nb * nb : nb * (nb + 1) / 2;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm0 = (warp >> 1) * 32, wn0 = (warp & 1) * 32;
+  for (int q = blockIdx.y; q < npairs; q += gridDim.y) {
+    int I, J;
+    pair_of(q, nb, GGA, I, J);
+    Acc acc;
+    acc.zero();
+    gemm_tile<true, true>(acc, Z + sb * 128, 128, (int64_t)I * 64, phi + sb * 128, 128, (int64_t)J * 64, 0, 128,
+                          smem);
+#pragma unroll
+    for (int ii = 0; ii < 4; ++ii) {
+      const int i = I * 64 + wm0 + ii * 8 + (lane >> 2);
+      const int fi = i < n ? sfn[i] : -1;
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj)
+#pragma unroll
+        for (int e = 0; e < 2; ++e) {
+          const int j = J * 64 + wn0 + jj * 8 + 2 * (lane & 3) + e;
+          const int fj = j < n ? sfn[j] : -1;
+          if (fi >= 0 && fj >= 0 && (GGA || fi <= fj)) atomicAdd(V + (int64_t)fi * ldv + fj, acc.v[ii][jj][e]);
+        }
+    }
+  }
+}
+
+}  // namespace
+
+// ham[spin + ispin*(j(j+1)/2 + k)] = V(k, j), k <= j; GGA: H(k, j) + H(j, k)
+__global__ void k_spack(const double* __restrict__ V, int64_t nbas, bool sym2, int ispin, int spin,
+                        double* __restrict__ ham) {
+  const int64_t len = nbas * (nbas + 1) / 2;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < len;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    int64_t j = (int64_t)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
+    while (j * (j + 1) / 2 > idx) --j;
+    while ((j + 1) * (j + 2) / 2 <= idx) ++j;
+    const int64_t k = idx - j * (j + 1) / 2;
+    double v = V[k * nbas + j];
+    if (sym2) v += V[j * nbas + k];
+    ham[spin + (int64_t)ispin * idx] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host planning
+// ---------------------------------------------------------------------------
+namespace {
+
+uint64_t spread3(uint64_t v) {  // 21 bits -> every third bit
+  v &= 0x1fffff;
+  v = (v | v << 32) & 0x1f00000000ffffull;
+  v = (v | v << 16) & 0x1f0000ff0000ffull;
+  v = (v | v << 8) & 0x100f00f00f00f00full;
+  v = (v | v << 4) & 0x10c30c30c30c30c3ull;
+  v = (v | v << 2) & 0x1249249249249249ull;
+  return v;
+}
+
+// Morton order of the grid points (ties by index: deterministic)
+std::vector<int64_t> morton_order(const double* g, int64_t n) {
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int d = 0; d < 3; ++d)
+    for (int64_t i = 0; i < n; ++i) {
+      lo[d] = std::min(lo[d], g[d * n + i]);
+      hi[d] = std::max(hi[d], g[d * n + i]);
+    }
+  std::vector<std::pair<uint64_t, int64_t>> key((size_t)n);
+  for (int64_t i = 0; i < n; ++i) {
+    uint64_t k = 0;
+    for (int d = 0; d < 3; ++d) {
+      const double span = hi[d] - lo[d];
+      const double u = span > 0 ? (g[d * n + i] - lo[d]) / span : 0.0;
+      const uint64_t q = (uint64_t)std::min(2097151.0, std::max(0.0, u * 2097151.0));
+      k |= spread3(q) << d;
+    }
+    key[(size_t)i] = {k, i};
+  }
+  std::sort(key.begin(), key.end());
+  std::vector<int64_t> perm((size_t)n);
+  for (int64_t i = 0; i < n; ++i) perm[(size_t)i] = key[(size_t)i].second;
+  return perm;
+}
+
+// Squared radius beyond which radial function rr of shell S is dropped.
+double listing_r2(const DevShell& S, int rr, const double* exps, const double* norms, const double* contr,
+                  double threshold, double sa_fac) {
+  std::vector<double> cf((size_t)S.nexp, 0.0);
+  if (rr < S.nunc) cf[(size_t)rr] = 1.0;
+  else
+    for (int e = 0; e < S.nexp; ++e) cf[(size_t)e] = contr[S.con_off + e + (int64_t)S.nexp * (rr - S.nunc)];
+  double amin = 1e300;
+  for (int e = 0; e < S.nexp; ++e)
+    if (cf[(size_t)e] != 0.0) amin = std::min(amin, exps[S.exp_off + e]);
+  if (amin == 1e300) return 0.0;  // identically zero function
+  // every primitive vanishes where alpha_min r^2 >= 50; margin for rounding
+  const double r2cut = 50.0 / amin * (1.0 + 1e-9);
+  if (threshold <= 0.0) return r2cut;
+  // bound on |phi| and |grad phi| at distance r:
+  //   sum_e |c_e| N_e exp(-a_e r^2) (r^l + 2 a_e r^(l+1) + (2l+1) r^(l-1)) * sa_fac
+  const int l = S.l;
+  auto bound = [&](double r) {
+    double b = 0.0;
+    for (int e = 0; e < S.nexp; ++e) {
+      if (cf[(size_t)e] == 0.0) continue;
+      const double a = exps[S.exp_off + e];
+      if (a * r * r >= 50.0) continue;
+      const double g = std::fabs(cf[(size_t)e]) * norms[S.exp_off + e] * std::exp(-a * r * r);
+      double poly = std::pow(r, l) + 2.0 * a * std::pow(r, l + 1);
+      if (l > 0) poly += (2 * l + 1) * std::pow(r, l - 1);
+      b += g * poly;
+    }
+    return b * sa_fac;
+  };
+  const double rcut = std::sqrt(r2cut);
+  const int nstep = 4000;
+  const double dr = rcut / nstep;
+  for (int i = nstep; i >= 0; --i) {
+    const double r = i * dr;
+    if (bound(r) >= threshold) {
+      const double R = std::min(rcut, r + dr);
+      return R * R;
+    }
+  }
+  return 0.0;
+}
+
+}  // namespace
+
+void screen_destroy(ScreenPlan* sp) {
+  if (!sp) return;
+  if (sp->mixed) screen_mixed_destroy(sp->mixed);
+  for (void* p : sp->allocs) cudaFree(p);
+  for (auto& e : sp->ev)
+    if (e) cudaEventDestroy(e);
+  delete sp;
+}
+
+void screen_stats(const ScreenPlan* sp, int64_t* ntiles, int64_t* nslots, int64_t* nlisted, double* sum_n2,
+                  int64_t* nchunks) {
+  if (ntiles) *ntiles = sp->ntiles;
+  if (nslots) *nslots = sp->nslots;
+  if (nlisted) *nlisted = sp->nlisted;
+  if (sum_n2) *sum_n2 = sp->sum_n2;
+  if (nchunks) *nchunks = (int64_t)sp->chunk_t0.size() - 1;
+}
+
+#define SP_TRY(call, what)                                                       \
+  do {                                                                           \
+    cudaError_t e_ = (call);                                                     \
+    if (e_ != cudaSuccess) {                                                     \
+      err = std::string(what) + ": " + cudaGetErrorString(e_);                   \
+      screen_destroy(sp);                                                        \
+      return e_ == cudaErrorMemoryAllocation ? PGXC_ENOMEM : PGXC_ECUDA;         \
+    }                                                                            \
+  } while (0)
+
+int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, cudaStream_t st, std::string& err) {
+  *out = nullptr;
+  ScreenPlan* sp = new ScreenPlan();
+  sp->gga = in.gga;
+  sp->nbas = in.nbas;
+  const std::vector<DevShell>& shells = *in.shells;
+  for (const DevShell& S : shells)
+    if (S.nrad > 64) {
+      err = "screened build: a shell has more than 64 radial functions";
+      screen_destroy(sp);
+      return PGXC_ENOTSUP;
+    }
+  for (auto& e : sp->ev) SP_TRY(cudaEventCreate(&e), "cudaEventCreate");
+  // --- Morton-ordered, 128-point tiles -----------------------------------
+  const int64_t n = in.npts;
+  const int64_t ntiles = (n + 127) / 128;
+  sp->ntiles = ntiles;
+  {
+    std::vector<int64_t> perm = morton_order(in.grdpts, n);
+    perm.resize((size_t)ntiles * 128, -1);
+    int64_t* dperm;
+    SP_TRY(cudaMalloc(&dperm, sizeof(int64_t) * perm.size()), "cudaMalloc");
+    const size_t nq = perm.size();
+    cudaError_t e = cudaMemcpy(dperm, perm.data(), sizeof(int64_t) * nq, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = sp_alloc(sp, &sp->qx, 4 * nq);
+    if (e == cudaSuccess) {
+      sp->qy = sp->qx + nq;
+      sp->qz = sp->qx + 2 * nq;
+      sp->qw = sp->qx + 3 * nq;
+      k_gather_points<<<(unsigned)((nq + 255) / 256), 256, 0, st>>>(dperm, (int64_t)nq, a.px, a.py, a.pz, a.w,
+                                                                   sp->qx, sp->qy, sp->qz, sp->qw);
+      e = cudaStreamSynchronize(st);
+    }
+    cudaFree(dperm);
+    SP_TRY(e, "grid reordering");
+  }
+  // --- tile-atom distances ------------------------------------------------
+  std::vector<float> d2((size_t)ntiles * in.natm);
+  {
+    float* dd2;
+    SP_TRY(cudaMalloc(&dd2, sizeof(float) * d2.size()), "cudaMalloc");
+    k_tile_atom_d2<<<(unsigned)ntiles, 128, 0, st>>>(sp->qx, sp->qy, sp->qz, a.atoms, in.natm, dd2);
+    cudaError_t e = cudaStreamSynchronize(st);
+    if (e == cudaSuccess) e = cudaMemcpy(d2.data(), dd2, sizeof(float) * d2.size(), cudaMemcpyDeviceToHost);
+    cudaFree(dd2);
+    SP_TRY(e, "tile distances");
+  }
+  // --- listing radii -------------------------------------------------------
+  double sa_fac[kMaxL + 1];
+  for (int l = 0; l <= kMaxL; ++l) {
+    sa_fac[l] = 1.0;
+    if (!a.sa.identity)
+      for (int i = 0; i < 2 * l + 1; ++i) {
+        double s = 0.0;
+        for (int m = 0; m < 2 * l + 1; ++m) s += std::fabs(a.sa.c[l][i][m]);
+        sa_fac[l] = std::max(sa_fac[l], s);
+      }
+  }
+  const int nsh = (int)shells.size();
+  std::vector<std::vector<double>> R2((size_t)nsh);
+  std::vector<double> shR2((size_t)nsh, 0.0);
+  for (int s = 0; s < nsh; ++s) {
+    const DevShell& S = shells[(size_t)s];
+    R2[(size_t)s].resize((size_t)S.nrad);
+    for (int rr = 0; rr < S.nrad; ++rr) {
+      R2[(size_t)s][(size_t)rr] = listing_r2(S, rr, in.exps, in.norms, in.contr, in.threshold, sa_fac[S.l]);
+      shR2[(size_t)s] = std::max(shR2[(size_t)s], R2[(size_t)s][(size_t)rr]);
+    }
+  }
+  // --- per-tile lists --------------------------------------------------------
+  std::vector<int64_t> tso((size_t)ntiles + 1, 0);
+  std::vector<int> slot_fn, slot_tile;
+  std::vector<BasisItem> items[kMaxL + 1];
+  std::vector<int64_t> tile_items[kMaxL + 1];  // items before tile t, per L
+  for (int l = 0; l <= kMaxL; ++l) tile_items[l].assign((size_t)ntiles + 1, 0);
+  slot_fn.reserve((size_t)ntiles * 64);
+  for (int64_t t = 0; t < ntiles; ++t) {
+    const int64_t base = (int64_t)slot_fn.size();
+    for (int l = 0; l <= kMaxL; ++l) tile_items[l][(size_t)t] = (int64_t)items[l].size();
+    for (int s = 0; s < nsh; ++s) {
+      const DevShell& S = shells[(size_t)s];
+      const double dd = d2[(size_t)t * in.natm + S.atom];
+      if (!(dd < shR2[(size_t)s])) continue;
+      uint64_t mask = 0;
+      for (int rr = 0; rr < S.nrad; ++rr)
+        if (dd < R2[(size_t)s][(size_t)rr]) mask |= 1ull << rr;
+      const int nsig = __builtin_popcountll(mask);
+      BasisItem it{};
+      it.tile = (int)t;
+      it.shell = s;
+      it.slot = (int64_t)slot_fn.size();
+      it.nsig = nsig;
+      it.mask = mask;
+      items[S.l].push_back(it);
+      for (int i = 0; i < 2 * S.l + 1; ++i)
+        for (int rr = 0; rr < S.nrad; ++rr)
+          if (mask >> rr & 1) slot_fn.push_back(S.f0 + i * S.nrad + rr);
+    }
+    const int64_t listed = (int64_t)slot_fn.size() - base;
+    sp->nlisted += listed;
+    while (((int64_t)slot_fn.size() - base) % kSlotAlign) slot_fn.push_back(-1);
+    const int64_t nt = (int64_t)slot_fn.size() - base;
+    sp->sum_n2 += (double)listed * (double)listed;
+    sp->max_n = std::max(sp->max_n, (int)nt);
+    slot_tile.resize(slot_fn.size(), (int)t);
+    tso[(size_t)t + 1] = (int64_t)slot_fn.size();
+  }
+  for (int l = 0; l <= kMaxL; ++l) tile_items[l][(size_t)ntiles] = (int64_t)items[l].size();
+  sp->nslots = (int64_t)slot_fn.size();
+  sp->h_tso = tso;
+  // --- chunks -------------------------------------------------------------------
+  const bool mixed = in.precision != PGXC_PREC_FP64;
+  size_t freeb = 0, totb = 0;
+  SP_TRY(cudaMemGetInfo(&freeb, &totb), "cudaMemGetInfo");
+  const int64_t per_slot = 128 * 8 * (in.gga ? 5 : 2) + (mixed ? screen_mixed_bytes_per_slot() : 0);
+  const int64_t per_tile = 128 * 8 * 8 + (mixed ? screen_mixed_bytes_per_tile() : 0);
+  int64_t budget_slots = (int64_t)(0.45 * (double)freeb) / per_slot;
+  budget_slots = std::max<int64_t>(budget_slots, sp->max_n);
+  int64_t budget_tiles = std::max<int64_t>(1, (int64_t)(0.05 * (double)freeb) / per_tile);
+  if (in.max_chunk_points > 0) budget_tiles = std::min(budget_tiles, std::max<int64_t>(1, in.max_chunk_points / 128));
+  budget_tiles = std::min<int64_t>(budget_tiles, 1 << 16);
+  sp->chunk_t0.push_back(0);
+  {
+    int64_t t0 = 0;
+    for (int64_t t = 0; t < ntiles; ++t) {
+      const bool full_slots = tso[(size_t)t + 1] - tso[(size_t)t0] > budget_slots;
+      const bool full_tiles = t - t0 + 1 > budget_tiles;
+      if (t > t0 && (full_slots || full_tiles)) {
+        sp->chunk_t0.push_back(t);
+        t0 = t;
+      }
+    }
+    sp->chunk_t0.push_back(ntiles);
+  }
+  const size_t nch = sp->chunk_t0.size() - 1;
+  for (size_t c = 0; c < nch; ++c) {
+    const int64_t t0 = sp->chunk_t0[c], t1 = sp->chunk_t0[c + 1];
+    sp->chunk_tiles = std::max(sp->chunk_tiles, t1 - t0);
+    sp->chunk_slots = std::max(sp->chunk_slots, tso[(size_t)t1] - tso[(size_t)t0]);
+  }
+  for (int l = 0; l <= kMaxL; ++l)
+    for (size_t c = 0; c <= nch; ++c) sp->item_off[l].push_back(tile_items[l][(size_t)sp->chunk_t0[c]]);
+  // --- device copies and buffers ------------------------------------------------
+  SP_TRY(sp_alloc(sp, &sp->tso, tso.size()), "cudaMalloc");
+  SP_TRY(cudaMemcpy(sp->tso, tso.data(), sizeof(int64_t) * tso.size(), cudaMemcpyHostToDevice), "copy");
+  SP_TRY(sp_alloc(sp, &sp->slot_fn, slot_fn.size()), "cudaMalloc");
+  SP_TRY(sp_alloc(sp, &sp->slot_tile, slot_tile.size()), "cudaMalloc");
+  if (!slot_fn.empty()) {
+    SP_TRY(cudaMemcpy(sp->slot_fn, slot_fn.data(), sizeof(int) * slot_fn.size(), cudaMemcpyHostToDevice), "copy");
+    SP_TRY(cudaMemcpy(sp->slot_tile, slot_tile.data(), sizeof(int) * slot_tile.size(), cudaMemcpyHostToDevice),
+           "copy");
+  }
+  for (int l = 0; l <= kMaxL; ++l) {
+    SP_TRY(sp_alloc(sp, &sp->items[l], items[l].size()), "cudaMalloc");
+    if (!items[l].empty())
+      SP_TRY(cudaMemcpy(sp->items[l], items[l].data(), sizeof(BasisItem) * items[l].size(), cudaMemcpyHostToDevice),
+             "copy");
+  }
+  const size_t rows = (size_t)(sp->chunk_slots + kSlack) * 128;
+  SP_TRY(sp_alloc(sp, &sp->phi, rows), "cudaMalloc (phi)");
+  SP_TRY(sp_alloc(sp, &sp->Z, rows), "cudaMalloc (Z)");
+  SP_TRY(cudaMemset(sp->phi, 0, sizeof(double) * rows), "memset");
+  SP_TRY(cudaMemset(sp->Z, 0, sizeof(double) * rows), "memset");
+  if (in.gga) {
+    SP_TRY(sp_alloc(sp, &sp->gx, rows), "cudaMalloc (grad phi)");
+    SP_TRY(sp_alloc(sp, &sp->gy, rows), "cudaMalloc (grad phi)");
+    SP_TRY(sp_alloc(sp, &sp->gz, rows), "cudaMalloc (grad phi)");
+    SP_TRY(cudaMemset(sp->gx, 0, sizeof(double) * rows), "memset");
+    SP_TRY(cudaMemset(sp->gy, 0, sizeof(double) * rows), "memset");
+    SP_TRY(cudaMemset(sp->gz, 0, sizeof(double) * rows), "memset");
+  }
+  const int64_t cp = sp->chunk_tiles * 128;
+  SP_TRY(sp_alloc(sp, &sp->pt, 8 * (size_t)cp), "cudaMalloc");
+  SP_TRY(sp_alloc(sp, &sp->partial, 2 * (size_t)((cp + 255) / 256) + 2), "cudaMalloc");
+  SP_TRY(sp_alloc(sp, &sp->V, (size_t)in.nbas * in.nbas), "cudaMalloc (V)");
+  if (mixed) {
+    ScreenMixedInput mi;
+    mi.nbas = in.nbas;
+    mi.ldc = a.ldc;
+    mi.gga = in.gga;
+    mi.chunk_slots = sp->chunk_slots + kSlack;
+    mi.chunk_tiles = sp->chunk_tiles;
+    mi.max_n = sp->max_n;
+    const int st2 = screen_mixed_create(&sp->mixed, mi, err);
+    if (st2) {
+      screen_destroy(sp);
+      return st2;
+    }
+  }
+  *out = sp;
+  return PGXC_OK;
+}
+
+int screen_run(ScreenPlan* sp, const BuildArgs& a, cudaStream_t st, double* ham, int ispin, int spin,
+               ScreenTimes* tm, std::string& err) {
+  const bool gga = sp->gga;
+  ScreenTimes T;
+  cudaEvent_t* ev = sp->ev;
+#define SR_TRY(call)                                                          \
+  do {                                                                        \
+    cudaError_t e_ = (call);                                                  \
+    if (e_ != cudaSuccess) {                                                  \
+      err = std::string("screened build: ") + cudaGetErrorString(e_);         \
+      return PGXC_ECUDA;                                                      \
+    }                                                                         \
+  } while (0)
+  SR_TRY(cudaMemsetAsync(sp->V, 0, sizeof(double) * sp->nbas * sp->nbas, st));
+  if (sp->mixed) {
+    SR_TRY(cudaEventRecord(ev[0], st));
+    T.launches += screen_mixed_prepare(sp->mixed, a, st);
+    SR_TRY(cudaEventRecord(ev[1], st));
+  }
+  const int64_t cp = sp->chunk_tiles * 128;
+  BuildArgs b = a;  // per-chunk point arrays for the functional
+  b.ldp = cp;
+  b.w = nullptr;
+  b.rho = sp->pt;
+  b.grx = sp->pt + cp;
+  b.gry = sp->pt + 2 * cp;
+  b.grz = sp->pt + 3 * cp;
+  b.A = sp->pt + 4 * cp;
+  b.Bx = sp->pt + 5 * cp;
+  b.By = sp->pt + 6 * cp;
+  b.Bz = sp->pt + 7 * cp;
+  b.partial = sp->partial;
+  const size_t nch = sp->chunk_t0.size() - 1;
+  float ms;
+  for (size_t c = 0; c < nch; ++c) {
+    const int64_t t0 = sp->chunk_t0[c], t1 = sp->chunk_t0[c + 1], nt = t1 - t0;
+    const int64_t s0 = sp->h_tso[(size_t)t0], ns = sp->h_tso[(size_t)t1] - s0;
+    const int64_t npt = nt * 128;
+    SR_TRY(cudaEventRecord(ev[2], st));
+    // K1
+    {
+      auto launch_l = [&](auto Lc) {
+        constexpr int L = decltype(Lc)::value;
+        const int64_t i0 = sp->item_off[L][c], i1 = sp->item_off[L][c + 1];
+        if (i1 <= i0) return;
+        if (gga)
+          k_basis_items<L, true><<<(unsigned)(i1 - i0), 128, 0, st>>>(
+              sp->items[L] + i0, a.shells, a.atoms, a.exps, a.norms, a.contr, a.sa, sp->qx, sp->qy, sp->qz, s0,
+              sp->phi, sp->gx, sp->gy, sp->gz);
+        else
+          k_basis_items<L, false><<<(unsigned)(i1 - i0), 128, 0, st>>>(
+              sp->items[L] + i0, a.shells, a.atoms, a.exps, a.norms, a.contr, a.sa, sp->qx, sp->qy, sp->qz, s0,
+              sp->phi, nullptr, nullptr, nullptr);
+        ++T.launches;
+      };
+      launch_l(std::integral_constant<int, 0>());
+      launch_l(std::integral_constant<int, 1>());
+      launch_l(std::integral_constant<int, 2>());
+      launch_l(std::integral_constant<int, 3>());
+      const unsigned nb = (unsigned)std::max<int64_t>(1, std::min<int64_t>((ns * 128 + 255) / 256, 148 * 32));
+      if (gga) k_pad_zero<true><<<nb, 256, 0, st>>>(sp->slot_fn + s0, ns, sp->phi, sp->gx, sp->gy, sp->gz);
+      else k_pad_zero<false><<<nb, 256, 0, st>>>(sp->slot_fn + s0, ns, sp->phi, nullptr, nullptr, nullptr);
+      ++T.launches;
+      if (sp->mixed) T.launches += screen_mixed_basis(sp->mixed, sp->tso, t0, nt, s0, sp->phi, st);
+    }
+    SR_TRY(cudaEventRecord(ev[3], st));
+    // K3
+    SR_TRY(cudaEventRecord(ev[4], st));
+    if (sp->mixed) {
+      T.launches += screen_mixed_density(sp->mixed, sp->tso, sp->slot_fn, t0, nt, s0, sp->phi, sp->gx, sp->gy,
+                                         sp->gz, b.rho, b.grx, b.gry, b.grz, st);
+    } else {
+      const int smem = gemm_smem_bytes<false, false>() + (int)sizeof(int) * sp->max_n;
+      dim3 grid((unsigned)nt, 2);
+      if (gga) {
+        cudaFuncSetAttribute(k_sdensity<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        k_sdensity<true><<<grid, kGemmThreads, smem, st>>>(sp->phi, sp->gx, sp->gy, sp->gz, sp->tso, t0, s0,
+                                                           sp->slot_fn, a.P, a.ldc, b.rho, b.grx, b.gry, b.grz);
+      } else {
+        cudaFuncSetAttribute(k_sdensity<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        k_sdensity<false><<<grid, kGemmThreads, smem, st>>>(sp->phi, nullptr, nullptr, nullptr, sp->tso, t0, s0,
+                                                            sp->slot_fn, a.P, a.ldc, b.rho, nullptr, nullptr,
+                                                            nullptr);
+      }
+      ++T.launches;
+    }
+    SR_TRY(cudaEventRecord(ev[5], st));
+    // K2
+    {
+      BuildArgs bf = b;
+      bf.w = sp->qw;
+      launch_functional_f64(bf, t0 * 128, npt, gga, st);
+      T.launches += 2;
+    }
+    SR_TRY(cudaEventRecord(ev[6], st));
+    // K4
+    if (sp->mixed) {
+      T.launches += screen_mixed_potential(sp->mixed, sp->tso, sp->slot_fn, sp->slot_tile, t0, nt, s0, ns, sp->phi,
+                                           sp->gx, sp->gy, sp->gz, b.A, b.Bx, b.By, b.Bz, sp->V, sp->nbas, st,
+                                           ev[7], ev[8]);
+    } else {
+      const unsigned nb = (unsigned)std::max<int64_t>(1, std::min<int64_t>((ns * 128 + 255) / 256, 148 * 32));
+      if (gga)
+        k_szbuild<true><<<nb, 256, 0, st>>>(ns, sp->slot_tile + s0, t0, sp->phi, sp->gx, sp->gy, sp->gz, b.A, b.Bx,
+                                            b.By, b.Bz, sp->Z);
+      else
+        k_szbuild<false><<<nb, 256, 0, st>>>(ns, sp->slot_tile + s0, t0, sp->phi, nullptr, nullptr, nullptr, b.A,
+                                             nullptr, nullptr, nullptr, sp->Z);
+      SR_TRY(cudaEventRecord(ev[7], st));
+      const int smem = gemm_smem_bytes<true, true>() + (int)sizeof(int) * sp->max_n;
+      dim3 grid((unsigned)nt, 4);
+      if (gga) {
+        cudaFuncSetAttribute(k_svpot<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        k_svpot<true><<<grid, kGemmThreads, smem, st>>>(sp->phi, sp->Z, sp->tso, t0, s0, sp->slot_fn, sp->V,
+                                                        sp->nbas);
+      } else {
+        cudaFuncSetAttribute(k_svpot<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        k_svpot<false><<<grid, kGemmThreads, smem, st>>>(sp->phi, sp->Z, sp->tso, t0, s0, sp->slot_fn, sp->V,
+                                                         sp->nbas);
+      }
+      SR_TRY(cudaEventRecord(ev[8], st));
+      T.launches += 2;
+    }
+    SR_TRY(cudaGetLastError());
+    SR_TRY(cudaEventRecord(ev[9], st));
+    SR_TRY(cudaEventSynchronize(ev[9]));
+    SR_TRY(cudaEventElapsedTime(&ms, ev[2], ev[3])); T.basis += ms;
+    SR_TRY(cudaEventElapsedTime(&ms, ev[4], ev[5])); T.density += ms; T.x += ms;
+    SR_TRY(cudaEventElapsedTime(&ms, ev[5], ev[6])); T.functional += ms;
+    SR_TRY(cudaEventElapsedTime(&ms, ev[6], ev[9])); T.potential += ms;
+    SR_TRY(cudaEventElapsedTime(&ms, ev[7], ev[8])); T.v += ms;
+  }
+  if (sp->mixed) {
+    SR_TRY(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    T.density += ms;
+  }
+  SR_TRY(cudaEventRecord(ev[2], st));
+  {
+    const int64_t len = sp->nbas * (sp->nbas + 1) / 2;
+    const unsigned nb = (unsigned)std::min<int64_t>((len + 255) / 256, 148 * 8);
+    k_spack<<<nb, 256, 0, st>>>(sp->V, sp->nbas, gga, ispin, spin, ham);
+    ++T.launches;
+  }
+  SR_TRY(cudaGetLastError());
+  SR_TRY(cudaEventRecord(ev[3], st));
+  SR_TRY(cudaEventSynchronize(ev[3]));
+  SR_TRY(cudaEventElapsedTime(&ms, ev[2], ev[3]));
+  T.potential += ms;
+  if (sp->mixed) {
+    int flag = 0;
+    if (screen_mixed_error_flag(sp->mixed, st, &flag) != PGXC_OK) {
+      err = "screened build: error-flag read failed";
+      return PGXC_ECUDA;
+    }
+    if (flag) {
+      err = "screened build: a bounded tensor-core pipeline wait ran out";
+      return PGXC_ETIMEOUT;
+    }
+  }
+#undef SR_TRY
+  if (tm) *tm = T;
+  return PGXC_OK;
+}
+
+}  // namespace pgxc

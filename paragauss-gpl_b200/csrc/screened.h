@@ -1,0 +1,61 @@
+// screened.h -- the screened (tile-sparse) XC build.
+//
+// The grid is reordered along a Morton curve and cut into tiles of 128 points
+// (the reference's vla batches, made spatially compact).  For every tile the
+// basis functions that can be nonzero on it are listed once per geometry;
+// every per-cycle stage then works on the tile's compact [slot][128] block:
+// the basis is evaluated only for listed functions, X = phi P_sig gathers the
+// listed rows and columns of P, and V_sig = Z^T phi is scatter-added into V.
+//
+// A function is listed for a tile when, for some point of the tile,
+//   threshold == 0: some primitive has alpha r^2 < 50 (the reference's own
+//                   cutoff, modules/orbital_module.f90:1831-1854: every
+//                   unlisted function is exactly zero on the tile);
+//   threshold  > 0: in addition a bound on |phi| and |grad phi| reaches the
+//                   threshold.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+
+namespace pgxc {
+
+struct ScreenPlan;
+
+struct ScreenTimes {
+  float basis = 0, density = 0, functional = 0, potential = 0, x = 0, v = 0;
+  int64_t launches = 0;
+};
+
+// Host-side description of the context, for planning.
+struct ScreenInput {
+  const std::vector<DevShell>* shells;
+  const double* atoms;        // host, 3 x natm
+  int natm;
+  int64_t nbas;
+  const double* grdpts;       // host, npts x 4 column-major (x, y, z, w)
+  int64_t npts;
+  const double* exps;         // host
+  const double* norms;        // host
+  const double* contr;        // host
+  double threshold;
+  bool gga;
+  int precision;              // PGXC_PREC_*
+  int64_t max_chunk_points;   // 0: sized from free device memory
+};
+
+int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, cudaStream_t st, std::string& err);
+void screen_destroy(ScreenPlan* sp);
+// One build: P (FP64, a.P) must be ready; E_xc / N_el are Kahan-added into
+// a.acc; the packed matrix of spin `spin` is written to ham.
+int screen_run(ScreenPlan* sp, const BuildArgs& a, cudaStream_t st, double* ham, int ispin, int spin,
+               ScreenTimes* t, std::string& err);
+// Plan statistics: tiles, total slots (padded), listed functions, sum of n_t^2.
+void screen_stats(const ScreenPlan* sp, int64_t* ntiles, int64_t* nslots, int64_t* nlisted, double* sum_n2,
+                  int64_t* nchunks);
+
+}  // namespace pgxc

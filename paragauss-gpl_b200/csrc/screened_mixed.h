@@ -1,0 +1,46 @@
+// screened_mixed.h -- INT8 tensor-core (tcgen05 kind::i8, Ozaki split) stages
+// of the screened XC build.  The FP64 basis, the functional and the packing are
+// shared with the FP64 screened build (screened.cu).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+
+namespace pgxc {
+
+struct ScreenMixed;
+
+struct ScreenMixedInput {
+  int64_t nbas = 0, ldc = 0;
+  bool gga = false;
+  int64_t chunk_slots = 0;   // slot rows of the chunk buffers (slack included)
+  int64_t chunk_tiles = 0;
+  int max_n = 0;             // largest padded slot count of a tile
+};
+
+// device bytes per slot row and per tile of the chunk buffers
+int64_t screen_mixed_bytes_per_slot();
+int64_t screen_mixed_bytes_per_tile();
+int screen_mixed_create(ScreenMixed** out, const ScreenMixedInput& in, std::string& err);
+void screen_mixed_destroy(ScreenMixed* m);
+// INT8 digits of the FP64 density matrix a.P (per-row scales); returns launches
+int screen_mixed_prepare(ScreenMixed* m, const BuildArgs& a, cudaStream_t st);
+// INT8 digits of phi for the density contraction (per-point scales)
+int screen_mixed_basis(ScreenMixed* m, const int64_t* tso, int64_t t0, int64_t nt, int64_t s0, const double* phi,
+                       cudaStream_t st);
+int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
+                         const double* phi, const double* gx, const double* gy, const double* gz, double* rho,
+                         double* grx, double* gry, double* grz, cudaStream_t st);
+// Z digits (per-slot scales), then H[S_t, S_t] += Z_t^T phi_t scatter-added into V;
+// records k0 / k1 around the contraction kernel
+int screen_mixed_potential(ScreenMixed* m, const int64_t* tso, const int* slot_fn, const int* slot_tile, int64_t t0,
+                           int64_t nt, int64_t s0, int64_t ns, const double* phi, const double* gx, const double* gy,
+                           const double* gz, const double* A, const double* Bx, const double* By, const double* Bz,
+                           double* V, int64_t ldv, cudaStream_t st, cudaEvent_t k0, cudaEvent_t k1);
+// copies the device error flag (a bounded wait ran out) to *flag and clears it
+int screen_mixed_error_flag(ScreenMixed* m, cudaStream_t st, int* flag);
+
+}  // namespace pgxc

@@ -33,6 +33,7 @@ def lib():
     L.pgxc_default_options.argtypes = [P(abi.Options)]
     L.pgxc_create.argtypes = [P(abi.Geometry), P(abi.Basis), P(abi.Grid), P(abi.Options), P(vp)]
     L.pgxc_nbas.argtypes = [vp, P(ct.c_int32)]
+    L.pgxc_screen_stats.argtypes = [vp, P(ct.c_int64), P(ct.c_int64), P(ct.c_int64), P(ct.c_double)]
     L.pgxc_build.argtypes = [vp, abi._f64p, abi._f64p, ct.c_int32, ct.c_int32, ct.c_int32, abi._f64p, ct.c_int64,
                              P(ct.c_double), P(ct.c_double), P(abi.Timings)]
     L.pgxc_build_device.argtypes = [vp, vp, vp, ct.c_int32, ct.c_int32, ct.c_int32, vp, ct.c_int64, vp,
@@ -109,6 +110,12 @@ class Context:
                                      ct.byref(tm))
         _check(st, self.h)
         return tm.as_dict()
+
+    def screen_stats(self):
+        """{ntiles, nslots, nlisted, sum_n2} of a screened context."""
+        v = [ct.c_int64(), ct.c_int64(), ct.c_int64(), ct.c_double()]
+        _check(lib().pgxc_screen_stats(self.h, *[ct.byref(x) for x in v]), self.h)
+        return dict(ntiles=v[0].value, nslots=v[1].value, nlisted=v[2].value, sum_n2=v[3].value)
 
     def grid_weights(self):
         w = np.zeros(self.case.npts)

@@ -16,6 +16,7 @@ pytestmark = pytest.mark.gpu
 
 def run_mixed(case, **kw):
     ref_ham, ref_exc, ref_nel = O.xc_build(case)
+    kw.setdefault("screen_threshold", -1.0)
     with lib.Context(case, precision="mixed", **kw) as ctx:
         ham, exc, nel = ctx.build()
     return abs(exc - ref_exc), abs(nel - ref_nel), float(np.max(np.abs(ham - ref_ham)))

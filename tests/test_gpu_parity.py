@@ -1,8 +1,13 @@
 """FP64 GPU path (libpgxc through its C ABI) against the FP64 CPU oracle.
 
 Bar: E_xc and N_el within 1e-10 Eh / electrons and every packed V_xc element
-within 1e-10, as the drop-in requirement states.
+within 1e-10, as the drop-in requirement states.  Every build is checked in
+both layouts: dense (screen_threshold < 0) and screened with the reference's
+own cutoff (screen_threshold = 0, per-tile lists of the functions that are
+not identically zero).
 """
+import functools
+
 import numpy as np
 import pytest
 
@@ -12,6 +17,7 @@ from pgxc import cases, lib
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-10
+LAYOUTS = pytest.mark.parametrize("thr", [-1.0, 0.0], ids=["dense", "screened"])
 
 
 def compare(case, **kw):
@@ -22,32 +28,37 @@ def compare(case, **kw):
     return dE, dN, dV, (ref_ham, ref_exc, ref_nel), (ham, exc, nel)
 
 
+@LAYOUTS
 @pytest.mark.parametrize("xc", ["VWN", "PBE"])
-def test_water_fp64(xc):
+def test_water_fp64(xc, thr):
     c = cases.config(1)
     c.functional = xc
     O.weight_case(c)
-    dE, dN, dV, _, _ = compare(c)
+    dE, dN, dV, _, _ = compare(c, screen_threshold=thr)
     assert dE < TOL and dN < TOL and dV < TOL, (dE, dN, dV)
 
 
+@LAYOUTS
 @pytest.mark.parametrize("xc,seed,lmax", [("VWN", 1, 2), ("PBE", 2, 2), ("PBE", 3, 3), ("VWN", 4, 3)])
-def test_small_cases_multi_chunk(xc, seed, lmax):
+def test_small_cases_multi_chunk(xc, seed, lmax, thr):
     c = cases.small_case(functional=xc, seed=seed, lmax=lmax, natoms=5, nocc=7)
     O.weight_case(c)
-    # a chunk of 1024 points forces several chunks and the split-K accumulation across them
-    dE, dN, dV, _, _ = compare(c, max_chunk_points=1024)
+    # a chunk of 1024 points forces several chunks and the accumulation across them
+    dE, dN, dV, _, _ = compare(c, max_chunk_points=1024, screen_threshold=thr)
     assert dE < TOL and dN < TOL and dV < TOL, (dE, dN, dV)
 
 
-def test_accumulates_into_caller_arrays():
+@LAYOUTS
+def test_accumulates_into_caller_arrays(thr):
     c = cases.small_case(functional="PBE", seed=5)
     O.weight_case(c)
-    with lib.Context(c) as ctx:
+    with lib.Context(c, screen_threshold=thr) as ctx:
         h1, e1, n1 = ctx.build()
         h2 = np.full(c.xc_length, 0.25)
         h2, e2, n2 = ctx.build(ham=h2)
     np.testing.assert_allclose(h2 - 0.25, h1, atol=1e-14)
+    # E and N are reduced in a fixed order; V may differ in the last bits
+    # where the screened build scatter-adds with atomics
     assert e1 == e2 and n1 == n2
 
 
@@ -58,10 +69,11 @@ def test_device_becke_matches_oracle():
     np.testing.assert_allclose(w_gpu, w_ref, rtol=0, atol=2e-16)
 
 
-def test_raw_weight_grid_is_becke_scaled_on_device():
+@LAYOUTS
+def test_raw_weight_grid_is_becke_scaled_on_device(thr):
     c = cases.small_case(functional="PBE", seed=9)
     O.weight_case(c)
-    with lib.Context(c, weighted=False) as ctx:
+    with lib.Context(c, weighted=False, screen_threshold=thr) as ctx:
         w = ctx.grid_weights()
         ham, exc, nel = ctx.build()
     np.testing.assert_allclose(w, c.grid_w, rtol=1e-15, atol=0)
@@ -119,20 +131,44 @@ def test_orbital_values_and_gradients():
     np.testing.assert_allclose(gr, rgr, rtol=1e-12, atol=1e-14)
 
 
-def test_empty_occupation():
+@LAYOUTS
+def test_empty_occupation(thr):
     c = cases.small_case(functional="VWN", seed=10)
     O.weight_case(c)
     c.nocc = 0
     c.C = np.zeros((c.nbas, 0, 1))
     c.occ = np.zeros((0, 1))
-    dE, dN, dV, _, _ = compare(c)
+    dE, dN, dV, _, _ = compare(c, screen_threshold=thr)
     assert dE < TOL and dN < TOL and dV < TOL
 
 
-def test_ch60_pbe_full_size_fp64():
-    """The benchmark workload at full size: 60 atoms, 690 functions, ~1.16M points."""
+@functools.lru_cache(maxsize=1)
+def ch60():
     c = cases.config(2)
     O.weight_case(c)
-    dE, dN, dV, ref, got = compare(c)
-    print(f"CH60 PBE: E_xc={got[1]:.12f} |dE|={dE:.2e} |dN|={dN:.2e} max|dV|={dV:.2e}")
+    return c, O.xc_build(c)
+
+
+@LAYOUTS
+def test_ch60_pbe_full_size_fp64(thr):
+    """The benchmark workload at full size: 60 atoms, 690 functions, ~1.16M points."""
+    c, (ref_ham, ref_exc, ref_nel) = ch60()
+    with lib.Context(c, screen_threshold=thr) as ctx:
+        ham, exc, nel = ctx.build()
+    dE, dN, dV = abs(exc - ref_exc), abs(nel - ref_nel), float(np.max(np.abs(ham - ref_ham)))
+    print(f"CH60 PBE thr={thr}: E_xc={exc:.12f} |dE|={dE:.2e} |dN|={dN:.2e} max|dV|={dV:.2e}")
     assert dE < TOL and dN < TOL and dV < TOL, (dE, dN, dV)
+
+
+def test_ch60_pbe_threshold_1e10():
+    """Value screening at 1e-10 (the workload's stated threshold) against the
+    unscreened oracle: the dropped functions are below 1e-10 on their tiles."""
+    c, (ref_ham, ref_exc, ref_nel) = ch60()
+    with lib.Context(c, screen_threshold=1e-10) as ctx:
+        ham, exc, nel = ctx.build()
+        st = ctx.screen_stats()
+    dE, dN, dV = abs(exc - ref_exc), abs(nel - ref_nel), float(np.max(np.abs(ham - ref_ham)))
+    frac = st["sum_n2"] / (st["ntiles"] * c.nbas ** 2)
+    print(f"CH60 PBE thr=1e-10: |dE|={dE:.2e} |dN|={dN:.2e} max|dV|={dV:.2e} "
+          f"listed/tile={st['nlisted'] / st['ntiles']:.1f} work={frac:.3f} of dense")
+    assert dE < 1e-8 and dN < 1e-8 and dV < 1e-8, (dE, dN, dV)
