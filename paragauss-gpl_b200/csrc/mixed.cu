@@ -36,15 +36,13 @@
 
 #include "kernels.h"
 #include "mixed.h"
+#include "ozaki.cuh"
 #include "tc.cuh"
 
 namespace pgxc {
 
 namespace {
 
-constexpr int kSlices = 5;           // 7-bit digits per operand
-constexpr int kGroups = 5;           // digit-pair groups s + t = 0..4
-constexpr int kPairs = 15;
 constexpr int kRowsA = 128;          // M of every MMA
 constexpr int kRowsB = 96;           // N of every MMA
 constexpr int kBlkA = kRowsA * 32;   // one slice of a 128-row x 32-byte K block
@@ -54,34 +52,6 @@ constexpr int kOpB = kSlices * kBlkB;
 constexpr int kStages = 5;           // bulk-copy ring depth
 constexpr int kKStep = 32;           // K elements per int8 MMA
 constexpr int kAlignFn = 384;        // functions padded to lcm(128, 96)
-
-// digit-pair list (s, t, group s + t); the first pair of each group starts its accumulator
-__constant__ int c_oz_pairs[kPairs][3] = {{0, 0, 0}, {0, 1, 1}, {1, 0, 1}, {0, 2, 2}, {1, 1, 2},
-                                          {2, 0, 2}, {0, 3, 3}, {1, 2, 3}, {2, 1, 3}, {3, 0, 3},
-                                          {0, 4, 4}, {1, 3, 4}, {2, 2, 4}, {3, 1, 4}, {4, 0, 4}};
-__host__ __device__ constexpr bool pair_leads(int q) { return q == 0 || q == 1 || q == 3 || q == 6 || q == 10; }
-
-// offset of element (row r, K byte k) inside a rows x 32 K-major int8 block:
-// core matrices of 8 rows x 16 bytes; LBO (K halves) = 128 B, SBO (8-row groups) = 256 B
-__host__ __device__ constexpr int blk_off(int r, int k) {
-  return (r & 7) * 16 + (k & 15) + (k >> 4) * 128 + (r >> 3) * 256;
-}
-
-// power-of-two exponent e with |v| / 2^e < 1 for all |v| <= mx (0 for mx == 0)
-__device__ __forceinline__ int scale_exp(double mx) { return mx > 0.0 ? ilogb(mx) + 1 : 0; }
-
-// 5 balanced base-128 digits of round(v * 2^(34 - e)), most significant first:
-// v ~= 2^e * sum_s d_s 2^(-6-7s)
-__device__ __forceinline__ void digits(double v, int e, int8_t (&d)[kSlices]) {
-  long long q = llrint(ldexp(v, 34 - e));
-#pragma unroll
-  for (int s = kSlices - 1; s >= 1; --s) {
-    const long long r = ((q + 64) & 127) - 64;
-    d[s] = (int8_t)r;
-    q = (q - r) >> 7;
-  }
-  d[0] = (int8_t)q;  // |q| <= 64
-}
 
 }  // namespace
 
@@ -293,12 +263,6 @@ __device__ __forceinline__ void oz_read16(uint32_t trow, int c0, double (&x)[16]
   }
 }
 
-// 2^e built from the bit pattern; exponents below the normal range give
-// 2^-1022 (every such term is below 2^-960 in magnitude)
-__device__ __forceinline__ double pow2(int e) {
-  return __longlong_as_double((long long)(max(e, -1022) + 1023) << 52);
-}
-constexpr int kCombShift = -12 - 7 * (kGroups - 1);  // x * 2^kCombShift = sum_g 2^(-12-7g) D_g
 
 // ---------------------------------------------------------------------------
 // G1: density.  CTA = 128 points (TMEM lane = point).  For each 96-wide tile

@@ -46,3 +46,38 @@ def test_many_orbitals_two_chunks():
     O.weight_case(c)
     dE, dN, dV = run_mixed(c)
     assert dE < 1e-7 and dN < 1e-7 and dV < 1e-7, (dE, dN, dV)
+
+
+# ---------------------------------------------------------------------------
+# screened layout: per-tile lists, gathered P, scatter-added V
+# ---------------------------------------------------------------------------
+SCREENED = pytest.mark.parametrize("thr", [0.0, 1e-10], ids=["exact", "1e-10"])
+
+
+@SCREENED
+@pytest.mark.parametrize("xc", ["VWN", "PBE"])
+def test_water_mixed_screened(xc, thr):
+    c = cases.config(1)
+    c.functional = xc
+    O.weight_case(c)
+    dE, dN, dV = run_mixed(c, screen_threshold=thr)
+    print(f"water {xc} mixed screened {thr}: |dE|={dE:.2e} |dN|={dN:.2e} max|dV|={dV:.2e}")
+    assert dE < 1e-7 and dN < 1e-7 and dV < 1e-7, (dE, dN, dV)
+
+
+@SCREENED
+@pytest.mark.parametrize("xc,seed,lmax", [("PBE", 2, 2), ("VWN", 4, 3), ("PBE", 3, 3), ("VWN", 1, 2)])
+def test_small_mixed_screened_multi_chunk(xc, seed, lmax, thr):
+    c = cases.small_case(functional=xc, seed=seed, lmax=lmax, natoms=5, nocc=7)
+    O.weight_case(c)
+    dE, dN, dV = run_mixed(c, max_chunk_points=1024, screen_threshold=thr)
+    assert dE < 1e-7 and dN < 1e-7 and dV < 1e-7, (dE, dN, dV)
+
+
+def test_ch60_mixed_screened_full_size():
+    """The benchmark workload: 60 atoms, 690 functions, 1.16M points, 1e-10 screening."""
+    c = cases.config(2)
+    O.weight_case(c)
+    dE, dN, dV = run_mixed(c, screen_threshold=1e-10)
+    print(f"CH60 PBE mixed screened 1e-10: |dE|={dE:.2e} |dN|={dN:.2e} max|dV|={dV:.2e}")
+    assert dE < 1e-6 and dN < 1e-7 and dV < 1e-7, (dE, dN, dV)
