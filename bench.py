@@ -46,6 +46,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--max-chunk-points", type=int, default=0,
                    help="cap on grid points per device chunk (0: sized from free HBM)")
+    p.add_argument("--screen", type=float, default=1e-10,
+                   help="per-tile basis screening threshold (0: exact cutoff only, <0: dense layout)")
     p.add_argument("--profile", action="store_true",
                    help="one build only (for ncu): no warm-up loop, e2e, CPU baseline or peak probe")
     return p.parse_args()
@@ -198,7 +200,8 @@ def fp64_comparison(torch, case, sub, local, args):
     oracle at 1e-10) on the same GPU: its throughput and its V_xc, E_xc, N_el
     as the accuracy reference of the headline path."""
     from pgxc import lib
-    ctx = lib.Context(sub, precision="fp64", weighted=False, device=local, max_chunk_points=args.max_chunk_points)
+    ctx = lib.Context(sub, precision="fp64", weighted=False, device=local, max_chunk_points=args.max_chunk_points,
+                      screen_threshold=args.screen)
     dC = torch.from_numpy(case.c_fortran()).cuda()
     docc = torch.from_numpy(case.occ_fortran()).cuda()
     dham = torch.zeros(case.xc_length, dtype=torch.float64, device="cuda")
@@ -294,7 +297,9 @@ def main():
     fp64_leg = None
     if prec != "fp64" and world == 1 and not args.profile:
         fp64_leg = fp64_comparison(torch, case, sub, local, args)
-    ctx = lib.Context(sub, precision=prec, weighted=False, device=local, max_chunk_points=args.max_chunk_points)
+    ctx = lib.Context(sub, precision=prec, weighted=False, device=local, max_chunk_points=args.max_chunk_points,
+                      screen_threshold=args.screen)
+    screen = ctx.screen_stats() if args.screen >= 0 else None
     if args.profile:
         d = ctx.build(timings=True)
         print(json.dumps({"profile": True, "precision": prec, "E_xc": d[1], "N_el": d[2], "timings": d[3]}),

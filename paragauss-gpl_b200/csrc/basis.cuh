@@ -99,11 +99,13 @@ __device__ __forceinline__ double prim_value(double alpha, double norm, double r
 // at row base + i*nsel + k, column p of the [row][ld] arrays.  The dense
 // layout is mask = all nrad bits, base = S.f0 (row = function index); the
 // screened layout is the tile's significant radial functions and their slot.
-// exps/norms/contr may point to shared memory (plain loads).
+// exps/norms/contr/rng may point to shared memory (plain loads); rng is the
+// shell's [lo, hi) primitive range per contraction (used when S.seg).
 template <int L, bool GRAD>
 __device__ __forceinline__ void shell_at_point(const DevShell& S, const DevSA& sa, double x, double y, double z,
                                                const double* exps, const double* norms, const double* contr,
-                                               bool valid, uint64_t mask, int64_t base, int nsel, int64_t p,
+                                               const int2* rng, bool valid, uint64_t mask, int64_t base, int nsel,
+                                               int64_t p,
                                                int64_t ld, double* __restrict__ phi, double* __restrict__ gx,
                                                double* __restrict__ gy, double* __restrict__ gz) {
   double Y[16];
@@ -134,6 +136,37 @@ __device__ __forceinline__ void shell_at_point(const DevShell& S, const DevSA& s
   const double* ex = exps + S.exp_off;
   const double* nr = norms + S.exp_off;
   const double* cc = contr + S.con_off;
+  if (S.seg) {
+    // segmented contractions: each selected radial function sums only its own primitives
+    uint64_t rem = mask;
+    for (int k = 0; k < nsel; ++k) {
+      const int rr = __ffsll((long long)rem) - 1;
+      rem &= rem - 1;
+      const int2 rg = rng[rr];
+      double Rr = 0.0, dR = 0.0;
+      if (valid) {
+        for (int e = rg.x; e < rg.y; ++e) {
+          const double alpha = ex[e];
+          const double v = prim_value(alpha, nr[e], r2);
+          const double cf = cc[e + (int64_t)S.nexp * rr];
+          Rr += cf * v;
+          dR += cf * ((-2.0 * alpha) * v);
+        }
+      }
+#pragma unroll
+      for (int i = 0; i < 2 * L + 1; ++i) {
+        const int64_t f = base + (int64_t)i * nsel + k;
+        phi[f * ld + p] = Ys[i] * Rr;
+        if (GRAD) {
+          const double h = Ys[i] * dR;
+          gx[f * ld + p] = x * h + dYs[0][i] * Rr;
+          gy[f * ld + p] = y * h + dYs[1][i] * Rr;
+          gz[f * ld + p] = z * h + dYs[2][i] * Rr;
+        }
+      }
+    }
+    return;
+  }
   uint64_t rem = mask;
   for (int k0 = 0; k0 < nsel; k0 += kRadGroup) {
     int rr[kRadGroup];
@@ -191,9 +224,12 @@ constexpr int kStagePrim = 64;
 constexpr int kStageCon = 512;
 struct ShellStage {
   double e[kStagePrim], n[kStagePrim], c[kStageCon];
+  int2 r[64];
 };
+// Stages the shell (when it fits) and its contraction ranges; returns the
+// range pointer to use (shared memory).
 __device__ __forceinline__ bool stage_shell(ShellStage& st, DevShell& S, const double* exps, const double* norms,
-                                            const double* contr) {
+                                            const double* contr, const int2* rng) {
   const bool staged = S.nexp <= kStagePrim && S.nexp * S.ncontr <= kStageCon;
   if (staged) {
     const double *e_src = exps + S.exp_off, *n_src = norms + S.exp_off, *c_src = contr + S.con_off;
@@ -205,6 +241,8 @@ __device__ __forceinline__ bool stage_shell(ShellStage& st, DevShell& S, const d
     S.exp_off = 0;
     S.con_off = 0;
   }
+  if (S.seg)
+    for (int i = threadIdx.x; i < S.nrad; i += blockDim.x) st.r[i] = rng[S.rad_off + i];
   __syncthreads();
   return staged;
 }
@@ -219,13 +257,14 @@ template <int L, bool GRAD>
 __global__ void __launch_bounds__(128) k_basis_l(const DevShell* __restrict__ shells, const int* __restrict__ ids,
                                                  const double* __restrict__ atoms, const double* __restrict__ exps,
                                                  const double* __restrict__ norms, const double* __restrict__ contr,
-                                                 DevSA sa, const double* __restrict__ px, const double* __restrict__ py,
+                                                 const int2* __restrict__ rng, DevSA sa, const double* __restrict__ px,
+                                                 const double* __restrict__ py,
                                                  const double* __restrict__ pz, int64_t p0, int64_t nvalid, int64_t ld,
                                                  double* __restrict__ phi, double* __restrict__ gx,
                                                  double* __restrict__ gy, double* __restrict__ gz) {
   __shared__ ShellStage st;
   DevShell S = shells[ids[blockIdx.y]];
-  const bool staged = stage_shell(st, S, exps, norms, contr);
+  const bool staged = stage_shell(st, S, exps, norms, contr, rng);
   const int64_t p = (int64_t)blockIdx.x * 128 + threadIdx.x;
   if (p >= ld) return;
   const bool valid = p < nvalid;
@@ -235,8 +274,8 @@ __global__ void __launch_bounds__(128) k_basis_l(const DevShell* __restrict__ sh
     y = py[p0 + p] - atoms[3 * S.atom + 1];
     z = pz[p0 + p] - atoms[3 * S.atom + 2];
   }
-  shell_at_point<L, GRAD>(S, sa, x, y, z, staged ? st.e : exps, staged ? st.n : norms, staged ? st.c : contr, valid,
-                          all_radial(S.nrad), S.f0, S.nrad, p, ld, phi, gx, gy, gz);
+  shell_at_point<L, GRAD>(S, sa, x, y, z, staged ? st.e : exps, staged ? st.n : norms, staged ? st.c : contr, st.r,
+                          valid, all_radial(S.nrad), S.f0, S.nrad, p, ld, phi, gx, gy, gz);
 }
 
 // ---------------------------------------------------------------------------
@@ -258,7 +297,8 @@ __global__ void __launch_bounds__(128) k_basis_items(const BasisItem* __restrict
                                                      const DevShell* __restrict__ shells,
                                                      const double* __restrict__ atoms, const double* __restrict__ exps,
                                                      const double* __restrict__ norms,
-                                                     const double* __restrict__ contr, DevSA sa,
+                                                     const double* __restrict__ contr,
+                                                     const int2* __restrict__ rng, DevSA sa,
                                                      const double* __restrict__ qx, const double* __restrict__ qy,
                                                      const double* __restrict__ qz, int64_t s0,
                                                      double* __restrict__ phi, double* __restrict__ gx,
@@ -266,13 +306,13 @@ __global__ void __launch_bounds__(128) k_basis_items(const BasisItem* __restrict
   __shared__ ShellStage st;
   const BasisItem it = items[blockIdx.x];
   DevShell S = shells[it.shell];
-  const bool staged = stage_shell(st, S, exps, norms, contr);
+  const bool staged = stage_shell(st, S, exps, norms, contr, rng);
   const int64_t q = (int64_t)it.tile * 128 + threadIdx.x;
   const double x = qx[q] - atoms[3 * S.atom];
   const double y = qy[q] - atoms[3 * S.atom + 1];
   const double z = qz[q] - atoms[3 * S.atom + 2];
-  shell_at_point<L, GRAD>(S, sa, x, y, z, staged ? st.e : exps, staged ? st.n : norms, staged ? st.c : contr, true,
-                          it.mask, it.slot - s0, it.nsig, threadIdx.x, 128, phi, gx, gy, gz);
+  shell_at_point<L, GRAD>(S, sa, x, y, z, staged ? st.e : exps, staged ? st.n : norms, staged ? st.c : contr, st.r,
+                          true, it.mask, it.slot - s0, it.nsig, threadIdx.x, 128, phi, gx, gy, gz);
 }
 
 }  // namespace pgxc

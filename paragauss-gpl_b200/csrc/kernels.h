@@ -21,6 +21,7 @@ struct BuildArgs {
   const double* exps = nullptr;
   const double* norms = nullptr;
   const double* contr = nullptr;
+  const int2* rng = nullptr;       // [lo, hi) primitive range of each contraction of segmented shells
   DevSA sa;
   XcConst xc;
   // grid (SoA, whole grid)

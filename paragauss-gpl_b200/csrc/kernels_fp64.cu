@@ -36,10 +36,10 @@ static void launch_basis_one_l(const BuildArgs& a, const double* px, const doubl
   if (a.nshl[L] == 0) return;
   dim3 grid((unsigned)((ld + 127) / 128), (unsigned)a.nshl[L]);
   if (gx)
-    k_basis_l<L, true><<<grid, 128, 0, st>>>(a.shells, a.shl[L], a.atoms, a.exps, a.norms, a.contr, a.sa, px,
+    k_basis_l<L, true><<<grid, 128, 0, st>>>(a.shells, a.shl[L], a.atoms, a.exps, a.norms, a.contr, a.rng, a.sa, px,
                                                      py, pz, p0, nvalid, ld, phi, gx, gy, gz);
   else
-    k_basis_l<L, false><<<grid, 128, 0, st>>>(a.shells, a.shl[L], a.atoms, a.exps, a.norms, a.contr, a.sa,
+    k_basis_l<L, false><<<grid, 128, 0, st>>>(a.shells, a.shl[L], a.atoms, a.exps, a.norms, a.contr, a.rng, a.sa,
                                                       px, py, pz, p0, nvalid, ld, phi, nullptr, nullptr, nullptr);
 }
 

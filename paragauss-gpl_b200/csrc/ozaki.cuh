@@ -62,6 +62,32 @@ __device__ __forceinline__ void oz_digits(long long q, int8_t (&d)[kSlices]) {
 }
 __device__ __forceinline__ void digits(double v, int e, int8_t (&d)[kSlices]) { oz_digits(oz_int(v, e), d); }
 
+// q + kOzOff has the base-128 digits u_s = d_s + 64 (u_0 in [0, 128], the
+// others in [0, 127]): the balanced digits without carries
+constexpr long long kOzOff = 64LL * ((1LL << 28) + (1LL << 21) + (1LL << 14) + (1LL << 7) + 1);
+
+// the digits of four integers, one 32-bit word per slice (byte u = digit of q[u])
+__device__ __forceinline__ void oz_pack4(const long long (&q)[4], uint32_t (&w)[kSlices]) {
+  uint32_t u[4][kSlices];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const long long v = q[i] + kOzOff;
+    const uint32_t lo = (uint32_t)v;
+    u[i][0] = (uint32_t)(v >> 28);
+    u[i][1] = (lo >> 21) & 127u;
+    u[i][2] = (lo >> 14) & 127u;
+    u[i][3] = (lo >> 7) & 127u;
+    u[i][4] = lo & 127u;
+  }
+  // byte-wise u - 64 (mod 256) without carries between bytes: add 0xC0 to the
+  // low 7 bits and fix bit 7 by XOR (u_0 = 128 gives 64)
+#pragma unroll
+  for (int s = 0; s < kSlices; ++s) {
+    const uint32_t a = u[0][s] | (u[1][s] << 8) | (u[2][s] << 16) | (u[3][s] << 24);
+    w[s] = ((a & 0x7f7f7f7fu) + 0x40404040u) ^ ((a & 0x80808080u) ^ 0x80808080u);
+  }
+}
+
 // combine the kGroups INT32 accumulator values of one element (as loaded
 // from TMEM) exactly into x = sum_g D_g 2^(7(4-g))
 __device__ __forceinline__ double oz_combine(const uint32_t (&g)[kGroups]) {

@@ -289,6 +289,42 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
   if (ncon_tot) CUDA_TRY(c, cudaMemcpy(dcontr, bas->contractions, sizeof(double) * ncon_tot, cudaMemcpyHostToDevice));
   a.shells = dsh;
   {
+    // contraction ranges: a shell is segmented when it has no bare primitives
+    // and every contraction's nonzero coefficients form its own contiguous,
+    // disjoint range of primitives (each primitive then feeds one function)
+    std::vector<int2> rng;
+    for (DevShell& S : c->shells) {
+      S.seg = 0;
+      S.rad_off = (int)rng.size();
+      if (S.nunc != 0 || S.ncontr == 0) continue;
+      std::vector<int2> r((size_t)S.ncontr);
+      bool seg = true;
+      std::vector<int> owner((size_t)S.nexp, -1);
+      for (int j = 0; j < S.ncontr && seg; ++j) {
+        int lo = -1, hi = -1;
+        for (int e = 0; e < S.nexp; ++e)
+          if (bas->contractions[S.con_off + e + (int64_t)S.nexp * j] != 0.0) {
+            if (lo < 0) lo = e;
+            hi = e + 1;
+          }
+        if (lo < 0) lo = hi = 0;
+        for (int e = lo; e < hi && seg; ++e) {
+          if (owner[(size_t)e] >= 0) seg = false;
+          owner[(size_t)e] = j;
+        }
+        r[(size_t)j] = make_int2(lo, hi);
+      }
+      if (!seg) continue;
+      S.seg = 1;
+      rng.insert(rng.end(), r.begin(), r.end());
+    }
+    int2* drng = nullptr;
+    if ((st = dalloc(c, &drng, std::max<size_t>(rng.size(), 1)))) return fail(st);
+    if (!rng.empty()) CUDA_TRY(c, cudaMemcpy(drng, rng.data(), rng.size() * sizeof(int2), cudaMemcpyHostToDevice));
+    a.rng = drng;
+    CUDA_TRY(c, cudaMemcpy(dsh, c->shells.data(), c->shells.size() * sizeof(DevShell), cudaMemcpyHostToDevice));
+  }
+  {
     std::vector<int> ids[kMaxL + 1];
     for (int i = 0; i < (int)c->shells.size(); ++i) ids[c->shells[i].l].push_back(i);
     for (int l = 0; l <= kMaxL; ++l) {

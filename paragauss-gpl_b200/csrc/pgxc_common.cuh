@@ -25,6 +25,8 @@ struct DevShell {
   int exp_off;   // into exponents / norms
   int con_off;   // into contractions (nexp x ncontr column-major)
   int f0;        // first basis function
+  int seg;       // 1: every contraction uses its own contiguous range of primitives
+  int rad_off;   // into the radial-range table (seg shells): [lo, hi) per contraction
   int pad_;
   double min_exp;  // smallest exponent: bounds the shell's spatial extent
 };

@@ -297,7 +297,7 @@ __global__ void k_szbuild(int64_t nslots, const int* __restrict__ slot_tile, int
   }
 }
 
-// (I, J) of pair q of the tile's 64-blocks: all nb^2 (GGA) or I <= J (LDA)
+// (I, J) of pair q of the tile's nb 64-slot blocks: all nb^2 (GGA) or I <= J (LDA)
 __device__ __forceinline__ void pair_of(int q, int nb, bool all, int& I, int& J) {
   if (all) {
     I = q / nb;
@@ -313,7 +313,8 @@ __device__ __forceinline__ void pair_of(int q, int nb, bool all, int& I, int& J)
 }
 
 // K4 (screened): H[fn_i][fn_j] += sum_p Z[i][p] phi[j][p] for the slots i, j
-// of one tile; LDA keeps fn_i <= fn_j only (H is symmetric).
+// of one tile; LDA keeps fn_i <= fn_j only (H is symmetric), GGA the whole
+// square (V = H + H^T in k_spack).
 template <bool GGA>
 __global__ void __launch_bounds__(kGemmThreads) k_svpot(const double* __restrict__ phi, const double* __restrict__ Z,
                                                        const int64_t* __restrict__ tso, int64_t t0, int64_t s0,
@@ -348,7 +349,7 @@ __global__ void __launch_bounds__(kGemmThreads) k_svpot(const double* __restrict
         for (int e = 0; e < 2; ++e) {
           const int j = J * 64 + wn0 + jj * 8 + 2 * (lane & 3) + e;
           const int fj = j < n ? sfn[j] : -1;
-          if (fi >= 0 && fj >= 0 && (GGA || fi <= fj)) atomicAdd(V + (int64_t)fi * ldv + fj, acc.v[ii][jj][e]);
+          if (fi >= 0 && fj >= 0 && (GGA || fj >= fi)) atomicAdd(V + (int64_t)fi * ldv + fj, acc.v[ii][jj][e]);
         }
     }
   }
@@ -356,7 +357,7 @@ __global__ void __launch_bounds__(kGemmThreads) k_svpot(const double* __restrict
 
 }  // namespace
 
-// ham[spin + ispin*(j(j+1)/2 + k)] = V(k, j), k <= j; GGA: H(k, j) + H(j, k)
+// ham[spin + ispin*(j(j+1)/2 + k)] = H(k, j), k <= j; GGA: H(k, j) + H(j, k)
 __global__ void k_spack(const double* __restrict__ V, int64_t nbas, bool sym2, int ispin, int spin,
                         double* __restrict__ ham) {
   const int64_t len = nbas * (nbas + 1) / 2;
@@ -725,11 +726,11 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, cudaStream_t st, double* ham,
         if (i1 <= i0) return;
         if (gga)
           k_basis_items<L, true><<<(unsigned)(i1 - i0), 128, 0, st>>>(
-              sp->items[L] + i0, a.shells, a.atoms, a.exps, a.norms, a.contr, a.sa, sp->qx, sp->qy, sp->qz, s0,
+              sp->items[L] + i0, a.shells, a.atoms, a.exps, a.norms, a.contr, a.rng, a.sa, sp->qx, sp->qy, sp->qz, s0,
               sp->phi, sp->gx, sp->gy, sp->gz);
         else
           k_basis_items<L, false><<<(unsigned)(i1 - i0), 128, 0, st>>>(
-              sp->items[L] + i0, a.shells, a.atoms, a.exps, a.norms, a.contr, a.sa, sp->qx, sp->qy, sp->qz, s0,
+              sp->items[L] + i0, a.shells, a.atoms, a.exps, a.norms, a.contr, a.rng, a.sa, sp->qx, sp->qy, sp->qz, s0,
               sp->phi, nullptr, nullptr, nullptr);
         ++T.launches;
       };

@@ -41,8 +41,9 @@ constexpr int kBlkB = kN * 32;             // one slice of a 48-row x 32-byte K 
 constexpr int kOpA = kSlices * kBlkA;      // 20480
 constexpr int kOpB = kSlices * kBlkB;      // 7680
 constexpr int kAccCols = kGroups * kN;     // 240 TMEM columns per accumulator set
-constexpr int kDStages = 4;
-constexpr int kVStages = 4;
+constexpr int kDStages = 3;                // density: A (phi digit) ring
+constexpr int kBStages = 6;                // density: gathered B (P digit) ring
+constexpr int kVStages = 6;
 constexpr int kDigBytesPerSlot = 640;      // 128 points x 5 slices
 
 }  // namespace
@@ -61,6 +62,7 @@ struct ScreenMixed {
   int* e_Z = nullptr;                // [chunk_slots]
   int* e_F = nullptr;
   int* err = nullptr;
+  int nsm = 148;
   std::vector<void*> allocs;
 };
 
@@ -133,18 +135,18 @@ __global__ void __launch_bounds__(128) k_sm_quant_pts(const int64_t* __restrict_
   for (int kb = 0; kb < n / 32; ++kb) {
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      int8_t d[kSlices][16];
+      uint32_t w[4][kSlices];
 #pragma unroll
-      for (int k = 0; k < 16; ++k) {
-        int8_t q[kSlices];
-        digits(src[(int64_t)(kb * 32 + h * 16 + k) * 128], e, q);
+      for (int g = 0; g < 4; ++g) {
+        long long q[4];
 #pragma unroll
-        for (int s = 0; s < kSlices; ++s) d[s][k] = q[s];
+        for (int u = 0; u < 4; ++u) q[u] = oz_int(src[(int64_t)(kb * 32 + h * 16 + g * 4 + u) * 128], e);
+        oz_pack4(q, w[g]);
       }
 #pragma unroll
       for (int s = 0; s < kSlices; ++s)
         *reinterpret_cast<uint4*>(dst + (int64_t)kb * kOpA + s * kBlkA + blk_off(p, h * 16)) =
-            *reinterpret_cast<const uint4*>(d[s]);
+            make_uint4(w[0][s], w[1][s], w[2][s], w[3][s]);
     }
   }
 }
@@ -163,17 +165,26 @@ __device__ __forceinline__ unsigned long long gather_slice(const unsigned long l
 // ---------------------------------------------------------------------------
 // X = phi_t P[S_t, S_t] with fused rho / grad rho
 // ---------------------------------------------------------------------------
+// epilogue operands: phi (and grad phi) of 6 slots x 128 points per buffer
+constexpr int kECols = 6;
+constexpr int kERing = 4;
+constexpr int kEBuf = 4 * kECols * 128;  // doubles
 struct DensSmem {
   alignas(1024) int8_t a[kDStages][kOpA];
-  alignas(1024) int8_t b[kDStages][kOpB];
-  double red[4][128];
+  alignas(1024) int8_t b[kBStages][kOpB];
+  alignas(128) double e[kERing][kEBuf];   // [array][column][point]
   uint64_t full[kDStages];
   uint64_t empty[kDStages];
+  uint64_t b_full[kBStages];
+  uint64_t b_empty[kBStages];
   uint64_t acc_full[2];
   uint64_t acc_empty[2];
+  uint64_t e_full[kERing];
+  uint64_t e_empty[kERing];
   uint32_t tslot;
 };
-constexpr int kDensThreads = 448;  // warps 0-7 epilogue, 8 MMA, 9 A copies, 10-13 B gather
+// warps 0-7 epilogue, 8 MMA, 9 A copies, 10-13 B gather, 14 epilogue-operand copies
+constexpr int kDensThreads = 480;
 
 // TMEM -> 16 + 8 combined FP64 values of one accumulator set (columns c0..c0+23)
 __device__ __forceinline__ void read_acc24(uint32_t taddr, double (&x)[24]) {
@@ -205,32 +216,38 @@ __device__ __forceinline__ void read_acc24(uint32_t taddr, double (&x)[24]) {
   }
 }
 
+// Persistent: CTA c takes the chunk's tiles c, c + G, c + 2G, ... (G = grid
+// size); the copy / MMA / epilogue pipeline runs on across tile boundaries.
+// rho and grad rho are accumulated with atomics (the two column halves of a
+// point and nothing else), so they must be zero on entry.
 template <bool GGA>
 __global__ void __launch_bounds__(kDensThreads, 1)
-    k_sm_density(const int64_t* __restrict__ tso, const int* __restrict__ slot_fn, int64_t t0, int64_t s0,
-                 const int8_t* __restrict__ tA, const int* __restrict__ e_pt,
+    k_sm_density(const int64_t* __restrict__ tso, const int* __restrict__ slot_fn, int64_t t0, int64_t nt,
+                 int64_t s0, const int8_t* __restrict__ tA, const int* __restrict__ e_pt,
                  const unsigned long long* __restrict__ P8, const int* __restrict__ e_P, int64_t nbas,
                  const double* __restrict__ phi, const double* __restrict__ gx, const double* __restrict__ gy,
                  const double* __restrict__ gz, double* __restrict__ rho, double* __restrict__ grx,
                  double* __restrict__ gry, double* __restrict__ grz, int* err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   DensSmem& S = *reinterpret_cast<DensSmem*>(smem_raw);
-  int* sfn = reinterpret_cast<int*>(smem_raw + sizeof(DensSmem));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int64_t t = t0 + blockIdx.x;
-  const int64_t sb = tso[t] - s0;
-  const int n = (int)(tso[t + 1] - tso[t]);
-  const int nK = n / 32, nN = (n + kN - 1) / kN, total = nK * nN;
-  for (int i = tid; i < n; i += blockDim.x) sfn[i] = slot_fn[tso[t] + i];
   if (warp == 0) tc::tmem_alloc(&S.tslot, 512);
   if (tid == 0) {
     for (int s = 0; s < kDStages; ++s) {
-      tc::mbar_init(&S.full[s], 1 + 128);
+      tc::mbar_init(&S.full[s], 1);
       tc::mbar_init(&S.empty[s], 1);
+    }
+    for (int s = 0; s < kBStages; ++s) {
+      tc::mbar_init(&S.b_full[s], 128);
+      tc::mbar_init(&S.b_empty[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
       tc::mbar_init(&S.acc_full[b], 1);
       tc::mbar_init(&S.acc_empty[b], 256);
+    }
+    for (int r = 0; r < kERing; ++r) {
+      tc::mbar_init(&S.e_full[r], 1);
+      tc::mbar_init(&S.e_empty[r], 128);
     }
     tc::mbar_fence_init();
   }
@@ -239,138 +256,211 @@ __global__ void __launch_bounds__(kDensThreads, 1)
   tc::fence_after_sync();
   const uint32_t tbase = S.tslot;
   bool ok = true;
-  double r_acc = 0.0, g_acc[3] = {0.0, 0.0, 0.0};
-  if (warp == 8) {
+  if (warp == 14) {
+    if (lane == 0) {  // epilogue operands: per slot block j, half h, group u: 6 slots of phi (grad phi)
+      int e = 0;
+      for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
+        const int64_t sb = tso[t0 + ti] - s0;
+        const int n = (int)(tso[t0 + ti + 1] - tso[t0 + ti]);
+        const int nN = (n + kN - 1) / kN;
+        for (int j = 0; j < nN && ok; ++j) {
+          if (j + 1 < nN) {  // next block into L2
+            const int rows = min(kN, n - (j + 1) * kN);
+            const int64_t off = (sb + (int64_t)(j + 1) * kN) * 128;
+            const uint32_t bytes = (uint32_t)rows * 128 * sizeof(double);
+            tc::bulk_prefetch_l2(phi + off, bytes);
+            if (GGA) {
+              tc::bulk_prefetch_l2(gx + off, bytes);
+              tc::bulk_prefetch_l2(gy + off, bytes);
+              tc::bulk_prefetch_l2(gz + off, bytes);
+            }
+          }
+          for (int u = 0; u < 4 && ok; ++u)
+            for (int h = 0; h < 2; ++h, ++e) {
+              const int r = e % kERing;
+              if (e >= kERing && !tc::mbar_wait(&S.e_empty[r], ((e / kERing) - 1) & 1)) {
+                ok = false;
+                break;
+              }
+              const int c0 = j * kN + h * 24 + u * kECols;
+              const int nc = max(0, min(kECols, n - c0));
+              if (nc == 0) {
+                tc::mbar_arrive(&S.e_full[r]);
+                continue;
+              }
+              const uint32_t bytes = (uint32_t)nc * 128 * sizeof(double);
+              const int64_t off = (sb + c0) * 128;
+              tc::mbar_expect_tx(&S.e_full[r], (GGA ? 4 : 1) * bytes);
+              tc::bulk_g2s(S.e[r], phi + off, bytes, &S.e_full[r]);
+              if (GGA) {
+                tc::bulk_g2s(S.e[r] + kECols * 128, gx + off, bytes, &S.e_full[r]);
+                tc::bulk_g2s(S.e[r] + 2 * kECols * 128, gy + off, bytes, &S.e_full[r]);
+                tc::bulk_g2s(S.e[r] + 3 * kECols * 128, gz + off, bytes, &S.e_full[r]);
+              }
+            }
+        }
+      }
+      if (!ok) atomicExch(err, 1);
+    }
+  } else if (warp == 8) {
     if (lane == 0) {  // MMA issuer
       const uint32_t idesc = tc::idesc_s8(kM, kN);
-      int it = 0;
-      for (int j = 0; j < nN && ok; ++j) {
-        const int b = j & 1;
-        if (j >= 2 && !tc::mbar_wait(&S.acc_empty[b], ((j >> 1) - 1) & 1)) ok = false;
-        tc::fence_after_sync();
-        for (int k = 0; k < nK && ok; ++k, ++it) {
-          const int s = it % kDStages;
-          if (!tc::mbar_wait(&S.full[s], (it / kDStages) & 1)) {
+      int it = 0, jj = 0;
+      for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
+        const int n = (int)(tso[t0 + ti + 1] - tso[t0 + ti]);
+        const int nK = n / 32, nN = (n + kN - 1) / kN;
+        for (int j = 0; j < nN && ok; ++j, ++jj) {
+          const int b = jj & 1;
+          if (jj >= 2 && !tc::mbar_wait(&S.acc_empty[b], ((jj >> 1) - 1) & 1)) {
             ok = false;
             break;
           }
           tc::fence_after_sync();
-          oz_mma_pairs(tbase + b * kAccCols, kN, tc::smem_u32(S.a[s]), kBlkA, tc::smem_u32(S.b[s]), kBlkB, idesc,
-                       k == 0);
-          tc::mma_commit(&S.empty[s]);
+          for (int k = 0; k < nK; ++k, ++it) {
+            const int s = it % kDStages, sbb = it % kBStages;
+            if (!tc::mbar_wait(&S.full[s], (it / kDStages) & 1) ||
+                !tc::mbar_wait(&S.b_full[sbb], (it / kBStages) & 1)) {
+              ok = false;
+              break;
+            }
+            tc::fence_after_sync();
+            oz_mma_pairs(tbase + b * kAccCols, kN, tc::smem_u32(S.a[s]), kBlkA, tc::smem_u32(S.b[sbb]), kBlkB, idesc,
+                         k == 0);
+            tc::mma_commit(&S.empty[s]);
+            tc::mma_commit(&S.b_empty[sbb]);
+          }
+          tc::mma_commit(&S.acc_full[b]);
         }
-        tc::mma_commit(&S.acc_full[b]);  // also after a failed wait: releases the epilogue
-      }
-      if (!ok) {
-        atomicExch(err, 1);
-        for (int j = 0; j < nN; ++j) tc::mma_commit(&S.acc_full[j & 1]);
-      }
-    }
-  } else if (warp == 9) {
-    if (lane == 0) {  // A producer: the tile's digits of phi, one 32-slot K block per stage
-      const int8_t* src = tA + sb * kDigBytesPerSlot;
-      for (int it = 0; it < total && ok; ++it) {
-        const int s = it % kDStages, k = it % nK;
-        if (it >= kDStages && !tc::mbar_wait(&S.empty[s], ((it / kDStages) - 1) & 1)) ok = false;
-        if (!ok) break;
-        tc::mbar_expect_tx(&S.full[s], kOpA);
-        tc::bulk_g2s(S.a[s], src + (int64_t)k * kOpA, kOpA, &S.full[s]);
       }
       if (!ok) atomicExch(err, 1);
     }
-  } else if (warp >= 10) {  // B producers: P8[fn(nu)][fn(mu)] gathered into the K-major digit block
+  } else if (warp == 9) {
+    if (lane == 0) {  // A producer: digits of phi, one 32-slot K block per stage
+      int it = 0;
+      for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
+        const int64_t sb = tso[t0 + ti] - s0;
+        const int n = (int)(tso[t0 + ti + 1] - tso[t0 + ti]);
+        const int nK = n / 32, nN = (n + kN - 1) / kN;
+        const int8_t* src = tA + sb * kDigBytesPerSlot;
+        for (int j = 0; j < nN && ok; ++j)
+          for (int k = 0; k < nK; ++k, ++it) {
+            const int s = it % kDStages;
+            if (it >= kDStages && !tc::mbar_wait(&S.empty[s], ((it / kDStages) - 1) & 1)) {
+              ok = false;
+              break;
+            }
+            tc::mbar_expect_tx(&S.full[s], kOpA);
+            tc::bulk_g2s(S.a[s], src + (int64_t)k * kOpA, kOpA, &S.full[s]);
+          }
+      }
+      if (!ok) atomicExch(err, 1);
+    }
+  } else if (warp >= 10 && warp < 14) {  // B producers: P8[fn(nu)][fn(mu)] gathered into the K-major digit block
+    // thread g: tasks g and g + 128 (rows r = task / 4, 8 K values from 8 (task % 4));
+    // warps 10-11 have two tasks, 12-13 one (uniform per warp)
     const int g = tid - 320;
-    for (int it = 0; it < total && ok; ++it) {
-      const int s = it % kDStages, j = it / nK, k = it % nK;
-      if (it >= kDStages && !tc::mbar_wait(&S.empty[s], ((it / kDStages) - 1) & 1)) {
-        ok = false;
-        break;
-      }
-      for (int task = g; task < kN * 4; task += 128) {
-        const int r = task >> 2, grp = task & 3;
-        const int nu = j * kN + r;
-        const int fnv = nu < n ? sfn[nu] : -1;
-        unsigned long long w[8];
+    const bool two = g < kN * 4 - 128;
+    int it = 0;
+    for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
+      const int64_t sg = tso[t0 + ti];
+      const int n = (int)(tso[t0 + ti + 1] - sg);
+      const int nK = n / 32, nN = (n + kN - 1) / kN;
+      const int* sfn = slot_fn + sg;
+      for (int j = 0; j < nN && ok; ++j) {
+        const int nu0 = j * kN + (g >> 2), nu1 = j * kN + ((g + 128) >> 2);
+        const int fnv0 = nu0 < n ? __ldg(sfn + nu0) : -1;
+        const int fnv1 = (two && nu1 < n) ? __ldg(sfn + nu1) : -1;
+        const int grp0 = g & 3, grp1 = (g + 128) & 3;
+        for (int k = 0; k < nK; ++k, ++it) {
+          const int sbb = it % kBStages;
+          const int fmu_lane = __ldg(sfn + k * 32 + lane);
+          if (it >= kBStages && !tc::mbar_wait(&S.b_empty[sbb], ((it / kBStages) - 1) & 1)) {
+            ok = false;
+            break;
+          }
+          unsigned long long w0[8], w1[8];
 #pragma unroll
-        for (int u = 0; u < 8; ++u) {
-          const int fmu = sfn[k * 32 + grp * 8 + u];
-          w[u] = (fnv >= 0 && fmu >= 0) ? __ldg(P8 + (int64_t)fnv * nbas + fmu) : 0ull;
+          for (int u = 0; u < 8; ++u) {
+            const int f0 = __shfl_sync(0xffffffffu, fmu_lane, grp0 * 8 + u);
+            const int f1 = __shfl_sync(0xffffffffu, fmu_lane, grp1 * 8 + u);
+            w0[u] = (fnv0 >= 0 && f0 >= 0) ? __ldg(P8 + (int64_t)fnv0 * nbas + f0) : 0ull;
+            w1[u] = (fnv1 >= 0 && f1 >= 0) ? __ldg(P8 + (int64_t)fnv1 * nbas + f1) : 0ull;
+          }
+#pragma unroll
+          for (int sl = 0; sl < kSlices; ++sl) {
+            *reinterpret_cast<unsigned long long*>(S.b[sbb] + sl * kBlkB + blk_off(g >> 2, grp0 * 8)) =
+                gather_slice(w0, sl);
+            if (two)
+              *reinterpret_cast<unsigned long long*>(S.b[sbb] + sl * kBlkB + blk_off((g + 128) >> 2, grp1 * 8)) =
+                  gather_slice(w1, sl);
+          }
+          tc::fence_proxy_async();
+          tc::mbar_arrive(&S.b_full[sbb]);
         }
-#pragma unroll
-        for (int sl = 0; sl < kSlices; ++sl)
-          *reinterpret_cast<unsigned long long*>(S.b[s] + sl * kBlkB + blk_off(r, grp * 8)) = gather_slice(w, sl);
       }
-      tc::fence_proxy_async();
-      tc::mbar_arrive(&S.full[s]);
     }
     if (!ok) atomicExch(err, 1);
   } else {  // epilogue: point row = 32 (warp & 3) + lane, columns 24 (warp >> 2) .. +24 of each slot block
     const int row = (warp & 3) * 32 + lane, half = warp >> 2;
     const uint32_t trow = tbase + ((uint32_t)((warp & 3) * 32) << 16) + half * 24;
-    const double rs = pow2(e_pt[(int64_t)blockIdx.x * 128 + row] + kCombShift);
-    for (int j = 0; j < nN; ++j) {
-      const int b = j & 1;
-      if (!tc::mbar_wait(&S.acc_full[b], (j >> 1) & 1)) {
-        ok = false;
-        break;
+    int jj = 0;
+    for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
+      const int64_t sg = tso[t0 + ti];
+      const int n = (int)(tso[t0 + ti + 1] - sg);
+      const int nN = (n + kN - 1) / kN;
+      const int* sfn = slot_fn + sg;
+      const double rs = pow2(e_pt[ti * 128 + row] + kCombShift);
+      double r_acc = 0.0, g_acc[3] = {0.0, 0.0, 0.0};
+      for (int j = 0; j < nN && ok; ++j, ++jj) {
+        const int b = jj & 1;
+        if (!tc::mbar_wait(&S.acc_full[b], (jj >> 1) & 1)) {
+          ok = false;
+          break;
+        }
+        tc::fence_after_sync();
+        double x[24];
+        read_acc24(trow + b * kAccCols, x);
+        tc::fence_before_sync();
+        tc::mbar_arrive(&S.acc_empty[b]);
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int e = (jj * 4 + u) * 2 + half, r = e % kERing;
+          if (!tc::mbar_wait(&S.e_full[r], (e / kERing) & 1)) {
+            ok = false;
+            break;
+          }
+          const int c0 = j * kN + half * 24 + u * kECols;
+          const double* eb = S.e[r];
+#pragma unroll
+          for (int v = 0; v < kECols; ++v) {
+            const int c = c0 + v;
+            if (c < n) {
+              const int f = __ldg(sfn + c);
+              const double X = f >= 0 ? x[u * kECols + v] * (rs * pow2(__ldg(e_P + f))) : 0.0;
+              r_acc += X * eb[v * 128 + row];
+              if (GGA) {
+                g_acc[0] += X * eb[(kECols + v) * 128 + row];
+                g_acc[1] += X * eb[(2 * kECols + v) * 128 + row];
+                g_acc[2] += X * eb[(3 * kECols + v) * 128 + row];
+              }
+            }
+          }
+          tc::mbar_arrive(&S.e_empty[r]);
+        }
       }
-      tc::fence_after_sync();
-      double x[24];
-      read_acc24(trow + b * kAccCols, x);
-      tc::fence_before_sync();
-      tc::mbar_arrive(&S.acc_empty[b]);
-      const int c0 = j * kN + half * 24;
-#pragma unroll
-      for (int cc = 0; cc < 24; cc += 4) {
-        if (c0 + cc >= n) break;
-        double v[4], w0[4], w1[4], w2[4], sc[4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int c = c0 + cc + u;  // n is a multiple of 32, so c < n for the whole group of 4
-          const int64_t o = (sb + c) * 128 + row;
-          const int f = sfn[c];
-          sc[u] = f >= 0 ? pow2(__ldg(e_P + f)) : 0.0;
-          v[u] = __ldg(phi + o);
-          if (GGA) {
-            w0[u] = __ldg(gx + o);
-            w1[u] = __ldg(gy + o);
-            w2[u] = __ldg(gz + o);
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const double X = x[cc + u] * (rs * sc[u]);
-          r_acc += X * v[u];
-          if (GGA) {
-            g_acc[0] += X * w0[u];
-            g_acc[1] += X * w1[u];
-            g_acc[2] += X * w2[u];
-          }
-        }
+      if (!ok) break;
+      const int64_t p = ti * 128 + row;
+      atomicAdd(rho + p, r_acc);
+      if (GGA) {
+        atomicAdd(grx + p, 2.0 * g_acc[0]);
+        atomicAdd(gry + p, 2.0 * g_acc[1]);
+        atomicAdd(grz + p, 2.0 * g_acc[2]);
       }
     }
     if (!ok) atomicExch(err, 1);
   }
-  // combine the two column halves of each point
-  if (warp >= 4 && warp < 8) {
-    const int row = (warp & 3) * 32 + lane;
-    S.red[0][row] = r_acc;
-    S.red[1][row] = g_acc[0];
-    S.red[2][row] = g_acc[1];
-    S.red[3][row] = g_acc[2];
-  }
   tc::fence_before_sync();
   __syncthreads();
-  if (warp < 4) {
-    const int row = warp * 32 + lane;
-    const int64_t p = (int64_t)blockIdx.x * 128 + row;
-    rho[p] = r_acc + S.red[0][row];
-    if (GGA) {
-      grx[p] = 2.0 * (g_acc[0] + S.red[1][row]);
-      gry[p] = 2.0 * (g_acc[1] + S.red[2][row]);
-      grz[p] = 2.0 * (g_acc[2] + S.red[3][row]);
-    }
-  }
   if (warp == 0) tc::tmem_dealloc(tbase, 512);
 }
 
@@ -384,7 +474,7 @@ __device__ __forceinline__ double warp_max(double v) {
 }
 
 template <bool GGA>
-__global__ void __launch_bounds__(256) k_sm_zquant(const int64_t* __restrict__ tso, int64_t t0, int64_t s0,
+__global__ void __launch_bounds__(256, 2) k_sm_zquant(const int64_t* __restrict__ tso, int64_t t0, int64_t s0,
                                                    const double* __restrict__ phi, const double* __restrict__ gx,
                                                    const double* __restrict__ gy, const double* __restrict__ gz,
                                                    const double* __restrict__ A, const double* __restrict__ Bx,
@@ -420,11 +510,11 @@ __global__ void __launch_bounds__(256) k_sm_zquant(const int64_t* __restrict__ t
 #pragma unroll
     for (int u = 0; u < 4; ++u) z[u] = sA[p0 + u] * f[u];
     if (GGA) {
-      const double* gs[3] = {gx, gy, gz};
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
-        const double2 a = *reinterpret_cast<const double2*>(gs[c] + o);
-        const double2 b = *reinterpret_cast<const double2*>(gs[c] + o + 2);
+        const double* g = c == 0 ? gx : (c == 1 ? gy : gz);
+        const double2 a = *reinterpret_cast<const double2*>(g + o);
+        const double2 b = *reinterpret_cast<const double2*>(g + o + 2);
         z[0] += sB[c][p0] * a.x;
         z[1] += sB[c][p0 + 1] * a.y;
         z[2] += sB[c][p0 + 2] * b.x;
@@ -438,67 +528,57 @@ __global__ void __launch_bounds__(256) k_sm_zquant(const int64_t* __restrict__ t
       e_Z[sb + i] = ez;
       e_F[sb + i] = ef;
     }
-    int8_t dz[4][kSlices], df[4][kSlices];
+    long long qz[4], qf[4];
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
-      digits(z[u], ez, dz[u]);
-      digits(f[u], ef, df[u]);
+      qz[u] = oz_int(z[u], ez);
+      qf[u] = oz_int(f[u], ef);
     }
+    uint32_t wz[kSlices], wf[kSlices];
+    oz_pack4(qz, wz);
+    oz_pack4(qf, wf);
 #pragma unroll
     for (int sl = 0; sl < kSlices; ++sl) {
       const int64_t off = tile_off + (int64_t)(kstep * kSlices + sl) * n * 32 + blk_off(i, kin);
-      uint32_t wz = 0, wf = 0;
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        wz |= (uint32_t)(uint8_t)dz[u][sl] << (8 * u);
-        wf |= (uint32_t)(uint8_t)df[u][sl] << (8 * u);
-      }
-      *reinterpret_cast<uint32_t*>(tZ + off) = wz;
-      *reinterpret_cast<uint32_t*>(tF + off) = wf;
+      *reinterpret_cast<uint32_t*>(tZ + off) = wz[sl];
+      *reinterpret_cast<uint32_t*>(tF + off) = wf[sl];
     }
   }
 }
 
 // ---------------------------------------------------------------------------
-// H[S_t, S_t] += Z_t^T phi_t, scatter-added into V
+// H[S_t, S_t] += Z_t^T phi_t, scatter-added into V (LDA: fn_i <= fn_j only,
+// H is symmetric; GGA: the whole square, V = H + H^T when packing).
+// Pairs of 128-slot row blocks I and 48-slot column blocks J, K = the tile's
+// 128 points in 4 steps.  Persistent like k_sm_density.
 // ---------------------------------------------------------------------------
 struct VSmem {
-  alignas(1024) int8_t a[4][kOpA];          // the Z digits of one 128-slot block, all 4 K steps
-  int8_t pad_[8192];                        // keeps one CTA per SM (each holds all 512 TMEM columns)
-  alignas(1024) int8_t b[kVStages][kOpB];   // phi digits of one 48-slot block, one K step
-  uint64_t a_full, a_empty;
-  uint64_t b_full[kVStages];
-  uint64_t b_empty[kVStages];
+  alignas(1024) int8_t a[kVStages][kOpA];
+  alignas(1024) int8_t b[kVStages][kOpB];
+  uint64_t full[kVStages];
+  uint64_t empty[kVStages];
   uint64_t acc_full[2];
   uint64_t acc_empty[2];
   uint32_t tslot;
 };
 constexpr int kVThreads = 320;  // warps 0-7 epilogue, 8 MMA, 9 producer
 
-// first 48-slot block with a column j >= 128 I (LDA keeps j >= i only)
+// first 48-slot block of pair row I: LDA needs columns j >= 128 I only
 __device__ __forceinline__ int first_J(int I, bool all) { return all ? 0 : (kM * I) / kN; }
 
 template <bool GGA>
 __global__ void __launch_bounds__(kVThreads, 1)
-    k_sm_vpot(const int64_t* __restrict__ tso, const int* __restrict__ slot_fn, int64_t t0, int64_t s0,
+    k_sm_vpot(const int64_t* __restrict__ tso, const int* __restrict__ slot_fn, int64_t t0, int64_t nt, int64_t s0,
               const int8_t* __restrict__ tZ, const int8_t* __restrict__ tF, const int* __restrict__ e_Z,
               const int* __restrict__ e_F, double* __restrict__ V, int64_t ldv, int* err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   VSmem& S = *reinterpret_cast<VSmem*>(smem_raw);
-  int* sfn = reinterpret_cast<int*>(smem_raw + sizeof(VSmem));
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int64_t t = t0 + blockIdx.x;
-  const int64_t sb = tso[t] - s0;
-  const int n = (int)(tso[t + 1] - tso[t]);
-  const int nI = (n + kM - 1) / kM, nJ = (n + kN - 1) / kN;
-  for (int i = tid; i < n; i += blockDim.x) sfn[i] = slot_fn[tso[t] + i];
   if (warp == 0) tc::tmem_alloc(&S.tslot, 512);
   if (tid == 0) {
-    tc::mbar_init(&S.a_full, 1);
-    tc::mbar_init(&S.a_empty, 1);
     for (int s = 0; s < kVStages; ++s) {
-      tc::mbar_init(&S.b_full[s], 1);
-      tc::mbar_init(&S.b_empty[s], 1);
+      tc::mbar_init(&S.full[s], 1);
+      tc::mbar_init(&S.empty[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
       tc::mbar_init(&S.acc_full[b], 1);
@@ -510,100 +590,101 @@ __global__ void __launch_bounds__(kVThreads, 1)
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tbase = S.tslot;
-  const int8_t* zsrc = tZ + sb * kDigBytesPerSlot;
-  const int8_t* fsrc = tF + sb * kDigBytesPerSlot;
-  const int64_t blk = (int64_t)n * 32;  // bytes of one (K step, slice) block of the tile
   bool ok = true;
   if (warp == 9) {
-    if (lane == 0) {  // producer
-      int pi = 0;
-      for (int I = 0; I < nI && ok; ++I) {
-        if (I > 0 && !tc::mbar_wait(&S.a_empty, (I - 1) & 1)) {
-          ok = false;
-          break;
-        }
-        tc::mbar_expect_tx(&S.a_full, 4 * kOpA);
-        for (int k = 0; k < 4; ++k)
-          for (int sl = 0; sl < kSlices; ++sl)
-            tc::bulk_g2s(S.a[k] + sl * kBlkA, zsrc + (k * kSlices + sl) * blk + (int64_t)I * kM * 32, kBlkA,
-                         &S.a_full);
-        for (int J = first_J(I, GGA); J < nJ && ok; ++J, ++pi) {
-          for (int k = 0; k < 4; ++k) {
-            const int ib = pi * 4 + k, s = ib % kVStages;
-            if (ib >= kVStages && !tc::mbar_wait(&S.b_empty[s], ((ib / kVStages) - 1) & 1)) {
-              ok = false;
-              break;
+    if (lane == 0) {  // producer: per pair and K step, Z rows of block I and phi rows of block J
+      int it = 0;
+      for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
+        const int64_t sb = tso[t0 + ti] - s0;
+        const int n = (int)(tso[t0 + ti + 1] - tso[t0 + ti]);
+        const int nI = (n + kM - 1) / kM, nJ = (n + kN - 1) / kN;
+        const int8_t* zsrc = tZ + sb * kDigBytesPerSlot;
+        const int8_t* fsrc = tF + sb * kDigBytesPerSlot;
+        const int64_t blk = (int64_t)n * 32;  // bytes of one (K step, slice) block of the tile
+        for (int I = 0; I < nI && ok; ++I)
+          for (int J = first_J(I, GGA); J < nJ && ok; ++J)
+            for (int k = 0; k < 4; ++k, ++it) {
+              const int s = it % kVStages;
+              if (it >= kVStages && !tc::mbar_wait(&S.empty[s], ((it / kVStages) - 1) & 1)) {
+                ok = false;
+                break;
+              }
+              tc::mbar_expect_tx(&S.full[s], kOpA + kOpB);
+              for (int sl = 0; sl < kSlices; ++sl) {
+                tc::bulk_g2s(S.a[s] + sl * kBlkA, zsrc + (k * kSlices + sl) * blk + (int64_t)I * kM * 32, kBlkA,
+                             &S.full[s]);
+                tc::bulk_g2s(S.b[s] + sl * kBlkB, fsrc + (k * kSlices + sl) * blk + (int64_t)J * kN * 32, kBlkB,
+                             &S.full[s]);
+              }
             }
-            tc::mbar_expect_tx(&S.b_full[s], kOpB);
-            for (int sl = 0; sl < kSlices; ++sl)
-              tc::bulk_g2s(S.b[s] + sl * kBlkB, fsrc + (k * kSlices + sl) * blk + (int64_t)J * kN * 32, kBlkB,
-                           &S.b_full[s]);
-          }
-        }
       }
       if (!ok) atomicExch(err, 1);
     }
   } else if (warp == 8) {
     if (lane == 0) {  // MMA issuer
       const uint32_t idesc = tc::idesc_s8(kM, kN);
-      int pi = 0;
-      for (int I = 0; I < nI && ok; ++I) {
-        if (!tc::mbar_wait(&S.a_full, I & 1)) {
-          ok = false;
-          break;
-        }
-        tc::fence_after_sync();
-        for (int J = first_J(I, GGA); J < nJ && ok; ++J, ++pi) {
-          const int b = pi & 1;
-          if (pi >= 2 && !tc::mbar_wait(&S.acc_empty[b], ((pi >> 1) - 1) & 1)) ok = false;
-          tc::fence_after_sync();
-          for (int k = 0; k < 4 && ok; ++k) {
-            const int ib = pi * 4 + k, s = ib % kVStages;
-            if (!tc::mbar_wait(&S.b_full[s], (ib / kVStages) & 1)) {
+      int it = 0, pp = 0;
+      for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
+        const int n = (int)(tso[t0 + ti + 1] - tso[t0 + ti]);
+        const int nI = (n + kM - 1) / kM, nJ = (n + kN - 1) / kN;
+        for (int I = 0; I < nI && ok; ++I)
+          for (int J = first_J(I, GGA); J < nJ && ok; ++J, ++pp) {
+            const int b = pp & 1;
+            if (pp >= 2 && !tc::mbar_wait(&S.acc_empty[b], ((pp >> 1) - 1) & 1)) {
               ok = false;
               break;
             }
             tc::fence_after_sync();
-            oz_mma_pairs(tbase + b * kAccCols, kN, tc::smem_u32(S.a[k]), kBlkA, tc::smem_u32(S.b[s]), kBlkB, idesc,
-                         k == 0);
-            tc::mma_commit(&S.b_empty[s]);
+            for (int k = 0; k < 4; ++k, ++it) {
+              const int s = it % kVStages;
+              if (!tc::mbar_wait(&S.full[s], (it / kVStages) & 1)) {
+                ok = false;
+                break;
+              }
+              tc::fence_after_sync();
+              oz_mma_pairs(tbase + b * kAccCols, kN, tc::smem_u32(S.a[s]), kBlkA, tc::smem_u32(S.b[s]), kBlkB,
+                           idesc, k == 0);
+              tc::mma_commit(&S.empty[s]);
+            }
+            tc::mma_commit(&S.acc_full[b]);
           }
-          tc::mma_commit(&S.acc_full[b]);
-        }
-        tc::mma_commit(&S.a_empty);
       }
-      if (!ok) {
-        atomicExch(err, 1);
-        for (int q = 0; q < 2; ++q) tc::mma_commit(&S.acc_full[q]);
-      }
+      if (!ok) atomicExch(err, 1);
     }
   } else {  // epilogue: slot row i = 128 I + 32 (warp & 3) + lane, columns 24 (warp >> 2) .. of each block
     const int half = warp >> 2;
     const uint32_t trow = tbase + ((uint32_t)((warp & 3) * 32) << 16) + half * 24;
-    int pi = 0;
-    for (int I = 0; I < nI && ok; ++I) {
-      const int i = I * kM + (warp & 3) * 32 + lane;
-      const int fi = i < n ? sfn[i] : -1;
-      const int ez = i < n ? e_Z[sb + i] : 0;
-      for (int J = first_J(I, GGA); J < nJ; ++J, ++pi) {
-        const int b = pi & 1;
-        if (!tc::mbar_wait(&S.acc_full[b], (pi >> 1) & 1)) {
-          ok = false;
-          break;
-        }
-        tc::fence_after_sync();
-        double x[24];
-        read_acc24(trow + b * kAccCols, x);
-        tc::fence_before_sync();
-        tc::mbar_arrive(&S.acc_empty[b]);
-        if (fi < 0) continue;
-        const int j0 = J * kN + half * 24;
+    int pp = 0;
+    for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
+      const int64_t sg = tso[t0 + ti];
+      const int64_t sb = sg - s0;
+      const int n = (int)(tso[t0 + ti + 1] - sg);
+      const int nI = (n + kM - 1) / kM, nJ = (n + kN - 1) / kN;
+      const int* sfn = slot_fn + sg;
+      for (int I = 0; I < nI && ok; ++I) {
+        const int i = I * kM + (warp & 3) * 32 + lane;
+        const int fi = i < n ? __ldg(sfn + i) : -1;
+        const int ezi = i < n ? __ldg(e_Z + sb + i) : 0;
+        for (int J = first_J(I, GGA); J < nJ; ++J, ++pp) {
+          const int b = pp & 1;
+          if (!tc::mbar_wait(&S.acc_full[b], (pp >> 1) & 1)) {
+            ok = false;
+            break;
+          }
+          tc::fence_after_sync();
+          double x[24];
+          read_acc24(trow + b * kAccCols, x);
+          tc::fence_before_sync();
+          tc::mbar_arrive(&S.acc_empty[b]);
+          if (fi < 0) continue;
+          const int j0 = J * kN + half * 24;
 #pragma unroll
-        for (int c = 0; c < 24; ++c) {
-          const int j = j0 + c;
-          const int fj = j < n ? sfn[j] : -1;
-          if (fj >= 0 && (GGA || fj >= fi))
-            atomicAdd(V + (int64_t)fi * ldv + fj, x[c] * pow2(ez + __ldg(e_F + sb + j) + kCombShift));
+          for (int c = 0; c < 24; ++c) {
+            const int j = j0 + c;
+            const int fj = j < n ? __ldg(sfn + j) : -1;
+            if (fj >= 0 && (GGA || fj >= fi))
+              atomicAdd(V + (int64_t)fi * ldv + fj, x[c] * pow2(ezi + __ldg(e_F + sb + j) + kCombShift));
+          }
         }
       }
     }
@@ -649,12 +730,14 @@ int screen_mixed_create(ScreenMixed** out, const ScreenMixedInput& in, std::stri
     screen_mixed_destroy(m);
     return e == cudaErrorMemoryAllocation ? PGXC_ENOMEM : PGXC_ECUDA;
   }
-  const int dsm = (int)sizeof(DensSmem) + 4 * in.max_n;
-  const int vsm = (int)sizeof(VSmem) + 4 * in.max_n;
+  const int dsm = (int)sizeof(DensSmem), vsm = (int)sizeof(VSmem);
   cudaFuncSetAttribute(k_sm_density<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm);
   cudaFuncSetAttribute(k_sm_density<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm);
   cudaFuncSetAttribute(k_sm_vpot<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, vsm);
   e = cudaFuncSetAttribute(k_sm_vpot<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, vsm);
+  int dev = 0;
+  if (e == cudaSuccess) e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&m->nsm, cudaDevAttrMultiProcessorCount, dev);
   if (e != cudaSuccess) {
     err = std::string("screened mixed-precision kernels: ") + cudaGetErrorString(e) +
           " (a tile lists too many functions for shared memory)";
@@ -687,15 +770,21 @@ int screen_mixed_basis(ScreenMixed* m, const int64_t* tso, int64_t t0, int64_t n
 int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
                          const double* phi, const double* gx, const double* gy, const double* gz, double* rho,
                          double* grx, double* gry, double* grz, cudaStream_t st) {
-  const int smem = (int)sizeof(DensSmem) + 4 * m->max_n;
+  cudaMemsetAsync(rho, 0, sizeof(double) * nt * 128, st);
+  if (m->gga) {
+    cudaMemsetAsync(grx, 0, sizeof(double) * nt * 128, st);
+    cudaMemsetAsync(gry, 0, sizeof(double) * nt * 128, st);
+    cudaMemsetAsync(grz, 0, sizeof(double) * nt * 128, st);
+  }
+  const unsigned grid = (unsigned)std::min<int64_t>(nt, m->nsm);
+  const int smem = (int)sizeof(DensSmem);
   if (m->gga)
-    k_sm_density<true><<<(unsigned)nt, kDensThreads, smem, st>>>(tso, slot_fn, t0, s0, m->tA, m->e_pt, m->P8,
-                                                                 m->e_P, m->nbas, phi, gx, gy, gz, rho, grx, gry,
-                                                                 grz, m->err);
+    k_sm_density<true><<<grid, kDensThreads, smem, st>>>(tso, slot_fn, t0, nt, s0, m->tA, m->e_pt, m->P8, m->e_P,
+                                                         m->nbas, phi, gx, gy, gz, rho, grx, gry, grz, m->err);
   else
-    k_sm_density<false><<<(unsigned)nt, kDensThreads, smem, st>>>(tso, slot_fn, t0, s0, m->tA, m->e_pt, m->P8,
-                                                                  m->e_P, m->nbas, phi, nullptr, nullptr, nullptr,
-                                                                  rho, nullptr, nullptr, nullptr, m->err);
+    k_sm_density<false><<<grid, kDensThreads, smem, st>>>(tso, slot_fn, t0, nt, s0, m->tA, m->e_pt, m->P8, m->e_P,
+                                                          m->nbas, phi, nullptr, nullptr, nullptr, rho, nullptr,
+                                                          nullptr, nullptr, m->err);
   return 1;
 }
 
@@ -712,13 +801,14 @@ int screen_mixed_potential(ScreenMixed* m, const int64_t* tso, const int* slot_f
     k_sm_zquant<false><<<(unsigned)nt, 256, 0, st>>>(tso, t0, s0, phi, nullptr, nullptr, nullptr, A, nullptr,
                                                      nullptr, nullptr, m->tZ, m->tF, m->e_Z, m->e_F);
   cudaEventRecord(k0, st);
-  const int smem = (int)sizeof(VSmem) + 4 * m->max_n;
+  const unsigned grid = (unsigned)std::min<int64_t>(nt, m->nsm);
+  const int smem = (int)sizeof(VSmem);
   if (m->gga)
-    k_sm_vpot<true><<<(unsigned)nt, kVThreads, smem, st>>>(tso, slot_fn, t0, s0, m->tZ, m->tF, m->e_Z, m->e_F, V,
-                                                           ldv, m->err);
+    k_sm_vpot<true><<<grid, kVThreads, smem, st>>>(tso, slot_fn, t0, nt, s0, m->tZ, m->tF, m->e_Z, m->e_F, V, ldv,
+                                                   m->err);
   else
-    k_sm_vpot<false><<<(unsigned)nt, kVThreads, smem, st>>>(tso, slot_fn, t0, s0, m->tZ, m->tF, m->e_Z, m->e_F, V,
-                                                            ldv, m->err);
+    k_sm_vpot<false><<<grid, kVThreads, smem, st>>>(tso, slot_fn, t0, nt, s0, m->tZ, m->tF, m->e_Z, m->e_F, V, ldv,
+                                                    m->err);
   cudaEventRecord(k1, st);
   return 2;
 }
