@@ -65,7 +65,7 @@ OZAKI_PAIRS = 15
 
 # ---------------------------------------------------------------------------
 def workload_desc(case):
-    return (f"{case.name}: {len(case.coords)} atoms, {case.nbas} spherical fns (l<=2), "
+    return (f"{case.name}: {len(case.coords)} atoms, {case.nbas} spherical fns (l<=3), "
             f"{case.npts} grid pts ({case.meta['nrad']} radial x {case.meta['nang']}-class angular per atom), "
             f"nocc={case.nocc}, {case.functional}")
 
@@ -219,6 +219,12 @@ def fp64_comparison(torch, case, sub, local, args):
     out = {"ham": dham.cpu().numpy(), "exc": float(dsum[0]), "nel": float(dsum[1]), "ms": ms,
            "value": case.npts / (ms * 1e-3)}
     ctx.close()
+    if args.screen >= 0:
+        ctx = lib.Context(sub, precision="fp64", weighted=False, device=local,
+                          max_chunk_points=args.max_chunk_points, screen_threshold=-1.0)
+        step()
+        out["dense_ms"] = cuda_timer(torch, step, 2) / 2
+        ctx.close()
     del dC, docc, dham, dsum
     torch.cuda.empty_cache()
     return out
@@ -367,45 +373,59 @@ def main():
     h2d = (nb * nocc + nocc) * 8
     d2h = (case.xc_length + 2) * 8
 
-    # roofline of the dominant contraction kernel (per-launch averages from the library's events)
-    fx, fv = algorithmic_flops(sub)
-    xs, vs = last_tm["xgemm_ms"], last_tm["vgemm_ms"]
-    if xs >= vs:
-        kname, kflops, kms = "density contraction X = phi P (+ fused rho, grad rho)", fx, xs
+    # roofline of the density kernel (the largest kernel of the build), per
+    # launch from the library's CUDA events around it
+    gga = case.functional == "PBE"
+    arrays = 4 if gga else 1
+    if screen is not None:
+        nlisted, sum_n2, ntl = screen["nlisted"], screen["sum_n2"], screen["ntiles"]
+        kflops = 2.0 * 128 * sum_n2                       # X = phi_sig P_sig, 2 B n_b^2 per tile
+        kbytes = 8.0 * arrays * 128 * (nlisted + ntl)     # phi (+ grad phi) of every listed pair, rho (+ grad rho)
     else:
-        kname, kflops, kms = "potential contraction V += phi^T Z", fv, vs
+        kflops = 2.0 * case.npts * case.nbas ** 2
+        kbytes = 8.0 * arrays * case.npts * (case.nbas + 1)
+    kms = last_tm["xgemm_ms"]
     roof = None
     if rank == 0:
-        achieved = kflops / (kms * 1e-3) / 1e12
-        extra = {}
+        mp = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        achieved = kbytes / (kms * 1e-3) / 1e9
+        tflops = kflops / (kms * 1e-3) / 1e12
         if prec == "fp64":
-            peak = fp64_peak_tflops(torch)
-            peak_src = "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor pipe); not in MEASURED_PEAKS.json"
+            tpeak = fp64_peak_tflops(torch)
+            tsrc = "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor pipe)"
+            tissued = tflops
         else:
-            mp = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-            peak = mp["bf16_tflops"] * INT8_PER_BF16
-            peak_src = ("INT8 dense tensor rate taken as 2 x MEASURED_PEAKS.json bf16_tflops (burst) of measured; "
-                        "achieved counts algorithmic (FP64-equivalent) flops, 2*npts*nbas^2")
-            extra = {"int8_tops_issued": achieved * OZAKI_PAIRS,
-                     "int8_frac": achieved * OZAKI_PAIRS / peak,
-                     "int8_note": f"{OZAKI_PAIRS} INT8 MMAs per FP64-equivalent product (Ozaki digit pairs)"}
+            tpeak = mp["bf16_tflops"] * INT8_PER_BF16
+            tsrc = "INT8 dense rate taken as 2 x MEASURED_PEAKS.json bf16_tflops (burst), of measured"
+            tissued = tflops * OZAKI_PAIRS
         traffic = None
         tf = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tf):
-            traffic = json.load(open(tf)).get(f"{prec}:{case.functional}")
-        roof = {"bound": "tensor", "kernel": kname, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_src,
-                "kernel_ms_per_build": kms, "flops_per_build": kflops,
-                "phase_ms": {k: last_tm[k] for k in ("basis_ms", "density_ms", "functional_ms", "potential_ms")},
-                **extra}
+            traffic = json.load(open(tf)).get(f"{prec}:{case.functional}:{args.screen:g}")
+        roof = {"bound": "hbm", "kernel": "density: X = phi_sig P_sig with fused rho, grad rho "
+                                          + ("(k_sm_density, tcgen05 kind::i8)" if prec != "fp64" else
+                                             "(k_sdensity, DMMA)" if screen is not None else "(k_density, DMMA)"),
+                "achieved": achieved, "peak": mp["hbm_gbs"], "unit": "GB/s", "frac": achieved / mp["hbm_gbs"],
+                "traffic": traffic, "peak_source": "MEASURED_PEAKS.json hbm_gbs, of measured",
+                "algorithmic_bytes": kbytes, "kernel_ms_per_build": kms,
+                "tensor": {"algorithmic_tflops": tflops, "issued_tflops_or_tops": tissued, "peak": tpeak,
+                           "frac_issued": tissued / tpeak, "peak_source": tsrc,
+                           "flops_per_build": kflops},
+                "phase_ms": {k: last_tm[k] for k in ("basis_ms", "density_ms", "functional_ms", "potential_ms",
+                                                     "xgemm_ms", "vgemm_ms")}}
 
     out = None
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": max(args.warmup, 3), "ms_per_step": per_step, "higher_is_better": True, "scaling": "strong",
-            "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "s8xs8->s32 (5-digit Ozaki) + f64", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "s8 x s8 -> s32 tensor (5-digit Ozaki split of f64) + f64", "data": "synthetic",
             "config": {"workload": workload_desc(case), "precision": prec,
+                       "screening": ("none (dense)" if screen is None else
+                                     f"per 128-point tile, threshold {args.screen:g}: "
+                                     f"{screen['nlisted'] / screen['ntiles']:.1f} listed functions per tile "
+                                     f"of {case.nbas}, {screen['sum_n2'] / (screen['ntiles'] * case.nbas ** 2):.3f} "
+                                     f"of the dense n^2 work"),
                        "parallelism": f"grid split over {world} GPU(s), NCCL all-reduce of packed V_xc",
                        "l2": "no flush: each build streams several GB of basis/Z data (inputs larger than L2)"},
             "xc_builds_per_s": 1e3 / per_step, "E_xc": exc, "N_el": nel,
@@ -414,7 +434,9 @@ def main():
                 "speedup": fp64_leg["ms"] / per_step,
                 "dE_xc": exc - fp64_leg["exc"], "dN_el": nel - fp64_leg["nel"],
                 "max_dV_xc": float(np.max(np.abs(dham.cpu().numpy() - fp64_leg["ham"]))),
-                "note": "FP64 GPU build on the same GPU in this run; it matches the FP64 oracle to 1e-10"},
+                "fp64_dense_ms_per_step": fp64_leg.get("dense_ms"),
+                "note": "FP64 GPU build, same screening, same GPU, this run (matches the FP64 oracle to 1e-10); "
+                        "fp64_dense: the unscreened FP64 build"},
             "roofline": roof,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": ms_e / args.steps},

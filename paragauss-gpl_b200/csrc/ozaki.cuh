@@ -100,15 +100,46 @@ __device__ __forceinline__ double oz_combine(const uint32_t (&g)[kGroups]) {
 // issue the 15 digit-pair MMAs of one K step: A and B blocks of kSlices
 // slices each (slice stride a_slice / b_slice bytes), accumulators at
 // d_tmem + g * d_group columns
+// (8-row groups of each slice a_sbo / b_sbo bytes apart)
 __device__ __forceinline__ void oz_mma_pairs(uint32_t d_tmem, uint32_t d_group, uint32_t abase, uint32_t a_slice,
-                                             uint32_t bbase, uint32_t b_slice, uint32_t idesc, bool first) {
+                                             uint32_t bbase, uint32_t b_slice, uint32_t idesc, bool first,
+                                             uint32_t a_sbo = 256, uint32_t b_sbo = 256) {
 #pragma unroll
   for (int q = 0; q < kPairs; ++q) {
     const int s = c_oz_pairs[q][0], t = c_oz_pairs[q][1], g = c_oz_pairs[q][2];
-    const uint64_t ad = tc::smem_desc(abase + s * a_slice, 128, 256);
-    const uint64_t bd = tc::smem_desc(bbase + t * b_slice, 128, 256);
+    const uint64_t ad = tc::smem_desc(abase + s * a_slice, 128, a_sbo);
+    const uint64_t bd = tc::smem_desc(bbase + t * b_slice, 128, b_sbo);
     tc::mma_s8(d_tmem + g * d_group, ad, bd, idesc, !(first && pair_leads(q)));
   }
+}
+
+// The same 15 products as 5 MMAs: for digit slice s of A, the pairs (s, t),
+// t = 0..4-s, go to the accumulator groups s + t, which are consecutive
+// 48-column blocks of TMEM; with the 5 slices of B stored one after another
+// (48 rows each, canonical layout) they are one MMA of N = 48 (5 - s) whose
+// output starts at group s.  A is read from shared memory 5 times per K step
+// instead of 15 (the MMAs are bound by shared-memory bandwidth otherwise).
+// The first MMA (s = 0, N = 240) covers every group, so it alone starts the
+// accumulators.
+template <int NB>
+__device__ __forceinline__ void oz_mma_fused(uint32_t d_tmem, uint32_t abase, uint32_t a_slice, uint32_t a_sbo,
+                                             uint32_t bbase, bool first) {
+#pragma unroll
+  for (int s = 0; s < kSlices; ++s) {
+    const uint64_t ad = tc::smem_desc(abase + s * a_slice, 128, a_sbo);
+    const uint64_t bd = tc::smem_desc(bbase, 128, 256);
+    tc::mma_s8(d_tmem + s * NB, ad, bd, tc::idesc_s8(128, NB * (kSlices - s)), !(first && s == 0));
+  }
+}
+
+// Slice-interleaved K-major block: 8-row groups of [slice][8 rows x 32 bytes]
+// (256 bytes per slice, 1280 per group), so that any run of whole 8-row
+// groups is one contiguous range holding all 5 slices.  Within a slice the
+// layout is the canonical one (LBO 128 between K halves, SBO 1280 between
+// 8-row groups).
+constexpr int kIlvGroup = kSlices * 256;
+__host__ __device__ constexpr int ilv_off(int r, int k, int s) {
+  return (r >> 3) * kIlvGroup + s * 256 + (r & 7) * 16 + (k & 15) + (k >> 4) * 128;
 }
 
 }  // namespace

@@ -48,6 +48,7 @@ struct ScreenPlan {
   int64_t* tso = nullptr;   // [ntiles+1] first slot of each tile
   int* slot_fn = nullptr;   // [nslots] function of each slot, -1 for padding
   int* slot_tile = nullptr; // [nslots]
+  int64_t* b_off = nullptr;  // [ntiles+1] first density B stage of each tile (INT8 path)
   BasisItem* items[kMaxL + 1] = {};
   // host copies of the partition
   std::vector<int64_t> h_tso;
@@ -607,24 +608,36 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
   int64_t budget_tiles = std::max<int64_t>(1, (int64_t)(0.05 * (double)freeb) / per_tile);
   if (in.max_chunk_points > 0) budget_tiles = std::min(budget_tiles, std::max<int64_t>(1, in.max_chunk_points / 128));
   budget_tiles = std::min<int64_t>(budget_tiles, 1 << 16);
+  // INT8 path: the gathered density B operand, per tile
+  std::vector<int64_t> boff((size_t)ntiles + 1, 0);
+  if (mixed)
+    for (int64_t t = 0; t < ntiles; ++t)
+      boff[(size_t)t + 1] = boff[(size_t)t] + screen_mixed_bstages(tso[(size_t)t + 1] - tso[(size_t)t]);
+  const int64_t budget_bstages =
+      mixed ? std::max<int64_t>((int64_t)(0.25 * (double)freeb) / screen_mixed_bytes_per_bstage(),
+                                screen_mixed_bstages(sp->max_n))
+            : INT64_MAX;
   sp->chunk_t0.push_back(0);
   {
     int64_t t0 = 0;
     for (int64_t t = 0; t < ntiles; ++t) {
       const bool full_slots = tso[(size_t)t + 1] - tso[(size_t)t0] > budget_slots;
       const bool full_tiles = t - t0 + 1 > budget_tiles;
-      if (t > t0 && (full_slots || full_tiles)) {
+      const bool full_b = boff[(size_t)t + 1] - boff[(size_t)t0] > budget_bstages;
+      if (t > t0 && (full_slots || full_tiles || full_b)) {
         sp->chunk_t0.push_back(t);
         t0 = t;
       }
     }
     sp->chunk_t0.push_back(ntiles);
   }
+  int64_t chunk_bstages = 0;
   const size_t nch = sp->chunk_t0.size() - 1;
   for (size_t c = 0; c < nch; ++c) {
     const int64_t t0 = sp->chunk_t0[c], t1 = sp->chunk_t0[c + 1];
     sp->chunk_tiles = std::max(sp->chunk_tiles, t1 - t0);
     sp->chunk_slots = std::max(sp->chunk_slots, tso[(size_t)t1] - tso[(size_t)t0]);
+    chunk_bstages = std::max(chunk_bstages, boff[(size_t)t1] - boff[(size_t)t0]);
   }
   for (int l = 0; l <= kMaxL; ++l)
     for (size_t c = 0; c <= nch; ++c) sp->item_off[l].push_back(tile_items[l][(size_t)sp->chunk_t0[c]]);
@@ -669,6 +682,10 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
     mi.chunk_slots = sp->chunk_slots + kSlack;
     mi.chunk_tiles = sp->chunk_tiles;
     mi.max_n = sp->max_n;
+    mi.chunk_bstages = chunk_bstages;
+    SP_TRY(sp_alloc(sp, &sp->b_off, boff.size()), "cudaMalloc");
+    SP_TRY(cudaMemcpy(sp->b_off, boff.data(), sizeof(int64_t) * boff.size(), cudaMemcpyHostToDevice), "copy");
+    mi.b_off = sp->b_off;
     const int st2 = screen_mixed_create(&sp->mixed, mi, err);
     if (st2) {
       screen_destroy(sp);

@@ -1,8 +1,8 @@
 // screened_mixed.cu -- INT8 tensor-core stages of the screened XC build.
 //
 // Both contractions of a tile run on tcgen05.mma kind::i8 with the Ozaki
-// split of ozaki.cuh (15 digit-pair MMAs per K step, exact INT32
-// accumulation in TMEM, FP64 combination):
+// split of ozaki.cuh (15 digit-pair products per K step issued as 5 MMAs of
+// N = 240..48, exact INT32 accumulation in TMEM, FP64 combination):
 //
 //   k_sm_quant_pts   phi_t -> INT8 digits, one scale per point          (A of X)
 //   k_sm_rowexp_P,   P -> packed digits P8[nu][mu] (5 bytes of a 64-bit
@@ -12,11 +12,14 @@
 //                    warps, two TMEM accumulator sets (MMA of slot block j+1
 //                    overlaps the epilogue of block j); fused FP64 epilogue
 //                    rho += X phi, grad rho += 2 X grad phi
-//   k_sm_zquant      Z = A phi (+ B . grad phi) in FP64 and the digits of Z
-//                    and phi, one scale per (tile, slot)                (A, B of V)
-//   k_sm_vpot        H[S_t, S_t] += Z_t^T phi_t, 128 x 48 slot blocks, K = the
+//   k_sm_zquant      Z = A phi (+ B . grad phi) in FP64 and the digits of phi
+//                    (slice-interleaved per 8 slots: one copy per A block) and
+//                    of Z (slices one after another), one scale per
+//                    (tile, slot)                                       (A, B of V)
+//   k_sm_vpot        H[S_t, S_t] += Z_t^T phi_t computed as phi_t Z_t^T (TMEM
+//                    lane = column j of H), 128 x 48 slot blocks, K = the
 //                    tile's 128 points; scaled in FP64 and scatter-added
-//                    into the full matrix with atomics
+//                    into the full matrix with atomics that run along rows
 //
 // Every mbarrier wait is bounded (tc::kWaitLimit); a wait that runs out sets
 // the device error flag and the kernel winds down.
@@ -41,9 +44,7 @@ constexpr int kBlkB = kN * 32;             // one slice of a 48-row x 32-byte K 
 constexpr int kOpA = kSlices * kBlkA;      // 20480
 constexpr int kOpB = kSlices * kBlkB;      // 7680
 constexpr int kAccCols = kGroups * kN;     // 240 TMEM columns per accumulator set
-constexpr int kDStages = 3;                // density: A (phi digit) ring
-constexpr int kBStages = 6;                // density: gathered B (P digit) ring
-constexpr int kVStages = 6;
+constexpr int kDStages = 4;                // density: operand ring (A and gathered B of one K step)
 constexpr int kDigBytesPerSlot = 640;      // 128 points x 5 slices
 
 }  // namespace
@@ -56,11 +57,14 @@ struct ScreenMixed {
   unsigned long long* P8 = nullptr;  // [nbas][nbas]
   int* e_P = nullptr;                // [nbas]
   int8_t* tA = nullptr;              // density A digits, [slot block of 32][slice][128 x 32] per tile
+  int8_t* tB = nullptr;              // density B digits, [stage][slice][48 x 32] per tile
+  const int64_t* b_off = nullptr;    // [ntiles + 1] first B stage of each tile
   int* e_pt = nullptr;               // [chunk_tiles * 128]
-  int8_t* tZ = nullptr;              // V operand digits, [kstep][slice][n x 32] per tile
-  int8_t* tF = nullptr;
-  int* e_Z = nullptr;                // [chunk_slots]
-  int* e_F = nullptr;
+  int8_t* tF = nullptr;              // V operand A (phi), [kstep][8-slot group][slice][8 x 32] per tile
+  int8_t* tZ = nullptr;              // V operand B (Z), [kstep][slice][n x 32] per tile
+  double* zs = nullptr;              // [chunk_slots] 2^e of each slot's Z digits
+  double* fs = nullptr;              // [chunk_slots] 2^(e - 40) of each slot's phi digits (the combine shift folded in)
+  double* ps = nullptr;              // [chunk_slots] 2^e_P of each slot's function (0 for padding)
   int* err = nullptr;
   int nsm = 148;
   std::vector<void*> allocs;
@@ -163,6 +167,50 @@ __device__ __forceinline__ unsigned long long gather_slice(const unsigned long l
 }
 
 // ---------------------------------------------------------------------------
+// B operand of the density contraction, per tile: for slot block j (48 rows
+// nu) and K step k (32 slots mu) the 5 digit slices of P[fn(nu)][fn(mu)] in
+// the K-major MMA layout, stored at stage b_off[t] + j nK + k; rows past the
+// tile's slots are zero.  One block per tile, thread = (row, 8 K values).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(192) k_sm_gather_B(const int64_t* __restrict__ tso,
+                                                    const int* __restrict__ slot_fn,
+                                                    const int64_t* __restrict__ b_off, int64_t t0, int64_t s0,
+                                                    const unsigned long long* __restrict__ P8,
+                                                    const int* __restrict__ e_P, int64_t nbas,
+                                                    int8_t* __restrict__ tB, double* __restrict__ ps) {
+  extern __shared__ int sfn[];
+  const int64_t t = t0 + blockIdx.x;
+  const int64_t sg = tso[t];
+  const int n = (int)(tso[t + 1] - sg);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    const int f = slot_fn[sg + i];
+    sfn[i] = f;
+    ps[sg - s0 + i] = f >= 0 ? pow2(e_P[f]) : 0.0;  // the row scale of P for the density epilogue
+  }
+  __syncthreads();
+  const int nK = n / 32, nN = (n + kN - 1) / kN;
+  const int r = threadIdx.x >> 2, grp = threadIdx.x & 3;
+  int8_t* out = tB + (b_off[t] - b_off[t0]) * kOpB;
+  for (int j = 0; j < nN; ++j) {
+    const int nu = j * kN + r;
+    const int fnv = nu < n ? sfn[nu] : -1;
+    const unsigned long long* prow = P8 + (int64_t)max(fnv, 0) * nbas;
+    for (int k = 0; k < nK; ++k) {
+      unsigned long long w[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int fmu = sfn[k * 32 + grp * 8 + u];
+        w[u] = (fnv >= 0 && fmu >= 0) ? __ldg(prow + fmu) : 0ull;
+      }
+      int8_t* o = out + (int64_t)(j * nK + k) * kOpB;
+#pragma unroll
+      for (int sl = 0; sl < kSlices; ++sl)
+        *reinterpret_cast<unsigned long long*>(o + sl * kBlkB + blk_off(r, grp * 8)) = gather_slice(w, sl);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // X = phi_t P[S_t, S_t] with fused rho / grad rho
 // ---------------------------------------------------------------------------
 // epilogue operands: phi (and grad phi) of 6 slots x 128 points per buffer
@@ -171,20 +219,18 @@ constexpr int kERing = 4;
 constexpr int kEBuf = 4 * kECols * 128;  // doubles
 struct DensSmem {
   alignas(1024) int8_t a[kDStages][kOpA];
-  alignas(1024) int8_t b[kBStages][kOpB];
+  alignas(1024) int8_t b[kDStages][kOpB];
   alignas(128) double e[kERing][kEBuf];   // [array][column][point]
   uint64_t full[kDStages];
   uint64_t empty[kDStages];
-  uint64_t b_full[kBStages];
-  uint64_t b_empty[kBStages];
   uint64_t acc_full[2];
   uint64_t acc_empty[2];
   uint64_t e_full[kERing];
   uint64_t e_empty[kERing];
   uint32_t tslot;
 };
-// warps 0-7 epilogue, 8 MMA, 9 A copies, 10-13 B gather, 14 epilogue-operand copies
-constexpr int kDensThreads = 480;
+// warps 0-7 epilogue, 8 MMA, 9 operand copies, 10 epilogue-operand copies
+constexpr int kDensThreads = 352;
 
 // TMEM -> 16 + 8 combined FP64 values of one accumulator set (columns c0..c0+23)
 __device__ __forceinline__ void read_acc24(uint32_t taddr, double (&x)[24]) {
@@ -224,7 +270,7 @@ template <bool GGA>
 __global__ void __launch_bounds__(kDensThreads, 1)
     k_sm_density(const int64_t* __restrict__ tso, const int* __restrict__ slot_fn, int64_t t0, int64_t nt,
                  int64_t s0, const int8_t* __restrict__ tA, const int* __restrict__ e_pt,
-                 const unsigned long long* __restrict__ P8, const int* __restrict__ e_P, int64_t nbas,
+                 const int8_t* __restrict__ tB, const int64_t* __restrict__ b_off, const double* __restrict__ ps,
                  const double* __restrict__ phi, const double* __restrict__ gx, const double* __restrict__ gy,
                  const double* __restrict__ gz, double* __restrict__ rho, double* __restrict__ grx,
                  double* __restrict__ gry, double* __restrict__ grz, int* err) {
@@ -236,10 +282,6 @@ __global__ void __launch_bounds__(kDensThreads, 1)
     for (int s = 0; s < kDStages; ++s) {
       tc::mbar_init(&S.full[s], 1);
       tc::mbar_init(&S.empty[s], 1);
-    }
-    for (int s = 0; s < kBStages; ++s) {
-      tc::mbar_init(&S.b_full[s], 128);
-      tc::mbar_init(&S.b_empty[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
       tc::mbar_init(&S.acc_full[b], 1);
@@ -256,7 +298,7 @@ __global__ void __launch_bounds__(kDensThreads, 1)
   tc::fence_after_sync();
   const uint32_t tbase = S.tslot;
   bool ok = true;
-  if (warp == 14) {
+  if (warp == 10) {
     if (lane == 0) {  // epilogue operands: per slot block j, half h, group u: 6 slots of phi (grad phi)
       int e = 0;
       for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
@@ -304,7 +346,6 @@ __global__ void __launch_bounds__(kDensThreads, 1)
     }
   } else if (warp == 8) {
     if (lane == 0) {  // MMA issuer
-      const uint32_t idesc = tc::idesc_s8(kM, kN);
       int it = 0, jj = 0;
       for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
         const int n = (int)(tso[t0 + ti + 1] - tso[t0 + ti]);
@@ -317,17 +358,14 @@ __global__ void __launch_bounds__(kDensThreads, 1)
           }
           tc::fence_after_sync();
           for (int k = 0; k < nK; ++k, ++it) {
-            const int s = it % kDStages, sbb = it % kBStages;
-            if (!tc::mbar_wait(&S.full[s], (it / kDStages) & 1) ||
-                !tc::mbar_wait(&S.b_full[sbb], (it / kBStages) & 1)) {
+            const int s = it % kDStages;
+            if (!tc::mbar_wait(&S.full[s], (it / kDStages) & 1)) {
               ok = false;
               break;
             }
             tc::fence_after_sync();
-            oz_mma_pairs(tbase + b * kAccCols, kN, tc::smem_u32(S.a[s]), kBlkA, tc::smem_u32(S.b[sbb]), kBlkB, idesc,
-                         k == 0);
+            oz_mma_fused<kN>(tbase + b * kAccCols, tc::smem_u32(S.a[s]), kBlkA, 256, tc::smem_u32(S.b[s]), k == 0);
             tc::mma_commit(&S.empty[s]);
-            tc::mma_commit(&S.b_empty[sbb]);
           }
           tc::mma_commit(&S.acc_full[b]);
         }
@@ -335,13 +373,14 @@ __global__ void __launch_bounds__(kDensThreads, 1)
       if (!ok) atomicExch(err, 1);
     }
   } else if (warp == 9) {
-    if (lane == 0) {  // A producer: digits of phi, one 32-slot K block per stage
+    if (lane == 0) {  // operand producer: per K step the phi digits (A) and the gathered P digits (B)
       int it = 0;
       for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
         const int64_t sb = tso[t0 + ti] - s0;
         const int n = (int)(tso[t0 + ti + 1] - tso[t0 + ti]);
         const int nK = n / 32, nN = (n + kN - 1) / kN;
-        const int8_t* src = tA + sb * kDigBytesPerSlot;
+        const int8_t* asrc = tA + sb * kDigBytesPerSlot;
+        const int8_t* bsrc = tB + (b_off[t0 + ti] - b_off[t0]) * kOpB;
         for (int j = 0; j < nN && ok; ++j)
           for (int k = 0; k < nK; ++k, ++it) {
             const int s = it % kDStages;
@@ -349,70 +388,29 @@ __global__ void __launch_bounds__(kDensThreads, 1)
               ok = false;
               break;
             }
-            tc::mbar_expect_tx(&S.full[s], kOpA);
-            tc::bulk_g2s(S.a[s], src + (int64_t)k * kOpA, kOpA, &S.full[s]);
+            tc::mbar_expect_tx(&S.full[s], kOpA + kOpB);
+            tc::bulk_g2s(S.a[s], asrc + (int64_t)k * kOpA, kOpA, &S.full[s]);
+            tc::bulk_g2s(S.b[s], bsrc + (int64_t)(j * nK + k) * kOpB, kOpB, &S.full[s]);
           }
       }
       if (!ok) atomicExch(err, 1);
     }
-  } else if (warp >= 10 && warp < 14) {  // B producers: P8[fn(nu)][fn(mu)] gathered into the K-major digit block
-    // thread g: tasks g and g + 128 (rows r = task / 4, 8 K values from 8 (task % 4));
-    // warps 10-11 have two tasks, 12-13 one (uniform per warp)
-    const int g = tid - 320;
-    const bool two = g < kN * 4 - 128;
-    int it = 0;
-    for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
-      const int64_t sg = tso[t0 + ti];
-      const int n = (int)(tso[t0 + ti + 1] - sg);
-      const int nK = n / 32, nN = (n + kN - 1) / kN;
-      const int* sfn = slot_fn + sg;
-      for (int j = 0; j < nN && ok; ++j) {
-        const int nu0 = j * kN + (g >> 2), nu1 = j * kN + ((g + 128) >> 2);
-        const int fnv0 = nu0 < n ? __ldg(sfn + nu0) : -1;
-        const int fnv1 = (two && nu1 < n) ? __ldg(sfn + nu1) : -1;
-        const int grp0 = g & 3, grp1 = (g + 128) & 3;
-        for (int k = 0; k < nK; ++k, ++it) {
-          const int sbb = it % kBStages;
-          const int fmu_lane = __ldg(sfn + k * 32 + lane);
-          if (it >= kBStages && !tc::mbar_wait(&S.b_empty[sbb], ((it / kBStages) - 1) & 1)) {
-            ok = false;
-            break;
-          }
-          unsigned long long w0[8], w1[8];
-#pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            const int f0 = __shfl_sync(0xffffffffu, fmu_lane, grp0 * 8 + u);
-            const int f1 = __shfl_sync(0xffffffffu, fmu_lane, grp1 * 8 + u);
-            w0[u] = (fnv0 >= 0 && f0 >= 0) ? __ldg(P8 + (int64_t)fnv0 * nbas + f0) : 0ull;
-            w1[u] = (fnv1 >= 0 && f1 >= 0) ? __ldg(P8 + (int64_t)fnv1 * nbas + f1) : 0ull;
-          }
-#pragma unroll
-          for (int sl = 0; sl < kSlices; ++sl) {
-            *reinterpret_cast<unsigned long long*>(S.b[sbb] + sl * kBlkB + blk_off(g >> 2, grp0 * 8)) =
-                gather_slice(w0, sl);
-            if (two)
-              *reinterpret_cast<unsigned long long*>(S.b[sbb] + sl * kBlkB + blk_off((g + 128) >> 2, grp1 * 8)) =
-                  gather_slice(w1, sl);
-          }
-          tc::fence_proxy_async();
-          tc::mbar_arrive(&S.b_full[sbb]);
-        }
-      }
-    }
-    if (!ok) atomicExch(err, 1);
   } else {  // epilogue: point row = 32 (warp & 3) + lane, columns 24 (warp >> 2) .. +24 of each slot block
     const int row = (warp & 3) * 32 + lane, half = warp >> 2;
     const uint32_t trow = tbase + ((uint32_t)((warp & 3) * 32) << 16) + half * 24;
     int jj = 0;
     for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
       const int64_t sg = tso[t0 + ti];
+      const int64_t sb = sg - s0;
       const int n = (int)(tso[t0 + ti + 1] - sg);
       const int nN = (n + kN - 1) / kN;
-      const int* sfn = slot_fn + sg;
       const double rs = pow2(e_pt[ti * 128 + row] + kCombShift);
       double r_acc = 0.0, g_acc[3] = {0.0, 0.0, 0.0};
       for (int j = 0; j < nN && ok; ++j, ++jj) {
         const int b = jj & 1;
+        // the P row scale of column lane (< 24) of this warp's half, broadcast below
+        const int cl = j * kN + half * 24 + lane;
+        const double psl = (lane < 24 && cl < n) ? __ldg(ps + sb + cl) : 0.0;
         if (!tc::mbar_wait(&S.acc_full[b], (jj >> 1) & 1)) {
           ok = false;
           break;
@@ -433,10 +431,8 @@ __global__ void __launch_bounds__(kDensThreads, 1)
           const double* eb = S.e[r];
 #pragma unroll
           for (int v = 0; v < kECols; ++v) {
-            const int c = c0 + v;
-            if (c < n) {
-              const int f = __ldg(sfn + c);
-              const double X = f >= 0 ? x[u * kECols + v] * (rs * pow2(__ldg(e_P + f))) : 0.0;
+            const double X = x[u * kECols + v] * (rs * __shfl_sync(0xffffffffu, psl, u * kECols + v));
+            if (c0 + v < n) {
               r_acc += X * eb[v * 128 + row];
               if (GGA) {
                 g_acc[0] += X * eb[(kECols + v) * 128 + row];
@@ -480,7 +476,7 @@ __global__ void __launch_bounds__(256, 2) k_sm_zquant(const int64_t* __restrict_
                                                    const double* __restrict__ A, const double* __restrict__ Bx,
                                                    const double* __restrict__ By, const double* __restrict__ Bz,
                                                    int8_t* __restrict__ tZ, int8_t* __restrict__ tF,
-                                                   int* __restrict__ e_Z, int* __restrict__ e_F) {
+                                                   double* __restrict__ zs, double* __restrict__ fs) {
   __shared__ double sA[128], sB[3][128];
   const int64_t t = t0 + blockIdx.x;
   const int64_t sb = tso[t] - s0;
@@ -525,8 +521,8 @@ __global__ void __launch_bounds__(256, 2) k_sm_zquant(const int64_t* __restrict_
     const double mf = warp_max(fmax(fmax(fabs(f[0]), fabs(f[1])), fmax(fabs(f[2]), fabs(f[3]))));
     const int ez = scale_exp(mz), ef = scale_exp(mf);
     if (lane == 0) {
-      e_Z[sb + i] = ez;
-      e_F[sb + i] = ef;
+      zs[sb + i] = pow2(ez);
+      fs[sb + i] = pow2(ef + kCombShift);
     }
     long long qz[4], qf[4];
 #pragma unroll
@@ -539,22 +535,29 @@ __global__ void __launch_bounds__(256, 2) k_sm_zquant(const int64_t* __restrict_
     oz_pack4(qf, wf);
 #pragma unroll
     for (int sl = 0; sl < kSlices; ++sl) {
-      const int64_t off = tile_off + (int64_t)(kstep * kSlices + sl) * n * 32 + blk_off(i, kin);
-      *reinterpret_cast<uint32_t*>(tZ + off) = wz[sl];
-      *reinterpret_cast<uint32_t*>(tF + off) = wf[sl];
+      const int64_t kb = tile_off + (int64_t)kstep * n * (32 * kSlices);
+      *reinterpret_cast<uint32_t*>(tF + kb + ilv_off(i, kin, sl)) = wf[sl];
+      *reinterpret_cast<uint32_t*>(tZ + kb + (int64_t)sl * n * 32 + blk_off(i, kin)) = wz[sl];
     }
   }
 }
 
 // ---------------------------------------------------------------------------
-// H[S_t, S_t] += Z_t^T phi_t, scatter-added into V (LDA: fn_i <= fn_j only,
-// H is symmetric; GGA: the whole square, V = H + H^T when packing).
-// Pairs of 128-slot row blocks I and 48-slot column blocks J, K = the tile's
-// 128 points in 4 steps.  Persistent like k_sm_density.
+// H[S_t, S_t] += Z_t^T phi_t, scatter-added into V with FP64 atomics (LDA:
+// fn_i <= fn_j only, H is symmetric; GGA: the whole square, V = H + H^T when
+// packing, the ham + ham^T of modules/xc_hamiltonian.f90:1559-1566).
+// Computed as D = phi_J Z_I^T: the 128 TMEM lanes are columns j of H, so the
+// 32 atomics of a warp instruction run along one row of V (consecutive
+// functions, few sectors).  Pairs of 128-slot blocks J (A, phi) and 48-slot
+// blocks I (B, Z); K = the tile's 128 points in 4 steps; each A block is one
+// copy of whole 8-slot groups and stays resident for its 48-slot blocks.
+// Persistent like k_sm_density.
 // ---------------------------------------------------------------------------
+constexpr int kVStages = 8;
 struct VSmem {
-  alignas(1024) int8_t a[kVStages][kOpA];
-  alignas(1024) int8_t b[kVStages][kOpB];
+  alignas(1024) int8_t a[2][4][kOpA];      // phi digits of a 128-slot block, all 4 K steps, double-buffered
+  alignas(1024) int8_t b[kVStages][kOpB];  // Z digits of a 48-slot block, one K step
+  uint64_t a_full[2], a_empty[2];
   uint64_t full[kVStages];
   uint64_t empty[kVStages];
   uint64_t acc_full[2];
@@ -563,19 +566,23 @@ struct VSmem {
 };
 constexpr int kVThreads = 320;  // warps 0-7 epilogue, 8 MMA, 9 producer
 
-// first 48-slot block of pair row I: LDA needs columns j >= 128 I only
-__device__ __forceinline__ int first_J(int I, bool all) { return all ? 0 : (kM * I) / kN; }
+// LDA keeps j >= i: the last 48-slot row block I of column block J
+__device__ __forceinline__ int last_I(int J, int nI, bool all) { return all ? nI : min(nI, (kM * J + kM - 1) / kN + 1); }
 
 template <bool GGA>
 __global__ void __launch_bounds__(kVThreads, 1)
     k_sm_vpot(const int64_t* __restrict__ tso, const int* __restrict__ slot_fn, int64_t t0, int64_t nt, int64_t s0,
-              const int8_t* __restrict__ tZ, const int8_t* __restrict__ tF, const int* __restrict__ e_Z,
-              const int* __restrict__ e_F, double* __restrict__ V, int64_t ldv, int* err) {
+              const int8_t* __restrict__ tF, const int8_t* __restrict__ tZ, const double* __restrict__ fs,
+              const double* __restrict__ zs, double* __restrict__ V, int64_t ldv, int* err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   VSmem& S = *reinterpret_cast<VSmem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   if (warp == 0) tc::tmem_alloc(&S.tslot, 512);
   if (tid == 0) {
+    for (int q = 0; q < 2; ++q) {
+      tc::mbar_init(&S.a_full[q], 1);
+      tc::mbar_init(&S.a_empty[q], 1);
+    }
     for (int s = 0; s < kVStages; ++s) {
       tc::mbar_init(&S.full[s], 1);
       tc::mbar_init(&S.empty[s], 1);
@@ -592,43 +599,53 @@ __global__ void __launch_bounds__(kVThreads, 1)
   const uint32_t tbase = S.tslot;
   bool ok = true;
   if (warp == 9) {
-    if (lane == 0) {  // producer: per pair and K step, Z rows of block I and phi rows of block J
-      int it = 0;
+    if (lane == 0) {  // producer: the phi block of each J once, the Z block of each (J, I) pair per K step
+      int it = 0, ia = 0;
       for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
         const int64_t sb = tso[t0 + ti] - s0;
         const int n = (int)(tso[t0 + ti + 1] - tso[t0 + ti]);
-        const int nI = (n + kM - 1) / kM, nJ = (n + kN - 1) / kN;
-        const int8_t* zsrc = tZ + sb * kDigBytesPerSlot;
+        const int nJ = (n + kM - 1) / kM, nI = (n + kN - 1) / kN;
         const int8_t* fsrc = tF + sb * kDigBytesPerSlot;
-        const int64_t blk = (int64_t)n * 32;  // bytes of one (K step, slice) block of the tile
-        for (int I = 0; I < nI && ok; ++I)
-          for (int J = first_J(I, GGA); J < nJ && ok; ++J)
+        const int8_t* zsrc = tZ + sb * kDigBytesPerSlot;
+        const int64_t kblk = (int64_t)n * 32 * kSlices;  // bytes of one K step of the tile
+        for (int J = 0; J < nJ && ok; ++J, ++ia) {
+          const int qa = ia & 1;
+          if (ia >= 2 && !tc::mbar_wait(&S.a_empty[qa], ((ia >> 1) - 1) & 1)) {
+            ok = false;
+            break;
+          }
+          tc::mbar_expect_tx(&S.a_full[qa], 4 * kOpA);
+          for (int k = 0; k < 4; ++k)
+            tc::bulk_g2s(S.a[qa][k], fsrc + k * kblk + (int64_t)J * (kM / 8) * kIlvGroup, kOpA, &S.a_full[qa]);
+          for (int I = 0; I < last_I(J, nI, GGA) && ok; ++I)
             for (int k = 0; k < 4; ++k, ++it) {
               const int s = it % kVStages;
               if (it >= kVStages && !tc::mbar_wait(&S.empty[s], ((it / kVStages) - 1) & 1)) {
                 ok = false;
                 break;
               }
-              tc::mbar_expect_tx(&S.full[s], kOpA + kOpB);
-              for (int sl = 0; sl < kSlices; ++sl) {
-                tc::bulk_g2s(S.a[s] + sl * kBlkA, zsrc + (k * kSlices + sl) * blk + (int64_t)I * kM * 32, kBlkA,
+              tc::mbar_expect_tx(&S.full[s], kOpB);
+              for (int sl = 0; sl < kSlices; ++sl)
+                tc::bulk_g2s(S.b[s] + sl * kBlkB, zsrc + k * kblk + (int64_t)sl * n * 32 + (int64_t)I * kN * 32, kBlkB,
                              &S.full[s]);
-                tc::bulk_g2s(S.b[s] + sl * kBlkB, fsrc + (k * kSlices + sl) * blk + (int64_t)J * kN * 32, kBlkB,
-                             &S.full[s]);
-              }
             }
+        }
       }
       if (!ok) atomicExch(err, 1);
     }
   } else if (warp == 8) {
     if (lane == 0) {  // MMA issuer
-      const uint32_t idesc = tc::idesc_s8(kM, kN);
-      int it = 0, pp = 0;
+      int it = 0, pp = 0, ia = 0;
       for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
         const int n = (int)(tso[t0 + ti + 1] - tso[t0 + ti]);
-        const int nI = (n + kM - 1) / kM, nJ = (n + kN - 1) / kN;
-        for (int I = 0; I < nI && ok; ++I)
-          for (int J = first_J(I, GGA); J < nJ && ok; ++J, ++pp) {
+        const int nJ = (n + kM - 1) / kM, nI = (n + kN - 1) / kN;
+        for (int J = 0; J < nJ && ok; ++J, ++ia) {
+          const int qa = ia & 1;
+          if (!tc::mbar_wait(&S.a_full[qa], (ia >> 1) & 1)) {
+            ok = false;
+            break;
+          }
+          for (int I = 0; I < last_I(J, nI, GGA) && ok; ++I, ++pp) {
             const int b = pp & 1;
             if (pp >= 2 && !tc::mbar_wait(&S.acc_empty[b], ((pp >> 1) - 1) & 1)) {
               ok = false;
@@ -642,16 +659,18 @@ __global__ void __launch_bounds__(kVThreads, 1)
                 break;
               }
               tc::fence_after_sync();
-              oz_mma_pairs(tbase + b * kAccCols, kN, tc::smem_u32(S.a[s]), kBlkA, tc::smem_u32(S.b[s]), kBlkB,
-                           idesc, k == 0);
+              oz_mma_fused<kN>(tbase + b * kAccCols, tc::smem_u32(S.a[qa][k]), 256, kIlvGroup, tc::smem_u32(S.b[s]),
+                               k == 0);
               tc::mma_commit(&S.empty[s]);
             }
             tc::mma_commit(&S.acc_full[b]);
           }
+          tc::mma_commit(&S.a_empty[qa]);
+        }
       }
       if (!ok) atomicExch(err, 1);
     }
-  } else {  // epilogue: slot row i = 128 I + 32 (warp & 3) + lane, columns 24 (warp >> 2) .. of each block
+  } else {  // epilogue: column j = 128 J + 32 (warp & 3) + lane of H, rows 24 (warp >> 2) .. of each 48-slot block
     const int half = warp >> 2;
     const uint32_t trow = tbase + ((uint32_t)((warp & 3) * 32) << 16) + half * 24;
     int pp = 0;
@@ -659,14 +678,18 @@ __global__ void __launch_bounds__(kVThreads, 1)
       const int64_t sg = tso[t0 + ti];
       const int64_t sb = sg - s0;
       const int n = (int)(tso[t0 + ti + 1] - sg);
-      const int nI = (n + kM - 1) / kM, nJ = (n + kN - 1) / kN;
+      const int nJ = (n + kM - 1) / kM, nI = (n + kN - 1) / kN;
       const int* sfn = slot_fn + sg;
-      for (int I = 0; I < nI && ok; ++I) {
-        const int i = I * kM + (warp & 3) * 32 + lane;
-        const int fi = i < n ? __ldg(sfn + i) : -1;
-        const int ezi = i < n ? __ldg(e_Z + sb + i) : 0;
-        for (int J = first_J(I, GGA); J < nJ; ++J, ++pp) {
+      for (int J = 0; J < nJ && ok; ++J) {
+        const int j = J * kM + (warp & 3) * 32 + lane;
+        const int fj = j < n ? __ldg(sfn + j) : -1;
+        const double fsj = j < n ? __ldg(fs + sb + j) : 0.0;
+        for (int I = 0; I < last_I(J, nI, GGA); ++I, ++pp) {
           const int b = pp & 1;
+          // row i of lane (< 24) of this warp's 24: its function and scale, broadcast below
+          const int il = I * kN + half * 24 + lane;
+          const int fil = (lane < 24 && il < n) ? __ldg(sfn + il) : -1;
+          const double zsl = (lane < 24 && il < n) ? __ldg(zs + sb + il) : 0.0;
           if (!tc::mbar_wait(&S.acc_full[b], (pp >> 1) & 1)) {
             ok = false;
             break;
@@ -676,14 +699,11 @@ __global__ void __launch_bounds__(kVThreads, 1)
           read_acc24(trow + b * kAccCols, x);
           tc::fence_before_sync();
           tc::mbar_arrive(&S.acc_empty[b]);
-          if (fi < 0) continue;
-          const int j0 = J * kN + half * 24;
 #pragma unroll
           for (int c = 0; c < 24; ++c) {
-            const int j = j0 + c;
-            const int fj = j < n ? __ldg(sfn + j) : -1;
-            if (fj >= 0 && (GGA || fj >= fi))
-              atomicAdd(V + (int64_t)fi * ldv + fj, x[c] * pow2(ezi + __ldg(e_F + sb + j) + kCombShift));
+            const int fi = __shfl_sync(0xffffffffu, fil, c);
+            const double zsc = __shfl_sync(0xffffffffu, zsl, c);
+            if (fj >= 0 && fi >= 0 && (GGA || fj >= fi)) atomicAdd(V + (int64_t)fi * ldv + fj, x[c] * (fsj * zsc));
           }
         }
       }
@@ -698,6 +718,8 @@ __global__ void __launch_bounds__(kVThreads, 1)
 }  // namespace
 
 int64_t screen_mixed_bytes_per_slot() { return 3 * kDigBytesPerSlot + 8; }
+int64_t screen_mixed_bstages(int64_t n) { return ((n + kN - 1) / kN) * (n / 32); }
+int64_t screen_mixed_bytes_per_bstage() { return kOpB; }
 int64_t screen_mixed_bytes_per_tile() { return 128 * 4; }
 
 int screen_mixed_create(ScreenMixed** out, const ScreenMixedInput& in, std::string& err) {
@@ -714,11 +736,14 @@ int screen_mixed_create(ScreenMixed** out, const ScreenMixedInput& in, std::stri
   if (e == cudaSuccess) e = sm_alloc(m, &m->P8, (size_t)in.nbas * in.nbas);
   if (e == cudaSuccess) e = sm_alloc(m, &m->e_P, (size_t)in.nbas);
   if (e == cudaSuccess) e = sm_alloc(m, &m->tA, dig);
+  if (e == cudaSuccess) e = sm_alloc(m, &m->tB, (size_t)in.chunk_bstages * kOpB);
+  m->b_off = in.b_off;
   if (e == cudaSuccess) e = sm_alloc(m, &m->tZ, dig);
   if (e == cudaSuccess) e = sm_alloc(m, &m->tF, dig);
   if (e == cudaSuccess) e = sm_alloc(m, &m->e_pt, (size_t)in.chunk_tiles * 128);
-  if (e == cudaSuccess) e = sm_alloc(m, &m->e_Z, (size_t)in.chunk_slots);
-  if (e == cudaSuccess) e = sm_alloc(m, &m->e_F, (size_t)in.chunk_slots);
+  if (e == cudaSuccess) e = sm_alloc(m, &m->zs, (size_t)in.chunk_slots);
+  if (e == cudaSuccess) e = sm_alloc(m, &m->fs, (size_t)in.chunk_slots);
+  if (e == cudaSuccess) e = sm_alloc(m, &m->ps, (size_t)in.chunk_slots);
   if (e == cudaSuccess) e = sm_alloc(m, &m->err, 1);
   // the slack rows after a chunk's last slot are read (never used) by whole-block copies
   if (e == cudaSuccess) e = cudaMemset(m->tA, 0, dig);
@@ -730,11 +755,12 @@ int screen_mixed_create(ScreenMixed** out, const ScreenMixedInput& in, std::stri
     screen_mixed_destroy(m);
     return e == cudaErrorMemoryAllocation ? PGXC_ENOMEM : PGXC_ECUDA;
   }
-  const int dsm = (int)sizeof(DensSmem), vsm = (int)sizeof(VSmem);
+  const int dsm = (int)sizeof(DensSmem);
+  cudaFuncSetAttribute(k_sm_gather_B, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * in.max_n);
   cudaFuncSetAttribute(k_sm_density<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm);
   cudaFuncSetAttribute(k_sm_density<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm);
-  cudaFuncSetAttribute(k_sm_vpot<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, vsm);
-  e = cudaFuncSetAttribute(k_sm_vpot<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, vsm);
+  cudaFuncSetAttribute(k_sm_vpot<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(VSmem));
+  e = cudaFuncSetAttribute(k_sm_vpot<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(VSmem));
   int dev = 0;
   if (e == cudaSuccess) e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&m->nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -776,16 +802,18 @@ int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn,
     cudaMemsetAsync(gry, 0, sizeof(double) * nt * 128, st);
     cudaMemsetAsync(grz, 0, sizeof(double) * nt * 128, st);
   }
+  k_sm_gather_B<<<(unsigned)nt, 192, 4 * m->max_n, st>>>(tso, slot_fn, m->b_off, t0, s0, m->P8, m->e_P, m->nbas,
+                                                         m->tB, m->ps);
   const unsigned grid = (unsigned)std::min<int64_t>(nt, m->nsm);
   const int smem = (int)sizeof(DensSmem);
   if (m->gga)
-    k_sm_density<true><<<grid, kDensThreads, smem, st>>>(tso, slot_fn, t0, nt, s0, m->tA, m->e_pt, m->P8, m->e_P,
-                                                         m->nbas, phi, gx, gy, gz, rho, grx, gry, grz, m->err);
+    k_sm_density<true><<<grid, kDensThreads, smem, st>>>(tso, slot_fn, t0, nt, s0, m->tA, m->e_pt, m->tB, m->b_off,
+                                                         m->ps, phi, gx, gy, gz, rho, grx, gry, grz, m->err);
   else
-    k_sm_density<false><<<grid, kDensThreads, smem, st>>>(tso, slot_fn, t0, nt, s0, m->tA, m->e_pt, m->P8, m->e_P,
-                                                          m->nbas, phi, nullptr, nullptr, nullptr, rho, nullptr,
+    k_sm_density<false><<<grid, kDensThreads, smem, st>>>(tso, slot_fn, t0, nt, s0, m->tA, m->e_pt, m->tB, m->b_off,
+                                                          m->ps, phi, nullptr, nullptr, nullptr, rho, nullptr,
                                                           nullptr, nullptr, m->err);
-  return 1;
+  return 2;
 }
 
 int screen_mixed_potential(ScreenMixed* m, const int64_t* tso, const int* slot_fn, const int* slot_tile, int64_t t0,
@@ -796,18 +824,17 @@ int screen_mixed_potential(ScreenMixed* m, const int64_t* tso, const int* slot_f
   (void)ns;
   if (m->gga)
     k_sm_zquant<true><<<(unsigned)nt, 256, 0, st>>>(tso, t0, s0, phi, gx, gy, gz, A, Bx, By, Bz, m->tZ, m->tF,
-                                                    m->e_Z, m->e_F);
+                                                    m->zs, m->fs);
   else
     k_sm_zquant<false><<<(unsigned)nt, 256, 0, st>>>(tso, t0, s0, phi, nullptr, nullptr, nullptr, A, nullptr,
-                                                     nullptr, nullptr, m->tZ, m->tF, m->e_Z, m->e_F);
+                                                     nullptr, nullptr, m->tZ, m->tF, m->zs, m->fs);
   cudaEventRecord(k0, st);
   const unsigned grid = (unsigned)std::min<int64_t>(nt, m->nsm);
-  const int smem = (int)sizeof(VSmem);
   if (m->gga)
-    k_sm_vpot<true><<<grid, kVThreads, smem, st>>>(tso, slot_fn, t0, nt, s0, m->tZ, m->tF, m->e_Z, m->e_F, V, ldv,
+    k_sm_vpot<true><<<grid, kVThreads, (int)sizeof(VSmem), st>>>(tso, slot_fn, t0, nt, s0, m->tF, m->tZ, m->fs, m->zs, V, ldv,
                                                    m->err);
   else
-    k_sm_vpot<false><<<grid, kVThreads, smem, st>>>(tso, slot_fn, t0, nt, s0, m->tZ, m->tF, m->e_Z, m->e_F, V, ldv,
+    k_sm_vpot<false><<<grid, kVThreads, (int)sizeof(VSmem), st>>>(tso, slot_fn, t0, nt, s0, m->tF, m->tZ, m->fs, m->zs, V, ldv,
                                                     m->err);
   cudaEventRecord(k1, st);
   return 2;

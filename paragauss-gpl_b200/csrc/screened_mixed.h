@@ -19,11 +19,16 @@ struct ScreenMixedInput {
   int64_t chunk_slots = 0;   // slot rows of the chunk buffers (slack included)
   int64_t chunk_tiles = 0;
   int max_n = 0;             // largest padded slot count of a tile
+  int64_t chunk_bstages = 0; // density B stages of the largest chunk
+  const int64_t* b_off = nullptr;  // device [ntiles + 1]: first density B stage of each tile
 };
 
 // device bytes per slot row and per tile of the chunk buffers
 int64_t screen_mixed_bytes_per_slot();
 int64_t screen_mixed_bytes_per_tile();
+// density B stages (48-slot blocks x 32-slot K steps) of a tile with n slots, and bytes per stage
+int64_t screen_mixed_bstages(int64_t n);
+int64_t screen_mixed_bytes_per_bstage();
 int screen_mixed_create(ScreenMixed** out, const ScreenMixedInput& in, std::string& err);
 void screen_mixed_destroy(ScreenMixed* m);
 // INT8 digits of the FP64 density matrix a.P (per-row scales); returns launches
