@@ -107,7 +107,7 @@ __device__ __forceinline__ void shell_at_point(const DevShell& S, const DevSA& s
                                                const int2* rng, bool valid, uint64_t mask, int64_t base, int nsel,
                                                int64_t p,
                                                int64_t ld, double* __restrict__ phi, double* __restrict__ gx,
-                                               double* __restrict__ gy, double* __restrict__ gz) {
+                                               double* __restrict__ gy, double* __restrict__ gz, double& vmax) {
   double Y[16];
   double dY[3][16];
   solid_harmonics<L, double>(x, y, z, Y, dY);
@@ -157,6 +157,7 @@ __device__ __forceinline__ void shell_at_point(const DevShell& S, const DevSA& s
       for (int i = 0; i < 2 * L + 1; ++i) {
         const int64_t f = base + (int64_t)i * nsel + k;
         phi[f * ld + p] = Ys[i] * Rr;
+        vmax = fmax(vmax, fabs(Ys[i] * Rr));
         if (GRAD) {
           const double h = Ys[i] * dR;
           gx[f * ld + p] = x * h + dYs[0][i] * Rr;
@@ -206,6 +207,7 @@ __device__ __forceinline__ void shell_at_point(const DevShell& S, const DevSA& s
         if (rr[r] >= 0) {
           const int64_t f = base + (int64_t)i * nsel + k0 + r;
           phi[f * ld + p] = Ys[i] * Rr[r];
+          vmax = fmax(vmax, fabs(Ys[i] * Rr[r]));
           if (GRAD) {
             const double h = Ys[i] * dR[r];
             gx[f * ld + p] = x * h + dYs[0][i] * Rr[r];
@@ -274,14 +276,16 @@ __global__ void __launch_bounds__(128) k_basis_l(const DevShell* __restrict__ sh
     y = py[p0 + p] - atoms[3 * S.atom + 1];
     z = pz[p0 + p] - atoms[3 * S.atom + 2];
   }
+  double vmax = 0.0;
   shell_at_point<L, GRAD>(S, sa, x, y, z, staged ? st.e : exps, staged ? st.n : norms, staged ? st.c : contr, st.r,
-                          valid, all_radial(S.nrad), S.f0, S.nrad, p, ld, phi, gx, gy, gz);
+                          valid, all_radial(S.nrad), S.f0, S.nrad, p, ld, phi, gx, gy, gz, vmax);
 }
 
 // ---------------------------------------------------------------------------
 // K1 (screened): one block per work item = the significant radial functions
 // of one shell on the 128 points of one tile.  Rows are slots of the chunk's
-// compact [slot][128] arrays (slot - s0).
+// compact [slot][128] arrays (slot - s0); with pmax, the largest |phi| of
+// each point of the chunk (tile - t0) is max-reduced into it.
 // ---------------------------------------------------------------------------
 struct BasisItem {
   int tile;                 // global tile index
@@ -300,9 +304,10 @@ __global__ void __launch_bounds__(128) k_basis_items(const BasisItem* __restrict
                                                      const double* __restrict__ contr,
                                                      const int2* __restrict__ rng, DevSA sa,
                                                      const double* __restrict__ qx, const double* __restrict__ qy,
-                                                     const double* __restrict__ qz, int64_t s0,
+                                                     const double* __restrict__ qz, int64_t s0, int64_t t0,
                                                      double* __restrict__ phi, double* __restrict__ gx,
-                                                     double* __restrict__ gy, double* __restrict__ gz) {
+                                                     double* __restrict__ gy, double* __restrict__ gz,
+                                                     unsigned long long* __restrict__ pmax) {
   __shared__ ShellStage st;
   const BasisItem it = items[blockIdx.x];
   DevShell S = shells[it.shell];
@@ -311,8 +316,11 @@ __global__ void __launch_bounds__(128) k_basis_items(const BasisItem* __restrict
   const double x = qx[q] - atoms[3 * S.atom];
   const double y = qy[q] - atoms[3 * S.atom + 1];
   const double z = qz[q] - atoms[3 * S.atom + 2];
+  double vmax = 0.0;
   shell_at_point<L, GRAD>(S, sa, x, y, z, staged ? st.e : exps, staged ? st.n : norms, staged ? st.c : contr, st.r,
-                          true, it.mask, it.slot - s0, it.nsig, threadIdx.x, 128, phi, gx, gy, gz);
+                          true, it.mask, it.slot - s0, it.nsig, threadIdx.x, 128, phi, gx, gy, gz, vmax);
+  // largest |phi| of each point over the tile's functions (non-negative doubles order like their bits)
+  if (pmax) atomicMax(pmax + ((int64_t)it.tile - t0) * 128 + threadIdx.x, (unsigned long long)__double_as_longlong(vmax));
 }
 
 }  // namespace pgxc

@@ -60,6 +60,7 @@ struct ScreenPlan {
   double* pt = nullptr;      // 8 point arrays of chunk_tiles*128
   double* partial = nullptr;
   double* V = nullptr;       // [nbas][nbas]
+  unsigned long long* pmax = nullptr;  // [chunk_tiles*128] largest |phi| per point (INT8 path)
   ScreenMixed* mixed = nullptr;
   cudaEvent_t ev[10] = {};
   std::vector<void*> allocs;
@@ -683,6 +684,7 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
     mi.chunk_tiles = sp->chunk_tiles;
     mi.max_n = sp->max_n;
     mi.chunk_bstages = chunk_bstages;
+    SP_TRY(sp_alloc(sp, &sp->pmax, (size_t)sp->chunk_tiles * 128), "cudaMalloc");
     SP_TRY(sp_alloc(sp, &sp->b_off, boff.size()), "cudaMalloc");
     SP_TRY(cudaMemcpy(sp->b_off, boff.data(), sizeof(int64_t) * boff.size(), cudaMemcpyHostToDevice), "copy");
     mi.b_off = sp->b_off;
@@ -736,6 +738,7 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, cudaStream_t st, double* ham,
     const int64_t npt = nt * 128;
     SR_TRY(cudaEventRecord(ev[2], st));
     // K1
+    if (sp->pmax) SR_TRY(cudaMemsetAsync(sp->pmax, 0, sizeof(unsigned long long) * nt * 128, st));
     {
       auto launch_l = [&](auto Lc) {
         constexpr int L = decltype(Lc)::value;
@@ -744,11 +747,11 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, cudaStream_t st, double* ham,
         if (gga)
           k_basis_items<L, true><<<(unsigned)(i1 - i0), 128, 0, st>>>(
               sp->items[L] + i0, a.shells, a.atoms, a.exps, a.norms, a.contr, a.rng, a.sa, sp->qx, sp->qy, sp->qz, s0,
-              sp->phi, sp->gx, sp->gy, sp->gz);
+              t0, sp->phi, sp->gx, sp->gy, sp->gz, sp->pmax);
         else
           k_basis_items<L, false><<<(unsigned)(i1 - i0), 128, 0, st>>>(
               sp->items[L] + i0, a.shells, a.atoms, a.exps, a.norms, a.contr, a.rng, a.sa, sp->qx, sp->qy, sp->qz, s0,
-              sp->phi, nullptr, nullptr, nullptr);
+              t0, sp->phi, nullptr, nullptr, nullptr, sp->pmax);
         ++T.launches;
       };
       launch_l(std::integral_constant<int, 0>());
@@ -759,7 +762,7 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, cudaStream_t st, double* ham,
       if (gga) k_pad_zero<true><<<nb, 256, 0, st>>>(sp->slot_fn + s0, ns, sp->phi, sp->gx, sp->gy, sp->gz);
       else k_pad_zero<false><<<nb, 256, 0, st>>>(sp->slot_fn + s0, ns, sp->phi, nullptr, nullptr, nullptr);
       ++T.launches;
-      if (sp->mixed) T.launches += screen_mixed_basis(sp->mixed, sp->tso, t0, nt, s0, sp->phi, st);
+      if (sp->mixed) T.launches += screen_mixed_basis(sp->mixed, sp->tso, t0, nt, s0, sp->phi, sp->pmax, st);
     }
     SR_TRY(cudaEventRecord(ev[3], st));
     // K3

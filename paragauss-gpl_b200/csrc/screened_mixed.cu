@@ -116,24 +116,18 @@ __global__ void k_sm_quant_P(const double* __restrict__ P, int64_t ldc, int64_t 
 }
 
 // rows = the tile's 128 points, K = its slots; one scale per point (largest
-// |phi| over the tile's slots)
+// |phi| over the tile's slots, from pmax)
 __global__ void __launch_bounds__(128) k_sm_quant_pts(const int64_t* __restrict__ tso, int64_t t0, int64_t s0,
-                                                      const double* __restrict__ phi, int* __restrict__ e_pt,
-                                                      int8_t* __restrict__ tA) {
+                                                      const double* __restrict__ phi,
+                                                      const unsigned long long* __restrict__ pmax,
+                                                      int* __restrict__ e_pt, int8_t* __restrict__ tA) {
   const int64_t t = t0 + blockIdx.x;
   const int64_t sb = tso[t] - s0;
   const int n = (int)(tso[t + 1] - tso[t]);
   const int p = threadIdx.x;
   const double* src = phi + sb * 128 + p;
-  double m8[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-  for (int i = 0; i < n; i += 8) {  // n is a multiple of 32
-#pragma unroll
-    for (int j = 0; j < 8; ++j) m8[j] = fmax(m8[j], fabs(src[(int64_t)(i + j) * 128]));
-  }
-  double mx = 0.0;
-#pragma unroll
-  for (int j = 0; j < 8; ++j) mx = fmax(mx, m8[j]);
-  const int e = scale_exp(mx);
+  // largest |phi| of the point over the tile's slots, recorded by the basis kernel
+  const int e = scale_exp(__longlong_as_double((long long)pmax[(int64_t)blockIdx.x * 128 + p]));
   e_pt[(int64_t)blockIdx.x * 128 + p] = e;
   int8_t* dst = tA + sb * kDigBytesPerSlot;
   for (int kb = 0; kb < n / 32; ++kb) {
@@ -216,6 +210,7 @@ __global__ void __launch_bounds__(192) k_sm_gather_B(const int64_t* __restrict__
 // epilogue operands: phi (and grad phi) of 6 slots x 128 points per buffer
 constexpr int kECols = 6;
 constexpr int kERing = 4;
+constexpr int kEGroups = 24 / kECols;  // staged groups per column half of a slot block
 constexpr int kEBuf = 4 * kECols * 128;  // doubles
 struct DensSmem {
   alignas(1024) int8_t a[kDStages][kOpA];
@@ -299,25 +294,14 @@ __global__ void __launch_bounds__(kDensThreads, 1)
   const uint32_t tbase = S.tslot;
   bool ok = true;
   if (warp == 10) {
-    if (lane == 0) {  // epilogue operands: per slot block j, half h, group u: 6 slots of phi (grad phi)
+    if (lane == 0) {  // epilogue operands: per slot block j, half h, group u: kECols slots of phi (grad phi)
       int e = 0;
       for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
         const int64_t sb = tso[t0 + ti] - s0;
         const int n = (int)(tso[t0 + ti + 1] - tso[t0 + ti]);
         const int nN = (n + kN - 1) / kN;
         for (int j = 0; j < nN && ok; ++j) {
-          if (j + 1 < nN) {  // next block into L2
-            const int rows = min(kN, n - (j + 1) * kN);
-            const int64_t off = (sb + (int64_t)(j + 1) * kN) * 128;
-            const uint32_t bytes = (uint32_t)rows * 128 * sizeof(double);
-            tc::bulk_prefetch_l2(phi + off, bytes);
-            if (GGA) {
-              tc::bulk_prefetch_l2(gx + off, bytes);
-              tc::bulk_prefetch_l2(gy + off, bytes);
-              tc::bulk_prefetch_l2(gz + off, bytes);
-            }
-          }
-          for (int u = 0; u < 4 && ok; ++u)
+          for (int u = 0; u < kEGroups && ok; ++u)
             for (int h = 0; h < 2; ++h, ++e) {
               const int r = e % kERing;
               if (e >= kERing && !tc::mbar_wait(&S.e_empty[r], ((e / kERing) - 1) & 1)) {
@@ -421,8 +405,8 @@ __global__ void __launch_bounds__(kDensThreads, 1)
         tc::fence_before_sync();
         tc::mbar_arrive(&S.acc_empty[b]);
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int e = (jj * 4 + u) * 2 + half, r = e % kERing;
+        for (int u = 0; u < kEGroups; ++u) {
+          const int e = (jj * kEGroups + u) * 2 + half, r = e % kERing;
           if (!tc::mbar_wait(&S.e_full[r], (e / kERing) & 1)) {
             ok = false;
             break;
@@ -495,49 +479,57 @@ __global__ void __launch_bounds__(256, 2) k_sm_zquant(const int64_t* __restrict_
   const int p0 = lane * 4;
   const int kstep = lane >> 3, kin = (lane & 7) * 4;
   const int64_t tile_off = sb * kDigBytesPerSlot;
-  for (int i = warp; i < n; i += 8) {
-    const int64_t o = (sb + i) * 128 + p0;
-    double f[4], z[4];
-    {
+  // two slots per warp and iteration: the loads of both are in flight together
+  for (int i0 = warp; i0 < n; i0 += 16) {
+    double f[2][4], z[2][4];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int i = i0 + 8 * h;
+      const int64_t o = (sb + min(i, n - 1)) * 128 + p0;
       const double2 a = *reinterpret_cast<const double2*>(phi + o);
       const double2 b = *reinterpret_cast<const double2*>(phi + o + 2);
-      f[0] = a.x; f[1] = a.y; f[2] = b.x; f[3] = b.y;
-    }
+      f[h][0] = a.x; f[h][1] = a.y; f[h][2] = b.x; f[h][3] = b.y;
+      if (GGA) {
 #pragma unroll
-    for (int u = 0; u < 4; ++u) z[u] = sA[p0 + u] * f[u];
-    if (GGA) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const double* g = c == 0 ? gx : (c == 1 ? gy : gz);
-        const double2 a = *reinterpret_cast<const double2*>(g + o);
-        const double2 b = *reinterpret_cast<const double2*>(g + o + 2);
-        z[0] += sB[c][p0] * a.x;
-        z[1] += sB[c][p0 + 1] * a.y;
-        z[2] += sB[c][p0 + 2] * b.x;
-        z[3] += sB[c][p0 + 3] * b.y;
+        for (int c = 0; c < 3; ++c) {
+          const double* g = c == 0 ? gx : (c == 1 ? gy : gz);
+          const double2 ga = *reinterpret_cast<const double2*>(g + o);
+          const double2 gb = *reinterpret_cast<const double2*>(g + o + 2);
+          z[h][0] = (c == 0 ? 0.0 : z[h][0]) + sB[c][p0] * ga.x;
+          z[h][1] = (c == 0 ? 0.0 : z[h][1]) + sB[c][p0 + 1] * ga.y;
+          z[h][2] = (c == 0 ? 0.0 : z[h][2]) + sB[c][p0 + 2] * gb.x;
+          z[h][3] = (c == 0 ? 0.0 : z[h][3]) + sB[c][p0 + 3] * gb.y;
+        }
       }
     }
-    const double mz = warp_max(fmax(fmax(fabs(z[0]), fabs(z[1])), fmax(fabs(z[2]), fabs(z[3]))));
-    const double mf = warp_max(fmax(fmax(fabs(f[0]), fabs(f[1])), fmax(fabs(f[2]), fabs(f[3]))));
-    const int ez = scale_exp(mz), ef = scale_exp(mf);
-    if (lane == 0) {
-      zs[sb + i] = pow2(ez);
-      fs[sb + i] = pow2(ef + kCombShift);
-    }
-    long long qz[4], qf[4];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      qz[u] = oz_int(z[u], ez);
-      qf[u] = oz_int(f[u], ef);
-    }
-    uint32_t wz[kSlices], wf[kSlices];
-    oz_pack4(qz, wz);
-    oz_pack4(qf, wf);
+    for (int h = 0; h < 2; ++h) {
+      const int i = i0 + 8 * h;
+      if (i >= n) break;
 #pragma unroll
-    for (int sl = 0; sl < kSlices; ++sl) {
+      for (int u = 0; u < 4; ++u) z[h][u] = GGA ? z[h][u] + sA[p0 + u] * f[h][u] : sA[p0 + u] * f[h][u];
+      const double mz = warp_max(fmax(fmax(fabs(z[h][0]), fabs(z[h][1])), fmax(fabs(z[h][2]), fabs(z[h][3]))));
+      const double mf = warp_max(fmax(fmax(fabs(f[h][0]), fabs(f[h][1])), fmax(fabs(f[h][2]), fabs(f[h][3]))));
+      const int ez = scale_exp(mz), ef = scale_exp(mf);
+      if (lane == 0) {
+        zs[sb + i] = pow2(ez);
+        fs[sb + i] = pow2(ef + kCombShift);
+      }
+      long long qz[4], qf[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        qz[u] = oz_int(z[h][u], ez);
+        qf[u] = oz_int(f[h][u], ef);
+      }
+      uint32_t wz[kSlices], wf[kSlices];
+      oz_pack4(qz, wz);
+      oz_pack4(qf, wf);
       const int64_t kb = tile_off + (int64_t)kstep * n * (32 * kSlices);
-      *reinterpret_cast<uint32_t*>(tF + kb + ilv_off(i, kin, sl)) = wf[sl];
-      *reinterpret_cast<uint32_t*>(tZ + kb + (int64_t)sl * n * 32 + blk_off(i, kin)) = wz[sl];
+#pragma unroll
+      for (int sl = 0; sl < kSlices; ++sl) {
+        *reinterpret_cast<uint32_t*>(tF + kb + ilv_off(i, kin, sl)) = wf[sl];
+        *reinterpret_cast<uint32_t*>(tZ + kb + (int64_t)sl * n * 32 + blk_off(i, kin)) = wz[sl];
+      }
     }
   }
 }
@@ -788,8 +780,8 @@ int screen_mixed_prepare(ScreenMixed* m, const BuildArgs& a, cudaStream_t st) {
 }
 
 int screen_mixed_basis(ScreenMixed* m, const int64_t* tso, int64_t t0, int64_t nt, int64_t s0, const double* phi,
-                       cudaStream_t st) {
-  k_sm_quant_pts<<<(unsigned)nt, 128, 0, st>>>(tso, t0, s0, phi, m->e_pt, m->tA);
+                       const unsigned long long* pmax, cudaStream_t st) {
+  k_sm_quant_pts<<<(unsigned)nt, 128, 0, st>>>(tso, t0, s0, phi, pmax, m->e_pt, m->tA);
   return 1;
 }
 
