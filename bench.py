@@ -13,9 +13,10 @@ one full XC build (basis, density, functional, V_xc) over the whole grid.
 
 `--impl reference` times the CPU path of the reference algorithm instead
 (the FP64 oracle port, all host threads, bounded sample per step).
-With torchrun (N > 1) the grid is split into contiguous point ranges, one per
-GPU, and the packed V_xc plus {E_xc, N_el} are summed with an NCCL
-all-reduce: the reduction ParaGauss does with MPI_Reduce in xc_sndrcv.
+With torchrun (N > 1) the grid is split into spatially compact blocks (Morton
+order, whole 128-point tiles), one per GPU, and [packed V_xc, E_xc, N_el] is
+summed with one NCCL all-reduce per build: the reduction ParaGauss does with
+MPI_Reduce in xc_sndrcv.
 """
 import argparse
 import json
@@ -145,20 +146,11 @@ def fp64_peak_tflops(torch):
 
 
 def shard(case, rank, world):
-    """Contiguous 64-aligned point range of this rank (xc_sndrcv partition analogue)."""
+    """This rank's spatially compact block of the grid (pgxc.dist)."""
     if world == 1:
         return case
-    from pgxc import cases as C
-    n = case.npts
-    per = -(-n // world)
-    per = -(-per // 64) * 64
-    lo, hi = min(rank * per, n), min((rank + 1) * per, n)
-    sub = C.Case(**{**case.__dict__})
-    sub.grid_xyz = case.grid_xyz[lo:hi]
-    sub.grid_wraw = case.grid_wraw[lo:hi]
-    sub.point_atom = case.point_atom[lo:hi]
-    sub.grid_w = None if case.grid_w is None else case.grid_w[lo:hi]
-    return sub
+    from pgxc import dist as D
+    return D.shard_case(case, D.spatial_shards(case.grid_xyz, world)[rank])
 
 
 def algorithmic_flops(case):
@@ -316,17 +308,15 @@ def main():
     nb, nocc = case.nbas, case.nocc
     dC = torch.from_numpy(case.c_fortran()).cuda()
     docc = torch.from_numpy(case.occ_fortran()).cuda()
-    dham = torch.zeros(case.xc_length, dtype=torch.float64, device="cuda")
-    dsum = torch.zeros(2, dtype=torch.float64, device="cuda")
+    # [packed V, E_xc, N_el]: one all-reduce per build over NCCL (xc_sndrcv)
+    dbuf = torch.zeros(case.xc_length + 2, dtype=torch.float64, device="cuda")
+    dham, dsum = dbuf[:-2], dbuf[-2:]
     last_tm = {}
 
     def step():
-        dham.zero_()
-        dsum.zero_()
         last_tm.update(ctx.build_device(dC.data_ptr(), docc.data_ptr(), dham.data_ptr(), dsum.data_ptr()))
         if world > 1:
-            dist.all_reduce(dham)
-            dist.all_reduce(dsum)
+            dist.all_reduce(dbuf)
 
     for _ in range(max(args.warmup, 3)):
         step()
@@ -353,9 +343,9 @@ def main():
         ham_host[:] = 0.0
         h, e, q = ctx.build(C=C_host.numpy(), occ=occ_host.numpy(), ham=ham_host)
         if world > 1:
-            th = torch.from_numpy(h).cuda()
-            dist.all_reduce(th)
-            h[:] = th.cpu().numpy()
+            tb = torch.from_numpy(np.concatenate([h, [e, q]])).cuda()
+            dist.all_reduce(tb)
+            h[:] = tb[:-2].cpu().numpy()
         return e
 
     for _ in range(2):
@@ -426,7 +416,8 @@ def main():
                                      f"{screen['nlisted'] / screen['ntiles']:.1f} listed functions per tile "
                                      f"of {case.nbas}, {screen['sum_n2'] / (screen['ntiles'] * case.nbas ** 2):.3f} "
                                      f"of the dense n^2 work"),
-                       "parallelism": f"grid split over {world} GPU(s), NCCL all-reduce of packed V_xc",
+                       "parallelism": (f"grid split over {world} GPU(s) in Morton blocks of 128-point tiles, "
+                                       "one NCCL all-reduce of [packed V_xc, E_xc, N_el] per build"),
                        "l2": "no flush: each build streams several GB of basis/Z data (inputs larger than L2)"},
             "xc_builds_per_s": 1e3 / per_step, "E_xc": exc, "N_el": nel,
             "vs_fp64": None if fp64_leg is None else {

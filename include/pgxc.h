@@ -49,9 +49,10 @@ extern "C" {
 
 /* ---- precision modes ------------------------------------------------- */
 #define PGXC_PREC_FP64        0  /* FP64 everywhere (FP64 tensor pipe): the drop-in */
-/* FP32 basis; both contractions on the INT8 tensor cores with an Ozaki split
-   (4 signed 7-bit digits per operand, exact INT32 accumulation); FP64
-   functional and grid sums */
+/* Both contractions (X = phi P and V = Z^T phi) on the INT8 tensor cores
+   with an Ozaki split: 5 balanced 7-bit digits per FP64 operand, the 15
+   digit pairs of weight >= 2^-34, exact INT32 accumulation, one FP64
+   combination; basis, functional, grid sums and V_xc stay FP64 */
 #define PGXC_PREC_MIXED_INT8  1
 
 /* Geometry: unique_atoms(:)%position(1:3,1) in bohr, atom-major xyz triplets. */

@@ -1,6 +1,6 @@
-// mixed.h -- the mixed-precision path of the XC build: FP32 basis, both
-// contractions on the INT8 tensor cores (Ozaki split, exact integer
-// accumulation), FP64 functional and sums.
+// mixed.h -- the dense-layout INT8 build: FP64 basis, both contractions on
+// the INT8 tensor cores (Ozaki split, exact integer accumulation), FP64
+// functional and sums.
 #pragma once
 
 #include <cstdint>

@@ -1,6 +1,6 @@
-"""Mixed-precision GPU path (FP32 basis, Ozaki-split INT8 tcgen05
-contractions with exact integer accumulation, FP64 functional and sums)
-against the FP64 CPU oracle.
+"""INT8 ("mixed") GPU builds, dense and screened (FP64 basis, Ozaki-split
+INT8 tcgen05 contractions with exact integer accumulation, FP64 functional
+and sums) against the FP64 CPU oracle.
 
 Bar: |dE_xc| < 1e-7 Eh, |dN_el| < 1e-7 and every V_xc element within 1e-7
 (the mixed-mode targets are 1e-6 Eh on E_xc and 1e-7 on V_xc).
