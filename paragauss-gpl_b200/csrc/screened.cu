@@ -7,7 +7,7 @@
 //                     basis work items (tile, shell, radial mask) and chunks.
 // Per build (screen_run), per chunk of tiles:
 //   k_basis_items     phi, grad phi of listed functions only     [K1]
-//   k_pad_zero        zero rows of padding slots
+//   k_pad_zero        zero the padding slots at the end of each tile's list
 //   k_sdensity        X = phi_t P[S_t, S_t] on DMMA, P gathered by cp.async,
 //                     fused rho, grad rho                          [K3]
 //   k_functional      (kernels_fp64.cu)                            [K2]
@@ -48,6 +48,7 @@ struct ScreenPlan {
   int64_t* tso = nullptr;   // [ntiles+1] first slot of each tile
   int* slot_fn = nullptr;   // [nslots] function of each slot, -1 for padding
   int* slot_tile = nullptr; // [nslots]
+  int* listed = nullptr;    // [ntiles] listed (not padding) slots of each tile
   int64_t* b_off = nullptr;  // [ntiles+1] first density B stage of each tile (INT8 path)
   BasisItem* items[kMaxL + 1] = {};
   // host copies of the partition
@@ -122,12 +123,16 @@ __global__ void __launch_bounds__(128) k_tile_atom_d2(const double* __restrict__
 // ---------------------------------------------------------------------------
 // FP64 kernels
 // ---------------------------------------------------------------------------
+// Zero the padding slots of each tile (the slots after its listed
+// functions: tso[t] + listed[t] .. tso[t+1]).  grid = chunk tiles.
 template <bool GGA>
-__global__ void k_pad_zero(const int* __restrict__ slot_fn, int64_t nslots, double* __restrict__ phi,
-                           double* __restrict__ gx, double* __restrict__ gy, double* __restrict__ gz) {
-  const int64_t total = nslots * 128;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (int64_t)gridDim.x * blockDim.x) {
-    if (slot_fn[e >> 7] >= 0) continue;
+__global__ void __launch_bounds__(128) k_pad_zero(const int64_t* __restrict__ tso, const int* __restrict__ listed,
+                                                  int64_t t0, int64_t s0, double* __restrict__ phi,
+                                                  double* __restrict__ gx, double* __restrict__ gy,
+                                                  double* __restrict__ gz) {
+  const int64_t t = t0 + blockIdx.x;
+  const int64_t r0 = tso[t] - s0 + listed[t], r1 = tso[t + 1] - s0;
+  for (int64_t e = r0 * 128 + threadIdx.x; e < r1 * 128; e += 128) {
     phi[e] = 0.0;
     if (GGA) {
       gx[e] = 0.0;
@@ -339,19 +344,21 @@ __global__ void __launch_bounds__(kGemmThreads) k_svpot(const double* __restrict
     pair_of(q, nb, GGA, I, J);
     Acc acc;
     acc.zero();
-    gemm_tile<true, true>(acc, Z + sb * 128, 128, (int64_t)I * 64, phi + sb * 128, 128, (int64_t)J * 64, 0, 128,
+    // acc[j][i] = sum_p phi_j Z_i: rows of the fragment run along j, so the
+    // atomics of a warp instruction hit 4 rows of V in runs of 8 functions
+    gemm_tile<true, true>(acc, phi + sb * 128, 128, (int64_t)J * 64, Z + sb * 128, 128, (int64_t)I * 64, 0, 128,
                           smem);
 #pragma unroll
-    for (int ii = 0; ii < 4; ++ii) {
-      const int i = I * 64 + wm0 + ii * 8 + (lane >> 2);
-      const int fi = i < n ? sfn[i] : -1;
+    for (int jj = 0; jj < 4; ++jj) {
+      const int j = J * 64 + wm0 + jj * 8 + (lane >> 2);
+      const int fj = j < n ? sfn[j] : -1;
 #pragma unroll
-      for (int jj = 0; jj < 4; ++jj)
+      for (int ii = 0; ii < 4; ++ii)
 #pragma unroll
         for (int e = 0; e < 2; ++e) {
-          const int j = J * 64 + wn0 + jj * 8 + 2 * (lane & 3) + e;
-          const int fj = j < n ? sfn[j] : -1;
-          if (fi >= 0 && fj >= 0 && (GGA || fj >= fi)) atomicAdd(V + (int64_t)fi * ldv + fj, acc.v[ii][jj][e]);
+          const int i = I * 64 + wn0 + ii * 8 + 2 * (lane & 3) + e;
+          const int fi = i < n ? sfn[i] : -1;
+          if (fi >= 0 && fj >= 0 && (GGA || fj >= fi)) atomicAdd(V + (int64_t)fi * ldv + fj, acc.v[jj][ii][e]);
         }
     }
   }
@@ -559,7 +566,7 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
   }
   // --- per-tile lists --------------------------------------------------------
   std::vector<int64_t> tso((size_t)ntiles + 1, 0);
-  std::vector<int> slot_fn, slot_tile;
+  std::vector<int> slot_fn, slot_tile, listed_t((size_t)ntiles, 0);
   std::vector<BasisItem> items[kMaxL + 1];
   std::vector<int64_t> tile_items[kMaxL + 1];  // items before tile t, per L
   for (int l = 0; l <= kMaxL; ++l) tile_items[l].assign((size_t)ntiles + 1, 0);
@@ -587,6 +594,7 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
           if (mask >> rr & 1) slot_fn.push_back(S.f0 + i * S.nrad + rr);
     }
     const int64_t listed = (int64_t)slot_fn.size() - base;
+    listed_t[(size_t)t] = (int)listed;
     sp->nlisted += listed;
     while (((int64_t)slot_fn.size() - base) % kSlotAlign) slot_fn.push_back(-1);
     const int64_t nt = (int64_t)slot_fn.size() - base;
@@ -645,6 +653,8 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
   // --- device copies and buffers ------------------------------------------------
   SP_TRY(sp_alloc(sp, &sp->tso, tso.size()), "cudaMalloc");
   SP_TRY(cudaMemcpy(sp->tso, tso.data(), sizeof(int64_t) * tso.size(), cudaMemcpyHostToDevice), "copy");
+  SP_TRY(sp_alloc(sp, &sp->listed, listed_t.size()), "cudaMalloc");
+  SP_TRY(cudaMemcpy(sp->listed, listed_t.data(), sizeof(int) * listed_t.size(), cudaMemcpyHostToDevice), "copy");
   SP_TRY(sp_alloc(sp, &sp->slot_fn, slot_fn.size()), "cudaMalloc");
   SP_TRY(sp_alloc(sp, &sp->slot_tile, slot_tile.size()), "cudaMalloc");
   if (!slot_fn.empty()) {
@@ -758,9 +768,8 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, cudaStream_t st, double* ham,
       launch_l(std::integral_constant<int, 1>());
       launch_l(std::integral_constant<int, 2>());
       launch_l(std::integral_constant<int, 3>());
-      const unsigned nb = (unsigned)std::max<int64_t>(1, std::min<int64_t>((ns * 128 + 255) / 256, 148 * 32));
-      if (gga) k_pad_zero<true><<<nb, 256, 0, st>>>(sp->slot_fn + s0, ns, sp->phi, sp->gx, sp->gy, sp->gz);
-      else k_pad_zero<false><<<nb, 256, 0, st>>>(sp->slot_fn + s0, ns, sp->phi, nullptr, nullptr, nullptr);
+      if (gga) k_pad_zero<true><<<(unsigned)nt, 128, 0, st>>>(sp->tso, sp->listed, t0, s0, sp->phi, sp->gx, sp->gy, sp->gz);
+      else k_pad_zero<false><<<(unsigned)nt, 128, 0, st>>>(sp->tso, sp->listed, t0, s0, sp->phi, nullptr, nullptr, nullptr);
       ++T.launches;
       if (sp->mixed) T.launches += screen_mixed_basis(sp->mixed, sp->tso, t0, nt, s0, sp->phi, sp->pmax, st);
     }

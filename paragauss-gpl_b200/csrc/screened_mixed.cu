@@ -166,6 +166,7 @@ __device__ __forceinline__ unsigned long long gather_slice(const unsigned long l
 // the K-major MMA layout, stored at stage b_off[t] + j nK + k; rows past the
 // tile's slots are zero.  One block per tile, thread = (row, 8 K values).
 // ---------------------------------------------------------------------------
+constexpr int kGatherSplit = 4;  // blocks per tile: block y takes the slot blocks j = y, y + 4, ...
 __global__ void __launch_bounds__(192) k_sm_gather_B(const int64_t* __restrict__ tso,
                                                     const int* __restrict__ slot_fn,
                                                     const int64_t* __restrict__ b_off, int64_t t0, int64_t s0,
@@ -179,27 +180,34 @@ __global__ void __launch_bounds__(192) k_sm_gather_B(const int64_t* __restrict__
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
     const int f = slot_fn[sg + i];
     sfn[i] = f;
-    ps[sg - s0 + i] = f >= 0 ? pow2(e_P[f]) : 0.0;  // the row scale of P for the density epilogue
+    if (blockIdx.y == 0) ps[sg - s0 + i] = f >= 0 ? pow2(e_P[f]) : 0.0;  // P's row scale for the density epilogue
   }
   __syncthreads();
   const int nK = n / 32, nN = (n + kN - 1) / kN;
   const int r = threadIdx.x >> 2, grp = threadIdx.x & 3;
   int8_t* out = tB + (b_off[t] - b_off[t0]) * kOpB;
-  for (int j = 0; j < nN; ++j) {
+  for (int j = blockIdx.y; j < nN; j += kGatherSplit) {
     const int nu = j * kN + r;
     const int fnv = nu < n ? sfn[nu] : -1;
     const unsigned long long* prow = P8 + (int64_t)max(fnv, 0) * nbas;
-    for (int k = 0; k < nK; ++k) {
-      unsigned long long w[8];
+    for (int k = 0; k < nK; k += 2) {  // two K steps per pass: 16 loads in flight (nK is even or ends the loop)
+      unsigned long long w[2][8];
 #pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        const int fmu = sfn[k * 32 + grp * 8 + u];
-        w[u] = (fnv >= 0 && fmu >= 0) ? __ldg(prow + fmu) : 0ull;
+      for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int kk = min(k + h, nK - 1);
+          const int fmu = sfn[kk * 32 + grp * 8 + u];
+          w[h][u] = (fnv >= 0 && fmu >= 0) ? __ldg(prow + fmu) : 0ull;
+        }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (k + h >= nK) break;
+        int8_t* o = out + (int64_t)(j * nK + k + h) * kOpB;
+#pragma unroll
+        for (int sl = 0; sl < kSlices; ++sl)
+          *reinterpret_cast<unsigned long long*>(o + sl * kBlkB + blk_off(r, grp * 8)) = gather_slice(w[h], sl);
       }
-      int8_t* o = out + (int64_t)(j * nK + k) * kOpB;
-#pragma unroll
-      for (int sl = 0; sl < kSlices; ++sl)
-        *reinterpret_cast<unsigned long long*>(o + sl * kBlkB + blk_off(r, grp * 8)) = gather_slice(w, sl);
     }
   }
 }
@@ -794,8 +802,8 @@ int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn,
     cudaMemsetAsync(gry, 0, sizeof(double) * nt * 128, st);
     cudaMemsetAsync(grz, 0, sizeof(double) * nt * 128, st);
   }
-  k_sm_gather_B<<<(unsigned)nt, 192, 4 * m->max_n, st>>>(tso, slot_fn, m->b_off, t0, s0, m->P8, m->e_P, m->nbas,
-                                                         m->tB, m->ps);
+  k_sm_gather_B<<<dim3((unsigned)nt, kGatherSplit), 192, 4 * m->max_n, st>>>(tso, slot_fn, m->b_off, t0, s0, m->P8,
+                                                                             m->e_P, m->nbas, m->tB, m->ps);
   const unsigned grid = (unsigned)std::min<int64_t>(nt, m->nsm);
   const int smem = (int)sizeof(DensSmem);
   if (m->gga)
