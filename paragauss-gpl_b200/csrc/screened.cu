@@ -771,7 +771,8 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, cudaStream_t st, double* ham,
       if (gga) k_pad_zero<true><<<(unsigned)nt, 128, 0, st>>>(sp->tso, sp->listed, t0, s0, sp->phi, sp->gx, sp->gy, sp->gz);
       else k_pad_zero<false><<<(unsigned)nt, 128, 0, st>>>(sp->tso, sp->listed, t0, s0, sp->phi, nullptr, nullptr, nullptr);
       ++T.launches;
-      if (sp->mixed) T.launches += screen_mixed_basis(sp->mixed, sp->tso, t0, nt, s0, sp->phi, sp->pmax, st);
+      if (sp->mixed)
+        T.launches += screen_mixed_basis(sp->mixed, sp->tso, sp->slot_fn, t0, nt, s0, sp->phi, sp->pmax, st);
     }
     SR_TRY(cudaEventRecord(ev[3], st));
     // K3

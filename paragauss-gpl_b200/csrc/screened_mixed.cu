@@ -787,10 +787,12 @@ int screen_mixed_prepare(ScreenMixed* m, const BuildArgs& a, cudaStream_t st) {
   return 2;
 }
 
-int screen_mixed_basis(ScreenMixed* m, const int64_t* tso, int64_t t0, int64_t nt, int64_t s0, const double* phi,
-                       const unsigned long long* pmax, cudaStream_t st) {
+int screen_mixed_basis(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
+                       const double* phi, const unsigned long long* pmax, cudaStream_t st) {
   k_sm_quant_pts<<<(unsigned)nt, 128, 0, st>>>(tso, t0, s0, phi, pmax, m->e_pt, m->tA);
-  return 1;
+  k_sm_gather_B<<<dim3((unsigned)nt, kGatherSplit), 192, 4 * m->max_n, st>>>(tso, slot_fn, m->b_off, t0, s0, m->P8,
+                                                                             m->e_P, m->nbas, m->tB, m->ps);
+  return 2;
 }
 
 int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
@@ -802,8 +804,6 @@ int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn,
     cudaMemsetAsync(gry, 0, sizeof(double) * nt * 128, st);
     cudaMemsetAsync(grz, 0, sizeof(double) * nt * 128, st);
   }
-  k_sm_gather_B<<<dim3((unsigned)nt, kGatherSplit), 192, 4 * m->max_n, st>>>(tso, slot_fn, m->b_off, t0, s0, m->P8,
-                                                                             m->e_P, m->nbas, m->tB, m->ps);
   const unsigned grid = (unsigned)std::min<int64_t>(nt, m->nsm);
   const int smem = (int)sizeof(DensSmem);
   if (m->gga)
@@ -813,7 +813,7 @@ int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn,
     k_sm_density<false><<<grid, kDensThreads, smem, st>>>(tso, slot_fn, t0, nt, s0, m->tA, m->e_pt, m->tB, m->b_off,
                                                           m->ps, phi, nullptr, nullptr, nullptr, rho, nullptr,
                                                           nullptr, nullptr, m->err);
-  return 2;
+  return 1;
 }
 
 int screen_mixed_potential(ScreenMixed* m, const int64_t* tso, const int* slot_fn, const int* slot_tile, int64_t t0,

@@ -33,10 +33,11 @@ int screen_mixed_create(ScreenMixed** out, const ScreenMixedInput& in, std::stri
 void screen_mixed_destroy(ScreenMixed* m);
 // INT8 digits of the FP64 density matrix a.P (per-row scales); returns launches
 int screen_mixed_prepare(ScreenMixed* m, const BuildArgs& a, cudaStream_t st);
-// INT8 digits of phi for the density contraction; per-point scales from
-// pmax (the bit patterns of the largest |phi| of each point of the chunk)
-int screen_mixed_basis(ScreenMixed* m, const int64_t* tso, int64_t t0, int64_t nt, int64_t s0, const double* phi,
-                       const unsigned long long* pmax, cudaStream_t st);
+// Operands of the density contraction: INT8 digits of phi (per-point scales
+// from pmax, the bit patterns of the largest |phi| of each point of the
+// chunk) and the gathered digits of P[S_t, S_t] of every tile
+int screen_mixed_basis(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
+                       const double* phi, const unsigned long long* pmax, cudaStream_t st);
 int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
                          const double* phi, const double* gx, const double* gy, const double* gz, double* rho,
                          double* grx, double* gry, double* grz, cudaStream_t st);
