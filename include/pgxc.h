@@ -106,7 +106,8 @@ typedef struct pgxc_grid {
 
 typedef struct pgxc_options {
   int32_t functional;            /* PGXC_XC_VWN | PGXC_XC_PBE               */
-  int32_t ispin;                 /* 1 or 2                                  */
+  int32_t ispin;                 /* 1 or 2; 2 (open shell) needs screen_threshold >= 0,
+                                  * the dense layout returns PGXC_ENOTSUP */
   int32_t precision;             /* PGXC_PREC_*                             */
   int32_t batch_points;          /* points per tile, 0 -> 128 (machineparameters_veclen); only 128 */
   double  screen_threshold;      /* per-tile screening of basis functions:

@@ -72,13 +72,16 @@ void launch_basis_points_f64(const BuildArgs& a, const double* px, const double*
 void launch_pmat_f64(const BuildArgs& a, int64_t kpad, cudaStream_t st);
 void launch_density_f64(const BuildArgs& a, bool gga, cudaStream_t st);
 void launch_functional_f64(const BuildArgs& a, int64_t p0, int64_t nvalid, bool gga, cudaStream_t st);
+// open shell: pa / pb = 8 point columns of ld per spin (rho, grad rho, A, B)
+void launch_functional2_f64(const XcConst& K, const double* w, double* pa, double* pb, int64_t ld, int64_t p0,
+                            int64_t nvalid, bool gga, double* partial, double* acc, cudaStream_t st);
 void launch_zbuild_f64(const BuildArgs& a, bool gga, cudaStream_t st);
 void launch_vpot_f64(const BuildArgs& a, bool gga, cudaStream_t st);
 void launch_pack(const BuildArgs& a, int64_t nbas, int ispin, int spin, double* ham, cudaStream_t st);
 
 // point-wise functional and Becke weights (standalone entry points)
-void launch_xc_points(int functional, int64_t n, const double* rho, const double* gam, double* f, double* fr,
-                      double* fg, cudaStream_t st);
+void launch_xc_points(int functional, int ispin, int64_t n, const double* rho, const double* gam, double* f,
+                      double* fr, double* fg, cudaStream_t st);
 void launch_becke(const double* atoms, double* dist, int natm, const double* px, const double* py, const double* pz,
                   const int* owner, int64_t n, double* w, cudaStream_t st);
 // message returned by pgxc_last_error(NULL)

@@ -104,9 +104,35 @@ __global__ void k_xc_points(XcConst K, int functional, int64_t n, const double* 
   }
 }
 
-void launch_xc_points(int functional, int64_t n, const double* rho, const double* gam, double* f, double* fr,
-                      double* fg, cudaStream_t st) {
-  k_xc_points<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(make_xc_const(), functional, n, rho, gam, f, fr, fg);
+// open shell: rho (n, 2), gam (n, 3) = (aa, bb, ab), fr (n, 2), fg (n, 3), column-major
+template <bool GGA>
+__global__ void k_xc_points2(XcConst K, int64_t n, const double* __restrict__ rho, const double* __restrict__ gam,
+                             double* __restrict__ f, double* __restrict__ fr, double* __restrict__ fg) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const double r[2] = {rho[p], rho[p + n]};
+  const double g[3] = {GGA ? gam[p] : 0.0, GGA ? gam[p + n] : 0.0, GGA ? gam[p + 2 * n] : 0.0};
+  double F, Fr[2], Fg[3];
+  xc_open<GGA>(K, r, g, F, Fr, Fg);
+  f[p] = F;
+  fr[p] = Fr[0];
+  fr[p + n] = Fr[1];
+  if (GGA) {
+    fg[p] = Fg[0];
+    fg[p + n] = Fg[1];
+    fg[p + 2 * n] = Fg[2];
+  }
+}
+
+void launch_xc_points(int functional, int ispin, int64_t n, const double* rho, const double* gam, double* f,
+                      double* fr, double* fg, cudaStream_t st) {
+  const unsigned nb = (unsigned)((n + 255) / 256);
+  if (ispin == 1)
+    k_xc_points<<<nb, 256, 0, st>>>(make_xc_const(), functional, n, rho, gam, f, fr, fg);
+  else if (functional == PGXC_XC_PBE)
+    k_xc_points2<true><<<nb, 256, 0, st>>>(make_xc_const(), n, rho, gam, f, fr, fg);
+  else
+    k_xc_points2<false><<<nb, 256, 0, st>>>(make_xc_const(), n, rho, gam, f, fr, fg);
 }
 
 }  // namespace pgxc

@@ -270,6 +270,72 @@ __global__ void k_sum_partials(const double* __restrict__ partial, int nblocks, 
   }
 }
 
+// Open shell (ispin = 2).  pa / pb hold the point arrays of spin a / b, each
+// as 8 columns of ld: rho, grad rho (x, y, z), A, B (x, y, z).  Per spin s,
+// A_s = w df/drho_s (VWN) or w df/drho_s / 2 (PBE) and
+// B_s = w (2 df/dgamma_ss grad rho_s + df/dgamma_ab grad rho_s')
+// (modules/xc_hamiltonian.f90:1429-1446); partials of w f and w (rho_a + rho_b).
+template <bool GGA>
+__global__ void __launch_bounds__(256) k_functional2(XcConst K, int64_t p0, int64_t nvalid, int64_t n,
+                                                     const double* __restrict__ w, double* __restrict__ pa,
+                                                     double* __restrict__ pb, int64_t ld,
+                                                     double* __restrict__ partial) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0.0, q = 0.0;
+  if (p < n) {
+    const double wt = (p < nvalid) ? w[p0 + p] : 0.0;
+    const double rho[2] = {fmax(pa[p], 0.0), fmax(pb[p], 0.0)};
+    double ga[3] = {0, 0, 0}, gb[3] = {0, 0, 0}, gam[3] = {0, 0, 0};
+    if (GGA) {
+      for (int c = 0; c < 3; ++c) {
+        ga[c] = pa[(1 + c) * ld + p];
+        gb[c] = pb[(1 + c) * ld + p];
+      }
+      gam[0] = ga[0] * ga[0] + ga[1] * ga[1] + ga[2] * ga[2];
+      gam[1] = gb[0] * gb[0] + gb[1] * gb[1] + gb[2] * gb[2];
+      gam[2] = ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2];
+    }
+    double f, fr[2], fg[3];
+    xc_open<GGA>(K, rho, gam, f, fr, fg);
+    if (GGA) {
+      pa[4 * ld + p] = 0.5 * fr[0] * wt;
+      pb[4 * ld + p] = 0.5 * fr[1] * wt;
+      for (int c = 0; c < 3; ++c) {
+        pa[(5 + c) * ld + p] = wt * (2.0 * fg[0] * ga[c] + fg[2] * gb[c]);
+        pb[(5 + c) * ld + p] = wt * (2.0 * fg[1] * gb[c] + fg[2] * ga[c]);
+      }
+    } else {
+      pa[4 * ld + p] = fr[0] * wt;
+      pb[4 * ld + p] = fr[1] * wt;
+    }
+    e = f * wt;
+    q = (rho[0] + rho[1]) * wt;
+  }
+  __shared__ double se[256], sq[256];
+  se[threadIdx.x] = e;
+  sq[threadIdx.x] = q;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      se[threadIdx.x] += se[threadIdx.x + s];
+      sq[threadIdx.x] += sq[threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    partial[2 * blockIdx.x] = se[0];
+    partial[2 * blockIdx.x + 1] = sq[0];
+  }
+}
+
+void launch_functional2_f64(const XcConst& K, const double* w, double* pa, double* pb, int64_t ld, int64_t p0,
+                            int64_t nvalid, bool gga, double* partial, double* acc, cudaStream_t st) {
+  const unsigned nb = (unsigned)((ld + 255) / 256);
+  if (gga) k_functional2<true><<<nb, 256, 0, st>>>(K, p0, nvalid, ld, w, pa, pb, ld, partial);
+  else k_functional2<false><<<nb, 256, 0, st>>>(K, p0, nvalid, ld, w, pa, pb, ld, partial);
+  k_sum_partials<<<1, 256, 0, st>>>(partial, (int)nb, acc);
+}
+
 void launch_functional_f64(const BuildArgs& a, int64_t p0, int64_t nvalid, bool gga, cudaStream_t st) {
   const unsigned nb = (unsigned)((a.ldp + 255) / 256);
   if (gga)

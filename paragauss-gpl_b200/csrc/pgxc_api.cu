@@ -38,6 +38,10 @@ struct pgxc_ctx {
   // device buffers not in BuildArgs
   double* d_ham = nullptr;
   double* d_dist = nullptr;
+  // open shell: the second spin's orbitals, occupations and density matrix
+  double* C2 = nullptr;
+  double* occ2 = nullptr;
+  double* P2 = nullptr;
   int nocc_cap = 0;
   int64_t chunk = 0;
   double* h_ham = nullptr;      // pinned staging for the packed matrix
@@ -233,7 +237,8 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
   if (o.functional != PGXC_XC_VWN && o.functional != PGXC_XC_PBE)
     return fail(set_err(c, PGXC_EINVAL, "unknown functional id"));
   if (o.ispin != 1 && o.ispin != 2) return fail(set_err(c, PGXC_EINVAL, "ispin must be 1 or 2"));
-  if (o.ispin == 2) return fail(set_err(c, PGXC_ENOTSUP, "open-shell (ispin=2) builds are not implemented yet"));
+  if (o.ispin == 2 && !(o.screen_threshold >= 0.0))
+    return fail(set_err(c, PGXC_ENOTSUP, "open-shell (ispin=2) builds need the screened layout (screen_threshold >= 0)"));
   if (o.precision != PGXC_PREC_FP64 && o.precision != PGXC_PREC_MIXED_INT8)
     return fail(set_err(c, PGXC_EINVAL, "unknown precision mode"));
   if (!grid || grid->npts <= 0 || !grid->grdpts) return fail(set_err(c, PGXC_EINVAL, "empty grid"));
@@ -367,6 +372,7 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
     // screened build: per-tile significant-function lists; only P, the
     // accumulators and the packed matrix are shared with the dense layout
     if ((st = dalloc(c, &a.acc, 4)) || (st = dalloc(c, &a.P, (size_t)a.ldc * a.ldc))) return fail(st);
+    if (o.ispin == 2 && (st = dalloc(c, &c->P2, (size_t)a.ldc * a.ldc))) return fail(st);
     if ((st = dalloc(c, &c->d_ham, (size_t)o.ispin * c->nbas * (c->nbas + 1) / 2))) return fail(st);
     CUDA_TRY(c, cudaMallocHost(&c->h_ham, sizeof(double) * o.ispin * c->nbas * (c->nbas + 1) / 2));
     CUDA_TRY(c, cudaMallocHost(&c->h_acc, sizeof(double) * 4));
@@ -382,6 +388,7 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
     in.contr = bas->contractions;
     in.threshold = o.screen_threshold;
     in.gga = gga;
+    in.ispin = o.ispin;
     in.precision = o.precision;
     in.max_chunk_points = o.max_chunk_points;
     std::string e;
@@ -474,10 +481,33 @@ static int ensure_occ(pgxc_ctx* c, int nocc) {
   if ((st = dalloc(c, &C, (size_t)kpad * a.ldc)) || (st = dalloc(c, &Cocc, (size_t)kpad * a.ldc)) ||
       (st = dalloc(c, &occ, kpad)))
     return st;
+  if (c->opt.ispin == 2 && ((st = dalloc(c, &c->C2, (size_t)kpad * a.ldc)) || (st = dalloc(c, &c->occ2, kpad))))
+    return st;
   a.C = C;
   a.Cocc = Cocc;
   a.occ = occ;
   c->nocc_cap = kpad;
+  return PGXC_OK;
+}
+
+// Copy the orbitals C (nbas x nocc per spin, spin blocks of nbas*nocc) and the
+// occupations (nocc per spin) into the padded device buffers: spin a into
+// a.C / a.occ, spin b (open shell) into C2 / occ2.  Padding rows and columns are zero.
+static int upload_orbitals(pgxc_ctx* c, const double* C, const double* occ, int32_t nbas, int32_t nocc, int64_t kpad,
+                           cudaMemcpyKind kind) {
+  BuildArgs& a = c->a;
+  cudaStream_t s = c->stream;
+  for (int sp = 0; sp < c->opt.ispin; ++sp) {
+    double* dC = sp ? c->C2 : a.C;
+    double* docc = sp ? c->occ2 : (double*)a.occ;
+    CUDA_TRY(c, cudaMemsetAsync(dC, 0, sizeof(double) * kpad * a.ldc, s));
+    CUDA_TRY(c, cudaMemsetAsync(docc, 0, sizeof(double) * kpad, s));
+    if (nocc > 0) {
+      CUDA_TRY(c, cudaMemcpy2DAsync(dC, sizeof(double) * a.ldc, C + (size_t)sp * nbas * nocc, sizeof(double) * nbas,
+                                    sizeof(double) * nbas, nocc, kind, s));
+      CUDA_TRY(c, cudaMemcpyAsync(docc, occ + (size_t)sp * nocc, sizeof(double) * nocc, kind, s));
+    }
+  }
   return PGXC_OK;
 }
 
@@ -491,11 +521,18 @@ static int run_build(pgxc_ctx* c, int nocc, pgxc_timings* tm) {
     CUDA_TRY(c, cudaMemsetAsync(a.acc, 0, 4 * sizeof(double), s));
     CUDA_TRY(c, cudaEventRecord(c->ev[1], s));
     launch_pmat_f64(a, kpad, s);
+    if (c->opt.ispin == 2) {
+      BuildArgs b = a;  // second spin: its orbitals and occupations into P2 (Cocc is scratch)
+      b.C = c->C2;
+      b.occ = c->occ2;
+      b.P = c->P2;
+      launch_pmat_f64(b, kpad, s);
+    }
     CUDA_TRY(c, cudaGetLastError());
     CUDA_TRY(c, cudaEventRecord(c->ev[2], s));
     ScreenTimes T;
     std::string e;
-    const int st = screen_run(c->screen, a, s, c->d_ham, c->opt.ispin, 0, &T, e);
+    const int st = screen_run(c->screen, a, c->P2, s, c->d_ham, &T, e);
     if (st) return set_err(c, st, e);
     float ms = 0;
     CUDA_TRY(c, cudaEventElapsedTime(&ms, c->ev[1], c->ev[2]));
@@ -506,7 +543,7 @@ static int run_build(pgxc_ctx* c, int nocc, pgxc_timings* tm) {
       tm->potential_ms = T.potential;
       tm->xgemm_ms = T.x;
       tm->vgemm_ms = T.v;
-      tm->kernel_launches = T.launches + 2;
+      tm->kernel_launches = T.launches + 2 * c->opt.ispin;
     }
     return PGXC_OK;
   }
@@ -608,13 +645,7 @@ int pgxc_build(pgxc_ctx* c, const double* C, const double* occ, int32_t nbas, in
   cudaStream_t s = c->stream;
   const int64_t kpad = round_up(std::max(nocc, 1), 16);
   CUDA_TRY(c, cudaEventRecord(c->ev[0], s));
-  CUDA_TRY(c, cudaMemsetAsync(a.C, 0, sizeof(double) * kpad * a.ldc, s));
-  CUDA_TRY(c, cudaMemsetAsync((double*)a.occ, 0, sizeof(double) * kpad, s));
-  if (nocc > 0) {
-    CUDA_TRY(c, cudaMemcpy2DAsync(a.C, sizeof(double) * a.ldc, C, sizeof(double) * nbas, sizeof(double) * nbas, nocc,
-                                  cudaMemcpyHostToDevice, s));
-    CUDA_TRY(c, cudaMemcpyAsync((double*)a.occ, occ, sizeof(double) * nocc, cudaMemcpyHostToDevice, s));
-  }
+  if ((st = upload_orbitals(c, C, occ, nbas, nocc, kpad, cudaMemcpyHostToDevice))) return st;
   CUDA_TRY(c, cudaEventRecord(c->ev[1], s));
   CUDA_TRY(c, cudaEventSynchronize(c->ev[1]));
   float h2d = 0;
@@ -657,13 +688,7 @@ int pgxc_build_device(pgxc_ctx* c, const double* d_C, const double* d_occ, int32
   cudaStream_t s = c->stream;
   const int64_t kpad = round_up(std::max(nocc, 1), 16);
   CUDA_TRY(c, cudaEventRecord(c->ev[0], s));
-  CUDA_TRY(c, cudaMemsetAsync(a.C, 0, sizeof(double) * kpad * a.ldc, s));
-  CUDA_TRY(c, cudaMemsetAsync((double*)a.occ, 0, sizeof(double) * kpad, s));
-  if (nocc > 0) {
-    CUDA_TRY(c, cudaMemcpy2DAsync(a.C, sizeof(double) * a.ldc, d_C, sizeof(double) * nbas, sizeof(double) * nbas,
-                                  nocc, cudaMemcpyDeviceToDevice, s));
-    CUDA_TRY(c, cudaMemcpyAsync((double*)a.occ, d_occ, sizeof(double) * nocc, cudaMemcpyDeviceToDevice, s));
-  }
+  if ((st = upload_orbitals(c, d_C, d_occ, nbas, nocc, kpad, cudaMemcpyDeviceToDevice))) return st;
   pgxc_timings local{};
   if ((st = run_build(c, nocc, &local))) return st;
   CUDA_TRY(c, cudaMemcpyAsync(d_ham, c->d_ham, sizeof(double) * xc_length, cudaMemcpyDeviceToDevice, s));
@@ -730,23 +755,27 @@ int pgxc_orbital_calculate(pgxc_ctx* c, int64_t npts, const double* pts, double*
 int pgxc_xc_functionals(int32_t functional, int32_t ispin, int64_t n, const double* rho, const double* gam, double* f,
                         double* fr, double* fg) {
   if (functional != PGXC_XC_VWN && functional != PGXC_XC_PBE) return set_err(nullptr, PGXC_EINVAL, "functional");
-  if (ispin != 1) return set_err(nullptr, PGXC_ENOTSUP, "only ispin=1 point functionals are implemented");
+  if (ispin != 1 && ispin != 2) return set_err(nullptr, PGXC_EINVAL, "ispin must be 1 or 2");
   if (n < 0 || !rho || !f || !fr) return set_err(nullptr, PGXC_EINVAL, "bad arguments");
   const bool gga = functional == PGXC_XC_PBE;
   if (gga && (!gam || !fg)) return set_err(nullptr, PGXC_EINVAL, "PBE needs gam and fg");
   if (n == 0) return PGXC_OK;
   int st = check_device(nullptr, -1);
   if (st) return st;
+  const int64_t ng = 2 * ispin - 1;  // columns of gam and fg
+  // device layout: rho (ispin), gam (ng), f (1), fr (ispin), fg (ng) columns of n
+  const int64_t cols = 2 * ispin + 2 * ng + 1;
   double* d;
-  if (cudaMalloc(&d, sizeof(double) * 5 * n) != cudaSuccess) return set_err(nullptr, PGXC_ENOMEM, "cudaMalloc");
-  cudaMemcpy(d, rho, sizeof(double) * n, cudaMemcpyHostToDevice);
-  if (gga) cudaMemcpy(d + n, gam, sizeof(double) * n, cudaMemcpyHostToDevice);
-  launch_xc_points(functional, n, d, d + n, d + 2 * n, d + 3 * n, d + 4 * n, 0);
+  if (cudaMalloc(&d, sizeof(double) * cols * n) != cudaSuccess) return set_err(nullptr, PGXC_ENOMEM, "cudaMalloc");
+  double *drho = d, *dgam = d + ispin * n, *df = dgam + ng * n, *dfr = df + n, *dfg = dfr + ispin * n;
+  cudaMemcpy(drho, rho, sizeof(double) * ispin * n, cudaMemcpyHostToDevice);
+  if (gga) cudaMemcpy(dgam, gam, sizeof(double) * ng * n, cudaMemcpyHostToDevice);
+  launch_xc_points(functional, ispin, n, drho, dgam, df, dfr, dfg, 0);
   cudaError_t e = cudaDeviceSynchronize();
   if (e == cudaSuccess) {
-    cudaMemcpy(f, d + 2 * n, sizeof(double) * n, cudaMemcpyDeviceToHost);
-    cudaMemcpy(fr, d + 3 * n, sizeof(double) * n, cudaMemcpyDeviceToHost);
-    if (gga) cudaMemcpy(fg, d + 4 * n, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(f, df, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    cudaMemcpy(fr, dfr, sizeof(double) * ispin * n, cudaMemcpyDeviceToHost);
+    if (gga) cudaMemcpy(fg, dfg, sizeof(double) * ng * n, cudaMemcpyDeviceToHost);
   }
   cudaFree(d);
   if (e != cudaSuccess) return set_err(nullptr, PGXC_ECUDA, cudaGetErrorString(e));

@@ -42,6 +42,7 @@ struct ScreenPlan {
   double sum_n2 = 0.0;
   int max_n = 0;
   bool gga = false;
+  int ispin = 1;
   int64_t nbas = 0;
   // device, whole grid
   double *qx = nullptr, *qy = nullptr, *qz = nullptr, *qw = nullptr;  // Morton-ordered points [ntiles*128]
@@ -58,12 +59,12 @@ struct ScreenPlan {
   int64_t chunk_slots = 0, chunk_tiles = 0;        // buffer capacities
   // device, per chunk
   double *phi = nullptr, *gx = nullptr, *gy = nullptr, *gz = nullptr, *Z = nullptr;
-  double* pt = nullptr;      // 8 point arrays of chunk_tiles*128
+  double* pt = nullptr;      // 8 point arrays of chunk_tiles*128 per spin
   double* partial = nullptr;
-  double* V = nullptr;       // [nbas][nbas]
+  double* V = nullptr;       // [ispin][nbas][nbas]
   unsigned long long* pmax = nullptr;  // [chunk_tiles*128] largest |phi| per point (INT8 path)
   ScreenMixed* mixed = nullptr;
-  cudaEvent_t ev[10] = {};
+  cudaEvent_t ev[12] = {};
   std::vector<void*> allocs;
 };
 
@@ -499,6 +500,7 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
   *out = nullptr;
   ScreenPlan* sp = new ScreenPlan();
   sp->gga = in.gga;
+  sp->ispin = in.ispin;
   sp->nbas = in.nbas;
   const std::vector<DevShell>& shells = *in.shells;
   for (const DevShell& S : shells)
@@ -611,7 +613,7 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
   size_t freeb = 0, totb = 0;
   SP_TRY(cudaMemGetInfo(&freeb, &totb), "cudaMemGetInfo");
   const int64_t per_slot = 128 * 8 * (in.gga ? 5 : 2) + (mixed ? screen_mixed_bytes_per_slot() : 0);
-  const int64_t per_tile = 128 * 8 * 8 + (mixed ? screen_mixed_bytes_per_tile() : 0);
+  const int64_t per_tile = 128 * 8 * 8 * in.ispin + (mixed ? screen_mixed_bytes_per_tile() : 0);
   int64_t budget_slots = (int64_t)(0.45 * (double)freeb) / per_slot;
   budget_slots = std::max<int64_t>(budget_slots, sp->max_n);
   int64_t budget_tiles = std::max<int64_t>(1, (int64_t)(0.05 * (double)freeb) / per_tile);
@@ -682,14 +684,15 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
     SP_TRY(cudaMemset(sp->gz, 0, sizeof(double) * rows), "memset");
   }
   const int64_t cp = sp->chunk_tiles * 128;
-  SP_TRY(sp_alloc(sp, &sp->pt, 8 * (size_t)cp), "cudaMalloc");
+  SP_TRY(sp_alloc(sp, &sp->pt, 8 * (size_t)in.ispin * cp), "cudaMalloc");
   SP_TRY(sp_alloc(sp, &sp->partial, 2 * (size_t)((cp + 255) / 256) + 2), "cudaMalloc");
-  SP_TRY(sp_alloc(sp, &sp->V, (size_t)in.nbas * in.nbas), "cudaMalloc (V)");
+  SP_TRY(sp_alloc(sp, &sp->V, (size_t)in.ispin * in.nbas * in.nbas), "cudaMalloc (V)");
   if (mixed) {
     ScreenMixedInput mi;
     mi.nbas = in.nbas;
     mi.ldc = a.ldc;
     mi.gga = in.gga;
+    mi.nspin = in.ispin;
     mi.chunk_slots = sp->chunk_slots + kSlack;
     mi.chunk_tiles = sp->chunk_tiles;
     mi.max_n = sp->max_n;
@@ -708,9 +711,12 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
   return PGXC_OK;
 }
 
-int screen_run(ScreenPlan* sp, const BuildArgs& a, cudaStream_t st, double* ham, int ispin, int spin,
-               ScreenTimes* tm, std::string& err) {
+int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_t st, double* ham, ScreenTimes* tm,
+               std::string& err) {
   const bool gga = sp->gga;
+  const int ispin = sp->ispin;
+  const double* P[2] = {a.P, Pb};
+  const int64_t nb2 = sp->nbas * sp->nbas;
   ScreenTimes T;
   cudaEvent_t* ev = sp->ev;
 #define SR_TRY(call)                                                          \
@@ -721,25 +727,30 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, cudaStream_t st, double* ham,
       return PGXC_ECUDA;                                                      \
     }                                                                         \
   } while (0)
-  SR_TRY(cudaMemsetAsync(sp->V, 0, sizeof(double) * sp->nbas * sp->nbas, st));
+  SR_TRY(cudaMemsetAsync(sp->V, 0, sizeof(double) * ispin * nb2, st));
   if (sp->mixed) {
     SR_TRY(cudaEventRecord(ev[0], st));
-    T.launches += screen_mixed_prepare(sp->mixed, a, st);
+    for (int s = 0; s < ispin; ++s) T.launches += screen_mixed_prepare(sp->mixed, P[s], a.ldc, s, st);
     SR_TRY(cudaEventRecord(ev[1], st));
   }
   const int64_t cp = sp->chunk_tiles * 128;
-  BuildArgs b = a;  // per-chunk point arrays for the functional
-  b.ldp = cp;
-  b.w = nullptr;
-  b.rho = sp->pt;
-  b.grx = sp->pt + cp;
-  b.gry = sp->pt + 2 * cp;
-  b.grz = sp->pt + 3 * cp;
-  b.A = sp->pt + 4 * cp;
-  b.Bx = sp->pt + 5 * cp;
-  b.By = sp->pt + 6 * cp;
-  b.Bz = sp->pt + 7 * cp;
-  b.partial = sp->partial;
+  // per-chunk point arrays of spin s: 8 columns of cp (rho, grad rho, A, B) from pt + 8 s cp
+  BuildArgs b[2];
+  for (int s = 0; s < ispin; ++s) {
+    double* q = sp->pt + 8 * s * cp;
+    b[s] = a;
+    b[s].ldp = cp;
+    b[s].w = nullptr;
+    b[s].rho = q;
+    b[s].grx = q + cp;
+    b[s].gry = q + 2 * cp;
+    b[s].grz = q + 3 * cp;
+    b[s].A = q + 4 * cp;
+    b[s].Bx = q + 5 * cp;
+    b[s].By = q + 6 * cp;
+    b[s].Bz = q + 7 * cp;
+    b[s].partial = sp->partial;
+  }
   const size_t nch = sp->chunk_t0.size() - 1;
   float ms;
   for (size_t c = 0; c < nch; ++c) {
@@ -775,62 +786,72 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, cudaStream_t st, double* ham,
         T.launches += screen_mixed_basis(sp->mixed, sp->tso, sp->slot_fn, t0, nt, s0, sp->phi, sp->pmax, st);
     }
     SR_TRY(cudaEventRecord(ev[3], st));
-    // K3
+    // K3, per spin
     SR_TRY(cudaEventRecord(ev[4], st));
-    if (sp->mixed) {
-      T.launches += screen_mixed_density(sp->mixed, sp->tso, sp->slot_fn, t0, nt, s0, sp->phi, sp->gx, sp->gy,
-                                         sp->gz, b.rho, b.grx, b.gry, b.grz, st);
-    } else {
-      const int smem = gemm_smem_bytes<false, false>() + (int)sizeof(int) * sp->max_n;
-      dim3 grid((unsigned)nt, 2);
-      if (gga) {
-        cudaFuncSetAttribute(k_sdensity<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        k_sdensity<true><<<grid, kGemmThreads, smem, st>>>(sp->phi, sp->gx, sp->gy, sp->gz, sp->tso, t0, s0,
-                                                           sp->slot_fn, a.P, a.ldc, b.rho, b.grx, b.gry, b.grz);
+    for (int s = 0; s < ispin; ++s) {
+      if (sp->mixed) {
+        if (s > 0) T.launches += screen_mixed_gather(sp->mixed, sp->tso, sp->slot_fn, t0, nt, s0, s, st);
+        T.launches += screen_mixed_density(sp->mixed, sp->tso, sp->slot_fn, t0, nt, s0, sp->phi, sp->gx, sp->gy,
+                                           sp->gz, b[s].rho, b[s].grx, b[s].gry, b[s].grz, st);
       } else {
-        cudaFuncSetAttribute(k_sdensity<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        k_sdensity<false><<<grid, kGemmThreads, smem, st>>>(sp->phi, nullptr, nullptr, nullptr, sp->tso, t0, s0,
-                                                            sp->slot_fn, a.P, a.ldc, b.rho, nullptr, nullptr,
-                                                            nullptr);
+        const int smem = gemm_smem_bytes<false, false>() + (int)sizeof(int) * sp->max_n;
+        dim3 grid((unsigned)nt, 2);
+        if (gga) {
+          cudaFuncSetAttribute(k_sdensity<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+          k_sdensity<true><<<grid, kGemmThreads, smem, st>>>(sp->phi, sp->gx, sp->gy, sp->gz, sp->tso, t0, s0,
+                                                             sp->slot_fn, P[s], a.ldc, b[s].rho, b[s].grx, b[s].gry,
+                                                             b[s].grz);
+        } else {
+          cudaFuncSetAttribute(k_sdensity<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+          k_sdensity<false><<<grid, kGemmThreads, smem, st>>>(sp->phi, nullptr, nullptr, nullptr, sp->tso, t0, s0,
+                                                              sp->slot_fn, P[s], a.ldc, b[s].rho, nullptr, nullptr,
+                                                              nullptr);
+        }
+        ++T.launches;
       }
-      ++T.launches;
     }
     SR_TRY(cudaEventRecord(ev[5], st));
     // K2
-    {
-      BuildArgs bf = b;
+    if (ispin == 1) {
+      BuildArgs bf = b[0];
       bf.w = sp->qw;
       launch_functional_f64(bf, t0 * 128, npt, gga, st);
-      T.launches += 2;
-    }
-    SR_TRY(cudaEventRecord(ev[6], st));
-    // K4
-    if (sp->mixed) {
-      T.launches += screen_mixed_potential(sp->mixed, sp->tso, sp->slot_fn, sp->slot_tile, t0, nt, s0, ns, sp->phi,
-                                           sp->gx, sp->gy, sp->gz, b.A, b.Bx, b.By, b.Bz, sp->V, sp->nbas, st,
-                                           ev[7], ev[8]);
     } else {
-      const unsigned nb = (unsigned)std::max<int64_t>(1, std::min<int64_t>((ns * 128 + 255) / 256, 148 * 32));
-      if (gga)
-        k_szbuild<true><<<nb, 256, 0, st>>>(ns, sp->slot_tile + s0, t0, sp->phi, sp->gx, sp->gy, sp->gz, b.A, b.Bx,
-                                            b.By, b.Bz, sp->Z);
-      else
-        k_szbuild<false><<<nb, 256, 0, st>>>(ns, sp->slot_tile + s0, t0, sp->phi, nullptr, nullptr, nullptr, b.A,
-                                             nullptr, nullptr, nullptr, sp->Z);
-      SR_TRY(cudaEventRecord(ev[7], st));
-      const int smem = gemm_smem_bytes<true, true>() + (int)sizeof(int) * sp->max_n;
-      dim3 grid((unsigned)nt, 4);
-      if (gga) {
-        cudaFuncSetAttribute(k_svpot<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        k_svpot<true><<<grid, kGemmThreads, smem, st>>>(sp->phi, sp->Z, sp->tso, t0, s0, sp->slot_fn, sp->V,
-                                                        sp->nbas);
+      launch_functional2_f64(a.xc, sp->qw, b[0].rho, b[1].rho, cp, t0 * 128, npt, gga, sp->partial, a.acc, st);
+    }
+    T.launches += 2;
+    SR_TRY(cudaEventRecord(ev[6], st));
+    // K4, per spin: the contraction of spin s is bracketed by ev[7 + 3s], ev[8 + 3s]
+    for (int s = 0; s < ispin; ++s) {
+      double* Vs = sp->V + s * nb2;
+      cudaEvent_t k0 = ev[7 + 3 * s], k1 = ev[8 + 3 * s];
+      if (sp->mixed) {
+        T.launches += screen_mixed_potential(sp->mixed, sp->tso, sp->slot_fn, sp->slot_tile, t0, nt, s0, ns, sp->phi,
+                                             sp->gx, sp->gy, sp->gz, b[s].A, b[s].Bx, b[s].By, b[s].Bz, Vs, sp->nbas,
+                                             st, k0, k1);
       } else {
-        cudaFuncSetAttribute(k_svpot<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        k_svpot<false><<<grid, kGemmThreads, smem, st>>>(sp->phi, sp->Z, sp->tso, t0, s0, sp->slot_fn, sp->V,
-                                                         sp->nbas);
+        const unsigned nbk = (unsigned)std::max<int64_t>(1, std::min<int64_t>((ns * 128 + 255) / 256, 148 * 32));
+        if (gga)
+          k_szbuild<true><<<nbk, 256, 0, st>>>(ns, sp->slot_tile + s0, t0, sp->phi, sp->gx, sp->gy, sp->gz, b[s].A,
+                                               b[s].Bx, b[s].By, b[s].Bz, sp->Z);
+        else
+          k_szbuild<false><<<nbk, 256, 0, st>>>(ns, sp->slot_tile + s0, t0, sp->phi, nullptr, nullptr, nullptr,
+                                                b[s].A, nullptr, nullptr, nullptr, sp->Z);
+        SR_TRY(cudaEventRecord(k0, st));
+        const int smem = gemm_smem_bytes<true, true>() + (int)sizeof(int) * sp->max_n;
+        dim3 grid((unsigned)nt, 4);
+        if (gga) {
+          cudaFuncSetAttribute(k_svpot<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+          k_svpot<true><<<grid, kGemmThreads, smem, st>>>(sp->phi, sp->Z, sp->tso, t0, s0, sp->slot_fn, Vs,
+                                                          sp->nbas);
+        } else {
+          cudaFuncSetAttribute(k_svpot<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+          k_svpot<false><<<grid, kGemmThreads, smem, st>>>(sp->phi, sp->Z, sp->tso, t0, s0, sp->slot_fn, Vs,
+                                                           sp->nbas);
+        }
+        SR_TRY(cudaEventRecord(k1, st));
+        T.launches += 2;
       }
-      SR_TRY(cudaEventRecord(ev[8], st));
-      T.launches += 2;
     }
     SR_TRY(cudaGetLastError());
     SR_TRY(cudaEventRecord(ev[9], st));
@@ -839,7 +860,10 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, cudaStream_t st, double* ham,
     SR_TRY(cudaEventElapsedTime(&ms, ev[4], ev[5])); T.density += ms; T.x += ms;
     SR_TRY(cudaEventElapsedTime(&ms, ev[5], ev[6])); T.functional += ms;
     SR_TRY(cudaEventElapsedTime(&ms, ev[6], ev[9])); T.potential += ms;
-    SR_TRY(cudaEventElapsedTime(&ms, ev[7], ev[8])); T.v += ms;
+    for (int s = 0; s < ispin; ++s) {
+      SR_TRY(cudaEventElapsedTime(&ms, ev[7 + 3 * s], ev[8 + 3 * s]));
+      T.v += ms;
+    }
   }
   if (sp->mixed) {
     SR_TRY(cudaEventElapsedTime(&ms, ev[0], ev[1]));
@@ -848,9 +872,11 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, cudaStream_t st, double* ham,
   SR_TRY(cudaEventRecord(ev[2], st));
   {
     const int64_t len = sp->nbas * (sp->nbas + 1) / 2;
-    const unsigned nb = (unsigned)std::min<int64_t>((len + 255) / 256, 148 * 8);
-    k_spack<<<nb, 256, 0, st>>>(sp->V, sp->nbas, gga, ispin, spin, ham);
-    ++T.launches;
+    const unsigned nbk = (unsigned)std::min<int64_t>((len + 255) / 256, 148 * 8);
+    for (int s = 0; s < ispin; ++s) {
+      k_spack<<<nbk, 256, 0, st>>>(sp->V + s * nb2, sp->nbas, gga, ispin, s, ham);
+      ++T.launches;
+    }
   }
   SR_TRY(cudaGetLastError());
   SR_TRY(cudaEventRecord(ev[3], st));

@@ -44,16 +44,19 @@ struct ScreenInput {
   const double* contr;        // host
   double threshold;
   bool gga;
+  int ispin = 1;              // 2: open shell, one density and one V_xc per spin
   int precision;              // PGXC_PREC_*
   int64_t max_chunk_points;   // 0: sized from free device memory
 };
 
 int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, cudaStream_t st, std::string& err);
 void screen_destroy(ScreenPlan* sp);
-// One build: P (FP64, a.P) must be ready; E_xc / N_el are Kahan-added into
-// a.acc; the packed matrix of spin `spin` is written to ham.
-int screen_run(ScreenPlan* sp, const BuildArgs& a, cudaStream_t st, double* ham, int ispin, int spin,
-               ScreenTimes* t, std::string& err);
+// One build: the FP64 density matrices must be ready (a.P; for an open shell
+// also Pb, the second spin's, with the same leading dimension a.ldc); E_xc /
+// N_el are Kahan-added into a.acc; the packed matrix (both spins interleaved
+// for an open shell) is written to ham.
+int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_t st, double* ham, ScreenTimes* t,
+               std::string& err);
 // Plan statistics: tiles, total slots (padded), listed functions, sum of n_t^2.
 void screen_stats(const ScreenPlan* sp, int64_t* ntiles, int64_t* nslots, int64_t* nlisted, double* sum_n2,
                   int64_t* nchunks);

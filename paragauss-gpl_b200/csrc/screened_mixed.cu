@@ -54,8 +54,9 @@ struct ScreenMixed {
   bool gga = false;
   int64_t chunk_slots = 0, chunk_tiles = 0;
   int max_n = 0;
-  unsigned long long* P8 = nullptr;  // [nbas][nbas]
-  int* e_P = nullptr;                // [nbas]
+  int nspin = 1;
+  unsigned long long* P8[2] = {};    // [nbas][nbas] per spin
+  int* e_P[2] = {};                  // [nbas] per spin
   int8_t* tA = nullptr;              // density A digits, [slot block of 32][slice][128 x 32] per tile
   int8_t* tB = nullptr;              // density B digits, [stage][slice][48 x 32] per tile
   const int64_t* b_off = nullptr;    // [ntiles + 1] first B stage of each tile
@@ -731,10 +732,13 @@ int screen_mixed_create(ScreenMixed** out, const ScreenMixedInput& in, std::stri
   m->chunk_slots = in.chunk_slots;
   m->chunk_tiles = in.chunk_tiles;
   m->max_n = in.max_n;
+  m->nspin = in.nspin;
   cudaError_t e = cudaSuccess;
   const size_t dig = (size_t)in.chunk_slots * kDigBytesPerSlot;
-  if (e == cudaSuccess) e = sm_alloc(m, &m->P8, (size_t)in.nbas * in.nbas);
-  if (e == cudaSuccess) e = sm_alloc(m, &m->e_P, (size_t)in.nbas);
+  for (int s = 0; s < in.nspin; ++s) {
+    if (e == cudaSuccess) e = sm_alloc(m, &m->P8[s], (size_t)in.nbas * in.nbas);
+    if (e == cudaSuccess) e = sm_alloc(m, &m->e_P[s], (size_t)in.nbas);
+  }
   if (e == cudaSuccess) e = sm_alloc(m, &m->tA, dig);
   if (e == cudaSuccess) e = sm_alloc(m, &m->tB, (size_t)in.chunk_bstages * kOpB);
   m->b_off = in.b_off;
@@ -780,19 +784,24 @@ void screen_mixed_destroy(ScreenMixed* m) {
   delete m;
 }
 
-int screen_mixed_prepare(ScreenMixed* m, const BuildArgs& a, cudaStream_t st) {
-  k_sm_rowexp_P<<<(unsigned)m->nbas, 256, 0, st>>>(a.P, a.ldc, m->nbas, m->e_P);
+int screen_mixed_prepare(ScreenMixed* m, const double* P, int64_t ldc, int spin, cudaStream_t st) {
+  k_sm_rowexp_P<<<(unsigned)m->nbas, 256, 0, st>>>(P, ldc, m->nbas, m->e_P[spin]);
   const unsigned nb = (unsigned)std::max<int64_t>(1, std::min<int64_t>((m->nbas * m->nbas + 255) / 256, 148 * 16));
-  k_sm_quant_P<<<nb, 256, 0, st>>>(a.P, a.ldc, m->nbas, m->e_P, m->P8);
+  k_sm_quant_P<<<nb, 256, 0, st>>>(P, ldc, m->nbas, m->e_P[spin], m->P8[spin]);
   return 2;
 }
 
 int screen_mixed_basis(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
                        const double* phi, const unsigned long long* pmax, cudaStream_t st) {
   k_sm_quant_pts<<<(unsigned)nt, 128, 0, st>>>(tso, t0, s0, phi, pmax, m->e_pt, m->tA);
-  k_sm_gather_B<<<dim3((unsigned)nt, kGatherSplit), 192, 4 * m->max_n, st>>>(tso, slot_fn, m->b_off, t0, s0, m->P8,
-                                                                             m->e_P, m->nbas, m->tB, m->ps);
-  return 2;
+  return 1 + screen_mixed_gather(m, tso, slot_fn, t0, nt, s0, 0, st);
+}
+
+int screen_mixed_gather(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
+                        int spin, cudaStream_t st) {
+  k_sm_gather_B<<<dim3((unsigned)nt, kGatherSplit), 192, 4 * m->max_n, st>>>(
+      tso, slot_fn, m->b_off, t0, s0, m->P8[spin], m->e_P[spin], m->nbas, m->tB, m->ps);
+  return 1;
 }
 
 int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,

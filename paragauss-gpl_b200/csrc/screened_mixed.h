@@ -16,6 +16,7 @@ struct ScreenMixed;
 struct ScreenMixedInput {
   int64_t nbas = 0, ldc = 0;
   bool gga = false;
+  int nspin = 1;             // density matrices kept in digit form (2 for open shell)
   int64_t chunk_slots = 0;   // slot rows of the chunk buffers (slack included)
   int64_t chunk_tiles = 0;
   int max_n = 0;             // largest padded slot count of a tile
@@ -31,13 +32,16 @@ int64_t screen_mixed_bstages(int64_t n);
 int64_t screen_mixed_bytes_per_bstage();
 int screen_mixed_create(ScreenMixed** out, const ScreenMixedInput& in, std::string& err);
 void screen_mixed_destroy(ScreenMixed* m);
-// INT8 digits of the FP64 density matrix a.P (per-row scales); returns launches
-int screen_mixed_prepare(ScreenMixed* m, const BuildArgs& a, cudaStream_t st);
+// INT8 digits of the FP64 density matrix P of spin `spin` (per-row scales); returns launches
+int screen_mixed_prepare(ScreenMixed* m, const double* P, int64_t ldc, int spin, cudaStream_t st);
 // Operands of the density contraction: INT8 digits of phi (per-point scales
 // from pmax, the bit patterns of the largest |phi| of each point of the
-// chunk) and the gathered digits of P[S_t, S_t] of every tile
+// chunk) and the gathered digits of P[S_t, S_t] of every tile (spin 0)
 int screen_mixed_basis(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
                        const double* phi, const unsigned long long* pmax, cudaStream_t st);
+// the gathered digits of P_spin[S_t, S_t] of every tile (replaces the previous spin's)
+int screen_mixed_gather(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
+                        int spin, cudaStream_t st);
 int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
                          const double* phi, const double* gx, const double* gy, const double* gz, double* rho,
                          double* grx, double* gry, double* grz, cudaStream_t st);

@@ -1,7 +1,9 @@
-// xc_functional.cuh -- per-point XC functionals in FP64, closed-shell (ispin=1).
+// xc_functional.cuh -- per-point XC functionals in FP64.
 //
-// Restates ParaGauss's functional pieces with hand-derived first derivatives
-// (the reference obtains them with its forward-mode AD types):
+// Closed shell (ispin = 1) with hand-derived first derivatives; open shell
+// (ispin = 2) with forward-mode dual numbers in (rho_a, rho_b, gamma), the
+// role of the reference's ad2x1..ad2x3 types (autodiff/autodiff2.f90).
+// Restated pieces:
 //   Slater exchange       modules/exchange.f90:511-601  (x_lda)
 //   VWN5 correlation      modules/vwnc.f90:122-297      (c_lda, vwn_ldac)
 //   PW92 correlation      modules/pw_ldac_module.f90:127-312, :591-651
@@ -31,6 +33,10 @@ struct XcConst {
   // PBE correlation
   double pbe_fi;        // (0.5^(2/3)+0.5^(2/3)) * (1/2^(1/3))
   double pbe_ct;        // pi/(16 (3 pi^2)^(1/3))
+  // open shell
+  double vwn_ffact;     // (1/2) / (2^(1/3) - 1)
+  double pw_cf;         // 1 / (2^(4/3) - 2)
+  double pbe_two13i;    // 1 / 2^(1/3)
 };
 
 __host__ inline XcConst make_xc_const() {
@@ -46,6 +52,9 @@ __host__ inline XcConst make_xc_const() {
   c.pbe_mu = 0.066725 * (pi_x * pi_x / 3.0);
   c.pbe_fi = (std::pow(0.5, 2.0 / 3.0) + std::pow(0.5, 2.0 / 3.0)) * (1.0 / std::pow(2.0, 1.0 / 3.0));
   c.pbe_ct = pi_p / (4.0 * 4.0 * std::pow(3.0 * pi_p * pi_p, 1.0 / 3.0));
+  c.vwn_ffact = 0.5 / (std::pow(2.0, 1.0 / 3.0) - 1.0);
+  c.pw_cf = 1.0 / (std::pow(2.0, 4.0 / 3.0) - 2.0);
+  c.pbe_two13i = 1.0 / std::pow(2.0, 1.0 / 3.0);
   return c;
 }
 
@@ -103,6 +112,32 @@ __device__ __forceinline__ void xc_vwn(const XcConst& K, double n, double& f, do
   fr += ecpara - ap * de * X / 6.0;             // dX/dn = -X/(6S)
 }
 
+// PBE exchange enhancement of the closed-shell functional e(n, g): e_x G(s^2),
+// the 1 of (1+G) omitted (x_gga, exchange.f90:325-439); adds F, dF/dn, dF/dg.
+__device__ __forceinline__ void pbe_x(const XcConst& K, double n, double g, double& f, double& fr, double& fg) {
+  double ex = 0.0, exr = 0.0;
+  if (n > 0.0) {
+    const double c = cbrt(n);
+    ex = K.xalpha * n * c;
+    exr = (4.0 / 3.0) * K.xalpha * c;
+  }
+  double s2 = 0.0, s2r = 0.0, s2g = 0.0;
+  if (n >= 1.0e-20) {
+    const double c = cbrt(n);
+    const double n83 = n * n * c * c;
+    s2g = 1.0 / n83 * K.s2_fact;
+    s2 = g * s2g;
+    s2r = -(8.0 / 3.0) * s2 / n;
+  }
+  const double kappa = 0.804, mu = K.pbe_mu;
+  const double den = kappa + mu * s2;
+  const double G = kappa * mu * s2 / den;
+  const double Gs = kappa * kappa * mu / (den * den);
+  f += ex * G;
+  fr += exr * G + ex * Gs * s2r;
+  fg += ex * Gs * s2g;
+}
+
 // "PBE": Slater + PW92 + PBE exchange enhancement + PBE correlation H.
 // n = total density, g = |grad n|^2; returns f, df/dn, df/dg.
 __device__ __forceinline__ void xc_pbe(const XcConst& K, double n, double g, double& f, double& fr,
@@ -123,29 +158,7 @@ __device__ __forceinline__ void xc_pbe(const XcConst& K, double n, double g, dou
     if (!frozen) fr += E - rs * dE / 3.0;
   }
   // PBE exchange: e_x * G(s^2), the 1 of (1+G) omitted (x_gga)
-  {
-    double ex = 0.0, exr = 0.0;
-    if (n > 0.0) {
-      const double c = cbrt(n);
-      ex = K.xalpha * n * c;
-      exr = (4.0 / 3.0) * K.xalpha * c;
-    }
-    double s2 = 0.0, s2r = 0.0, s2g = 0.0;
-    if (n >= 1.0e-20) {
-      const double c = cbrt(n);
-      const double n83 = n * n * c * c;
-      s2g = 1.0 / n83 * K.s2_fact;
-      s2 = g * s2g;
-      s2r = -(8.0 / 3.0) * s2 / n;
-    }
-    const double kappa = 0.804, mu = K.pbe_mu;
-    const double den = kappa + mu * s2;
-    const double G = kappa * mu * s2 / den;
-    const double Gs = kappa * kappa * mu / (den * den);
-    f += ex * G;
-    fr += exr * G + ex * Gs * s2r;
-    fg += ex * Gs * s2g;
-  }
+  pbe_x(K, n, g, f, fr, fg);
   // PBE correlation H (c_gga with na = nb = n/2)
   if (n > 0.0) {
     const double beta = 0.066725;
@@ -198,6 +211,180 @@ __device__ __forceinline__ void xc_pbe(const XcConst& K, double n, double g, dou
     fr += H + n * dHn;
     fg += n * dHg;
   }
+}
+
+// ---------------------------------------------------------------------------
+// Open shell (ispin = 2).  D3 carries a value and its derivatives with
+// respect to three independent inputs; the spin-resolved correlation pieces
+// are written once on D3, exchange reuses the closed-shell forms through the
+// spin scaling e_x[rho_a, rho_b] = (e_x[2 rho_a] + e_x[2 rho_b]) / 2.
+// ---------------------------------------------------------------------------
+struct D3 {
+  double v, d[3];
+};
+__device__ __forceinline__ D3 d3c(double x) { return D3{x, {0.0, 0.0, 0.0}}; }
+__device__ __forceinline__ D3 d3v(int i, double x) {
+  D3 r = d3c(x);
+  r.d[i] = 1.0;
+  return r;
+}
+__device__ __forceinline__ D3 operator+(D3 a, D3 b) { return D3{a.v + b.v, {a.d[0] + b.d[0], a.d[1] + b.d[1], a.d[2] + b.d[2]}}; }
+__device__ __forceinline__ D3 operator-(D3 a, D3 b) { return D3{a.v - b.v, {a.d[0] - b.d[0], a.d[1] - b.d[1], a.d[2] - b.d[2]}}; }
+__device__ __forceinline__ D3 operator-(D3 a) { return D3{-a.v, {-a.d[0], -a.d[1], -a.d[2]}}; }
+__device__ __forceinline__ D3 operator*(D3 a, D3 b) {
+  return D3{a.v * b.v, {a.d[0] * b.v + a.v * b.d[0], a.d[1] * b.v + a.v * b.d[1], a.d[2] * b.v + a.v * b.d[2]}};
+}
+__device__ __forceinline__ D3 operator/(D3 a, D3 b) {
+  const double q = b.v * b.v;
+  return D3{a.v / b.v,
+            {(a.d[0] * b.v - a.v * b.d[0]) / q, (a.d[1] * b.v - a.v * b.d[1]) / q, (a.d[2] * b.v - a.v * b.d[2]) / q}};
+}
+__device__ __forceinline__ D3 operator+(D3 a, double b) { a.v += b; return a; }
+__device__ __forceinline__ D3 operator+(double b, D3 a) { a.v += b; return a; }
+__device__ __forceinline__ D3 operator-(D3 a, double b) { a.v -= b; return a; }
+__device__ __forceinline__ D3 operator-(double b, D3 a) { return d3c(b) - a; }
+__device__ __forceinline__ D3 operator*(D3 a, double b) { return D3{a.v * b, {a.d[0] * b, a.d[1] * b, a.d[2] * b}}; }
+__device__ __forceinline__ D3 operator*(double b, D3 a) { return a * b; }
+__device__ __forceinline__ D3 operator/(D3 a, double b) { return D3{a.v / b, {a.d[0] / b, a.d[1] / b, a.d[2] / b}}; }
+__device__ __forceinline__ D3 operator/(double b, D3 a) { return d3c(b) / a; }
+// chain rule with f(a.v) and f'(a.v)
+__device__ __forceinline__ D3 d3f(D3 a, double f, double df) {
+  return D3{f, {df * a.d[0], df * a.d[1], df * a.d[2]}};
+}
+__device__ __forceinline__ D3 d3pow(D3 a, double p) { return d3f(a, pow(a.v, p), p * pow(a.v, p - 1.0)); }
+__device__ __forceinline__ D3 d3sqrt(D3 a) { const double r = sqrt(a.v); return d3f(a, r, 0.5 / r); }
+__device__ __forceinline__ D3 d3log(D3 a) { return d3f(a, log(a.v), 1.0 / a.v); }
+__device__ __forceinline__ D3 d3exp(D3 a) { const double e = exp(a.v); return d3f(a, e, e); }
+__device__ __forceinline__ D3 d3atan(D3 a) { return d3f(a, atan(a.v), 1.0 / (1.0 + a.v * a.v)); }
+
+// VWN interpolation ec(X; B, C, X0), vwnc.f90:199-212
+__device__ __forceinline__ D3 vwn_ec3(D3 X, double B, double C, double X0) {
+  const double Q = sqrt(4.0 * C - B * B);
+  const double XX0 = (X0 + B) * X0 + C;
+  const D3 XXX = (X + B) * X + C;
+  const D3 FXX = d3atan(Q / (2.0 * X + B));
+  const D3 Xm = X - X0;
+  return d3log(X * X / XXX) + (2.0 * B / Q) * FXX -
+         (B * X0 / XX0) * (d3log(Xm * Xm / XXX) + ((2.0 * (B + 2.0 * X0)) / Q) * FXX);
+}
+
+// VWN5 c_lda(na, nb) with the spin interpolation, vwnc.f90:160-223: n * eps_c
+__device__ __forceinline__ D3 vwn_c_lda(const XcConst& K, D3 na, D3 nb) {
+  const double aa = -0.0337740 / 2.0, ba = 1.13107, ca = 13.0045, x0a = -0.0047584;
+  const double af = 0.0310907 / 2.0, bf = 7.06042, cf = 18.0578, x0f = -0.32500;
+  const double ap = 0.0621841 / 2.0, bp = 3.72744, cp = 12.9352, x0p = -0.10498;
+  const double ffact = K.vwn_ffact;
+  const double dfact = (4.0 / 3.0) * ffact;
+  const double ddfzero = (1.0 / 3.0) * dfact * 2.0;
+  const D3 sums = na + nb + 1.0e-50;
+  const D3 X = d3sqrt(d3pow(K.vwn_fact / sums, K.vwn_third));
+  const D3 zeta = (na - nb) / sums;
+  const D3 ecpara = ap * vwn_ec3(X, bp, cp, x0p);
+  const D3 ecferr = af * vwn_ec3(X, bf, cf, x0f);
+  const D3 alphac = aa * vwn_ec3(X, ba, ca, x0a);
+  const D3 betac = (ddfzero / alphac) * (ecferr - ecpara) - 1.0;
+  const D3 fz = ffact * (d3pow(1.0 + zeta, 4.0 / 3.0) + d3pow(1.0 - zeta, 4.0 / 3.0) - 2.0);
+  const D3 z2 = zeta * zeta;
+  const D3 deltec = alphac * (fz / ddfzero) * (1.0 + betac * (z2 * z2));
+  return (ecpara + deltec) * sums;
+}
+
+// PW92 G(rs) for the three parameter sets (1 ECU, 2 ECP, 3 -alpha_c),
+// pw_ldac_module.f90:171-192 with set_param :591-651
+__device__ __forceinline__ D3 pw92_g3(D3 rs, int what) {
+  double a, a1, b1, b2, b3, b4;
+  if (what == 1) { a = 0.031091; a1 = 0.21370; b1 = 7.5957; b2 = 3.5876; b3 = 1.6382; b4 = 0.49294; }
+  else if (what == 2) { a = 0.015545; a1 = 0.20548; b1 = 14.1189; b2 = 6.1977; b3 = 3.3662; b4 = 0.62517; }
+  else { a = 0.016887; a1 = 0.11125; b1 = 10.357; b2 = 3.6231; b3 = 0.88026; b4 = 0.49671; }
+  const D3 rs12 = d3pow(rs, 0.5);
+  const D3 Q0 = -2.0 * a * (1.0 + a1 * rs);
+  const D3 Q1 = 2.0 * a * (b1 * rs12 + b2 * rs + b3 * (rs * rs12) + b4 * (rs * rs));
+  return Q0 * d3log(1.0 + 1.0 / Q1);
+}
+
+// PW92 c_lda(na, nb), pw_ldac_module.f90:127-194: n * eps_c
+__device__ __forceinline__ D3 pw92_c_lda(const XcConst& K, D3 na, D3 nb) {
+  const double deps = 1.0e-30;
+  const double cf = K.pw_cf;
+  const double cfzz = 2.0 * (4.0 / 3.0) * (1.0 / 3.0) * cf;
+  D3 nn = na + nb;
+  if (nn.v < deps) nn = d3c(deps);  // frozen: no derivative (the reference fixes it)
+  const D3 rs = K.pw_crs / d3pow(nn, 1.0 / 3.0);
+  const D3 ecu = pw92_g3(rs, 1), ecp = pw92_g3(rs, 2), malf = pw92_g3(rs, 3);
+  const D3 z = (na - nb) / nn;
+  const D3 z2 = z * z;
+  const D3 z4 = z2 * z2;
+  const D3 f = cf * (d3pow(1.0 + z + deps, 4.0 / 3.0) + d3pow(1.0 - z + deps, 4.0 / 3.0) - 2.0);
+  return nn * (ecu + (ecp - ecu) * f * z4 - malf * f * (1.0 - z4) / cfzz);
+}
+
+// PBE correlation H(na, nb, g2), pbe_ggcxc_module.f90:96-145: n * H;
+// g2 = |grad n|^2 of the total density
+__device__ __forceinline__ D3 pbe_c_gga(const XcConst& K, D3 na, D3 nb, D3 g2) {
+  const double beta = 0.066725, gam = 0.03109069086965489503494086371, deps = 1.0e-30;
+  const D3 n = na + nb;
+  if (n.v <= 0.0) return d3c(0.0);
+  const D3 eldac = pw92_c_lda(K, na, nb) / n;
+  D3 za = na / n, zb = nb / n;
+  if (za.v < deps) za = d3c(deps);
+  if (zb.v < deps) zb = d3c(deps);
+  const D3 fi = (d3pow(za, 2.0 / 3.0) + d3pow(zb, 2.0 / 3.0)) * K.pbe_two13i;
+  const D3 fi2 = fi * fi;
+  const D3 fi3 = fi2 * fi;
+  const D3 A = (beta / gam) / (d3exp(-eldac / (gam * fi3)) - 1.0 + deps);
+  const D3 t2 = g2 / (fi2 * d3pow(n, 7.0 / 3.0) + deps) * K.pbe_ct;
+  const D3 x = A * t2;
+  const D3 rat = (1.0 + x) / (1.0 + x + x * x);
+  return n * (gam * fi3 * d3log(1.0 + (beta / gam) * t2 * rat));
+}
+
+// Open-shell functional at one point: rho[2] = (rho_a, rho_b), gam[3] =
+// (gamma_aa, gamma_bb, gamma_ab); f, fr[2] = df/drho_s, fg[3] = df/dgamma_*.
+// xc_functionals composition (xc_func.f90:187-305), as for ispin = 1.
+template <bool GGA>
+__device__ __forceinline__ void xc_open(const XcConst& K, const double (&rho)[2], const double (&gam)[3], double& f,
+                                        double (&fr)[2], double (&fg)[3]) {
+  f = 0.0;
+  fr[0] = fr[1] = 0.0;
+  fg[0] = fg[1] = fg[2] = 0.0;
+  // Slater, spin-scaled
+  for (int s = 0; s < 2; ++s) {
+    double F = 0.0, Fn = 0.0;
+    slater(K, 2.0 * rho[s], F, Fn);
+    f += F / 2.0;
+    fr[s] += Fn;
+  }
+  const D3 na = d3v(0, rho[0]), nb = d3v(1, rho[1]);
+  if (!GGA) {
+    const D3 c = vwn_c_lda(K, na, nb);
+    f += c.v;
+    fr[0] += c.d[0];
+    fr[1] += c.d[1];
+    return;
+  }
+  {
+    const D3 c = pw92_c_lda(K, na, nb);
+    f += c.v;
+    fr[0] += c.d[0];
+    fr[1] += c.d[1];
+  }
+  // PBE exchange, spin-scaled: e(2 rho_s, 4 gamma_ss) / 2
+  for (int s = 0; s < 2; ++s) {
+    double F = 0.0, Fn = 0.0, Fg = 0.0;
+    pbe_x(K, 2.0 * rho[s], 4.0 * gam[s], F, Fn, Fg);
+    f += 0.5 * F;
+    fr[s] += Fn;
+    fg[s] += 2.0 * Fg;
+  }
+  // PBE correlation H of the total gradient |grad rho_a + grad rho_b|^2
+  const D3 g2 = d3v(2, gam[0] + gam[1] + 2.0 * gam[2]);
+  const D3 c = pbe_c_gga(K, na, nb, g2);
+  f += c.v;
+  fr[0] += c.d[0];
+  fr[1] += c.d[1];
+  fg[0] += c.d[2];
+  fg[1] += c.d[2];
+  fg[2] += 2.0 * c.d[2];
 }
 
 }  // namespace pgxc

@@ -153,15 +153,23 @@ class Context:
 
 
 def xc_functionals(xc, rho, gam=None):
-    rho = np.ascontiguousarray(rho, dtype=np.float64)
+    """Point functional on the device.  Closed shell: rho (n,), gam (n,) or
+    None -> f, fr, fg of shape (n,).  Open shell: rho (n, 2), gam (n, 3) =
+    (aa, bb, ab) or None -> f (n,), fr (n, 2), fg (n, 3)."""
+    rho = np.asarray(rho, dtype=np.float64)
+    ispin = 2 if rho.ndim == 2 else 1
     n = len(rho)
-    g = np.ascontiguousarray(gam, dtype=np.float64) if gam is not None else None
+    ng = 2 * ispin - 1
+    r = np.ascontiguousarray(rho.reshape(n, ispin).T).reshape(-1)
+    g = None if gam is None else np.ascontiguousarray(np.asarray(gam, dtype=np.float64).reshape(n, ng).T).reshape(-1)
     f = np.zeros(n)
-    fr = np.zeros(n)
-    fg = np.zeros(n) if g is not None else None
-    _check(lib().pgxc_xc_functionals(abi.XC_IDS[xc], 1, n, abi.f64p(rho), abi.f64p(g), abi.f64p(f), abi.f64p(fr),
+    fr = np.zeros(n * ispin)
+    fg = np.zeros(n * ng) if g is not None else None
+    _check(lib().pgxc_xc_functionals(abi.XC_IDS[xc], ispin, n, abi.f64p(r), abi.f64p(g), abi.f64p(f), abi.f64p(fr),
                                      abi.f64p(fg)))
-    return f, fr, fg
+    if ispin == 1:
+        return f, fr, fg
+    return f, fr.reshape(ispin, n).T, None if fg is None else fg.reshape(ng, n).T
 
 
 def becke_weights(case):

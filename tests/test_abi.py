@@ -88,8 +88,12 @@ def test_rejects_high_l_and_nonfinite(case):
     assert _create(bad)[0] == abi.PGXC_EINVAL
 
 
-def test_open_shell_is_reported_unsupported(case):
-    assert _create(case, ispin=2)[0] == abi.PGXC_ENOTSUP
+def test_open_shell_needs_the_screened_layout(case):
+    """ispin=2 is built by the screened layout only; the dense layout
+    (screen_threshold < 0) reports it unsupported before touching a device."""
+    st, msg = _create(case, ispin=2, screen_threshold=-1.0)
+    assert st == abi.PGXC_ENOTSUP and "screened" in msg
+    assert _create(case, ispin=2)[0] != abi.PGXC_ENOTSUP
 
 
 @pytest.mark.skipif(gpu_available(), reason="checks the no-device path")

@@ -1,0 +1,157 @@
+"""Open-shell (ispin = 2) GPU builds against the FP64 CPU oracle.
+
+The screened layout builds both spins: one basis evaluation per chunk, a
+density contraction per spin, one pass of the spin-polarised functional
+(Slater and PBE exchange spin-scaled, VWN5 or PW92 + PBE correlation of
+(rho_a, rho_b) and |grad rho_a + grad rho_b|^2) and a potential contraction
+per spin, packed with the spin stride of ham_xc_arr
+(modules/xc_hamiltonian.f90:1018-1034, :1559-1566).
+
+Bars as for the closed shell: 1e-10 for FP64, 1e-7 for the INT8 build.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from pgxc import cases, lib
+from conftest import fg_tolerance
+
+pytestmark = pytest.mark.gpu
+
+XA = 0.75 * (3 / np.pi) ** (1 / 3)
+
+
+def _spin_points(n, seed):
+    """rho (n, 2) and gam (n, 3) over many decades, with polarised and
+    one-spin-empty points and |gam_ab| <= sqrt(gam_aa gam_bb)."""
+    rng = np.random.default_rng(seed)
+    ra = 10 ** rng.uniform(-12, 3, n)
+    zeta = rng.uniform(-1, 1, n)
+    zeta[: n // 10] = 1.0          # beta empty
+    zeta[n // 10: n // 5] = -1.0   # alpha empty
+    rb = ra * (1 - zeta) / (1 + zeta + 1e-300)
+    rb[: n // 10] = 0.0
+    ra[n // 10: n // 5] = 0.0
+    rb[n // 10: n // 5] = 10 ** rng.uniform(-12, 3, n // 5 - n // 10)
+    gaa = np.where(ra > 0, ra ** (8 / 3) * 10 ** rng.uniform(-6, 2, n), 0.0)
+    gbb = np.where(rb > 0, rb ** (8 / 3) * 10 ** rng.uniform(-6, 2, n), 0.0)
+    gab = rng.uniform(-1, 1, n) * np.sqrt(gaa * gbb)
+    rho = np.stack([ra, rb], 1)
+    gam = np.stack([gaa, gbb, gab], 1)
+    rho = np.concatenate([np.zeros((2, 2)), [[1e-30, 0.0]], rho])
+    gam = np.concatenate([np.zeros((3, 3)), gam])
+    return rho, gam
+
+
+@pytest.mark.parametrize("xc", ["VWN", "PBE"])
+def test_point_functionals_open_shell(xc):
+    rho, gam = _spin_points(600, 5)
+    f, fr, fg = lib.xc_functionals(xc, rho, gam if xc == "PBE" else None)
+    rf, rfr, rfg = O.functionals(xc, 2, rho, gam)
+    # measured against the size of the spin-scaled Slater term (see the closed-shell test)
+    rt = rho.sum(1)
+    well = rt >= 1e-10
+    sf = XA * (rho[:, 0] ** (4 / 3) + rho[:, 1] ** (4 / 3)) * 2 ** (1 / 3)
+    sr = XA * rt ** (1 / 3)
+    tol_f = np.where(well, 1e-12 * (np.abs(rf) + sf), 1e-8 * np.abs(rf) + 1e-40)
+    assert np.all(np.abs(f - rf) <= tol_f), np.max(np.abs(f - rf) / tol_f)
+    for s in range(2):
+        tol_r = np.where(well, 1e-11 * (np.abs(rfr[:, s]) + sr), 1e-5 * np.abs(rfr[:, s]) + 1e-16)
+        err = np.abs(fr[:, s] - rfr[:, s])
+        assert np.all(err <= tol_r), (s, np.max(err / tol_r))
+    if xc == "PBE":
+        # error of each df/dgamma measured by what it contributes to the
+        # energy density, |d fg| gamma_scale <= 1e-10 (|f| + |e_x|)
+        gs = gam[:, 0] + gam[:, 1] + 2 * np.abs(gam[:, 2])
+        for k in range(3):
+            err = np.abs(fg[:, k] - rfg[:, k])
+            tol = 1e-10 * np.abs(rfg[:, k]) + np.where(gs > 0, 1e-10 * (np.abs(rf) + sf) / np.maximum(gs, 1e-300), 0)
+            tol = np.where(well, tol, np.inf)
+            assert np.all(err <= tol + 1e-300), (k, np.max(err / (tol + 1e-300)))
+
+
+def test_point_functionals_equal_spins_match_closed_shell():
+    rng = np.random.default_rng(3)
+    rho = 10 ** rng.uniform(-8, 3, 300)
+    gam = rho ** (8 / 3) * 10 ** rng.uniform(-4, 2, 300)
+    for xc in ("VWN", "PBE"):
+        f1, fr1, fg1 = lib.xc_functionals(xc, rho, gam if xc == "PBE" else None)
+        f2, fr2, fg2 = lib.xc_functionals(xc, np.stack([rho / 2, rho / 2], 1),
+                                          np.stack([gam / 4] * 3, 1) if xc == "PBE" else None)
+        np.testing.assert_allclose(f2, f1, rtol=1e-12)
+        # the closed-shell outputs are 1-D
+        np.testing.assert_allclose(fr2[:, 0], fr1, rtol=1e-10)
+        np.testing.assert_allclose(fr2[:, 1], fr1, rtol=1e-10)
+        if xc == "PBE":
+            fsum = (fg2[:, 0] + fg2[:, 1] + fg2[:, 2]) / 4
+            assert np.all(np.abs(fsum - fg1) <= fg_tolerance(rho, gam, f1, fg1))
+
+
+def _build(case, **kw):
+    with lib.Context(case, **kw) as ctx:
+        return ctx.build()
+
+
+def _compare(case, **kw):
+    ref_ham, ref_exc, ref_nel = O.xc_build(case)
+    ham, exc, nel = _build(case, **kw)
+    return abs(exc - ref_exc), abs(nel - ref_nel), float(np.max(np.abs(ham - ref_ham)))
+
+
+BUILDS = pytest.mark.parametrize("precision,thr,tol", [("fp64", 0.0, 1e-10), ("mixed", 0.0, 1e-7),
+                                                       ("mixed", 1e-10, 1e-7)],
+                                 ids=["fp64", "int8-exact", "int8-1e-10"])
+
+
+@BUILDS
+@pytest.mark.parametrize("xc,seed,lmax", [("VWN", 1, 2), ("PBE", 2, 2), ("PBE", 3, 3), ("VWN", 4, 3)])
+def test_open_shell_build(xc, seed, lmax, precision, thr, tol):
+    c = cases.small_case(functional=xc, seed=seed, lmax=lmax, natoms=5, nocc=7, ispin=2)
+    O.weight_case(c)
+    dE, dN, dV = _compare(c, precision=precision, screen_threshold=thr, max_chunk_points=1024)
+    print(f"open shell {xc} {precision} {thr}: |dE|={dE:.2e} |dN|={dN:.2e} max|dV|={dV:.2e}")
+    assert dE < tol and dN < tol and dV < tol, (dE, dN, dV)
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-12), ("mixed", 1e-8)])
+@pytest.mark.parametrize("xc", ["VWN", "PBE"])
+def test_equal_spins_reproduce_closed_shell(xc, precision, tol):
+    """ispin = 2 with identical alpha and beta orbitals of occupation 1 gives
+    the ispin = 1 build (occupation 2) in both spin blocks."""
+    c = cases.small_case(functional=xc, seed=31)
+    O.weight_case(c)
+    h1, e1, n1 = _build(c, precision=precision)
+    c.ispin = 2
+    c.C = np.concatenate([c.C, c.C], axis=2)
+    c.occ = np.ones((c.nocc, 2))
+    h2, e2, n2 = _build(c, precision=precision)
+    assert abs(e1 - e2) < tol and abs(n1 - n2) < tol
+    np.testing.assert_allclose(h2[0::2], h1, atol=tol)
+    np.testing.assert_allclose(h2[1::2], h1, atol=tol)
+
+
+def test_open_shell_device_pointers_match_host_build():
+    torch = pytest.importorskip("torch")
+    c = cases.small_case(functional="PBE", seed=12, ispin=2)
+    O.weight_case(c)
+    with lib.Context(c, screen_threshold=0.0) as ctx:
+        h, e, n = ctx.build()
+        dC = torch.from_numpy(c.c_fortran()).cuda()
+        docc = torch.from_numpy(c.occ_fortran()).cuda()
+        dham = torch.zeros(c.xc_length, dtype=torch.float64, device="cuda")
+        dsum = torch.zeros(2, dtype=torch.float64, device="cuda")
+        ctx.build_device(dC.data_ptr(), docc.data_ptr(), dham.data_ptr(), dsum.data_ptr())
+        torch.cuda.synchronize()
+    np.testing.assert_allclose(dham.cpu().numpy(), h, atol=1e-13)
+    assert abs(float(dsum[0]) - e) < 1e-13 and abs(float(dsum[1]) - n) < 1e-13
+
+
+def test_open_shell_empty_beta():
+    """No beta electrons: the beta density is zero everywhere; the alpha block
+    and the beta potential (a functional derivative at rho_b = 0) still match."""
+    c = cases.small_case(functional="PBE", seed=14, ispin=2)
+    c.occ = c.occ.copy()
+    c.occ[:, 1] = 0.0
+    O.weight_case(c)
+    dE, dN, dV = _compare(c, screen_threshold=0.0)
+    assert dE < 1e-10 and dN < 1e-10 and dV < 1e-10, (dE, dN, dV)

@@ -13,6 +13,7 @@ import pytest
 
 import oracle as O
 from pgxc import cases, lib
+from conftest import fg_tolerance
 
 pytestmark = pytest.mark.gpu
 
@@ -103,20 +104,6 @@ def test_point_functionals(xc):
     assert np.all(np.abs(fr - rfr[:, 0]) <= tol_r), np.max(np.abs(fr - rfr[:, 0]) / tol_r)
     if xc == "PBE":
         assert np.all(np.abs(fg - rfg[:, 0]) <= fg_tolerance(rho, gam, rf, rfg[:, 0]))
-
-
-def fg_tolerance(rho, gam, rf, rfg):
-    """Tolerance for df/dgamma.  Exchange and correlation gradient terms cancel
-    by construction as s -> 0 (mu = beta pi^2/3), so the scale is the size of
-    the exchange term |e_x| mu s2_fact / rho^(8/3), capped by what matters for
-    the energy density, (|f| + |e_x|) / gamma."""
-    xa = 0.75 * (3 / np.pi) ** (1 / 3)
-    with np.errstate(divide="ignore", invalid="ignore"):
-        ex = xa * rho ** (4 / 3)
-        s2g = 1.0 / (4 * (3 * np.pi ** 2) ** (2 / 3)) / rho ** (8 / 3)
-        sx = np.where(rho > 0, ex * 0.2195164512208958 * s2g, 0.0)
-        se = np.where(gam > 0, (np.abs(rf) + ex) / gam, np.inf)
-    return 1e-10 * (np.abs(rfg) + np.minimum(sx, se)) + 1e-300
 
 
 def test_orbital_values_and_gradients():
