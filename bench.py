@@ -211,7 +211,8 @@ def fp64_comparison(torch, case, sub, local, args):
     out = {"ham": dham.cpu().numpy(), "exc": float(dsum[0]), "nel": float(dsum[1]), "ms": ms,
            "value": case.npts / (ms * 1e-3)}
     ctx.close()
-    if args.screen >= 0:
+    # the unscreened build costs 4 N nbas^2 flop: time it only where that is seconds
+    if args.screen >= 0 and 4.0 * case.npts * case.nbas ** 2 < 2e14:
         ctx = lib.Context(sub, precision="fp64", weighted=False, device=local,
                           max_chunk_points=args.max_chunk_points, screen_threshold=-1.0)
         step()
@@ -391,7 +392,7 @@ def main():
         traffic = None
         tf = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tf):
-            traffic = json.load(open(tf)).get(f"{prec}:{case.functional}:{args.screen:g}")
+            traffic = json.load(open(tf)).get(f"{case.name}:{prec}:{args.screen:g}")
         roof = {"bound": "hbm", "kernel": "density: X = phi_sig P_sig with fused rho, grad rho "
                                           + ("(k_sm_density, tcgen05 kind::i8)" if prec != "fp64" else
                                              "(k_sdensity, DMMA)" if screen is not None else "(k_density, DMMA)"),
