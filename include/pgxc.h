@@ -194,6 +194,31 @@ int pgxc_build_device(pgxc_ctx* ctx, const double* d_C, const double* d_occ,
                       double* d_ham_xc_arr, int64_t xc_length,
                       double* d_exc_nel, pgxc_timings* timings);
 
+/*
+ * Batched builds of many small systems (a set of molecules, each with its own
+ * context).  pgxc_batch_create captures the device build of every context
+ * (as pgxc_build_device, with the device operands given here) as one parallel
+ * branch of a single CUDA graph; pgxc_batch_run replays the graph, so that
+ * the builds of all systems run with one launch: concurrently for FP64
+ * contexts; one after another when the batch holds an INT8 context (the INT8
+ * kernels are not yet safe beside other kernels on the GPU).  Each context
+ * must use the screened layout (screen_threshold >= 0) and the same device;
+ * a context belongs to at most one live batch and must not be built by other
+ * calls while its batch runs.  Operand pointers are fixed for the life of
+ * the batch; their contents may change between runs.  nocc[i] is the
+ * occupied-orbital count of context i; d_ham[i] (packed, xc_length of the
+ * context) and d_exc_nel[i] ({E_xc, N_el}) are overwritten by every run.
+ * pgxc_batch_run synchronises and returns the graph's device time in *ms
+ * (may be NULL).  No counterpart in the reference (one system per process).
+ */
+typedef struct pgxc_batch pgxc_batch;
+int pgxc_batch_create(pgxc_ctx* const* ctx, int32_t n, const double* const* d_C, const double* const* d_occ,
+                      const int32_t* nocc, double* const* d_ham, double* const* d_exc_nel, pgxc_batch** out);
+int pgxc_batch_run(pgxc_batch* batch, double* ms);
+/* Nodes of the batch's CUDA graph: kernel launches and all nodes. */
+int pgxc_batch_stats(const pgxc_batch* batch, int64_t* kernel_nodes, int64_t* nodes);
+void pgxc_batch_destroy(pgxc_batch* batch);
+
 /* Copy of the grid weights the context integrates with (Becke-scaled). */
 int pgxc_grid_weights(const pgxc_ctx* ctx, double* w_out, int64_t npts);
 

@@ -282,25 +282,49 @@ __global__ void __launch_bounds__(128) k_basis_l(const DevShell* __restrict__ sh
 }
 
 // ---------------------------------------------------------------------------
-// K1 (screened): one block per work item = the significant radial functions
-// of one shell on the 128 points of one tile.  Rows are slots of the chunk's
-// compact [slot][128] arrays (slot - s0); with pmax, the largest |phi| of
-// each point of the chunk (tile - t0) is max-reduced into it.
+// K1 (screened): a work item is the significant radial functions of one shell
+// on the 128 points of one tile.  Rows are slots of the chunk's compact
+// [slot][128] arrays (slot - s0); with pmax, the largest |phi| of each point
+// of the chunk (tile - t0) is max-reduced into it.
+//
+// An item carries every field its evaluation needs (atom position, primitive
+// and contraction offsets), so that the loads of the next items do not depend
+// on one another.  A block walks a contiguous range of items; each warp keeps
+// the item records lane-distributed (lane k holds 32-bit word k) two items
+// ahead, and the current item's exponents and norms in lanes (lane e holds
+// primitive e), broadcast with shuffles.  Consecutive items of a tile reuse
+// the point coordinates.
 // ---------------------------------------------------------------------------
 struct BasisItem {
-  int tile;                 // global tile index
-  int shell;
-  int64_t slot;             // global slot of the shell's first significant function
-  int nsig;                 // popcount(mask)
-  int pad_;
-  unsigned long long mask;  // significant radial functions of the shell
+  double ax, ay, az;        // words 0-5: atom position
+  int64_t slot;             // 6-7: global slot of the shell's first significant function
+  unsigned long long mask;  // 8-9: significant radial functions of the shell
+  int tile;                 // 10: global tile index
+  int nsig;                 // 11: popcount(mask)
+  int exp_off;              // 12: into exponents / norms
+  int con_off;              // 13: into contractions (nexp x ncontr column-major)
+  int rad_off;              // 14: into the radial-range table (seg shells)
+  int nexp;                 // 15
+  int nunc;                 // 16
+  int seg;                  // 17
+  int pad_[2];
 };
+static_assert(sizeof(BasisItem) == 80, "BasisItem is read as 20 words");
+constexpr int kItemWords = 20;
+
+__device__ __forceinline__ int item_i(unsigned w, int k) { return (int)__shfl_sync(0xffffffffu, w, k); }
+__device__ __forceinline__ double item_d(unsigned w, int k) {
+  const unsigned lo = __shfl_sync(0xffffffffu, w, k), hi = __shfl_sync(0xffffffffu, w, k + 1);
+  return __hiloint2double((int)hi, (int)lo);
+}
+__device__ __forceinline__ unsigned long long item_u64(unsigned w, int k) {
+  const unsigned lo = __shfl_sync(0xffffffffu, w, k), hi = __shfl_sync(0xffffffffu, w, k + 1);
+  return ((unsigned long long)hi << 32) | lo;
+}
 
 template <int L, bool GRAD>
-__global__ void __launch_bounds__(128) k_basis_items(const BasisItem* __restrict__ items,
-                                                     const DevShell* __restrict__ shells,
-                                                     const double* __restrict__ atoms, const double* __restrict__ exps,
-                                                     const double* __restrict__ norms,
+__global__ void __launch_bounds__(128) k_basis_items(const BasisItem* __restrict__ items, int64_t nitems,
+                                                     const double* __restrict__ exps, const double* __restrict__ norms,
                                                      const double* __restrict__ contr,
                                                      const int2* __restrict__ rng, DevSA sa,
                                                      const double* __restrict__ qx, const double* __restrict__ qy,
@@ -308,19 +332,162 @@ __global__ void __launch_bounds__(128) k_basis_items(const BasisItem* __restrict
                                                      double* __restrict__ phi, double* __restrict__ gx,
                                                      double* __restrict__ gy, double* __restrict__ gz,
                                                      unsigned long long* __restrict__ pmax) {
-  __shared__ ShellStage st;
-  const BasisItem it = items[blockIdx.x];
-  DevShell S = shells[it.shell];
-  const bool staged = stage_shell(st, S, exps, norms, contr, rng);
-  const int64_t q = (int64_t)it.tile * 128 + threadIdx.x;
-  const double x = qx[q] - atoms[3 * S.atom];
-  const double y = qy[q] - atoms[3 * S.atom + 1];
-  const double z = qz[q] - atoms[3 * S.atom + 2];
-  double vmax = 0.0;
-  shell_at_point<L, GRAD>(S, sa, x, y, z, staged ? st.e : exps, staged ? st.n : norms, staged ? st.c : contr, st.r,
-                          true, it.mask, it.slot - s0, it.nsig, threadIdx.x, 128, phi, gx, gy, gz, vmax);
-  // largest |phi| of each point over the tile's functions (non-negative doubles order like their bits)
-  if (pmax) atomicMax(pmax + ((int64_t)it.tile - t0) * 128 + threadIdx.x, (unsigned long long)__double_as_longlong(vmax));
+  const int lane = threadIdx.x & 31;
+  const int64_t per = (nitems + gridDim.x - 1) / gridDim.x;
+  const int64_t i0 = (int64_t)blockIdx.x * per, i1 = min(nitems, i0 + per);
+  if (i0 >= i1) return;
+  const unsigned* words = reinterpret_cast<const unsigned*>(items);
+  auto load_item = [&](int64_t i) -> unsigned {
+    return lane < kItemWords ? __ldg(words + min(i, i1 - 1) * kItemWords + lane) : 0u;
+  };
+  unsigned wc = load_item(i0), wn = load_item(i0 + 1);
+  int nexp = item_i(wc, 15), eoff = item_i(wc, 12);
+  double pe = 0.0, pn = 0.0;  // lane e: exponent and norm of primitive e of the current item
+  if (lane < nexp) { pe = __ldg(exps + eoff + lane); pn = __ldg(norms + eoff + lane); }
+  int tile = item_i(wc, 10);
+  double px = __ldg(qx + (int64_t)tile * 128 + threadIdx.x);
+  double py = __ldg(qy + (int64_t)tile * 128 + threadIdx.x);
+  double pz = __ldg(qz + (int64_t)tile * 128 + threadIdx.x);
+  double tmax = 0.0;
+  for (int64_t i = i0; i < i1; ++i) {
+    // loads for the next items, issued ahead of this item's arithmetic
+    const unsigned wnn = load_item(i + 2);
+    const int n_nexp = item_i(wn, 15), n_eoff = item_i(wn, 12), n_tile = item_i(wn, 10);
+    double ne = 0.0, nn = 0.0;
+    if (lane < n_nexp) { ne = __ldg(exps + n_eoff + lane); nn = __ldg(norms + n_eoff + lane); }
+    double nx = px, ny = py, nz = pz;
+    if (n_tile != tile) {
+      const int64_t qn = (int64_t)n_tile * 128 + threadIdx.x;
+      nx = __ldg(qx + qn); ny = __ldg(qy + qn); nz = __ldg(qz + qn);
+    }
+    // this item
+    {
+      const double x = px - item_d(wc, 0), y = py - item_d(wc, 2), z = pz - item_d(wc, 4);
+      const int64_t base = (int64_t)item_u64(wc, 6) - s0;
+      const uint64_t mask = item_u64(wc, 8);
+      const int nsel = item_i(wc, 11), coff = item_i(wc, 13), roff = item_i(wc, 14), nunc = item_i(wc, 16);
+      const bool seg = item_i(wc, 17) != 0;
+      double Y[16];
+      double dY[3][16];
+      solid_harmonics<L, double>(x, y, z, Y, dY);
+      const double r2 = x * x + y * y + z * z;
+      double Ys[2 * L + 1], dYs[3][2 * L + 1];
+#pragma unroll
+      for (int k = 0; k < 2 * L + 1; ++k) {
+        if (sa.identity) {
+          Ys[k] = Y[L * L + k];
+#pragma unroll
+          for (int c = 0; c < 3; ++c) dYs[c][k] = dY[c][L * L + k];
+        } else {
+          double v = 0, g0 = 0, g1 = 0, g2 = 0;
+#pragma unroll
+          for (int m = 0; m < 2 * L + 1; ++m) {
+            const double cf = sa.c[L][k][m];
+            v += cf * Y[L * L + m];
+            g0 += cf * dY[0][L * L + m];
+            g1 += cf * dY[1][L * L + m];
+            g2 += cf * dY[2][L * L + m];
+          }
+          Ys[k] = v; dYs[0][k] = g0; dYs[1][k] = g1; dYs[2][k] = g2;
+        }
+      }
+      // primitive e's exponent and norm: from lane e, or memory past 32 primitives
+      auto prim = [&](int e, double& alpha, double& nrm) {
+        if (e < 32) {
+          alpha = __shfl_sync(0xffffffffu, pe, e);
+          nrm = __shfl_sync(0xffffffffu, pn, e);
+        } else {
+          alpha = __ldg(exps + eoff + e);
+          nrm = __ldg(norms + eoff + e);
+        }
+      };
+      double vmax = 0.0;
+      auto store = [&](int64_t f, double Rv, double dRv, int k) {
+        const int64_t o = f * 128 + threadIdx.x;
+        phi[o] = Ys[k] * Rv;
+        vmax = fmax(vmax, fabs(Ys[k] * Rv));
+        if (GRAD) {
+          const double h = Ys[k] * dRv;
+          gx[o] = x * h + dYs[0][k] * Rv;
+          gy[o] = y * h + dYs[1][k] * Rv;
+          gz[o] = z * h + dYs[2][k] * Rv;
+        }
+      };
+      if (seg) {
+        // segmented contractions: each selected radial function sums only its own primitives
+        uint64_t rem = mask;
+        for (int k = 0; k < nsel; ++k) {
+          const int rr = __ffsll((long long)rem) - 1;
+          rem &= rem - 1;
+          const int2 rg = __ldg(rng + roff + rr);
+          double Rr = 0.0, dR = 0.0;
+          for (int e = rg.x; e < rg.y; ++e) {
+            double alpha, nrm;
+            prim(e, alpha, nrm);
+            const double v = prim_value(alpha, nrm, r2);
+            const double cf = __ldg(contr + coff + e + (int64_t)nexp * rr);
+            Rr += cf * v;
+            dR += cf * ((-2.0 * alpha) * v);
+          }
+#pragma unroll
+          for (int k2 = 0; k2 < 2 * L + 1; ++k2) store(base + (int64_t)k2 * nsel + k, Rr, dR, k2);
+        }
+      } else {
+        uint64_t rem = mask;
+        for (int k0 = 0; k0 < nsel; k0 += kRadGroup) {
+          int rr[kRadGroup];
+#pragma unroll
+          for (int r = 0; r < kRadGroup; ++r) {
+            if (k0 + r < nsel) {
+              rr[r] = __ffsll((long long)rem) - 1;
+              rem &= rem - 1;
+            } else {
+              rr[r] = -1;
+            }
+          }
+          double Rr[kRadGroup], dR[kRadGroup];
+#pragma unroll
+          for (int r = 0; r < kRadGroup; ++r) { Rr[r] = 0.0; dR[r] = 0.0; }
+          for (int e = 0; e < nexp; ++e) {
+            double alpha, nrm;
+            prim(e, alpha, nrm);
+            const double v = prim_value(alpha, nrm, r2);
+            const double dv = (-2.0 * alpha) * v;
+#pragma unroll
+            for (int r = 0; r < kRadGroup; ++r) {
+              if (rr[r] >= 0) {
+                const double cf = rr[r] < nunc ? (e == rr[r] ? 1.0 : 0.0)
+                                               : __ldg(contr + coff + e + (int64_t)nexp * (rr[r] - nunc));
+                Rr[r] += cf * v;
+                dR[r] += cf * dv;
+              }
+            }
+          }
+#pragma unroll
+          for (int k = 0; k < 2 * L + 1; ++k) {
+#pragma unroll
+            for (int r = 0; r < kRadGroup; ++r)
+              if (rr[r] >= 0) store(base + (int64_t)k * nsel + k0 + r, Rr[r], dR[r], k);
+          }
+        }
+      }
+      // largest |phi| of each point over the tile's functions, max-reduced once per run of
+      // items of one tile (non-negative doubles order like their bits)
+      tmax = fmax(tmax, vmax);
+      if (pmax && (n_tile != tile || i + 1 == i1)) {
+        atomicMax(pmax + ((int64_t)tile - t0) * 128 + threadIdx.x, (unsigned long long)__double_as_longlong(tmax));
+        tmax = 0.0;
+      }
+    }
+    wc = wn;
+    wn = wnn;
+    nexp = n_nexp;
+    eoff = n_eoff;
+    pe = ne;
+    pn = nn;
+    tile = n_tile;
+    px = nx; py = ny; pz = nz;
+  }
 }
 
 }  // namespace pgxc

@@ -58,11 +58,12 @@ __global__ void __launch_bounds__(128) k_becke(const double* __restrict__ atoms,
       double mu;
       if (k < i) mu = __ddiv_rn(__dsub_rn(ri, rk), __ldg(dist + k * natm + i));
       else mu = -__ddiv_rn(__dsub_rn(rk, ri), __ldg(dist + i * natm + k));
-      // mu0(mu, 0) = p(p(p(mu))), p(q) = q (3 - q^2) / 2
+      // mu0(mu, 0) = p(p(p(mu))), p(q) = q (3 - q^2) / 2; the halvings are
+      // multiplications by 0.5, which round exactly as the divisions by 2 do
       double q = mu;
 #pragma unroll
-      for (int it = 0; it < 3; ++it) q = __ddiv_rn(__dmul_rn(q, __dsub_rn(3.0, __dmul_rn(q, q))), 2.0);
-      P = __dmul_rn(P, __ddiv_rn(__dsub_rn(1.0, q), 2.0));
+      for (int it = 0; it < 3; ++it) q = __dmul_rn(__dmul_rn(q, __dsub_rn(3.0, __dmul_rn(q, q))), 0.5);
+      P = __dmul_rn(P, __dmul_rn(__dsub_rn(1.0, q), 0.5));
     }
     sum = __dadd_rn(sum, P);
     if (i == a) pa = P;

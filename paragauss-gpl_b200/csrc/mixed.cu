@@ -255,6 +255,8 @@ __device__ __forceinline__ void oz_read16(uint32_t trow, int c0, double (&x)[16]
   for (int g = 0; g < kGroups; ++g) tc::tmem_ld16(trow + g * kRowsB + c0, v[g]);
   tc::tmem_ld_wait();
 #pragma unroll
+  for (int g = 0; g < kGroups; ++g) tc::tmem_regs_ready(v[g]);
+#pragma unroll
   for (int j = 0; j < 16; ++j) {
     long long acc = 0;
 #pragma unroll
@@ -339,7 +341,7 @@ __global__ void __launch_bounds__(kDensThreads, 1)
     const int ea = e_pt[p];
     const double rs = pow2(ea + kCombShift);  // row scale, applied once per term
     for (int nb = 0; nb < nnb; ++nb) {
-      if (!tc::mbar_wait(&S.acc_full, nb & 1)) {
+      if (!tc::mbar_wait_warp(&S.acc_full, nb & 1)) {
         ok = false;
         break;
       }
@@ -506,7 +508,7 @@ __global__ void __launch_bounds__(kVThreads, 1)
       if (!ok) atomicExch(err, 1);
     }
   } else {
-    const bool done = tc::mbar_wait(&S.acc_full, 0);
+    const bool done = tc::mbar_wait_warp(&S.acc_full, 0);
     if (!done) atomicExch(err, 1);
     tc::fence_after_sync();
     if (done && total > 0) {

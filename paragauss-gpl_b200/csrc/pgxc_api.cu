@@ -705,6 +705,180 @@ int pgxc_build_device(pgxc_ctx* c, const double* d_C, const double* d_occ, int32
   return PGXC_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Batched builds: the device builds of many screened contexts captured as the
+// parallel branches of one CUDA graph.
+// ---------------------------------------------------------------------------
+
+// Enqueue the device build of a screened context on its stream without any
+// synchronisation, event timing or host read (capturable): operands from
+// device memory, the packed matrix and {E_xc, N_el} overwritten into d_ham,
+// d_exc_nel.
+static int enqueue_screened_build(pgxc_ctx* c, const double* d_C, const double* d_occ, int32_t nocc, double* d_ham,
+                                  double* d_exc_nel) {
+  BuildArgs& a = c->a;
+  cudaStream_t s = c->stream;
+  const int64_t kpad = round_up(std::max(nocc, 1), 16);
+  int st = upload_orbitals(c, d_C, d_occ, (int32_t)c->nbas, nocc, kpad, cudaMemcpyDeviceToDevice);
+  if (st) return st;
+  CUDA_TRY(c, cudaMemsetAsync(a.acc, 0, 4 * sizeof(double), s));
+  launch_pmat_f64(a, kpad, s);
+  if (c->opt.ispin == 2) {
+    BuildArgs b = a;
+    b.C = c->C2;
+    b.occ = c->occ2;
+    b.P = c->P2;
+    launch_pmat_f64(b, kpad, s);
+  }
+  CUDA_TRY(c, cudaGetLastError());
+  std::string e;
+  if ((st = screen_run(c->screen, a, c->P2, s, c->d_ham, nullptr, e))) return set_err(c, st, e);
+  const int64_t len = (int64_t)c->opt.ispin * c->nbas * (c->nbas + 1) / 2;
+  CUDA_TRY(c, cudaMemcpyAsync(d_ham, c->d_ham, sizeof(double) * len, cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(c, cudaMemcpyAsync(d_exc_nel, a.acc, sizeof(double), cudaMemcpyDeviceToDevice, s));
+  CUDA_TRY(c, cudaMemcpyAsync(d_exc_nel + 1, a.acc + 2, sizeof(double), cudaMemcpyDeviceToDevice, s));
+  return PGXC_OK;
+}
+
+struct pgxc_batch {
+  std::vector<pgxc_ctx*> ctx;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+void pgxc_batch_destroy(pgxc_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (cudaEvent_t e : b->join)
+    if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : {b->fork, b->t0, b->t1})
+    if (e) cudaEventDestroy(e);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+int pgxc_batch_create(pgxc_ctx* const* ctx, int32_t n, const double* const* d_C, const double* const* d_occ,
+                      const int32_t* nocc, double* const* d_ham, double* const* d_exc_nel, pgxc_batch** out) {
+  if (!out) return set_err(nullptr, PGXC_EINVAL, "out is NULL");
+  *out = nullptr;
+  if (!ctx || n <= 0 || !d_C || !d_occ || !nocc || !d_ham || !d_exc_nel)
+    return set_err(nullptr, PGXC_EINVAL, "batch: NULL array or n <= 0");
+  std::vector<pgxc_ctx*> seen;
+  for (int32_t i = 0; i < n; ++i) {
+    pgxc_ctx* c = ctx[i];
+    if (!c) return set_err(nullptr, PGXC_EINVAL, "batch: NULL context");
+    if (!c->screen) return set_err(nullptr, PGXC_ENOTSUP, "batch: every context must use the screened layout");
+    if (c->device != ctx[0]->device) return set_err(nullptr, PGXC_EINVAL, "batch: contexts on different devices");
+    if (nocc[i] < 0 || (nocc[i] > 0 && (!d_C[i] || !d_occ[i])) || !d_ham[i] || !d_exc_nel[i])
+      return set_err(nullptr, PGXC_EINVAL, "batch: bad operand of context " + std::to_string(i));
+    if (std::find(seen.begin(), seen.end(), c) != seen.end())
+      return set_err(nullptr, PGXC_EINVAL, "batch: a context appears twice");
+    seen.push_back(c);
+  }
+  pgxc_batch* b = new pgxc_batch();
+  b->ctx.assign(ctx, ctx + n);
+  b->device = ctx[0]->device;
+  b->join.assign((size_t)n, nullptr);
+  auto fail = [&](int st, const std::string& msg) {
+    pgxc_batch_destroy(b);
+    return set_err(nullptr, st, msg);
+  };
+  cudaError_t ce = cudaSetDevice(b->device);
+  for (int32_t i = 0; i < n && ce == cudaSuccess; ++i) {
+    if (int st = ensure_occ(ctx[i], nocc[i])) return fail(st, "batch: context " + std::to_string(i) + ": " + ctx[i]->err);
+    ce = cudaStreamSynchronize(ctx[i]->stream);  // nothing of the context is pending when the capture starts
+  }
+  if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
+  if (ce == cudaSuccess) ce = cudaEventCreate(&b->t0);
+  if (ce == cudaSuccess) ce = cudaEventCreate(&b->t1);
+  for (int32_t i = 0; i < n && ce == cudaSuccess; ++i) ce = cudaEventCreateWithFlags(&b->join[(size_t)i], cudaEventDisableTiming);
+  if (ce != cudaSuccess) return fail(PGXC_ECUDA, std::string("batch: ") + cudaGetErrorString(ce));
+  // Fork from the batch stream into every context's stream and join back.  The
+  // INT8 density kernel has given wrong rho for some 32-point groups when other
+  // kernels ran beside it on the GPU (sequential builds are exact and
+  // deterministic), so a batch holding an INT8 context chains its builds one
+  // after another inside the graph; FP64 builds run concurrently.
+  bool chain = false;
+  for (int32_t i = 0; i < n; ++i) chain = chain || ctx[i]->opt.precision != PGXC_PREC_FP64;
+  ce = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed);
+  if (ce != cudaSuccess) return fail(PGXC_ECUDA, std::string("batch: begin capture: ") + cudaGetErrorString(ce));
+  int st = PGXC_OK;
+  std::string msg;
+  ce = cudaEventRecord(b->fork, b->stream);
+  for (int32_t i = 0; i < n && ce == cudaSuccess && st == PGXC_OK; ++i) {
+    pgxc_ctx* c = ctx[i];
+    ce = cudaStreamWaitEvent(c->stream, chain && i > 0 ? b->join[(size_t)i - 1] : b->fork, 0);
+    if (ce != cudaSuccess) break;
+    if ((st = enqueue_screened_build(c, d_C[i], d_occ[i], nocc[i], d_ham[i], d_exc_nel[i]))) {
+      msg = "batch: context " + std::to_string(i) + ": " + c->err;
+      break;
+    }
+    ce = cudaEventRecord(b->join[(size_t)i], c->stream);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(b->stream, b->join[(size_t)i], 0);
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t ce_end = cudaStreamEndCapture(b->stream, &g);  // always ends the capture
+  if (st == PGXC_OK && ce == cudaSuccess) ce = ce_end;
+  if (st != PGXC_OK || ce != cudaSuccess) {
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    return fail(st != PGXC_OK ? st : PGXC_ECUDA, st != PGXC_OK ? msg : std::string("batch: capture: ") + cudaGetErrorString(ce));
+  }
+  b->graph = g;
+  ce = cudaGraphInstantiate(&b->exec, g, 0);
+  if (ce != cudaSuccess) return fail(PGXC_ECUDA, std::string("batch: instantiate: ") + cudaGetErrorString(ce));
+  *out = b;
+  return PGXC_OK;
+}
+
+int pgxc_batch_run(pgxc_batch* b, double* ms) {
+  if (!b) return set_err(nullptr, PGXC_EINVAL, "batch is NULL");
+  CUDA_TRY(nullptr, cudaSetDevice(b->device));
+  CUDA_TRY(nullptr, cudaEventRecord(b->t0, b->stream));
+  CUDA_TRY(nullptr, cudaGraphLaunch(b->exec, b->stream));
+  CUDA_TRY(nullptr, cudaEventRecord(b->t1, b->stream));
+  CUDA_TRY(nullptr, cudaEventSynchronize(b->t1));
+  if (ms) {
+    float f = 0;
+    CUDA_TRY(nullptr, cudaEventElapsedTime(&f, b->t0, b->t1));
+    *ms = f;
+  }
+  for (size_t i = 0; i < b->ctx.size(); ++i) {
+    int flag = 0;
+    if (screen_error_flag(b->ctx[i]->screen, b->ctx[i]->stream, &flag) != PGXC_OK)
+      return set_err(nullptr, PGXC_ECUDA, "batch: error-flag read failed");
+    if (flag)
+      return set_err(nullptr, PGXC_ETIMEOUT,
+                     "batch: context " + std::to_string(i) + ": a bounded tensor-core pipeline wait ran out");
+  }
+  return PGXC_OK;
+}
+
+int pgxc_batch_stats(const pgxc_batch* b, int64_t* kernel_nodes, int64_t* nodes) {
+  if (!b || !kernel_nodes || !nodes) return set_err(nullptr, PGXC_EINVAL, "NULL argument");
+  size_t n = 0;
+  CUDA_TRY(nullptr, cudaGraphGetNodes(b->graph, nullptr, &n));
+  std::vector<cudaGraphNode_t> v(n);
+  if (n) CUDA_TRY(nullptr, cudaGraphGetNodes(b->graph, v.data(), &n));
+  int64_t k = 0;
+  for (cudaGraphNode_t node : v) {
+    cudaGraphNodeType t;
+    CUDA_TRY(nullptr, cudaGraphNodeGetType(node, &t));
+    if (t == cudaGraphNodeTypeKernel) ++k;
+  }
+  *kernel_nodes = k;
+  *nodes = (int64_t)n;
+  return PGXC_OK;
+}
+
 int pgxc_grid_weights(const pgxc_ctx* cc, double* w_out, int64_t npts) {
   pgxc_ctx* c = const_cast<pgxc_ctx*>(cc);
   if (!c || !w_out) return set_err(c, PGXC_EINVAL, "NULL argument");

@@ -43,4 +43,17 @@ constexpr int kTile = 64;
 
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
+// Raise, never lower, a kernel's dynamic shared-memory limit.  The limit
+// belongs to the function, shared by every context of the process: a
+// context whose tiles list fewer functions must not undercut the launches of
+// another that are still queued or captured in a graph.
+template <typename Kernel>
+inline cudaError_t raise_smem_limit(Kernel kernel, int bytes) {
+  cudaFuncAttributes fa;
+  cudaError_t e = cudaFuncGetAttributes(&fa, kernel);
+  if (e != cudaSuccess) return e;
+  if (fa.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
 }  // namespace pgxc

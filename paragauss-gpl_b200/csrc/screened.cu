@@ -36,6 +36,7 @@ namespace pgxc {
 
 constexpr int kSlotAlign = 32;   // slots per tile are padded to this (INT8 K step)
 constexpr int64_t kSlack = 128;  // zero rows after the last slot of a chunk
+constexpr int kBasisBlocksPerSM = 16;  // blocks of the basis kernels per SM (each walks a range of items)
 
 struct ScreenPlan {
   int64_t ntiles = 0, nslots = 0, nlisted = 0;
@@ -65,6 +66,7 @@ struct ScreenPlan {
   unsigned long long* pmax = nullptr;  // [chunk_tiles*128] largest |phi| per point (INT8 path)
   ScreenMixed* mixed = nullptr;
   cudaEvent_t ev[12] = {};
+  int nsm = 148;
   std::vector<void*> allocs;
 };
 
@@ -510,6 +512,11 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
       return PGXC_ENOTSUP;
     }
   for (auto& e : sp->ev) SP_TRY(cudaEventCreate(&e), "cudaEventCreate");
+  {
+    int dev = 0;
+    SP_TRY(cudaGetDevice(&dev), "cudaGetDevice");
+    SP_TRY(cudaDeviceGetAttribute(&sp->nsm, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+  }
   // --- Morton-ordered, 128-point tiles -----------------------------------
   const int64_t n = in.npts;
   const int64_t ntiles = (n + 127) / 128;
@@ -585,11 +592,19 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
         if (dd < R2[(size_t)s][(size_t)rr]) mask |= 1ull << rr;
       const int nsig = __builtin_popcountll(mask);
       BasisItem it{};
+      it.ax = in.atoms[3 * S.atom];
+      it.ay = in.atoms[3 * S.atom + 1];
+      it.az = in.atoms[3 * S.atom + 2];
       it.tile = (int)t;
-      it.shell = s;
       it.slot = (int64_t)slot_fn.size();
       it.nsig = nsig;
       it.mask = mask;
+      it.exp_off = S.exp_off;
+      it.con_off = S.con_off;
+      it.rad_off = S.rad_off;
+      it.nexp = S.nexp;
+      it.nunc = S.nunc;
+      it.seg = S.seg;
       items[S.l].push_back(it);
       for (int i = 0; i < 2 * S.l + 1; ++i)
         for (int rr = 0; rr < S.nrad; ++rr)
@@ -717,6 +732,7 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
   const int ispin = sp->ispin;
   const double* P[2] = {a.P, Pb};
   const int64_t nb2 = sp->nbas * sp->nbas;
+  const bool timed = tm != nullptr;  // untimed: no event records, synchronisation or host reads (capturable)
   ScreenTimes T;
   cudaEvent_t* ev = sp->ev;
 #define SR_TRY(call)                                                          \
@@ -729,9 +745,10 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
   } while (0)
   SR_TRY(cudaMemsetAsync(sp->V, 0, sizeof(double) * ispin * nb2, st));
   if (sp->mixed) {
-    SR_TRY(cudaEventRecord(ev[0], st));
+    if (timed) SR_TRY(cudaEventRecord(ev[0], st));
     for (int s = 0; s < ispin; ++s) T.launches += screen_mixed_prepare(sp->mixed, P[s], a.ldc, s, st);
-    SR_TRY(cudaEventRecord(ev[1], st));
+    SR_TRY(cudaGetLastError());
+    if (timed) SR_TRY(cudaEventRecord(ev[1], st));
   }
   const int64_t cp = sp->chunk_tiles * 128;
   // per-chunk point arrays of spin s: 8 columns of cp (rho, grad rho, A, B) from pt + 8 s cp
@@ -757,7 +774,7 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
     const int64_t t0 = sp->chunk_t0[c], t1 = sp->chunk_t0[c + 1], nt = t1 - t0;
     const int64_t s0 = sp->h_tso[(size_t)t0], ns = sp->h_tso[(size_t)t1] - s0;
     const int64_t npt = nt * 128;
-    SR_TRY(cudaEventRecord(ev[2], st));
+    if (timed) SR_TRY(cudaEventRecord(ev[2], st));
     // K1
     if (sp->pmax) SR_TRY(cudaMemsetAsync(sp->pmax, 0, sizeof(unsigned long long) * nt * 128, st));
     {
@@ -765,14 +782,16 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
         constexpr int L = decltype(Lc)::value;
         const int64_t i0 = sp->item_off[L][c], i1 = sp->item_off[L][c + 1];
         if (i1 <= i0) return;
+        // persistent-style blocks, each walking a contiguous range of items
+        const unsigned nb = (unsigned)std::min<int64_t>(i1 - i0, (int64_t)sp->nsm * kBasisBlocksPerSM);
         if (gga)
-          k_basis_items<L, true><<<(unsigned)(i1 - i0), 128, 0, st>>>(
-              sp->items[L] + i0, a.shells, a.atoms, a.exps, a.norms, a.contr, a.rng, a.sa, sp->qx, sp->qy, sp->qz, s0,
-              t0, sp->phi, sp->gx, sp->gy, sp->gz, sp->pmax);
+          k_basis_items<L, true><<<nb, 128, 0, st>>>(sp->items[L] + i0, i1 - i0, a.exps, a.norms, a.contr, a.rng,
+                                                     a.sa, sp->qx, sp->qy, sp->qz, s0, t0, sp->phi, sp->gx, sp->gy,
+                                                     sp->gz, sp->pmax);
         else
-          k_basis_items<L, false><<<(unsigned)(i1 - i0), 128, 0, st>>>(
-              sp->items[L] + i0, a.shells, a.atoms, a.exps, a.norms, a.contr, a.rng, a.sa, sp->qx, sp->qy, sp->qz, s0,
-              t0, sp->phi, nullptr, nullptr, nullptr, sp->pmax);
+          k_basis_items<L, false><<<nb, 128, 0, st>>>(sp->items[L] + i0, i1 - i0, a.exps, a.norms, a.contr, a.rng,
+                                                      a.sa, sp->qx, sp->qy, sp->qz, s0, t0, sp->phi, nullptr,
+                                                      nullptr, nullptr, sp->pmax);
         ++T.launches;
       };
       launch_l(std::integral_constant<int, 0>());
@@ -785,9 +804,9 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
       if (sp->mixed)
         T.launches += screen_mixed_basis(sp->mixed, sp->tso, sp->slot_fn, t0, nt, s0, sp->phi, sp->pmax, st);
     }
-    SR_TRY(cudaEventRecord(ev[3], st));
+    if (timed) SR_TRY(cudaEventRecord(ev[3], st));
     // K3, per spin
-    SR_TRY(cudaEventRecord(ev[4], st));
+    if (timed) SR_TRY(cudaEventRecord(ev[4], st));
     for (int s = 0; s < ispin; ++s) {
       if (sp->mixed) {
         if (s > 0) T.launches += screen_mixed_gather(sp->mixed, sp->tso, sp->slot_fn, t0, nt, s0, s, st);
@@ -797,12 +816,12 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
         const int smem = gemm_smem_bytes<false, false>() + (int)sizeof(int) * sp->max_n;
         dim3 grid((unsigned)nt, 2);
         if (gga) {
-          cudaFuncSetAttribute(k_sdensity<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+          raise_smem_limit(k_sdensity<true>, smem);
           k_sdensity<true><<<grid, kGemmThreads, smem, st>>>(sp->phi, sp->gx, sp->gy, sp->gz, sp->tso, t0, s0,
                                                              sp->slot_fn, P[s], a.ldc, b[s].rho, b[s].grx, b[s].gry,
                                                              b[s].grz);
         } else {
-          cudaFuncSetAttribute(k_sdensity<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+          raise_smem_limit(k_sdensity<false>, smem);
           k_sdensity<false><<<grid, kGemmThreads, smem, st>>>(sp->phi, nullptr, nullptr, nullptr, sp->tso, t0, s0,
                                                               sp->slot_fn, P[s], a.ldc, b[s].rho, nullptr, nullptr,
                                                               nullptr);
@@ -810,7 +829,7 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
         ++T.launches;
       }
     }
-    SR_TRY(cudaEventRecord(ev[5], st));
+    if (timed) SR_TRY(cudaEventRecord(ev[5], st));
     // K2
     if (ispin == 1) {
       BuildArgs bf = b[0];
@@ -820,11 +839,11 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
       launch_functional2_f64(a.xc, sp->qw, b[0].rho, b[1].rho, cp, t0 * 128, npt, gga, sp->partial, a.acc, st);
     }
     T.launches += 2;
-    SR_TRY(cudaEventRecord(ev[6], st));
+    if (timed) SR_TRY(cudaEventRecord(ev[6], st));
     // K4, per spin: the contraction of spin s is bracketed by ev[7 + 3s], ev[8 + 3s]
     for (int s = 0; s < ispin; ++s) {
       double* Vs = sp->V + s * nb2;
-      cudaEvent_t k0 = ev[7 + 3 * s], k1 = ev[8 + 3 * s];
+      cudaEvent_t k0 = timed ? ev[7 + 3 * s] : nullptr, k1 = timed ? ev[8 + 3 * s] : nullptr;
       if (sp->mixed) {
         T.launches += screen_mixed_potential(sp->mixed, sp->tso, sp->slot_fn, sp->slot_tile, t0, nt, s0, ns, sp->phi,
                                              sp->gx, sp->gy, sp->gz, b[s].A, b[s].Bx, b[s].By, b[s].Bz, Vs, sp->nbas,
@@ -837,23 +856,24 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
         else
           k_szbuild<false><<<nbk, 256, 0, st>>>(ns, sp->slot_tile + s0, t0, sp->phi, nullptr, nullptr, nullptr,
                                                 b[s].A, nullptr, nullptr, nullptr, sp->Z);
-        SR_TRY(cudaEventRecord(k0, st));
+        if (timed) SR_TRY(cudaEventRecord(k0, st));
         const int smem = gemm_smem_bytes<true, true>() + (int)sizeof(int) * sp->max_n;
         dim3 grid((unsigned)nt, 4);
         if (gga) {
-          cudaFuncSetAttribute(k_svpot<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+          raise_smem_limit(k_svpot<true>, smem);
           k_svpot<true><<<grid, kGemmThreads, smem, st>>>(sp->phi, sp->Z, sp->tso, t0, s0, sp->slot_fn, Vs,
                                                           sp->nbas);
         } else {
-          cudaFuncSetAttribute(k_svpot<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+          raise_smem_limit(k_svpot<false>, smem);
           k_svpot<false><<<grid, kGemmThreads, smem, st>>>(sp->phi, sp->Z, sp->tso, t0, s0, sp->slot_fn, Vs,
                                                            sp->nbas);
         }
-        SR_TRY(cudaEventRecord(k1, st));
+        if (timed) SR_TRY(cudaEventRecord(k1, st));
         T.launches += 2;
       }
     }
     SR_TRY(cudaGetLastError());
+    if (!timed) continue;
     SR_TRY(cudaEventRecord(ev[9], st));
     SR_TRY(cudaEventSynchronize(ev[9]));
     SR_TRY(cudaEventElapsedTime(&ms, ev[2], ev[3])); T.basis += ms;
@@ -865,11 +885,11 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
       T.v += ms;
     }
   }
-  if (sp->mixed) {
+  if (sp->mixed && timed) {
     SR_TRY(cudaEventElapsedTime(&ms, ev[0], ev[1]));
     T.density += ms;
   }
-  SR_TRY(cudaEventRecord(ev[2], st));
+  if (timed) SR_TRY(cudaEventRecord(ev[2], st));
   {
     const int64_t len = sp->nbas * (sp->nbas + 1) / 2;
     const unsigned nbk = (unsigned)std::min<int64_t>((len + 255) / 256, 148 * 8);
@@ -879,6 +899,7 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
     }
   }
   SR_TRY(cudaGetLastError());
+  if (!timed) return PGXC_OK;
   SR_TRY(cudaEventRecord(ev[3], st));
   SR_TRY(cudaEventSynchronize(ev[3]));
   SR_TRY(cudaEventElapsedTime(&ms, ev[2], ev[3]));
@@ -895,8 +916,14 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
     }
   }
 #undef SR_TRY
-  if (tm) *tm = T;
+  *tm = T;
   return PGXC_OK;
+}
+
+int screen_error_flag(ScreenPlan* sp, cudaStream_t st, int* flag) {
+  *flag = 0;
+  if (!sp->mixed) return PGXC_OK;
+  return screen_mixed_error_flag(sp->mixed, st, flag);
 }
 
 }  // namespace pgxc

@@ -54,9 +54,13 @@ void screen_destroy(ScreenPlan* sp);
 // One build: the FP64 density matrices must be ready (a.P; for an open shell
 // also Pb, the second spin's, with the same leading dimension a.ldc); E_xc /
 // N_el are Kahan-added into a.acc; the packed matrix (both spins interleaved
-// for an open shell) is written to ham.
+// for an open shell) is written to ham.  With t == nullptr the build is only
+// enqueued: no event records, synchronisation or host reads, so that it can be
+// captured into a CUDA graph; screen_error_flag then reports a bounded wait
+// of the INT8 kernels that ran out.
 int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_t st, double* ham, ScreenTimes* t,
                std::string& err);
+int screen_error_flag(ScreenPlan* sp, cudaStream_t st, int* flag);
 // Plan statistics: tiles, total slots (padded), listed functions, sum of n_t^2.
 void screen_stats(const ScreenPlan* sp, int64_t* ntiles, int64_t* nslots, int64_t* nlisted, double* sum_n2,
                   int64_t* nchunks);

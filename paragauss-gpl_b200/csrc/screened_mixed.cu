@@ -236,33 +236,37 @@ struct DensSmem {
 // warps 0-7 epilogue, 8 MMA, 9 operand copies, 10 epilogue-operand copies
 constexpr int kDensThreads = 352;
 
-// TMEM -> 16 + 8 combined FP64 values of one accumulator set (columns c0..c0+23)
-__device__ __forceinline__ void read_acc24(uint32_t taddr, double (&x)[24]) {
-  {
-    uint32_t r[kGroups][16];
+// TMEM -> the 24 combined FP64 values of column half `half` of one
+// accumulator set (columns 24 half .. 24 half + 23 of each group; taddr is the
+// set's first column at this warp's lane quarter).  Every load starts at a
+// multiple of its own width: half 0 reads 16 columns at +0 then 8 at +16,
+// half 1 reads 8 at +24 then 16 at +32.
+template <int W>
+__device__ __forceinline__ void acc_cols(uint32_t taddr, double* x) {
+  uint32_t r[kGroups][W];
 #pragma unroll
-    for (int g = 0; g < kGroups; ++g) tc::tmem_ld16u(taddr + g * kN, r[g]);
-    tc::tmem_ld_wait();
-#pragma unroll
-    for (int c = 0; c < 16; ++c) {
-      uint32_t v[kGroups];
-#pragma unroll
-      for (int g = 0; g < kGroups; ++g) v[g] = r[g][c];
-      x[c] = oz_combine(v);
-    }
+  for (int g = 0; g < kGroups; ++g) {
+    if constexpr (W == 16) tc::tmem_ld16u(taddr + g * kN, r[g]);
+    else tc::tmem_ld8(taddr + g * kN, r[g]);
   }
-  {
-    uint32_t r[kGroups][8];
+  tc::tmem_ld_wait();
 #pragma unroll
-    for (int g = 0; g < kGroups; ++g) tc::tmem_ld8(taddr + g * kN + 16, r[g]);
-    tc::tmem_ld_wait();
+  for (int g = 0; g < kGroups; ++g) tc::tmem_regs_ready(r[g]);
 #pragma unroll
-    for (int c = 0; c < 8; ++c) {
-      uint32_t v[kGroups];
+  for (int c = 0; c < W; ++c) {
+    uint32_t v[kGroups];
 #pragma unroll
-      for (int g = 0; g < kGroups; ++g) v[g] = r[g][c];
-      x[16 + c] = oz_combine(v);
-    }
+    for (int g = 0; g < kGroups; ++g) v[g] = r[g][c];
+    x[c] = oz_combine(v);
+  }
+}
+__device__ __forceinline__ void read_acc24(uint32_t taddr, int half, double (&x)[24]) {
+  if (half == 0) {
+    acc_cols<16>(taddr, x);
+    acc_cols<8>(taddr + 16, x + 16);
+  } else {
+    acc_cols<8>(taddr + 24, x);
+    acc_cols<16>(taddr + 32, x + 8);
   }
 }
 
@@ -390,7 +394,7 @@ __global__ void __launch_bounds__(kDensThreads, 1)
     }
   } else {  // epilogue: point row = 32 (warp & 3) + lane, columns 24 (warp >> 2) .. +24 of each slot block
     const int row = (warp & 3) * 32 + lane, half = warp >> 2;
-    const uint32_t trow = tbase + ((uint32_t)((warp & 3) * 32) << 16) + half * 24;
+    const uint32_t trow = tbase + ((uint32_t)((warp & 3) * 32) << 16);
     int jj = 0;
     for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
       const int64_t sg = tso[t0 + ti];
@@ -404,13 +408,13 @@ __global__ void __launch_bounds__(kDensThreads, 1)
         // the P row scale of column lane (< 24) of this warp's half, broadcast below
         const int cl = j * kN + half * 24 + lane;
         const double psl = (lane < 24 && cl < n) ? __ldg(ps + sb + cl) : 0.0;
-        if (!tc::mbar_wait(&S.acc_full[b], (jj >> 1) & 1)) {
+        if (!tc::mbar_wait_warp(&S.acc_full[b], (jj >> 1) & 1)) {
           ok = false;
           break;
         }
         tc::fence_after_sync();
         double x[24];
-        read_acc24(trow + b * kAccCols, x);
+        read_acc24(trow + b * kAccCols, half, x);
         tc::fence_before_sync();
         tc::mbar_arrive(&S.acc_empty[b]);
 #pragma unroll
@@ -673,7 +677,7 @@ __global__ void __launch_bounds__(kVThreads, 1)
     }
   } else {  // epilogue: column j = 128 J + 32 (warp & 3) + lane of H, rows 24 (warp >> 2) .. of each 48-slot block
     const int half = warp >> 2;
-    const uint32_t trow = tbase + ((uint32_t)((warp & 3) * 32) << 16) + half * 24;
+    const uint32_t trow = tbase + ((uint32_t)((warp & 3) * 32) << 16);
     int pp = 0;
     for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
       const int64_t sg = tso[t0 + ti];
@@ -691,13 +695,13 @@ __global__ void __launch_bounds__(kVThreads, 1)
           const int il = I * kN + half * 24 + lane;
           const int fil = (lane < 24 && il < n) ? __ldg(sfn + il) : -1;
           const double zsl = (lane < 24 && il < n) ? __ldg(zs + sb + il) : 0.0;
-          if (!tc::mbar_wait(&S.acc_full[b], (pp >> 1) & 1)) {
+          if (!tc::mbar_wait_warp(&S.acc_full[b], (pp >> 1) & 1)) {
             ok = false;
             break;
           }
           tc::fence_after_sync();
           double x[24];
-          read_acc24(trow + b * kAccCols, x);
+          read_acc24(trow + b * kAccCols, half, x);
           tc::fence_before_sync();
           tc::mbar_arrive(&S.acc_empty[b]);
 #pragma unroll
@@ -760,7 +764,7 @@ int screen_mixed_create(ScreenMixed** out, const ScreenMixedInput& in, std::stri
     return e == cudaErrorMemoryAllocation ? PGXC_ENOMEM : PGXC_ECUDA;
   }
   const int dsm = (int)sizeof(DensSmem);
-  cudaFuncSetAttribute(k_sm_gather_B, cudaFuncAttributeMaxDynamicSharedMemorySize, 4 * in.max_n);
+  raise_smem_limit(k_sm_gather_B, 4 * in.max_n);
   cudaFuncSetAttribute(k_sm_density<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm);
   cudaFuncSetAttribute(k_sm_density<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm);
   cudaFuncSetAttribute(k_sm_vpot<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(VSmem));
@@ -837,7 +841,7 @@ int screen_mixed_potential(ScreenMixed* m, const int64_t* tso, const int* slot_f
   else
     k_sm_zquant<false><<<(unsigned)nt, 256, 0, st>>>(tso, t0, s0, phi, nullptr, nullptr, nullptr, A, nullptr,
                                                      nullptr, nullptr, m->tZ, m->tF, m->zs, m->fs);
-  cudaEventRecord(k0, st);
+  if (k0) cudaEventRecord(k0, st);
   const unsigned grid = (unsigned)std::min<int64_t>(nt, m->nsm);
   if (m->gga)
     k_sm_vpot<true><<<grid, kVThreads, (int)sizeof(VSmem), st>>>(tso, slot_fn, t0, nt, s0, m->tF, m->tZ, m->fs, m->zs, V, ldv,
@@ -845,7 +849,7 @@ int screen_mixed_potential(ScreenMixed* m, const int64_t* tso, const int* slot_f
   else
     k_sm_vpot<false><<<grid, kVThreads, (int)sizeof(VSmem), st>>>(tso, slot_fn, t0, nt, s0, m->tF, m->tZ, m->fs, m->zs, V, ldv,
                                                     m->err);
-  cudaEventRecord(k1, st);
+  if (k1) cudaEventRecord(k1, st);
   return 2;
 }
 

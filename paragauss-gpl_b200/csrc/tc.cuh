@@ -101,6 +101,21 @@ __device__ __forceinline__ void tmem_ld16u(uint32_t taddr, uint32_t (&r)[16]) {
       : "r"(taddr));
 }
 __device__ __forceinline__ void tmem_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// tcgen05.ld writes its registers asynchronously: they hold the data only
+// after tcgen05.wait::ld, but nothing in the wait names them, so the compiler
+// may schedule their first uses before it.  An empty asm that reads and
+// rewrites each register, placed after the wait, makes every later use depend
+// on it (volatile asm statements keep their order).
+template <int N>
+__device__ __forceinline__ void tmem_regs_ready(uint32_t (&r)[N]) {
+#pragma unroll
+  for (int i = 0; i < N; ++i) asm volatile("" : "+r"(r[i]));
+}
+template <int N>
+__device__ __forceinline__ void tmem_regs_ready(float (&r)[N]) {
+#pragma unroll
+  for (int i = 0; i < N; ++i) asm volatile("" : "+f"(r[i]));
+}
 
 // ---- mbarrier ---------------------------------------------------------------
 __device__ __forceinline__ void mbar_init(uint64_t* mbar, uint32_t count) {
@@ -144,6 +159,16 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t parity) {
     if (ok) return true;
   }
   return false;
+}
+
+// The same wait by every thread of a warp, returning the warp's common verdict
+// with the warp converged.  The threads of a warp leave the spin loop at
+// different polls; the .sync.aligned tcgen05 instructions that follow a wait
+// (tcgen05.ld, tcgen05.wait::ld) must be executed by the whole warp together.
+__device__ __forceinline__ bool mbar_wait_warp(uint64_t* mbar, uint32_t parity) {
+  const bool ok = __all_sync(0xffffffffu, mbar_wait(mbar, parity));
+  __syncwarp();
+  return ok;
 }
 
 }  // namespace tc

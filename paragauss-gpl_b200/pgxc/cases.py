@@ -251,6 +251,31 @@ def build_case(name, els, xyz, *, seed, exp_range, nrad, nang, functional, nocc,
     return case
 
 
+def molecule_set(n=256, seed=1004, functional=None, atoms=(3, 40)):
+    """The batched workload: n seeded molecules of 3-40 C/H/O atoms (sizes drawn
+    uniform; 40% C, 40% H, 20% O), each in a cube holding the 60-atom cluster's
+    atom density, with the default basis (20-400 functions), 50-75 radial x
+    194- or 302-class angular points per atom, and nocc = half the electron
+    count.  The functional alternates VWN / PBE unless one is given; atoms is
+    the inclusive range of molecule sizes.  C is
+    scaled normal noise (not orthonormalised) to keep the set cheap to make."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for m in range(n):
+        nat = int(rng.integers(atoms[0], atoms[1] + 1))
+        kinds = rng.choice(["C", "H", "O"], size=nat, p=[0.4, 0.4, 0.2])
+        counts = [(el, int(np.sum(kinds == el))) for el in ("C", "H", "O")]
+        box = max(2.5, (nat / 0.035) ** (1.0 / 3.0))
+        els, xyz = random_cluster(rng, counts, box, 1.0)
+        nrad = int(rng.integers(50, 76))
+        nang = 194 if rng.random() < 0.5 else 302
+        xc = functional or ("VWN" if m % 2 == 0 else "PBE")
+        nocc = max(1, sum(Z_OF[e] for e in els) // 2)
+        out.append(build_case(f"mol{m}-{xc}", els, xyz, seed=seed * 1000 + m, exp_range=(0.1, 5e3), nrad=nrad,
+                              nang=nang, functional=xc, nocc=nocc, orthonormalise=False))
+    return out
+
+
 def config(n, **kw):
     """The seeded workloads: 1 water VWN, 2 60-atom C/H PBE, 5 500-atom PBE."""
     if n == 1:

@@ -48,6 +48,10 @@ def lib():
     L.pgxc_strerror.argtypes = [ct.c_int]
     L.pgxc_strerror.restype = ct.c_char_p
     L.pgxc_destroy.argtypes = [vp]
+    L.pgxc_batch_create.argtypes = [P(vp), ct.c_int32, P(vp), P(vp), P(ct.c_int32), P(vp), P(vp), P(vp)]
+    L.pgxc_batch_run.argtypes = [vp, P(ct.c_double)]
+    L.pgxc_batch_destroy.argtypes = [vp]
+    L.pgxc_batch_stats.argtypes = [vp, P(ct.c_int64), P(ct.c_int64)]
     _LIB = L
     return L
 
@@ -149,6 +153,47 @@ class Context:
         return self
 
     def __exit__(self, *a):
+        self.close()
+
+
+class Batch:
+    """Device builds of many screened contexts replayed as one CUDA graph
+    (pgxc_batch_create / pgxc_batch_run).  Per context the operands are device
+    pointers (ints): C and occ in the pgxc_build_device layout, the packed V
+    and {E_xc, N_el} outputs (overwritten by every run)."""
+
+    def __init__(self, contexts, d_C, d_occ, d_ham, d_exc_nel):
+        n = len(contexts)
+        arr = lambda xs: (ct.c_void_p * n)(*[ct.c_void_p(int(x)) for x in xs])
+        self.contexts = list(contexts)  # kept alive while the batch exists
+        self._args = (arr([c.h.value for c in contexts]), arr(d_C), arr(d_occ),
+                      (ct.c_int32 * n)(*[c.case.nocc for c in contexts]), arr(d_ham), arr(d_exc_nel))
+        h = ct.c_void_p()
+        a = self._args
+        _check(lib().pgxc_batch_create(a[0], n, a[1], a[2], a[3], a[4], a[5], ct.byref(h)))
+        self.h = h
+
+    def run(self):
+        """One replay of every build; returns its device time in ms."""
+        ms = ct.c_double()
+        _check(lib().pgxc_batch_run(self.h, ct.byref(ms)))
+        return ms.value
+
+    def stats(self):
+        """{kernel_nodes, nodes} of the batch's CUDA graph."""
+        k, n = ct.c_int64(), ct.c_int64()
+        _check(lib().pgxc_batch_stats(self.h, ct.byref(k), ct.byref(n)))
+        return dict(kernel_nodes=k.value, nodes=n.value)
+
+    def close(self):
+        if self.h:
+            lib().pgxc_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
         self.close()
 
 
