@@ -238,9 +238,7 @@ constexpr int kDensThreads = 352;
 
 // TMEM -> the 24 combined FP64 values of column half `half` of one
 // accumulator set (columns 24 half .. 24 half + 23 of each group; taddr is the
-// set's first column at this warp's lane quarter).  Every load starts at a
-// multiple of its own width: half 0 reads 16 columns at +0 then 8 at +16,
-// half 1 reads 8 at +24 then 16 at +32.
+// set's first column at this warp's lane quarter): 16 columns, then 8.
 template <int W>
 __device__ __forceinline__ void acc_cols(uint32_t taddr, double* x) {
   uint32_t r[kGroups][W];
@@ -261,13 +259,8 @@ __device__ __forceinline__ void acc_cols(uint32_t taddr, double* x) {
   }
 }
 __device__ __forceinline__ void read_acc24(uint32_t taddr, int half, double (&x)[24]) {
-  if (half == 0) {
-    acc_cols<16>(taddr, x);
-    acc_cols<8>(taddr + 16, x + 16);
-  } else {
-    acc_cols<8>(taddr + 24, x);
-    acc_cols<16>(taddr + 32, x + 8);
-  }
+  acc_cols<16>(taddr + half * 24, x);
+  acc_cols<8>(taddr + half * 24 + 16, x + 16);
 }
 
 // Persistent: CTA c takes the chunk's tiles c, c + G, c + 2G, ... (G = grid

@@ -70,6 +70,17 @@ def test_device_becke_matches_oracle():
     np.testing.assert_allclose(w_gpu, w_ref, rtol=0, atol=2e-16)
 
 
+def test_device_becke_many_atoms_bit_identical():
+    """72 atoms, 25,200 points: the device weights are the oracle's bit for bit."""
+    rng = np.random.default_rng(21)
+    els, xyz = cases.random_cluster(rng, [("C", 36), ("H", 36)], 13.0, 1.1)
+    c = cases.build_case("becke72", els, xyz, seed=21, exp_range=(0.1, 100.0), nrad=8, nang=50,
+                         functional="VWN", nocc=1, orthonormalise=False)
+    w_gpu = lib.becke_weights(c)
+    w_ref = O.becke(c)
+    assert np.array_equal(w_gpu, w_ref), float(np.max(np.abs(w_gpu - w_ref)))
+
+
 @LAYOUTS
 def test_raw_weight_grid_is_becke_scaled_on_device(thr):
     c = cases.small_case(functional="PBE", seed=9)
