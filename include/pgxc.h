@@ -183,6 +183,19 @@ int pgxc_build(pgxc_ctx* ctx, const double* C, const double* occ,
                double* exc, double* nel, pgxc_timings* timings);
 
 /*
+ * Same build from the density matrix itself, for callers that form P
+ * (P_s = sum_j occ_js C_js C_js^T per spin) themselves:
+ *   P : nbas x nbas per spin, column-major, spin blocks of nbas*nbas,
+ *       symmetric (host memory).
+ * ham_xc_arr, exc and nel are accumulated into exactly as by pgxc_build.
+ * Replaces the occupied-orbital products of density_calc_nl
+ * (modules/density_calc_module.f90:1498-1538) by the P form of the same rho.
+ */
+int pgxc_build_density(pgxc_ctx* ctx, const double* P, int32_t nbas, int32_t ispin,
+                       double* ham_xc_arr, int64_t xc_length,
+                       double* exc, double* nel, pgxc_timings* timings);
+
+/*
  * Same build with every operand already in device memory of the context's
  * device (for callers that keep C on the GPU).  d_exc_nel receives
  * {E_xc, N_el} (overwritten, not accumulated); d_ham_xc_arr is overwritten

@@ -648,6 +648,25 @@ int mixed_prepare(MixedState* m, const BuildArgs& a, int nocc, cudaStream_t st) 
   return 3;
 }
 
+// A density matrix given by the caller (ldc x ldc, nbas x nbas used) -> the padded copy.
+__global__ void k_oz_copy_P(const double* __restrict__ Pin, int64_t ldc, int64_t nbas, int64_t ldk,
+                            double* __restrict__ P) {
+  const int64_t i = (int64_t)blockIdx.y * 16 + threadIdx.y, j = (int64_t)blockIdx.x * 16 + threadIdx.x;
+  if (i >= ldk || j >= ldk) return;
+  P[i * ldk + j] = (i < nbas && j < nbas) ? Pin[i * ldc + j] : 0.0;
+}
+
+int mixed_prepare_P(MixedState* m, const double* P, int64_t ldc, cudaStream_t st) {
+  dim3 b2(16, 16), g2((unsigned)(m->ldk / 16), (unsigned)(m->ldk / 16));
+  k_oz_copy_P<<<g2, b2, 0, st>>>(P, ldc, m->nbas, m->ldk, m->P);
+  k_oz_rowexp_P<<<(unsigned)m->ldk, 256, 0, st>>>(m->P, m->ldk, m->e_P);
+  const int nks = (int)(m->ldk / kKStep);
+  k_oz_quant_P<<<dim3((unsigned)(m->ldk / kRowsB), (unsigned)nks), kRowsB, 0, st>>>(m->P, m->ldk, m->e_P, nks,
+                                                                                  m->tB1);
+  cudaMemsetAsync(m->vpart, 0, sizeof(double) * m->nsplit * m->ntiles * kRowsA * kRowsB, st);
+  return 3;
+}
+
 int mixed_basis(MixedState* m, const BuildArgs& a, int64_t p0, int64_t nvalid, bool gga, cudaStream_t st) {
   launch_basis(a, a.px, a.py, a.pz, p0, nvalid, m->ldp, m->phi, gga ? m->gx : nullptr, m->gy, m->gz, st);
   const int nksf = (int)(m->ldk / kKStep);

@@ -19,6 +19,8 @@ void mixed_destroy(MixedState* m);
 int64_t mixed_row_align();
 // Each launcher returns the number of kernels it launched.
 int mixed_prepare(MixedState* m, const BuildArgs& a, int nocc, cudaStream_t st);
+// the same from a density matrix P given in device memory (ldc x ldc)
+int mixed_prepare_P(MixedState* m, const double* P, int64_t ldc, cudaStream_t st);
 // copies the device error flag (set by a bounded wait that ran out) to *flag and clears it
 int mixed_error_flag(MixedState* m, cudaStream_t st, int* flag);
 int mixed_basis(MixedState* m, const BuildArgs& a, int64_t p0, int64_t nvalid, bool gga, cudaStream_t st);

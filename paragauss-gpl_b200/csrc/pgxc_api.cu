@@ -512,7 +512,8 @@ static int upload_orbitals(pgxc_ctx* c, const double* C, const double* occ, int3
 }
 
 // The device part of a build; C / occ already in a.C / a.occ (padded).
-static int run_build(pgxc_ctx* c, int nocc, pgxc_timings* tm) {
+// p_given: the density matrices are already in a.P (and P2), written by the caller's P.
+static int run_build(pgxc_ctx* c, int nocc, pgxc_timings* tm, bool p_given = false) {
   BuildArgs& a = c->a;
   cudaStream_t s = c->stream;
   const bool gga = c->opt.functional == PGXC_XC_PBE;
@@ -520,8 +521,8 @@ static int run_build(pgxc_ctx* c, int nocc, pgxc_timings* tm) {
   if (c->screen) {
     CUDA_TRY(c, cudaMemsetAsync(a.acc, 0, 4 * sizeof(double), s));
     CUDA_TRY(c, cudaEventRecord(c->ev[1], s));
-    launch_pmat_f64(a, kpad, s);
-    if (c->opt.ispin == 2) {
+    if (!p_given) launch_pmat_f64(a, kpad, s);
+    if (c->opt.ispin == 2 && !p_given) {
       BuildArgs b = a;  // second spin: its orbitals and occupations into P2 (Cocc is scratch)
       b.C = c->C2;
       b.occ = c->occ2;
@@ -543,7 +544,7 @@ static int run_build(pgxc_ctx* c, int nocc, pgxc_timings* tm) {
       tm->potential_ms = T.potential;
       tm->xgemm_ms = T.x;
       tm->vgemm_ms = T.v;
-      tm->kernel_launches = T.launches + 2 * c->opt.ispin;
+      tm->kernel_launches = T.launches + (p_given ? 0 : 2 * c->opt.ispin);
     }
     return PGXC_OK;
   }
@@ -553,8 +554,8 @@ static int run_build(pgxc_ctx* c, int nocc, pgxc_timings* tm) {
   CUDA_TRY(c, cudaMemsetAsync(a.vpart, 0, sizeof(double) * a.nsplit * a.ntiles * kTile * kTile, s));
   CUDA_TRY(c, cudaEventRecord(c->ev[1], s));
   if (c->mixed) {
-    launches += mixed_prepare(c->mixed, a, nocc, s);
-  } else {
+    launches += p_given ? mixed_prepare_P(c->mixed, a.P, a.ldc, s) : mixed_prepare(c->mixed, a, nocc, s);
+  } else if (!p_given) {
     launch_pmat_f64(a, kpad, s);
     launches += 2;
   }
@@ -631,6 +632,9 @@ static int check_build_args(pgxc_ctx* c, int32_t nbas, int32_t nocc, int32_t isp
   return PGXC_OK;
 }
 
+static int host_build_tail(pgxc_ctx* c, int nocc, bool p_given, double* ham, int64_t xc_length, double* exc,
+                           double* nel, pgxc_timings* tm);
+
 int pgxc_build(pgxc_ctx* c, const double* C, const double* occ, int32_t nbas, int32_t nocc, int32_t ispin,
                double* ham, int64_t xc_length, double* exc, double* nel, pgxc_timings* tm) {
   if (!c) return set_err(nullptr, PGXC_EINVAL, "ctx is NULL");
@@ -641,17 +645,26 @@ int pgxc_build(pgxc_ctx* c, const double* C, const double* occ, int32_t nbas, in
     return set_err(c, PGXC_ENONFINITE, "non-finite C or occ");
   CUDA_TRY(c, cudaSetDevice(c->device));
   if ((st = ensure_occ(c, nocc))) return st;
+  const int64_t kpad = round_up(std::max(nocc, 1), 16);
+  CUDA_TRY(c, cudaEventRecord(c->ev[0], c->stream));
+  if ((st = upload_orbitals(c, C, occ, nbas, nocc, kpad, cudaMemcpyHostToDevice))) return st;
+  return host_build_tail(c, nocc, false, ham, xc_length, exc, nel, tm);
+}
+
+// The rest of a host-buffer build whose inputs were enqueued after c->ev[0]:
+// the device build, the D2H of the packed matrix and of the two sums, added
+// into the caller's arrays.
+static int host_build_tail(pgxc_ctx* c, int nocc, bool p_given, double* ham, int64_t xc_length, double* exc,
+                           double* nel, pgxc_timings* tm) {
   BuildArgs& a = c->a;
   cudaStream_t s = c->stream;
-  const int64_t kpad = round_up(std::max(nocc, 1), 16);
-  CUDA_TRY(c, cudaEventRecord(c->ev[0], s));
-  if ((st = upload_orbitals(c, C, occ, nbas, nocc, kpad, cudaMemcpyHostToDevice))) return st;
+  int st;
   CUDA_TRY(c, cudaEventRecord(c->ev[1], s));
   CUDA_TRY(c, cudaEventSynchronize(c->ev[1]));
   float h2d = 0;
   CUDA_TRY(c, cudaEventElapsedTime(&h2d, c->ev[0], c->ev[1]));
   pgxc_timings local{};
-  if ((st = run_build(c, nocc, &local))) return st;
+  if ((st = run_build(c, nocc, &local, p_given))) return st;
   // D2H of the packed matrix and the two sums
   cudaEvent_t e0 = c->ev[5], e1 = c->ev[6];
   CUDA_TRY(c, cudaEventRecord(e0, s));
@@ -674,6 +687,26 @@ int pgxc_build(pgxc_ctx* c, const double* C, const double* occ, int32_t nbas, in
     tm->total_ms = tot;
   }
   return PGXC_OK;
+}
+
+int pgxc_build_density(pgxc_ctx* c, const double* P, int32_t nbas, int32_t ispin, double* ham, int64_t xc_length,
+                       double* exc, double* nel, pgxc_timings* tm) {
+  if (!c) return set_err(nullptr, PGXC_EINVAL, "ctx is NULL");
+  int st = check_build_args(c, nbas, 0, ispin, xc_length);
+  if (st) return st;
+  if (!P || !ham || !exc || !nel) return set_err(c, PGXC_EINVAL, "NULL output/input");
+  if (!all_finite(P, (int64_t)ispin * nbas * nbas)) return set_err(c, PGXC_ENONFINITE, "non-finite P");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  BuildArgs& a = c->a;
+  cudaStream_t s = c->stream;
+  CUDA_TRY(c, cudaEventRecord(c->ev[0], s));
+  for (int sp = 0; sp < ispin; ++sp) {
+    double* dP = sp ? c->P2 : a.P;
+    CUDA_TRY(c, cudaMemsetAsync(dP, 0, sizeof(double) * a.ldc * a.ldc, s));
+    CUDA_TRY(c, cudaMemcpy2DAsync(dP, sizeof(double) * a.ldc, P + (size_t)sp * nbas * nbas, sizeof(double) * nbas,
+                                  sizeof(double) * nbas, nbas, cudaMemcpyHostToDevice, s));
+  }
+  return host_build_tail(c, 0, true, ham, xc_length, exc, nel, tm);
 }
 
 int pgxc_build_device(pgxc_ctx* c, const double* d_C, const double* d_occ, int32_t nbas, int32_t nocc, int32_t ispin,

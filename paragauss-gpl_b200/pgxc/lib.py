@@ -38,6 +38,8 @@ def lib():
                              P(ct.c_double), P(ct.c_double), P(abi.Timings)]
     L.pgxc_build_device.argtypes = [vp, vp, vp, ct.c_int32, ct.c_int32, ct.c_int32, vp, ct.c_int64, vp,
                                     P(abi.Timings)]
+    L.pgxc_build_density.argtypes = [vp, abi._f64p, ct.c_int32, ct.c_int32, abi._f64p, ct.c_int64, P(ct.c_double),
+                                     P(ct.c_double), P(abi.Timings)]
     L.pgxc_grid_weights.argtypes = [vp, abi._f64p, ct.c_int64]
     L.pgxc_orbital_calculate.argtypes = [vp, ct.c_int64, abi._f64p, abi._f64p, abi._f64p]
     L.pgxc_xc_functionals.argtypes = [ct.c_int32, ct.c_int32, ct.c_int64, abi._f64p, abi._f64p, abi._f64p,
@@ -104,6 +106,19 @@ class Context:
         _check(st, self.h)
         if timings:
             return ham, exc.value, nel.value, tm.as_dict()
+        return ham, exc.value, nel.value
+
+    def build_density(self, P, ham=None):
+        """Build from density matrices P (ispin, nbas, nbas); returns (ham_xc_arr, exc, nel)."""
+        c = self.case
+        Pf = np.ascontiguousarray(np.asarray(P, dtype=np.float64).reshape(c.ispin, c.nbas, c.nbas)).reshape(-1)
+        if ham is None:
+            ham = np.zeros(c.xc_length)
+        exc = ct.c_double(0.0)
+        nel = ct.c_double(0.0)
+        tm = abi.Timings()
+        _check(lib().pgxc_build_density(self.h, abi.f64p(Pf), c.nbas, c.ispin, abi.f64p(ham), c.xc_length,
+                                        ct.byref(exc), ct.byref(nel), ct.byref(tm)), self.h)
         return ham, exc.value, nel.value
 
     def build_device(self, d_C, d_occ, d_ham, d_exc_nel):

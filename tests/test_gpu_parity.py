@@ -170,3 +170,32 @@ def test_ch60_pbe_threshold_1e10():
     print(f"CH60 PBE thr=1e-10: |dE|={dE:.2e} |dN|={dN:.2e} max|dV|={dV:.2e} "
           f"listed/tile={st['nlisted'] / st['ntiles']:.1f} work={frac:.3f} of dense")
     assert dE < 1e-8 and dN < 1e-8 and dV < 1e-8, (dE, dN, dV)
+
+
+@pytest.mark.parametrize("precision,thr,tol", [("fp64", -1.0, 1e-12), ("fp64", 0.0, 1e-12), ("mixed", -1.0, 1e-9),
+                                               ("mixed", 1e-10, 1e-9)],
+                         ids=["fp64-dense", "fp64-screened", "int8-dense", "int8-screened"])
+def test_build_from_density_matrix(precision, thr, tol):
+    """pgxc_build_density with P = C diag(occ) C^T gives the pgxc_build result
+    (P formed on the host here, on the device there: they differ in rounding
+    only), and accumulates into the caller's arrays the same way."""
+    c = cases.small_case(functional="PBE", seed=15, lmax=3)
+    O.weight_case(c)
+    with lib.Context(c, precision=precision, screen_threshold=thr) as ctx:
+        h1, e1, n1 = ctx.build()
+        h2, e2, n2 = ctx.build_density(c.density_matrix(), ham=np.full(c.xc_length, 0.5))
+    assert abs(e2 - e1) < tol and abs(n2 - n1) < tol, (e2 - e1, n2 - n1)
+    np.testing.assert_allclose(h2 - 0.5, h1, atol=tol)
+    ref_ham, ref_exc, ref_nel = O.xc_build(c)
+    bar = TOL if precision == "fp64" else 1e-7
+    assert abs(e2 - ref_exc) < bar and np.max(np.abs(h2 - 0.5 - ref_ham)) < bar
+
+
+def test_build_from_density_matrix_open_shell():
+    c = cases.small_case(functional="VWN", seed=16, ispin=2)
+    O.weight_case(c)
+    with lib.Context(c, screen_threshold=0.0) as ctx:
+        h1, e1, n1 = ctx.build()
+        h2, e2, n2 = ctx.build_density(c.density_matrix())
+    assert abs(e2 - e1) < 1e-12 and abs(n2 - n1) < 1e-12
+    np.testing.assert_allclose(h2, h1, atol=1e-12)
