@@ -118,6 +118,14 @@ typedef struct pgxc_options {
                                   *         bound stays below the threshold on the tile;
                                   *   <0 -> no screening (dense layout) */
   int32_t device;                /* CUDA ordinal, -1 -> current device      */
+  int32_t keep_orbitals;         /* screened layout: keep the basis values (and
+                                  * their INT8 digits) of the whole grid on the
+                                  * device after the first build and reuse them
+                                  * in later builds of the same geometry, as the
+                                  * reference's orbitals_in_memory does
+                                  * (orbitalstore_module.f90); 0 -> evaluate in
+                                  * every build.  Creation fails with
+                                  * PGXC_ENOMEM when they do not fit. */
   int64_t max_chunk_points;      /* 0 -> sized from free HBM                */
 } pgxc_options;
 

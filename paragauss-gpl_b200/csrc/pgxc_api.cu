@@ -116,6 +116,7 @@ void pgxc_default_options(pgxc_options* o) {
   o->batch_points = 128;
   o->screen_threshold = 0.0;
   o->device = -1;
+  o->keep_orbitals = 0;
   o->max_chunk_points = 0;
 }
 
@@ -390,6 +391,7 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
     in.gga = gga;
     in.ispin = o.ispin;
     in.precision = o.precision;
+    in.keep_basis = o.keep_orbitals != 0;
     in.max_chunk_points = o.max_chunk_points;
     std::string e;
     st = screen_create(&c->screen, in, a, c->stream, e);

@@ -45,6 +45,8 @@ struct ScreenPlan {
   bool gga = false;
   int ispin = 1;
   int64_t nbas = 0;
+  bool keep = false;         // basis values (and INT8 point digits) of all slots stay resident
+  bool basis_ready = false;  // ... and a completed build has filled them
   // device, whole grid
   double *qx = nullptr, *qy = nullptr, *qz = nullptr, *qw = nullptr;  // Morton-ordered points [ntiles*128]
   int64_t* tso = nullptr;   // [ntiles+1] first slot of each tile
@@ -504,6 +506,7 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
   sp->gga = in.gga;
   sp->ispin = in.ispin;
   sp->nbas = in.nbas;
+  sp->keep = in.keep_basis;
   const std::vector<DevShell>& shells = *in.shells;
   for (const DevShell& S : shells)
     if (S.nrad > 64) {
@@ -627,6 +630,17 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
   const bool mixed = in.precision != PGXC_PREC_FP64;
   size_t freeb = 0, totb = 0;
   SP_TRY(cudaMemGetInfo(&freeb, &totb), "cudaMemGetInfo");
+  if (sp->keep) {
+    // resident basis values and point digits of every slot: phi (+ grad phi), INT8 digits
+    const double need = (double)(sp->nslots + kSlack) * 128 * (8.0 * (in.gga ? 4 : 1) + (mixed ? 5.0 : 0.0));
+    if (need > 0.6 * (double)freeb) {
+      err = "screened build: the basis values of the whole grid (" + std::to_string((int64_t)(need / 1e9)) +
+            " GB) do not fit beside the build's buffers; create the context without keep_orbitals";
+      screen_destroy(sp);
+      return PGXC_ENOMEM;
+    }
+    freeb -= (size_t)need;
+  }
   const int64_t per_slot = 128 * 8 * (in.gga ? 5 : 2) + (mixed ? screen_mixed_bytes_per_slot() : 0);
   const int64_t per_tile = 128 * 8 * 8 * in.ispin + (mixed ? screen_mixed_bytes_per_tile() : 0);
   int64_t budget_slots = (int64_t)(0.45 * (double)freeb) / per_slot;
@@ -686,17 +700,19 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
              "copy");
   }
   const size_t rows = (size_t)(sp->chunk_slots + kSlack) * 128;
-  SP_TRY(sp_alloc(sp, &sp->phi, rows), "cudaMalloc (phi)");
+  // basis arrays: one chunk's rows, or every slot of the grid when they stay resident
+  const size_t brows = sp->keep ? (size_t)(sp->nslots + kSlack) * 128 : rows;
+  SP_TRY(sp_alloc(sp, &sp->phi, brows), "cudaMalloc (phi)");
   SP_TRY(sp_alloc(sp, &sp->Z, rows), "cudaMalloc (Z)");
-  SP_TRY(cudaMemset(sp->phi, 0, sizeof(double) * rows), "memset");
+  SP_TRY(cudaMemset(sp->phi, 0, sizeof(double) * brows), "memset");
   SP_TRY(cudaMemset(sp->Z, 0, sizeof(double) * rows), "memset");
   if (in.gga) {
-    SP_TRY(sp_alloc(sp, &sp->gx, rows), "cudaMalloc (grad phi)");
-    SP_TRY(sp_alloc(sp, &sp->gy, rows), "cudaMalloc (grad phi)");
-    SP_TRY(sp_alloc(sp, &sp->gz, rows), "cudaMalloc (grad phi)");
-    SP_TRY(cudaMemset(sp->gx, 0, sizeof(double) * rows), "memset");
-    SP_TRY(cudaMemset(sp->gy, 0, sizeof(double) * rows), "memset");
-    SP_TRY(cudaMemset(sp->gz, 0, sizeof(double) * rows), "memset");
+    SP_TRY(sp_alloc(sp, &sp->gx, brows), "cudaMalloc (grad phi)");
+    SP_TRY(sp_alloc(sp, &sp->gy, brows), "cudaMalloc (grad phi)");
+    SP_TRY(sp_alloc(sp, &sp->gz, brows), "cudaMalloc (grad phi)");
+    SP_TRY(cudaMemset(sp->gx, 0, sizeof(double) * brows), "memset");
+    SP_TRY(cudaMemset(sp->gy, 0, sizeof(double) * brows), "memset");
+    SP_TRY(cudaMemset(sp->gz, 0, sizeof(double) * brows), "memset");
   }
   const int64_t cp = sp->chunk_tiles * 128;
   SP_TRY(sp_alloc(sp, &sp->pt, 8 * (size_t)in.ispin * cp), "cudaMalloc");
@@ -712,6 +728,10 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
     mi.chunk_tiles = sp->chunk_tiles;
     mi.max_n = sp->max_n;
     mi.chunk_bstages = chunk_bstages;
+    if (sp->keep) {
+      mi.resident_slots = sp->nslots + kSlack;
+      mi.resident_tiles = sp->ntiles;
+    }
     SP_TRY(sp_alloc(sp, &sp->pmax, (size_t)sp->chunk_tiles * 128), "cudaMalloc");
     SP_TRY(sp_alloc(sp, &sp->b_off, boff.size()), "cudaMalloc");
     SP_TRY(cudaMemcpy(sp->b_off, boff.data(), sizeof(int64_t) * boff.size(), cudaMemcpyHostToDevice), "copy");
@@ -733,6 +753,8 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
   const double* P[2] = {a.P, Pb};
   const int64_t nb2 = sp->nbas * sp->nbas;
   const bool timed = tm != nullptr;  // untimed: no event records, synchronisation or host reads (capturable)
+  // resident basis values filled by an earlier build: skip their evaluation (K1)
+  const bool eval_basis = !(sp->keep && sp->basis_ready);
   ScreenTimes T;
   cudaEvent_t* ev = sp->ev;
 #define SR_TRY(call)                                                          \
@@ -774,10 +796,18 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
     const int64_t t0 = sp->chunk_t0[c], t1 = sp->chunk_t0[c + 1], nt = t1 - t0;
     const int64_t s0 = sp->h_tso[(size_t)t0], ns = sp->h_tso[(size_t)t1] - s0;
     const int64_t npt = nt * 128;
+    // this chunk's rows of the basis arrays (resident: the chunk's place among all slots)
+    const int64_t so = sp->keep ? s0 : 0, to = sp->keep ? t0 : 0;
+    double* phi = sp->phi + so * 128;
+    double* gxc = gga ? sp->gx + so * 128 : nullptr;
+    double* gyc = gga ? sp->gy + so * 128 : nullptr;
+    double* gzc = gga ? sp->gz + so * 128 : nullptr;
     if (timed) SR_TRY(cudaEventRecord(ev[2], st));
     // K1
-    if (sp->pmax) SR_TRY(cudaMemsetAsync(sp->pmax, 0, sizeof(unsigned long long) * nt * 128, st));
-    {
+    if (!eval_basis) {
+      if (sp->mixed) T.launches += screen_mixed_gather(sp->mixed, sp->tso, sp->slot_fn, t0, nt, s0, 0, st);
+    } else {
+      if (sp->pmax) SR_TRY(cudaMemsetAsync(sp->pmax, 0, sizeof(unsigned long long) * nt * 128, st));
       auto launch_l = [&](auto Lc) {
         constexpr int L = decltype(Lc)::value;
         const int64_t i0 = sp->item_off[L][c], i1 = sp->item_off[L][c + 1];
@@ -786,11 +816,10 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
         const unsigned nb = (unsigned)std::min<int64_t>(i1 - i0, (int64_t)sp->nsm * kBasisBlocksPerSM);
         if (gga)
           k_basis_items<L, true><<<nb, 128, 0, st>>>(sp->items[L] + i0, i1 - i0, a.exps, a.norms, a.contr, a.rng,
-                                                     a.sa, sp->qx, sp->qy, sp->qz, s0, t0, sp->phi, sp->gx, sp->gy,
-                                                     sp->gz, sp->pmax);
+                                                     a.sa, sp->qx, sp->qy, sp->qz, s0, t0, phi, gxc, gyc, gzc, sp->pmax);
         else
           k_basis_items<L, false><<<nb, 128, 0, st>>>(sp->items[L] + i0, i1 - i0, a.exps, a.norms, a.contr, a.rng,
-                                                      a.sa, sp->qx, sp->qy, sp->qz, s0, t0, sp->phi, nullptr,
+                                                      a.sa, sp->qx, sp->qy, sp->qz, s0, t0, phi, nullptr,
                                                       nullptr, nullptr, sp->pmax);
         ++T.launches;
       };
@@ -798,11 +827,11 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
       launch_l(std::integral_constant<int, 1>());
       launch_l(std::integral_constant<int, 2>());
       launch_l(std::integral_constant<int, 3>());
-      if (gga) k_pad_zero<true><<<(unsigned)nt, 128, 0, st>>>(sp->tso, sp->listed, t0, s0, sp->phi, sp->gx, sp->gy, sp->gz);
-      else k_pad_zero<false><<<(unsigned)nt, 128, 0, st>>>(sp->tso, sp->listed, t0, s0, sp->phi, nullptr, nullptr, nullptr);
+      if (gga) k_pad_zero<true><<<(unsigned)nt, 128, 0, st>>>(sp->tso, sp->listed, t0, s0, phi, gxc, gyc, gzc);
+      else k_pad_zero<false><<<(unsigned)nt, 128, 0, st>>>(sp->tso, sp->listed, t0, s0, phi, nullptr, nullptr, nullptr);
       ++T.launches;
       if (sp->mixed)
-        T.launches += screen_mixed_basis(sp->mixed, sp->tso, sp->slot_fn, t0, nt, s0, sp->phi, sp->pmax, st);
+        T.launches += screen_mixed_basis(sp->mixed, sp->tso, sp->slot_fn, t0, nt, s0, phi, sp->pmax, so, to, st);
     }
     if (timed) SR_TRY(cudaEventRecord(ev[3], st));
     // K3, per spin
@@ -810,19 +839,19 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
     for (int s = 0; s < ispin; ++s) {
       if (sp->mixed) {
         if (s > 0) T.launches += screen_mixed_gather(sp->mixed, sp->tso, sp->slot_fn, t0, nt, s0, s, st);
-        T.launches += screen_mixed_density(sp->mixed, sp->tso, sp->slot_fn, t0, nt, s0, sp->phi, sp->gx, sp->gy,
-                                           sp->gz, b[s].rho, b[s].grx, b[s].gry, b[s].grz, st);
+        T.launches += screen_mixed_density(sp->mixed, sp->tso, sp->slot_fn, t0, nt, s0, phi, gxc, gyc, gzc,
+                                           b[s].rho, b[s].grx, b[s].gry, b[s].grz, so, to, st);
       } else {
         const int smem = gemm_smem_bytes<false, false>() + (int)sizeof(int) * sp->max_n;
         dim3 grid((unsigned)nt, 2);
         if (gga) {
           raise_smem_limit(k_sdensity<true>, smem);
-          k_sdensity<true><<<grid, kGemmThreads, smem, st>>>(sp->phi, sp->gx, sp->gy, sp->gz, sp->tso, t0, s0,
+          k_sdensity<true><<<grid, kGemmThreads, smem, st>>>(phi, gxc, gyc, gzc, sp->tso, t0, s0,
                                                              sp->slot_fn, P[s], a.ldc, b[s].rho, b[s].grx, b[s].gry,
                                                              b[s].grz);
         } else {
           raise_smem_limit(k_sdensity<false>, smem);
-          k_sdensity<false><<<grid, kGemmThreads, smem, st>>>(sp->phi, nullptr, nullptr, nullptr, sp->tso, t0, s0,
+          k_sdensity<false><<<grid, kGemmThreads, smem, st>>>(phi, nullptr, nullptr, nullptr, sp->tso, t0, s0,
                                                               sp->slot_fn, P[s], a.ldc, b[s].rho, nullptr, nullptr,
                                                               nullptr);
         }
@@ -845,27 +874,27 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
       double* Vs = sp->V + s * nb2;
       cudaEvent_t k0 = timed ? ev[7 + 3 * s] : nullptr, k1 = timed ? ev[8 + 3 * s] : nullptr;
       if (sp->mixed) {
-        T.launches += screen_mixed_potential(sp->mixed, sp->tso, sp->slot_fn, sp->slot_tile, t0, nt, s0, ns, sp->phi,
-                                             sp->gx, sp->gy, sp->gz, b[s].A, b[s].Bx, b[s].By, b[s].Bz, Vs, sp->nbas,
+        T.launches += screen_mixed_potential(sp->mixed, sp->tso, sp->slot_fn, sp->slot_tile, t0, nt, s0, ns, phi,
+                                             gxc, gyc, gzc, b[s].A, b[s].Bx, b[s].By, b[s].Bz, Vs, sp->nbas,
                                              st, k0, k1);
       } else {
         const unsigned nbk = (unsigned)std::max<int64_t>(1, std::min<int64_t>((ns * 128 + 255) / 256, 148 * 32));
         if (gga)
-          k_szbuild<true><<<nbk, 256, 0, st>>>(ns, sp->slot_tile + s0, t0, sp->phi, sp->gx, sp->gy, sp->gz, b[s].A,
+          k_szbuild<true><<<nbk, 256, 0, st>>>(ns, sp->slot_tile + s0, t0, phi, gxc, gyc, gzc, b[s].A,
                                                b[s].Bx, b[s].By, b[s].Bz, sp->Z);
         else
-          k_szbuild<false><<<nbk, 256, 0, st>>>(ns, sp->slot_tile + s0, t0, sp->phi, nullptr, nullptr, nullptr,
+          k_szbuild<false><<<nbk, 256, 0, st>>>(ns, sp->slot_tile + s0, t0, phi, nullptr, nullptr, nullptr,
                                                 b[s].A, nullptr, nullptr, nullptr, sp->Z);
         if (timed) SR_TRY(cudaEventRecord(k0, st));
         const int smem = gemm_smem_bytes<true, true>() + (int)sizeof(int) * sp->max_n;
         dim3 grid((unsigned)nt, 4);
         if (gga) {
           raise_smem_limit(k_svpot<true>, smem);
-          k_svpot<true><<<grid, kGemmThreads, smem, st>>>(sp->phi, sp->Z, sp->tso, t0, s0, sp->slot_fn, Vs,
+          k_svpot<true><<<grid, kGemmThreads, smem, st>>>(phi, sp->Z, sp->tso, t0, s0, sp->slot_fn, Vs,
                                                           sp->nbas);
         } else {
           raise_smem_limit(k_svpot<false>, smem);
-          k_svpot<false><<<grid, kGemmThreads, smem, st>>>(sp->phi, sp->Z, sp->tso, t0, s0, sp->slot_fn, Vs,
+          k_svpot<false><<<grid, kGemmThreads, smem, st>>>(phi, sp->Z, sp->tso, t0, s0, sp->slot_fn, Vs,
                                                            sp->nbas);
         }
         if (timed) SR_TRY(cudaEventRecord(k1, st));
@@ -916,6 +945,7 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
     }
   }
 #undef SR_TRY
+  if (sp->keep) sp->basis_ready = true;  // a completed build has filled the resident basis values
   *tm = T;
   return PGXC_OK;
 }

@@ -47,6 +47,7 @@ struct ScreenInput {
   int ispin = 1;              // 2: open shell, one density and one V_xc per spin
   int precision;              // PGXC_PREC_*
   int64_t max_chunk_points;   // 0: sized from free device memory
+  bool keep_basis = false;    // basis values of the whole grid stay resident across builds
 };
 
 int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, cudaStream_t st, std::string& err);

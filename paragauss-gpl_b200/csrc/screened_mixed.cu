@@ -732,22 +732,23 @@ int screen_mixed_create(ScreenMixed** out, const ScreenMixedInput& in, std::stri
   m->nspin = in.nspin;
   cudaError_t e = cudaSuccess;
   const size_t dig = (size_t)in.chunk_slots * kDigBytesPerSlot;
+  const size_t dig_a = (size_t)std::max(in.chunk_slots, in.resident_slots) * kDigBytesPerSlot;
   for (int s = 0; s < in.nspin; ++s) {
     if (e == cudaSuccess) e = sm_alloc(m, &m->P8[s], (size_t)in.nbas * in.nbas);
     if (e == cudaSuccess) e = sm_alloc(m, &m->e_P[s], (size_t)in.nbas);
   }
-  if (e == cudaSuccess) e = sm_alloc(m, &m->tA, dig);
+  if (e == cudaSuccess) e = sm_alloc(m, &m->tA, dig_a);
   if (e == cudaSuccess) e = sm_alloc(m, &m->tB, (size_t)in.chunk_bstages * kOpB);
   m->b_off = in.b_off;
   if (e == cudaSuccess) e = sm_alloc(m, &m->tZ, dig);
   if (e == cudaSuccess) e = sm_alloc(m, &m->tF, dig);
-  if (e == cudaSuccess) e = sm_alloc(m, &m->e_pt, (size_t)in.chunk_tiles * 128);
+  if (e == cudaSuccess) e = sm_alloc(m, &m->e_pt, (size_t)std::max(in.chunk_tiles, in.resident_tiles) * 128);
   if (e == cudaSuccess) e = sm_alloc(m, &m->zs, (size_t)in.chunk_slots);
   if (e == cudaSuccess) e = sm_alloc(m, &m->fs, (size_t)in.chunk_slots);
   if (e == cudaSuccess) e = sm_alloc(m, &m->ps, (size_t)in.chunk_slots);
   if (e == cudaSuccess) e = sm_alloc(m, &m->err, 1);
   // the slack rows after a chunk's last slot are read (never used) by whole-block copies
-  if (e == cudaSuccess) e = cudaMemset(m->tA, 0, dig);
+  if (e == cudaSuccess) e = cudaMemset(m->tA, 0, dig_a);
   if (e == cudaSuccess) e = cudaMemset(m->tZ, 0, dig);
   if (e == cudaSuccess) e = cudaMemset(m->tF, 0, dig);
   if (e == cudaSuccess) e = cudaMemset(m->err, 0, sizeof(int));
@@ -789,8 +790,9 @@ int screen_mixed_prepare(ScreenMixed* m, const double* P, int64_t ldc, int spin,
 }
 
 int screen_mixed_basis(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
-                       const double* phi, const unsigned long long* pmax, cudaStream_t st) {
-  k_sm_quant_pts<<<(unsigned)nt, 128, 0, st>>>(tso, t0, s0, phi, pmax, m->e_pt, m->tA);
+                       const double* phi, const unsigned long long* pmax, int64_t so, int64_t to, cudaStream_t st) {
+  k_sm_quant_pts<<<(unsigned)nt, 128, 0, st>>>(tso, t0, s0, phi, pmax, m->e_pt + to * 128,
+                                              m->tA + so * kDigBytesPerSlot);
   return 1 + screen_mixed_gather(m, tso, slot_fn, t0, nt, s0, 0, st);
 }
 
@@ -803,7 +805,9 @@ int screen_mixed_gather(ScreenMixed* m, const int64_t* tso, const int* slot_fn, 
 
 int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
                          const double* phi, const double* gx, const double* gy, const double* gz, double* rho,
-                         double* grx, double* gry, double* grz, cudaStream_t st) {
+                         double* grx, double* gry, double* grz, int64_t so, int64_t to, cudaStream_t st) {
+  const int8_t* tA = m->tA + so * kDigBytesPerSlot;
+  const int* e_pt = m->e_pt + to * 128;
   cudaMemsetAsync(rho, 0, sizeof(double) * nt * 128, st);
   if (m->gga) {
     cudaMemsetAsync(grx, 0, sizeof(double) * nt * 128, st);
@@ -813,10 +817,10 @@ int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn,
   const unsigned grid = (unsigned)std::min<int64_t>(nt, m->nsm);
   const int smem = (int)sizeof(DensSmem);
   if (m->gga)
-    k_sm_density<true><<<grid, kDensThreads, smem, st>>>(tso, slot_fn, t0, nt, s0, m->tA, m->e_pt, m->tB, m->b_off,
+    k_sm_density<true><<<grid, kDensThreads, smem, st>>>(tso, slot_fn, t0, nt, s0, tA, e_pt, m->tB, m->b_off,
                                                          m->ps, phi, gx, gy, gz, rho, grx, gry, grz, m->err);
   else
-    k_sm_density<false><<<grid, kDensThreads, smem, st>>>(tso, slot_fn, t0, nt, s0, m->tA, m->e_pt, m->tB, m->b_off,
+    k_sm_density<false><<<grid, kDensThreads, smem, st>>>(tso, slot_fn, t0, nt, s0, tA, e_pt, m->tB, m->b_off,
                                                           m->ps, phi, nullptr, nullptr, nullptr, rho, nullptr,
                                                           nullptr, nullptr, m->err);
   return 1;

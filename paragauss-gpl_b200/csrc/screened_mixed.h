@@ -22,6 +22,8 @@ struct ScreenMixedInput {
   int max_n = 0;             // largest padded slot count of a tile
   int64_t chunk_bstages = 0; // density B stages of the largest chunk
   const int64_t* b_off = nullptr;  // device [ntiles + 1]: first density B stage of each tile
+  // resident point digits (basis kept across builds): slot rows and tiles of the whole grid, 0 -> per chunk
+  int64_t resident_slots = 0, resident_tiles = 0;
 };
 
 // device bytes per slot row and per tile of the chunk buffers
@@ -37,14 +39,15 @@ int screen_mixed_prepare(ScreenMixed* m, const double* P, int64_t ldc, int spin,
 // Operands of the density contraction: INT8 digits of phi (per-point scales
 // from pmax, the bit patterns of the largest |phi| of each point of the
 // chunk) and the gathered digits of P[S_t, S_t] of every tile (spin 0)
+// so / to: the chunk's first slot / tile in the resident digit arrays (0 when they are per chunk)
 int screen_mixed_basis(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
-                       const double* phi, const unsigned long long* pmax, cudaStream_t st);
+                       const double* phi, const unsigned long long* pmax, int64_t so, int64_t to, cudaStream_t st);
 // the gathered digits of P_spin[S_t, S_t] of every tile (replaces the previous spin's)
 int screen_mixed_gather(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
                         int spin, cudaStream_t st);
 int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
                          const double* phi, const double* gx, const double* gy, const double* gz, double* rho,
-                         double* grx, double* gry, double* grz, cudaStream_t st);
+                         double* grx, double* gry, double* grz, int64_t so, int64_t to, cudaStream_t st);
 // Z digits (per-slot scales), then H[S_t, S_t] += Z_t^T phi_t scatter-added into V;
 // records k0 / k1 around the contraction kernel
 int screen_mixed_potential(ScreenMixed* m, const int64_t* tso, const int* slot_fn, const int* slot_tile, int64_t t0,

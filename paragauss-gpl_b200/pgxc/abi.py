@@ -65,6 +65,7 @@ class Options(ct.Structure):
         ("batch_points", ct.c_int32),
         ("screen_threshold", ct.c_double),
         ("device", ct.c_int32),
+        ("keep_orbitals", ct.c_int32),
         ("max_chunk_points", ct.c_int64),
     ]
 

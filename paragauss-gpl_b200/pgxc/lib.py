@@ -68,7 +68,7 @@ class Context:
     """One geometry: pgxc_create ... pgxc_destroy."""
 
     def __init__(self, case, precision="fp64", weighted=True, device=-1, max_chunk_points=0,
-                 screen_threshold=0.0, batch_points=128):
+                 screen_threshold=0.0, batch_points=128, keep_orbitals=False):
         L = lib()
         self.case = case
         self._m = abi.Marshalled(case, weighted=weighted)
@@ -81,6 +81,7 @@ class Context:
         o.max_chunk_points = max_chunk_points
         o.screen_threshold = screen_threshold
         o.batch_points = batch_points
+        o.keep_orbitals = int(bool(keep_orbitals))
         self.opt = o
         h = ct.c_void_p()
         st = L.pgxc_create(ct.byref(self._m.geometry), ct.byref(self._m.basis), ct.byref(self._m.grid),
