@@ -156,7 +156,7 @@ def shard(case, rank, world):
 def algorithmic_flops(case):
     n, N = case.nbas, case.npts
     x = 2.0 * N * n * n
-    v = 2.0 * N * n * n if case.functional == "PBE" else 1.0 * N * n * n
+    v = 2.0 * N * n * n if case.functional != "VWN" else 1.0 * N * n * n
     return x, v
 
 
@@ -523,7 +523,7 @@ def main():
 
     # roofline of the density kernel (the largest kernel of the build), per
     # launch from the library's CUDA events around it
-    gga = case.functional == "PBE"
+    gga = case.functional != "VWN"
     arrays = 4 if gga else 1
     if screen is not None:
         nlisted, sum_n2, ntl = screen["nlisted"], screen["sum_n2"], screen["ntiles"]

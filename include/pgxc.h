@@ -41,11 +41,17 @@ extern "C" {
 #define PGXC_ENONFINITE -6   /* NaN/Inf in an input or a result             */
 #define PGXC_ENODEV     -7   /* no CUDA device / extension unusable         */
 
-/* ---- functional ids: the two XC keywords on the path ----------------- */
+/* ---- functional ids: XC keywords of the reference ---------------------- */
 /* XC="VWN": Slater exchange + VWN5 correlation (modules/xc_cntrl.f90:460-465) */
 #define PGXC_XC_VWN 1
 /* XC="PBE": Slater + PW92 + PBE-X enhancement + PBE-C H (xc_cntrl.f90:652-670) */
 #define PGXC_XC_PBE 2
+/* revPBE: Slater + PW92 + revPBE exchange (kappa 1.245) + PBE correlation
+ * (keyword "revPBE", modules/xc_cntrl.f90:766-776) */
+#define PGXC_XC_REVPBE 3
+/* PBEsol: Slater + PW92 + PBEsol exchange (mu 10/81) + PBEsol correlation
+ * (beta 0.046; keyword "PBESOL", modules/xc_cntrl.f90:788-798) */
+#define PGXC_XC_PBESOL 4
 
 /* ---- precision modes ------------------------------------------------- */
 #define PGXC_PREC_FP64        0  /* FP64 everywhere (FP64 tensor pipe): the drop-in */
@@ -105,7 +111,7 @@ typedef struct pgxc_grid {
 } pgxc_grid;
 
 typedef struct pgxc_options {
-  int32_t functional;            /* PGXC_XC_VWN | PGXC_XC_PBE               */
+  int32_t functional;            /* PGXC_XC_VWN | _PBE | _REVPBE | _PBESOL   */
   int32_t ispin;                 /* 1 or 2; 2 (open shell) needs screen_threshold >= 0,
                                   * the dense layout returns PGXC_ENOTSUP */
   int32_t precision;             /* PGXC_PREC_*                             */

@@ -119,12 +119,24 @@ D x_lda(D rho) {
 }
 
 // ---------------------------------------------------------------------------
-// PBE exchange enhancement (the "1" of 1+G is omitted; XALPHA supplies it):
-// x_gga modules/exchange.f90:325-439, g_pbe :617-639, g_becke86_form
-// :858-867.  kappa = 0.804, mu = beta*pi^2/3 with beta = 0.066725.
+// PBE-form exchange enhancement (the "1" of 1+G is omitted; XALPHA supplies
+// it): x_gga modules/exchange.f90:325-439, g_becke86_form :858-867, with
+// kappa and mu of g_pbe :617-639 (0.804, beta pi^2/3 with beta = 0.066725),
+// g_revpbe :641-655 (1.245, the same mu) or g_pbesol :657-670 (0.804, 10/81).
 // Returns F, dF/dn, dF/dgam of the RKS functional e(n, gam).
 // ---------------------------------------------------------------------------
-void x_gga_pbe(double n, double gam, double& F, double& dFdn, double& dFdg) {
+struct GgaPar {
+  double kappa, mu, beta_c;  // exchange kappa, mu; correlation beta (pbe_ggcc :249-270)
+};
+GgaPar gga_par(int xc) {
+  const double pi = PI_EXCH;
+  const double mu_pbe = 0.066725 * (pi * pi / 3.0);
+  if (xc == PGXC_XC_REVPBE) return {1.245, mu_pbe, 0.066725};
+  if (xc == PGXC_XC_PBESOL) return {0.804, 10.0 / 81.0, 0.046};
+  return {0.804, mu_pbe, 0.066725};
+}
+
+void x_gga_pbe(const GgaPar& P, double n, double gam, double& F, double& dFdn, double& dFdg) {
   const double pi = PI_EXCH;
   const double xalpha = -(3.0 / 4.0) * std::pow(3.0 / pi, 1.0 / 3.0);
   D rho = var(0, n);
@@ -136,8 +148,7 @@ void x_gga_pbe(double n, double gam, double& F, double& dFdn, double& dFdg) {
     s2_0 = gam * s2_g;
     s2_r = -(8.0 / 3.0) * s2_0 / n;
   }
-  const double kappa = 0.804, beta = 0.066725;
-  const double mu = beta * (pi * pi / 3.0);
+  const double kappa = P.kappa, mu = P.mu;
   D s2 = var(0, s2_0);
   D G = kappa * mu * s2 / (kappa + mu * s2);
   F += ex.v * G.v;
@@ -232,13 +243,12 @@ D c_lda(D na, D nb) {
 
 // ---------------------------------------------------------------------------
 // PBE correlation H term: c_gga, modules/pbe_ggcxc_module.f90:96-145,
-// driver pbe_ggcc :214-348 (beta = 0.066725,
+// driver pbe_ggcc :214-348 (beta = 0.066725, or 0.046 for PBEsol;
 // gamma = 0.03109069086965489503494086371).
 // ---------------------------------------------------------------------------
-D c_gga(D na, D nb, D g2) {
+D c_gga(double beta, D na, D nb, D g2) {
   const double zero = 0.0, one = 1.0, two = 2.0, three = 3.0, four = 4.0, seven = 7.0;
   const double deps = 1.0e-30, pi = 3.14159265358979324;
-  const double beta = 0.066725;
   const double gamma = 0.03109069086965489503494086371;
   D n = na + nb;
   if (n.v <= zero) return cst(0.0);
@@ -268,6 +278,7 @@ void functional_point(int xc, int ispin, const double* rho, const double* gam,
   f = 0.0;
   fr[0] = fr[1] = 0.0;
   fg[0] = fg[1] = fg[2] = 0.0;
+  const GgaPar P = gga_par(xc);
   // Slater exchange (exchange_lda, exchange.f90:511-565)
   if (ispin == 1) {
     D e = x_lda(var(0, rho[0]));
@@ -291,12 +302,12 @@ void functional_point(int xc, int ispin, const double* rho, const double* gam,
   // PBE exchange (exchange_gga, exchange.f90:206-292)
   if (ispin == 1) {
     double F = 0, Fn = 0, Fg = 0;
-    x_gga_pbe(rho[0], gam[0], F, Fn, Fg);
+    x_gga_pbe(P, rho[0], gam[0], F, Fn, Fg);
     f += F; fr[0] += Fn; fg[0] += Fg;
   } else {
     for (int s = 0; s < 2; ++s) {
       double F = 0, Fn = 0, Fg = 0;
-      x_gga_pbe(2.0 * rho[s], 4.0 * gam[s], F, Fn, Fg);
+      x_gga_pbe(P, 2.0 * rho[s], 4.0 * gam[s], F, Fn, Fg);
       f += 0.5 * F; fr[s] += Fn; fg[s] += 2.0 * Fg;
     }
   }
@@ -304,12 +315,12 @@ void functional_point(int xc, int ispin, const double* rho, const double* gam,
   if (ispin == 1) {
     D nn = var(0, rho[0]);
     D g2 = var(1, gam[0]);
-    D c = c_gga(0.5 * nn, 0.5 * nn, g2);
+    D c = c_gga(P.beta_c, 0.5 * nn, 0.5 * nn, g2);
     f += c.v; fr[0] += c.d[0]; fg[0] += c.d[1];
   } else {
     D na = var(0, rho[0]), nb = var(1, rho[1]);
     D g2 = var(2, gam[0] + gam[1] + 2.0 * gam[2]);
-    D c = c_gga(na, nb, g2);
+    D c = c_gga(P.beta_c, na, nb, g2);
     f += c.v; fr[0] += c.d[0]; fr[1] += c.d[1];
     fg[0] += c.d[2]; fg[1] += c.d[2]; fg[2] += 2.0 * c.d[2];
   }
@@ -625,18 +636,18 @@ int oracle_orbitals(const pgxc_geometry* geo, const pgxc_basis* bas, int64_t npt
 // VWN), outputs f (n), fr (n,ispin), fg (n,2ispin-1) (may be NULL for VWN).
 int oracle_functionals(int32_t xc, int32_t ispin, int64_t n, const double* rho, const double* gam,
                        double* f, double* fr, double* fg) {
-  if ((xc != PGXC_XC_VWN && xc != PGXC_XC_PBE) || (ispin != 1 && ispin != 2)) return PGXC_EINVAL;
+  if (xc < PGXC_XC_VWN || xc > PGXC_XC_PBESOL || (ispin != 1 && ispin != 2)) return PGXC_EINVAL;
   const int ng = 2 * ispin - 1;
   for (int64_t i = 0; i < n; ++i) {
     double r[2] = {rho[i], ispin == 2 ? rho[i + n] : 0.0};
     double g[3] = {0, 0, 0};
-    if (xc == PGXC_XC_PBE)
+    if (xc != PGXC_XC_VWN)
       for (int c = 0; c < ng; ++c) g[c] = gam[i + n * c];
     double F, Fr[2], Fg[3];
     functional_point(xc, ispin, r, g, F, Fr, Fg);
     f[i] = F;
     for (int s = 0; s < ispin; ++s) fr[i + n * s] = Fr[s];
-    if (fg && xc == PGXC_XC_PBE)
+    if (fg && xc != PGXC_XC_VWN)
       for (int c = 0; c < ng; ++c) fg[i + n * c] = Fg[c];
   }
   return PGXC_OK;
@@ -708,7 +719,7 @@ int oracle_xc_build(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_
   const int64_t nb = B.nbas;
   if (nb != nbas_in || (ispin != 1 && ispin != 2) || nocc < 0) return PGXC_EINVAL;
   if (xc_length != (int64_t)ispin * nb * (nb + 1) / 2) return PGXC_EINVAL;
-  if (xc != PGXC_XC_VWN && xc != PGXC_XC_PBE) return PGXC_EINVAL;
+  if (xc < PGXC_XC_VWN || xc > PGXC_XC_PBESOL) return PGXC_EINVAL;
   if (grid->weights_are_raw) return PGXC_EINVAL;  // the oracle integrates a weighted grid
   if (vla <= 0 || vla > 128) vla = 128;
   const int64_t npts = grid->npts;
@@ -718,7 +729,7 @@ int oracle_xc_build(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_
   const double* gy = gx + npts;
   const double* gz = gy + npts;
   const double* gw = gz + npts;
-  const bool gga = (xc == PGXC_XC_PBE);
+  const bool gga = (xc != PGXC_XC_VWN);
   const int64_t nbatch = (pt_hi - pt_lo + vla - 1) / vla;
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);

@@ -235,7 +235,7 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
     pgxc_destroy(c);
     return st;
   };
-  if (o.functional != PGXC_XC_VWN && o.functional != PGXC_XC_PBE)
+  if (o.functional < PGXC_XC_VWN || o.functional > PGXC_XC_PBESOL)
     return fail(set_err(c, PGXC_EINVAL, "unknown functional id"));
   if (o.ispin != 1 && o.ispin != 2) return fail(set_err(c, PGXC_EINVAL, "ispin must be 1 or 2"));
   if (o.ispin == 2 && !(o.screen_threshold >= 0.0))
@@ -263,7 +263,7 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
   c->npts = grid->npts;
   BuildArgs& a = c->a;
   a.nshells = (int)c->shells.size();
-  a.xc = make_xc_const();
+  a.xc = make_xc_const(o.functional);
   // symmetry adaptation table
   std::memset(&a.sa, 0, sizeof(a.sa));
   a.sa.identity = 1;
@@ -368,7 +368,7 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   }
   a.ldc = round_up(c->nbas, kTile);
-  const bool gga = o.functional == PGXC_XC_PBE;
+  const bool gga = o.functional != PGXC_XC_VWN;
   if (o.screen_threshold >= 0.0) {
     // screened build: per-tile significant-function lists; only P, the
     // accumulators and the packed matrix are shared with the dense layout
@@ -518,7 +518,7 @@ static int upload_orbitals(pgxc_ctx* c, const double* C, const double* occ, int3
 static int run_build(pgxc_ctx* c, int nocc, pgxc_timings* tm, bool p_given = false) {
   BuildArgs& a = c->a;
   cudaStream_t s = c->stream;
-  const bool gga = c->opt.functional == PGXC_XC_PBE;
+  const bool gga = c->opt.functional != PGXC_XC_VWN;
   const int64_t kpad = round_up(std::max(nocc, 1), 16);
   if (c->screen) {
     CUDA_TRY(c, cudaMemsetAsync(a.acc, 0, 4 * sizeof(double), s));
@@ -963,10 +963,10 @@ int pgxc_orbital_calculate(pgxc_ctx* c, int64_t npts, const double* pts, double*
 
 int pgxc_xc_functionals(int32_t functional, int32_t ispin, int64_t n, const double* rho, const double* gam, double* f,
                         double* fr, double* fg) {
-  if (functional != PGXC_XC_VWN && functional != PGXC_XC_PBE) return set_err(nullptr, PGXC_EINVAL, "functional");
+  if (functional < PGXC_XC_VWN || functional > PGXC_XC_PBESOL) return set_err(nullptr, PGXC_EINVAL, "functional");
   if (ispin != 1 && ispin != 2) return set_err(nullptr, PGXC_EINVAL, "ispin must be 1 or 2");
   if (n < 0 || !rho || !f || !fr) return set_err(nullptr, PGXC_EINVAL, "bad arguments");
-  const bool gga = functional == PGXC_XC_PBE;
+  const bool gga = functional != PGXC_XC_VWN;
   if (gga && (!gam || !fg)) return set_err(nullptr, PGXC_EINVAL, "PBE needs gam and fg");
   if (n == 0) return PGXC_OK;
   int st = check_device(nullptr, -1);

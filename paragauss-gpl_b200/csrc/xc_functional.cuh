@@ -16,6 +16,8 @@
 
 #include <cmath>
 
+#include "../../include/pgxc.h"
+
 namespace pgxc {
 
 // Constants that the reference computes with library pow(); filled on the
@@ -29,7 +31,9 @@ struct XcConst {
   double pw_crs;        // (3/(4 pi))^(1/3)
   // PBE exchange
   double s2_fact;       // 1/(4 (3 pi^2)^(2/3))
-  double pbe_mu;        // beta*pi^2/3
+  double pbe_kappa;     // enhancement-factor kappa (PBE 0.804, revPBE 1.245)
+  double pbe_mu;        // beta*pi^2/3 (PBE, revPBE) or 10/81 (PBEsol)
+  double pbe_beta;      // correlation beta (PBE 0.066725, PBEsol 0.046)
   // PBE correlation
   double pbe_fi;        // (0.5^(2/3)+0.5^(2/3)) * (1/2^(1/3))
   double pbe_ct;        // pi/(16 (3 pi^2)^(1/3))
@@ -39,7 +43,10 @@ struct XcConst {
   double pbe_two13i;    // 1 / 2^(1/3)
 };
 
-__host__ inline XcConst make_xc_const() {
+// Constants of the functional (PGXC_XC_*): the GGA keywords differ only in
+// the PBE-form parameters (exchange.f90 g_pbe / g_revpbe / g_pbesol :617-670,
+// pbe_ggcxc_module.f90 pbe_ggcc :249-270).
+__host__ inline XcConst make_xc_const(int functional = PGXC_XC_PBE) {
   XcConst c;
   const double pi_x = 3.14159265358979324;  // exchange.f90 uses constants.f90 pi
   c.xalpha = -(3.0 / 4.0) * std::pow(3.0 / pi_x, 1.0 / 3.0);
@@ -49,7 +56,9 @@ __host__ inline XcConst make_xc_const() {
   const double pi_p = 3.14159265358979324;   // pw_ldac_module.f90:120
   c.pw_crs = std::pow(3.0 / (4.0 * pi_p), 1.0 / 3.0);
   c.s2_fact = 1.0 / (4.0 * std::pow(3.0 * pi_x * pi_x, 2.0 / 3.0));
-  c.pbe_mu = 0.066725 * (pi_x * pi_x / 3.0);
+  c.pbe_kappa = functional == PGXC_XC_REVPBE ? 1.245 : 0.804;
+  c.pbe_mu = functional == PGXC_XC_PBESOL ? 10.0 / 81.0 : 0.066725 * (pi_x * pi_x / 3.0);
+  c.pbe_beta = functional == PGXC_XC_PBESOL ? 0.046 : 0.066725;
   c.pbe_fi = (std::pow(0.5, 2.0 / 3.0) + std::pow(0.5, 2.0 / 3.0)) * (1.0 / std::pow(2.0, 1.0 / 3.0));
   c.pbe_ct = pi_p / (4.0 * 4.0 * std::pow(3.0 * pi_p * pi_p, 1.0 / 3.0));
   c.vwn_ffact = 0.5 / (std::pow(2.0, 1.0 / 3.0) - 1.0);
@@ -129,7 +138,7 @@ __device__ __forceinline__ void pbe_x(const XcConst& K, double n, double g, doub
     s2 = g * s2g;
     s2r = -(8.0 / 3.0) * s2 / n;
   }
-  const double kappa = 0.804, mu = K.pbe_mu;
+  const double kappa = K.pbe_kappa, mu = K.pbe_mu;
   const double den = kappa + mu * s2;
   const double G = kappa * mu * s2 / den;
   const double Gs = kappa * kappa * mu / (den * den);
@@ -161,7 +170,7 @@ __device__ __forceinline__ void xc_pbe(const XcConst& K, double n, double g, dou
   pbe_x(K, n, g, f, fr, fg);
   // PBE correlation H (c_gga with na = nb = n/2)
   if (n > 0.0) {
-    const double beta = 0.066725;
+    const double beta = K.pbe_beta;
     const double gam = 0.03109069086965489503494086371;
     const double deps = 1.0e-30;
     double EL, dEL;
@@ -321,7 +330,7 @@ __device__ __forceinline__ D3 pw92_c_lda(const XcConst& K, D3 na, D3 nb) {
 // PBE correlation H(na, nb, g2), pbe_ggcxc_module.f90:96-145: n * H;
 // g2 = |grad n|^2 of the total density
 __device__ __forceinline__ D3 pbe_c_gga(const XcConst& K, D3 na, D3 nb, D3 g2) {
-  const double beta = 0.066725, gam = 0.03109069086965489503494086371, deps = 1.0e-30;
+  const double beta = K.pbe_beta, gam = 0.03109069086965489503494086371, deps = 1.0e-30;
   const D3 n = na + nb;
   if (n.v <= 0.0) return d3c(0.0);
   const D3 eldac = pw92_c_lda(K, na, nb) / n;

@@ -18,7 +18,9 @@ PGXC_ENODEV = -7
 
 XC_VWN = 1
 XC_PBE = 2
-XC_IDS = {"VWN": XC_VWN, "PBE": XC_PBE}
+XC_REVPBE = 3
+XC_PBESOL = 4
+XC_IDS = {"VWN": XC_VWN, "PBE": XC_PBE, "revPBE": XC_REVPBE, "PBEsol": XC_PBESOL}
 
 PREC_FP64 = 0
 PREC_MIXED_INT8 = 1

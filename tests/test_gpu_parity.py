@@ -94,12 +94,12 @@ def test_raw_weight_grid_is_becke_scaled_on_device(thr):
     assert np.max(np.abs(ham - ref_ham)) < TOL
 
 
-@pytest.mark.parametrize("xc", ["VWN", "PBE"])
+@pytest.mark.parametrize("xc", ["VWN", "PBE", "revPBE", "PBEsol"])
 def test_point_functionals(xc):
     rng = np.random.default_rng(1)
     rho = np.concatenate([[0.0, 1e-35, 1e-31, 1e-25, 1e-21, 1e-19], 10 ** rng.uniform(-14, 3, 500)])
     gam = np.concatenate([[0.0] * 6, 10 ** rng.uniform(-20, 4, 500)])
-    f, fr, fg = lib.xc_functionals(xc, rho, gam if xc == "PBE" else None)
+    f, fr, fg = lib.xc_functionals(xc, rho, gam if xc != "VWN" else None)
     rf, rfr, rfg = O.functionals(xc, 1, rho, gam)
     # Errors are measured against the size of the Slater term at each point:
     # the pieces of f and df/drho have mixed signs, so a relative test on the
@@ -113,7 +113,7 @@ def test_point_functionals(xc):
     tol_r = np.where(well, 1e-11 * (np.abs(rfr[:, 0]) + sr), 1e-5 * np.abs(rfr[:, 0]) + 1e-16)
     assert np.all(np.abs(f - rf) <= tol_f), np.max(np.abs(f - rf) / tol_f)
     assert np.all(np.abs(fr - rfr[:, 0]) <= tol_r), np.max(np.abs(fr - rfr[:, 0]) / tol_r)
-    if xc == "PBE":
+    if xc != "VWN":
         assert np.all(np.abs(fg - rfg[:, 0]) <= fg_tolerance(rho, gam, rf, rfg[:, 0]))
 
 
@@ -199,3 +199,16 @@ def test_build_from_density_matrix_open_shell():
         h2, e2, n2 = ctx.build_density(c.density_matrix())
     assert abs(e2 - e1) < 1e-12 and abs(n2 - n1) < 1e-12
     np.testing.assert_allclose(h2, h1, atol=1e-12)
+
+
+@pytest.mark.parametrize("layout,precision,thr,tol", [("dense", "fp64", -1.0, TOL), ("screened", "fp64", 0.0, TOL),
+                                                      ("screened", "mixed", 1e-10, 1e-7)],
+                         ids=["fp64-dense", "fp64-screened", "int8-screened"])
+@pytest.mark.parametrize("xc,seed", [("revPBE", 2), ("PBEsol", 3)])
+def test_pbe_variant_builds(xc, seed, layout, precision, thr, tol):
+    """revPBE and PBEsol (the PBE-form keywords with other kappa, mu, beta)
+    through every layout, against the oracle."""
+    c = cases.small_case(functional=xc, seed=seed, lmax=3, natoms=5, nocc=7)
+    O.weight_case(c)
+    dE, dN, dV, _, _ = compare(c, precision=precision, screen_threshold=thr, max_chunk_points=1024)
+    assert dE < tol and dN < tol and dV < tol, (dE, dN, dV)

@@ -17,7 +17,10 @@ RHO = np.array([1e-12, 1e-6, 1e-3, 0.05, 0.7, 3.0, 120.0])
 GAM = np.array([1e-20, 1e-9, 1e-5, 0.02, 0.9, 10.0, 5e4])
 
 
-@pytest.mark.parametrize("xc", ["VWN", "PBE"])
+ALL_XC = ["VWN", "PBE", "revPBE", "PBEsol"]
+
+
+@pytest.mark.parametrize("xc", ALL_XC)
 def test_functional_derivatives_fd(xc):
     rho = RHO.copy()
     gam = GAM.copy()
@@ -27,7 +30,7 @@ def test_functional_derivatives_fd(xc):
     fm, _, _ = O.functionals(xc, 1, rho - h, gam)
     num = (fp - fm) / (2 * h)
     np.testing.assert_allclose(fr[:, 0], num, rtol=2e-6, atol=1e-12)
-    if xc == "PBE":
+    if xc != "VWN":
         hg = 1e-4 * gam
         gp, _, _ = O.functionals(xc, 1, rho, gam + hg)
         gm, _, _ = O.functionals(xc, 1, rho, gam - hg)
@@ -37,7 +40,7 @@ def test_functional_derivatives_fd(xc):
         np.testing.assert_allclose(fg[ok, 0], ((gp - gm) / (2 * hg))[ok], rtol=1e-6)
 
 
-@pytest.mark.parametrize("xc", ["VWN", "PBE"])
+@pytest.mark.parametrize("xc", ALL_XC)
 def test_functional_spin_consistency(xc):
     """ispin=2 with rho_a = rho_b = rho/2 reproduces the ispin=1 functional."""
     rho = RHO.copy()
@@ -48,13 +51,32 @@ def test_functional_spin_consistency(xc):
     f2, fr2, fg2 = O.functionals(xc, 2, r2, g2)
     np.testing.assert_allclose(f2, f1, rtol=1e-12, atol=1e-300)
     np.testing.assert_allclose(fr2[:, 0], fr1[:, 0], rtol=1e-10, atol=1e-14)
-    if xc == "PBE":
+    if xc != "VWN":
         # d/dg_aa + d/dg_bb + d/dg_ab of g = g_aa + g_bb + 2 g_ab
         np.testing.assert_allclose((fg2[:, 0] + fg2[:, 1] + fg2[:, 2]) / 4, fg1[:, 0], rtol=1e-9, atol=1e-14)
 
 
+def test_pbe_variants_closed_form():
+    """revPBE differs from PBE only in the exchange kappa (1.245): the
+    difference of the two is e_x (G_rev - G_pbe), G = kappa mu s^2/(kappa + mu s^2)
+    (g_becke86_form); without a gradient PBEsol and revPBE equal PBE."""
+    rho, gam = RHO[1:], GAM[1:]
+    pi = 3.14159265358979324
+    ex = -(3 / 4) * (3 / pi) ** (1 / 3) * rho ** (4 / 3)
+    s2 = gam / (4 * (3 * pi ** 2) ** (2 / 3) * rho ** (8 / 3))
+    mu = 0.066725 * pi ** 2 / 3
+    g = lambda k, m: k * m * s2 / (k + m * s2)
+    fp, _, _ = O.functionals("PBE", 1, rho, gam)
+    fr, _, _ = O.functionals("revPBE", 1, rho, gam)
+    want = ex * (g(1.245, mu) - g(0.804, mu))
+    assert np.all(np.abs((fr - fp) - want) <= 1e-9 * np.abs(want) + 1e-13 * np.abs(fp)), (fr - fp, want)
+    z = np.zeros_like(rho)
+    for xc in ("revPBE", "PBEsol"):
+        np.testing.assert_array_equal(O.functionals(xc, 1, rho, z)[0], O.functionals("PBE", 1, rho, z)[0])
+
+
 def test_functional_zero_density():
-    for xc in ("VWN", "PBE"):
+    for xc in ALL_XC:
         f, fr, fg = O.functionals(xc, 1, np.zeros(3), np.zeros(3))
         assert np.all(np.isfinite(f)) and np.all(np.abs(f) < 1e-40)
         assert np.all(np.isfinite(fr)) and np.all(np.isfinite(fg))
@@ -86,9 +108,13 @@ def test_basis_normalised_and_gradients(small_cases):
         np.testing.assert_allclose(gr[:, d, :], (pp - pm) / (2 * h), rtol=1e-5, atol=1e-8)
 
 
-@pytest.mark.parametrize("xc", ["VWN", "PBE"])
+@pytest.mark.parametrize("xc", ALL_XC)
 def test_dE_dC_equals_2_occ_V_C(small_cases, xc):
-    c = small_cases[xc]
+    if xc in small_cases:
+        c = small_cases[xc]
+    else:
+        c = cases.small_case(functional=xc, seed=13)
+        O.weight_case(c)
     ham, e0, _ = O.xc_build(c)
     V = O.unpack(ham, c.nbas)
     grad = 2 * c.occ[:, 0][None, :] * (V @ c.C[:, :, 0])
