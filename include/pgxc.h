@@ -52,6 +52,9 @@ extern "C" {
 /* PBEsol: Slater + PW92 + PBEsol exchange (mu 10/81) + PBEsol correlation
  * (beta 0.046; keyword "PBESOL", modules/xc_cntrl.f90:788-798) */
 #define PGXC_XC_PBESOL 4
+/* BP86: Slater + VWN5 + Becke 88 exchange + Perdew 86 correlation
+ * (keyword "BP", modules/xc_cntrl.f90:508-520) */
+#define PGXC_XC_BP86 5
 
 /* ---- precision modes ------------------------------------------------- */
 #define PGXC_PREC_FP64        0  /* FP64 everywhere (FP64 tensor pipe): the drop-in */
@@ -111,7 +114,7 @@ typedef struct pgxc_grid {
 } pgxc_grid;
 
 typedef struct pgxc_options {
-  int32_t functional;            /* PGXC_XC_VWN | _PBE | _REVPBE | _PBESOL   */
+  int32_t functional;            /* PGXC_XC_VWN | _PBE | _REVPBE | _PBESOL | _BP86 */
   int32_t ispin;                 /* 1 or 2; 2 (open shell) needs screen_threshold >= 0,
                                   * the dense layout returns PGXC_ENOTSUP */
   int32_t precision;             /* PGXC_PREC_*                             */

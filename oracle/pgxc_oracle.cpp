@@ -104,6 +104,7 @@ inline D dlog(D a) { D r; r.v = std::log(a.v); for (int i = 0; i < 3; ++i) r.d[i
 inline D dsqrt(D a) { D r; r.v = std::sqrt(a.v); for (int i = 0; i < 3; ++i) r.d[i] = a.d[i] / (2.0 * r.v); return r; }
 inline D datan(D a) { D r; r.v = std::atan(a.v); for (int i = 0; i < 3; ++i) r.d[i] = a.d[i] / (1.0 + a.v * a.v); return r; }
 inline D fix(D a) { return cst(a.v); }
+inline D dasinh(D a) { D r; r.v = std::asinh(a.v); for (int i = 0; i < 3; ++i) r.d[i] = a.d[i] / std::sqrt(1.0 + a.v * a.v); return r; }
 
 // ---------------------------------------------------------------------------
 // Slater exchange: x_lda, modules/exchange.f90:567-601 and exchange_lda
@@ -127,13 +128,33 @@ D x_lda(D rho) {
 // ---------------------------------------------------------------------------
 struct GgaPar {
   double kappa, mu, beta_c;  // exchange kappa, mu; correlation beta (pbe_ggcc :249-270)
+  bool b88;                  // exchange enhancement of Becke 88 (g_becke88) instead of the PBE form
 };
 GgaPar gga_par(int xc) {
   const double pi = PI_EXCH;
   const double mu_pbe = 0.066725 * (pi * pi / 3.0);
-  if (xc == PGXC_XC_REVPBE) return {1.245, mu_pbe, 0.066725};
-  if (xc == PGXC_XC_PBESOL) return {0.804, 10.0 / 81.0, 0.046};
-  return {0.804, mu_pbe, 0.066725};
+  if (xc == PGXC_XC_REVPBE) return {1.245, mu_pbe, 0.066725, false};
+  if (xc == PGXC_XC_PBESOL) return {0.804, 10.0 / 81.0, 0.046, false};
+  if (xc == PGXC_XC_BP86) return {0.0, 0.0, 0.0, true};
+  return {0.804, mu_pbe, 0.066725, false};
+}
+
+// Becke 88 enhancement: g_becke88 (exchange.f90:672-705, the BECKE88_0042
+// parameters: beta = 0.0042, A = 6 beta 2^(1/3) (3 pi^2)^(1/3) 2,
+// D = A 4 pi / 9, B = 2 (6 pi^2)^(1/3)) in g_becke88_form (:964-991):
+// G = D s^2 / (1 + A s asinh(B s)), or its series D s^2 - B A D s^4 when
+// s^2 <= 1e-4.
+D g_becke88(D s2) {
+  const double pi = PI_EXCH;
+  const double beta = 0.0042;
+  const double A = 6.0 * beta * std::pow(2.0, 1.0 / 3.0) * std::pow(3.0 * pi * pi, 1.0 / 3.0) * 2.0;
+  const double Dd = A * (4.0 * pi) / 9.0;
+  const double B = 2.0 * std::pow(6.0 * pi * pi, 1.0 / 3.0);
+  if (s2.v > 1.0e-4) {
+    D s = dsqrt(s2);
+    return s2 * Dd / (1.0 + A * s * dasinh(B * s));
+  }
+  return s2 * (Dd + s2 * (-B * A * Dd));
 }
 
 void x_gga_pbe(const GgaPar& P, double n, double gam, double& F, double& dFdn, double& dFdg) {
@@ -150,7 +171,7 @@ void x_gga_pbe(const GgaPar& P, double n, double gam, double& F, double& dFdn, d
   }
   const double kappa = P.kappa, mu = P.mu;
   D s2 = var(0, s2_0);
-  D G = kappa * mu * s2 / (kappa + mu * s2);
+  D G = P.b88 ? g_becke88(s2) : kappa * mu * s2 / (kappa + mu * s2);
   F += ex.v * G.v;
   dFdn += ex.d[0] * G.v + ex.v * G.d[0] * s2_r;
   dFdg += ex.v * G.d[0] * s2_g;
@@ -273,6 +294,64 @@ D c_gga(double beta, D na, D nb, D g2) {
 // xc_functionals (modules/xc_func.f90:187-305) for the two keywords.
 // rho[ispin], gam[2*ispin-1] (aa, bb, ab); outputs f, fr[ispin], fg[2ispin-1].
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Perdew 86 gradient correlation: perdew_calc, modules/becke_perdew_module.f90
+// :125-260 (constants :83-118), its own first derivatives.  Closed shell:
+// rho[0], gam[0]; open shell: rho[0..1], gam = (aa, bb, ab).  Adds f, fr, fg.
+// ---------------------------------------------------------------------------
+void perdew86(int ispin, const double* rho, const double* gam, double& f, double* fr, double* fg) {
+  const double deps = 1.0e-30, third = 1.0 / 3.0;
+  const double alpha = 0.023266, beta = 7.389e-6, gammas = 8.723, delta = 0.472, f_wave = 0.11;
+  const double cfac = 0.001667, ocfac = 0.002568, rs_fac = 0.62035049089940001667;
+  const double c_infi = cfac + ocfac, fi_fac = 1.745 * f_wave * c_infi;
+  const double e4_beta = beta * 1.0e4, two_delta = 2.0 * delta, two_beta = 2.0 * beta, f3_e4_beta = 3.0 * e4_beta;
+  const double two_oth = 1.25992104989487316476, f5twelf = (5.0 / 6.0) / 2.0;
+  double sums, xi = 0, xi_u = 0, xi_d = 0, dm = 1.0, ddm_xi = 0;
+  if (ispin == 1) {
+    sums = rho[0] + deps;
+  } else {
+    sums = rho[0] + rho[1] + deps;
+    xi = (rho[0] - rho[1]) / sums;
+    xi_u = (1.0 - xi) / sums;
+    xi_d = -(1.0 + xi) / sums;
+    dm = (1.0 / two_oth) / std::sqrt(std::pow((1.0 + xi) / 2.0, 5.0 / 3.0) + std::pow((1.0 - xi) / 2.0, 5.0 / 3.0));
+    ddm_xi = f5twelf * dm * dm * dm * two_oth * two_oth *
+             (std::pow((1.0 - xi) / 2.0, 2.0 / 3.0) - std::pow((1.0 + xi) / 2.0, 2.0 / 3.0));
+  }
+  const double rothrd = std::pow(sums, third), rof4th = sums * rothrd;
+  const double rs = rs_fac / rothrd, rs2 = rs * rs, rs3 = rs2 * rs;
+  const double gr2 = ispin == 1 ? gam[0] : gam[0] + gam[1] + 2.0 * gam[2];
+  const double gr = std::sqrt(gr2);
+  const double cden = 1.0 + gammas * rs + delta * rs2 + e4_beta * rs3;
+  const double ovcf = ocfac + alpha * rs + beta * rs2;
+  const double c_rho = cfac + ovcf / cden;
+  const double fi_g = fi_fac / (c_rho * std::pow(sums, 7.0 / 6.0));
+  const double fi = fi_g * gr;
+  const double exp_fi = std::exp(-fi);
+  const double dP_g_restr = (exp_fi * c_rho / rof4th) * (1.0 - fi_g * gr / 2.0);
+  const double t1 = (alpha + two_beta * rs) / cden;
+  const double t2 = (gammas + two_delta * rs + f3_e4_beta * rs2) * ovcf / (cden * cden);
+  const double dC_dRho = -third * rs / sums * (t1 - t2);
+  const double dfi_rho_g = -(fi_fac / std::pow(c_rho * std::pow(sums, 7.0 / 6.0), 2)) * std::sqrt(rothrd) *
+                           (dC_dRho * sums + (7.0 / 6.0) * c_rho);
+  const double dfi_rho = dfi_rho_g * gr;
+  const double P = c_rho / rof4th * exp_fi * gr2;
+  const double dP_rho = (exp_fi / rof4th) * (dC_dRho - (4.0 / 3.0) * c_rho / sums - c_rho * dfi_rho) * gr2;
+  if (ispin == 1) {
+    fr[0] += dP_rho;
+    fg[0] += dP_g_restr;
+    f += P;
+  } else {
+    const double dP_g = dP_g_restr * dm;
+    fg[0] += dP_g;
+    fg[1] += dP_g;
+    fg[2] += 2.0 * dP_g;
+    fr[0] += dP_rho * dm + ddm_xi * xi_u * P;
+    fr[1] += dP_rho * dm + ddm_xi * xi_d * P;
+    f += P * dm;
+  }
+}
+
 void functional_point(int xc, int ispin, const double* rho, const double* gam,
                       double& f, double* fr, double* fg) {
   f = 0.0;
@@ -289,16 +368,17 @@ void functional_point(int xc, int ispin, const double* rho, const double* gam,
       f += e.v / 2.0; fr[s] += e.d[0];
     }
   }
-  if (xc == PGXC_XC_VWN) {
+  if (xc == PGXC_XC_VWN || xc == PGXC_XC_BP86) {
     // vwn_ldac, vwnc.f90:225-297
     D c;
     if (ispin == 1) { D nn = var(0, rho[0]); c = vwn::c_lda(0.5 * nn, 0.5 * nn); f += c.v; fr[0] += c.d[0]; }
     else { c = vwn::c_lda(var(0, rho[0]), var(1, rho[1])); f += c.v; fr[0] += c.d[0]; fr[1] += c.d[1]; }
-    return;
+    if (xc == PGXC_XC_VWN) return;
+  } else {
+    // PBE-form keywords: pw_ldac (pw_ldac_module.f90:197-312)
+    if (ispin == 1) { D nn = var(0, rho[0]); D c = pw92::c_lda(0.5 * nn, 0.5 * nn); f += c.v; fr[0] += c.d[0]; }
+    else { D c = pw92::c_lda(var(0, rho[0]), var(1, rho[1])); f += c.v; fr[0] += c.d[0]; fr[1] += c.d[1]; }
   }
-  // PBE: pw_ldac (pw_ldac_module.f90:197-312)
-  if (ispin == 1) { D nn = var(0, rho[0]); D c = pw92::c_lda(0.5 * nn, 0.5 * nn); f += c.v; fr[0] += c.d[0]; }
-  else { D c = pw92::c_lda(var(0, rho[0]), var(1, rho[1])); f += c.v; fr[0] += c.d[0]; fr[1] += c.d[1]; }
   // PBE exchange (exchange_gga, exchange.f90:206-292)
   if (ispin == 1) {
     double F = 0, Fn = 0, Fg = 0;
@@ -310,6 +390,10 @@ void functional_point(int xc, int ispin, const double* rho, const double* gam,
       x_gga_pbe(P, 2.0 * rho[s], 4.0 * gam[s], F, Fn, Fg);
       f += 0.5 * F; fr[s] += Fn; fg[s] += 2.0 * Fg;
     }
+  }
+  if (xc == PGXC_XC_BP86) {  // "BP": Perdew 86 correlation (xc_cntrl.f90:508-520)
+    perdew86(ispin, rho, gam, f, fr, fg);
+    return;
   }
   // PBE correlation H (pbe_ggcc, pbe_ggcxc_module.f90:214-348)
   if (ispin == 1) {
@@ -636,7 +720,7 @@ int oracle_orbitals(const pgxc_geometry* geo, const pgxc_basis* bas, int64_t npt
 // VWN), outputs f (n), fr (n,ispin), fg (n,2ispin-1) (may be NULL for VWN).
 int oracle_functionals(int32_t xc, int32_t ispin, int64_t n, const double* rho, const double* gam,
                        double* f, double* fr, double* fg) {
-  if (xc < PGXC_XC_VWN || xc > PGXC_XC_PBESOL || (ispin != 1 && ispin != 2)) return PGXC_EINVAL;
+  if (xc < PGXC_XC_VWN || xc > PGXC_XC_BP86 || (ispin != 1 && ispin != 2)) return PGXC_EINVAL;
   const int ng = 2 * ispin - 1;
   for (int64_t i = 0; i < n; ++i) {
     double r[2] = {rho[i], ispin == 2 ? rho[i + n] : 0.0};
@@ -719,7 +803,7 @@ int oracle_xc_build(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_
   const int64_t nb = B.nbas;
   if (nb != nbas_in || (ispin != 1 && ispin != 2) || nocc < 0) return PGXC_EINVAL;
   if (xc_length != (int64_t)ispin * nb * (nb + 1) / 2) return PGXC_EINVAL;
-  if (xc < PGXC_XC_VWN || xc > PGXC_XC_PBESOL) return PGXC_EINVAL;
+  if (xc < PGXC_XC_VWN || xc > PGXC_XC_BP86) return PGXC_EINVAL;
   if (grid->weights_are_raw) return PGXC_EINVAL;  // the oracle integrates a weighted grid
   if (vla <= 0 || vla > 128) vla = 128;
   const int64_t npts = grid->npts;

@@ -96,7 +96,7 @@ __global__ void k_xc_points(XcConst K, int functional, int64_t n, const double* 
   if (p >= n) return;
   if (functional != PGXC_XC_VWN) {
     double a, b, c;
-    xc_pbe(K, rho[p], gam[p], a, b, c);
+    xc_gga(K, rho[p], gam[p], a, b, c);
     f[p] = a; fr[p] = b; fg[p] = c;
   } else {
     double a, b;

@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(256) k_functional(XcConst K, int64_t p0, int64
       const double g0 = grx[p], g1 = gry[p], g2 = grz[p];
       const double g = g0 * g0 + g1 * g1 + g2 * g2;
       double f, fr, fg;
-      xc_pbe(K, r, g, f, fr, fg);
+      xc_gga(K, r, g, f, fr, fg);
       A[p] = 0.5 * fr * wt;
       const double b = wt * 2.0 * fg;
       Bx[p] = b * g0;

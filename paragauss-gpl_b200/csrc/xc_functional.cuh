@@ -34,6 +34,9 @@ struct XcConst {
   double pbe_kappa;     // enhancement-factor kappa (PBE 0.804, revPBE 1.245)
   double pbe_mu;        // beta*pi^2/3 (PBE, revPBE) or 10/81 (PBEsol)
   double pbe_beta;      // correlation beta (PBE 0.066725, PBEsol 0.046)
+  // Becke 88 (BP86): exchange enhancement constants of g_becke88, and the kind of GGA
+  double b88_A, b88_B, b88_D;
+  int bp86;             // 1: Slater + VWN5 + Becke 88 + Perdew 86; 0: the PBE-form keywords
   // PBE correlation
   double pbe_fi;        // (0.5^(2/3)+0.5^(2/3)) * (1/2^(1/3))
   double pbe_ct;        // pi/(16 (3 pi^2)^(1/3))
@@ -59,6 +62,11 @@ __host__ inline XcConst make_xc_const(int functional = PGXC_XC_PBE) {
   c.pbe_kappa = functional == PGXC_XC_REVPBE ? 1.245 : 0.804;
   c.pbe_mu = functional == PGXC_XC_PBESOL ? 10.0 / 81.0 : 0.066725 * (pi_x * pi_x / 3.0);
   c.pbe_beta = functional == PGXC_XC_PBESOL ? 0.046 : 0.066725;
+  // g_becke88, exchange.f90:672-705 (BECKE88_0042: beta = 0.0042)
+  c.b88_A = 6.0 * 0.0042 * std::pow(2.0, 1.0 / 3.0) * std::pow(3.0 * pi_x * pi_x, 1.0 / 3.0) * 2.0;
+  c.b88_D = c.b88_A * (4.0 * pi_x) / 9.0;
+  c.b88_B = 2.0 * std::pow(6.0 * pi_x * pi_x, 1.0 / 3.0);
+  c.bp86 = functional == PGXC_XC_BP86 ? 1 : 0;
   c.pbe_fi = (std::pow(0.5, 2.0 / 3.0) + std::pow(0.5, 2.0 / 3.0)) * (1.0 / std::pow(2.0, 1.0 / 3.0));
   c.pbe_ct = pi_p / (4.0 * 4.0 * std::pow(3.0 * pi_p * pi_p, 1.0 / 3.0));
   c.vwn_ffact = 0.5 / (std::pow(2.0, 1.0 / 3.0) - 1.0);
@@ -121,8 +129,9 @@ __device__ __forceinline__ void xc_vwn(const XcConst& K, double n, double& f, do
   fr += ecpara - ap * de * X / 6.0;             // dX/dn = -X/(6S)
 }
 
-// PBE exchange enhancement of the closed-shell functional e(n, g): e_x G(s^2),
-// the 1 of (1+G) omitted (x_gga, exchange.f90:325-439); adds F, dF/dn, dF/dg.
+// GGA exchange enhancement of the closed-shell functional e(n, g): e_x G(s^2),
+// the 1 of (1+G) omitted (x_gga, exchange.f90:325-439), G of the PBE form or
+// of Becke 88 (BP86); adds F, dF/dn, dF/dg.
 __device__ __forceinline__ void pbe_x(const XcConst& K, double n, double g, double& f, double& fr, double& fg) {
   double ex = 0.0, exr = 0.0;
   if (n > 0.0) {
@@ -138,10 +147,28 @@ __device__ __forceinline__ void pbe_x(const XcConst& K, double n, double g, doub
     s2 = g * s2g;
     s2r = -(8.0 / 3.0) * s2 / n;
   }
-  const double kappa = K.pbe_kappa, mu = K.pbe_mu;
-  const double den = kappa + mu * s2;
-  const double G = kappa * mu * s2 / den;
-  const double Gs = kappa * kappa * mu / (den * den);
+  double G, Gs;  // G(s^2) and dG/ds^2
+  if (K.bp86) {
+    // Becke 88: G = D s^2 / (1 + A s asinh(B s)), below s^2 = 1e-4 its series
+    // D s^2 - B A D s^4 (g_becke88_form, exchange.f90:964-991)
+    const double A = K.b88_A, B = K.b88_B, Dd = K.b88_D;
+    if (s2 > 1.0e-4) {
+      const double s = sqrt(s2), bs = B * s, ash = asinh(bs);
+      const double den = 1.0 + A * s * ash;
+      // d(A s asinh(B s))/ds^2 = A (asinh(B s) + B s / sqrt(1 + B^2 s^2)) / (2 s)
+      const double dden = A * (ash + bs / sqrt(1.0 + bs * bs)) / (2.0 * s);
+      G = Dd * s2 / den;
+      Gs = Dd / den - Dd * s2 * dden / (den * den);
+    } else {
+      G = s2 * (Dd - B * A * Dd * s2);
+      Gs = Dd - 2.0 * B * A * Dd * s2;
+    }
+  } else {
+    const double kappa = K.pbe_kappa, mu = K.pbe_mu;
+    const double den = kappa + mu * s2;
+    G = kappa * mu * s2 / den;
+    Gs = kappa * kappa * mu / (den * den);
+  }
   f += ex * G;
   fr += exr * G + ex * Gs * s2r;
   fg += ex * Gs * s2g;
@@ -347,6 +374,76 @@ __device__ __forceinline__ D3 pbe_c_gga(const XcConst& K, D3 na, D3 nb, D3 g2) {
   return n * (gam * fi3 * d3log(1.0 + (beta / gam) * t2 * rat));
 }
 
+// Perdew 86 gradient correlation with its first derivatives (perdew_calc,
+// modules/becke_perdew_module.f90:125-260; constants :83-118).  ispin = 1:
+// rho[0], gam[0]; ispin = 2: rho[0..1], gam = (aa, bb, ab), the correlation
+// of the total gradient scaled by the spin factor d(zeta).  Adds f, fr, fg.
+__device__ __forceinline__ void perdew86(int ispin, const double* rho, const double* gam, double& f, double* fr,
+                                         double* fg) {
+  const double deps = 1.0e-30, third = 1.0 / 3.0;
+  const double alpha = 0.023266, beta = 7.389e-6, gammas = 8.723, delta = 0.472;
+  const double cfac = 0.001667, ocfac = 0.002568, rs_fac = 0.62035049089940001667;
+  const double fi_fac = 1.745 * 0.11 * (cfac + ocfac);
+  const double e4_beta = beta * 1.0e4, two_oth = 1.25992104989487316476;
+  double sums, xi_u = 0, xi_d = 0, dm = 1.0, ddm_xi = 0;
+  if (ispin == 1) {
+    sums = rho[0] + deps;
+  } else {
+    sums = rho[0] + rho[1] + deps;
+    const double xi = (rho[0] - rho[1]) / sums;
+    xi_u = (1.0 - xi) / sums;
+    xi_d = -(1.0 + xi) / sums;
+    const double up = (1.0 + xi) / 2.0, dn = (1.0 - xi) / 2.0;
+    dm = (1.0 / two_oth) / sqrt(pow(up, 5.0 / 3.0) + pow(dn, 5.0 / 3.0));
+    ddm_xi = (5.0 / 12.0) * dm * dm * dm * two_oth * two_oth * (pow(dn, 2.0 / 3.0) - pow(up, 2.0 / 3.0));
+  }
+  const double rothrd = cbrt(sums), rof4th = sums * rothrd;
+  const double rs = rs_fac / rothrd, rs2 = rs * rs, rs3 = rs2 * rs;
+  const double gr2 = ispin == 1 ? gam[0] : gam[0] + gam[1] + 2.0 * gam[2];
+  const double gr = sqrt(gr2);
+  const double cden = 1.0 + gammas * rs + delta * rs2 + e4_beta * rs3;
+  const double ovcf = ocfac + alpha * rs + beta * rs2;
+  const double c_rho = cfac + ovcf / cden;
+  const double r76 = sums * sqrt(rothrd);  // sums^(7/6)
+  const double fi_g = fi_fac / (c_rho * r76);
+  const double exp_fi = exp(-fi_g * gr);
+  const double dP_g = (exp_fi * c_rho / rof4th) * (1.0 - fi_g * gr / 2.0);
+  const double t1 = (alpha + 2.0 * beta * rs) / cden;
+  const double t2 = (gammas + 2.0 * delta * rs + 3.0 * e4_beta * rs2) * ovcf / (cden * cden);
+  const double dC = -third * rs / sums * (t1 - t2);
+  const double cr = c_rho * r76;
+  const double dfi_rho = -(fi_fac / (cr * cr)) * sqrt(rothrd) * (dC * sums + (7.0 / 6.0) * c_rho) * gr;
+  const double P = c_rho / rof4th * exp_fi * gr2;
+  const double dP_rho = (exp_fi / rof4th) * (dC - (4.0 / 3.0) * c_rho / sums - c_rho * dfi_rho) * gr2;
+  if (ispin == 1) {
+    f += P;
+    fr[0] += dP_rho;
+    fg[0] += dP_g;
+  } else {
+    f += P * dm;
+    fr[0] += dP_rho * dm + ddm_xi * xi_u * P;
+    fr[1] += dP_rho * dm + ddm_xi * xi_d * P;
+    fg[0] += dP_g * dm;
+    fg[1] += dP_g * dm;
+    fg[2] += 2.0 * dP_g * dm;
+  }
+}
+
+// "BP": Slater + VWN5 + Becke 88 exchange + Perdew 86 correlation
+// (modules/xc_cntrl.f90:508-520); n = total density, g = |grad n|^2.
+__device__ __forceinline__ void xc_bp86(const XcConst& K, double n, double g, double& f, double& fr, double& fg) {
+  xc_vwn(K, n, f, fr);  // Slater + VWN5
+  fg = 0.0;
+  pbe_x(K, n, g, f, fr, fg);  // K.bp86: the Becke 88 enhancement
+  perdew86(1, &n, &g, f, &fr, &fg);
+}
+
+// The closed-shell GGA keyword of K: BP86 or one of the PBE-form keywords.
+__device__ __forceinline__ void xc_gga(const XcConst& K, double n, double g, double& f, double& fr, double& fg) {
+  if (K.bp86) xc_bp86(K, n, g, f, fr, fg);
+  else xc_pbe(K, n, g, f, fr, fg);
+}
+
 // Open-shell functional at one point: rho[2] = (rho_a, rho_b), gam[3] =
 // (gamma_aa, gamma_bb, gamma_ab); f, fr[2] = df/drho_s, fg[3] = df/dgamma_*.
 // xc_functionals composition (xc_func.f90:187-305), as for ispin = 1.
@@ -364,11 +461,22 @@ __device__ __forceinline__ void xc_open(const XcConst& K, const double (&rho)[2]
     fr[s] += Fn;
   }
   const D3 na = d3v(0, rho[0]), nb = d3v(1, rho[1]);
-  if (!GGA) {
+  if (!GGA || K.bp86) {
     const D3 c = vwn_c_lda(K, na, nb);
     f += c.v;
     fr[0] += c.d[0];
     fr[1] += c.d[1];
+    if (GGA) {
+      // BP86: Becke 88 exchange, spin-scaled, and Perdew 86 correlation
+      for (int s = 0; s < 2; ++s) {
+        double F = 0.0, Fn = 0.0, Fg = 0.0;
+        pbe_x(K, 2.0 * rho[s], 4.0 * gam[s], F, Fn, Fg);
+        f += 0.5 * F;
+        fr[s] += Fn;
+        fg[s] += 2.0 * Fg;
+      }
+      perdew86(2, rho, gam, f, fr, fg);
+    }
     return;
   }
   {

@@ -20,7 +20,8 @@ XC_VWN = 1
 XC_PBE = 2
 XC_REVPBE = 3
 XC_PBESOL = 4
-XC_IDS = {"VWN": XC_VWN, "PBE": XC_PBE, "revPBE": XC_REVPBE, "PBEsol": XC_PBESOL}
+XC_BP86 = 5
+XC_IDS = {"VWN": XC_VWN, "PBE": XC_PBE, "revPBE": XC_REVPBE, "PBEsol": XC_PBESOL, "BP86": XC_BP86}
 
 PREC_FP64 = 0
 PREC_MIXED_INT8 = 1

@@ -43,7 +43,7 @@ def _spin_points(n, seed):
     return rho, gam
 
 
-@pytest.mark.parametrize("xc", ["VWN", "PBE", "revPBE", "PBEsol"])
+@pytest.mark.parametrize("xc", ["VWN", "PBE", "revPBE", "PBEsol", "BP86"])
 def test_point_functionals_open_shell(xc):
     rho, gam = _spin_points(600, 5)
     f, fr, fg = lib.xc_functionals(xc, rho, gam if xc != "VWN" else None)
@@ -104,7 +104,7 @@ BUILDS = pytest.mark.parametrize("precision,thr,tol", [("fp64", 0.0, 1e-10), ("m
 
 
 @BUILDS
-@pytest.mark.parametrize("xc,seed,lmax", [("VWN", 1, 2), ("PBE", 2, 2), ("PBE", 3, 3), ("VWN", 4, 3)])
+@pytest.mark.parametrize("xc,seed,lmax", [("VWN", 1, 2), ("PBE", 2, 2), ("PBE", 3, 3), ("VWN", 4, 3), ("BP86", 5, 2)])
 def test_open_shell_build(xc, seed, lmax, precision, thr, tol):
     c = cases.small_case(functional=xc, seed=seed, lmax=lmax, natoms=5, nocc=7, ispin=2)
     O.weight_case(c)

@@ -94,7 +94,7 @@ def test_raw_weight_grid_is_becke_scaled_on_device(thr):
     assert np.max(np.abs(ham - ref_ham)) < TOL
 
 
-@pytest.mark.parametrize("xc", ["VWN", "PBE", "revPBE", "PBEsol"])
+@pytest.mark.parametrize("xc", ["VWN", "PBE", "revPBE", "PBEsol", "BP86"])
 def test_point_functionals(xc):
     rng = np.random.default_rng(1)
     rho = np.concatenate([[0.0, 1e-35, 1e-31, 1e-25, 1e-21, 1e-19], 10 ** rng.uniform(-14, 3, 500)])
@@ -204,10 +204,10 @@ def test_build_from_density_matrix_open_shell():
 @pytest.mark.parametrize("layout,precision,thr,tol", [("dense", "fp64", -1.0, TOL), ("screened", "fp64", 0.0, TOL),
                                                       ("screened", "mixed", 1e-10, 1e-7)],
                          ids=["fp64-dense", "fp64-screened", "int8-screened"])
-@pytest.mark.parametrize("xc,seed", [("revPBE", 2), ("PBEsol", 3)])
-def test_pbe_variant_builds(xc, seed, layout, precision, thr, tol):
+@pytest.mark.parametrize("xc,seed", [("revPBE", 2), ("PBEsol", 3), ("BP86", 4)])
+def test_gga_keyword_builds(xc, seed, layout, precision, thr, tol):
     """revPBE and PBEsol (the PBE-form keywords with other kappa, mu, beta)
-    through every layout, against the oracle."""
+    and BP86 (Becke 88 + Perdew 86) through every layout, against the oracle."""
     c = cases.small_case(functional=xc, seed=seed, lmax=3, natoms=5, nocc=7)
     O.weight_case(c)
     dE, dN, dV, _, _ = compare(c, precision=precision, screen_threshold=thr, max_chunk_points=1024)

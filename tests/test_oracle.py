@@ -17,7 +17,7 @@ RHO = np.array([1e-12, 1e-6, 1e-3, 0.05, 0.7, 3.0, 120.0])
 GAM = np.array([1e-20, 1e-9, 1e-5, 0.02, 0.9, 10.0, 5e4])
 
 
-ALL_XC = ["VWN", "PBE", "revPBE", "PBEsol"]
+ALL_XC = ["VWN", "PBE", "revPBE", "PBEsol", "BP86"]
 
 
 @pytest.mark.parametrize("xc", ALL_XC)
