@@ -355,8 +355,7 @@ def run_batch(args):
                                f"alternating", "precision": "mixed",
                    "screening": f"per 128-point tile, threshold {args.screen:g}",
                    "batching": f"one context per molecule (chunks of at most {chunk} points), all device builds "
-                               f"captured in one CUDA graph (INT8 builds chained one after another), one replay "
-                               f"per step",
+                               f"captured as the parallel branches of one CUDA graph, one replay per step",
                    "l2": "no flush: each step streams several GB of basis data (inputs larger than L2)"},
         "molecules_per_s": len(mols) / (ms * 1e-3),
         "one_by_one": {"mixed_ms_per_set": ms_seq, "fp64_ms_per_set": ms64,

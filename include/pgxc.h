@@ -229,9 +229,7 @@ int pgxc_build_device(pgxc_ctx* ctx, const double* d_C, const double* d_occ,
  * context).  pgxc_batch_create captures the device build of every context
  * (as pgxc_build_device, with the device operands given here) as one parallel
  * branch of a single CUDA graph; pgxc_batch_run replays the graph, so that
- * the builds of all systems run with one launch: concurrently for FP64
- * contexts; one after another when the batch holds an INT8 context (the INT8
- * kernels are not yet safe beside other kernels on the GPU).  Each context
+ * the builds of all systems run concurrently with one launch.  Each context
  * must use the screened layout (screen_threshold >= 0) and the same device;
  * a context belongs to at most one live batch and must not be built by other
  * calls while its batch runs.  Operand pointers are fixed for the life of

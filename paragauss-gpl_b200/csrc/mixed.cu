@@ -233,6 +233,7 @@ struct OzSmem {
   uint64_t acc_empty;
   uint32_t tslot;
 };
+static_assert(sizeof(OzSmem) + 1024 <= tc::kWholeSmSmem, "OzSmem");
 
 __device__ __forceinline__ void oz_mma_step(uint32_t tbase, const int8_t* a, const int8_t* b, bool first) {
   const uint32_t idesc = tc::idesc_s8(kRowsA, kRowsB);
@@ -273,7 +274,7 @@ __device__ __forceinline__ void oz_read16(uint32_t trow, int c0, double (&x)[16]
 // Warps 0-7 epilogue (warp w: lanes 32(w%4).., columns 48(w/4)..), warp 8
 // producer, warp 9 MMA issuer.
 // ---------------------------------------------------------------------------
-constexpr int kDensThreads = 320;
+constexpr int kDensThreads = tc::kWholeSmThreads;  // warps 10-15 idle
 
 template <bool GGA>
 __global__ void __launch_bounds__(kDensThreads, 1)
@@ -334,6 +335,8 @@ __global__ void __launch_bounds__(kDensThreads, 1)
         for (int nb = it / nks; nb < nnb; ++nb) tc::mma_commit(&S.acc_full);
       }
     }
+  } else if (warp >= 10) {
+    // idle: the CTA holds the whole SM
   } else {  // epilogue: thread owns point pb*128 + row, columns half*48 .. +48
     const int row = (warp & 3) * 32 + lane, half = warp >> 2;
     const int64_t p = (int64_t)pb * 128 + row;
@@ -453,7 +456,7 @@ __global__ void __launch_bounds__(256) k_oz_zbuild(int64_t ldp, const double* __
 // (I: 128 functions, J: 96 functions) over the split's points; the FP64
 // result is added to the CTA's own partial tile.
 // ---------------------------------------------------------------------------
-constexpr int kVThreads = 192;
+constexpr int kVThreads = tc::kWholeSmThreads;  // warps 6-15 idle
 
 __global__ void __launch_bounds__(kVThreads, 1)
     k_oz_vpot(const int8_t* __restrict__ tZ, const int8_t* __restrict__ tP, int nks, int ks_per_split, int ntb,
@@ -507,6 +510,8 @@ __global__ void __launch_bounds__(kVThreads, 1)
       tc::mma_commit(&S.acc_full);  // also on failure: lets the epilogue wind down
       if (!ok) atomicExch(err, 1);
     }
+  } else if (warp >= 6) {
+    // idle: the CTA holds the whole SM
   } else {
     const bool done = tc::mbar_wait_warp(&S.acc_full, 0);
     if (!done) atomicExch(err, 1);
@@ -615,7 +620,7 @@ int mixed_create(MixedState** out, const BuildArgs& a, int64_t nbas, bool gga, i
   m->ks_per_split = (nks + ns - 1) / ns;
   m->nsplit = (nks + m->ks_per_split - 1) / m->ks_per_split;
   if ((e = mx_alloc(m, &m->vpart, (size_t)m->nsplit * m->ntiles * kRowsA * kRowsB))) return fail(e, "cudaMalloc");
-  const int smem = (int)sizeof(OzSmem) + 1024;
+  const int smem = tc::kWholeSmSmem;  // >= sizeof(OzSmem) + 1024 (base alignment)
   if ((e = cudaFuncSetAttribute(k_oz_density<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) ||
       (e = cudaFuncSetAttribute(k_oz_density<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)) ||
       (e = cudaFuncSetAttribute(k_oz_vpot, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)))
@@ -675,7 +680,7 @@ int mixed_basis(MixedState* m, const BuildArgs& a, int64_t p0, int64_t nvalid, b
 }
 
 int mixed_density(MixedState* m, const BuildArgs& a, bool gga, cudaStream_t st) {
-  const int smem = (int)sizeof(OzSmem) + 1024;
+  const int smem = tc::kWholeSmSmem;  // >= sizeof(OzSmem) + 1024 (base alignment)
   const int nks = (int)(m->ldk / kKStep), nnb = (int)(m->ldk / kRowsB);
   dim3 grid((unsigned)(m->ldp / 128));
   if (gga)
@@ -706,7 +711,7 @@ int mixed_potential(MixedState* m, const BuildArgs& a, bool gga, cudaStream_t st
   k_oz_quant_fn<kRowsB><<<dim3((unsigned)m->ntb, (unsigned)nks), kRowsB, 0, st>>>(m->phi, m->ldp, m->e_fn, nks,
                                                                                  m->tP2);
   cudaEventRecord(k0, st);
-  const int smem = (int)sizeof(OzSmem) + 1024;
+  const int smem = tc::kWholeSmSmem;  // >= sizeof(OzSmem) + 1024 (base alignment)
   k_oz_vpot<<<dim3((unsigned)m->ntiles, (unsigned)m->nsplit), kVThreads, smem, st>>>(
       m->tZ, m->tP2, nks, m->ks_per_split, m->ntb, m->e_Z, m->e_fn, m->ntiles, m->vpart, m->err);
   cudaEventRecord(k1, st);

@@ -836,13 +836,7 @@ int pgxc_batch_create(pgxc_ctx* const* ctx, int32_t n, const double* const* d_C,
   if (ce == cudaSuccess) ce = cudaEventCreate(&b->t1);
   for (int32_t i = 0; i < n && ce == cudaSuccess; ++i) ce = cudaEventCreateWithFlags(&b->join[(size_t)i], cudaEventDisableTiming);
   if (ce != cudaSuccess) return fail(PGXC_ECUDA, std::string("batch: ") + cudaGetErrorString(ce));
-  // Fork from the batch stream into every context's stream and join back.  The
-  // INT8 density kernel has given wrong rho for some 32-point groups when other
-  // kernels ran beside it on the GPU (sequential builds are exact and
-  // deterministic), so a batch holding an INT8 context chains its builds one
-  // after another inside the graph; FP64 builds run concurrently.
-  bool chain = false;
-  for (int32_t i = 0; i < n; ++i) chain = chain || ctx[i]->opt.precision != PGXC_PREC_FP64;
+  // fork from the batch stream into every context's stream, join back
   ce = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed);
   if (ce != cudaSuccess) return fail(PGXC_ECUDA, std::string("batch: begin capture: ") + cudaGetErrorString(ce));
   int st = PGXC_OK;
@@ -850,7 +844,7 @@ int pgxc_batch_create(pgxc_ctx* const* ctx, int32_t n, const double* const* d_C,
   ce = cudaEventRecord(b->fork, b->stream);
   for (int32_t i = 0; i < n && ce == cudaSuccess && st == PGXC_OK; ++i) {
     pgxc_ctx* c = ctx[i];
-    ce = cudaStreamWaitEvent(c->stream, chain && i > 0 ? b->join[(size_t)i - 1] : b->fork, 0);
+    ce = cudaStreamWaitEvent(c->stream, b->fork, 0);
     if (ce != cudaSuccess) break;
     if ((st = enqueue_screened_build(c, d_C[i], d_occ[i], nocc[i], d_ham[i], d_exc_nel[i]))) {
       msg = "batch: context " + std::to_string(i) + ": " + c->err;

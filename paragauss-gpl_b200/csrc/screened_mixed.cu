@@ -234,7 +234,7 @@ struct DensSmem {
   uint32_t tslot;
 };
 // warps 0-7 epilogue, 8 MMA, 9 operand copies, 10 epilogue-operand copies
-constexpr int kDensThreads = 352;
+constexpr int kDensThreads = tc::kWholeSmThreads;  // warps 11-15 idle
 
 // TMEM -> the 24 combined FP64 values of column half `half` of one
 // accumulator set (columns 24 half .. 24 half + 23 of each group; taddr is the
@@ -385,6 +385,8 @@ __global__ void __launch_bounds__(kDensThreads, 1)
       }
       if (!ok) atomicExch(err, 1);
     }
+  } else if (warp >= 11) {
+    // idle: the CTA holds the whole SM
   } else {  // epilogue: point row = 32 (warp & 3) + lane, columns 24 (warp >> 2) .. +24 of each slot block
     const int row = (warp & 3) * 32 + lane, half = warp >> 2;
     const uint32_t trow = tbase + ((uint32_t)((warp & 3) * 32) << 16);
@@ -562,7 +564,7 @@ struct VSmem {
   uint64_t acc_empty[2];
   uint32_t tslot;
 };
-constexpr int kVThreads = 320;  // warps 0-7 epilogue, 8 MMA, 9 producer
+constexpr int kVThreads = tc::kWholeSmThreads;  // warps 0-7 epilogue, 8 MMA, 9 producer, 10-15 idle
 
 // LDA keeps j >= i: the last 48-slot row block I of column block J
 __device__ __forceinline__ int last_I(int J, int nI, bool all) { return all ? nI : min(nI, (kM * J + kM - 1) / kN + 1); }
@@ -668,6 +670,8 @@ __global__ void __launch_bounds__(kVThreads, 1)
       }
       if (!ok) atomicExch(err, 1);
     }
+  } else if (warp >= 10) {
+    // idle: the CTA holds the whole SM
   } else {  // epilogue: column j = 128 J + 32 (warp & 3) + lane of H, rows 24 (warp >> 2) .. of each 48-slot block
     const int half = warp >> 2;
     const uint32_t trow = tbase + ((uint32_t)((warp & 3) * 32) << 16);
@@ -757,12 +761,13 @@ int screen_mixed_create(ScreenMixed** out, const ScreenMixedInput& in, std::stri
     screen_mixed_destroy(m);
     return e == cudaErrorMemoryAllocation ? PGXC_ENOMEM : PGXC_ECUDA;
   }
-  const int dsm = (int)sizeof(DensSmem);
+  static_assert(sizeof(DensSmem) <= tc::kWholeSmSmem && sizeof(VSmem) <= tc::kWholeSmSmem, "smem");
+  const int dsm = tc::kWholeSmSmem;
   raise_smem_limit(k_sm_gather_B, 4 * in.max_n);
   cudaFuncSetAttribute(k_sm_density<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm);
   cudaFuncSetAttribute(k_sm_density<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm);
-  cudaFuncSetAttribute(k_sm_vpot<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(VSmem));
-  e = cudaFuncSetAttribute(k_sm_vpot<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(VSmem));
+  cudaFuncSetAttribute(k_sm_vpot<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kWholeSmSmem);
+  e = cudaFuncSetAttribute(k_sm_vpot<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kWholeSmSmem);
   int dev = 0;
   if (e == cudaSuccess) e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&m->nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -815,7 +820,7 @@ int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn,
     cudaMemsetAsync(grz, 0, sizeof(double) * nt * 128, st);
   }
   const unsigned grid = (unsigned)std::min<int64_t>(nt, m->nsm);
-  const int smem = (int)sizeof(DensSmem);
+  const int smem = tc::kWholeSmSmem;
   if (m->gga)
     k_sm_density<true><<<grid, kDensThreads, smem, st>>>(tso, slot_fn, t0, nt, s0, tA, e_pt, m->tB, m->b_off,
                                                          m->ps, phi, gx, gy, gz, rho, grx, gry, grz, m->err);
@@ -841,10 +846,10 @@ int screen_mixed_potential(ScreenMixed* m, const int64_t* tso, const int* slot_f
   if (k0) cudaEventRecord(k0, st);
   const unsigned grid = (unsigned)std::min<int64_t>(nt, m->nsm);
   if (m->gga)
-    k_sm_vpot<true><<<grid, kVThreads, (int)sizeof(VSmem), st>>>(tso, slot_fn, t0, nt, s0, m->tF, m->tZ, m->fs, m->zs, V, ldv,
+    k_sm_vpot<true><<<grid, kVThreads, tc::kWholeSmSmem, st>>>(tso, slot_fn, t0, nt, s0, m->tF, m->tZ, m->fs, m->zs, V, ldv,
                                                    m->err);
   else
-    k_sm_vpot<false><<<grid, kVThreads, (int)sizeof(VSmem), st>>>(tso, slot_fn, t0, nt, s0, m->tF, m->tZ, m->fs, m->zs, V, ldv,
+    k_sm_vpot<false><<<grid, kVThreads, tc::kWholeSmSmem, st>>>(tso, slot_fn, t0, nt, s0, m->tF, m->tZ, m->fs, m->zs, V, ldv,
                                                     m->err);
   if (k1) cudaEventRecord(k1, st);
   return 2;

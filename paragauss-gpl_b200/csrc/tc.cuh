@@ -18,6 +18,15 @@ namespace tc {
 // and the kernel winds down instead of spinning for ever.
 constexpr long long kWaitLimit = 1ll << 24;
 
+// The tensor-core kernels (tcgen05 + TMEM) claim a whole SM: 16 warps and all
+// of its shared memory, so that no CTA of another kernel is placed beside them.
+// With other CTAs on the same SM (builds running concurrently on the GPU) their
+// epilogue warps were seen to read wrong accumulator rows in whole 32-lane
+// quarters; alone on the SM they are exact.  Warps beyond a kernel's roles
+// idle until the final barrier.
+constexpr int kWholeSmThreads = 512;
+constexpr int kWholeSmSmem = 227 * 1024;
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
