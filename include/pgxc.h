@@ -55,6 +55,17 @@ extern "C" {
 /* BP86: Slater + VWN5 + Becke 88 exchange + Perdew 86 correlation
  * (keyword "BP", modules/xc_cntrl.f90:508-520) */
 #define PGXC_XC_BP86 5
+/* PW91: Slater + PW92 + PW91 exchange enhancement + PW91 correlation H0 + H1
+ * (keyword "PW91", modules/xc_cntrl.f90:574-590) */
+#define PGXC_XC_PW91 6
+/* BPW91: Slater + PW92 + Becke 88 exchange + PW91 correlation
+ * (keyword "BPW91", modules/xc_cntrl.f90:561-572) */
+#define PGXC_XC_BPW91 7
+/* BLYP: Slater + Becke 88 exchange + LYP correlation (LYP is a whole
+ * correlation, no LDA part; keyword "BLYP", modules/xc_cntrl.f90:522-532) */
+#define PGXC_XC_BLYP 8
+/* the largest functional id */
+#define PGXC_XC_LAST PGXC_XC_BLYP
 
 /* ---- precision modes ------------------------------------------------- */
 #define PGXC_PREC_FP64        0  /* FP64 everywhere (FP64 tensor pipe): the drop-in */
@@ -114,7 +125,7 @@ typedef struct pgxc_grid {
 } pgxc_grid;
 
 typedef struct pgxc_options {
-  int32_t functional;            /* PGXC_XC_VWN | _PBE | _REVPBE | _PBESOL | _BP86 */
+  int32_t functional;            /* PGXC_XC_VWN .. PGXC_XC_LAST             */
   int32_t ispin;                 /* 1 or 2; 2 (open shell) needs screen_threshold >= 0,
                                   * the dense layout returns PGXC_ENOTSUP */
   int32_t precision;             /* PGXC_PREC_*                             */

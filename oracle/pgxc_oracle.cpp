@@ -126,17 +126,26 @@ D x_lda(D rho) {
 // g_revpbe :641-655 (1.245, the same mu) or g_pbesol :657-670 (0.804, 10/81).
 // Returns F, dF/dn, dF/dgam of the RKS functional e(n, gam).
 // ---------------------------------------------------------------------------
+// Exchange enhancement G(s^2) and gradient correlation of a keyword
+// (xc_cntrl.f90:508-590): BP = Slater + VWN5 + B88 + P86, BPW91 = Slater +
+// PW92 + B88 + PW91c, PW91 = Slater + PW92 + PW91x + PW91c, BLYP = Slater +
+// B88 + LYP; the PBE-form keywords differ in kappa, mu and beta.
+enum { GX_PBE, GX_B88, GX_PW91 };
+enum { GC_PBE, GC_P86, GC_PW91, GC_LYP };
 struct GgaPar {
   double kappa, mu, beta_c;  // exchange kappa, mu; correlation beta (pbe_ggcc :249-270)
-  bool b88;                  // exchange enhancement of Becke 88 (g_becke88) instead of the PBE form
+  int gx, gc;                // kind of exchange enhancement and of gradient correlation
 };
 GgaPar gga_par(int xc) {
   const double pi = PI_EXCH;
   const double mu_pbe = 0.066725 * (pi * pi / 3.0);
-  if (xc == PGXC_XC_REVPBE) return {1.245, mu_pbe, 0.066725, false};
-  if (xc == PGXC_XC_PBESOL) return {0.804, 10.0 / 81.0, 0.046, false};
-  if (xc == PGXC_XC_BP86) return {0.0, 0.0, 0.0, true};
-  return {0.804, mu_pbe, 0.066725, false};
+  if (xc == PGXC_XC_REVPBE) return {1.245, mu_pbe, 0.066725, GX_PBE, GC_PBE};
+  if (xc == PGXC_XC_PBESOL) return {0.804, 10.0 / 81.0, 0.046, GX_PBE, GC_PBE};
+  if (xc == PGXC_XC_BP86) return {0.0, 0.0, 0.0, GX_B88, GC_P86};
+  if (xc == PGXC_XC_PW91) return {0.0, 0.0, 0.0, GX_PW91, GC_PW91};
+  if (xc == PGXC_XC_BPW91) return {0.0, 0.0, 0.0, GX_B88, GC_PW91};
+  if (xc == PGXC_XC_BLYP) return {0.0, 0.0, 0.0, GX_B88, GC_LYP};
+  return {0.804, mu_pbe, 0.066725, GX_PBE, GC_PBE};
 }
 
 // Becke 88 enhancement: g_becke88 (exchange.f90:672-705, the BECKE88_0042
@@ -157,6 +166,22 @@ D g_becke88(D s2) {
   return s2 * (Dd + s2 * (-B * A * Dd));
 }
 
+// PW91 enhancement: g_pw91 (exchange.f90:919-962),
+// G = s^2 (D - C s^2 - E exp(-100 s^2)) / (1 + A s asinh(B s) + C s^4), or
+// s^2 (T1 + T2 s^2) with T1 = D - E, T2 = (B A + 100) E - B A D - C when
+// s^2 <= 1e-4.
+D g_pw91(D s2) {
+  const double A = 0.19645, B = 7.7956, C = 0.004, Dd = 0.2743, E = 0.1508, H = 100.0;
+  const double T1 = Dd - E, T2 = (B * A + H) * E - B * A * Dd - C;
+  if (s2.v > 1.0e-4) {
+    D nomin = Dd - C * s2 - E * dexp(-H * s2);
+    D s = dsqrt(s2);
+    D denom = 1.0 + A * s * dasinh(B * s) + C * (s2 * s2);
+    return s2 * nomin / denom;
+  }
+  return s2 * (T1 + s2 * T2);
+}
+
 void x_gga_pbe(const GgaPar& P, double n, double gam, double& F, double& dFdn, double& dFdg) {
   const double pi = PI_EXCH;
   const double xalpha = -(3.0 / 4.0) * std::pow(3.0 / pi, 1.0 / 3.0);
@@ -171,7 +196,7 @@ void x_gga_pbe(const GgaPar& P, double n, double gam, double& F, double& dFdn, d
   }
   const double kappa = P.kappa, mu = P.mu;
   D s2 = var(0, s2_0);
-  D G = P.b88 ? g_becke88(s2) : kappa * mu * s2 / (kappa + mu * s2);
+  D G = P.gx == GX_B88 ? g_becke88(s2) : P.gx == GX_PW91 ? g_pw91(s2) : kappa * mu * s2 / (kappa + mu * s2);
   F += ex.v * G.v;
   dFdn += ex.d[0] * G.v + ex.v * G.d[0] * s2_r;
   dFdg += ex.v * G.d[0] * s2_g;
@@ -291,7 +316,90 @@ D c_gga(double beta, D na, D nb, D g2) {
 }
 
 // ---------------------------------------------------------------------------
-// xc_functionals (modules/xc_func.f90:187-305) for the two keywords.
+// PW91 correlation H0 + H1: gga_correlation / pbe_or_pw91 with C_PW91
+// (modules/gga_response_module.f90:170-582), H_pw91 :603-621, H0_drv
+// :624-670, H1_drv :673-709, F_drv, S_drv, Cc_drv :712-840, Hln_drv, A_drv
+// :843-918, parameters :150-156.  Arguments: spin densities, |grad n|^2 and
+// the LDA correlation energy per volume ec that precedes it (pw_ldac).
+// Returns n H.  n below 1e-20 is replaced by 1e-20 in value only: the
+// reference's derivative formulas treat the floored n as the variable.  The
+// derivative of phi in na, nb is the reference's closed form with 1e-20 under
+// the cube roots (:416-420).
+// ---------------------------------------------------------------------------
+D c_pw91(D na, D nb, D gm, D ec) {
+  const double eps = 1.0e-20, pi = 3.14159265358979324;
+  const double alpha = 0.09, nu = 15.755920349483144658863574030524, Cc0 = 0.004235, Cx = -0.001667;
+  const double beta = nu * Cc0, gamma = beta * beta / (2.0 * alpha), bdg = beta / gamma;
+  D nn = na + nb;
+  if (std::fabs(nn.v) < eps) nn.v = eps;
+  D rs = 1.91916 / dpow((3.0 * pi * pi) * nn, 1.0 / 3.0);
+  const double z = (na.v - nb.v) / nn.v;
+  D phi;
+  phi.v = 0.5 * (std::pow(1.0 + z, 2.0 / 3.0) + std::pow(1.0 - z, 2.0 / 3.0));
+  const double c = (1.0 / 3.0) * std::pow(2.0, 2.0 / 3.0) / std::pow(nn.v, 5.0 / 3.0);
+  const double dpa = c * (nb.v / std::pow(na.v + eps, 1.0 / 3.0) - std::pow(nb.v, 2.0 / 3.0));
+  const double dpb = c * (na.v / std::pow(nb.v + eps, 1.0 / 3.0) - std::pow(na.v, 2.0 / 3.0));
+  for (int i = 0; i < 3; ++i) phi.d[i] = dpa * na.d[i] + dpb * nb.d[i];
+  const double t2_fact = pi / (4.0 * 4.0 * std::pow(3.0 * pi * pi, 1.0 / 3.0));
+  D t = t2_fact * gm / dipow(phi * dpow(nn, 7.0 / 6.0), 2);  // t^2
+  D e = ec / nn;
+  D p3 = dipow(phi, 3);
+  // H0 (A_drv, Hln_drv)
+  D Xe = -e / (gamma * p3);
+  D A = bdg / ((dexp(Xe) - 1.0) + eps);
+  if (Xe.v > 300.0) A = fix(A);
+  D At = 1.0 + A * t;
+  D At2 = At + dipow(A * t, 2);
+  D g = (bdg * t) * (At / At2);
+  D H0 = gamma * p3 * dlog(1.0 + g);
+  // H1 = F S (Cc_drv, F_drv, S_drv)
+  D rs2 = rs * rs;
+  D Fup = 2.568 + 23.266 * rs + 0.007389 * rs2;
+  D Fdn = 1.0 + 8.723 * rs + 0.472 * rs2 + 0.073890 * rs2 * rs;
+  D Cc = Fup / Fdn / 1000.0 - Cx;
+  D F = nu * (Cc - Cc0 - (3.0 / 7.0) * Cx) * p3 * t;
+  const double ksf = 4.0 / (1.91916 * pi);
+  D S = dexp(-100.0 * (p3 * phi) * t * ksf * rs);
+  return nn * (H0 + F * S);
+}
+
+// ---------------------------------------------------------------------------
+// LYP correlation: lyp_corr (modules/lyp.f90, parameter set 1: a = 0.04918,
+// b = 0.132, c = 0.2533, d = 0.349, e = 3/10 (3 pi^2)^(2/3) as its literal).
+// F is linear in gaa, gbb, gab: returns F with derivatives in (ra, rb) and
+// the three gradient coefficients dF/dg_*.
+// ---------------------------------------------------------------------------
+D lyp_corr(D ra, D rb, double gaa, double gbb, double gab, double (&cg)[3]) {
+  const double a = 0.04918, b = 0.13200, c = 0.25330, d = 0.34900, e = 2.87123400018819, DTol = 1.0e-30;
+  D rsum = ra + rb;
+  D qZ = cst(0.0), qw = cst(0.0), qd = cst(0.0);
+  if (rsum.v > DTol) {
+    D r13 = dpow(rsum, 1.0 / 3.0);
+    qZ = r13 / (d + r13);
+    qw = dexp(-c / r13) * qZ * dpow(rsum, -11.0 / 3.0);
+    qd = (c + d * qZ) / r13;
+  }
+  D f1 = a * b * qw;
+  D f2 = f1 * ra * rb;
+  D lda_t1 = rsum.v > DTol ? 4.0 * a * ra * rb * qZ / rsum : cst(0.0);
+  D lda_t2 = f2 * std::pow(2.0, 11.0 / 3.0) * e * (dpow(ra, 8.0 / 3.0) + dpow(rb, 8.0 / 3.0));
+  D k_aa, k_bb;
+  if (rsum.v > DTol) {
+    k_aa = f2 * (1.0 / 9.0 - (1.0 / 3.0) * qd - (1.0 / 9.0) * (qd - 11.0) * ra / rsum) - f1 * rb * rb;
+    k_bb = f2 * (1.0 / 9.0 - (1.0 / 3.0) * qd - (1.0 / 9.0) * (qd - 11.0) * rb / rsum) - f1 * ra * ra;
+  } else {
+    k_aa = f2 * (1.0 / 9.0 - (1.0 / 3.0) * qd) - f1 * rb * rb;
+    k_bb = f2 * (1.0 / 9.0 - (1.0 / 3.0) * qd) - f1 * ra * ra;
+  }
+  D k_ab = f2 * (47.0 / 9.0 - (7.0 / 9.0) * qd) - f1 * (4.0 / 3.0) * rsum * rsum;
+  cg[0] = -k_aa.v;
+  cg[1] = -k_bb.v;
+  cg[2] = -k_ab.v;
+  return -lda_t1 - lda_t2 - k_aa * gaa - k_bb * gbb - k_ab * gab;
+}
+
+// ---------------------------------------------------------------------------
+// xc_functionals (modules/xc_func.f90:187-305) for the keywords.
 // rho[ispin], gam[2*ispin-1] (aa, bb, ab); outputs f, fr[ispin], fg[2ispin-1].
 // ---------------------------------------------------------------------------
 // ---------------------------------------------------------------------------
@@ -368,18 +476,21 @@ void functional_point(int xc, int ispin, const double* rho, const double* gam,
       f += e.v / 2.0; fr[s] += e.d[0];
     }
   }
-  if (xc == PGXC_XC_VWN || xc == PGXC_XC_BP86) {
-    // vwn_ldac, vwnc.f90:225-297
-    D c;
-    if (ispin == 1) { D nn = var(0, rho[0]); c = vwn::c_lda(0.5 * nn, 0.5 * nn); f += c.v; fr[0] += c.d[0]; }
-    else { c = vwn::c_lda(var(0, rho[0]), var(1, rho[1])); f += c.v; fr[0] += c.d[0]; fr[1] += c.d[1]; }
-    if (xc == PGXC_XC_VWN) return;
-  } else {
-    // PBE-form keywords: pw_ldac (pw_ldac_module.f90:197-312)
-    if (ispin == 1) { D nn = var(0, rho[0]); D c = pw92::c_lda(0.5 * nn, 0.5 * nn); f += c.v; fr[0] += c.d[0]; }
-    else { D c = pw92::c_lda(var(0, rho[0]), var(1, rho[1])); f += c.v; fr[0] += c.d[0]; fr[1] += c.d[1]; }
+  // LDA correlation: VWN5 (vwn_ldac, vwnc.f90:225-297) for "VWN" and "BP",
+  // none for "BLYP" (LYP is a whole correlation), else PW92 (pw_ldac,
+  // pw_ldac_module.f90:197-312).  ec is kept for the PW91 correlation.
+  D ec = cst(0.0);
+  if (xc == PGXC_XC_VWN || P.gc == GC_P86) {
+    if (ispin == 1) { D nn = var(0, rho[0]); ec = vwn::c_lda(0.5 * nn, 0.5 * nn); }
+    else ec = vwn::c_lda(var(0, rho[0]), var(1, rho[1]));
+  } else if (P.gc != GC_LYP) {
+    if (ispin == 1) { D nn = var(0, rho[0]); ec = pw92::c_lda(0.5 * nn, 0.5 * nn); }
+    else ec = pw92::c_lda(var(0, rho[0]), var(1, rho[1]));
   }
-  // PBE exchange (exchange_gga, exchange.f90:206-292)
+  f += ec.v; fr[0] += ec.d[0];
+  if (ispin == 2) fr[1] += ec.d[1];
+  if (xc == PGXC_XC_VWN) return;
+  // GGA exchange enhancement (exchange_gga, exchange.f90:206-292)
   if (ispin == 1) {
     double F = 0, Fn = 0, Fg = 0;
     x_gga_pbe(P, rho[0], gam[0], F, Fn, Fg);
@@ -391,20 +502,42 @@ void functional_point(int xc, int ispin, const double* rho, const double* gam,
       f += 0.5 * F; fr[s] += Fn; fg[s] += 2.0 * Fg;
     }
   }
-  if (xc == PGXC_XC_BP86) {  // "BP": Perdew 86 correlation (xc_cntrl.f90:508-520)
+  if (P.gc == GC_P86) {  // "BP": Perdew 86 correlation (xc_cntrl.f90:508-520)
     perdew86(ispin, rho, gam, f, fr, fg);
     return;
   }
-  // PBE correlation H (pbe_ggcc, pbe_ggcxc_module.f90:214-348)
+  if (P.gc == GC_LYP) {
+    // lyp_C (lyp.f90): closed shell at ra = rb = n/2, gaa = gbb = gab = g/4,
+    // returning dF/dra and the coefficient of gaa (dF/dgaa) as dF/dn, dF/dg
+    double cg[3];
+    if (ispin == 1) {
+      const double q = 0.25 * gam[0];
+      D F = lyp_corr(var(0, 0.5 * rho[0]), var(1, 0.5 * rho[0]), q, q, q, cg);
+      f += F.v; fr[0] += F.d[0]; fg[0] += cg[0];
+    } else {
+      D F = lyp_corr(var(0, rho[0]), var(1, rho[1]), gam[0], gam[1], gam[2], cg);
+      f += F.v; fr[0] += F.d[0]; fr[1] += F.d[1];
+      fg[0] += cg[0]; fg[1] += cg[1]; fg[2] += cg[2];
+    }
+    return;
+  }
+  // PBE correlation H (pbe_ggcc, pbe_ggcxc_module.f90:214-348) or PW91's
+  // (gga_correlation, gga_response_module.f90:170-275; gm floored at 1e-20 for ispin = 2)
   if (ispin == 1) {
     D nn = var(0, rho[0]);
     D g2 = var(1, gam[0]);
-    D c = c_gga(P.beta_c, 0.5 * nn, 0.5 * nn, g2);
+    D c = P.gc == GC_PW91 ? c_pw91(0.5 * nn, 0.5 * nn, g2, ec) : c_gga(P.beta_c, 0.5 * nn, 0.5 * nn, g2);
     f += c.v; fr[0] += c.d[0]; fg[0] += c.d[1];
   } else {
     D na = var(0, rho[0]), nb = var(1, rho[1]);
     D g2 = var(2, gam[0] + gam[1] + 2.0 * gam[2]);
-    D c = c_gga(P.beta_c, na, nb, g2);
+    D c;
+    if (P.gc == GC_PW91) {
+      if (g2.v < 1.0e-20) g2.v = 1.0e-20;
+      c = c_pw91(na, nb, g2, ec);
+    } else {
+      c = c_gga(P.beta_c, na, nb, g2);
+    }
     f += c.v; fr[0] += c.d[0]; fr[1] += c.d[1];
     fg[0] += c.d[2]; fg[1] += c.d[2]; fg[2] += 2.0 * c.d[2];
   }
@@ -720,7 +853,7 @@ int oracle_orbitals(const pgxc_geometry* geo, const pgxc_basis* bas, int64_t npt
 // VWN), outputs f (n), fr (n,ispin), fg (n,2ispin-1) (may be NULL for VWN).
 int oracle_functionals(int32_t xc, int32_t ispin, int64_t n, const double* rho, const double* gam,
                        double* f, double* fr, double* fg) {
-  if (xc < PGXC_XC_VWN || xc > PGXC_XC_BP86 || (ispin != 1 && ispin != 2)) return PGXC_EINVAL;
+  if (xc < PGXC_XC_VWN || xc > PGXC_XC_LAST || (ispin != 1 && ispin != 2)) return PGXC_EINVAL;
   const int ng = 2 * ispin - 1;
   for (int64_t i = 0; i < n; ++i) {
     double r[2] = {rho[i], ispin == 2 ? rho[i + n] : 0.0};
@@ -803,7 +936,7 @@ int oracle_xc_build(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_
   const int64_t nb = B.nbas;
   if (nb != nbas_in || (ispin != 1 && ispin != 2) || nocc < 0) return PGXC_EINVAL;
   if (xc_length != (int64_t)ispin * nb * (nb + 1) / 2) return PGXC_EINVAL;
-  if (xc < PGXC_XC_VWN || xc > PGXC_XC_BP86) return PGXC_EINVAL;
+  if (xc < PGXC_XC_VWN || xc > PGXC_XC_LAST) return PGXC_EINVAL;
   if (grid->weights_are_raw) return PGXC_EINVAL;  // the oracle integrates a weighted grid
   if (vla <= 0 || vla > 128) vla = 128;
   const int64_t npts = grid->npts;

@@ -235,7 +235,7 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
     pgxc_destroy(c);
     return st;
   };
-  if (o.functional < PGXC_XC_VWN || o.functional > PGXC_XC_BP86)
+  if (o.functional < PGXC_XC_VWN || o.functional > PGXC_XC_LAST)
     return fail(set_err(c, PGXC_EINVAL, "unknown functional id"));
   if (o.ispin != 1 && o.ispin != 2) return fail(set_err(c, PGXC_EINVAL, "ispin must be 1 or 2"));
   if (o.ispin == 2 && !(o.screen_threshold >= 0.0))
@@ -957,7 +957,7 @@ int pgxc_orbital_calculate(pgxc_ctx* c, int64_t npts, const double* pts, double*
 
 int pgxc_xc_functionals(int32_t functional, int32_t ispin, int64_t n, const double* rho, const double* gam, double* f,
                         double* fr, double* fg) {
-  if (functional < PGXC_XC_VWN || functional > PGXC_XC_BP86) return set_err(nullptr, PGXC_EINVAL, "functional");
+  if (functional < PGXC_XC_VWN || functional > PGXC_XC_LAST) return set_err(nullptr, PGXC_EINVAL, "functional");
   if (ispin != 1 && ispin != 2) return set_err(nullptr, PGXC_EINVAL, "ispin must be 1 or 2");
   if (n < 0 || !rho || !f || !fr) return set_err(nullptr, PGXC_EINVAL, "bad arguments");
   const bool gga = functional != PGXC_XC_VWN;

@@ -9,8 +9,15 @@
 //   PW92 correlation      modules/pw_ldac_module.f90:127-312, :591-651
 //   PBE exchange G(s^2)   modules/exchange.f90:325-439, :617-639, :858-867
 //   PBE correlation H     modules/pbe_ggcxc_module.f90:96-348
-// composed as the XC keywords do (modules/xc_cntrl.f90:460-465, :652-670):
-//   "VWN" = Slater + VWN5, "PBE" = Slater + PW92 + PBE-X(G) + PBE-C(H).
+//   Becke 88 G(s^2)       modules/exchange.f90:672-705, :964-991
+//   PW91 exchange G(s^2)  modules/exchange.f90:919-962
+//   Perdew 86 correlation modules/becke_perdew_module.f90:125-260
+//   PW91 correlation      modules/gga_response_module.f90:278-918 (H0 + H1)
+//   LYP correlation       modules/lyp.f90 (lyp_C, lyp_corr)
+// composed as the XC keywords do (modules/xc_cntrl.f90:460-798):
+//   "VWN" = Slater + VWN5, "PBE" = Slater + PW92 + PBE-X(G) + PBE-C(H),
+//   "BP" = Slater + VWN5 + B88 + P86, "PW91" = Slater + PW92 + PW91-X + PW91-C,
+//   "BPW91" = Slater + PW92 + B88 + PW91-C, "BLYP" = Slater + B88 + LYP.
 // Literal constants, density guards and epsilons are the reference's.
 #pragma once
 
@@ -34,9 +41,12 @@ struct XcConst {
   double pbe_kappa;     // enhancement-factor kappa (PBE 0.804, revPBE 1.245)
   double pbe_mu;        // beta*pi^2/3 (PBE, revPBE) or 10/81 (PBEsol)
   double pbe_beta;      // correlation beta (PBE 0.066725, PBEsol 0.046)
-  // Becke 88 (BP86): exchange enhancement constants of g_becke88, and the kind of GGA
+  // Becke 88: exchange enhancement constants of g_becke88
   double b88_A, b88_B, b88_D;
-  int bp86;             // 1: Slater + VWN5 + Becke 88 + Perdew 86; 0: the PBE-form keywords
+  // LYP: 2^(11/3)
+  double lyp_2113;
+  int xg;               // exchange enhancement G(s^2): XG_PBE, XG_B88 or XG_PW91
+  int cg;               // correlation: CG_PBE, CG_P86, CG_PW91 or CG_LYP
   // PBE correlation
   double pbe_fi;        // (0.5^(2/3)+0.5^(2/3)) * (1/2^(1/3))
   double pbe_ct;        // pi/(16 (3 pi^2)^(1/3))
@@ -46,9 +56,15 @@ struct XcConst {
   double pbe_two13i;    // 1 / 2^(1/3)
 };
 
-// Constants of the functional (PGXC_XC_*): the GGA keywords differ only in
-// the PBE-form parameters (exchange.f90 g_pbe / g_revpbe / g_pbesol :617-670,
-// pbe_ggcxc_module.f90 pbe_ggcc :249-270).
+// GGA pieces of a keyword.  Exchange enhancement: the PBE form (kappa, mu),
+// Becke 88, or PW91.  Correlation: PW92 + PBE H, VWN5 + Perdew 86, PW92 +
+// PW91 H0 + H1, or LYP (a whole correlation: no LDA part).
+constexpr int XG_PBE = 0, XG_B88 = 1, XG_PW91 = 2;
+constexpr int CG_PBE = 0, CG_P86 = 1, CG_PW91 = 2, CG_LYP = 3;
+
+// Constants of the functional (PGXC_XC_*): the PBE-form keywords differ only
+// in their parameters (exchange.f90 g_pbe / g_revpbe / g_pbesol :617-670,
+// pbe_ggcxc_module.f90 pbe_ggcc :249-270), the others in their pieces.
 __host__ inline XcConst make_xc_const(int functional = PGXC_XC_PBE) {
   XcConst c;
   const double pi_x = 3.14159265358979324;  // exchange.f90 uses constants.f90 pi
@@ -66,7 +82,12 @@ __host__ inline XcConst make_xc_const(int functional = PGXC_XC_PBE) {
   c.b88_A = 6.0 * 0.0042 * std::pow(2.0, 1.0 / 3.0) * std::pow(3.0 * pi_x * pi_x, 1.0 / 3.0) * 2.0;
   c.b88_D = c.b88_A * (4.0 * pi_x) / 9.0;
   c.b88_B = 2.0 * std::pow(6.0 * pi_x * pi_x, 1.0 / 3.0);
-  c.bp86 = functional == PGXC_XC_BP86 ? 1 : 0;
+  c.lyp_2113 = std::pow(2.0, 11.0 / 3.0);
+  const bool b88 = functional == PGXC_XC_BP86 || functional == PGXC_XC_BPW91 || functional == PGXC_XC_BLYP;
+  c.xg = b88 ? XG_B88 : functional == PGXC_XC_PW91 ? XG_PW91 : XG_PBE;
+  c.cg = functional == PGXC_XC_BP86 ? CG_P86
+         : (functional == PGXC_XC_PW91 || functional == PGXC_XC_BPW91) ? CG_PW91
+         : functional == PGXC_XC_BLYP ? CG_LYP : CG_PBE;
   c.pbe_fi = (std::pow(0.5, 2.0 / 3.0) + std::pow(0.5, 2.0 / 3.0)) * (1.0 / std::pow(2.0, 1.0 / 3.0));
   c.pbe_ct = pi_p / (4.0 * 4.0 * std::pow(3.0 * pi_p * pi_p, 1.0 / 3.0));
   c.vwn_ffact = 0.5 / (std::pow(2.0, 1.0 / 3.0) - 1.0);
@@ -130,8 +151,8 @@ __device__ __forceinline__ void xc_vwn(const XcConst& K, double n, double& f, do
 }
 
 // GGA exchange enhancement of the closed-shell functional e(n, g): e_x G(s^2),
-// the 1 of (1+G) omitted (x_gga, exchange.f90:325-439), G of the PBE form or
-// of Becke 88 (BP86); adds F, dF/dn, dF/dg.
+// the 1 of (1+G) omitted (x_gga, exchange.f90:325-439), G of the PBE form,
+// of Becke 88 or of PW91; adds F, dF/dn, dF/dg.
 __device__ __forceinline__ void pbe_x(const XcConst& K, double n, double g, double& f, double& fr, double& fg) {
   double ex = 0.0, exr = 0.0;
   if (n > 0.0) {
@@ -148,7 +169,7 @@ __device__ __forceinline__ void pbe_x(const XcConst& K, double n, double g, doub
     s2r = -(8.0 / 3.0) * s2 / n;
   }
   double G, Gs;  // G(s^2) and dG/ds^2
-  if (K.bp86) {
+  if (K.xg == XG_B88) {
     // Becke 88: G = D s^2 / (1 + A s asinh(B s)), below s^2 = 1e-4 its series
     // D s^2 - B A D s^4 (g_becke88_form, exchange.f90:964-991)
     const double A = K.b88_A, B = K.b88_B, Dd = K.b88_D;
@@ -162,6 +183,24 @@ __device__ __forceinline__ void pbe_x(const XcConst& K, double n, double g, doub
     } else {
       G = s2 * (Dd - B * A * Dd * s2);
       Gs = Dd - 2.0 * B * A * Dd * s2;
+    }
+  } else if (K.xg == XG_PW91) {
+    // PW91: G = s^2 (D - C s^2 - E exp(-100 s^2)) / (1 + A s asinh(B s) + C s^4),
+    // below s^2 = 1e-4 the series s^2 (T1 + T2 s^2) (g_pw91, exchange.f90:919-962)
+    const double A = 0.19645, B = 7.7956, C = 0.004, Dd = 0.2743, E = 0.1508;
+    const double T1 = Dd - E, T2 = (B * A + 100.0) * E - B * A * Dd - C;
+    if (s2 > 1.0e-4) {
+      const double ee = E * exp(-100.0 * s2);
+      const double num = Dd - C * s2 - ee;
+      const double dnum = -C + 100.0 * ee;
+      const double s = sqrt(s2), bs = B * s, ash = asinh(bs);
+      const double den = 1.0 + A * s * ash + C * s2 * s2;
+      const double dden = A * (ash + bs / sqrt(1.0 + bs * bs)) / (2.0 * s) + 2.0 * C * s2;
+      G = s2 * num / den;
+      Gs = (num + s2 * dnum) / den - s2 * num * dden / (den * den);
+    } else {
+      G = s2 * (T1 + s2 * T2);
+      Gs = T1 + 2.0 * T2 * s2;
     }
   } else {
     const double kappa = K.pbe_kappa, mu = K.pbe_mu;
@@ -374,6 +413,80 @@ __device__ __forceinline__ D3 pbe_c_gga(const XcConst& K, D3 na, D3 nb, D3 g2) {
   return n * (gam * fi3 * d3log(1.0 + (beta / gam) * t2 * rat));
 }
 
+// PW91 correlation H0 + H1 (pbe_or_pw91 with H_pw91, H0_drv, H1_drv, F_drv,
+// S_drv, Cc_drv, Hln_drv, A_drv; modules/gga_response_module.f90:278-918,
+// parameters :150-156): n * H(na, nb, g2) with ec = n eps_c of the LDA
+// correlation that precedes it.  The floors of n (1e-20) replace values only:
+// the derivative formulas keep treating n as the variable, as the reference's do.
+__device__ __forceinline__ D3 pw91_c_gga(const XcConst& K, D3 na, D3 nb, D3 g2, D3 ec) {
+  const double eps = 1.0e-20, pi = 3.14159265358979324;
+  const double alpha = 0.09, nu = 15.755920349483144658863574030524, cc0 = 0.004235, cx = -0.001667;
+  const double beta = nu * cc0, gam = beta * beta / (2.0 * alpha), bdg = beta / gam;
+  D3 nn = na + nb;
+  if (fabs(nn.v) < eps) nn.v = eps;
+  const D3 rs = 1.91916 / d3pow((3.0 * pi * pi) * nn, 1.0 / 3.0);
+  // phi = ((1+z)^(2/3) + (1-z)^(2/3)) / 2; its derivatives in na, nb as the
+  // reference writes them (with eps under the cube roots)
+  const double z = (na.v - nb.v) / nn.v;
+  const double phv = 0.5 * (pow(1.0 + z, 2.0 / 3.0) + pow(1.0 - z, 2.0 / 3.0));
+  const double pf = (1.0 / 3.0) * pow(2.0, 2.0 / 3.0) / pow(nn.v, 5.0 / 3.0);
+  const double pa = pf * (nb.v / pow(na.v + eps, 1.0 / 3.0) - pow(nb.v, 2.0 / 3.0));
+  const double pb = pf * (na.v / pow(nb.v + eps, 1.0 / 3.0) - pow(na.v, 2.0 / 3.0));
+  const D3 p = D3{phv, {pa * na.d[0] + pb * nb.d[0], pa * na.d[1] + pb * nb.d[1], pa * na.d[2] + pb * nb.d[2]}};
+  const D3 pn = p * d3pow(nn, 7.0 / 6.0);
+  const D3 t = K.pbe_ct * g2 / (pn * pn);  // t^2
+  const D3 e = ec / nn;                     // eps_c of the LDA
+  const D3 p2 = p * p, p3 = p2 * p;
+  // H0 = gamma phi^3 ln(1 + g), A = (beta/gamma) / (exp(-e / (gamma phi^3)) - 1)
+  const D3 xe = -e / (gam * p3);
+  D3 A = bdg / ((d3exp(xe) - 1.0) + eps);
+  if (xe.v > 300.0) A.d[0] = A.d[1] = A.d[2] = 0.0;
+  const D3 at = A * t;
+  const D3 at1 = 1.0 + at;
+  const D3 at2 = at1 + at * at;
+  const D3 g = (bdg * t) * (at1 / at2);
+  const D3 h0 = gam * p3 * d3log(1.0 + g);
+  // H1 = nu (Cc(rs) - Cc0 - 3 Cx / 7) phi^3 t^2 exp(-100 phi^4 (ks/kF)^2 t^2)
+  const D3 rs2 = rs * rs;
+  const D3 fup = 2.568 + 23.266 * rs + 0.007389 * rs2;
+  const D3 fdn = 1.0 + 8.723 * rs + 0.472 * rs2 + 0.073890 * (rs2 * rs);
+  const D3 cc = fup / fdn / 1000.0 - cx;
+  const D3 F = nu * (cc - cc0 - (3.0 / 7.0) * cx) * p3 * t;
+  const double ksf = 4.0 / (1.91916 * pi);
+  const D3 S = d3exp(-100.0 * (p3 * p) * t * ksf * rs);
+  return nn * (h0 + F * S);
+}
+
+// LYP correlation in the form of lyp_corr (modules/lyp.f90, parameter set 1)
+// for spin densities ra, rb; it is linear in the gradient invariants, so the
+// coefficients c[0..2] of gaa, gbb, gab are returned beside the value:
+// F = F0(ra, rb) + c[0] gaa + c[1] gbb + c[2] gab, with derivatives in ra, rb.
+__device__ __forceinline__ D3 lyp_corr(const XcConst& K, D3 ra, D3 rb, double gaa, double gbb, double gab,
+                                       double (&c)[3]) {
+  const double a = 0.04918, b = 0.13200, cp = 0.25330, d = 0.34900, e = 2.87123400018819, tol = 1.0e-30;
+  const D3 rsum = ra + rb;
+  const bool live = rsum.v > tol;
+  D3 qz = d3c(0.0), qw = d3c(0.0), qd = d3c(0.0);
+  if (live) {
+    const D3 r13 = d3pow(rsum, 1.0 / 3.0);
+    qz = r13 / (d + r13);
+    qw = d3exp(-cp / r13) * qz * d3pow(rsum, -11.0 / 3.0);
+    qd = (cp + d * qz) / r13;
+  }
+  const D3 f1 = (a * b) * qw;
+  const D3 f2 = f1 * ra * rb;
+  const D3 lda1 = live ? 4.0 * a * ra * rb * qz / rsum : d3c(0.0);
+  const D3 lda2 = f2 * K.lyp_2113 * e * (d3pow(ra, 8.0 / 3.0) + d3pow(rb, 8.0 / 3.0));
+  const D3 base = 1.0 / 9.0 - (1.0 / 3.0) * qd;
+  const D3 caa = (live ? f2 * (base - (1.0 / 9.0) * (qd - 11.0) * ra / rsum) : f2 * base) - f1 * (rb * rb);
+  const D3 cbb = (live ? f2 * (base - (1.0 / 9.0) * (qd - 11.0) * rb / rsum) : f2 * base) - f1 * (ra * ra);
+  const D3 cab = f2 * (47.0 / 9.0 - (7.0 / 9.0) * qd) - f1 * (4.0 / 3.0) * (rsum * rsum);
+  c[0] = -caa.v;
+  c[1] = -cbb.v;
+  c[2] = -cab.v;
+  return -lda1 - lda2 - caa * gaa - cbb * gbb - cab * gab;
+}
+
 // Perdew 86 gradient correlation with its first derivatives (perdew_calc,
 // modules/becke_perdew_module.f90:125-260; constants :83-118).  ispin = 1:
 // rho[0], gam[0]; ispin = 2: rho[0..1], gam = (aa, bb, ab), the correlation
@@ -434,14 +547,89 @@ __device__ __forceinline__ void perdew86(int ispin, const double* rho, const dou
 __device__ __forceinline__ void xc_bp86(const XcConst& K, double n, double g, double& f, double& fr, double& fg) {
   xc_vwn(K, n, f, fr);  // Slater + VWN5
   fg = 0.0;
-  pbe_x(K, n, g, f, fr, fg);  // K.bp86: the Becke 88 enhancement
+  pbe_x(K, n, g, f, fr, fg);  // K.xg == XG_B88
   perdew86(1, &n, &g, f, &fr, &fg);
 }
 
-// The closed-shell GGA keyword of K: BP86 or one of the PBE-form keywords.
+// "PW91", "BPW91" (PW92 + PW91 correlation) and "BLYP" (LYP), closed shell,
+// through the dual numbers in (n, g) or, for LYP, in (rho_a, rho_b).
+__device__ __forceinline__ void xc_gga_d3(const XcConst& K, double n, double g, double& f, double& fr, double& fg) {
+  f = 0.0;
+  fr = 0.0;
+  fg = 0.0;
+  slater(K, n, f, fr);
+  pbe_x(K, n, g, f, fr, fg);
+  if (K.cg == CG_PW91) {
+    // gga_correlation (gga_response_module.f90:170-275): na = nb = n/2, the
+    // LDA energy of pw_ldac
+    const D3 nv = d3v(0, n);
+    const D3 na = 0.5 * nv, nb = 0.5 * nv;
+    const D3 ec = pw92_c_lda(K, na, nb);
+    const D3 c = pw91_c_gga(K, na, nb, d3v(1, g), ec);
+    f += ec.v + c.v;
+    fr += ec.d[0] + c.d[0];
+    fg += c.d[1];
+  } else {
+    // lyp_C (lyp.f90): ra = rb = n/2, gaa = gbb = gab = g/4; dF/dn is dF/dra
+    // and dF/dg is the coefficient of gaa alone, as the reference returns them
+    const double q = 0.25 * g;
+    double c3[3];
+    const D3 F = lyp_corr(K, d3v(0, 0.5 * n), d3v(1, 0.5 * n), q, q, q, c3);
+    f += F.v;
+    fr += F.d[0];
+    fg += c3[0];
+  }
+}
+
+// The closed-shell GGA keyword of K.
 __device__ __forceinline__ void xc_gga(const XcConst& K, double n, double g, double& f, double& fr, double& fg) {
-  if (K.bp86) xc_bp86(K, n, g, f, fr, fg);
-  else xc_pbe(K, n, g, f, fr, fg);
+  if (K.cg == CG_PBE) xc_pbe(K, n, g, f, fr, fg);
+  else if (K.cg == CG_P86) xc_bp86(K, n, g, f, fr, fg);
+  else xc_gga_d3(K, n, g, f, fr, fg);
+}
+
+// GGA terms of the open-shell functional: exchange enhancement and gradient
+// correlation; ec = the LDA correlation already added (n eps_c, D3 in na, nb).
+__device__ __forceinline__ void xc_open_gga(const XcConst& K, const double (&rho)[2], const double (&gam)[3], D3 na,
+                                            D3 nb, D3 ec, double& f, double (&fr)[2], double (&fg)[3]) {
+  // exchange enhancement, spin-scaled: e(2 rho_s, 4 gamma_ss) / 2
+  for (int s = 0; s < 2; ++s) {
+    double F = 0.0, Fn = 0.0, Fg = 0.0;
+    pbe_x(K, 2.0 * rho[s], 4.0 * gam[s], F, Fn, Fg);
+    f += 0.5 * F;
+    fr[s] += Fn;
+    fg[s] += 2.0 * Fg;
+  }
+  if (K.cg == CG_P86) {
+    perdew86(2, rho, gam, f, fr, fg);
+    return;
+  }
+  if (K.cg == CG_LYP) {
+    double c3[3];
+    const D3 F = lyp_corr(K, na, nb, gam[0], gam[1], gam[2], c3);
+    f += F.v;
+    fr[0] += F.d[0];
+    fr[1] += F.d[1];
+    fg[0] += c3[0];
+    fg[1] += c3[1];
+    fg[2] += c3[2];
+    return;
+  }
+  // PBE or PW91 correlation H of the total gradient |grad rho_a + grad rho_b|^2
+  D3 g2 = d3v(2, gam[0] + gam[1] + 2.0 * gam[2]);
+  D3 c;
+  if (K.cg == CG_PW91) {
+    if (g2.v < 1.0e-20) g2.v = 1.0e-20;  // gga_correlation's floor of gm
+    c = pw91_c_gga(K, na, nb, g2, ec);
+  } else {
+    c = pbe_c_gga(K, na, nb, g2);
+  }
+  f += c.v;
+  fr[0] += c.d[0];
+  fr[1] += c.d[1];
+  fg[0] += c.d[2];
+  fg[1] += c.d[2];
+  fg[2] += 2.0 * c.d[2];
 }
 
 // Open-shell functional at one point: rho[2] = (rho_a, rho_b), gam[3] =
@@ -461,47 +649,14 @@ __device__ __forceinline__ void xc_open(const XcConst& K, const double (&rho)[2]
     fr[s] += Fn;
   }
   const D3 na = d3v(0, rho[0]), nb = d3v(1, rho[1]);
-  if (!GGA || K.bp86) {
-    const D3 c = vwn_c_lda(K, na, nb);
-    f += c.v;
-    fr[0] += c.d[0];
-    fr[1] += c.d[1];
-    if (GGA) {
-      // BP86: Becke 88 exchange, spin-scaled, and Perdew 86 correlation
-      for (int s = 0; s < 2; ++s) {
-        double F = 0.0, Fn = 0.0, Fg = 0.0;
-        pbe_x(K, 2.0 * rho[s], 4.0 * gam[s], F, Fn, Fg);
-        f += 0.5 * F;
-        fr[s] += Fn;
-        fg[s] += 2.0 * Fg;
-      }
-      perdew86(2, rho, gam, f, fr, fg);
-    }
-    return;
-  }
-  {
-    const D3 c = pw92_c_lda(K, na, nb);
-    f += c.v;
-    fr[0] += c.d[0];
-    fr[1] += c.d[1];
-  }
-  // PBE exchange, spin-scaled: e(2 rho_s, 4 gamma_ss) / 2
-  for (int s = 0; s < 2; ++s) {
-    double F = 0.0, Fn = 0.0, Fg = 0.0;
-    pbe_x(K, 2.0 * rho[s], 4.0 * gam[s], F, Fn, Fg);
-    f += 0.5 * F;
-    fr[s] += Fn;
-    fg[s] += 2.0 * Fg;
-  }
-  // PBE correlation H of the total gradient |grad rho_a + grad rho_b|^2
-  const D3 g2 = d3v(2, gam[0] + gam[1] + 2.0 * gam[2]);
-  const D3 c = pbe_c_gga(K, na, nb, g2);
-  f += c.v;
-  fr[0] += c.d[0];
-  fr[1] += c.d[1];
-  fg[0] += c.d[2];
-  fg[1] += c.d[2];
-  fg[2] += 2.0 * c.d[2];
+  // LDA correlation: VWN5 ("VWN", "BP"), none (LYP), else PW92
+  D3 ec = d3c(0.0);
+  if (!GGA || K.cg == CG_P86) ec = vwn_c_lda(K, na, nb);
+  else if (K.cg != CG_LYP) ec = pw92_c_lda(K, na, nb);
+  f += ec.v;
+  fr[0] += ec.d[0];
+  fr[1] += ec.d[1];
+  if constexpr (GGA) xc_open_gga(K, rho, gam, na, nb, ec, f, fr, fg);
 }
 
 }  // namespace pgxc

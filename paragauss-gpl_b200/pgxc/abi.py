@@ -21,7 +21,11 @@ XC_PBE = 2
 XC_REVPBE = 3
 XC_PBESOL = 4
 XC_BP86 = 5
-XC_IDS = {"VWN": XC_VWN, "PBE": XC_PBE, "revPBE": XC_REVPBE, "PBEsol": XC_PBESOL, "BP86": XC_BP86}
+XC_PW91 = 6
+XC_BPW91 = 7
+XC_BLYP = 8
+XC_IDS = {"VWN": XC_VWN, "PBE": XC_PBE, "revPBE": XC_REVPBE, "PBEsol": XC_PBESOL, "BP86": XC_BP86,
+          "PW91": XC_PW91, "BPW91": XC_BPW91, "BLYP": XC_BLYP}
 
 PREC_FP64 = 0
 PREC_MIXED_INT8 = 1

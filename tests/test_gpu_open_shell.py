@@ -43,20 +43,40 @@ def _spin_points(n, seed):
     return rho, gam
 
 
-@pytest.mark.parametrize("xc", ["VWN", "PBE", "revPBE", "PBEsol", "BP86"])
+def _oracle_noise(xc, rho, gam, rf, rfr, rfg, trials=6):
+    """How far the oracle's own f, df/drho and df/dgamma move when the inputs
+    move by a few ulps: the conditioning of each point.  Where one spin is
+    empty, the PW91 correlation's d/drho of that spin runs through the
+    reference's 1e-20 under a cube root and is ill-conditioned."""
+    rng = np.random.default_rng(11)
+    nf, nr, ng = np.zeros_like(rf), np.zeros_like(rfr), np.zeros_like(rfg)
+    for _ in range(trials):
+        p = rho * (1 + 4e-16 * rng.standard_normal(rho.shape))
+        g = gam * (1 + 4e-16 * rng.standard_normal(gam.shape))
+        e, a, b = O.functionals(xc, 2, p, g)
+        nf = np.maximum(nf, np.abs(e - rf))
+        nr = np.maximum(nr, np.abs(a - rfr))
+        ng = np.maximum(ng, np.abs(b - rfg))
+    return nf, nr, ng
+
+
+@pytest.mark.parametrize("xc", ["VWN", "PBE", "revPBE", "PBEsol", "BP86", "PW91", "BPW91", "BLYP"])
 def test_point_functionals_open_shell(xc):
     rho, gam = _spin_points(600, 5)
     f, fr, fg = lib.xc_functionals(xc, rho, gam if xc != "VWN" else None)
     rf, rfr, rfg = O.functionals(xc, 2, rho, gam)
+    noise_f, noise_r, noise_g = _oracle_noise(xc, rho, gam, rf, rfr, rfg)
     # measured against the size of the spin-scaled Slater term (see the closed-shell test)
     rt = rho.sum(1)
     well = rt >= 1e-10
     sf = XA * (rho[:, 0] ** (4 / 3) + rho[:, 1] ** (4 / 3)) * 2 ** (1 / 3)
     sr = XA * rt ** (1 / 3)
-    tol_f = np.where(well, 1e-12 * (np.abs(rf) + sf), 1e-8 * np.abs(rf) + 1e-40)
+    tol_f = np.where(well, 1e-12 * (np.abs(rf) + sf), 1e-8 * (np.abs(rf) + sf) + 1e-40)
+    tol_f = np.maximum(tol_f, 8 * noise_f)
     assert np.all(np.abs(f - rf) <= tol_f), np.max(np.abs(f - rf) / tol_f)
     for s in range(2):
         tol_r = np.where(well, 1e-11 * (np.abs(rfr[:, s]) + sr), 1e-5 * np.abs(rfr[:, s]) + 1e-16)
+        tol_r = np.maximum(tol_r, 8 * noise_r[:, s])
         err = np.abs(fr[:, s] - rfr[:, s])
         assert np.all(err <= tol_r), (s, np.max(err / tol_r))
     if xc != "VWN":
@@ -66,7 +86,7 @@ def test_point_functionals_open_shell(xc):
         for k in range(3):
             err = np.abs(fg[:, k] - rfg[:, k])
             tol = 1e-10 * np.abs(rfg[:, k]) + np.where(gs > 0, 1e-10 * (np.abs(rf) + sf) / np.maximum(gs, 1e-300), 0)
-            tol = np.where(well, tol, np.inf)
+            tol = np.maximum(np.where(well, tol, np.inf), 8 * noise_g[:, k])
             assert np.all(err <= tol + 1e-300), (k, np.max(err / (tol + 1e-300)))
 
 
@@ -74,15 +94,22 @@ def test_point_functionals_equal_spins_match_closed_shell():
     rng = np.random.default_rng(3)
     rho = 10 ** rng.uniform(-8, 3, 300)
     gam = rho ** (8 / 3) * 10 ** rng.uniform(-4, 2, 300)
-    for xc in ("VWN", "PBE"):
-        f1, fr1, fg1 = lib.xc_functionals(xc, rho, gam if xc == "PBE" else None)
+    for xc in ("VWN", "PBE", "PW91", "BLYP"):
+        gga = xc != "VWN"
+        if xc == "PW91":
+            # the open shell floors |grad rho|^2 at 1e-20, the closed shell does
+            # not (gga_correlation, gga_response_module.f90:219-227)
+            rho, gam = rho[gam >= 1e-20], gam[gam >= 1e-20]
+        f1, fr1, fg1 = lib.xc_functionals(xc, rho, gam if gga else None)
         f2, fr2, fg2 = lib.xc_functionals(xc, np.stack([rho / 2, rho / 2], 1),
-                                          np.stack([gam / 4] * 3, 1) if xc == "PBE" else None)
+                                          np.stack([gam / 4] * 3, 1) if gga else None)
         np.testing.assert_allclose(f2, f1, rtol=1e-12)
         # the closed-shell outputs are 1-D
         np.testing.assert_allclose(fr2[:, 0], fr1, rtol=1e-10)
         np.testing.assert_allclose(fr2[:, 1], fr1, rtol=1e-10)
-        if xc == "PBE":
+        # closed-shell BLYP returns the LYP coefficient of gamma_aa as df/dgamma
+        # (as lyp.f90 does), not the sum over the three invariants
+        if xc in ("PBE", "PW91"):
             fsum = (fg2[:, 0] + fg2[:, 1] + fg2[:, 2]) / 4
             assert np.all(np.abs(fsum - fg1) <= fg_tolerance(rho, gam, f1, fg1))
 
@@ -104,7 +131,8 @@ BUILDS = pytest.mark.parametrize("precision,thr,tol", [("fp64", 0.0, 1e-10), ("m
 
 
 @BUILDS
-@pytest.mark.parametrize("xc,seed,lmax", [("VWN", 1, 2), ("PBE", 2, 2), ("PBE", 3, 3), ("VWN", 4, 3), ("BP86", 5, 2)])
+@pytest.mark.parametrize("xc,seed,lmax", [("VWN", 1, 2), ("PBE", 2, 2), ("PBE", 3, 3), ("VWN", 4, 3), ("BP86", 5, 2),
+                                          ("PW91", 6, 2), ("BLYP", 7, 3)])
 def test_open_shell_build(xc, seed, lmax, precision, thr, tol):
     c = cases.small_case(functional=xc, seed=seed, lmax=lmax, natoms=5, nocc=7, ispin=2)
     O.weight_case(c)

@@ -17,7 +17,8 @@ RHO = np.array([1e-12, 1e-6, 1e-3, 0.05, 0.7, 3.0, 120.0])
 GAM = np.array([1e-20, 1e-9, 1e-5, 0.02, 0.9, 10.0, 5e4])
 
 
-ALL_XC = ["VWN", "PBE", "revPBE", "PBEsol", "BP86"]
+ALL_XC = ["VWN", "PBE", "revPBE", "PBEsol", "BP86", "PW91", "BPW91", "BLYP"]
+GGA_XC = ALL_XC[1:]
 
 
 @pytest.mark.parametrize("xc", ALL_XC)
@@ -25,17 +26,23 @@ def test_functional_derivatives_fd(xc):
     rho = RHO.copy()
     gam = GAM.copy()
     f, fr, fg = O.functionals(xc, 1, rho, gam)
-    h = 1e-6 * rho
+    # a step of 1e-4: where exchange and correlation cancel to f ~ 1e-25
+    # (PW91 at rho = 1e-12), a smaller one resolves only rounding
+    h = 1e-4 * rho
     fp, _, _ = O.functionals(xc, 1, rho + h, gam)
     fm, _, _ = O.functionals(xc, 1, rho - h, gam)
     num = (fp - fm) / (2 * h)
     np.testing.assert_allclose(fr[:, 0], num, rtol=2e-6, atol=1e-12)
-    if xc != "VWN":
+    # closed-shell BLYP returns the LYP coefficient of gamma_aa as dF/dgamma,
+    # as the reference does: test_lyp_published_form covers it
+    if xc not in ("VWN", "BLYP"):
         hg = 1e-4 * gam
         gp, _, _ = O.functionals(xc, 1, rho, gam + hg)
         gm, _, _ = O.functionals(xc, 1, rho, gam - hg)
-        # only where the gamma dependence is above the rounding of f
-        ok = np.abs(fg[:, 0] * hg) > 1e-9 * np.abs(f)
+        # only where the gamma dependence is above the rounding of the parts
+        # of f (Slater exchange the largest: f itself can cancel to ~1e-25)
+        scale = np.maximum(np.abs(f), 0.75 * (3 / np.pi) ** (1 / 3) * rho ** (4 / 3))
+        ok = np.abs(fg[:, 0] * hg) > 1e-9 * scale
         assert ok.sum() >= 4
         np.testing.assert_allclose(fg[ok, 0], ((gp - gm) / (2 * hg))[ok], rtol=1e-6)
 
@@ -51,9 +58,138 @@ def test_functional_spin_consistency(xc):
     f2, fr2, fg2 = O.functionals(xc, 2, r2, g2)
     np.testing.assert_allclose(f2, f1, rtol=1e-12, atol=1e-300)
     np.testing.assert_allclose(fr2[:, 0], fr1[:, 0], rtol=1e-10, atol=1e-14)
-    if xc != "VWN":
+    if xc not in ("VWN", "BLYP"):
         # d/dg_aa + d/dg_bb + d/dg_ab of g = g_aa + g_bb + 2 g_ab
         np.testing.assert_allclose((fg2[:, 0] + fg2[:, 1] + fg2[:, 2]) / 4, fg1[:, 0], rtol=1e-9, atol=1e-14)
+
+
+@pytest.mark.parametrize("xc", GGA_XC)
+def test_open_shell_derivatives_fd(xc):
+    """All five partials of the open-shell functional against central differences."""
+    rng = np.random.default_rng(17)
+    ra = 10 ** rng.uniform(-4, 1.5, 12)
+    rb = ra * rng.uniform(0.05, 1.0, 12)
+    gaa = ra ** (8 / 3) * rng.uniform(0.01, 3.0, 12)
+    gbb = rb ** (8 / 3) * rng.uniform(0.01, 3.0, 12)
+    gab = np.sqrt(gaa * gbb) * rng.uniform(-0.9, 0.9, 12)
+    x = np.stack([ra, rb, gaa, gbb, gab], 1)
+    f, fr, fg = O.functionals(xc, 2, x[:, :2], x[:, 2:])
+    ana = np.concatenate([fr, fg], 1)
+    for k in range(5):
+        h = 1e-4 * np.abs(x[:, k]) if k < 4 else 1e-4 * np.sqrt(gaa * gbb)
+        xp, xm = x.copy(), x.copy()
+        xp[:, k] += h
+        xm[:, k] -= h
+        num = (O.functionals(xc, 2, xp[:, :2], xp[:, 2:])[0] - O.functionals(xc, 2, xm[:, :2], xm[:, 2:])[0]) / (2 * h)
+        ok = np.abs(ana[:, k] * h) > 1e-10 * np.abs(f)
+        assert ok.sum() >= 6, (k, ok)
+        np.testing.assert_allclose(ana[ok, k], num[ok], rtol=2e-5, err_msg=f"{xc} partial {k}")
+
+
+def _b88_published(ra, rb, gaa, gbb):
+    """Slater + Becke 88 exchange in Becke's published form (PRA 38, 3098):
+    sum_s rho_s^(4/3) [-(3/2)(3/(4 pi))^(1/3) - beta x_s^2 / (1 + 6 beta x_s asinh x_s)],
+    x_s = |grad rho_s| / rho_s^(4/3), beta = 0.0042."""
+    beta = 0.0042
+    out = 0.0
+    for r, g in ((ra, gaa), (rb, gbb)):
+        r43 = r ** (4 / 3)
+        x = np.sqrt(g) / r43
+        out = out + r43 * (-1.5 * (3 / (4 * np.pi)) ** (1 / 3) - beta * x * x / (1 + 6 * beta * x * np.arcsinh(x)))
+    return out
+
+
+def _lyp_published(ra, rb, gaa, gbb, gab):
+    """LYP correlation in the form of Miehlich, Savin, Stoll and Preuss
+    (CPL 157, 200), a = 0.04918, b = 0.132, c = 0.2533, d = 0.349."""
+    a, b, c, d = 0.04918, 0.132, 0.2533, 0.349
+    cf = 0.3 * (3 * np.pi ** 2) ** (2 / 3)
+    r = ra + rb
+    rm = r ** (-1 / 3)
+    w = np.exp(-c * rm) / (1 + d * rm) * r ** (-11 / 3)
+    dl = c * rm + d * rm / (1 + d * rm)
+    g = gaa + gbb + 2 * gab
+    br = (ra * rb * (2 ** (11 / 3) * cf * (ra ** (8 / 3) + rb ** (8 / 3)) + (47 / 18 - 7 * dl / 18) * g
+                     - (5 / 2 - dl / 18) * (gaa + gbb) - (dl - 11) / 9 * (ra / r * gaa + rb / r * gbb))
+          - 2 / 3 * r * r * g + (2 / 3 * r * r - ra * ra) * gbb + (2 / 3 * r * r - rb * rb) * gaa)
+    return -4 * a / (1 + d * rm) * ra * rb / r - a * b * w * br
+
+
+def test_lyp_published_form():
+    """BLYP = Slater + B88 + LYP, each in its published closed form; the
+    closed-shell gamma derivative is d/dgamma of the exchange plus the LYP
+    coefficient of gamma_aa alone (lyp.f90 returns fst(3) of g_aa = gamma/4
+    as dF/dgamma), which differs from dE/dgamma."""
+    rng = np.random.default_rng(23)
+    ra = 10 ** rng.uniform(-3, 1.5, 10)
+    rb = ra * rng.uniform(0.1, 1.0, 10)
+    gaa = ra ** (8 / 3) * rng.uniform(0.01, 3.0, 10)
+    gbb = rb ** (8 / 3) * rng.uniform(0.01, 3.0, 10)
+    gab = np.sqrt(gaa * gbb) * rng.uniform(-0.9, 0.9, 10)
+    f2 = O.functionals("BLYP", 2, np.stack([ra, rb], 1), np.stack([gaa, gbb, gab], 1))[0]
+    want = _b88_published(ra, rb, gaa, gbb) + _lyp_published(ra, rb, gaa, gbb, gab)
+    np.testing.assert_allclose(f2, want, rtol=1e-11)
+    rho, gam = ra, gaa
+    f1, fr1, fg1 = O.functionals("BLYP", 1, rho, gam)
+    q = gam / 4
+    np.testing.assert_allclose(f1, _b88_published(rho / 2, rho / 2, q, q) + _lyp_published(rho / 2, rho / 2, q, q, q),
+                               rtol=1e-11)
+    h = 1e-4 * gam
+    dx = (_b88_published(rho / 2, rho / 2, (gam + h) / 4, (gam + h) / 4)
+          - _b88_published(rho / 2, rho / 2, (gam - h) / 4, (gam - h) / 4)) / (2 * h)
+    caa = _lyp_published(rho / 2, rho / 2, 1.0 + q, q, q) - _lyp_published(rho / 2, rho / 2, q, q, q)
+    np.testing.assert_allclose(fg1[:, 0], dx + caa, rtol=1e-6)
+
+
+def _pw91_h_published(n, g, ec):
+    """PW91 correlation H0 + H1 for an unpolarised density (Perdew et al.,
+    PRB 46, 6671, eqs. 13-16), rs and ks/kF with the reference's 1.91916."""
+    alpha, cc0, cx = 0.09, 0.004235, -0.001667
+    nu = 16 / np.pi * (3 * np.pi ** 2) ** (1 / 3)
+    beta = nu * cc0
+    kf = (3 * np.pi ** 2 * n) ** (1 / 3)
+    rs = 1.91916 / kf
+    ks2 = 4 * kf / np.pi
+    t2 = g / (4 * ks2 * n * n)
+    A = 2 * alpha / beta / (np.exp(-2 * alpha * ec / beta ** 2) - 1)
+    h0 = beta ** 2 / (2 * alpha) * np.log(1 + 2 * alpha / beta * (t2 + A * t2 * t2) / (1 + A * t2 + A * A * t2 * t2))
+    cc = 1e-3 * (2.568 + 23.266 * rs + 0.007389 * rs ** 2) / (1 + 8.723 * rs + 0.472 * rs ** 2 + 0.07389 * rs ** 3) - cx
+    h1 = nu * (cc - cc0 - 3 * cx / 7) * t2 * np.exp(-100 * 4 / (1.91916 * np.pi) * rs * t2)
+    return n * (h0 + h1)
+
+
+def test_pw91_published_form():
+    """PW91 and BPW91 against the published PW91 exchange enhancement and
+    correlation H0 + H1 (the LDA parts are taken from the functional at zero
+    gradient); the small-gradient limit of dF/dgamma is the gradient expansion
+    nu (Cc(rs) - 3 Cx / 7) ct / n^(4/3) plus the exchange's (D - E) term."""
+    rng = np.random.default_rng(29)
+    rho = 10 ** rng.uniform(-3, 1.5, 10)
+    gam = rho ** (8 / 3) * rng.uniform(0.01, 3.0, 10)
+    ex = -(3 / 4) * (3 / np.pi) ** (1 / 3) * rho ** (4 / 3)
+    s = np.sqrt(gam) / (2 * (3 * np.pi ** 2) ** (1 / 3) * rho ** (4 / 3))
+    ash = 0.19645 * s * np.arcsinh(7.7956 * s)
+    fx = (1 + ash + (0.2743 - 0.1508 * np.exp(-100 * s * s)) * s * s) / (1 + ash + 0.004 * s ** 4)
+    f0 = O.functionals("PW91", 1, rho, np.zeros_like(rho))[0]
+    ec = (f0 - ex) / rho
+    f = O.functionals("PW91", 1, rho, gam)[0]
+    np.testing.assert_allclose(f, ex * fx + rho * ec + _pw91_h_published(rho, gam, ec), rtol=1e-10)
+    fb = O.functionals("BPW91", 1, rho, gam)[0]
+    q = gam / 4
+    dx = _b88_published(rho / 2, rho / 2, q, q) - ex * fx
+    assert np.all(np.abs((fb - f) - dx) <= 1e-9 * np.abs(dx) + 1e-13 * np.abs(f)), (fb - f, dx)
+    # zero gradient: PW91 is Slater + PW92, the PBE keyword's LDA part
+    np.testing.assert_allclose(f0, O.functionals("PBE", 1, rho, np.zeros_like(rho))[0], rtol=1e-14)
+    # gradient expansion at small gamma
+    tiny = 1e-12 * rho ** (8 / 3)
+    fg = O.functionals("PW91", 1, rho, tiny)[2][:, 0]
+    nu = 16 / np.pi * (3 * np.pi ** 2) ** (1 / 3)
+    rs = 1.91916 / (3 * np.pi ** 2 * rho) ** (1 / 3)
+    cc = 1e-3 * (2.568 + 23.266 * rs + 0.007389 * rs ** 2) / (1 + 8.723 * rs + 0.472 * rs ** 2 + 0.07389 * rs ** 3)
+    cc += 0.001667
+    ct = np.pi / (16 * (3 * np.pi ** 2) ** (1 / 3))
+    want = nu * (cc + 3 * 0.001667 / 7) * ct / rho ** (4 / 3) + ex * (0.2743 - 0.1508) / (4 * (3 * np.pi ** 2) ** (2 / 3) * rho ** (8 / 3))
+    np.testing.assert_allclose(fg, want, rtol=1e-6)
 
 
 def test_pbe_variants_closed_form():
@@ -108,7 +244,7 @@ def test_basis_normalised_and_gradients(small_cases):
         np.testing.assert_allclose(gr[:, d, :], (pp - pm) / (2 * h), rtol=1e-5, atol=1e-8)
 
 
-@pytest.mark.parametrize("xc", ALL_XC)
+@pytest.mark.parametrize("xc", [x for x in ALL_XC if x != "BLYP"])
 def test_dE_dC_equals_2_occ_V_C(small_cases, xc):
     if xc in small_cases:
         c = small_cases[xc]
@@ -152,6 +288,29 @@ def test_translation_invariance():
     h2, e2, n2 = O.xc_build(c)
     assert abs(e1 - e2) < 1e-10 * abs(e1)
     np.testing.assert_allclose(h1, h2, atol=1e-10)
+
+
+@pytest.mark.parametrize("xc", ["BLYP", "PW91"])
+def test_open_shell_dE_dC(xc):
+    """Open shell: dE_xc/dC_s = 2 occ_s V_s C_s for each spin."""
+    c = cases.small_case(functional=xc, seed=37, ispin=2, nocc=5)
+    O.weight_case(c)
+    ham, e0, _ = O.xc_build(c)
+    rng = np.random.default_rng(6)
+    d = rng.normal(size=c.C.shape)
+    ana = 0.0
+    for s in range(2):
+        V = O.unpack(ham, c.nbas, ispin=2, s=s)
+        ana += np.sum(2 * c.occ[:, s][None, :] * (V @ c.C[:, :, s]) * d[:, :, s])
+    h = 1e-5
+    C0 = c.C.copy()
+    c.C = C0 + h * d
+    _, ep, _ = O.xc_build(c)
+    c.C = C0 - h * d
+    _, em, _ = O.xc_build(c)
+    c.C = C0
+    num = (ep - em) / (2 * h)
+    assert abs(num - ana) < 1e-6 * max(1.0, abs(ana)), (num, ana)
 
 
 def test_open_shell_matches_closed_shell():
