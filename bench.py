@@ -154,9 +154,10 @@ def shard(case, rank, world):
 
 
 def algorithmic_flops(case):
+    from pgxc import abi
     n, N = case.nbas, case.npts
     x = 2.0 * N * n * n
-    v = 2.0 * N * n * n if case.functional != "VWN" else 1.0 * N * n * n
+    v = 2.0 * N * n * n if abi.is_gga(case.functional) else 1.0 * N * n * n
     return x, v
 
 
@@ -522,7 +523,8 @@ def main():
 
     # roofline of the density kernel (the largest kernel of the build), per
     # launch from the library's CUDA events around it
-    gga = case.functional != "VWN"
+    from pgxc import abi
+    gga = abi.is_gga(case.functional)
     arrays = 4 if gga else 1
     if screen is not None:
         nlisted, sum_n2, ntl = screen["nlisted"], screen["sum_n2"], screen["ntiles"]

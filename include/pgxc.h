@@ -64,8 +64,24 @@ extern "C" {
 /* BLYP: Slater + Becke 88 exchange + LYP correlation (LYP is a whole
  * correlation, no LDA part; keyword "BLYP", modules/xc_cntrl.f90:522-532) */
 #define PGXC_XC_BLYP 8
+/* XALPHA: Slater exchange alone, an LDA (keyword "XALPHA", modules/xc_cntrl.f90:454-458) */
+#define PGXC_XC_XALPHA 9
+/* B88: Slater + Becke 88 exchange, no correlation (keyword "B88", modules/xc_cntrl.f90:534-543) */
+#define PGXC_XC_B88 10
+/* PBEN: Slater + PW92 + PBEN exchange kappa (1 - exp(-mu s^2 / kappa)) + PBE
+ * correlation (keyword "PBEN", modules/xc_cntrl.f90:714-732) */
+#define PGXC_XC_PBEN 11
+/* VMT, VT{8,4}, VMTsol, VT{8,4}sol: Slater + PW92 + the VMT / VT84 exchange
+ * enhancements (PBE or PBEsol mu) + PBE correlation (keywords "VMT", "VT84",
+ * "VMTsol", "VT84sol", modules/xc_cntrl.f90:900-950) */
+#define PGXC_XC_VMT 12
+#define PGXC_XC_VT84 13
+#define PGXC_XC_VMTSOL 14
+#define PGXC_XC_VT84SOL 15
 /* the largest functional id */
-#define PGXC_XC_LAST PGXC_XC_BLYP
+#define PGXC_XC_LAST PGXC_XC_VT84SOL
+/* nonzero for the GGA keywords (all but the two LDAs) */
+#define PGXC_XC_IS_GGA(id) ((id) != PGXC_XC_VWN && (id) != PGXC_XC_XALPHA)
 
 /* ---- precision modes ------------------------------------------------- */
 #define PGXC_PREC_FP64        0  /* FP64 everywhere (FP64 tensor pipe): the drop-in */

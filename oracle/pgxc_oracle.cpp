@@ -130,22 +130,34 @@ D x_lda(D rho) {
 // (xc_cntrl.f90:508-590): BP = Slater + VWN5 + B88 + P86, BPW91 = Slater +
 // PW92 + B88 + PW91c, PW91 = Slater + PW92 + PW91x + PW91c, BLYP = Slater +
 // B88 + LYP; the PBE-form keywords differ in kappa, mu and beta.
-enum { GX_PBE, GX_B88, GX_PW91 };
-enum { GC_PBE, GC_P86, GC_PW91, GC_LYP };
+enum { GX_PBE, GX_B88, GX_PW91, GX_PBEN, GX_VMT, GX_VT84 };
+enum { GC_PBE, GC_P86, GC_PW91, GC_LYP, GC_NONE };
+enum { LC_VWN, LC_PW92, LC_NONE };
 struct GgaPar {
   double kappa, mu, beta_c;  // exchange kappa, mu; correlation beta (pbe_ggcc :249-270)
-  int gx, gc;                // kind of exchange enhancement and of gradient correlation
+  int gx, gc, lc;            // exchange enhancement, gradient correlation, LDA correlation
+  double alpha;              // VMT / VT84 alpha (exchange.f90:723-797)
 };
 GgaPar gga_par(int xc) {
   const double pi = PI_EXCH;
-  const double mu_pbe = 0.066725 * (pi * pi / 3.0);
-  if (xc == PGXC_XC_REVPBE) return {1.245, mu_pbe, 0.066725, GX_PBE, GC_PBE};
-  if (xc == PGXC_XC_PBESOL) return {0.804, 10.0 / 81.0, 0.046, GX_PBE, GC_PBE};
-  if (xc == PGXC_XC_BP86) return {0.0, 0.0, 0.0, GX_B88, GC_P86};
-  if (xc == PGXC_XC_PW91) return {0.0, 0.0, 0.0, GX_PW91, GC_PW91};
-  if (xc == PGXC_XC_BPW91) return {0.0, 0.0, 0.0, GX_B88, GC_PW91};
-  if (xc == PGXC_XC_BLYP) return {0.0, 0.0, 0.0, GX_B88, GC_LYP};
-  return {0.804, mu_pbe, 0.066725, GX_PBE, GC_PBE};
+  const double mu_pbe = 0.066725 * (pi * pi / 3.0), mu_sol = 10.0 / 81.0;
+  switch (xc) {
+    case PGXC_XC_VWN: return {0, 0, 0, GX_PBE, GC_NONE, LC_VWN, 0};
+    case PGXC_XC_XALPHA: return {0, 0, 0, GX_PBE, GC_NONE, LC_NONE, 0};
+    case PGXC_XC_REVPBE: return {1.245, mu_pbe, 0.066725, GX_PBE, GC_PBE, LC_PW92, 0};
+    case PGXC_XC_PBESOL: return {0.804, mu_sol, 0.046, GX_PBE, GC_PBE, LC_PW92, 0};
+    case PGXC_XC_BP86: return {0, 0, 0, GX_B88, GC_P86, LC_VWN, 0};
+    case PGXC_XC_PW91: return {0, 0, 0, GX_PW91, GC_PW91, LC_PW92, 0};
+    case PGXC_XC_BPW91: return {0, 0, 0, GX_B88, GC_PW91, LC_PW92, 0};
+    case PGXC_XC_BLYP: return {0, 0, 0, GX_B88, GC_LYP, LC_NONE, 0};
+    case PGXC_XC_B88: return {0, 0, 0, GX_B88, GC_NONE, LC_NONE, 0};
+    case PGXC_XC_PBEN: return {0.804, mu_pbe, 0.066725, GX_PBEN, GC_PBE, LC_PW92, 0};
+    case PGXC_XC_VMT: return {0, mu_pbe, 0.066725, GX_VMT, GC_PBE, LC_PW92, 0.002762};
+    case PGXC_XC_VT84: return {0, mu_pbe, 0.066725, GX_VT84, GC_PBE, LC_PW92, 0.000069};
+    case PGXC_XC_VMTSOL: return {0, mu_sol, 0.066725, GX_VMT, GC_PBE, LC_PW92, 0.0015532};
+    case PGXC_XC_VT84SOL: return {0, mu_sol, 0.066725, GX_VT84, GC_PBE, LC_PW92, 0.000023};
+    default: return {0.804, mu_pbe, 0.066725, GX_PBE, GC_PBE, LC_PW92, 0};
+  }
 }
 
 // Becke 88 enhancement: g_becke88 (exchange.f90:672-705, the BECKE88_0042
@@ -182,6 +194,25 @@ D g_pw91(D s2) {
   return s2 * (T1 + s2 * T2);
 }
 
+// PBEN: g_pben (exchange.f90:869-902), G = kappa (1 - exp(-x)), x = mu s^2 /
+// kappa, or kappa x (1 - x/2 + x^2/6 - x^3/24 + x^4/120) when x <= 1e-4.
+D g_pben(double kappa, double mu, D s2) {
+  D x = mu * s2 / kappa;
+  if (x.v > 1.0e-4) return kappa * (1.0 - dexp(-x));
+  return kappa * x * (1.0 + x * (-1.0 / 2.0 + x * (1.0 / 6.0 + x * (-1.0 / 24.0 + x * (1.0 / 120.0)))));
+}
+
+// VMT: g_vmt_form (exchange.f90:799-817), mu s^2 exp(-alpha s^2) / (mu s^2 + 1);
+// VT84 adds g_vt84_2nd_term (:819-856), (1 - exp(-alpha s^4)) (1/s^2 - 1), or
+// its series alpha s^2 (1 - s^2 - alpha s^4/2 + alpha s^6/2 + alpha^2 s^8/6)
+// when s^2 <= 1e-4.
+D g_vmt(double mu, double alpha, D s2, bool vt84) {
+  D G = mu * s2 * dexp(-alpha * s2) / (mu * s2 + 1.0);
+  if (!vt84) return G;
+  if (s2.v > 1.0e-4) return G + (1.0 - dexp(-alpha * s2 * s2)) * (1.0 / s2 - 1.0);
+  return G + alpha * s2 * (1.0 + s2 * (-1.0 + s2 * (-alpha / 2.0 + s2 * (alpha / 2.0 + s2 * (alpha * alpha / 6.0)))));
+}
+
 void x_gga_pbe(const GgaPar& P, double n, double gam, double& F, double& dFdn, double& dFdg) {
   const double pi = PI_EXCH;
   const double xalpha = -(3.0 / 4.0) * std::pow(3.0 / pi, 1.0 / 3.0);
@@ -196,7 +227,12 @@ void x_gga_pbe(const GgaPar& P, double n, double gam, double& F, double& dFdn, d
   }
   const double kappa = P.kappa, mu = P.mu;
   D s2 = var(0, s2_0);
-  D G = P.gx == GX_B88 ? g_becke88(s2) : P.gx == GX_PW91 ? g_pw91(s2) : kappa * mu * s2 / (kappa + mu * s2);
+  D G = P.gx == GX_B88    ? g_becke88(s2)
+        : P.gx == GX_PW91  ? g_pw91(s2)
+        : P.gx == GX_PBEN  ? g_pben(kappa, mu, s2)
+        : P.gx == GX_VMT   ? g_vmt(mu, P.alpha, s2, false)
+        : P.gx == GX_VT84  ? g_vmt(mu, P.alpha, s2, true)
+                           : kappa * mu * s2 / (kappa + mu * s2);
   F += ex.v * G.v;
   dFdn += ex.d[0] * G.v + ex.v * G.d[0] * s2_r;
   dFdg += ex.v * G.d[0] * s2_g;
@@ -477,19 +513,20 @@ void functional_point(int xc, int ispin, const double* rho, const double* gam,
     }
   }
   // LDA correlation: VWN5 (vwn_ldac, vwnc.f90:225-297) for "VWN" and "BP",
-  // none for "BLYP" (LYP is a whole correlation), else PW92 (pw_ldac,
-  // pw_ldac_module.f90:197-312).  ec is kept for the PW91 correlation.
+  // none for "XALPHA", "B88" and "BLYP" (LYP is a whole correlation), else
+  // PW92 (pw_ldac, pw_ldac_module.f90:197-312).  ec is kept for the PW91
+  // correlation.
   D ec = cst(0.0);
-  if (xc == PGXC_XC_VWN || P.gc == GC_P86) {
+  if (P.lc == LC_VWN) {
     if (ispin == 1) { D nn = var(0, rho[0]); ec = vwn::c_lda(0.5 * nn, 0.5 * nn); }
     else ec = vwn::c_lda(var(0, rho[0]), var(1, rho[1]));
-  } else if (P.gc != GC_LYP) {
+  } else if (P.lc == LC_PW92) {
     if (ispin == 1) { D nn = var(0, rho[0]); ec = pw92::c_lda(0.5 * nn, 0.5 * nn); }
     else ec = pw92::c_lda(var(0, rho[0]), var(1, rho[1]));
   }
   f += ec.v; fr[0] += ec.d[0];
   if (ispin == 2) fr[1] += ec.d[1];
-  if (xc == PGXC_XC_VWN) return;
+  if (!PGXC_XC_IS_GGA(xc)) return;
   // GGA exchange enhancement (exchange_gga, exchange.f90:206-292)
   if (ispin == 1) {
     double F = 0, Fn = 0, Fg = 0;
@@ -502,6 +539,7 @@ void functional_point(int xc, int ispin, const double* rho, const double* gam,
       f += 0.5 * F; fr[s] += Fn; fg[s] += 2.0 * Fg;
     }
   }
+  if (P.gc == GC_NONE) return;  // "B88"
   if (P.gc == GC_P86) {  // "BP": Perdew 86 correlation (xc_cntrl.f90:508-520)
     perdew86(ispin, rho, gam, f, fr, fg);
     return;
@@ -858,13 +896,13 @@ int oracle_functionals(int32_t xc, int32_t ispin, int64_t n, const double* rho, 
   for (int64_t i = 0; i < n; ++i) {
     double r[2] = {rho[i], ispin == 2 ? rho[i + n] : 0.0};
     double g[3] = {0, 0, 0};
-    if (xc != PGXC_XC_VWN)
+    if (PGXC_XC_IS_GGA(xc))
       for (int c = 0; c < ng; ++c) g[c] = gam[i + n * c];
     double F, Fr[2], Fg[3];
     functional_point(xc, ispin, r, g, F, Fr, Fg);
     f[i] = F;
     for (int s = 0; s < ispin; ++s) fr[i + n * s] = Fr[s];
-    if (fg && xc != PGXC_XC_VWN)
+    if (fg && PGXC_XC_IS_GGA(xc))
       for (int c = 0; c < ng; ++c) fg[i + n * c] = Fg[c];
   }
   return PGXC_OK;
@@ -946,7 +984,7 @@ int oracle_xc_build(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_
   const double* gy = gx + npts;
   const double* gz = gy + npts;
   const double* gw = gz + npts;
-  const bool gga = (xc != PGXC_XC_VWN);
+  const bool gga = PGXC_XC_IS_GGA(xc);
   const int64_t nbatch = (pt_hi - pt_lo + vla - 1) / vla;
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);

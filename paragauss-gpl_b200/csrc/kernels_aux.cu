@@ -94,7 +94,7 @@ __global__ void k_xc_points(XcConst K, int functional, int64_t n, const double* 
                             double* __restrict__ f, double* __restrict__ fr, double* __restrict__ fg) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
-  if (functional != PGXC_XC_VWN) {
+  if (PGXC_XC_IS_GGA(functional)) {
     double a, b, c;
     xc_gga(K, rho[p], gam[p], a, b, c);
     f[p] = a; fr[p] = b; fg[p] = c;
@@ -130,7 +130,7 @@ void launch_xc_points(int functional, int ispin, int64_t n, const double* rho, c
   const unsigned nb = (unsigned)((n + 255) / 256);
   if (ispin == 1)
     k_xc_points<<<nb, 256, 0, st>>>(make_xc_const(functional), functional, n, rho, gam, f, fr, fg);
-  else if (functional != PGXC_XC_VWN)
+  else if (PGXC_XC_IS_GGA(functional))
     k_xc_points2<true><<<nb, 256, 0, st>>>(make_xc_const(functional), n, rho, gam, f, fr, fg);
   else
     k_xc_points2<false><<<nb, 256, 0, st>>>(make_xc_const(functional), n, rho, gam, f, fr, fg);

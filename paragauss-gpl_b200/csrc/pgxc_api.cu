@@ -368,7 +368,7 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   }
   a.ldc = round_up(c->nbas, kTile);
-  const bool gga = o.functional != PGXC_XC_VWN;
+  const bool gga = PGXC_XC_IS_GGA(o.functional);
   if (o.screen_threshold >= 0.0) {
     // screened build: per-tile significant-function lists; only P, the
     // accumulators and the packed matrix are shared with the dense layout
@@ -518,7 +518,7 @@ static int upload_orbitals(pgxc_ctx* c, const double* C, const double* occ, int3
 static int run_build(pgxc_ctx* c, int nocc, pgxc_timings* tm, bool p_given = false) {
   BuildArgs& a = c->a;
   cudaStream_t s = c->stream;
-  const bool gga = c->opt.functional != PGXC_XC_VWN;
+  const bool gga = PGXC_XC_IS_GGA(c->opt.functional);
   const int64_t kpad = round_up(std::max(nocc, 1), 16);
   if (c->screen) {
     CUDA_TRY(c, cudaMemsetAsync(a.acc, 0, 4 * sizeof(double), s));
@@ -960,7 +960,7 @@ int pgxc_xc_functionals(int32_t functional, int32_t ispin, int64_t n, const doub
   if (functional < PGXC_XC_VWN || functional > PGXC_XC_LAST) return set_err(nullptr, PGXC_EINVAL, "functional");
   if (ispin != 1 && ispin != 2) return set_err(nullptr, PGXC_EINVAL, "ispin must be 1 or 2");
   if (n < 0 || !rho || !f || !fr) return set_err(nullptr, PGXC_EINVAL, "bad arguments");
-  const bool gga = functional != PGXC_XC_VWN;
+  const bool gga = PGXC_XC_IS_GGA(functional);
   if (gga && (!gam || !fg)) return set_err(nullptr, PGXC_EINVAL, "PBE needs gam and fg");
   if (n == 0) return PGXC_OK;
   int st = check_device(nullptr, -1);

@@ -11,13 +11,16 @@
 //   PBE correlation H     modules/pbe_ggcxc_module.f90:96-348
 //   Becke 88 G(s^2)       modules/exchange.f90:672-705, :964-991
 //   PW91 exchange G(s^2)  modules/exchange.f90:919-962
+//   PBEN, VMT, VT84 G(s^2) modules/exchange.f90:723-856, :869-902
 //   Perdew 86 correlation modules/becke_perdew_module.f90:125-260
 //   PW91 correlation      modules/gga_response_module.f90:278-918 (H0 + H1)
 //   LYP correlation       modules/lyp.f90 (lyp_C, lyp_corr)
 // composed as the XC keywords do (modules/xc_cntrl.f90:460-798):
 //   "VWN" = Slater + VWN5, "PBE" = Slater + PW92 + PBE-X(G) + PBE-C(H),
 //   "BP" = Slater + VWN5 + B88 + P86, "PW91" = Slater + PW92 + PW91-X + PW91-C,
-//   "BPW91" = Slater + PW92 + B88 + PW91-C, "BLYP" = Slater + B88 + LYP.
+//   "BPW91" = Slater + PW92 + B88 + PW91-C, "BLYP" = Slater + B88 + LYP,
+//   "XALPHA" = Slater, "B88" = Slater + B88, "PBEN" / "VMT" / "VT84" /
+//   "VMTsol" / "VT84sol" = Slater + PW92 + their G + PBE-C.
 // Literal constants, density guards and epsilons are the reference's.
 #pragma once
 
@@ -45,8 +48,10 @@ struct XcConst {
   double b88_A, b88_B, b88_D;
   // LYP: 2^(11/3)
   double lyp_2113;
-  int xg;               // exchange enhancement G(s^2): XG_PBE, XG_B88 or XG_PW91
-  int cg;               // correlation: CG_PBE, CG_P86, CG_PW91 or CG_LYP
+  double vmt_alpha;     // alpha of the VMT / VT84 enhancements
+  int xg;               // exchange enhancement G(s^2): XG_*
+  int cg;               // gradient correlation: CG_*
+  int lc;               // LDA correlation: LC_VWN, LC_PW92 or LC_NONE
   // PBE correlation
   double pbe_fi;        // (0.5^(2/3)+0.5^(2/3)) * (1/2^(1/3))
   double pbe_ct;        // pi/(16 (3 pi^2)^(1/3))
@@ -59,8 +64,9 @@ struct XcConst {
 // GGA pieces of a keyword.  Exchange enhancement: the PBE form (kappa, mu),
 // Becke 88, or PW91.  Correlation: PW92 + PBE H, VWN5 + Perdew 86, PW92 +
 // PW91 H0 + H1, or LYP (a whole correlation: no LDA part).
-constexpr int XG_PBE = 0, XG_B88 = 1, XG_PW91 = 2;
-constexpr int CG_PBE = 0, CG_P86 = 1, CG_PW91 = 2, CG_LYP = 3;
+constexpr int XG_PBE = 0, XG_B88 = 1, XG_PW91 = 2, XG_PBEN = 3, XG_VMT = 4, XG_VT84 = 5;
+constexpr int CG_PBE = 0, CG_P86 = 1, CG_PW91 = 2, CG_LYP = 3, CG_NONE = 4;
+constexpr int LC_VWN = 0, LC_PW92 = 1, LC_NONE = 2;
 
 // Constants of the functional (PGXC_XC_*): the PBE-form keywords differ only
 // in their parameters (exchange.f90 g_pbe / g_revpbe / g_pbesol :617-670,
@@ -76,18 +82,30 @@ __host__ inline XcConst make_xc_const(int functional = PGXC_XC_PBE) {
   c.pw_crs = std::pow(3.0 / (4.0 * pi_p), 1.0 / 3.0);
   c.s2_fact = 1.0 / (4.0 * std::pow(3.0 * pi_x * pi_x, 2.0 / 3.0));
   c.pbe_kappa = functional == PGXC_XC_REVPBE ? 1.245 : 0.804;
-  c.pbe_mu = functional == PGXC_XC_PBESOL ? 10.0 / 81.0 : 0.066725 * (pi_x * pi_x / 3.0);
+  const bool sol = functional == PGXC_XC_PBESOL || functional == PGXC_XC_VMTSOL || functional == PGXC_XC_VT84SOL;
+  c.pbe_mu = sol ? 10.0 / 81.0 : 0.066725 * (pi_x * pi_x / 3.0);
   c.pbe_beta = functional == PGXC_XC_PBESOL ? 0.046 : 0.066725;
   // g_becke88, exchange.f90:672-705 (BECKE88_0042: beta = 0.0042)
   c.b88_A = 6.0 * 0.0042 * std::pow(2.0, 1.0 / 3.0) * std::pow(3.0 * pi_x * pi_x, 1.0 / 3.0) * 2.0;
   c.b88_D = c.b88_A * (4.0 * pi_x) / 9.0;
   c.b88_B = 2.0 * std::pow(6.0 * pi_x * pi_x, 1.0 / 3.0);
   c.lyp_2113 = std::pow(2.0, 11.0 / 3.0);
-  const bool b88 = functional == PGXC_XC_BP86 || functional == PGXC_XC_BPW91 || functional == PGXC_XC_BLYP;
-  c.xg = b88 ? XG_B88 : functional == PGXC_XC_PW91 ? XG_PW91 : XG_PBE;
-  c.cg = functional == PGXC_XC_BP86 ? CG_P86
-         : (functional == PGXC_XC_PW91 || functional == PGXC_XC_BPW91) ? CG_PW91
-         : functional == PGXC_XC_BLYP ? CG_LYP : CG_PBE;
+  // g_vmt :723-737, g_vt84 :739-760, g_vmtsol :762-775, g_vt84sol :777-797
+  c.vmt_alpha = functional == PGXC_XC_VMT ? 0.002762 : functional == PGXC_XC_VT84 ? 0.000069
+                : functional == PGXC_XC_VMTSOL ? 0.0015532 : functional == PGXC_XC_VT84SOL ? 0.000023 : 0.0;
+  const int f = functional;
+  const bool b88 = f == PGXC_XC_BP86 || f == PGXC_XC_BPW91 || f == PGXC_XC_BLYP || f == PGXC_XC_B88;
+  c.xg = b88 ? XG_B88
+         : f == PGXC_XC_PW91 ? XG_PW91
+         : f == PGXC_XC_PBEN ? XG_PBEN
+         : (f == PGXC_XC_VMT || f == PGXC_XC_VMTSOL) ? XG_VMT
+         : (f == PGXC_XC_VT84 || f == PGXC_XC_VT84SOL) ? XG_VT84 : XG_PBE;
+  c.cg = f == PGXC_XC_BP86 ? CG_P86
+         : (f == PGXC_XC_PW91 || f == PGXC_XC_BPW91) ? CG_PW91
+         : f == PGXC_XC_BLYP ? CG_LYP
+         : (f == PGXC_XC_B88 || !PGXC_XC_IS_GGA(f)) ? CG_NONE : CG_PBE;
+  c.lc = (f == PGXC_XC_VWN || f == PGXC_XC_BP86) ? LC_VWN
+         : (f == PGXC_XC_XALPHA || f == PGXC_XC_B88 || f == PGXC_XC_BLYP) ? LC_NONE : LC_PW92;
   c.pbe_fi = (std::pow(0.5, 2.0 / 3.0) + std::pow(0.5, 2.0 / 3.0)) * (1.0 / std::pow(2.0, 1.0 / 3.0));
   c.pbe_ct = pi_p / (4.0 * 4.0 * std::pow(3.0 * pi_p * pi_p, 1.0 / 3.0));
   c.vwn_ffact = 0.5 / (std::pow(2.0, 1.0 / 3.0) - 1.0);
@@ -135,11 +153,12 @@ __device__ __forceinline__ void slater(const XcConst& K, double n, double& f, do
 }
 
 // "VWN": Slater + VWN5 (c_lda at na = nb = n/2, where the spin
-// interpolation vanishes identically).
+// interpolation vanishes identically); "XALPHA" (K.lc == LC_NONE): Slater.
 __device__ __forceinline__ void xc_vwn(const XcConst& K, double n, double& f, double& fr) {
   f = 0.0;
   fr = 0.0;
   slater(K, n, f, fr);
+  if (K.lc == LC_NONE) return;
   const double ap = 0.0621841 / 2.0, bp = 3.72744, cp = 12.9352, x0p = -0.10498;
   const double S = n + 1.0e-50;                 // sums = na + nb + deps
   const double X = sqrt(pow(K.vwn_fact / S, K.vwn_third));
@@ -152,7 +171,7 @@ __device__ __forceinline__ void xc_vwn(const XcConst& K, double n, double& f, do
 
 // GGA exchange enhancement of the closed-shell functional e(n, g): e_x G(s^2),
 // the 1 of (1+G) omitted (x_gga, exchange.f90:325-439), G of the PBE form,
-// of Becke 88 or of PW91; adds F, dF/dn, dF/dg.
+// of Becke 88, PW91, PBEN, VMT or VT84; adds F, dF/dn, dF/dg.
 __device__ __forceinline__ void pbe_x(const XcConst& K, double n, double g, double& f, double& fr, double& fg) {
   double ex = 0.0, exr = 0.0;
   if (n > 0.0) {
@@ -201,6 +220,38 @@ __device__ __forceinline__ void pbe_x(const XcConst& K, double n, double g, doub
     } else {
       G = s2 * (T1 + s2 * T2);
       Gs = T1 + 2.0 * T2 * s2;
+    }
+  } else if (K.xg == XG_PBEN) {
+    // PBEN: G = kappa (1 - exp(-x)), x = mu s^2 / kappa; below x = 1e-4 its
+    // series to x^5 (g_pben, exchange.f90:869-902)
+    const double kappa = K.pbe_kappa, mu = K.pbe_mu;
+    const double x = mu * s2 / kappa;
+    if (x > 1.0e-4) {
+      const double e = exp(-x);
+      G = kappa * (1.0 - e);
+      Gs = mu * e;
+    } else {
+      G = kappa * x * (1.0 + x * (-1.0 / 2.0 + x * (1.0 / 6.0 + x * (-1.0 / 24.0 + x * (1.0 / 120.0)))));
+      Gs = mu * (1.0 + x * (-1.0 + x * (1.0 / 2.0 + x * (-1.0 / 6.0 + x * (1.0 / 24.0)))));
+    }
+  } else if (K.xg == XG_VMT || K.xg == XG_VT84) {
+    // VMT form mu s^2 exp(-alpha s^2) / (mu s^2 + 1) (g_vmt_form :799-817);
+    // VT84 adds (1 - exp(-alpha s^4)) (1/s^2 - 1), below s^2 = 1e-4 its
+    // series (g_vt84_2nd_term :819-856)
+    const double mu = K.pbe_mu, a = K.vmt_alpha;
+    const double e = exp(-a * s2);
+    const double d = mu * s2 + 1.0;
+    G = mu * s2 * e / d;
+    Gs = mu * e * ((1.0 - a * s2) * d - mu * s2) / (d * d);
+    if (K.xg == XG_VT84) {
+      if (s2 > 1.0e-4) {
+        const double e4 = exp(-a * s2 * s2);
+        G += (1.0 - e4) * (1.0 / s2 - 1.0);
+        Gs += 2.0 * a * s2 * e4 * (1.0 / s2 - 1.0) - (1.0 - e4) / (s2 * s2);
+      } else {
+        G += a * s2 * (1.0 + s2 * (-1.0 + s2 * (-a / 2.0 + s2 * (a / 2.0 + s2 * (a * a / 6.0)))));
+        Gs += a * (1.0 + s2 * (-2.0 + s2 * (-1.5 * a + s2 * (2.0 * a + s2 * (5.0 * a * a / 6.0)))));
+      }
     }
   } else {
     const double kappa = K.pbe_kappa, mu = K.pbe_mu;
@@ -551,8 +602,9 @@ __device__ __forceinline__ void xc_bp86(const XcConst& K, double n, double g, do
   perdew86(1, &n, &g, f, &fr, &fg);
 }
 
-// "PW91", "BPW91" (PW92 + PW91 correlation) and "BLYP" (LYP), closed shell,
-// through the dual numbers in (n, g) or, for LYP, in (rho_a, rho_b).
+// "PW91", "BPW91" (PW92 + PW91 correlation), "BLYP" (LYP) and "B88" (no
+// correlation), closed shell, through the dual numbers in (n, g) or, for
+// LYP, in (rho_a, rho_b).
 __device__ __forceinline__ void xc_gga_d3(const XcConst& K, double n, double g, double& f, double& fr, double& fg) {
   f = 0.0;
   fr = 0.0;
@@ -569,7 +621,7 @@ __device__ __forceinline__ void xc_gga_d3(const XcConst& K, double n, double g, 
     f += ec.v + c.v;
     fr += ec.d[0] + c.d[0];
     fg += c.d[1];
-  } else {
+  } else if (K.cg == CG_LYP) {
     // lyp_C (lyp.f90): ra = rb = n/2, gaa = gbb = gab = g/4; dF/dn is dF/dra
     // and dF/dg is the coefficient of gaa alone, as the reference returns them
     const double q = 0.25 * g;
@@ -600,6 +652,7 @@ __device__ __forceinline__ void xc_open_gga(const XcConst& K, const double (&rho
     fr[s] += Fn;
     fg[s] += 2.0 * Fg;
   }
+  if (K.cg == CG_NONE) return;
   if (K.cg == CG_P86) {
     perdew86(2, rho, gam, f, fr, fg);
     return;
@@ -649,10 +702,10 @@ __device__ __forceinline__ void xc_open(const XcConst& K, const double (&rho)[2]
     fr[s] += Fn;
   }
   const D3 na = d3v(0, rho[0]), nb = d3v(1, rho[1]);
-  // LDA correlation: VWN5 ("VWN", "BP"), none (LYP), else PW92
+  // LDA correlation: VWN5 ("VWN", "BP"), PW92, or none ("XALPHA", "B88", "BLYP")
   D3 ec = d3c(0.0);
-  if (!GGA || K.cg == CG_P86) ec = vwn_c_lda(K, na, nb);
-  else if (K.cg != CG_LYP) ec = pw92_c_lda(K, na, nb);
+  if (K.lc == LC_VWN) ec = vwn_c_lda(K, na, nb);
+  else if (K.lc == LC_PW92) ec = pw92_c_lda(K, na, nb);
   f += ec.v;
   fr[0] += ec.d[0];
   fr[1] += ec.d[1];

@@ -24,8 +24,22 @@ XC_BP86 = 5
 XC_PW91 = 6
 XC_BPW91 = 7
 XC_BLYP = 8
+XC_XALPHA = 9
+XC_B88 = 10
+XC_PBEN = 11
+XC_VMT = 12
+XC_VT84 = 13
+XC_VMTSOL = 14
+XC_VT84SOL = 15
 XC_IDS = {"VWN": XC_VWN, "PBE": XC_PBE, "revPBE": XC_REVPBE, "PBEsol": XC_PBESOL, "BP86": XC_BP86,
-          "PW91": XC_PW91, "BPW91": XC_BPW91, "BLYP": XC_BLYP}
+          "PW91": XC_PW91, "BPW91": XC_BPW91, "BLYP": XC_BLYP, "XALPHA": XC_XALPHA, "B88": XC_B88,
+          "PBEN": XC_PBEN, "VMT": XC_VMT, "VT84": XC_VT84, "VMTsol": XC_VMTSOL, "VT84sol": XC_VT84SOL}
+LDA_XC = ("VWN", "XALPHA")
+
+
+def is_gga(xc):
+    """True for the GGA keywords (PGXC_XC_IS_GGA)."""
+    return xc not in LDA_XC
 
 PREC_FP64 = 0
 PREC_MIXED_INT8 = 1

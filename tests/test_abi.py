@@ -61,7 +61,8 @@ def case():
 
 
 def test_rejects_bad_options(case):
-    assert _create(case, functional=9)[0] == abi.PGXC_EINVAL
+    assert _create(case, functional=max(abi.XC_IDS.values()) + 1)[0] == abi.PGXC_EINVAL
+    assert _create(case, functional=0)[0] == abi.PGXC_EINVAL
     assert _create(case, ispin=3)[0] == abi.PGXC_EINVAL
     assert _create(case, precision=7)[0] == abi.PGXC_EINVAL
 

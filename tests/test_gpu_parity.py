@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 import oracle as O
-from pgxc import cases, lib
+from pgxc import abi, cases, lib
 from conftest import fg_tolerance
 
 pytestmark = pytest.mark.gpu
@@ -94,12 +94,12 @@ def test_raw_weight_grid_is_becke_scaled_on_device(thr):
     assert np.max(np.abs(ham - ref_ham)) < TOL
 
 
-@pytest.mark.parametrize("xc", ["VWN", "PBE", "revPBE", "PBEsol", "BP86", "PW91", "BPW91", "BLYP"])
+@pytest.mark.parametrize("xc", list(abi.XC_IDS))
 def test_point_functionals(xc):
     rng = np.random.default_rng(1)
     rho = np.concatenate([[0.0, 1e-35, 1e-31, 1e-25, 1e-21, 1e-19], 10 ** rng.uniform(-14, 3, 500)])
     gam = np.concatenate([[0.0] * 6, 10 ** rng.uniform(-20, 4, 500)])
-    f, fr, fg = lib.xc_functionals(xc, rho, gam if xc != "VWN" else None)
+    f, fr, fg = lib.xc_functionals(xc, rho, gam if abi.is_gga(xc) else None)
     rf, rfr, rfg = O.functionals(xc, 1, rho, gam)
     # Errors are measured against the size of the Slater term at each point:
     # the pieces of f and df/drho have mixed signs, so a relative test on the
@@ -125,7 +125,7 @@ def test_point_functionals(xc):
         tol_g = np.maximum(tol_g, 8 * np.abs(pg[:, 0] - rfg[:, 0]))
     assert np.all(np.abs(f - rf) <= tol_f), np.max(np.abs(f - rf) / tol_f)
     assert np.all(np.abs(fr - rfr[:, 0]) <= tol_r), np.max(np.abs(fr - rfr[:, 0]) / tol_r)
-    if xc != "VWN":
+    if abi.is_gga(xc):
         assert np.all(np.abs(fg - rfg[:, 0]) <= tol_g), np.max(np.abs(fg - rfg[:, 0]) / tol_g)
 
 
@@ -217,11 +217,13 @@ def test_build_from_density_matrix_open_shell():
                                                       ("screened", "mixed", 1e-10, 1e-7)],
                          ids=["fp64-dense", "fp64-screened", "int8-screened"])
 @pytest.mark.parametrize("xc,seed", [("revPBE", 2), ("PBEsol", 3), ("BP86", 4), ("PW91", 5), ("BPW91", 6),
-                                     ("BLYP", 7)])
+                                     ("BLYP", 7), ("XALPHA", 8), ("B88", 9), ("PBEN", 10), ("VMT", 11),
+                                     ("VT84", 12), ("VMTsol", 13), ("VT84sol", 14)])
 def test_gga_keyword_builds(xc, seed, layout, precision, thr, tol):
     """revPBE and PBEsol (the PBE-form keywords with other kappa, mu, beta),
-    BP86 (Becke 88 + Perdew 86), PW91, BPW91 (Becke 88 + PW91 correlation)
-    and BLYP (Becke 88 + LYP) through every layout, against the oracle."""
+    BP86 (Becke 88 + Perdew 86), PW91, BPW91 (Becke 88 + PW91 correlation),
+    BLYP (Becke 88 + LYP), XALPHA, B88 and the PBEN / VMT / VT84 exchange
+    variants through every layout, against the oracle."""
     c = cases.small_case(functional=xc, seed=seed, lmax=3, natoms=5, nocc=7)
     O.weight_case(c)
     dE, dN, dV, _, _ = compare(c, precision=precision, screen_threshold=thr, max_chunk_points=1024)

@@ -10,15 +10,15 @@ import numpy as np
 import pytest
 
 import oracle as O
-from pgxc import cases
+from pgxc import abi, cases
 
 
 RHO = np.array([1e-12, 1e-6, 1e-3, 0.05, 0.7, 3.0, 120.0])
 GAM = np.array([1e-20, 1e-9, 1e-5, 0.02, 0.9, 10.0, 5e4])
 
 
-ALL_XC = ["VWN", "PBE", "revPBE", "PBEsol", "BP86", "PW91", "BPW91", "BLYP"]
-GGA_XC = ALL_XC[1:]
+ALL_XC = list(abi.XC_IDS)
+GGA_XC = [x for x in ALL_XC if abi.is_gga(x)]
 
 
 @pytest.mark.parametrize("xc", ALL_XC)
@@ -35,7 +35,7 @@ def test_functional_derivatives_fd(xc):
     np.testing.assert_allclose(fr[:, 0], num, rtol=2e-6, atol=1e-12)
     # closed-shell BLYP returns the LYP coefficient of gamma_aa as dF/dgamma,
     # as the reference does: test_lyp_published_form covers it
-    if xc not in ("VWN", "BLYP"):
+    if abi.is_gga(xc) and xc != "BLYP":
         hg = 1e-4 * gam
         gp, _, _ = O.functionals(xc, 1, rho, gam + hg)
         gm, _, _ = O.functionals(xc, 1, rho, gam - hg)
@@ -58,7 +58,7 @@ def test_functional_spin_consistency(xc):
     f2, fr2, fg2 = O.functionals(xc, 2, r2, g2)
     np.testing.assert_allclose(f2, f1, rtol=1e-12, atol=1e-300)
     np.testing.assert_allclose(fr2[:, 0], fr1[:, 0], rtol=1e-10, atol=1e-14)
-    if xc not in ("VWN", "BLYP"):
+    if abi.is_gga(xc) and xc != "BLYP":
         # d/dg_aa + d/dg_bb + d/dg_ab of g = g_aa + g_bb + 2 g_ab
         np.testing.assert_allclose((fg2[:, 0] + fg2[:, 1] + fg2[:, 2]) / 4, fg1[:, 0], rtol=1e-9, atol=1e-14)
 
@@ -82,6 +82,9 @@ def test_open_shell_derivatives_fd(xc):
         xm[:, k] -= h
         num = (O.functionals(xc, 2, xp[:, :2], xp[:, 2:])[0] - O.functionals(xc, 2, xm[:, :2], xm[:, 2:])[0]) / (2 * h)
         ok = np.abs(ana[:, k] * h) > 1e-10 * np.abs(f)
+        if not ok.any():  # no dependence at all (exchange alone has none on gamma_ab)
+            assert np.all(ana[:, k] == 0.0) and np.all(np.abs(num * h) <= 1e-12 * np.abs(f)), k
+            continue
         assert ok.sum() >= 6, (k, ok)
         np.testing.assert_allclose(ana[ok, k], num[ok], rtol=2e-5, err_msg=f"{xc} partial {k}")
 
@@ -139,6 +142,38 @@ def test_lyp_published_form():
           - _b88_published(rho / 2, rho / 2, (gam - h) / 4, (gam - h) / 4)) / (2 * h)
     caa = _lyp_published(rho / 2, rho / 2, 1.0 + q, q, q) - _lyp_published(rho / 2, rho / 2, q, q, q)
     np.testing.assert_allclose(fg1[:, 0], dx + caa, rtol=1e-6)
+
+
+def test_exchange_variants_published_form():
+    """XALPHA is Slater alone and B88 is Slater + Becke 88 (no correlation);
+    PBEN (kappa (1 - exp(-mu s^2 / kappa)), the RPBE form), VMT
+    (mu s^2 exp(-alpha s^2) / (1 + mu s^2)) and VT{8,4} (VMT plus
+    (1 - exp(-alpha s^4)) (1/s^2 - 1)) share PBE's LDA and correlation parts,
+    so each differs from PBE by e_x (F_x - F_PBE)."""
+    rng = np.random.default_rng(31)
+    rho = 10 ** rng.uniform(-3, 1.5, 12)
+    gam = rho ** (8 / 3) * 10 ** rng.uniform(-6, 1.5, 12)
+    pi = 3.14159265358979324
+    ex = -(3 / 4) * (3 / pi) ** (1 / 3) * rho ** (4 / 3)
+    np.testing.assert_allclose(O.functionals("XALPHA", 1, rho)[0], ex, rtol=1e-14)
+    q = gam / 4
+    np.testing.assert_allclose(O.functionals("B88", 1, rho, gam)[0], _b88_published(rho / 2, rho / 2, q, q), rtol=1e-12)
+    s2 = gam / (4 * (3 * pi ** 2) ** (2 / 3) * rho ** (8 / 3))
+    mu, sol = 0.066725 * pi ** 2 / 3, 10 / 81
+    vmt = lambda m, a: m * s2 * np.exp(-a * s2) / (1 + m * s2)
+    # the reference evaluates 1 - exp(-alpha s^4) as written above s^2 = 1e-4
+    # (it cancels to ~1e-16 / (alpha s^4) there) and its series below
+    vt84 = lambda m, a: vmt(m, a) + np.where(s2 > 1e-4, (1 - np.exp(-a * s2 * s2)) * (1 / s2 - 1),
+                                             -np.expm1(-a * s2 * s2) * (1 / s2 - 1))
+    want = {"PBEN": -0.804 * np.expm1(-mu * s2 / 0.804),
+            "VMT": vmt(mu, 0.002762), "VT84": vt84(mu, 0.000069),
+            "VMTsol": vmt(sol, 0.0015532), "VT84sol": vt84(sol, 0.000023)}
+    fp = O.functionals("PBE", 1, rho, gam)[0]
+    gp = 0.804 * mu * s2 / (0.804 + mu * s2)
+    for xc, g in want.items():
+        d = O.functionals(xc, 1, rho, gam)[0] - fp
+        w = ex * (g - gp)
+        assert np.all(np.abs(d - w) <= 1e-9 * np.abs(w) + 1e-13 * np.abs(fp)), (xc, d, w)
 
 
 def _pw91_h_published(n, g, ec):
