@@ -78,8 +78,16 @@ extern "C" {
 #define PGXC_XC_VT84 13
 #define PGXC_XC_VMTSOL 14
 #define PGXC_XC_VT84SOL 15
+/* HCTH/93, /120, /147, /407: Hamprecht-Cohen-Tozer-Handy exchange and
+ * correlation, a whole functional with no Slater or LDA part (keywords "HCTH"
+ * or "HCTHv1", "HCTH120" or "HCTHv2", "HCTH147" or "HCTHv3", "HCTH407" or
+ * "HCTHv4", modules/xc_cntrl.f90:801-831; modules/hcth.f90) */
+#define PGXC_XC_HCTH 16
+#define PGXC_XC_HCTH120 17
+#define PGXC_XC_HCTH147 18
+#define PGXC_XC_HCTH407 19
 /* the largest functional id */
-#define PGXC_XC_LAST PGXC_XC_VT84SOL
+#define PGXC_XC_LAST PGXC_XC_HCTH407
 /* nonzero for the GGA keywords (all but the two LDAs) */
 #define PGXC_XC_IS_GGA(id) ((id) != PGXC_XC_VWN && (id) != PGXC_XC_XALPHA)
 

@@ -435,6 +435,81 @@ D lyp_corr(D ra, D rb, double gaa, double gbb, double gab, double (&cg)[3]) {
 }
 
 // ---------------------------------------------------------------------------
+// HCTH: pg_hcth, hcth_x_calc, hcth_c_calc and pwldac of modules/hcth.f90;
+// coefficients CHCTH(0:4, {X, Caa, Cab}, version) (:80-150, the published
+// HCTH/93, /120, /147 and /407 sets).  Spin densities ra, rb and gamma_aa,
+// gamma_bb; adds f, fr[0..1], fg[0..1] (no gamma_ab dependence).
+// ---------------------------------------------------------------------------
+const double HCTH_C[4][3][5] = {
+    {{1.09320, -0.744056, 5.59920, -6.78549, 4.49357},
+     {0.222601, -0.0338622, -0.0125170, -0.802496, 1.55396},
+     {0.729974, 3.35287, -11.5430, 8.08564, -4.47857}},
+    {{1.09163, -0.747215, 5.07833, -4.10746, 1.17173},
+     {0.489508, -0.260699, 0.432917, -1.99247, 2.48531},
+     {0.514730, 6.92982, -24.7073, 23.1098, -11.3234}},
+    {{1.09025, -0.799194, 5.57212, -5.86760, 3.04544},
+     {0.562576, 0.0171436, -1.30636, 1.05747, 0.885429},
+     {0.542352, 7.01464, -28.3822, 35.0329, -20.4284}},
+    {{1.08184, -0.518339, 3.42562, -2.62901, 2.28855},
+     {1.18777, -2.40292, 5.61741, -9.17923, 6.24798},
+     {0.589076, 4.42374, -19.2218, 42.5721, -42.0052}}};
+
+// g(c, s2) = sum_n c_n u^n, u = s2/(1+s2), and dg/ds2
+void hcth_g(const double* c, double s2, double& g0, double& g1) {
+  const double u = s2 / (1.0 + s2), du = 1.0 / ((1.0 + s2) * (1.0 + s2));
+  g0 = 0.0;
+  g1 = 0.0;
+  for (int n = 4; n >= 1; --n) {
+    g0 = c[n] + u * g0;
+    g1 = n * c[n] + u * g1;
+  }
+  g0 = c[0] + u * g0;
+  g1 = g1 * du;
+}
+
+void hcth(int version, double ra, double rb, double gaa, double gbb, double& f, double* fr, double* fg) {
+  const double DEPS = 1.0e-15, pi = 3.14159265358979324;
+  const double* cx = HCTH_C[version - 1][0];
+  const double* caa = HCTH_C[version - 1][1];
+  const double* cab = HCTH_C[version - 1][2];
+  // exchange (hcth_x_calc, calc)
+  const double xalpha = -(3.0 / 2.0) * std::pow(3.0 / (4.0 * pi), 1.0 / 3.0);
+  const double r[2] = {ra, rb}, z[2] = {gaa, gbb};
+  for (int s = 0; s < 2; ++s) {
+    if (r[s] < DEPS) continue;
+    const double ex = xalpha * std::pow(r[s], 4.0 / 3.0);
+    const double dex = xalpha * std::pow(r[s], 1.0 / 3.0) * (4.0 / 3.0);
+    const double s2 = 0.004 * z[s] / std::pow(r[s], 8.0 / 3.0);
+    const double ds2r = -(8.0 / 3.0) * s2 / r[s];
+    const double ds2z = 0.004 / std::pow(r[s], 8.0 / 3.0);
+    double u, du;
+    hcth_g(cx, s2, u, du);
+    f += ex * u;
+    fr[s] += ex * du * ds2r + dex * u;
+    fg[s] += ex * du * ds2z;
+  }
+  // correlation (hcth_c_calc, pwldac)
+  if (ra + rb < DEPS) return;
+  D eaa = pw92::c_lda(var(0, ra), cst(0.0));
+  D ebb = pw92::c_lda(var(1, rb), cst(0.0));
+  D eab = pw92::c_lda(var(0, ra), var(1, rb)) - eaa - ebb;
+  const double ma = std::max(ra, DEPS), mb = std::max(rb, DEPS);
+  const double saa = gaa / std::pow(ma, 8.0 / 3.0), sbb = gbb / std::pow(mb, 8.0 / 3.0);
+  const double sab = 0.5 * (saa + sbb);
+  const double ds_aa_ra = -(8.0 / 3.0) * saa / ma, ds_bb_rb = -(8.0 / 3.0) * sbb / mb;
+  const double ds_aa_za = 1.0 / std::pow(ma, 8.0 / 3.0), ds_bb_zb = 1.0 / std::pow(mb, 8.0 / 3.0);
+  double uaa, duaa, ubb, dubb, uab, duab;
+  hcth_g(caa, 0.2 * saa, uaa, duaa);
+  hcth_g(caa, 0.2 * sbb, ubb, dubb);
+  hcth_g(cab, 0.006 * sab, uab, duab);
+  f += eaa.v * uaa + ebb.v * ubb + eab.v * uab;
+  fr[0] += eaa.d[0] * uaa + eaa.v * duaa * (0.2 * ds_aa_ra) + eab.d[0] * uab + eab.v * duab * (0.006 * 0.5 * ds_aa_ra);
+  fr[1] += ebb.d[1] * ubb + ebb.v * dubb * (0.2 * ds_bb_rb) + eab.d[1] * uab + eab.v * duab * (0.006 * 0.5 * ds_bb_rb);
+  fg[0] += eaa.v * duaa * (0.2 * ds_aa_za) + eab.v * duab * (0.006 * 0.5 * ds_aa_za);
+  fg[1] += ebb.v * dubb * (0.2 * ds_bb_zb) + eab.v * duab * (0.006 * 0.5 * ds_bb_zb);
+}
+
+// ---------------------------------------------------------------------------
 // xc_functionals (modules/xc_func.f90:187-305) for the keywords.
 // rho[ispin], gam[2*ispin-1] (aa, bb, ab); outputs f, fr[ispin], fg[2ispin-1].
 // ---------------------------------------------------------------------------
@@ -502,6 +577,19 @@ void functional_point(int xc, int ispin, const double* rho, const double* gam,
   fr[0] = fr[1] = 0.0;
   fg[0] = fg[1] = fg[2] = 0.0;
   const GgaPar P = gga_par(xc);
+  if (xc >= PGXC_XC_HCTH && xc <= PGXC_XC_HCTH407) {
+    // pg_hcth (hcth.f90): closed shell at ra = rb = n/2, gaa = gbb = g/4
+    const int v = xc - PGXC_XC_HCTH + 1;
+    if (ispin == 1) {
+      double r2[2] = {0, 0}, g2[2] = {0, 0};
+      hcth(v, 0.5 * rho[0], 0.5 * rho[0], 0.25 * gam[0], 0.25 * gam[0], f, r2, g2);
+      fr[0] = 0.5 * (r2[0] + r2[1]);
+      fg[0] = 0.25 * (g2[0] + g2[1]);
+    } else {
+      hcth(v, rho[0], rho[1], gam[0], gam[1], f, fr, fg);
+    }
+    return;
+  }
   // Slater exchange (exchange_lda, exchange.f90:511-565)
   if (ispin == 1) {
     D e = x_lda(var(0, rho[0]));

@@ -15,12 +15,14 @@
 //   Perdew 86 correlation modules/becke_perdew_module.f90:125-260
 //   PW91 correlation      modules/gga_response_module.f90:278-918 (H0 + H1)
 //   LYP correlation       modules/lyp.f90 (lyp_C, lyp_corr)
+//   HCTH                  modules/hcth.f90 (pg_hcth, hcth_x_calc, hcth_c_calc)
 // composed as the XC keywords do (modules/xc_cntrl.f90:460-798):
 //   "VWN" = Slater + VWN5, "PBE" = Slater + PW92 + PBE-X(G) + PBE-C(H),
 //   "BP" = Slater + VWN5 + B88 + P86, "PW91" = Slater + PW92 + PW91-X + PW91-C,
 //   "BPW91" = Slater + PW92 + B88 + PW91-C, "BLYP" = Slater + B88 + LYP,
 //   "XALPHA" = Slater, "B88" = Slater + B88, "PBEN" / "VMT" / "VT84" /
-//   "VMTsol" / "VT84sol" = Slater + PW92 + their G + PBE-C.
+//   "VMTsol" / "VT84sol" = Slater + PW92 + their G + PBE-C, "HCTH*" = HCTH
+//   exchange + correlation alone.
 // Literal constants, density guards and epsilons are the reference's.
 #pragma once
 
@@ -59,7 +61,30 @@ struct XcConst {
   double vwn_ffact;     // (1/2) / (2^(1/3) - 1)
   double pw_cf;         // 1 / (2^(4/3) - 2)
   double pbe_two13i;    // 1 / 2^(1/3)
+  // HCTH: version 1..4 (0: not HCTH), its power-series coefficients of
+  // exchange, same-spin and opposite-spin correlation, and the spin-resolved
+  // Slater constant -(3/2)(3/(4 pi))^(1/3)
+  int hcth;
+  double hcth_x[5], hcth_caa[5], hcth_cab[5];
+  double hcth_xa;
 };
+
+// HCTH coefficients c_0..c_4 of exchange, same-spin and opposite-spin
+// correlation for versions 1..4 (HCTH/93, /120, /147, /407), as tabulated in
+// modules/hcth.f90:80-150 (the published sets).
+constexpr double kHcth[4][3][5] = {
+    {{1.09320, -0.744056, 5.59920, -6.78549, 4.49357},
+     {0.222601, -0.0338622, -0.0125170, -0.802496, 1.55396},
+     {0.729974, 3.35287, -11.5430, 8.08564, -4.47857}},
+    {{1.09163, -0.747215, 5.07833, -4.10746, 1.17173},
+     {0.489508, -0.260699, 0.432917, -1.99247, 2.48531},
+     {0.514730, 6.92982, -24.7073, 23.1098, -11.3234}},
+    {{1.09025, -0.799194, 5.57212, -5.86760, 3.04544},
+     {0.562576, 0.0171436, -1.30636, 1.05747, 0.885429},
+     {0.542352, 7.01464, -28.3822, 35.0329, -20.4284}},
+    {{1.08184, -0.518339, 3.42562, -2.62901, 2.28855},
+     {1.18777, -2.40292, 5.61741, -9.17923, 6.24798},
+     {0.589076, 4.42374, -19.2218, 42.5721, -42.0052}}};
 
 // GGA pieces of a keyword.  Exchange enhancement: the PBE form (kappa, mu),
 // Becke 88, or PW91.  Correlation: PW92 + PBE H, VWN5 + Perdew 86, PW92 +
@@ -106,6 +131,14 @@ __host__ inline XcConst make_xc_const(int functional = PGXC_XC_PBE) {
          : (f == PGXC_XC_B88 || !PGXC_XC_IS_GGA(f)) ? CG_NONE : CG_PBE;
   c.lc = (f == PGXC_XC_VWN || f == PGXC_XC_BP86) ? LC_VWN
          : (f == PGXC_XC_XALPHA || f == PGXC_XC_B88 || f == PGXC_XC_BLYP) ? LC_NONE : LC_PW92;
+  c.hcth = (f >= PGXC_XC_HCTH && f <= PGXC_XC_HCTH407) ? f - PGXC_XC_HCTH + 1 : 0;
+  for (int n = 0; n < 5; ++n) {
+    const int v = c.hcth > 0 ? c.hcth - 1 : 0;
+    c.hcth_x[n] = kHcth[v][0][n];
+    c.hcth_caa[n] = kHcth[v][1][n];
+    c.hcth_cab[n] = kHcth[v][2][n];
+  }
+  c.hcth_xa = -(3.0 / 2.0) * std::pow(3.0 / (4.0 * 3.14159265358979324), 1.0 / 3.0);
   c.pbe_fi = (std::pow(0.5, 2.0 / 3.0) + std::pow(0.5, 2.0 / 3.0)) * (1.0 / std::pow(2.0, 1.0 / 3.0));
   c.pbe_ct = pi_p / (4.0 * 4.0 * std::pow(3.0 * pi_p * pi_p, 1.0 / 3.0));
   c.vwn_ffact = 0.5 / (std::pow(2.0, 1.0 / 3.0) - 1.0);
@@ -538,6 +571,67 @@ __device__ __forceinline__ D3 lyp_corr(const XcConst& K, D3 ra, D3 rb, double ga
   return -lda1 - lda2 - caa * gaa - cbb * gbb - cab * gab;
 }
 
+// HCTH power series g(s2) = sum_n c_n u^n, u = s2 / (1 + s2), and dg/ds2
+// (hcth.f90 g, in hcth_x_calc and hcth_c_calc).
+__device__ __forceinline__ void hcth_g(const double (&c)[5], double s2, double& g0, double& g1) {
+  const double u = s2 / (1.0 + s2);
+  const double du = 1.0 / ((1.0 + s2) * (1.0 + s2));
+  double a = 0.0, b = 0.0;
+#pragma unroll
+  for (int n = 4; n >= 1; --n) {
+    a = c[n] + u * a;
+    b = n * c[n] + u * b;
+  }
+  g0 = c[0] + u * a;
+  g1 = b * du;
+}
+
+// HCTH at one point of spin densities ra, rb and gamma_aa, gamma_bb (it has no
+// gamma_ab dependence): hcth_x_calc and hcth_c_calc (hcth.f90).  Adds f,
+// fr[0..1], fg[0..1].
+__device__ __forceinline__ void hcth_point(const XcConst& K, double ra, double rb, double gaa, double gbb, double& f,
+                                           double* fr, double* fg) {
+  const double deps = 1.0e-15;
+  // exchange, per spin: e_x,s g_x(0.004 gamma_ss / rho_s^(8/3))
+  const double rs[2] = {ra, rb}, gs[2] = {gaa, gbb};
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    const double r = rs[s];
+    if (r < deps) continue;
+    const double c = cbrt(r);
+    const double ex = K.hcth_xa * r * c;
+    const double dex = K.hcth_xa * c * (4.0 / 3.0);
+    const double r83 = r * r * c * c;
+    const double s2 = 0.004 * gs[s] / r83;
+    double u, du;
+    hcth_g(K.hcth_x, s2, u, du);
+    f += ex * u;
+    fr[s] += ex * du * (-(8.0 / 3.0) * s2 / r) + dex * u;
+    fg[s] += ex * du * (0.004 / r83);
+  }
+  // correlation: e_aa g_aa(0.2 s_aa^2) + e_bb g_aa(0.2 s_bb^2) + e_ab g_ab(0.006 s_avg^2),
+  // e_ss = PW92 of the fully polarised density rho_s, e_ab = PW92(ra, rb) - e_aa - e_bb
+  if (ra + rb < deps) return;
+  const D3 na = d3v(0, ra), nb = d3v(1, rb);
+  const D3 eaa = pw92_c_lda(K, na, d3c(0.0));
+  const D3 ebb = pw92_c_lda(K, nb, d3c(0.0));
+  const D3 eab = pw92_c_lda(K, na, nb) - eaa - ebb;
+  const double ma = fmax(ra, deps), mb = fmax(rb, deps);
+  const double ca = cbrt(ma), cb = cbrt(mb);
+  const double ia = 1.0 / (ma * ma * ca * ca), ib = 1.0 / (mb * mb * cb * cb);  // rho^(-8/3)
+  const double saa = gaa * ia, sbb = gbb * ib, sab = 0.5 * (saa + sbb);
+  const double daa = -(8.0 / 3.0) * saa / ma, dbb = -(8.0 / 3.0) * sbb / mb;
+  double uaa, duaa, ubb, dubb, uab, duab;
+  hcth_g(K.hcth_caa, 0.2 * saa, uaa, duaa);
+  hcth_g(K.hcth_caa, 0.2 * sbb, ubb, dubb);
+  hcth_g(K.hcth_cab, 0.006 * sab, uab, duab);
+  f += eaa.v * uaa + ebb.v * ubb + eab.v * uab;
+  fr[0] += eaa.d[0] * uaa + eaa.v * duaa * (0.2 * daa) + eab.d[0] * uab + eab.v * duab * (0.006 * 0.5 * daa);
+  fr[1] += ebb.d[1] * ubb + ebb.v * dubb * (0.2 * dbb) + eab.d[1] * uab + eab.v * duab * (0.006 * 0.5 * dbb);
+  fg[0] += eaa.v * duaa * (0.2 * ia) + eab.v * duab * (0.006 * 0.5 * ia);
+  fg[1] += ebb.v * dubb * (0.2 * ib) + eab.v * duab * (0.006 * 0.5 * ib);
+}
+
 // Perdew 86 gradient correlation with its first derivatives (perdew_calc,
 // modules/becke_perdew_module.f90:125-260; constants :83-118).  ispin = 1:
 // rho[0], gam[0]; ispin = 2: rho[0..1], gam = (aa, bb, ab), the correlation
@@ -633,9 +727,20 @@ __device__ __forceinline__ void xc_gga_d3(const XcConst& K, double n, double g, 
   }
 }
 
+// HCTH, closed shell (pg_hcth, hcth.f90): ra = rb = n/2, gaa = gbb = g/4,
+// df/dn = (df/dra + df/drb)/2, df/dg = (df/dgaa + df/dgbb)/4.
+__device__ __forceinline__ void xc_hcth(const XcConst& K, double n, double g, double& f, double& fr, double& fg) {
+  double r2[2] = {0.0, 0.0}, g2[2] = {0.0, 0.0};
+  f = 0.0;
+  hcth_point(K, 0.5 * n, 0.5 * n, 0.25 * g, 0.25 * g, f, r2, g2);
+  fr = 0.5 * (r2[0] + r2[1]);
+  fg = 0.25 * (g2[0] + g2[1]);
+}
+
 // The closed-shell GGA keyword of K.
 __device__ __forceinline__ void xc_gga(const XcConst& K, double n, double g, double& f, double& fr, double& fg) {
-  if (K.cg == CG_PBE) xc_pbe(K, n, g, f, fr, fg);
+  if (K.hcth) xc_hcth(K, n, g, f, fr, fg);
+  else if (K.cg == CG_PBE) xc_pbe(K, n, g, f, fr, fg);
   else if (K.cg == CG_P86) xc_bp86(K, n, g, f, fr, fg);
   else xc_gga_d3(K, n, g, f, fr, fg);
 }
@@ -694,6 +799,10 @@ __device__ __forceinline__ void xc_open(const XcConst& K, const double (&rho)[2]
   f = 0.0;
   fr[0] = fr[1] = 0.0;
   fg[0] = fg[1] = fg[2] = 0.0;
+  if (GGA && K.hcth) {
+    hcth_point(K, rho[0], rho[1], gam[0], gam[1], f, fr, fg);
+    return;
+  }
   // Slater, spin-scaled
   for (int s = 0; s < 2; ++s) {
     double F = 0.0, Fn = 0.0;

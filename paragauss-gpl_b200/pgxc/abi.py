@@ -31,9 +31,14 @@ XC_VMT = 12
 XC_VT84 = 13
 XC_VMTSOL = 14
 XC_VT84SOL = 15
+XC_HCTH = 16
+XC_HCTH120 = 17
+XC_HCTH147 = 18
+XC_HCTH407 = 19
 XC_IDS = {"VWN": XC_VWN, "PBE": XC_PBE, "revPBE": XC_REVPBE, "PBEsol": XC_PBESOL, "BP86": XC_BP86,
           "PW91": XC_PW91, "BPW91": XC_BPW91, "BLYP": XC_BLYP, "XALPHA": XC_XALPHA, "B88": XC_B88,
-          "PBEN": XC_PBEN, "VMT": XC_VMT, "VT84": XC_VT84, "VMTsol": XC_VMTSOL, "VT84sol": XC_VT84SOL}
+          "PBEN": XC_PBEN, "VMT": XC_VMT, "VT84": XC_VT84, "VMTsol": XC_VMTSOL, "VT84sol": XC_VT84SOL,
+          "HCTH": XC_HCTH, "HCTH120": XC_HCTH120, "HCTH147": XC_HCTH147, "HCTH407": XC_HCTH407}
 LDA_XC = ("VWN", "XALPHA")
 
 

@@ -87,6 +87,11 @@ def test_point_functionals_open_shell(xc):
             err = np.abs(fg[:, k] - rfg[:, k])
             tol = 1e-10 * np.abs(rfg[:, k]) + np.where(gs > 0, 1e-10 * (np.abs(rf) + sf) / np.maximum(gs, 1e-300), 0)
             tol = np.maximum(np.where(well, tol, np.inf), 8 * noise_g[:, k])
+            if xc.startswith("HCTH") and k < 2:
+                # HCTH floors rho_s at 1e-15 under rho_s^(-8/3) (hcth_c_calc): for an
+                # empty spin, d/dgamma_ss is 1e40 times a rounding residue of the PW92
+                # energies; it multiplies grad rho_s = 0 in V and is not compared
+                tol = np.where(rho[:, k] >= 1e-15, tol, np.inf)
             assert np.all(err <= tol + 1e-300), (k, np.max(err / (tol + 1e-300)))
 
 
@@ -94,7 +99,7 @@ def test_point_functionals_equal_spins_match_closed_shell():
     rng = np.random.default_rng(3)
     rho = 10 ** rng.uniform(-8, 3, 300)
     gam = rho ** (8 / 3) * 10 ** rng.uniform(-4, 2, 300)
-    for xc in ("VWN", "PBE", "PW91", "BLYP"):
+    for xc in ("VWN", "PBE", "PW91", "BLYP", "HCTH"):
         gga = xc != "VWN"
         if xc == "PW91":
             # the open shell floors |grad rho|^2 at 1e-20, the closed shell does
@@ -109,7 +114,7 @@ def test_point_functionals_equal_spins_match_closed_shell():
         np.testing.assert_allclose(fr2[:, 1], fr1, rtol=1e-10)
         # closed-shell BLYP returns the LYP coefficient of gamma_aa as df/dgamma
         # (as lyp.f90 does), not the sum over the three invariants
-        if xc in ("PBE", "PW91"):
+        if xc in ("PBE", "PW91", "HCTH"):
             fsum = (fg2[:, 0] + fg2[:, 1] + fg2[:, 2]) / 4
             assert np.all(np.abs(fsum - fg1) <= fg_tolerance(rho, gam, f1, fg1))
 
@@ -132,7 +137,7 @@ BUILDS = pytest.mark.parametrize("precision,thr,tol", [("fp64", 0.0, 1e-10), ("m
 
 @BUILDS
 @pytest.mark.parametrize("xc,seed,lmax", [("VWN", 1, 2), ("PBE", 2, 2), ("PBE", 3, 3), ("VWN", 4, 3), ("BP86", 5, 2),
-                                          ("PW91", 6, 2), ("BLYP", 7, 3)])
+                                          ("PW91", 6, 2), ("BLYP", 7, 3), ("HCTH407", 8, 2)])
 def test_open_shell_build(xc, seed, lmax, precision, thr, tol):
     c = cases.small_case(functional=xc, seed=seed, lmax=lmax, natoms=5, nocc=7, ispin=2)
     O.weight_case(c)

@@ -218,12 +218,13 @@ def test_build_from_density_matrix_open_shell():
                          ids=["fp64-dense", "fp64-screened", "int8-screened"])
 @pytest.mark.parametrize("xc,seed", [("revPBE", 2), ("PBEsol", 3), ("BP86", 4), ("PW91", 5), ("BPW91", 6),
                                      ("BLYP", 7), ("XALPHA", 8), ("B88", 9), ("PBEN", 10), ("VMT", 11),
-                                     ("VT84", 12), ("VMTsol", 13), ("VT84sol", 14)])
+                                     ("VT84", 12), ("VMTsol", 13), ("VT84sol", 14), ("HCTH", 15),
+                                     ("HCTH120", 16), ("HCTH147", 17), ("HCTH407", 18)])
 def test_gga_keyword_builds(xc, seed, layout, precision, thr, tol):
     """revPBE and PBEsol (the PBE-form keywords with other kappa, mu, beta),
     BP86 (Becke 88 + Perdew 86), PW91, BPW91 (Becke 88 + PW91 correlation),
-    BLYP (Becke 88 + LYP), XALPHA, B88 and the PBEN / VMT / VT84 exchange
-    variants through every layout, against the oracle."""
+    BLYP (Becke 88 + LYP), XALPHA, B88, the PBEN / VMT / VT84 exchange
+    variants and the four HCTH sets through every layout, against the oracle."""
     c = cases.small_case(functional=xc, seed=seed, lmax=3, natoms=5, nocc=7)
     O.weight_case(c)
     dE, dN, dV, _, _ = compare(c, precision=precision, screen_threshold=thr, max_chunk_points=1024)

@@ -26,12 +26,14 @@ def test_functional_derivatives_fd(xc):
     rho = RHO.copy()
     gam = GAM.copy()
     f, fr, fg = O.functionals(xc, 1, rho, gam)
-    # a step of 1e-4: where exchange and correlation cancel to f ~ 1e-25
-    # (PW91 at rho = 1e-12), a smaller one resolves only rounding
-    h = 1e-4 * rho
-    fp, _, _ = O.functionals(xc, 1, rho + h, gam)
-    fm, _, _ = O.functionals(xc, 1, rho - h, gam)
-    num = (fp - fm) / (2 * h)
+    # a step of 1e-3 with Richardson extrapolation: where exchange and
+    # correlation cancel (PW91 at rho = 1e-12 to f ~ 1e-25, HCTH to ~1e-16) a
+    # smaller step resolves only rounding, and at large s (VT84's 1/s^2) a
+    # plain central difference of this step is off by its h^2 term
+    def central(h):
+        return (O.functionals(xc, 1, rho + h, gam)[0] - O.functionals(xc, 1, rho - h, gam)[0]) / (2 * h)
+    h = 1e-3 * rho
+    num = (4 * central(h / 2) - central(h)) / 3
     np.testing.assert_allclose(fr[:, 0], num, rtol=2e-6, atol=1e-12)
     # closed-shell BLYP returns the LYP coefficient of gamma_aa as dF/dgamma,
     # as the reference does: test_lyp_published_form covers it
@@ -376,3 +378,44 @@ def test_becke_partition_of_unity(small_cases):
         cc.point_atom = np.full(len(pts), a, dtype=np.int32)
         tot += O.becke(cc)
     np.testing.assert_allclose(tot, 1.0, atol=1e-13)
+
+
+HCTH_SETS = {  # published c_0..c_4 of exchange, same-spin and opposite-spin correlation
+    "HCTH": ([1.09320, -0.744056, 5.59920, -6.78549, 4.49357], [0.222601, -0.0338622, -0.0125170, -0.802496, 1.55396],
+             [0.729974, 3.35287, -11.5430, 8.08564, -4.47857]),
+    "HCTH407": ([1.08184, -0.518339, 3.42562, -2.62901, 2.28855], [1.18777, -2.40292, 5.61741, -9.17923, 6.24798],
+                [0.589076, 4.42374, -19.2218, 42.5721, -42.0052]),
+}
+
+
+@pytest.mark.parametrize("xc", list(HCTH_SETS))
+def test_hcth_published_form(xc):
+    """HCTH (Hamprecht, Cohen, Tozer, Handy): sum over spins of
+    e_x,s g_x(0.004 s_s^2) + e_ss g_ss(0.2 s_s^2) + e_ab g_ab(0.006 (s_a^2 + s_b^2)/2),
+    g(x) = sum_n c_n (x / (1 + x))^n, s_s^2 = gamma_ss / rho_s^(8/3); the PW92
+    energies e_ss = e(rho_s, 0) and e_ab = e(ra, rb) - e_aa - e_bb are taken
+    from the PBE keyword at zero gradient (Slater subtracted)."""
+    cx, css, cab = (np.array(c) for c in HCTH_SETS[xc])
+    g = lambda c, x: sum(c[n] * (x / (1 + x)) ** n for n in range(5))
+    rng = np.random.default_rng(41)
+    ra = 10 ** rng.uniform(-3, 1.5, 10)
+    rb = ra * rng.uniform(0.1, 1.0, 10)
+    gaa = ra ** (8 / 3) * rng.uniform(0.01, 3.0, 10)
+    gbb = rb ** (8 / 3) * rng.uniform(0.01, 3.0, 10)
+    gab = np.sqrt(gaa * gbb) * 0.3
+    xs = lambda r: -1.5 * (3 / (4 * np.pi)) ** (1 / 3) * r ** (4 / 3)
+    z = np.zeros_like(ra)
+
+    def pw92(a, b):
+        return O.functionals("PBE", 2, np.stack([a, b], 1), np.zeros((len(a), 3)))[0] - xs(a) - xs(b)
+
+    eaa, ebb = pw92(ra, z), pw92(rb, z)
+    eab = pw92(ra, rb) - eaa - ebb
+    saa, sbb = gaa / ra ** (8 / 3), gbb / rb ** (8 / 3)
+    want = (xs(ra) * g(cx, 0.004 * saa) + xs(rb) * g(cx, 0.004 * sbb) + eaa * g(css, 0.2 * saa)
+            + ebb * g(css, 0.2 * sbb) + eab * g(cab, 0.006 * 0.5 * (saa + sbb)))
+    got = O.functionals(xc, 2, np.stack([ra, rb], 1), np.stack([gaa, gbb, gab], 1))[0]
+    np.testing.assert_allclose(got, want, rtol=1e-11)
+    # zero gradient: c_0 times each LDA piece
+    got0 = O.functionals(xc, 2, np.stack([ra, rb], 1), np.zeros((10, 3)))[0]
+    np.testing.assert_allclose(got0, cx[0] * (xs(ra) + xs(rb)) + css[0] * (eaa + ebb) + cab[0] * eab, rtol=1e-11)
