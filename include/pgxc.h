@@ -16,7 +16,8 @@
  *     function (modules/orbitalprojection_module.f90:30-45), radial functions
  *     = N_uncontracted primitives first, then contractions
  *     (modules/orbital_module.f90:1899-1930);
- *   - C1 only (one irrep, one partner); ispin 1 or 2.
+ *   - pgxc_build: C1 (one irrep, one partner); pgxc_build_sym: any irreps
+ *     and partners; ispin 1 or 2.
  *
  * Error convention: every entry returns PGXC_OK (0) or a negative PGXC_E*
  * code; nothing aborts and no C++ exception crosses the ABI.  There is no CPU
@@ -258,6 +259,54 @@ int pgxc_build_device(pgxc_ctx* ctx, const double* d_C, const double* d_occ,
                       int32_t nbas, int32_t nocc, int32_t ispin,
                       double* d_ham_xc_arr, int64_t xc_length,
                       double* d_exc_nel, pgxc_timings* timings);
+
+/*
+ * Symmetry-adapted bases (n_irrep >= 1 irreps, partners >= 1 each), as the
+ * reference's orbitals per irrep and partner (orbs_ob(i)%o(:,:,partner),
+ * orbital_module.f90:2421-2619, from the symadapt coefficients of
+ * unique_atom_module.f90).  Symmetry-adapted function fn of irrep i and
+ * partner p is sum over entries e with (irrep, partner, fn) = (i, p, fn) of
+ * coef[e] * chi_ao[e], chi the context's C1 basis functions (all atoms,
+ * equal atoms expanded).  Indices are 0-based; repeated entries add up.
+ */
+typedef struct pgxc_symmetry {
+  int32_t n_irrep;
+  const int32_t* dims;       /* [n_irrep] functions of each irrep (per partner) */
+  const int32_t* partners;   /* [n_irrep] */
+  int64_t nnz;
+  const int32_t* irrep;      /* [nnz] */
+  const int32_t* partner;    /* [nnz] */
+  const int32_t* fn;         /* [nnz] function within its irrep */
+  const int32_t* ao;         /* [nnz] C1 basis function */
+  const double* coef;        /* [nnz] */
+} pgxc_symmetry;
+
+/* Attach (or replace) the symmetry adaptation of a context. */
+int pgxc_set_symmetry(pgxc_ctx* ctx, const pgxc_symmetry* sym);
+
+/* ispin * sum_i dims_i (dims_i + 1) / 2: the ham_xc_arr length of pgxc_build_sym. */
+int pgxc_sym_xc_length(const pgxc_ctx* ctx, int64_t* xc_length);
+
+/*
+ * One XC build in the symmetry-adapted basis; replaces calc_xcks
+ * (modules/xc_hamiltonian.f90:812-1036) and calc_xcks_nl (:1280-1580) for
+ * any n_irrep and partners.
+ *   C[i]   : eigvec_occ(i)%m(dims_i, nocc[i], ispin), column-major
+ *   occ[i] : occ_num_occ(i)%m(nocc[i], ispin); the density weights each
+ *            partner by occ / partners_i (density_calc_nl, :1534-1538)
+ *   ham_xc_arr : per spin s, the irreps' packed triangles one after the other
+ *            with spin stride ispin, element (k,j), k<=j, of irrep i at
+ *            ham_xc_arr[s + ispin*(off_i + j*(j+1)/2 + k)], off_i = sum_{i'<i}
+ *            dims_i'(dims_i'+1)/2; V_i = 1/partners_i sum_p phi_p^T v phi_p,
+ *            ACCUMULATED (+=) as tristore and :1559-1566 do.
+ *   exc, nel : added to, as by pgxc_build.
+ * The grid may be the reference's symmetry-reduced one (weights times the
+ * number of equal atoms): the build integrates exactly the sums it does.
+ */
+int pgxc_build_sym(pgxc_ctx* ctx, const double* const* C, const double* const* occ,
+                   const int32_t* nocc, int32_t ispin,
+                   double* ham_xc_arr, int64_t xc_length,
+                   double* exc, double* nel, pgxc_timings* timings);
 
 /*
  * Batched builds of many small systems (a set of molecules, each with its own

@@ -48,6 +48,9 @@ def lib():
     L.oracle_xc_build.argtypes = [P(abi.Geometry), P(abi.Basis), P(abi.Grid), ct.c_int32, ct.c_int32,
                                   abi._f64p, abi._f64p, ct.c_int32, ct.c_int32, abi._f64p, ct.c_int64,
                                   abi._f64p, abi._f64p, ct.c_int32, ct.c_int32, ct.c_int64, ct.c_int64]
+    L.oracle_xc_build_sym.argtypes = [P(abi.Geometry), P(abi.Basis), P(abi.Grid), ct.c_int32, ct.c_int32,
+                                      P(abi.Symmetry), P(abi._f64p), P(abi._f64p), abi._i32p, abi._f64p, ct.c_int64,
+                                      P(ct.c_double), P(ct.c_double), ct.c_int32]
     L.oracle_overlap.argtypes = [P(abi.Geometry), P(abi.Basis), P(abi.Grid), abi._f64p, ct.c_int32]
     blas = _openblas_path()
     if blas:
@@ -123,6 +126,23 @@ def xc_build(case, vla=128, nthreads=0, pt_range=None):
                                abi.XC_IDS[case.functional], case.ispin, abi.f64p(C), abi.f64p(occ), case.nbas,
                                case.nocc, abi.f64p(ham), case.xc_length, ct.byref(exc), ct.byref(nel), vla,
                                nthreads, lo, hi)
+    assert st == 0, st
+    return ham, exc.value, nel.value
+
+
+def xc_build_sym(case, ad, Cs, occs, nthreads=0):
+    """Symmetry-adapted build (pgxc.symmetry.Adaptation, per-irrep C and occ);
+    returns (ham_xc_arr, exc, nel)."""
+    assert case.grid_w is not None
+    m = abi.Marshalled(case)
+    sy = abi.MarshalledSymmetry(ad)
+    o = abi.IrrepOrbitals(Cs, occs)
+    ham = np.zeros(ad.xc_length(case.ispin))
+    exc = ct.c_double(0.0)
+    nel = ct.c_double(0.0)
+    st = lib().oracle_xc_build_sym(ct.byref(m.geometry), ct.byref(m.basis), ct.byref(m.grid),
+                                   abi.XC_IDS[case.functional], case.ispin, ct.byref(sy.s), o.pC, o.pocc,
+                                   abi.i32p(o.nocc), abi.f64p(ham), len(ham), ct.byref(exc), ct.byref(nel), nthreads)
     assert st == 0, st
     return ham, exc.value, nel.value
 

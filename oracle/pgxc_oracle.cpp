@@ -1214,6 +1214,201 @@ int oracle_xc_build(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_
   return PGXC_OK;
 }
 
+// One XC build in a symmetry-adapted basis over the whole grid, restating the
+// irrep and partner loops of the reference: the orbitals of irrep i, partner
+// p evaluated as phi_ip = chi U_ip (orbs_ob(i)%o(:,:,p), orbital_module.f90
+// :2421-2619), the density with occ / partners (density_calc_nl,
+// density_calc_module.f90:1480-1545), ham_i = 1/np sum_p help_p^T phi_p and
+// the irreps' triangles packed one after the other per spin (calc_xcks
+// integrate / tristore, xc_hamiltonian.f90:951-1034; calc_xcks_nl
+// :1455-1566).  U is taken from the same entry lists as pgxc_set_symmetry.
+// Outputs are ACCUMULATED into ham_xc_arr, *exc, *nel.
+int oracle_xc_build_sym(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid* grid, int32_t xc,
+                        int32_t ispin, const pgxc_symmetry* sym, const double* const* C, const double* const* occ,
+                        const int32_t* nocc, double* ham_xc_arr, int64_t xc_length, double* exc, double* nel,
+                        int32_t nthreads) {
+  Basis B;
+  int st = make_basis(geo, bas, B);
+  if (st) return st;
+  const int64_t nb = B.nbas;
+  const int nirr = sym->n_irrep;
+  if (nirr < 1 || (ispin != 1 && ispin != 2) || xc < PGXC_XC_VWN || xc > PGXC_XC_LAST || grid->weights_are_raw)
+    return PGXC_EINVAL;
+  std::vector<int64_t> uofs(nirr), hofs(nirr);
+  int64_t ulen = 0, hlen = 0, plen = 0;
+  for (int i = 0; i < nirr; ++i) {
+    uofs[i] = ulen;
+    hofs[i] = hlen;
+    ulen += (int64_t)sym->partners[i] * nb * sym->dims[i];
+    hlen += (int64_t)sym->dims[i] * sym->dims[i];
+    plen += (int64_t)sym->dims[i] * (sym->dims[i] + 1) / 2;
+  }
+  if (xc_length != ispin * plen) return PGXC_EINVAL;
+  // dense U_ip (nb x dims_i) per irrep and partner
+  std::vector<double> U((size_t)ulen, 0.0);
+  for (int64_t e = 0; e < sym->nnz; ++e) {
+    const int i = sym->irrep[e], p = sym->partner[e], f = sym->fn[e], a = sym->ao[e];
+    if (i < 0 || i >= nirr || p < 0 || p >= sym->partners[i] || f < 0 || f >= sym->dims[i] || a < 0 || a >= nb)
+      return PGXC_EINVAL;
+    U[uofs[i] + (size_t)p * nb * sym->dims[i] + a + (size_t)nb * f] += sym->coef[e];
+  }
+  const int vla = 128;
+  const int64_t npts = grid->npts;
+  const double* gx = grid->grdpts;
+  const double* gy = gx + npts;
+  const double* gz = gy + npts;
+  const double* gw = gz + npts;
+  const bool gga = PGXC_XC_IS_GGA(xc);
+  const int64_t nbatch = (npts + vla - 1) / vla;
+  int dmax = 1, omax = 1;
+  for (int i = 0; i < nirr; ++i) {
+    dmax = std::max(dmax, (int)sym->dims[i]);
+    omax = std::max(omax, (int)nocc[i]);
+  }
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+  const int nth = omp_get_max_threads();
+#else
+  const int nth = 1;
+#endif
+  std::vector<ThreadWork> tw(nth);
+#ifdef _OPENMP
+#pragma omp parallel
+#endif
+  {
+#ifdef _OPENMP
+    ThreadWork& W = tw[omp_get_thread_num()];
+#else
+    ThreadWork& W = tw[0];
+#endif
+    W.ham.assign((size_t)ispin * hlen, 0.0);
+    W.phi.assign((size_t)vla * nb, 0.0);
+    if (gga) W.grads.assign((size_t)vla * 3 * nb, 0.0);
+    std::vector<double> sp((size_t)vla * dmax), sg((size_t)vla * 3 * dmax);
+    W.phiocc.assign((size_t)vla * omax, 0.0);
+    W.graphi.assign((size_t)vla * 3 * omax, 0.0);
+    W.help.assign((size_t)vla * dmax, 0.0);
+    std::vector<double> rho(2 * vla), grarho(6 * vla), gam(3 * vla), fxc(vla), fr(2 * vla), fg(3 * vla);
+    std::vector<double> Asc(2 * vla), Bv(6 * vla);
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 4)
+#endif
+    for (int64_t ib = 0; ib < nbatch; ++ib) {
+      const int64_t lo = ib * vla;
+      const int vl = (int)std::min<int64_t>(vla, npts - lo);
+      eval_basis(B, vl, gx + lo, gy + lo, gz + lo, W.phi.data(), gga ? W.grads.data() : nullptr, W.sh, W.rad0,
+                 W.rad1, W.prim0, W.prim1);
+      std::fill(rho.begin(), rho.end(), 0.0);
+      std::fill(grarho.begin(), grarho.end(), 0.0);
+      // density_calc_nl over irreps and partners
+      for (int i = 0; i < nirr; ++i) {
+        const int d = sym->dims[i], no = nocc[i], np = sym->partners[i];
+        if (d == 0 || no == 0) continue;
+        for (int p = 0; p < np; ++p) {
+          const double* Ui = U.data() + uofs[i] + (size_t)p * nb * d;
+          dgemm('n', 'n', vl, d, nb, 1.0, W.phi.data(), vl, Ui, nb, 0.0, sp.data(), vl);
+          if (gga) dgemm('n', 'n', 3 * vl, d, nb, 1.0, W.grads.data(), 3 * vl, Ui, nb, 0.0, sg.data(), 3 * vl);
+          for (int s = 0; s < ispin; ++s) {
+            const double* Cs = C[i] + (size_t)s * d * no;
+            dgemm('n', 'n', vl, no, d, 1.0, sp.data(), vl, Cs, d, 0.0, W.phiocc.data(), vl);
+            if (gga) dgemm('n', 'n', 3 * vl, no, d, 1.0, sg.data(), 3 * vl, Cs, d, 0.0, W.graphi.data(), 3 * vl);
+            for (int j = 0; j < no; ++j) {
+              const double o = occ[i][j + (size_t)no * s] / np;
+              const double* pj = W.phiocc.data() + (size_t)j * vl;
+              for (int k = 0; k < vl; ++k) rho[k + vla * s] += pj[k] * pj[k] * o;
+              if (gga) {
+                const double* gj = W.graphi.data() + (size_t)j * 3 * vl;
+                for (int c = 0; c < 3; ++c)
+                  for (int k = 0; k < vl; ++k) grarho[k + vla * (c + 3 * s)] += 2 * pj[k] * gj[c * vl + k] * o;
+              }
+            }
+          }
+        }
+      }
+      for (int k = 0; k < vl; ++k) {
+        if (!gga) break;
+        if (ispin == 1) {
+          gam[k] = grarho[k] * grarho[k] + grarho[k + vla] * grarho[k + vla] + grarho[k + 2 * vla] * grarho[k + 2 * vla];
+        } else {
+          double s0 = 0, s1 = 0, s2 = 0;
+          for (int c = 0; c < 3; ++c) {
+            const double a = grarho[k + vla * c], b = grarho[k + vla * (c + 3)];
+            s0 += a * a; s1 += b * b; s2 += a * b;
+          }
+          gam[k] = s0; gam[k + vla] = s1; gam[k + 2 * vla] = s2;
+        }
+      }
+      for (int s = 0; s < ispin; ++s)
+        for (int k = 0; k < vl; ++k) W.nel += rho[k + vla * s] * gw[lo + k];
+      for (int k = 0; k < vl; ++k) {
+        double r[2] = {rho[k], ispin == 2 ? rho[k + vla] : 0.0};
+        double g[3] = {gam[k], gam[k + vla], gam[k + 2 * vla]};
+        double F, Fr[2], Fg[3];
+        functional_point(xc, ispin, r, g, F, Fr, Fg);
+        fxc[k] = F;
+        fr[k] = Fr[0]; fr[k + vla] = Fr[1];
+        fg[k] = Fg[0]; fg[k + vla] = Fg[1]; fg[k + 2 * vla] = Fg[2];
+        W.exc += F * gw[lo + k];
+      }
+      // A and B per spin (:1429-1446), or w dfdrho (:955-957)
+      for (int s = 0; s < ispin; ++s)
+        for (int k = 0; k < vl; ++k) {
+          const double w = gw[lo + k];
+          Asc[k + vla * s] = gga ? 0.5 * fr[k + vla * s] * w : fr[k + vla * s] * w;
+          if (!gga) continue;
+          for (int c = 0; c < 3; ++c)
+            Bv[k + vla * (c + 3 * s)] = ispin == 1 ? w * 2.0 * fg[k] * grarho[k + vla * c]
+                                                   : w * (2.0 * fg[k + vla * s] * grarho[k + vla * (c + 3 * s)] +
+                                                          fg[k + 2 * vla] * grarho[k + vla * (c + 3 * (1 - s))]);
+        }
+      // integrate per irrep and partner
+      for (int i = 0; i < nirr; ++i) {
+        const int d = sym->dims[i], np = sym->partners[i];
+        if (d == 0) continue;
+        for (int p = 0; p < np; ++p) {
+          const double* Ui = U.data() + uofs[i] + (size_t)p * nb * d;
+          dgemm('n', 'n', vl, d, nb, 1.0, W.phi.data(), vl, Ui, nb, 0.0, sp.data(), vl);
+          if (gga) dgemm('n', 'n', 3 * vl, d, nb, 1.0, W.grads.data(), 3 * vl, Ui, nb, 0.0, sg.data(), 3 * vl);
+          for (int s = 0; s < ispin; ++s) {
+            for (int f = 0; f < d; ++f)
+              for (int k = 0; k < vl; ++k) {
+                double h = Asc[k + vla * s] * sp[(size_t)f * vl + k];
+                if (gga)
+                  for (int c = 0; c < 3; ++c) h += Bv[k + vla * (c + 3 * s)] * sg[(size_t)f * 3 * vl + c * vl + k];
+                W.help[(size_t)f * vl + k] = h;
+              }
+            double* ham = W.ham.data() + (size_t)s * hlen + hofs[i];
+            dgemm('t', 'n', d, d, vl, 1.0 / np, W.help.data(), vl, sp.data(), vl, 1.0, ham, d);
+          }
+        }
+      }
+    }
+  }
+  std::vector<double> ham((size_t)ispin * hlen, 0.0);
+  double e = 0.0, q = 0.0;
+  for (int t = 0; t < nth; ++t) {
+    if (tw[t].ham.empty()) continue;
+    for (size_t k = 0; k < ham.size(); ++k) ham[k] += tw[t].ham[k];
+    e += tw[t].exc;
+    q += tw[t].nel;
+  }
+  for (int s = 0; s < ispin; ++s) {
+    int64_t counter = s;
+    for (int i = 0; i < nirr; ++i) {
+      const int64_t d = sym->dims[i];
+      const double* h = ham.data() + (size_t)s * hlen + hofs[i];
+      for (int64_t j = 0; j < d; ++j)
+        for (int64_t k = 0; k <= j; ++k) {
+          ham_xc_arr[counter] += gga ? (h[j + d * k] + h[k + d * j]) : h[k + d * j];
+          counter += ispin;
+        }
+    }
+  }
+  *exc += e;
+  *nel += q;
+  return PGXC_OK;
+}
+
 // S(nbas,nbas) = sum_g w phi phi^T over the weighted grid (for tests).
 int oracle_overlap(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid* grid, double* S,
                    int32_t nthreads) {

@@ -18,8 +18,25 @@
 #include "mixed.h"
 #include "pgxc_common.cuh"
 #include "screened.h"
+#include "symmetry.h"
 
 using namespace pgxc;
+
+// Symmetry adaptation of a context (pgxc_set_symmetry): the device tables and
+// the host sizes a symmetric build needs.
+struct SymPlan {
+  SymDev dev;
+  std::vector<int> dims, partners, ipbase;
+  std::vector<int64_t> pkofs;
+  int nip = 0, max_dim = 0;
+  int64_t len = 0;                 // sum_i dims_i (dims_i + 1) / 2
+  double* d_ham = nullptr;         // ispin * len packed symmetric matrix
+  double* d_Csa = nullptr;         // the irreps' orbitals of one build
+  int64_t csa_cap = 0;
+  int64_t* d_cofs = nullptr;       // [ispin * n_irrep]
+  int* d_nocc = nullptr;           // [n_irrep]
+  int64_t* d_col0 = nullptr;       // [nip]
+};
 
 struct pgxc_ctx {
   int device = 0;
@@ -48,6 +65,7 @@ struct pgxc_ctx {
   double* h_acc = nullptr;      // pinned {E, cE, N, cN}
   MixedState* mixed = nullptr;  // tensor-core mixed-precision path (dense)
   ScreenPlan* screen = nullptr; // screened (tile-sparse) build, when screen_threshold >= 0
+  SymPlan* sym = nullptr;       // symmetry adaptation, when set
 };
 
 namespace {
@@ -102,6 +120,15 @@ bool all_finite(const double* p, int64_t n) {
   return true;
 }
 
+// A device copy of a host vector (a context allocation).
+template <typename T>
+int upload_vec(pgxc_ctx* c, const std::vector<T>& v, T** d) {
+  int st = dalloc(c, d, v.size());
+  if (st) return st;
+  if (!v.empty()) CUDA_TRY(c, cudaMemcpy(*d, v.data(), sizeof(T) * v.size(), cudaMemcpyHostToDevice));
+  return PGXC_OK;
+}
+
 }  // namespace
 
 void pgxc::set_global_error(const std::string& msg) { g_err = msg; }
@@ -142,6 +169,7 @@ void pgxc_destroy(pgxc_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->mixed) mixed_destroy(c->mixed);
   if (c->screen) screen_destroy(c->screen);
+  delete c->sym;
   for (void* p : c->allocs) cudaFree(p);
   if (c->h_ham) cudaFreeHost(c->h_ham);
   if (c->h_acc) cudaFreeHost(c->h_acc);
@@ -736,6 +764,234 @@ int pgxc_build_device(pgxc_ctx* c, const double* d_C, const double* d_occ, int32
   if (tm) {
     *tm = local;
     tm->total_ms = tot;
+  }
+  return PGXC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Symmetry-adapted builds (n_irrep >= 1, partners >= 1): the irreps' orbitals
+// are expanded into the C1 basis on the device, the C1 build runs on them,
+// and the C1 potential is projected onto each irrep (symmetry.h).
+// ---------------------------------------------------------------------------
+
+int pgxc_set_symmetry(pgxc_ctx* c, const pgxc_symmetry* y) {
+  if (!c) return set_err(nullptr, PGXC_EINVAL, "ctx is NULL");
+  if (!y || y->n_irrep < 1 || !y->dims || !y->partners || y->nnz < 0 ||
+      (y->nnz > 0 && (!y->irrep || !y->partner || !y->fn || !y->ao || !y->coef)))
+    return set_err(c, PGXC_EINVAL, "symmetry: n_irrep >= 1, dims, partners and the nnz entries are required");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  const int n = y->n_irrep;
+  SymPlan* P = new (std::nothrow) SymPlan;
+  if (!P) return set_err(c, PGXC_ENOMEM, "host allocation failed");
+  P->dims.assign(y->dims, y->dims + n);
+  P->partners.assign(y->partners, y->partners + n);
+  P->ipbase.resize(n);
+  P->pkofs.resize(n);
+  std::vector<int> ip_irrep;
+  std::vector<int64_t> colbase;
+  int64_t ncol = 0;
+  for (int i = 0; i < n; ++i) {
+    const int d = P->dims[i], np = P->partners[i];
+    if (d < 0 || np < 1) {
+      delete P;
+      return set_err(c, PGXC_EINVAL, "symmetry: dims >= 0 and partners >= 1 required");
+    }
+    P->ipbase[i] = P->nip;
+    P->pkofs[i] = P->len;
+    P->len += (int64_t)d * (d + 1) / 2;
+    P->max_dim = std::max(P->max_dim, d);
+    for (int p = 0; p < np; ++p) {
+      ip_irrep.push_back(i);
+      colbase.push_back(ncol);
+      ncol += d;
+    }
+    P->nip += np;
+  }
+  struct E { int ip, fn, ao; double coef; };
+  std::vector<E> ent((size_t)y->nnz);
+  for (int64_t e = 0; e < y->nnz; ++e) {
+    const int i = y->irrep[e], p = y->partner[e], f = y->fn[e], a = y->ao[e];
+    if (i < 0 || i >= n || p < 0 || p >= P->partners[i] || f < 0 || f >= P->dims[i] || a < 0 || a >= c->nbas ||
+        !std::isfinite(y->coef[e])) {
+      delete P;
+      return set_err(c, y->coef && !std::isfinite(y->coef[e]) ? PGXC_ENONFINITE : PGXC_EINVAL,
+                     "symmetry: entry " + std::to_string(e) + " out of range or non-finite");
+    }
+    ent[e] = E{P->ipbase[i] + p, f, a, y->coef[e]};
+  }
+  // rows of U by (ip, C1 function): the orbital gather
+  std::vector<E> rows = ent;
+  std::stable_sort(rows.begin(), rows.end(), [](const E& x, const E& z) { return x.ip != z.ip ? x.ip < z.ip : x.ao < z.ao; });
+  std::vector<int> grp_ip, grp_ao, row_fn;
+  std::vector<int64_t> grp_ptr;
+  std::vector<double> row_coef;
+  for (size_t e = 0; e < rows.size(); ++e) {
+    if (e == 0 || rows[e].ip != rows[e - 1].ip || rows[e].ao != rows[e - 1].ao) {
+      grp_ip.push_back(rows[e].ip);
+      grp_ao.push_back(rows[e].ao);
+      grp_ptr.push_back((int64_t)e);
+    }
+    row_fn.push_back(rows[e].fn);
+    row_coef.push_back(rows[e].coef);
+  }
+  grp_ptr.push_back((int64_t)rows.size());
+  // columns of U by (ip, symmetry-adapted function): the potential gather
+  std::vector<int64_t> col_ptr((size_t)ncol + 1, 0);
+  for (const E& x : ent) ++col_ptr[colbase[x.ip] + x.fn + 1];
+  for (int64_t k = 0; k < ncol; ++k) col_ptr[k + 1] += col_ptr[k];
+  std::vector<int> col_ao(ent.size());
+  std::vector<double> col_coef(ent.size());
+  {
+    std::vector<int64_t> fill(col_ptr.begin(), col_ptr.end() - 1);
+    for (const E& x : ent) {
+      const int64_t k = fill[colbase[x.ip] + x.fn]++;
+      col_ao[k] = x.ao;
+      col_coef[k] = x.coef;
+    }
+  }
+  SymDev& D = P->dev;
+  int *d_dims, *d_partners, *d_ipbase, *d_ip_irrep, *d_grp_ip, *d_grp_ao, *d_row_fn, *d_col_ao;
+  int64_t *d_pkofs, *d_grp_ptr, *d_colbase, *d_col_ptr;
+  double *d_row_coef, *d_col_coef;
+  int st;
+  if ((st = upload_vec(c, P->dims, &d_dims)) || (st = upload_vec(c, P->partners, &d_partners)) ||
+      (st = upload_vec(c, P->ipbase, &d_ipbase)) || (st = upload_vec(c, P->pkofs, &d_pkofs)) ||
+      (st = upload_vec(c, ip_irrep, &d_ip_irrep)) || (st = upload_vec(c, grp_ip, &d_grp_ip)) ||
+      (st = upload_vec(c, grp_ao, &d_grp_ao)) || (st = upload_vec(c, grp_ptr, &d_grp_ptr)) ||
+      (st = upload_vec(c, row_fn, &d_row_fn)) || (st = upload_vec(c, row_coef, &d_row_coef)) ||
+      (st = upload_vec(c, colbase, &d_colbase)) || (st = upload_vec(c, col_ptr, &d_col_ptr)) ||
+      (st = upload_vec(c, col_ao, &d_col_ao)) || (st = upload_vec(c, col_coef, &d_col_coef)) ||
+      (st = dalloc(c, &P->d_ham, (size_t)c->opt.ispin * P->len)) || (st = dalloc(c, &P->d_nocc, (size_t)n)) ||
+      (st = dalloc(c, &P->d_cofs, (size_t)c->opt.ispin * n)) || (st = dalloc(c, &P->d_col0, (size_t)P->nip))) {
+    delete P;
+    return st;
+  }
+  D.n_irrep = n;
+  D.dims = d_dims;
+  D.partners = d_partners;
+  D.ipbase = d_ipbase;
+  D.pkofs = d_pkofs;
+  D.ip_irrep = d_ip_irrep;
+  D.ngroups = (int)grp_ip.size();
+  D.grp_ip = d_grp_ip;
+  D.grp_ao = d_grp_ao;
+  D.grp_ptr = d_grp_ptr;
+  D.row_fn = d_row_fn;
+  D.row_coef = d_row_coef;
+  D.colbase = d_colbase;
+  D.col_ptr = d_col_ptr;
+  D.col_ao = d_col_ao;
+  D.col_coef = d_col_coef;
+  delete c->sym;
+  c->sym = P;
+  return PGXC_OK;
+}
+
+int pgxc_sym_xc_length(const pgxc_ctx* c, int64_t* xc_length) {
+  if (!c || !xc_length) return set_err(nullptr, PGXC_EINVAL, "NULL argument");
+  if (!c->sym) return set_err(nullptr, PGXC_EINVAL, "no symmetry set on this context");
+  *xc_length = (int64_t)c->opt.ispin * c->sym->len;
+  return PGXC_OK;
+}
+
+int pgxc_build_sym(pgxc_ctx* c, const double* const* C, const double* const* occ, const int32_t* nocc, int32_t ispin,
+                   double* ham, int64_t xc_length, double* exc, double* nel, pgxc_timings* tm) {
+  if (!c) return set_err(nullptr, PGXC_EINVAL, "ctx is NULL");
+  SymPlan* P = c->sym;
+  if (!P) return set_err(c, PGXC_EINVAL, "pgxc_build_sym needs pgxc_set_symmetry first");
+  if (ispin != c->opt.ispin) return set_err(c, PGXC_EINVAL, "ispin does not match the context");
+  if (xc_length != (int64_t)ispin * P->len)
+    return set_err(c, PGXC_EINVAL, "xc_length must be ispin * sum_i dims_i (dims_i + 1) / 2");
+  if (!ham || !exc || !nel || !nocc || !C || !occ) return set_err(c, PGXC_EINVAL, "NULL output/input");
+  const int n = P->dev.n_irrep;
+  int64_t ntot = 0, csa = 0;
+  int nocc_max = 0;
+  for (int i = 0; i < n; ++i) {
+    if (nocc[i] < 0) return set_err(c, PGXC_EINVAL, "nocc < 0");
+    const int64_t m = (int64_t)P->dims[i] * nocc[i] * ispin;
+    if (nocc[i] > 0 && (!occ[i] || (m > 0 && !C[i]))) return set_err(c, PGXC_EINVAL, "NULL C or occ of an irrep");
+    if ((m > 0 && !all_finite(C[i], m)) || (nocc[i] > 0 && !all_finite(occ[i], (int64_t)nocc[i] * ispin)))
+      return set_err(c, PGXC_ENONFINITE, "non-finite C or occ");
+    ntot += (int64_t)P->partners[i] * nocc[i];
+    csa += m;
+    nocc_max = std::max(nocc_max, (int)nocc[i]);
+  }
+  if (ntot > (1 << 30)) return set_err(c, PGXC_EINVAL, "too many orbitals");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  int st;
+  if ((st = ensure_occ(c, (int)ntot))) return st;
+  if (csa > P->csa_cap) {
+    if ((st = dalloc(c, &P->d_Csa, (size_t)csa))) return st;
+    P->csa_cap = csa;
+  }
+  // host layouts: the irreps' orbitals per spin, their offsets, the C1 column
+  // of each (irrep, partner) block and the C1 occupations occ / partners
+  const int64_t kpad = round_up(std::max<int64_t>(ntot, 1), 16);
+  std::vector<double> hC((size_t)csa), hocc((size_t)ispin * kpad, 0.0);
+  std::vector<int64_t> cofs((size_t)ispin * n), col0((size_t)P->nip);
+  std::vector<int> hnocc(nocc, nocc + n);
+  int64_t o = 0;
+  for (int s = 0; s < ispin; ++s)
+    for (int i = 0; i < n; ++i) {
+      const int64_t m = (int64_t)P->dims[i] * nocc[i];
+      cofs[(size_t)s * n + i] = o;
+      if (m > 0) std::memcpy(hC.data() + o, C[i] + (size_t)s * m, sizeof(double) * m);
+      o += m;
+    }
+  int64_t col = 0;
+  for (int i = 0; i < n; ++i)
+    for (int p = 0; p < P->partners[i]; ++p) {
+      col0[P->ipbase[i] + p] = col;
+      for (int s = 0; s < ispin; ++s)
+        for (int k = 0; k < nocc[i]; ++k)
+          hocc[(size_t)s * kpad + col + k] = occ[i][k + (size_t)nocc[i] * s] / P->partners[i];
+      col += nocc[i];
+    }
+  BuildArgs& a = c->a;
+  cudaStream_t s = c->stream;
+  CUDA_TRY(c, cudaEventRecord(c->ev[0], s));
+  if (csa > 0) CUDA_TRY(c, cudaMemcpyAsync(P->d_Csa, hC.data(), sizeof(double) * csa, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(c, cudaMemcpyAsync(P->d_cofs, cofs.data(), sizeof(int64_t) * cofs.size(), cudaMemcpyHostToDevice, s));
+  CUDA_TRY(c, cudaMemcpyAsync(P->d_nocc, hnocc.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+  CUDA_TRY(c, cudaMemcpyAsync(P->d_col0, col0.data(), sizeof(int64_t) * col0.size(), cudaMemcpyHostToDevice, s));
+  for (int sp = 0; sp < ispin; ++sp) {
+    double* dC = sp ? c->C2 : a.C;
+    double* docc = sp ? c->occ2 : (double*)a.occ;
+    CUDA_TRY(c, cudaMemsetAsync(dC, 0, sizeof(double) * kpad * a.ldc, s));
+    CUDA_TRY(c, cudaMemcpyAsync(docc, hocc.data() + (size_t)sp * kpad, sizeof(double) * kpad, cudaMemcpyHostToDevice, s));
+    launch_sym_orbitals(P->dev, P->d_Csa, P->d_cofs + (size_t)sp * n, P->d_nocc, P->d_col0, nocc_max, dC, a.ldc, s);
+  }
+  CUDA_TRY(c, cudaGetLastError());
+  CUDA_TRY(c, cudaEventRecord(c->ev[1], s));
+  CUDA_TRY(c, cudaEventSynchronize(c->ev[1]));
+  float h2d = 0;
+  CUDA_TRY(c, cudaEventElapsedTime(&h2d, c->ev[0], c->ev[1]));
+  pgxc_timings local{};
+  if ((st = run_build(c, (int)ntot, &local))) return st;
+  cudaEvent_t e0 = c->ev[5], e1 = c->ev[6];
+  CUDA_TRY(c, cudaEventRecord(e0, s));
+  launch_sym_potential(P->dev, P->max_dim, ispin, c->d_ham, P->d_ham, s);
+  CUDA_TRY(c, cudaGetLastError());
+  std::vector<double> hH((size_t)xc_length);
+  if (xc_length > 0)
+    CUDA_TRY(c, cudaMemcpyAsync(hH.data(), P->d_ham, sizeof(double) * xc_length, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaMemcpyAsync(c->h_acc, a.acc, sizeof(double) * 4, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaEventRecord(e1, s));
+  CUDA_TRY(c, cudaEventSynchronize(e1));
+  float d2h = 0, tot = 0;
+  CUDA_TRY(c, cudaEventElapsedTime(&d2h, e0, e1));
+  CUDA_TRY(c, cudaEventElapsedTime(&tot, c->ev[0], e1));
+  if (!std::isfinite(c->h_acc[0]) || !std::isfinite(c->h_acc[2]))
+    return set_err(c, PGXC_ENONFINITE, "non-finite E_xc or N_el");
+  for (int64_t i = 0; i < xc_length; ++i) ham[i] += hH[i];
+  *exc += c->h_acc[0];
+  *nel += c->h_acc[2];
+  if (tm) {
+    *tm = local;
+    tm->h2d_ms = h2d;
+    tm->d2h_ms = d2h;
+    tm->total_ms = tot;
+    tm->kernel_launches += ispin + 1;
   }
   return PGXC_OK;
 }

@@ -96,6 +96,44 @@ class Options(ct.Structure):
     ]
 
 
+class Symmetry(ct.Structure):
+    _fields_ = [
+        ("n_irrep", ct.c_int32),
+        ("dims", _i32p),
+        ("partners", _i32p),
+        ("nnz", ct.c_int64),
+        ("irrep", _i32p),
+        ("partner", _i32p),
+        ("fn", _i32p),
+        ("ao", _i32p),
+        ("coef", _f64p),
+    ]
+
+
+class MarshalledSymmetry:
+    """pgxc_symmetry over an adaptation (pgxc.symmetry.Adaptation); keeps the arrays alive."""
+
+    def __init__(self, ad):
+        self.dims = np.ascontiguousarray(ad.dims, dtype=np.int32)
+        self.partners = np.ascontiguousarray(ad.partners, dtype=np.int32)
+        self.e = ad.entries()
+        self.s = Symmetry(len(self.dims), i32p(self.dims), i32p(self.partners), len(self.e[0]), i32p(self.e[0]),
+                          i32p(self.e[1]), i32p(self.e[2]), i32p(self.e[3]), f64p(self.e[4]))
+
+
+class IrrepOrbitals:
+    """Per-irrep C (dims, nocc, ispin) and occ (nocc, ispin) as the Fortran
+    arrays, with the pointer arrays of pgxc_build_sym."""
+
+    def __init__(self, Cs, occs):
+        self.C = [np.ascontiguousarray(np.asarray(C, dtype=np.float64).transpose(2, 1, 0)).reshape(-1) for C in Cs]
+        self.occ = [np.ascontiguousarray(np.asarray(o, dtype=np.float64).T).reshape(-1) for o in occs]
+        self.nocc = np.array([np.asarray(o).shape[0] for o in occs], dtype=np.int32)
+        n = len(Cs)
+        self.pC = (_f64p * n)(*[f64p(c) for c in self.C])
+        self.pocc = (_f64p * n)(*[f64p(o) for o in self.occ])
+
+
 class Timings(ct.Structure):
     _fields_ = [
         ("h2d_ms", ct.c_double),

@@ -54,6 +54,10 @@ def lib():
     L.pgxc_batch_run.argtypes = [vp, P(ct.c_double)]
     L.pgxc_batch_destroy.argtypes = [vp]
     L.pgxc_batch_stats.argtypes = [vp, P(ct.c_int64), P(ct.c_int64)]
+    L.pgxc_set_symmetry.argtypes = [vp, P(abi.Symmetry)]
+    L.pgxc_sym_xc_length.argtypes = [vp, P(ct.c_int64)]
+    L.pgxc_build_sym.argtypes = [vp, P(abi._f64p), P(abi._f64p), abi._i32p, ct.c_int32, abi._f64p, ct.c_int64,
+                                 P(ct.c_double), P(ct.c_double), P(abi.Timings)]
     _LIB = L
     return L
 
@@ -105,6 +109,30 @@ class Context:
         st = lib().pgxc_build(self.h, abi.f64p(Cf), abi.f64p(of), c.nbas, c.nocc, c.ispin, abi.f64p(ham),
                               c.xc_length, ct.byref(exc), ct.byref(nel), ct.byref(tm))
         _check(st, self.h)
+        if timings:
+            return ham, exc.value, nel.value, tm.as_dict()
+        return ham, exc.value, nel.value
+
+    def set_symmetry(self, ad):
+        """Attach a symmetry adaptation (pgxc.symmetry.Adaptation)."""
+        self._sym = abi.MarshalledSymmetry(ad)
+        _check(lib().pgxc_set_symmetry(self.h, ct.byref(self._sym.s)), self.h)
+        n = ct.c_int64()
+        _check(lib().pgxc_sym_xc_length(self.h, ct.byref(n)), self.h)
+        self.sym_xc_length = n.value
+
+    def build_sym(self, Cs, occs, ham=None, timings=False):
+        """Symmetry-adapted build from per-irrep C (dims, nocc, ispin) and occ
+        (nocc, ispin); returns (ham_xc_arr, exc, nel[, timings])."""
+        o = abi.IrrepOrbitals(Cs, occs)
+        n = getattr(self, "sym_xc_length", 0)   # 0 before set_symmetry: the library reports the error
+        if ham is None:
+            ham = np.zeros(n)
+        exc = ct.c_double(0.0)
+        nel = ct.c_double(0.0)
+        tm = abi.Timings()
+        _check(lib().pgxc_build_sym(self.h, o.pC, o.pocc, abi.i32p(o.nocc), self.case.ispin, abi.f64p(ham),
+                                    n, ct.byref(exc), ct.byref(nel), ct.byref(tm)), self.h)
         if timings:
             return ham, exc.value, nel.value, tm.as_dict()
         return ham, exc.value, nel.value
