@@ -87,10 +87,23 @@ extern "C" {
 #define PGXC_XC_HCTH120 17
 #define PGXC_XC_HCTH147 18
 #define PGXC_XC_HCTH407 19
+/* NRECMV92: Slater + the non-relativistic Engel-Chevary-Macdonald-Vosko
+ * exchange enhancement (a 2/2 Pade in s^2, g_ecmv92), no correlation
+ * (keyword "NRECMV92", modules/xc_cntrl.f90:638-643) */
+#define PGXC_XC_NRECMV92 20
+/* PWLDA: Slater + PW92 correlation, an LDA (keywords "PWLDA", "PW-LDA",
+ * "PWLSD", "PW-LSD", modules/xc_cntrl.f90:467-475) */
+#define PGXC_XC_PWLDA 21
+/* The grid parts of the hybrids (their exact exchange is not a grid term):
+ * B3LYP = 0.80 Slater + 0.72 Becke 88 enhancement + 0.19 VWN5 + 0.81 LYP
+ * (keyword "B3LYP", modules/xc_cntrl.f90:965-985); PBE0 = 0.75 Slater + PW92 +
+ * 0.75 PBE exchange enhancement + PBE correlation ("PBE0", :996-1016) */
+#define PGXC_XC_B3LYP 22
+#define PGXC_XC_PBE0 23
 /* the largest functional id */
-#define PGXC_XC_LAST PGXC_XC_HCTH407
-/* nonzero for the GGA keywords (all but the two LDAs) */
-#define PGXC_XC_IS_GGA(id) ((id) != PGXC_XC_VWN && (id) != PGXC_XC_XALPHA)
+#define PGXC_XC_LAST PGXC_XC_PBE0
+/* nonzero for the GGA keywords (all but the three LDAs) */
+#define PGXC_XC_IS_GGA(id) ((id) != PGXC_XC_VWN && (id) != PGXC_XC_XALPHA && (id) != PGXC_XC_PWLDA)
 
 /* ---- precision modes ------------------------------------------------- */
 #define PGXC_PREC_FP64        0  /* FP64 everywhere (FP64 tensor pipe): the drop-in */

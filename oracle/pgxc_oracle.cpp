@@ -130,13 +130,16 @@ D x_lda(D rho) {
 // (xc_cntrl.f90:508-590): BP = Slater + VWN5 + B88 + P86, BPW91 = Slater +
 // PW92 + B88 + PW91c, PW91 = Slater + PW92 + PW91x + PW91c, BLYP = Slater +
 // B88 + LYP; the PBE-form keywords differ in kappa, mu and beta.
-enum { GX_PBE, GX_B88, GX_PW91, GX_PBEN, GX_VMT, GX_VT84 };
+enum { GX_PBE, GX_B88, GX_PW91, GX_PBEN, GX_VMT, GX_VT84, GX_ECMV92 };
 enum { GC_PBE, GC_P86, GC_PW91, GC_LYP, GC_NONE };
 enum { LC_VWN, LC_PW92, LC_NONE };
 struct GgaPar {
   double kappa, mu, beta_c;  // exchange kappa, mu; correlation beta (pbe_ggcc :249-270)
   int gx, gc, lc;            // exchange enhancement, gradient correlation, LDA correlation
   double alpha;              // VMT / VT84 alpha (exchange.f90:723-797)
+  // fractions of Slater, exchange enhancement, LDA and gradient correlation
+  // (frac of xc_functionals, xc_func.f90:284-305): 1 but in the hybrids
+  double fx_lda = 1.0, fx_g = 1.0, fc_lda = 1.0, fc_g = 1.0;
 };
 GgaPar gga_par(int xc) {
   const double pi = PI_EXCH;
@@ -156,6 +159,11 @@ GgaPar gga_par(int xc) {
     case PGXC_XC_VT84: return {0, mu_pbe, 0.066725, GX_VT84, GC_PBE, LC_PW92, 0.000069};
     case PGXC_XC_VMTSOL: return {0, mu_sol, 0.066725, GX_VMT, GC_PBE, LC_PW92, 0.0015532};
     case PGXC_XC_VT84SOL: return {0, mu_sol, 0.066725, GX_VT84, GC_PBE, LC_PW92, 0.000023};
+    case PGXC_XC_NRECMV92: return {0, 0, 0, GX_ECMV92, GC_NONE, LC_NONE, 0};
+    case PGXC_XC_PWLDA: return {0, 0, 0, GX_PBE, GC_NONE, LC_PW92, 0};
+    // hybrids' grid parts: "B3LYP" (xc_cntrl.f90:965-985), "PBE0" (:996-1016)
+    case PGXC_XC_B3LYP: return {0, 0, 0, GX_B88, GC_LYP, LC_VWN, 0, 0.80, 0.72, 0.19, 0.81};
+    case PGXC_XC_PBE0: return {0.804, mu_pbe, 0.066725, GX_PBE, GC_PBE, LC_PW92, 0, 0.75, 0.75, 1.0, 1.0};
     default: return {0.804, mu_pbe, 0.066725, GX_PBE, GC_PBE, LC_PW92, 0};
   }
 }
@@ -213,6 +221,14 @@ D g_vmt(double mu, double alpha, D s2, bool vt84) {
   return G + alpha * s2 * (1.0 + s2 * (-1.0 + s2 * (-alpha / 2.0 + s2 * (alpha / 2.0 + s2 * (alpha * alpha / 6.0)))));
 }
 
+// ECMV92: g_ecmv92 (exchange.f90:904-917), pade22 (:1144-1159) with
+// A = (0, 0.3402, 5.9955), B = (1, 27.5026, 5.7728) in x = s^2.
+D g_ecmv92(D s2) {
+  D nomin = 0.0 + s2 * (0.3402 + s2 * 5.9955);
+  D denom = 1.0 + s2 * (27.5026 + s2 * 5.7728);
+  return nomin / denom;
+}
+
 void x_gga_pbe(const GgaPar& P, double n, double gam, double& F, double& dFdn, double& dFdg) {
   const double pi = PI_EXCH;
   const double xalpha = -(3.0 / 4.0) * std::pow(3.0 / pi, 1.0 / 3.0);
@@ -232,6 +248,7 @@ void x_gga_pbe(const GgaPar& P, double n, double gam, double& F, double& dFdn, d
         : P.gx == GX_PBEN  ? g_pben(kappa, mu, s2)
         : P.gx == GX_VMT   ? g_vmt(mu, P.alpha, s2, false)
         : P.gx == GX_VT84  ? g_vmt(mu, P.alpha, s2, true)
+        : P.gx == GX_ECMV92 ? g_ecmv92(s2)
                            : kappa * mu * s2 / (kappa + mu * s2);
   F += ex.v * G.v;
   dFdn += ex.d[0] * G.v + ex.v * G.d[0] * s2_r;
@@ -590,20 +607,31 @@ void functional_point(int xc, int ispin, const double* rho, const double* gam,
     }
     return;
   }
+  // The pieces are summed with their fractions, as xc_functionals sums the
+  // contributions (f += frac * x, xc_func.f90:284-305).
+  double pf, pr[2], pg[3];
+  auto clear = [&]() { pf = 0.0; pr[0] = pr[1] = 0.0; pg[0] = pg[1] = pg[2] = 0.0; };
+  auto add = [&](double a) {
+    f += a * pf;
+    fr[0] += a * pr[0]; fr[1] += a * pr[1];
+    fg[0] += a * pg[0]; fg[1] += a * pg[1]; fg[2] += a * pg[2];
+  };
   // Slater exchange (exchange_lda, exchange.f90:511-565)
+  clear();
   if (ispin == 1) {
     D e = x_lda(var(0, rho[0]));
-    f += e.v; fr[0] += e.d[0];
+    pf += e.v; pr[0] += e.d[0];
   } else {
     for (int s = 0; s < 2; ++s) {
       D e = x_lda(var(0, 2.0 * rho[s]));
-      f += e.v / 2.0; fr[s] += e.d[0];
+      pf += e.v / 2.0; pr[s] += e.d[0];
     }
   }
-  // LDA correlation: VWN5 (vwn_ldac, vwnc.f90:225-297) for "VWN" and "BP",
-  // none for "XALPHA", "B88" and "BLYP" (LYP is a whole correlation), else
-  // PW92 (pw_ldac, pw_ldac_module.f90:197-312).  ec is kept for the PW91
-  // correlation.
+  add(P.fx_lda);
+  // LDA correlation: VWN5 (vwn_ldac, vwnc.f90:225-297) for "VWN", "BP" and
+  // "B3LYP", none for "XALPHA", "B88" and "BLYP" (LYP is a whole
+  // correlation), else PW92 (pw_ldac, pw_ldac_module.f90:197-312).  ec, as
+  // computed (not scaled), is kept for the PW91 correlation.
   D ec = cst(0.0);
   if (P.lc == LC_VWN) {
     if (ispin == 1) { D nn = var(0, rho[0]); ec = vwn::c_lda(0.5 * nn, 0.5 * nn); }
@@ -612,48 +640,49 @@ void functional_point(int xc, int ispin, const double* rho, const double* gam,
     if (ispin == 1) { D nn = var(0, rho[0]); ec = pw92::c_lda(0.5 * nn, 0.5 * nn); }
     else ec = pw92::c_lda(var(0, rho[0]), var(1, rho[1]));
   }
-  f += ec.v; fr[0] += ec.d[0];
-  if (ispin == 2) fr[1] += ec.d[1];
+  clear();
+  pf = ec.v; pr[0] = ec.d[0];
+  if (ispin == 2) pr[1] = ec.d[1];
+  add(P.fc_lda);
   if (!PGXC_XC_IS_GGA(xc)) return;
   // GGA exchange enhancement (exchange_gga, exchange.f90:206-292)
+  clear();
   if (ispin == 1) {
     double F = 0, Fn = 0, Fg = 0;
     x_gga_pbe(P, rho[0], gam[0], F, Fn, Fg);
-    f += F; fr[0] += Fn; fg[0] += Fg;
+    pf += F; pr[0] += Fn; pg[0] += Fg;
   } else {
     for (int s = 0; s < 2; ++s) {
       double F = 0, Fn = 0, Fg = 0;
       x_gga_pbe(P, 2.0 * rho[s], 4.0 * gam[s], F, Fn, Fg);
-      f += 0.5 * F; fr[s] += Fn; fg[s] += 2.0 * Fg;
+      pf += 0.5 * F; pr[s] += Fn; pg[s] += 2.0 * Fg;
     }
   }
-  if (P.gc == GC_NONE) return;  // "B88"
+  add(P.fx_g);
+  if (P.gc == GC_NONE) return;  // "B88", "NRECMV92"
+  clear();
   if (P.gc == GC_P86) {  // "BP": Perdew 86 correlation (xc_cntrl.f90:508-520)
-    perdew86(ispin, rho, gam, f, fr, fg);
-    return;
-  }
-  if (P.gc == GC_LYP) {
+    perdew86(ispin, rho, gam, pf, pr, pg);
+  } else if (P.gc == GC_LYP) {
     // lyp_C (lyp.f90): closed shell at ra = rb = n/2, gaa = gbb = gab = g/4,
     // returning dF/dra and the coefficient of gaa (dF/dgaa) as dF/dn, dF/dg
     double cg[3];
     if (ispin == 1) {
       const double q = 0.25 * gam[0];
       D F = lyp_corr(var(0, 0.5 * rho[0]), var(1, 0.5 * rho[0]), q, q, q, cg);
-      f += F.v; fr[0] += F.d[0]; fg[0] += cg[0];
+      pf += F.v; pr[0] += F.d[0]; pg[0] += cg[0];
     } else {
       D F = lyp_corr(var(0, rho[0]), var(1, rho[1]), gam[0], gam[1], gam[2], cg);
-      f += F.v; fr[0] += F.d[0]; fr[1] += F.d[1];
-      fg[0] += cg[0]; fg[1] += cg[1]; fg[2] += cg[2];
+      pf += F.v; pr[0] += F.d[0]; pr[1] += F.d[1];
+      pg[0] += cg[0]; pg[1] += cg[1]; pg[2] += cg[2];
     }
-    return;
-  }
-  // PBE correlation H (pbe_ggcc, pbe_ggcxc_module.f90:214-348) or PW91's
-  // (gga_correlation, gga_response_module.f90:170-275; gm floored at 1e-20 for ispin = 2)
-  if (ispin == 1) {
+  } else if (ispin == 1) {
+    // PBE correlation H (pbe_ggcc, pbe_ggcxc_module.f90:214-348) or PW91's
+    // (gga_correlation, gga_response_module.f90:170-275; gm floored at 1e-20 for ispin = 2)
     D nn = var(0, rho[0]);
     D g2 = var(1, gam[0]);
     D c = P.gc == GC_PW91 ? c_pw91(0.5 * nn, 0.5 * nn, g2, ec) : c_gga(P.beta_c, 0.5 * nn, 0.5 * nn, g2);
-    f += c.v; fr[0] += c.d[0]; fg[0] += c.d[1];
+    pf += c.v; pr[0] += c.d[0]; pg[0] += c.d[1];
   } else {
     D na = var(0, rho[0]), nb = var(1, rho[1]);
     D g2 = var(2, gam[0] + gam[1] + 2.0 * gam[2]);
@@ -664,9 +693,10 @@ void functional_point(int xc, int ispin, const double* rho, const double* gam,
     } else {
       c = c_gga(P.beta_c, na, nb, g2);
     }
-    f += c.v; fr[0] += c.d[0]; fr[1] += c.d[1];
-    fg[0] += c.d[2]; fg[1] += c.d[2]; fg[2] += 2.0 * c.d[2];
+    pf += c.v; pr[0] += c.d[0]; pr[1] += c.d[1];
+    pg[0] += c.d[2]; pg[1] += c.d[2]; pg[2] += 2.0 * c.d[2];
   }
+  add(P.fc_g);
 }
 
 // ---------------------------------------------------------------------------

@@ -22,7 +22,9 @@
 //   "BPW91" = Slater + PW92 + B88 + PW91-C, "BLYP" = Slater + B88 + LYP,
 //   "XALPHA" = Slater, "B88" = Slater + B88, "PBEN" / "VMT" / "VT84" /
 //   "VMTsol" / "VT84sol" = Slater + PW92 + their G + PBE-C, "HCTH*" = HCTH
-//   exchange + correlation alone.
+//   exchange + correlation alone, "NRECMV92" = Slater + ECMV92 G, "PWLDA" =
+//   Slater + PW92 (an LDA); the hybrids' grid parts "B3LYP" and "PBE0" weight
+//   the pieces by their fractions (the exact exchange is not a grid term).
 // Literal constants, density guards and epsilons are the reference's.
 #pragma once
 
@@ -54,6 +56,10 @@ struct XcConst {
   int xg;               // exchange enhancement G(s^2): XG_*
   int cg;               // gradient correlation: CG_*
   int lc;               // LDA correlation: LC_VWN, LC_PW92 or LC_NONE
+  // fractions of the pieces (xc_cntrl frac, applied as xc_functionals does,
+  // xc_func.f90:284-305): Slater, exchange enhancement, LDA correlation,
+  // gradient correlation; 1 except in the hybrids' grid parts
+  double fx_lda, fx_g, fc_lda, fc_g;
   // PBE correlation
   double pbe_fi;        // (0.5^(2/3)+0.5^(2/3)) * (1/2^(1/3))
   double pbe_ct;        // pi/(16 (3 pi^2)^(1/3))
@@ -89,7 +95,7 @@ constexpr double kHcth[4][3][5] = {
 // GGA pieces of a keyword.  Exchange enhancement: the PBE form (kappa, mu),
 // Becke 88, or PW91.  Correlation: PW92 + PBE H, VWN5 + Perdew 86, PW92 +
 // PW91 H0 + H1, or LYP (a whole correlation: no LDA part).
-constexpr int XG_PBE = 0, XG_B88 = 1, XG_PW91 = 2, XG_PBEN = 3, XG_VMT = 4, XG_VT84 = 5;
+constexpr int XG_PBE = 0, XG_B88 = 1, XG_PW91 = 2, XG_PBEN = 3, XG_VMT = 4, XG_VT84 = 5, XG_ECMV92 = 6;
 constexpr int CG_PBE = 0, CG_P86 = 1, CG_PW91 = 2, CG_LYP = 3, CG_NONE = 4;
 constexpr int LC_VWN = 0, LC_PW92 = 1, LC_NONE = 2;
 
@@ -119,18 +125,31 @@ __host__ inline XcConst make_xc_const(int functional = PGXC_XC_PBE) {
   c.vmt_alpha = functional == PGXC_XC_VMT ? 0.002762 : functional == PGXC_XC_VT84 ? 0.000069
                 : functional == PGXC_XC_VMTSOL ? 0.0015532 : functional == PGXC_XC_VT84SOL ? 0.000023 : 0.0;
   const int f = functional;
-  const bool b88 = f == PGXC_XC_BP86 || f == PGXC_XC_BPW91 || f == PGXC_XC_BLYP || f == PGXC_XC_B88;
+  const bool b88 =
+      f == PGXC_XC_BP86 || f == PGXC_XC_BPW91 || f == PGXC_XC_BLYP || f == PGXC_XC_B88 || f == PGXC_XC_B3LYP;
+  const bool ecmv = f == PGXC_XC_NRECMV92;
   c.xg = b88 ? XG_B88
+         : ecmv ? XG_ECMV92
          : f == PGXC_XC_PW91 ? XG_PW91
          : f == PGXC_XC_PBEN ? XG_PBEN
          : (f == PGXC_XC_VMT || f == PGXC_XC_VMTSOL) ? XG_VMT
          : (f == PGXC_XC_VT84 || f == PGXC_XC_VT84SOL) ? XG_VT84 : XG_PBE;
   c.cg = f == PGXC_XC_BP86 ? CG_P86
          : (f == PGXC_XC_PW91 || f == PGXC_XC_BPW91) ? CG_PW91
-         : f == PGXC_XC_BLYP ? CG_LYP
-         : (f == PGXC_XC_B88 || !PGXC_XC_IS_GGA(f)) ? CG_NONE : CG_PBE;
-  c.lc = (f == PGXC_XC_VWN || f == PGXC_XC_BP86) ? LC_VWN
-         : (f == PGXC_XC_XALPHA || f == PGXC_XC_B88 || f == PGXC_XC_BLYP) ? LC_NONE : LC_PW92;
+         : (f == PGXC_XC_BLYP || f == PGXC_XC_B3LYP) ? CG_LYP
+         : (f == PGXC_XC_B88 || ecmv || !PGXC_XC_IS_GGA(f)) ? CG_NONE : CG_PBE;
+  c.lc = (f == PGXC_XC_VWN || f == PGXC_XC_BP86 || f == PGXC_XC_B3LYP) ? LC_VWN
+         : (f == PGXC_XC_XALPHA || f == PGXC_XC_B88 || f == PGXC_XC_BLYP || ecmv) ? LC_NONE : LC_PW92;
+  c.fx_lda = c.fx_g = c.fc_lda = c.fc_g = 1.0;
+  if (f == PGXC_XC_B3LYP) {  // "B3LYP" (xc_cntrl.f90:965-985): 0.80 XAlpha, 0.72 B88, 0.19 VWN, 0.81 LYP
+    c.fx_lda = 0.80;
+    c.fx_g = 0.72;
+    c.fc_lda = 0.19;
+    c.fc_g = 0.81;
+  } else if (f == PGXC_XC_PBE0) {  // "PBE0" (:996-1016): 0.75 XAlpha, 0.75 PBE-X, PW92, PBE-C
+    c.fx_lda = 0.75;
+    c.fx_g = 0.75;
+  }
   c.hcth = (f >= PGXC_XC_HCTH && f <= PGXC_XC_HCTH407) ? f - PGXC_XC_HCTH + 1 : 0;
   for (int n = 0; n < 5; ++n) {
     const int v = c.hcth > 0 ? c.hcth - 1 : 0;
@@ -176,30 +195,41 @@ __device__ __forceinline__ void pw92_ecu(double rs, double& E, double& dE) {
   dE = -2.0 * a * a1 * Q2 - Q0 * dQ1 / (Q1 * (Q1 + 1.0));
 }
 
-// Slater exchange, closed shell: x_lda with rho > 0 guard.
+// Slater exchange, closed shell: x_lda with rho > 0 guard, times K.fx_lda.
 __device__ __forceinline__ void slater(const XcConst& K, double n, double& f, double& fr) {
   if (n > 0.0) {
     const double c = cbrt(n);
-    f += K.xalpha * n * c;
-    fr += (4.0 / 3.0) * K.xalpha * c;
+    f += K.fx_lda * (K.xalpha * n * c);
+    fr += K.fx_lda * ((4.0 / 3.0) * K.xalpha * c);
   }
 }
 
-// "VWN": Slater + VWN5 (c_lda at na = nb = n/2, where the spin
-// interpolation vanishes identically); "XALPHA" (K.lc == LC_NONE): Slater.
+// The LDA keywords, closed shell: "VWN" = Slater + VWN5 (c_lda at na = nb =
+// n/2, where the spin interpolation vanishes identically), "XALPHA" (K.lc ==
+// LC_NONE) = Slater, "PWLDA" (K.lc == LC_PW92) = Slater + PW92.
 __device__ __forceinline__ void xc_vwn(const XcConst& K, double n, double& f, double& fr) {
   f = 0.0;
   fr = 0.0;
   slater(K, n, f, fr);
   if (K.lc == LC_NONE) return;
+  if (K.lc == LC_PW92) {  // pw_ldac at na = nb = n/2: nn = n, frozen at 1e-30 below it
+    const bool frozen = n < 1.0e-30;
+    const double nn = frozen ? 1.0e-30 : n;
+    const double rs = K.pw_crs / cbrt(nn);
+    double E, dE;
+    pw92_ecu(rs, E, dE);
+    f += K.fc_lda * (nn * E);
+    if (!frozen) fr += K.fc_lda * (E - rs * dE / 3.0);
+    return;
+  }
   const double ap = 0.0621841 / 2.0, bp = 3.72744, cp = 12.9352, x0p = -0.10498;
   const double S = n + 1.0e-50;                 // sums = na + nb + deps
   const double X = sqrt(pow(K.vwn_fact / S, K.vwn_third));
   double e, de;
   vwn_ec(X, bp, cp, x0p, e, de);
   const double ecpara = ap * e;
-  f += ecpara * S;
-  fr += ecpara - ap * de * X / 6.0;             // dX/dn = -X/(6S)
+  f += K.fc_lda * (ecpara * S);
+  fr += K.fc_lda * (ecpara - ap * de * X / 6.0);   // dX/dn = -X/(6S)
 }
 
 // GGA exchange enhancement of the closed-shell functional e(n, g): e_x G(s^2),
@@ -254,6 +284,14 @@ __device__ __forceinline__ void pbe_x(const XcConst& K, double n, double g, doub
       G = s2 * (T1 + s2 * T2);
       Gs = T1 + 2.0 * T2 * s2;
     }
+  } else if (K.xg == XG_ECMV92) {
+    // ECMV92: the 2/2 Pade (0.3402 s^2 + 5.9955 s^4) / (1 + 27.5026 s^2 + 5.7728 s^4)
+    // (g_ecmv92 with pade22, exchange.f90:904-917, :1144-1159)
+    const double a1 = 0.3402, a2 = 5.9955, b1 = 27.5026, b2 = 5.7728;
+    const double num = s2 * (a1 + s2 * a2);
+    const double den = 1.0 + s2 * (b1 + s2 * b2);
+    G = num / den;
+    Gs = ((a1 + 2.0 * a2 * s2) * den - num * (b1 + 2.0 * b2 * s2)) / (den * den);
   } else if (K.xg == XG_PBEN) {
     // PBEN: G = kappa (1 - exp(-x)), x = mu s^2 / kappa; below x = 1e-4 its
     // series to x^5 (g_pben, exchange.f90:869-902)
@@ -292,9 +330,9 @@ __device__ __forceinline__ void pbe_x(const XcConst& K, double n, double g, doub
     G = kappa * mu * s2 / den;
     Gs = kappa * kappa * mu / (den * den);
   }
-  f += ex * G;
-  fr += exr * G + ex * Gs * s2r;
-  fg += ex * Gs * s2g;
+  f += K.fx_g * (ex * G);
+  fr += K.fx_g * (exr * G + ex * Gs * s2r);
+  fg += K.fx_g * (ex * Gs * s2g);
 }
 
 // "PBE": Slater + PW92 + PBE exchange enhancement + PBE correlation H.
@@ -313,8 +351,8 @@ __device__ __forceinline__ void xc_pbe(const XcConst& K, double n, double g, dou
     const double rs = K.pw_crs / cbrt(nn);
     double E, dE;
     pw92_ecu(rs, E, dE);
-    f += nn * E;
-    if (!frozen) fr += E - rs * dE / 3.0;
+    f += K.fc_lda * (nn * E);
+    if (!frozen) fr += K.fc_lda * (E - rs * dE / 3.0);
   }
   // PBE exchange: e_x * G(s^2), the 1 of (1+G) omitted (x_gga)
   pbe_x(K, n, g, f, fr, fg);
@@ -366,9 +404,9 @@ __device__ __forceinline__ void xc_pbe(const XcConst& K, double n, double g, dou
     const double H = ge * log(1.0 + u);
     const double dHn = ge * dun / (1.0 + u);
     const double dHg = ge * dug / (1.0 + u);
-    f += n * H;
-    fr += H + n * dHn;
-    fg += n * dHg;
+    f += K.fc_g * (n * H);
+    fr += K.fc_g * (H + n * dHn);
+    fg += K.fc_g * (n * dHg);
   }
 }
 
@@ -693,7 +731,11 @@ __device__ __forceinline__ void xc_bp86(const XcConst& K, double n, double g, do
   xc_vwn(K, n, f, fr);  // Slater + VWN5
   fg = 0.0;
   pbe_x(K, n, g, f, fr, fg);  // K.xg == XG_B88
-  perdew86(1, &n, &g, f, &fr, &fg);
+  double pf = 0.0, pr = 0.0, pg = 0.0;
+  perdew86(1, &n, &g, pf, &pr, &pg);
+  f += K.fc_g * pf;
+  fr += K.fc_g * pr;
+  fg += K.fc_g * pg;
 }
 
 // "PW91", "BPW91" (PW92 + PW91 correlation), "BLYP" (LYP) and "B88" (no
@@ -705,25 +747,30 @@ __device__ __forceinline__ void xc_gga_d3(const XcConst& K, double n, double g, 
   fg = 0.0;
   slater(K, n, f, fr);
   pbe_x(K, n, g, f, fr, fg);
+  // LDA correlation at na = nb = n/2: PW92 (pw_ldac), VWN5 (B3LYP) or none
+  const D3 nv = d3v(0, n);
+  const D3 na = 0.5 * nv, nb = 0.5 * nv;
+  D3 ec = d3c(0.0);
+  if (K.lc == LC_PW92) ec = pw92_c_lda(K, na, nb);
+  else if (K.lc == LC_VWN) ec = vwn_c_lda(K, na, nb);
+  f += K.fc_lda * ec.v;
+  fr += K.fc_lda * ec.d[0];
   if (K.cg == CG_PW91) {
     // gga_correlation (gga_response_module.f90:170-275): na = nb = n/2, the
-    // LDA energy of pw_ldac
-    const D3 nv = d3v(0, n);
-    const D3 na = 0.5 * nv, nb = 0.5 * nv;
-    const D3 ec = pw92_c_lda(K, na, nb);
+    // (unscaled) LDA energy of pw_ldac
     const D3 c = pw91_c_gga(K, na, nb, d3v(1, g), ec);
-    f += ec.v + c.v;
-    fr += ec.d[0] + c.d[0];
-    fg += c.d[1];
+    f += K.fc_g * c.v;
+    fr += K.fc_g * c.d[0];
+    fg += K.fc_g * c.d[1];
   } else if (K.cg == CG_LYP) {
     // lyp_C (lyp.f90): ra = rb = n/2, gaa = gbb = gab = g/4; dF/dn is dF/dra
     // and dF/dg is the coefficient of gaa alone, as the reference returns them
     const double q = 0.25 * g;
     double c3[3];
     const D3 F = lyp_corr(K, d3v(0, 0.5 * n), d3v(1, 0.5 * n), q, q, q, c3);
-    f += F.v;
-    fr += F.d[0];
-    fg += c3[0];
+    f += K.fc_g * F.v;
+    fr += K.fc_g * F.d[0];
+    fg += K.fc_g * c3[0];
   }
 }
 
@@ -740,7 +787,7 @@ __device__ __forceinline__ void xc_hcth(const XcConst& K, double n, double g, do
 // The closed-shell GGA keyword of K.
 __device__ __forceinline__ void xc_gga(const XcConst& K, double n, double g, double& f, double& fr, double& fg) {
   if (K.hcth) xc_hcth(K, n, g, f, fr, fg);
-  else if (K.cg == CG_PBE) xc_pbe(K, n, g, f, fr, fg);
+  else if (K.cg == CG_PBE && K.lc == LC_PW92) xc_pbe(K, n, g, f, fr, fg);
   else if (K.cg == CG_P86) xc_bp86(K, n, g, f, fr, fg);
   else xc_gga_d3(K, n, g, f, fr, fg);
 }
@@ -758,19 +805,27 @@ __device__ __forceinline__ void xc_open_gga(const XcConst& K, const double (&rho
     fg[s] += 2.0 * Fg;
   }
   if (K.cg == CG_NONE) return;
+  const double a = K.fc_g;
   if (K.cg == CG_P86) {
-    perdew86(2, rho, gam, f, fr, fg);
+    double pf = 0.0, pr[2] = {0.0, 0.0}, pg[3] = {0.0, 0.0, 0.0};
+    perdew86(2, rho, gam, pf, pr, pg);
+    f += a * pf;
+    fr[0] += a * pr[0];
+    fr[1] += a * pr[1];
+    fg[0] += a * pg[0];
+    fg[1] += a * pg[1];
+    fg[2] += a * pg[2];
     return;
   }
   if (K.cg == CG_LYP) {
     double c3[3];
     const D3 F = lyp_corr(K, na, nb, gam[0], gam[1], gam[2], c3);
-    f += F.v;
-    fr[0] += F.d[0];
-    fr[1] += F.d[1];
-    fg[0] += c3[0];
-    fg[1] += c3[1];
-    fg[2] += c3[2];
+    f += a * F.v;
+    fr[0] += a * F.d[0];
+    fr[1] += a * F.d[1];
+    fg[0] += a * c3[0];
+    fg[1] += a * c3[1];
+    fg[2] += a * c3[2];
     return;
   }
   // PBE or PW91 correlation H of the total gradient |grad rho_a + grad rho_b|^2
@@ -782,12 +837,12 @@ __device__ __forceinline__ void xc_open_gga(const XcConst& K, const double (&rho
   } else {
     c = pbe_c_gga(K, na, nb, g2);
   }
-  f += c.v;
-  fr[0] += c.d[0];
-  fr[1] += c.d[1];
-  fg[0] += c.d[2];
-  fg[1] += c.d[2];
-  fg[2] += 2.0 * c.d[2];
+  f += a * c.v;
+  fr[0] += a * c.d[0];
+  fr[1] += a * c.d[1];
+  fg[0] += a * c.d[2];
+  fg[1] += a * c.d[2];
+  fg[2] += a * 2.0 * c.d[2];
 }
 
 // Open-shell functional at one point: rho[2] = (rho_a, rho_b), gam[3] =
@@ -815,9 +870,9 @@ __device__ __forceinline__ void xc_open(const XcConst& K, const double (&rho)[2]
   D3 ec = d3c(0.0);
   if (K.lc == LC_VWN) ec = vwn_c_lda(K, na, nb);
   else if (K.lc == LC_PW92) ec = pw92_c_lda(K, na, nb);
-  f += ec.v;
-  fr[0] += ec.d[0];
-  fr[1] += ec.d[1];
+  f += K.fc_lda * ec.v;
+  fr[0] += K.fc_lda * ec.d[0];
+  fr[1] += K.fc_lda * ec.d[1];
   if constexpr (GGA) xc_open_gga(K, rho, gam, na, nb, ec, f, fr, fg);
 }
 

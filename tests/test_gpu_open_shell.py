@@ -137,7 +137,7 @@ BUILDS = pytest.mark.parametrize("precision,thr,tol", [("fp64", 0.0, 1e-10), ("m
 
 @BUILDS
 @pytest.mark.parametrize("xc,seed,lmax", [("VWN", 1, 2), ("PBE", 2, 2), ("PBE", 3, 3), ("VWN", 4, 3), ("BP86", 5, 2),
-                                          ("PW91", 6, 2), ("BLYP", 7, 3), ("HCTH407", 8, 2)])
+                                          ("PW91", 6, 2), ("BLYP", 7, 3), ("HCTH407", 8, 2), ("B3LYP", 9, 2)])
 def test_open_shell_build(xc, seed, lmax, precision, thr, tol):
     c = cases.small_case(functional=xc, seed=seed, lmax=lmax, natoms=5, nocc=7, ispin=2)
     O.weight_case(c)

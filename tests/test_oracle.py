@@ -19,6 +19,9 @@ GAM = np.array([1e-20, 1e-9, 1e-5, 0.02, 0.9, 10.0, 5e4])
 
 ALL_XC = list(abi.XC_IDS)
 GGA_XC = [x for x in ALL_XC if abi.is_gga(x)]
+# closed shell, LYP returns the coefficient of gamma_aa as dF/dgamma (lyp.f90):
+# not the gamma derivative of its energy
+LYP_XC = ("BLYP", "B3LYP")
 
 
 @pytest.mark.parametrize("xc", ALL_XC)
@@ -37,7 +40,7 @@ def test_functional_derivatives_fd(xc):
     np.testing.assert_allclose(fr[:, 0], num, rtol=2e-6, atol=1e-12)
     # closed-shell BLYP returns the LYP coefficient of gamma_aa as dF/dgamma,
     # as the reference does: test_lyp_published_form covers it
-    if abi.is_gga(xc) and xc != "BLYP":
+    if abi.is_gga(xc) and xc not in LYP_XC:
         hg = 1e-4 * gam
         gp, _, _ = O.functionals(xc, 1, rho, gam + hg)
         gm, _, _ = O.functionals(xc, 1, rho, gam - hg)
@@ -60,7 +63,7 @@ def test_functional_spin_consistency(xc):
     f2, fr2, fg2 = O.functionals(xc, 2, r2, g2)
     np.testing.assert_allclose(f2, f1, rtol=1e-12, atol=1e-300)
     np.testing.assert_allclose(fr2[:, 0], fr1[:, 0], rtol=1e-10, atol=1e-14)
-    if abi.is_gga(xc) and xc != "BLYP":
+    if abi.is_gga(xc) and xc not in LYP_XC:
         # d/dg_aa + d/dg_bb + d/dg_ab of g = g_aa + g_bb + 2 g_ab
         np.testing.assert_allclose((fg2[:, 0] + fg2[:, 1] + fg2[:, 2]) / 4, fg1[:, 0], rtol=1e-9, atol=1e-14)
 
@@ -170,12 +173,47 @@ def test_exchange_variants_published_form():
     want = {"PBEN": -0.804 * np.expm1(-mu * s2 / 0.804),
             "VMT": vmt(mu, 0.002762), "VT84": vt84(mu, 0.000069),
             "VMTsol": vmt(sol, 0.0015532), "VT84sol": vt84(sol, 0.000023)}
+    # NRECMV92: Slater times 1 + the ECMV92 2/2 Pade in s^2; PWLDA: Slater + PW92
+    pade = (0.3402 * s2 + 5.9955 * s2 ** 2) / (1 + 27.5026 * s2 + 5.7728 * s2 ** 2)
+    np.testing.assert_allclose(O.functionals("NRECMV92", 1, rho, gam)[0], ex * (1 + pade), rtol=1e-13)
+    z = np.zeros_like(rho)
+    for a, b in list(zip(O.functionals("PWLDA", 1, rho), O.functionals("PBE", 1, rho, z)))[:2]:  # f, df/drho
+        np.testing.assert_allclose(a, b, rtol=1e-14)
     fp = O.functionals("PBE", 1, rho, gam)[0]
     gp = 0.804 * mu * s2 / (0.804 + mu * s2)
     for xc, g in want.items():
         d = O.functionals(xc, 1, rho, gam)[0] - fp
         w = ex * (g - gp)
         assert np.all(np.abs(d - w) <= 1e-9 * np.abs(w) + 1e-13 * np.abs(fp)), (xc, d, w)
+
+
+def test_hybrid_grid_parts_are_their_fractions():
+    """B3LYP's grid part is 0.80 Slater + 0.72 B88 enhancement + 0.19 VWN5 +
+    0.81 LYP (each piece taken from keywords pinned above), PBE0's differs
+    from PBE by -0.25 (Slater + PBE exchange enhancement), the published PBE
+    exchange, spin-scaled; open shell, every output."""
+    rng = np.random.default_rng(43)
+    ra = 10 ** rng.uniform(-3, 1.5, 10)
+    rb = ra * rng.uniform(0.1, 1.0, 10)
+    gaa = ra ** (8 / 3) * rng.uniform(0.01, 3.0, 10)
+    gbb = rb ** (8 / 3) * rng.uniform(0.01, 3.0, 10)
+    gab = np.sqrt(gaa * gbb) * rng.uniform(-0.9, 0.9, 10)
+    r, g = np.stack([ra, rb], 1), np.stack([gaa, gbb, gab], 1)
+    F = lambda xc: O.functionals(xc, 2, r, g)
+    xa, b88, vwn, blyp, b3 = F("XALPHA"), F("B88"), F("VWN"), F("BLYP"), F("B3LYP")
+    for k in range(3):
+        want = 0.80 * xa[k] + 0.72 * (b88[k] - xa[k]) + 0.19 * (vwn[k] - xa[k]) + 0.81 * (blyp[k] - b88[k])
+        np.testing.assert_allclose(b3[k], want, rtol=1e-10, atol=1e-13 * np.max(np.abs(want)))
+    pi = 3.14159265358979324
+    mu = 0.066725 * pi ** 2 / 3
+
+    def x_pbe(n, gam):  # e_x (1 + G_PBE) of the closed-shell functional
+        ex = -(3 / 4) * (3 / pi) ** (1 / 3) * n ** (4 / 3)
+        s2 = gam / (4 * (3 * pi ** 2) ** (2 / 3) * n ** (8 / 3))
+        return ex * (1 + 0.804 * mu * s2 / (0.804 + mu * s2))
+
+    x = 0.5 * (x_pbe(2 * ra, 4 * gaa) + x_pbe(2 * rb, 4 * gbb))
+    np.testing.assert_allclose(F("PBE0")[0] - F("PBE")[0], -0.25 * x, rtol=1e-10)
 
 
 def _pw91_h_published(n, g, ec):
@@ -281,7 +319,7 @@ def test_basis_normalised_and_gradients(small_cases):
         np.testing.assert_allclose(gr[:, d, :], (pp - pm) / (2 * h), rtol=1e-5, atol=1e-8)
 
 
-@pytest.mark.parametrize("xc", [x for x in ALL_XC if x != "BLYP"])
+@pytest.mark.parametrize("xc", [x for x in ALL_XC if x not in LYP_XC])
 def test_dE_dC_equals_2_occ_V_C(small_cases, xc):
     if xc in small_cases:
         c = small_cases[xc]
@@ -327,7 +365,7 @@ def test_translation_invariance():
     np.testing.assert_allclose(h1, h2, atol=1e-10)
 
 
-@pytest.mark.parametrize("xc", ["BLYP", "PW91"])
+@pytest.mark.parametrize("xc", ["BLYP", "PW91", "B3LYP", "PBE0"])
 def test_open_shell_dE_dC(xc):
     """Open shell: dE_xc/dC_s = 2 occ_s V_s C_s for each spin."""
     c = cases.small_case(functional=xc, seed=37, ispin=2, nocc=5)
