@@ -100,8 +100,13 @@ extern "C" {
  * 0.75 PBE exchange enhancement + PBE correlation ("PBE0", :996-1016) */
 #define PGXC_XC_B3LYP 22
 #define PGXC_XC_PBE0 23
+/* LB94: Slater + VWN5 energy, with the van Leeuwen-Baerends correction added
+ * to the potential only, -beta rho^(1/3) x^2 / (1 + 3 beta x asinh x) per
+ * spin (keyword "LB94", modules/xc_cntrl.f90:500-506; baerends94_calc,
+ * modules/baerends_module.f90:91-134) */
+#define PGXC_XC_LB94 24
 /* the largest functional id */
-#define PGXC_XC_LAST PGXC_XC_PBE0
+#define PGXC_XC_LAST PGXC_XC_LB94
 /* nonzero for the GGA keywords (all but the three LDAs) */
 #define PGXC_XC_IS_GGA(id) ((id) != PGXC_XC_VWN && (id) != PGXC_XC_XALPHA && (id) != PGXC_XC_PWLDA)
 

@@ -130,7 +130,7 @@ D x_lda(D rho) {
 // (xc_cntrl.f90:508-590): BP = Slater + VWN5 + B88 + P86, BPW91 = Slater +
 // PW92 + B88 + PW91c, PW91 = Slater + PW92 + PW91x + PW91c, BLYP = Slater +
 // B88 + LYP; the PBE-form keywords differ in kappa, mu and beta.
-enum { GX_PBE, GX_B88, GX_PW91, GX_PBEN, GX_VMT, GX_VT84, GX_ECMV92 };
+enum { GX_PBE, GX_B88, GX_PW91, GX_PBEN, GX_VMT, GX_VT84, GX_ECMV92, GX_NONE };
 enum { GC_PBE, GC_P86, GC_PW91, GC_LYP, GC_NONE };
 enum { LC_VWN, LC_PW92, LC_NONE };
 struct GgaPar {
@@ -164,6 +164,8 @@ GgaPar gga_par(int xc) {
     // hybrids' grid parts: "B3LYP" (xc_cntrl.f90:965-985), "PBE0" (:996-1016)
     case PGXC_XC_B3LYP: return {0, 0, 0, GX_B88, GC_LYP, LC_VWN, 0, 0.80, 0.72, 0.19, 0.81};
     case PGXC_XC_PBE0: return {0.804, mu_pbe, 0.066725, GX_PBE, GC_PBE, LC_PW92, 0, 0.75, 0.75, 1.0, 1.0};
+    // "LB94" (xc_cntrl.f90:500-506): XAlpha + VWN + the baerends94 potential term
+    case PGXC_XC_LB94: return {0, 0, 0, GX_NONE, GC_NONE, LC_VWN, 0};
     default: return {0.804, mu_pbe, 0.066725, GX_PBE, GC_PBE, LC_PW92, 0};
   }
 }
@@ -230,6 +232,7 @@ D g_ecmv92(D s2) {
 }
 
 void x_gga_pbe(const GgaPar& P, double n, double gam, double& F, double& dFdn, double& dFdg) {
+  if (P.gx == GX_NONE) return;
   const double pi = PI_EXCH;
   const double xalpha = -(3.0 / 4.0) * std::pow(3.0 / pi, 1.0 / 3.0);
   D rho = var(0, n);
@@ -659,7 +662,22 @@ void functional_point(int xc, int ispin, const double* rho, const double* gam,
     }
   }
   add(P.fx_g);
-  if (P.gc == GC_NONE) return;  // "B88", "NRECMV92"
+  if (xc == PGXC_XC_LB94) {
+    // baerends94_calc (baerends_module.f90:91-134): beta is the module's
+    // default-real 0.05; arsinh(y) = log(y + sqrt(y^2 + 1)); no energy term
+    const double beta = (double)0.05f, deps = 1.0e-50, two13 = std::pow(2.0, 1.0 / 3.0);
+    auto dro = [&](double r, double g, double c) {
+      const double x = c * std::sqrt(g) / std::pow(r + deps, 4.0 / 3.0);
+      const double den = 1.0 + 3.0 * beta * x * std::log(x + std::sqrt(x * x + 1.0));
+      return beta * std::pow(r, 1.0 / 3.0) * x * x / den;
+    };
+    if (ispin == 1) fr[0] -= dro(rho[0], gam[0], two13) / two13;
+    else {
+      fr[0] -= dro(rho[0], gam[0], 1.0);
+      fr[1] -= dro(rho[1], gam[1], 1.0);
+    }
+  }
+  if (P.gc == GC_NONE) return;  // "B88", "NRECMV92", "LB94"
   clear();
   if (P.gc == GC_P86) {  // "BP": Perdew 86 correlation (xc_cntrl.f90:508-520)
     perdew86(ispin, rho, gam, pf, pr, pg);

@@ -60,6 +60,8 @@ struct XcConst {
   // xc_func.f90:284-305): Slater, exchange enhancement, LDA correlation,
   // gradient correlation; 1 except in the hybrids' grid parts
   double fx_lda, fx_g, fc_lda, fc_g;
+  int lb94;             // 1: add the LB94 potential correction ("LB94")
+  double lb94_two13;    // 2^(1/3)
   // PBE correlation
   double pbe_fi;        // (0.5^(2/3)+0.5^(2/3)) * (1/2^(1/3))
   double pbe_ct;        // pi/(16 (3 pi^2)^(1/3))
@@ -95,7 +97,7 @@ constexpr double kHcth[4][3][5] = {
 // GGA pieces of a keyword.  Exchange enhancement: the PBE form (kappa, mu),
 // Becke 88, or PW91.  Correlation: PW92 + PBE H, VWN5 + Perdew 86, PW92 +
 // PW91 H0 + H1, or LYP (a whole correlation: no LDA part).
-constexpr int XG_PBE = 0, XG_B88 = 1, XG_PW91 = 2, XG_PBEN = 3, XG_VMT = 4, XG_VT84 = 5, XG_ECMV92 = 6;
+constexpr int XG_PBE = 0, XG_B88 = 1, XG_PW91 = 2, XG_PBEN = 3, XG_VMT = 4, XG_VT84 = 5, XG_ECMV92 = 6, XG_NONE = 7;
 constexpr int CG_PBE = 0, CG_P86 = 1, CG_PW91 = 2, CG_LYP = 3, CG_NONE = 4;
 constexpr int LC_VWN = 0, LC_PW92 = 1, LC_NONE = 2;
 
@@ -141,6 +143,13 @@ __host__ inline XcConst make_xc_const(int functional = PGXC_XC_PBE) {
   c.lc = (f == PGXC_XC_VWN || f == PGXC_XC_BP86 || f == PGXC_XC_B3LYP) ? LC_VWN
          : (f == PGXC_XC_XALPHA || f == PGXC_XC_B88 || f == PGXC_XC_BLYP || ecmv) ? LC_NONE : LC_PW92;
   c.fx_lda = c.fx_g = c.fc_lda = c.fc_g = 1.0;
+  c.lb94 = f == PGXC_XC_LB94 ? 1 : 0;
+  c.lb94_two13 = std::pow(2.0, 1.0 / 3.0);
+  if (c.lb94) {  // "LB94": XAlpha + VWN + baerends94 (a potential term only)
+    c.xg = XG_NONE;
+    c.cg = CG_NONE;
+    c.lc = LC_VWN;
+  }
   if (f == PGXC_XC_B3LYP) {  // "B3LYP" (xc_cntrl.f90:965-985): 0.80 XAlpha, 0.72 B88, 0.19 VWN, 0.81 LYP
     c.fx_lda = 0.80;
     c.fx_g = 0.72;
@@ -236,6 +245,7 @@ __device__ __forceinline__ void xc_vwn(const XcConst& K, double n, double& f, do
 // the 1 of (1+G) omitted (x_gga, exchange.f90:325-439), G of the PBE form,
 // of Becke 88, PW91, PBEN, VMT or VT84; adds F, dF/dn, dF/dg.
 __device__ __forceinline__ void pbe_x(const XcConst& K, double n, double g, double& f, double& fr, double& fg) {
+  if (K.xg == XG_NONE) return;
   double ex = 0.0, exr = 0.0;
   if (n > 0.0) {
     const double c = cbrt(n);
@@ -609,6 +619,18 @@ __device__ __forceinline__ D3 lyp_corr(const XcConst& K, D3 ra, D3 rb, double ga
   return -lda1 - lda2 - caa * gaa - cbb * gbb - cab * gab;
 }
 
+// LB94 potential correction of one spin density (baerends94_calc,
+// modules/baerends_module.f90:91-134): -beta r^(1/3) x^2 / (1 + 3 beta x
+// asinh x), x = c |grad r| / (r + 1e-50)^(4/3), asinh as log(x + sqrt(x^2 + 1));
+// beta is the reference's single-precision 0.05.  Closed shell: r = n,
+// c = 2^(1/3) and the result divided by 2^(1/3); open shell: c = 1.
+__device__ __forceinline__ double lb94_dv(double r, double gam, double c) {
+  const double beta = (double)0.05f;
+  const double x = c * sqrt(gam) / pow(r + 1.0e-50, 4.0 / 3.0);
+  const double den = 1.0 + 3.0 * beta * x * log(x + sqrt(x * x + 1.0));
+  return beta * pow(r, 1.0 / 3.0) * x * x / den;
+}
+
 // HCTH power series g(s2) = sum_n c_n u^n, u = s2 / (1 + s2), and dg/ds2
 // (hcth.f90 g, in hcth_x_calc and hcth_c_calc).
 __device__ __forceinline__ void hcth_g(const double (&c)[5], double s2, double& g0, double& g1) {
@@ -772,6 +794,10 @@ __device__ __forceinline__ void xc_gga_d3(const XcConst& K, double n, double g, 
     fr += K.fc_g * F.d[0];
     fg += K.fc_g * c3[0];
   }
+  if (K.lb94) {
+    const double two13 = K.lb94_two13;
+    fr -= lb94_dv(n, g, two13) / two13;
+  }
 }
 
 // HCTH, closed shell (pg_hcth, hcth.f90): ra = rb = n/2, gaa = gbb = g/4,
@@ -803,6 +829,10 @@ __device__ __forceinline__ void xc_open_gga(const XcConst& K, const double (&rho
     f += 0.5 * F;
     fr[s] += Fn;
     fg[s] += 2.0 * Fg;
+  }
+  if (K.lb94) {
+    fr[0] -= lb94_dv(rho[0], gam[0], 1.0);
+    fr[1] -= lb94_dv(rho[1], gam[1], 1.0);
   }
   if (K.cg == CG_NONE) return;
   const double a = K.fc_g;

@@ -22,6 +22,8 @@ GGA_XC = [x for x in ALL_XC if abi.is_gga(x)]
 # closed shell, LYP returns the coefficient of gamma_aa as dF/dgamma (lyp.f90):
 # not the gamma derivative of its energy
 LYP_XC = ("BLYP", "B3LYP")
+# LB94 adds a potential without an energy: its df/drho is not dE/drho
+POTENTIAL_ONLY = ("LB94",)
 
 
 @pytest.mark.parametrize("xc", ALL_XC)
@@ -37,10 +39,11 @@ def test_functional_derivatives_fd(xc):
         return (O.functionals(xc, 1, rho + h, gam)[0] - O.functionals(xc, 1, rho - h, gam)[0]) / (2 * h)
     h = 1e-3 * rho
     num = (4 * central(h / 2) - central(h)) / 3
-    np.testing.assert_allclose(fr[:, 0], num, rtol=2e-6, atol=1e-12)
+    if xc not in POTENTIAL_ONLY:
+        np.testing.assert_allclose(fr[:, 0], num, rtol=2e-6, atol=1e-12)
     # closed-shell BLYP returns the LYP coefficient of gamma_aa as dF/dgamma,
     # as the reference does: test_lyp_published_form covers it
-    if abi.is_gga(xc) and xc not in LYP_XC:
+    if abi.is_gga(xc) and xc not in LYP_XC + POTENTIAL_ONLY:
         hg = 1e-4 * gam
         gp, _, _ = O.functionals(xc, 1, rho, gam + hg)
         gm, _, _ = O.functionals(xc, 1, rho, gam - hg)
@@ -63,7 +66,7 @@ def test_functional_spin_consistency(xc):
     f2, fr2, fg2 = O.functionals(xc, 2, r2, g2)
     np.testing.assert_allclose(f2, f1, rtol=1e-12, atol=1e-300)
     np.testing.assert_allclose(fr2[:, 0], fr1[:, 0], rtol=1e-10, atol=1e-14)
-    if abi.is_gga(xc) and xc not in LYP_XC:
+    if abi.is_gga(xc) and xc not in LYP_XC + POTENTIAL_ONLY:
         # d/dg_aa + d/dg_bb + d/dg_ab of g = g_aa + g_bb + 2 g_ab
         np.testing.assert_allclose((fg2[:, 0] + fg2[:, 1] + fg2[:, 2]) / 4, fg1[:, 0], rtol=1e-9, atol=1e-14)
 
@@ -81,6 +84,8 @@ def test_open_shell_derivatives_fd(xc):
     f, fr, fg = O.functionals(xc, 2, x[:, :2], x[:, 2:])
     ana = np.concatenate([fr, fg], 1)
     for k in range(5):
+        if xc in POTENTIAL_ONLY and k < 2:
+            continue
         h = 1e-4 * np.abs(x[:, k]) if k < 4 else 1e-4 * np.sqrt(gaa * gbb)
         xp, xm = x.copy(), x.copy()
         xp[:, k] += h
@@ -216,6 +221,28 @@ def test_hybrid_grid_parts_are_their_fractions():
     np.testing.assert_allclose(F("PBE0")[0] - F("PBE")[0], -0.25 * x, rtol=1e-10)
 
 
+def test_lb94_is_vwn_plus_a_potential():
+    """LB94: the VWN energy, and the potential of van Leeuwen and Baerends
+    added to df/drho_s: -beta rho_s^(1/3) x_s^2 / (1 + 3 beta x_s asinh x_s),
+    x_s = |grad rho_s| / rho_s^(4/3), with beta = 0.05 as the reference's
+    default-real constant (0.05 rounded to single precision)."""
+    rng = np.random.default_rng(47)
+    ra = 10 ** rng.uniform(-3, 1.5, 10)
+    rb = ra * rng.uniform(0.1, 1.0, 10)
+    gaa = ra ** (8 / 3) * rng.uniform(0.01, 3.0, 10)
+    gbb = rb ** (8 / 3) * rng.uniform(0.01, 3.0, 10)
+    r, g = np.stack([ra, rb], 1), np.stack([gaa, gbb, 0.3 * np.sqrt(gaa * gbb)], 1)
+    f, fr, fg = O.functionals("LB94", 2, r, g)
+    f0, fr0, _ = O.functionals("VWN", 2, r)
+    np.testing.assert_array_equal(f, f0)
+    assert np.all(fg == 0.0)
+    beta = float(np.float32(0.05))
+    for s, (rs, gs) in enumerate(((ra, gaa), (rb, gbb))):
+        x = np.sqrt(gs) / rs ** (4 / 3)
+        v = -beta * rs ** (1 / 3) * x * x / (1 + 3 * beta * x * np.arcsinh(x))
+        np.testing.assert_allclose(fr[:, s] - fr0[:, s], v, rtol=1e-10)
+
+
 def _pw91_h_published(n, g, ec):
     """PW91 correlation H0 + H1 for an unpolarised density (Perdew et al.,
     PRB 46, 6671, eqs. 13-16), rs and ks/kF with the reference's 1.91916."""
@@ -319,7 +346,7 @@ def test_basis_normalised_and_gradients(small_cases):
         np.testing.assert_allclose(gr[:, d, :], (pp - pm) / (2 * h), rtol=1e-5, atol=1e-8)
 
 
-@pytest.mark.parametrize("xc", [x for x in ALL_XC if x not in LYP_XC])
+@pytest.mark.parametrize("xc", [x for x in ALL_XC if x not in LYP_XC + POTENTIAL_ONLY])
 def test_dE_dC_equals_2_occ_V_C(small_cases, xc):
     if xc in small_cases:
         c = small_cases[xc]
