@@ -279,6 +279,20 @@ int pgxc_build_device(pgxc_ctx* ctx, const double* d_C, const double* d_occ,
                       double* d_exc_nel, pgxc_timings* timings);
 
 /*
+ * E_xc of several functionals on one density, as the post-SCF XC energies
+ * (post_scf_calc_xc_energy, modules/post_scf_module.f90:2204-2564, and the
+ * energy table of xc_func_get_exc, modules/xc_func.f90:1011-1200): one basis
+ * and density pass, then one functional pass per entry of functionals[n];
+ * exc[i] is overwritten with the energy of functionals[i], *nel (may be NULL)
+ * with the integrated charge.  Needs a screened context (PGXC_ENOTSUP
+ * otherwise); a GGA functional needs a context created with a GGA
+ * functional (its density gradients).  No potential is built.
+ */
+int pgxc_xc_energies(pgxc_ctx* ctx, const double* C, const double* occ,
+                     int32_t nbas, int32_t nocc, int32_t ispin,
+                     int32_t n, const int32_t* functionals, double* exc, double* nel);
+
+/*
  * Symmetry-adapted bases (n_irrep >= 1 irreps, partners >= 1 each), as the
  * reference's orbitals per irrep and partner (orbs_ob(i)%o(:,:,partner),
  * orbital_module.f90:2421-2619, from the symadapt coefficients of

@@ -66,6 +66,8 @@ struct pgxc_ctx {
   MixedState* mixed = nullptr;  // tensor-core mixed-precision path (dense)
   ScreenPlan* screen = nullptr; // screened (tile-sparse) build, when screen_threshold >= 0
   SymPlan* sym = nullptr;       // symmetry adaptation, when set
+  double* d_eacc = nullptr;     // {E, cE, N, cN} per functional of pgxc_xc_energies
+  int eacc_cap = 0;
 };
 
 namespace {
@@ -765,6 +767,75 @@ int pgxc_build_device(pgxc_ctx* c, const double* d_C, const double* d_occ, int32
     *tm = local;
     tm->total_ms = tot;
   }
+  return PGXC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Energies of several functionals on one density (post_scf_calc_xc_energy,
+// modules/post_scf_module.f90:2204-2564, with the energy table of
+// xc_func_get_exc, modules/xc_func.f90:1011-1200): one basis and density
+// pass, one functional pass per requested functional, no potential.
+// ---------------------------------------------------------------------------
+int pgxc_xc_energies(pgxc_ctx* c, const double* C, const double* occ, int32_t nbas, int32_t nocc, int32_t ispin,
+                     int32_t n, const int32_t* functionals, double* exc, double* nel) {
+  if (!c) return set_err(nullptr, PGXC_EINVAL, "ctx is NULL");
+  int st = check_build_args(c, nbas, nocc, ispin, (int64_t)ispin * nbas * (nbas + 1) / 2);
+  if (st) return st;
+  if (!c->screen) return set_err(c, PGXC_ENOTSUP, "pgxc_xc_energies needs a screened context (screen_threshold >= 0)");
+  if (n < 1 || !functionals || !exc || (nocc > 0 && (!C || !occ))) return set_err(c, PGXC_EINVAL, "NULL or empty input");
+  const bool gga = PGXC_XC_IS_GGA(c->opt.functional);
+  std::vector<XcConst> xcs((size_t)n);
+  std::vector<int> ggas((size_t)n);
+  for (int i = 0; i < n; ++i) {
+    const int f = functionals[i];
+    if (f < PGXC_XC_VWN || f > PGXC_XC_LAST) return set_err(c, PGXC_EINVAL, "functional id out of range");
+    if (PGXC_XC_IS_GGA(f) && !gga)
+      return set_err(c, PGXC_EINVAL, "a GGA energy needs a context created with a GGA functional (no grad rho)");
+    xcs[i] = make_xc_const(f);
+    ggas[i] = PGXC_XC_IS_GGA(f) ? 1 : 0;
+  }
+  if (!all_finite(C, (int64_t)nbas * nocc * ispin) || !all_finite(occ, (int64_t)nocc * ispin))
+    return set_err(c, PGXC_ENONFINITE, "non-finite C or occ");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  if ((st = ensure_occ(c, nocc))) return st;
+  if (n > c->eacc_cap) {
+    if ((st = dalloc(c, &c->d_eacc, (size_t)4 * n))) return st;
+    c->eacc_cap = n;
+  }
+  double* d_acc = c->d_eacc;
+  BuildArgs& a = c->a;
+  cudaStream_t s = c->stream;
+  const int64_t kpad = round_up(std::max(nocc, 1), 16);
+  if ((st = upload_orbitals(c, C, occ, nbas, nocc, kpad, cudaMemcpyHostToDevice))) return st;
+  CUDA_TRY(c, cudaMemsetAsync(a.acc, 0, 4 * sizeof(double), s));
+  CUDA_TRY(c, cudaMemsetAsync(d_acc, 0, 4 * sizeof(double) * n, s));
+  launch_pmat_f64(a, kpad, s);
+  if (ispin == 2) {
+    BuildArgs b = a;
+    b.C = c->C2;
+    b.occ = c->occ2;
+    b.P = c->P2;
+    launch_pmat_f64(b, kpad, s);
+  }
+  ScreenExtra x;
+  x.xc = xcs.data();
+  x.gga = ggas.data();
+  x.n = n;
+  x.acc = d_acc;
+  x.potential = false;
+  std::string e;
+  if ((st = screen_run(c->screen, a, c->P2, s, c->d_ham, nullptr, e, &x))) return set_err(c, st, e);
+  std::vector<double> h((size_t)4 * n);
+  CUDA_TRY(c, cudaMemcpyAsync(h.data(), d_acc, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, s));
+  CUDA_TRY(c, cudaStreamSynchronize(s));
+  int flag = 0;
+  if (screen_error_flag(c->screen, s, &flag) != PGXC_OK) return set_err(c, PGXC_ECUDA, "error-flag read failed");
+  if (flag) return set_err(c, PGXC_ETIMEOUT, "a bounded tensor-core pipeline wait ran out");
+  for (int i = 0; i < n; ++i) {
+    if (!std::isfinite(h[4 * i])) return set_err(c, PGXC_ENONFINITE, "non-finite E_xc");
+    exc[i] = h[4 * i];
+  }
+  if (nel) *nel = h[2];
   return PGXC_OK;
 }
 

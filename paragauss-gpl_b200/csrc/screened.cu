@@ -747,7 +747,8 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
 }
 
 int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_t st, double* ham, ScreenTimes* tm,
-               std::string& err) {
+               std::string& err, const ScreenExtra* extra) {
+  const bool potential = !extra || extra->potential;
   const bool gga = sp->gga;
   const int ispin = sp->ispin;
   const double* P[2] = {a.P, Pb};
@@ -870,7 +871,7 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
     T.launches += 2;
     if (timed) SR_TRY(cudaEventRecord(ev[6], st));
     // K4, per spin: the contraction of spin s is bracketed by ev[7 + 3s], ev[8 + 3s]
-    for (int s = 0; s < ispin; ++s) {
+    for (int s = 0; s < ispin && potential; ++s) {
       double* Vs = sp->V + s * nb2;
       cudaEvent_t k0 = timed ? ev[7 + 3 * s] : nullptr, k1 = timed ? ev[8 + 3 * s] : nullptr;
       if (sp->mixed) {
@@ -901,6 +902,20 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
         T.launches += 2;
       }
     }
+    // further functionals on the same density (after K4, whose A and B they overwrite)
+    for (int i = 0; extra && i < extra->n; ++i) {
+      if (ispin == 1) {
+        BuildArgs bx = b[0];
+        bx.w = sp->qw;
+        bx.xc = extra->xc[i];
+        bx.acc = extra->acc + 4 * i;
+        launch_functional_f64(bx, t0 * 128, npt, extra->gga[i] != 0, st);
+      } else {
+        launch_functional2_f64(extra->xc[i], sp->qw, b[0].rho, b[1].rho, cp, t0 * 128, npt, extra->gga[i] != 0,
+                               sp->partial, extra->acc + 4 * i, st);
+      }
+      T.launches += 2;
+    }
     SR_TRY(cudaGetLastError());
     if (!timed) continue;
     SR_TRY(cudaEventRecord(ev[9], st));
@@ -919,7 +934,7 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
     T.density += ms;
   }
   if (timed) SR_TRY(cudaEventRecord(ev[2], st));
-  {
+  if (potential) {
     const int64_t len = sp->nbas * (sp->nbas + 1) / 2;
     const unsigned nbk = (unsigned)std::min<int64_t>((len + 255) / 256, 148 * 8);
     for (int s = 0; s < ispin; ++s) {

@@ -59,8 +59,19 @@ void screen_destroy(ScreenPlan* sp);
 // enqueued: no event records, synchronisation or host reads, so that it can be
 // captured into a CUDA graph; screen_error_flag then reports a bounded wait
 // of the INT8 kernels that ran out.
+// Further functionals evaluated on the same density (energies only): E_xc and
+// N_el of functional i are Kahan-added into acc[4 i .. 4 i + 3] ({E, cE, N,
+// cN}, zeroed by the caller); with potential == false the potential
+// contractions and the packing are skipped and ham is not written.
+struct ScreenExtra {
+  const XcConst* xc = nullptr;   // host array of n
+  const int* gga = nullptr;      // host flags of n
+  int n = 0;
+  double* acc = nullptr;         // device, 4 n
+  bool potential = true;
+};
 int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_t st, double* ham, ScreenTimes* t,
-               std::string& err);
+               std::string& err, const ScreenExtra* extra = nullptr);
 int screen_error_flag(ScreenPlan* sp, cudaStream_t st, int* flag);
 // Plan statistics: tiles, total slots (padded), listed functions, sum of n_t^2.
 void screen_stats(const ScreenPlan* sp, int64_t* ntiles, int64_t* nslots, int64_t* nlisted, double* sum_n2,

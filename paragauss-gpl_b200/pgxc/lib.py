@@ -54,6 +54,8 @@ def lib():
     L.pgxc_batch_run.argtypes = [vp, P(ct.c_double)]
     L.pgxc_batch_destroy.argtypes = [vp]
     L.pgxc_batch_stats.argtypes = [vp, P(ct.c_int64), P(ct.c_int64)]
+    L.pgxc_xc_energies.argtypes = [vp, abi._f64p, abi._f64p, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32,
+                                   abi._i32p, abi._f64p, P(ct.c_double)]
     L.pgxc_set_symmetry.argtypes = [vp, P(abi.Symmetry)]
     L.pgxc_sym_xc_length.argtypes = [vp, P(ct.c_int64)]
     L.pgxc_build_sym.argtypes = [vp, P(abi._f64p), P(abi._f64p), abi._i32p, ct.c_int32, abi._f64p, ct.c_int64,
@@ -112,6 +114,19 @@ class Context:
         if timings:
             return ham, exc.value, nel.value, tm.as_dict()
         return ham, exc.value, nel.value
+
+    def xc_energies(self, functionals, C=None, occ=None):
+        """E_xc of each keyword in functionals on this context's density
+        (post-SCF energies); returns (list of E_xc, N_el)."""
+        c = self.case
+        Cf = c.c_fortran() if C is None else np.ascontiguousarray(C, dtype=np.float64).reshape(-1)
+        of = c.occ_fortran() if occ is None else np.ascontiguousarray(occ, dtype=np.float64).reshape(-1)
+        ids = np.array([abi.XC_IDS[f] for f in functionals], dtype=np.int32)
+        out = np.zeros(len(ids))
+        nel = ct.c_double(0.0)
+        _check(lib().pgxc_xc_energies(self.h, abi.f64p(Cf), abi.f64p(of), c.nbas, c.nocc, c.ispin, len(ids),
+                                      abi.i32p(ids), abi.f64p(out), ct.byref(nel)), self.h)
+        return list(out), nel.value
 
     def set_symmetry(self, ad):
         """Attach a symmetry adaptation (pgxc.symmetry.Adaptation)."""
