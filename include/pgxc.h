@@ -279,6 +279,21 @@ int pgxc_build_device(pgxc_ctx* ctx, const double* d_C, const double* d_occ,
                       double* d_exc_nel, pgxc_timings* timings);
 
 /*
+ * Post-SCF XC nuclear gradient: dE_xc/dR of every atom, ADDED into grad
+ * (natoms x 3: x, y, z of atom 0, then atom 1, ...), and E_xc added into *exc
+ * (may be NULL).  The grid moves with its atoms (each point with its
+ * point_atom) and the Becke weights are differentiated, so this is the
+ * derivative of the energy the builds integrate, as the reference's post-SCF
+ * gradients with weight gradients (post_scf_calc_xc_en_and_gr(_nl),
+ * modules/post_scf_module.f90:2569-3318, :3500-5193; density_calc_ph_nl,
+ * modules/density_calc_module.f90:2000-3315; becke1, modules/grid_module.f90
+ * :2499-2616).  Needs a context created with weights_are_raw (PGXC_ENOTSUP
+ * otherwise).  FP64 in every precision mode; C1 only.
+ */
+int pgxc_xc_gradient(pgxc_ctx* ctx, const double* C, const double* occ,
+                     int32_t nbas, int32_t nocc, int32_t ispin, double* grad, double* exc);
+
+/*
  * E_xc of several functionals on one density, as the post-SCF XC energies
  * (post_scf_calc_xc_energy, modules/post_scf_module.f90:2204-2564, and the
  * energy table of xc_func_get_exc, modules/xc_func.f90:1011-1200): one basis

@@ -51,6 +51,8 @@ def lib():
     L.oracle_xc_build_sym.argtypes = [P(abi.Geometry), P(abi.Basis), P(abi.Grid), ct.c_int32, ct.c_int32,
                                       P(abi.Symmetry), P(abi._f64p), P(abi._f64p), abi._i32p, abi._f64p, ct.c_int64,
                                       P(ct.c_double), P(ct.c_double), ct.c_int32]
+    L.oracle_xc_gradient.argtypes = [P(abi.Geometry), P(abi.Basis), P(abi.Grid), ct.c_int32, ct.c_int32,
+                                     abi._f64p, abi._f64p, ct.c_int32, ct.c_int32, abi._f64p, P(ct.c_double)]
     L.oracle_overlap.argtypes = [P(abi.Geometry), P(abi.Basis), P(abi.Grid), abi._f64p, ct.c_int32]
     blas = _openblas_path()
     if blas:
@@ -145,6 +147,18 @@ def xc_build_sym(case, ad, Cs, occs, nthreads=0):
                                    abi.i32p(o.nocc), abi.f64p(ham), len(ham), ct.byref(exc), ct.byref(nel), nthreads)
     assert st == 0, st
     return ham, exc.value, nel.value
+
+
+def xc_gradient(case):
+    """dE_xc/dR (natoms, 3) on the raw grid moving with its atoms, and E_xc."""
+    m = abi.Marshalled(case, weighted=False)
+    g = np.zeros(3 * len(case.coords))
+    e = ct.c_double(0.0)
+    st = lib().oracle_xc_gradient(ct.byref(m.geometry), ct.byref(m.basis), ct.byref(m.grid),
+                                  abi.XC_IDS[case.functional], case.ispin, abi.f64p(case.c_fortran()),
+                                  abi.f64p(case.occ_fortran()), case.nbas, case.nocc, abi.f64p(g), ct.byref(e))
+    assert st == 0, st
+    return g.reshape(-1, 3), e.value
 
 
 def overlap(case, nthreads=0):

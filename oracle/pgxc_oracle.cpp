@@ -965,6 +965,75 @@ struct ThreadWork {
   double exc = 0.0, nel = 0.0;
 };
 
+struct H2 {  // value, gradient and Hessian in (x, y, z)
+  double v, g[3], h[3][3];
+};
+inline H2 h2c(double a) { H2 r{}; r.v = a; return r; }
+inline H2 operator+(const H2& a, const H2& b) {
+  H2 r;
+  r.v = a.v + b.v;
+  for (int i = 0; i < 3; ++i) { r.g[i] = a.g[i] + b.g[i]; for (int j = 0; j < 3; ++j) r.h[i][j] = a.h[i][j] + b.h[i][j]; }
+  return r;
+}
+inline H2 operator-(const H2& a, const H2& b) {
+  H2 r;
+  r.v = a.v - b.v;
+  for (int i = 0; i < 3; ++i) { r.g[i] = a.g[i] - b.g[i]; for (int j = 0; j < 3; ++j) r.h[i][j] = a.h[i][j] - b.h[i][j]; }
+  return r;
+}
+inline H2 operator*(const H2& a, const H2& b) {
+  H2 r;
+  r.v = a.v * b.v;
+  for (int i = 0; i < 3; ++i) {
+    r.g[i] = a.g[i] * b.v + a.v * b.g[i];
+    for (int j = 0; j < 3; ++j) r.h[i][j] = a.h[i][j] * b.v + a.g[i] * b.g[j] + a.g[j] * b.g[i] + a.v * b.h[i][j];
+  }
+  return r;
+}
+inline H2 operator*(double s, const H2& a) {
+  H2 r;
+  r.v = s * a.v;
+  for (int i = 0; i < 3; ++i) { r.g[i] = s * a.g[i]; for (int j = 0; j < 3; ++j) r.h[i][j] = s * a.h[i][j]; }
+  return r;
+}
+inline H2 h2exp(const H2& a) {
+  const double e = std::exp(a.v);
+  H2 r;
+  r.v = e;
+  for (int i = 0; i < 3; ++i) {
+    r.g[i] = e * a.g[i];
+    for (int j = 0; j < 3; ++j) r.h[i][j] = e * (a.h[i][j] + a.g[i] * a.g[j]);
+  }
+  return r;
+}
+
+// Y_lm (l = 0..3) by the recursion of solid_harmonics_calculate
+// (solid_harmonics_module.f90:369-482), on H2: Y[l][m], m in the reference order
+void solid_harmonics_h2(const H2& x, const H2& y, const H2& z, int lmax, H2 Y[4][7]) {
+  const H2 r2 = x * x + y * y + z * z;
+  Y[0][0] = h2c(1.0);
+  if (lmax == 0) return;
+  Y[1][0] = z; Y[1][1] = x; Y[1][2] = y;
+  for (int l = 2; l <= lmax; ++l) {
+    const double lr = l, l1r = l - 1, ll1r = 2 * l - 1;
+    Y[l][0] = (1.0 / lr) * ((ll1r * z) * Y[l - 1][0] - (l1r * r2) * Y[l - 2][0]);
+    for (int im = 1; im <= l - 2; ++im) {
+      const double rlm = 1.0 / std::sqrt(lr * lr - im * im), rl1m = std::sqrt(l1r * l1r - im * im);
+      for (int mm = 2 * im - 1; mm <= 2 * im; ++mm)
+        Y[l][mm] = ((ll1r * rlm) * z) * Y[l - 1][mm] - ((rl1m * rlm) * r2) * Y[l - 2][mm];
+    }
+    {
+      const int im = l - 1;
+      const double rlm = 1.0 / std::sqrt(lr * lr - im * im);
+      for (int mm = 2 * im - 1; mm <= 2 * im; ++mm) Y[l][mm] = ((ll1r * rlm) * z) * Y[l - 1][mm];
+    }
+    const double rll = std::sqrt(ll1r / (2 * lr));
+    const H2 q2 = Y[l - 1][2 * l - 3], q1 = Y[l - 1][2 * l - 2];
+    Y[l][2 * l - 1] = rll * (x * q2 - y * q1);
+    Y[l][2 * l] = rll * (y * q2 + x * q1);
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -1454,6 +1523,165 @@ int oracle_xc_build_sym(const pgxc_geometry* geo, const pgxc_basis* bas, const p
   }
   *exc += e;
   *nel += q;
+  return PGXC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Post-SCF XC nuclear gradient (test infrastructure): dE_xc/dR of the energy
+// integrated on a grid that moves with its atoms, with the Becke weights
+// differentiated (post_scf_calc_xc_en_and_gr(_nl), post_scf_module.f90
+// :2569-3318, :3500-5193 with weight gradients, becke1 grid_module.f90
+// :2499-2616).  Restated independently of the device: the basis Hessians by
+// second-order forward differentiation (H2 below) of the reference's
+// recursion, the density from the occupied orbitals, the weight derivative by
+// dual numbers along the displacement of each atom.
+// ---------------------------------------------------------------------------
+int oracle_xc_gradient(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid* grid, int32_t xc,
+                       int32_t ispin, const double* C, const double* occ, int32_t nbas_in, int32_t nocc,
+                       double* grad, double* exc) {
+  Basis B;
+  int st = make_basis(geo, bas, B);
+  if (st) return st;
+  const int64_t nb = B.nbas, npts = grid->npts;
+  const int natm = B.natm;
+  if (nb != nbas_in || (ispin != 1 && ispin != 2) || !grid->weights_are_raw || !grid->point_atom) return PGXC_EINVAL;
+  const double* gx = grid->grdpts;
+  const double* gy = gx + npts;
+  const double* gz = gy + npts;
+  const double* wr = gz + npts;
+  const int* host = grid->point_atom;
+  const bool gga = PGXC_XC_IS_GGA(xc);
+  std::vector<int> fatom((size_t)nb);
+  for (const Shell& S : B.shells)
+    for (int f = 0; f < (2 * S.l + 1) * S.nrad; ++f) fatom[(size_t)S.f0 + f] = S.atom;
+  std::vector<double> G((size_t)3 * natm, 0.0);
+  double E = 0.0;
+  std::vector<double> val((size_t)10 * nb);  // phi, 3 grad, 6 Hessian (xx xy xz yy yz zz) per function
+  const int ci[6] = {0, 0, 0, 1, 1, 2}, di[6] = {0, 1, 2, 1, 2, 2};
+  auto hx = [](int c, int d) { int a = std::min(c, d), b = std::max(c, d); return a == 0 ? b : (a == 1 ? 2 + b : 5); };
+  for (int64_t p = 0; p < npts; ++p) {
+    // basis functions with Hessians at the point
+    for (const Shell& S : B.shells) {
+      const double* A = B.xyz + 3 * S.atom;
+      H2 x = h2c(gx[p] - A[0]), y = h2c(gy[p] - A[1]), z = h2c(gz[p] - A[2]);
+      x.g[0] = 1.0; y.g[1] = 1.0; z.g[2] = 1.0;
+      H2 Y[4][7];
+      solid_harmonics_h2(x, y, z, S.l, Y);
+      const H2 r2 = x * x + y * y + z * z;
+      std::vector<H2> prim((size_t)S.nexp);
+      for (int e = 0; e < S.nexp; ++e)
+        prim[e] = S.exps[e] * r2.v < 50.0 ? S.norms[e] * h2exp((-S.exps[e]) * r2) : h2c(0.0);
+      const int n = 2 * S.l + 1;
+      const std::vector<double>& T = B.sa[S.l];
+      for (int r = 0; r < S.nrad; ++r) {
+        H2 R = h2c(0.0);
+        if (r < S.nunc) R = prim[r];
+        else for (int e = 0; e < S.nexp; ++e) R = R + S.contr[e + (size_t)S.nexp * (r - S.nunc)] * prim[e];
+        for (int i = 0; i < n; ++i) {
+          H2 Ys = h2c(0.0);
+          for (int m = 0; m < n; ++m)
+            if (T[i * n + m] != 0.0) Ys = Ys + T[i * n + m] * Y[S.l][m];
+          const H2 phi = Ys * R;
+          const int64_t f = S.f0 + (int64_t)i * S.nrad + r;
+          val[10 * f] = phi.v;
+          for (int c = 0; c < 3; ++c) val[10 * f + 1 + c] = phi.g[c];
+          for (int k = 0; k < 6; ++k) val[10 * f + 4 + k] = phi.h[ci[k]][di[k]];
+        }
+      }
+    }
+    // Becke weight of the host with its derivative along each atom's displacement
+    const int h = host[p];
+    auto W_of = [&](int A) {  // dual in the 3 displacement components of atom A
+      D r[3] = {cst(gx[p]), cst(gy[p]), cst(gz[p])};
+      std::vector<D> R((size_t)3 * natm);
+      for (int b = 0; b < natm; ++b)
+        for (int k = 0; k < 3; ++k) R[3 * b + k] = b == A ? var(k, B.xyz[3 * b + k]) : cst(B.xyz[3 * b + k]);
+      if (h == A) for (int k = 0; k < 3; ++k) r[k] = var(k, r[k].v);
+      auto dist = [&](const D* u, const D* v) {
+        D t = (u[0] - v[0]) * (u[0] - v[0]) + (u[1] - v[1]) * (u[1] - v[1]) + (u[2] - v[2]) * (u[2] - v[2]);
+        return dsqrt(t);
+      };
+      D Z = cst(0.0), Ph = cst(0.0);
+      for (int b = 0; b < natm; ++b) {
+        D P = cst(1.0);
+        const D db = dist(r, &R[3 * b]);
+        for (int c = 0; c < natm; ++c) {
+          if (c == b) continue;
+          D mu = (db - dist(r, &R[3 * c])) / dist(&R[3 * b], &R[3 * c]);
+          D q = mu;
+          for (int it = 0; it < 3; ++it) q = 0.5 * q * (3.0 - q * q);
+          P = P * (0.5 * (1.0 - q));
+        }
+        Z = Z + P;
+        if (b == h) Ph = P;
+      }
+      return Ph / Z;
+    };
+    const double Wh = W_of(-1).v;
+    const double w = wr[p] * Wh;
+    // density from the occupied orbitals (density_calc_nl), and X' = P phi, Y'_j = P d_j phi
+    double rho[2] = {0, 0}, grr[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    std::vector<double> Xs((size_t)ispin * nb, 0.0), Yj((size_t)ispin * 3 * nb, 0.0);
+    for (int s = 0; s < ispin; ++s) {
+      const double* Cs = C + (size_t)s * nb * nocc;
+      for (int j = 0; j < nocc; ++j) {
+        double psi = 0, dpsi[3] = {0, 0, 0};
+        for (int64_t f = 0; f < nb; ++f) {
+          const double cf = Cs[f + (size_t)nb * j];
+          psi += cf * val[10 * f];
+          for (int c = 0; c < 3; ++c) dpsi[c] += cf * val[10 * f + 1 + c];
+        }
+        const double o = occ[j + (size_t)nocc * s];
+        rho[s] += o * psi * psi;
+        for (int c = 0; c < 3; ++c) grr[s][c] += 2.0 * o * psi * dpsi[c];
+        for (int64_t f = 0; f < nb; ++f) {
+          const double cf = o * Cs[f + (size_t)nb * j];
+          Xs[(size_t)s * nb + f] += cf * psi;
+          for (int c = 0; c < 3; ++c) Yj[((size_t)s * 3 + c) * nb + f] += cf * dpsi[c];
+        }
+      }
+    }
+    double gam[3] = {0, 0, 0};
+    for (int c = 0; c < 3; ++c) {
+      gam[0] += grr[0][c] * grr[0][c];
+      if (ispin == 2) { gam[1] += grr[1][c] * grr[1][c]; gam[2] += grr[0][c] * grr[1][c]; }
+    }
+    double F, Fr[2], Fg[3];
+    functional_point(xc, ispin, rho, gam, F, Fr, Fg);
+    E += w * F;
+    double a[2], b[2][3];
+    for (int s = 0; s < ispin; ++s) {
+      a[s] = w * Fr[s];
+      for (int c = 0; c < 3; ++c)
+        b[s][c] = !gga ? 0.0 : (ispin == 1 ? w * 2.0 * Fg[0] * grr[0][c]
+                                           : w * (2.0 * Fg[s] * grr[s][c] + Fg[2] * grr[1 - s][c]));
+    }
+    // orbital terms: -q to the function's atom, +q to the point's host
+    for (int64_t f = 0; f < nb; ++f) {
+      double q[3] = {0, 0, 0};
+      for (int s = 0; s < ispin; ++s) {
+        const double X = Xs[(size_t)s * nb + f];
+        for (int k = 0; k < 3; ++k) {
+          double t = a[s] * val[10 * f + 1 + k] * X;
+          for (int j = 0; j < 3; ++j)
+            t += b[s][j] * (val[10 * f + 4 + hx(k, j)] * X + val[10 * f + 1 + k] * Yj[((size_t)s * 3 + j) * nb + f]);
+          q[k] += 2.0 * t;
+        }
+      }
+      for (int k = 0; k < 3; ++k) {
+        G[3 * fatom[f] + k] -= q[k];
+        G[3 * h + k] += q[k];
+      }
+    }
+    // weight term: w_raw F dW_host/dR_A
+    if (F != 0.0)
+      for (int A = 0; A < natm; ++A) {
+        const D Wd = W_of(A);
+        for (int k = 0; k < 3; ++k) G[3 * A + k] += wr[p] * F * Wd.d[k];
+      }
+  }
+  for (int i = 0; i < 3 * natm; ++i) grad[i] += G[i];
+  if (exc) *exc += E;
   return PGXC_OK;
 }
 

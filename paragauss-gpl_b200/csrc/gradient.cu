@@ -1,0 +1,443 @@
+// gradient.cu -- kernels of the post-SCF XC nuclear gradient (gradient.h).
+//
+// FP64 throughout.  The gradient runs once per geometry, after the SCF: the
+// kernels are plain per-point / per-function loops; the four contractions
+// per spin (X = Phi P, Y_j = d_j Phi P) are library DGEMMs issued by the caller.
+#include <cmath>
+
+#include "basis.cuh"
+#include "gradient.h"
+#include "xc_functional.cuh"
+
+namespace pgxc {
+
+namespace {
+
+// Real solid harmonics, first and second derivatives, by the recursion of
+// solid_harmonics (basis.cuh, modules/solid_harmonics_module.f90:369-482)
+// differentiated twice.  H[k][.] holds xx, xy, xz, yy, yz, zz.
+template <int L>
+__device__ __forceinline__ void solid_harmonics_h(double x, double y, double z, double* Y, double (*dY)[16],
+                                                  double (*H)[16]) {
+  const double r2 = x * x + y * y + z * z;
+  const double xv[3] = {x, y, z};
+  constexpr int ci[6] = {0, 0, 0, 1, 1, 2}, di[6] = {0, 1, 2, 1, 2, 2};
+  for (int i = 0; i < 16; ++i) {
+    Y[i] = 0.0;
+    for (int c = 0; c < 3; ++c) dY[c][i] = 0.0;
+    for (int k = 0; k < 6; ++k) H[k][i] = 0.0;
+  }
+  Y[0] = 1.0;
+  if (L == 0) return;
+  Y[1] = z; Y[2] = x; Y[3] = y;
+  dY[2][1] = 1.0; dY[0][2] = 1.0; dY[1][3] = 1.0;
+#pragma unroll
+  for (int l = 2; l <= L; ++l) {
+    const int o = l * l, o1 = (l - 1) * (l - 1), o2 = (l - 2) * (l - 2);
+    const double lr = l, l1r = l - 1, ll1r = 2 * l - 1;
+    {
+      const double p1 = Y[o1], p2 = Y[o2];
+      Y[o] = (ll1r * z * p1 - l1r * r2 * p2) / lr;
+      for (int c = 0; c < 3; ++c)
+        dY[c][o] = (ll1r * ((c == 2 ? p1 : 0.0) + z * dY[c][o1]) - l1r * (2.0 * xv[c] * p2 + r2 * dY[c][o2])) / lr;
+      for (int k = 0; k < 6; ++k) {
+        const int c = ci[k], d = di[k];
+        const double t1 = (c == 2 ? dY[d][o1] : 0.0) + (d == 2 ? dY[c][o1] : 0.0) + z * H[k][o1];
+        const double t2 = (c == d ? 2.0 * p2 : 0.0) + 2.0 * xv[c] * dY[d][o2] + 2.0 * xv[d] * dY[c][o2] + r2 * H[k][o2];
+        H[k][o] = (ll1r * t1 - l1r * t2) / lr;
+      }
+    }
+    for (int im = 1; im <= l - 2; ++im) {
+      const double sim = im * im;
+      const double rlm = 1.0 / sqrt(lr * lr - sim);
+      const double rl1m = sqrt(l1r * l1r - sim);
+      const double a = ll1r * z * rlm;
+      const double b = rl1m * r2 * rlm;
+      for (int mm = 2 * im - 1; mm <= 2 * im; ++mm) {
+        const double p1 = Y[o1 + mm], p2 = Y[o2 + mm];
+        Y[o + mm] = a * p1 - b * p2;
+        for (int c = 0; c < 3; ++c)
+          dY[c][o + mm] = (c == 2 ? ll1r * rlm * p1 : 0.0) + a * dY[c][o1 + mm] - rl1m * 2.0 * xv[c] * rlm * p2 -
+                          b * dY[c][o2 + mm];
+        for (int k = 0; k < 6; ++k) {
+          const int c = ci[k], d = di[k];
+          H[k][o + mm] = (c == 2 ? ll1r * rlm * dY[d][o1 + mm] : 0.0) + (d == 2 ? ll1r * rlm * dY[c][o1 + mm] : 0.0) +
+                         a * H[k][o1 + mm] -
+                         rl1m * rlm * ((c == d ? 2.0 * p2 : 0.0) + 2.0 * xv[c] * dY[d][o2 + mm] + 2.0 * xv[d] * dY[c][o2 + mm]) -
+                         b * H[k][o2 + mm];
+        }
+      }
+    }
+    {
+      const int im = l - 1;
+      const double rlm = 1.0 / sqrt(lr * lr - (double)(im * im));
+      const double a = ll1r * z * rlm;
+      for (int mm = 2 * im - 1; mm <= 2 * im; ++mm) {
+        const double p1 = Y[o1 + mm];
+        Y[o + mm] = a * p1;
+        for (int c = 0; c < 3; ++c) dY[c][o + mm] = (c == 2 ? ll1r * rlm * p1 : 0.0) + a * dY[c][o1 + mm];
+        for (int k = 0; k < 6; ++k) {
+          const int c = ci[k], d = di[k];
+          H[k][o + mm] = (c == 2 ? ll1r * rlm * dY[d][o1 + mm] : 0.0) + (d == 2 ? ll1r * rlm * dY[c][o1 + mm] : 0.0) +
+                         a * H[k][o1 + mm];
+        }
+      }
+    }
+    {
+      const double rll = sqrt(ll1r / (2.0 * lr));
+      const int j2 = o1 + 2 * l - 3, j1 = o1 + 2 * l - 2;
+      const double q2 = Y[j2], q1 = Y[j1];
+      Y[o + 2 * l - 1] = (x * q2 - y * q1) * rll;
+      Y[o + 2 * l] = (y * q2 + x * q1) * rll;
+      for (int c = 0; c < 3; ++c) {
+        const double dx = c == 0, dy = c == 1;
+        dY[c][o + 2 * l - 1] = (dx * q2 + x * dY[c][j2] - dy * q1 - y * dY[c][j1]) * rll;
+        dY[c][o + 2 * l] = (dy * q2 + y * dY[c][j2] + dx * q1 + x * dY[c][j1]) * rll;
+      }
+      for (int k = 0; k < 6; ++k) {
+        const int c = ci[k], d = di[k];
+        const double cx = c == 0, cy = c == 1, dx = d == 0, dy = d == 1;
+        H[k][o + 2 * l - 1] = (cx * dY[d][j2] + dx * dY[c][j2] + x * H[k][j2] - cy * dY[d][j1] - dy * dY[c][j1] -
+                               y * H[k][j1]) * rll;
+        H[k][o + 2 * l] = (cy * dY[d][j2] + dy * dY[c][j2] + y * H[k][j2] + cx * dY[d][j1] + dx * dY[c][j1] +
+                           x * H[k][j1]) * rll;
+      }
+    }
+  }
+}
+
+// grid = (ld / 128, shells of L): phi, grad and Hessian of every function of the shell
+template <int L>
+__global__ void __launch_bounds__(128) k_basis_hess(const DevShell* __restrict__ shells, const int* __restrict__ ids,
+                                                    const double* __restrict__ atoms, const double* __restrict__ exps,
+                                                    const double* __restrict__ norms, const double* __restrict__ contr,
+                                                    const int2* __restrict__ rng, DevSA sa,
+                                                    const double* __restrict__ px, const double* __restrict__ py,
+                                                    const double* __restrict__ pz, int64_t p0, int64_t nvalid,
+                                                    int64_t ld, int64_t plane, double* __restrict__ out) {
+  const DevShell S = shells[ids[blockIdx.y]];
+  const int64_t p = (int64_t)blockIdx.x * 128 + threadIdx.x;
+  if (p >= ld) return;
+  const bool valid = p < nvalid;
+  double x = 0, y = 0, z = 0;
+  if (valid) {
+    x = px[p0 + p] - atoms[3 * S.atom];
+    y = py[p0 + p] - atoms[3 * S.atom + 1];
+    z = pz[p0 + p] - atoms[3 * S.atom + 2];
+  }
+  double Y[16], dY[3][16], H[6][16];
+  solid_harmonics_h<L>(x, y, z, Y, dY, H);
+  const double r2 = x * x + y * y + z * z;
+  const double xv[3] = {x, y, z};
+  constexpr int ci[6] = {0, 0, 0, 1, 1, 2}, di[6] = {0, 1, 2, 1, 2, 2};
+  // symmetry-adapted harmonics of this l
+  double Ys[2 * L + 1], dYs[3][2 * L + 1], Hs[6][2 * L + 1];
+  for (int i = 0; i < 2 * L + 1; ++i) {
+    double v = 0, g[3] = {0, 0, 0}, h[6] = {0, 0, 0, 0, 0, 0};
+    for (int m = 0; m < 2 * L + 1; ++m) {
+      const double cf = sa.identity ? (m == i ? 1.0 : 0.0) : sa.c[L][i][m];
+      v += cf * Y[L * L + m];
+      for (int c = 0; c < 3; ++c) g[c] += cf * dY[c][L * L + m];
+      for (int k = 0; k < 6; ++k) h[k] += cf * H[k][L * L + m];
+    }
+    Ys[i] = v;
+    for (int c = 0; c < 3; ++c) dYs[c][i] = g[c];
+    for (int k = 0; k < 6; ++k) Hs[k][i] = h[k];
+  }
+  const double* ex = exps + S.exp_off;
+  const double* nr = norms + S.exp_off;
+  const double* cc = contr + S.con_off;
+  for (int rr = 0; rr < S.nrad; ++rr) {
+    // R, dR = sum c (-2 alpha) v and d2R = sum c (4 alpha^2) v of radial function rr:
+    // d_c R = x_c dR, d_c d_d R = delta_cd dR + x_c x_d d2R
+    double R = 0.0, dR = 0.0, d2R = 0.0;
+    if (valid) {
+      int e0 = 0, e1 = S.nexp;
+      if (S.seg) {
+        const int2 rg = rng[S.rad_off + rr];
+        e0 = rg.x;
+        e1 = rg.y;
+      }
+      for (int e = e0; e < e1; ++e) {
+        double cf;
+        if (S.seg) cf = cc[e + (int64_t)S.nexp * rr];
+        else if (rr < S.nunc) cf = (e == rr) ? 1.0 : 0.0;
+        else cf = cc[e + (int64_t)S.nexp * (rr - S.nunc)];
+        const double alpha = ex[e];
+        const double v = prim_value(alpha, nr[e], r2);
+        R += cf * v;
+        dR += cf * (-2.0 * alpha) * v;
+        d2R += cf * (4.0 * alpha * alpha) * v;
+      }
+    }
+    for (int i = 0; i < 2 * L + 1; ++i) {
+      const int64_t f = S.f0 + (int64_t)i * S.nrad + rr;
+      double* o = out + f * ld + p;
+      o[0] = Ys[i] * R;
+      for (int c = 0; c < 3; ++c) o[(1 + c) * plane] = dYs[c][i] * R + Ys[i] * xv[c] * dR;
+      for (int k = 0; k < 6; ++k) {
+        const int c = ci[k], d = di[k];
+        o[(4 + k) * plane] = Hs[k][i] * R + (dYs[c][i] * xv[d] + dYs[d][i] * xv[c]) * dR +
+                             Ys[i] * ((c == d ? dR : 0.0) + xv[c] * xv[d] * d2R);
+      }
+    }
+  }
+}
+
+// index of the Hessian component (c, d) in xx, xy, xz, yy, yz, zz
+__device__ __forceinline__ int hidx(int c, int d) {
+  const int a = c < d ? c : d, b = c < d ? d : c;
+  return a == 0 ? b : (a == 1 ? 2 + b : 5);
+}
+
+__global__ void k_grad_points(XcConst K, bool gga, int ispin, int64_t nbas, int64_t ld, int64_t p0, int64_t nvalid,
+                              const double* __restrict__ w, const double* __restrict__ wraw,
+                              const double* __restrict__ B, int64_t plane, const double* __restrict__ XY,
+                              double* __restrict__ coef, double* __restrict__ ef, double* __restrict__ exc) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= ld) return;
+  if (p >= nvalid) {
+    for (int s = 0; s < ispin; ++s)
+      for (int c = 0; c < 4; ++c) coef[(4 * s + c) * ld + p] = 0.0;
+    ef[p] = 0.0;
+    return;
+  }
+  double rho[2] = {0, 0}, gr[2][3] = {{0, 0, 0}, {0, 0, 0}};
+  for (int s = 0; s < ispin; ++s) {
+    const double* X = XY + (4 * s) * plane;
+    for (int64_t f = 0; f < nbas; ++f) {
+      const double xv = X[f * ld + p];
+      rho[s] += B[f * ld + p] * xv;
+      if (gga)
+        for (int c = 0; c < 3; ++c) gr[s][c] += 2.0 * B[(1 + c) * plane + f * ld + p] * xv;
+    }
+  }
+  const double wp = w[p0 + p];
+  double f = 0.0, fr[2] = {0, 0}, fg[3] = {0, 0, 0};
+  if (ispin == 1) {
+    const double g = gr[0][0] * gr[0][0] + gr[0][1] * gr[0][1] + gr[0][2] * gr[0][2];
+    if (gga) xc_gga(K, rho[0], g, f, fr[0], fg[0]);
+    else xc_vwn(K, rho[0], f, fr[0]);
+    coef[p] = wp * fr[0];
+    for (int c = 0; c < 3; ++c) coef[(1 + c) * ld + p] = gga ? wp * 2.0 * fg[0] * gr[0][c] : 0.0;
+  } else {
+    const double r2[2] = {rho[0], rho[1]};
+    const double g3[3] = {gr[0][0] * gr[0][0] + gr[0][1] * gr[0][1] + gr[0][2] * gr[0][2],
+                          gr[1][0] * gr[1][0] + gr[1][1] * gr[1][1] + gr[1][2] * gr[1][2],
+                          gr[0][0] * gr[1][0] + gr[0][1] * gr[1][1] + gr[0][2] * gr[1][2]};
+    double fr2[2], fg3[3];
+    if (gga) xc_open<true>(K, r2, g3, f, fr2, fg3);
+    else xc_open<false>(K, r2, g3, f, fr2, fg3);
+    for (int s = 0; s < 2; ++s) {
+      coef[(4 * s) * ld + p] = wp * fr2[s];
+      for (int c = 0; c < 3; ++c)
+        coef[(4 * s + 1 + c) * ld + p] = gga ? wp * (2.0 * fg3[s] * gr[s][c] + fg3[2] * gr[1 - s][c]) : 0.0;
+    }
+  }
+  ef[p] = wraw[p0 + p] * f;
+  atomicAdd(exc, wp * f);
+}
+
+// q^s_mu,k(p) for one function and point, summed over spins
+__device__ __forceinline__ void q_terms(bool gga, int ispin, int64_t f, int64_t p, int64_t ld, int64_t plane,
+                                        const double* __restrict__ B, const double* __restrict__ XY,
+                                        const double* __restrict__ coef, double* q) {
+  const int64_t o = f * ld + p;
+  double d[3], H[6];
+  for (int c = 0; c < 3; ++c) d[c] = B[(1 + c) * plane + o];
+  if (gga)
+    for (int k = 0; k < 6; ++k) H[k] = B[(4 + k) * plane + o];
+  q[0] = q[1] = q[2] = 0.0;
+  for (int s = 0; s < ispin; ++s) {
+    const double X = XY[(4 * s) * plane + o];
+    const double a = coef[(4 * s) * ld + p];
+    for (int k = 0; k < 3; ++k) q[k] += 2.0 * a * d[k] * X;
+    if (!gga) continue;
+    double Yj[3], b[3];
+    for (int j = 0; j < 3; ++j) {
+      Yj[j] = XY[(4 * s + 1 + j) * plane + o];
+      b[j] = coef[(4 * s + 1 + j) * ld + p];
+    }
+    for (int k = 0; k < 3; ++k) {
+      double t = 0.0;
+      for (int j = 0; j < 3; ++j) t += b[j] * (H[hidx(k, j)] * X + d[k] * Yj[j]);
+      q[k] += 2.0 * t;
+    }
+  }
+}
+
+// grid = (nbas, ld / 256): -sum over the block's points of q_mu into atom(mu)
+__global__ void k_grad_fn(bool gga, int ispin, int64_t nbas, int64_t ld, int64_t nvalid, const int* __restrict__ fatom,
+                          const double* __restrict__ B, int64_t plane, const double* __restrict__ XY,
+                          const double* __restrict__ coef, double* __restrict__ grad) {
+  __shared__ double red[3][8];
+  const int64_t f = blockIdx.x;
+  const int64_t p = (int64_t)blockIdx.y * blockDim.x + threadIdx.x;
+  double q[3] = {0, 0, 0};
+  if (p < nvalid) q_terms(gga, ispin, f, p, ld, plane, B, XY, coef, q);
+  for (int k = 0; k < 3; ++k)
+    for (int off = 16; off > 0; off >>= 1) q[k] += __shfl_down_sync(0xffffffffu, q[k], off);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0)
+    for (int k = 0; k < 3; ++k) red[k][warp] = q[k];
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double s = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += red[threadIdx.x][i];
+    atomicAdd(grad + 3 * fatom[f] + threadIdx.x, -s);
+  }
+}
+
+// thread per point: +sum over functions of q into the point's host atom
+__global__ void k_grad_host(bool gga, int ispin, int64_t nbas, int64_t ld, int64_t p0, int64_t nvalid,
+                            const int* __restrict__ owner, const double* __restrict__ B, int64_t plane,
+                            const double* __restrict__ XY, const double* __restrict__ coef, double* __restrict__ grad) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= nvalid) return;
+  double t[3] = {0, 0, 0};
+  for (int64_t f = 0; f < nbas; ++f) {
+    double q[3];
+    q_terms(gga, ispin, f, p, ld, plane, B, XY, coef, q);
+    for (int k = 0; k < 3; ++k) t[k] += q[k];
+  }
+  const int h = owner[p0 + p];
+  for (int k = 0; k < 3; ++k) atomicAdd(grad + 3 * h + k, t[k]);
+}
+
+// Becke cell function s(mu) = (1 - p(p(p(mu)))) / 2, p(q) = q (3 - q^2) / 2, and ds/dmu
+__device__ __forceinline__ void becke_s(double mu, double& s, double& ds) {
+  const double q1 = 0.5 * mu * (3.0 - mu * mu);
+  const double q2 = 0.5 * q1 * (3.0 - q1 * q1);
+  const double q3 = 0.5 * q2 * (3.0 - q2 * q2);
+  s = 0.5 * (1.0 - q3);
+  ds = -0.5 * (1.5 * (1.0 - q2 * q2)) * (1.5 * (1.0 - q1 * q1)) * (1.5 * (1.0 - mu * mu));
+}
+
+// mu_BC at r, with the reference's pair orientation
+__device__ __forceinline__ double becke_mu(const double* A, int b, int c, const double* rv, double& dB, double& dC,
+                                           double& Rbc) {
+  double t[3];
+  for (int k = 0; k < 3; ++k) t[k] = rv[k] - A[3 * b + k];
+  dB = sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+  for (int k = 0; k < 3; ++k) t[k] = rv[k] - A[3 * c + k];
+  dC = sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+  for (int k = 0; k < 3; ++k) t[k] = A[3 * b + k] - A[3 * c + k];
+  Rbc = sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+  return (dB - dC) / Rbc;
+}
+
+// thread per point; per-atom sums in shared memory (3 natm doubles), then global atomics
+__global__ void k_grad_weights(const double* __restrict__ atoms, int natm, const double* __restrict__ px,
+                               const double* __restrict__ py, const double* __restrict__ pz,
+                               const int* __restrict__ owner, int64_t p0, int64_t nvalid,
+                               const double* __restrict__ ef, double* __restrict__ grad) {
+  extern __shared__ double sm[];
+  double* A = sm;              // 3 natm atom coordinates
+  double* G = sm + 3 * natm;   // 3 natm gradient sums
+  for (int i = threadIdx.x; i < 3 * natm; i += blockDim.x) {
+    A[i] = atoms[i];
+    G[i] = 0.0;
+  }
+  __syncthreads();
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < nvalid && ef[p] != 0.0) {
+    const double rv[3] = {px[p0 + p], py[p0 + p], pz[p0 + p]};
+    const int h = owner[p0 + p];
+    double Z = 0.0, Ph = 0.0;
+    for (int b = 0; b < natm; ++b) {
+      double P = 1.0;
+      for (int c = 0; c < natm; ++c) {
+        if (c == b) continue;
+        double dB, dC, R, s, ds;
+        becke_s(becke_mu(A, b, c, rv, dB, dC, R), s, ds);
+        P *= s;
+      }
+      Z += P;
+      if (b == h) Ph = P;
+    }
+    if (Z > 0.0) {
+      const double Wh = Ph / Z;
+      for (int b = 0; b < natm; ++b) {
+        const double cb = ef[p] * ((b == h ? 1.0 : 0.0) - Wh) / Z;
+        // product of the nonzero factors and their zero count: leave-one-out products
+        double pnz = 1.0;
+        int nz = 0;
+        for (int c = 0; c < natm; ++c) {
+          if (c == b) continue;
+          double dB, dC, R, s, ds;
+          becke_s(becke_mu(A, b, c, rv, dB, dC, R), s, ds);
+          if (s == 0.0) ++nz;
+          else pnz *= s;
+        }
+        if (nz > 1) continue;
+        for (int c = 0; c < natm; ++c) {
+          if (c == b) continue;
+          double dB, dC, R, s, ds;
+          const double mu = becke_mu(A, b, c, rv, dB, dC, R);
+          becke_s(mu, s, ds);
+          double L;
+          if (nz == 0) L = pnz / s;
+          else L = (s == 0.0) ? pnz : 0.0;
+          const double kap = cb * L * ds;
+          if (kap == 0.0) continue;
+          for (int k = 0; k < 3; ++k) {
+            const double ub = dB > 0.0 ? (rv[k] - A[3 * b + k]) / dB : 0.0;
+            const double uc = dC > 0.0 ? (rv[k] - A[3 * c + k]) / dC : 0.0;
+            const double rbc = (A[3 * b + k] - A[3 * c + k]) / (R * R);
+            atomicAdd(&G[3 * h + k], kap * (ub - uc) / R);         // the point moves with its host
+            atomicAdd(&G[3 * b + k], kap * (-ub / R - mu * rbc));
+            atomicAdd(&G[3 * c + k], kap * (uc / R + mu * rbc));
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 3 * natm; i += blockDim.x)
+    if (G[i] != 0.0) atomicAdd(grad + i, G[i]);
+}
+
+template <int L>
+void launch_hess_l(const BuildArgs& a, int64_t p0, int64_t nvalid, int64_t ld, int64_t plane, double* out,
+                   cudaStream_t st) {
+  if (a.nshl[L] == 0) return;
+  dim3 grid((unsigned)((ld + 127) / 128), (unsigned)a.nshl[L]);
+  k_basis_hess<L><<<grid, 128, 0, st>>>(a.shells, a.shl[L], a.atoms, a.exps, a.norms, a.contr, a.rng, a.sa, a.px, a.py,
+                                        a.pz, p0, nvalid, ld, plane, out);
+}
+
+}  // namespace
+
+void launch_basis_hess(const BuildArgs& a, int64_t p0, int64_t nvalid, int64_t ld, int64_t plane, double* out,
+                       cudaStream_t st) {
+  launch_hess_l<0>(a, p0, nvalid, ld, plane, out, st);
+  launch_hess_l<1>(a, p0, nvalid, ld, plane, out, st);
+  launch_hess_l<2>(a, p0, nvalid, ld, plane, out, st);
+  launch_hess_l<3>(a, p0, nvalid, ld, plane, out, st);
+}
+
+void launch_grad_points(const XcConst& K, bool gga, int ispin, int64_t nbas, int64_t ld, int64_t p0, int64_t nvalid,
+                        const double* w, const double* wraw, const double* basis, int64_t plane, const double* XY,
+                        double* coef, double* ef, double* exc, cudaStream_t st) {
+  k_grad_points<<<(unsigned)((ld + 127) / 128), 128, 0, st>>>(K, gga, ispin, nbas, ld, p0, nvalid, w, wraw, basis,
+                                                               plane, XY, coef, ef, exc);
+}
+
+void launch_grad_orbital(bool gga, int ispin, int64_t nbas, int64_t ld, int64_t p0, int64_t nvalid,
+                         const int* fatom, const int* owner, const double* basis, int64_t plane, const double* XY,
+                         const double* coef, double* grad, cudaStream_t st) {
+  dim3 grid((unsigned)nbas, (unsigned)((ld + 255) / 256));
+  k_grad_fn<<<grid, 256, 0, st>>>(gga, ispin, nbas, ld, nvalid, fatom, basis, plane, XY, coef, grad);
+  k_grad_host<<<(unsigned)((ld + 127) / 128), 128, 0, st>>>(gga, ispin, nbas, ld, p0, nvalid, owner, basis, plane,
+                                                             XY, coef, grad);
+}
+
+void launch_grad_weights(const double* atoms, int natm, const double* px, const double* py, const double* pz,
+                         const int* owner, int64_t p0, int64_t nvalid, const double* ef, double* grad, cudaStream_t st) {
+  const size_t smem = sizeof(double) * 6 * natm;
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_grad_weights, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_grad_weights<<<(unsigned)((nvalid + 127) / 128), 128, smem, st>>>(atoms, natm, px, py, pz, owner, p0, nvalid, ef,
+                                                                       grad);
+}
+
+}  // namespace pgxc

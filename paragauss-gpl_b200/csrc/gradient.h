@@ -1,0 +1,46 @@
+// gradient.h -- post-SCF XC nuclear gradient on the device.
+//
+// dE_xc/dR_A of E_xc = sum_g w_g f(rho(r_g), gamma(r_g)) with the grid
+// attached to the atoms (r_g = R_host + fixed offset) and w_g = w_raw(g)
+// W_host(r_g), the Becke weight of the host atom: the derivative of the
+// discrete energy the build integrates, as the reference's post-SCF
+// gradients with moving grid and weight gradients (post_scf_module.f90
+// :2930-3060, density_calc_ph_nl, grid_module.f90 becke1).
+//
+// With X^s = Phi P^s and Y^s_j = d_j Phi P^s (per chunk of points),
+//   q^s_mu,k(g) = 2 [a_s d_k phi_mu X^s_mu + sum_j b_sj (d_k d_j phi_mu X^s_mu + d_k phi_mu Y^s_j,mu)],
+// a_s = w df/drho_s and b_s = w (2 df/dgamma_ss grad rho_s + df/dgamma_ab grad rho_s'), the
+// orbital terms are  -sum_g q_mu(g) to atom(mu)  and  +sum_mu q_mu(g) to host(g);
+// the weight term is sum_g w_raw f dW_host(r_g)/dR.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+
+namespace pgxc {
+
+// Basis values, gradients and Hessians of every function on points
+// [p0, p0 + nvalid) of the context's grid: out[c * plane + f * ld + p],
+// c = 0 phi, 1..3 d/dx, d/dy, d/dz, 4..9 xx, xy, xz, yy, yz, zz.
+void launch_basis_hess(const BuildArgs& a, int64_t p0, int64_t nvalid, int64_t ld, int64_t plane, double* out,
+                       cudaStream_t st);
+
+// Per point of the chunk: rho_s, grad rho_s from X, Y and the basis values,
+// the functional, and the coefficients a_s, b_s (coef[(4 s + c) ld + p]) and
+// ef = w_raw f; E_xc = sum w f is added into *exc.
+void launch_grad_points(const XcConst& K, bool gga, int ispin, int64_t nbas, int64_t ld, int64_t p0, int64_t nvalid,
+                        const double* w, const double* wraw, const double* basis, int64_t plane, const double* XY,
+                        double* coef, double* ef, double* exc, cudaStream_t st);
+
+// The orbital terms: -sum_g q to atom(mu) (fatom[mu]) and +sum_mu q to host(g).
+void launch_grad_orbital(bool gga, int ispin, int64_t nbas, int64_t ld, int64_t p0, int64_t nvalid,
+                         const int* fatom, const int* owner, const double* basis, int64_t plane, const double* XY,
+                         const double* coef, double* grad, cudaStream_t st);
+
+// The weight term sum_g ef_g dW_host(r_g)/dR over the chunk's points.
+void launch_grad_weights(const double* atoms, int natm, const double* px, const double* py, const double* pz,
+                         const int* owner, int64_t p0, int64_t nvalid, const double* ef, double* grad, cudaStream_t st);
+
+}  // namespace pgxc

@@ -12,8 +12,10 @@
 #include <string>
 #include <vector>
 
+#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
+#include "gradient.h"
 #include "kernels.h"
 #include "mixed.h"
 #include "pgxc_common.cuh"
@@ -68,6 +70,9 @@ struct pgxc_ctx {
   SymPlan* sym = nullptr;       // symmetry adaptation, when set
   double* d_eacc = nullptr;     // {E, cE, N, cN} per functional of pgxc_xc_energies
   int eacc_cap = 0;
+  int* d_owner = nullptr;       // host atom of each point (raw-weight grids)
+  double* d_wraw = nullptr;     // the raw weights of those grids
+  cublasHandle_t cublas = nullptr;
 };
 
 namespace {
@@ -172,6 +177,7 @@ void pgxc_destroy(pgxc_ctx* c) {
   if (c->mixed) mixed_destroy(c->mixed);
   if (c->screen) screen_destroy(c->screen);
   delete c->sym;
+  if (c->cublas) cublasDestroy(c->cublas);
   for (void* p : c->allocs) cudaFree(p);
   if (c->h_ham) cudaFreeHost(c->h_ham);
   if (c->h_acc) cudaFreeHost(c->h_acc);
@@ -392,6 +398,10 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
         (st = dalloc(c, &c->d_dist, (size_t)c->natm * c->natm)))
       return fail(st);
     CUDA_TRY(c, cudaMemcpy(downer, grid->point_atom, sizeof(int) * n, cudaMemcpyHostToDevice));
+    // the raw weights and hosts stay for the nuclear gradient (pgxc_xc_gradient)
+    if ((st = dalloc(c, &c->d_wraw, n))) return fail(st);
+    CUDA_TRY(c, cudaMemcpy(c->d_wraw, dgrid + 3 * n, sizeof(double) * n, cudaMemcpyDeviceToDevice));
+    c->d_owner = downer;
     launch_becke(datoms, c->d_dist, c->natm, a.px, a.py, a.pz, downer, n, dbecke, c->stream);
     CUDA_TRY(c, cudaGetLastError());
     launch_scale_inplace(dgrid + 3 * n, dbecke, n, c->stream);
@@ -768,6 +778,120 @@ int pgxc_build_device(pgxc_ctx* c, const double* d_C, const double* d_occ, int32
     tm->total_ms = tot;
   }
   return PGXC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Post-SCF XC nuclear gradient (gradient.h): per chunk of points the basis
+// values with Hessians, X = Phi P and Y_j = d_j Phi P (library DGEMMs), the
+// functional's coefficients per point, the orbital terms and the Becke weight
+// term.  FP64, every layout; needs the raw grid (weights_are_raw, point_atom).
+// ---------------------------------------------------------------------------
+int pgxc_xc_gradient(pgxc_ctx* c, const double* C, const double* occ, int32_t nbas, int32_t nocc, int32_t ispin,
+                     double* grad, double* exc) {
+  if (!c) return set_err(nullptr, PGXC_EINVAL, "ctx is NULL");
+  int st = check_build_args(c, nbas, nocc, ispin, (int64_t)ispin * nbas * (nbas + 1) / 2);
+  if (st) return st;
+  if (!grad || (nocc > 0 && (!C || !occ))) return set_err(c, PGXC_EINVAL, "NULL output/input");
+  if (!c->d_owner)
+    return set_err(c, PGXC_ENOTSUP, "the XC gradient needs a grid created with raw weights and point_atom "
+                                    "(the grid moves with its atoms)");
+  if (!all_finite(C, (int64_t)nbas * nocc * ispin) || !all_finite(occ, (int64_t)nocc * ispin))
+    return set_err(c, PGXC_ENONFINITE, "non-finite C or occ");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  if ((st = ensure_occ(c, nocc))) return st;
+  BuildArgs& a = c->a;
+  cudaStream_t s = c->stream;
+  if (!c->cublas) {
+    if (cublasCreate(&c->cublas) != CUBLAS_STATUS_SUCCESS) return set_err(c, PGXC_ECUDA, "cublasCreate failed");
+  }
+  if (cublasSetStream(c->cublas, s) != CUBLAS_STATUS_SUCCESS) return set_err(c, PGXC_ECUDA, "cublasSetStream failed");
+  const int64_t kpad = round_up(std::max(nocc, 1), 16);
+  if ((st = upload_orbitals(c, C, occ, nbas, nocc, kpad, cudaMemcpyHostToDevice))) return st;
+  launch_pmat_f64(a, kpad, s);
+  if (ispin == 2) {
+    BuildArgs b = a;
+    b.C = c->C2;
+    b.occ = c->occ2;
+    b.P = c->P2;
+    launch_pmat_f64(b, kpad, s);
+  }
+  // function -> atom
+  std::vector<int> fatom((size_t)nbas);
+  for (const DevShell& S : c->shells)
+    for (int f = 0; f < (2 * S.l + 1) * S.nrad; ++f) fatom[(size_t)S.f0 + f] = S.atom;
+  // chunk of points: 10 basis planes + 4 ispin X/Y planes of nbas x ld, under ~1.5 GB
+  int64_t ld = 4096;
+  while (ld > 128 && (double)(10 + 4 * ispin) * nbas * ld * 8.0 > 1.5e9) ld /= 2;
+  const int64_t plane = (int64_t)nbas * ld;
+  double *basis = nullptr, *XY = nullptr, *coef = nullptr, *ef = nullptr, *dgrad = nullptr, *de = nullptr;
+  int* dfatom = nullptr;
+  std::vector<void*> mine;
+  auto scratch = [&](void** p, size_t bytes) -> int {
+    cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 8));
+    if (e != cudaSuccess) return set_err(c, PGXC_ENOMEM, std::string("gradient scratch: ") + cudaGetErrorString(e));
+    mine.push_back(*p);
+    return PGXC_OK;
+  };
+  auto release = [&]() { for (void* p : mine) cudaFree(p); };
+  if ((st = scratch((void**)&basis, sizeof(double) * 10 * plane)) ||
+      (st = scratch((void**)&XY, sizeof(double) * 4 * ispin * plane)) ||
+      (st = scratch((void**)&coef, sizeof(double) * 4 * ispin * ld)) || (st = scratch((void**)&ef, sizeof(double) * ld)) ||
+      (st = scratch((void**)&dgrad, sizeof(double) * 3 * c->natm)) || (st = scratch((void**)&de, sizeof(double))) ||
+      (st = scratch((void**)&dfatom, sizeof(int) * nbas))) {
+    release();
+    return st;
+  }
+  const bool gga = PGXC_XC_IS_GGA(c->opt.functional);
+  int rc = PGXC_OK;
+  do {
+    if (cudaMemcpyAsync(dfatom, fatom.data(), sizeof(int) * nbas, cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemsetAsync(dgrad, 0, sizeof(double) * 3 * c->natm, s) != cudaSuccess ||
+        cudaMemsetAsync(de, 0, sizeof(double), s) != cudaSuccess) {
+      rc = set_err(c, PGXC_ECUDA, "gradient set-up copies failed");
+      break;
+    }
+    const double one = 1.0, zero = 0.0;
+    for (int64_t p0 = 0; p0 < c->npts && rc == PGXC_OK; p0 += ld) {
+      const int64_t nv = std::min<int64_t>(ld, c->npts - p0);
+      launch_basis_hess(a, p0, nv, ld, plane, basis, s);
+      for (int sp = 0; sp < ispin; ++sp) {
+        const double* P = sp ? c->P2 : a.P;
+        for (int j = 0; j < (gga ? 4 : 1); ++j) {
+          // X (j = 0) or Y_j = (d_j Phi) P: (ld x nbas) = (ld x nbas)(nbas x nbas), P symmetric
+          if (cublasDgemm(c->cublas, CUBLAS_OP_N, CUBLAS_OP_N, (int)ld, (int)nbas, (int)nbas, &one, basis + j * plane,
+                          (int)ld, P, (int)a.ldc, &zero, XY + (4 * sp + j) * plane, (int)ld) != CUBLAS_STATUS_SUCCESS) {
+            rc = set_err(c, PGXC_ECUDA, "cublasDgemm failed");
+            break;
+          }
+        }
+      }
+      if (rc) break;
+      launch_grad_points(a.xc, gga, ispin, nbas, ld, p0, nv, a.w, c->d_wraw, basis, plane, XY, coef, ef, de, s);
+      launch_grad_orbital(gga, ispin, nbas, ld, p0, nv, dfatom, c->d_owner, basis, plane, XY, coef, dgrad, s);
+      launch_grad_weights(a.atoms, c->natm, a.px, a.py, a.pz, c->d_owner, p0, nv, ef, dgrad, s);
+      if (cudaGetLastError() != cudaSuccess) rc = set_err(c, PGXC_ECUDA, "gradient kernel launch failed");
+    }
+    if (rc) break;
+    std::vector<double> hg((size_t)3 * c->natm);
+    double he = 0.0;
+    if (cudaMemcpyAsync(hg.data(), dgrad, sizeof(double) * hg.size(), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaMemcpyAsync(&he, de, sizeof(double), cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+      rc = set_err(c, PGXC_ECUDA, "gradient read-back failed");
+      break;
+    }
+    for (size_t i = 0; i < hg.size(); ++i) {
+      if (!std::isfinite(hg[i])) {
+        rc = set_err(c, PGXC_ENONFINITE, "non-finite gradient");
+        break;
+      }
+      grad[i] += hg[i];
+    }
+    if (exc) *exc += he;
+  } while (false);
+  cudaStreamSynchronize(s);
+  release();
+  return rc;
 }
 
 // ---------------------------------------------------------------------------

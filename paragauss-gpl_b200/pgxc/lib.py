@@ -54,6 +54,8 @@ def lib():
     L.pgxc_batch_run.argtypes = [vp, P(ct.c_double)]
     L.pgxc_batch_destroy.argtypes = [vp]
     L.pgxc_batch_stats.argtypes = [vp, P(ct.c_int64), P(ct.c_int64)]
+    L.pgxc_xc_gradient.argtypes = [vp, abi._f64p, abi._f64p, ct.c_int32, ct.c_int32, ct.c_int32, abi._f64p,
+                                   P(ct.c_double)]
     L.pgxc_xc_energies.argtypes = [vp, abi._f64p, abi._f64p, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32,
                                    abi._i32p, abi._f64p, P(ct.c_double)]
     L.pgxc_set_symmetry.argtypes = [vp, P(abi.Symmetry)]
@@ -114,6 +116,18 @@ class Context:
         if timings:
             return ham, exc.value, nel.value, tm.as_dict()
         return ham, exc.value, nel.value
+
+    def xc_gradient(self, C=None, occ=None):
+        """dE_xc/dR (natoms, 3) with the grid moving with its atoms, and E_xc
+        (a context created with weighted=False: raw weights and point_atom)."""
+        c = self.case
+        Cf = c.c_fortran() if C is None else np.ascontiguousarray(C, dtype=np.float64).reshape(-1)
+        of = c.occ_fortran() if occ is None else np.ascontiguousarray(occ, dtype=np.float64).reshape(-1)
+        g = np.zeros(3 * len(c.coords))
+        e = ct.c_double(0.0)
+        _check(lib().pgxc_xc_gradient(self.h, abi.f64p(Cf), abi.f64p(of), c.nbas, c.nocc, c.ispin, abi.f64p(g),
+                                      ct.byref(e)), self.h)
+        return g.reshape(-1, 3), e.value
 
     def xc_energies(self, functionals, C=None, occ=None):
         """E_xc of each keyword in functionals on this context's density
