@@ -44,6 +44,9 @@ def parse():
     p.add_argument("--precision", default=None, help="fp64 | mixed (default: the headline path)")
     p.add_argument("--config", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-gradient", action="store_true", help="skip the XC nuclear gradient leg")
+    p.add_argument("--profile-gradient", action="store_true",
+                   help="create the raw-grid context of the workload and run one XC nuclear gradient (for ncu)")
     p.add_argument("--cpu-seconds", type=float, default=12.0)
     p.add_argument("--max-chunk-points", type=int, default=0,
                    help="cap on grid points per device chunk (0: sized from free HBM)")
@@ -257,6 +260,28 @@ def keep_orbitals_leg(torch, case, sub, local, args):
                     "the headline value evaluates them in every build"}
 
 
+def gradient_leg(torch, sub, local):
+    """One post-SCF XC nuclear gradient of the geometry (pgxc_xc_gradient:
+    moving grid, Becke weight derivatives; FP64), timed once after one
+    untimed call.  Reported beside the headline; not a step of it."""
+    from pgxc import lib
+    try:
+        ctx = lib.Context(sub, precision="fp64", weighted=False, device=local, screen_threshold=0.0)
+    except lib.PgxcError as e:
+        return {"unavailable": str(e)}
+    try:
+        ctx.xc_gradient()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g, e = ctx.xc_gradient()
+        ms = (time.perf_counter() - t0) * 1e3
+    finally:
+        ctx.close()
+    return {"ms": ms, "E_xc": e, "max_abs_component": float(abs(g).max()), "sum_over_atoms": float(abs(g.sum(0)).max()),
+            "note": "dE_xc/dR of every atom with the grid moving with its atoms and the Becke weights differentiated; "
+                    "host wall clock around one synchronous call (inputs from host memory)"}
+
+
 # ---------------------------------------------------------------------------
 def run_batch(args):
     """The batched workload: 256 seeded molecules of 3-40 atoms (LDA and PBE
@@ -450,6 +475,10 @@ def main():
     prec = args.precision or headline_precision()
     case = cases.config(args.config)
     sub = shard(case, rank, world)
+    if args.profile_gradient:
+        g = gradient_leg(torch, sub, local)
+        print(json.dumps({"profile_gradient": True, **g}), flush=True)
+        return
     fp64_leg = None
     if prec != "fp64" and world == 1 and not args.profile:
         fp64_leg = fp64_comparison(torch, case, sub, local, args)
@@ -600,6 +629,8 @@ def main():
         del dC, docc, dbuf, dham, dsum
         torch.cuda.empty_cache()
         out["keep_orbitals"] = keep_orbitals_leg(torch, case, sub, local, args)
+        if not args.no_gradient:
+            out["xc_gradient"] = gradient_leg(torch, sub, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(case, weights, args.cpu_seconds)
     if rank == 0:

@@ -305,93 +305,112 @@ __global__ void k_grad_host(bool gga, int ispin, int64_t nbas, int64_t ld, int64
 }
 
 // Becke cell function s(mu) = (1 - p(p(p(mu)))) / 2, p(q) = q (3 - q^2) / 2, and ds/dmu
+// Written with round-to-nearest intrinsics (no FMA contraction), so that
+// every call site rounds alike: a factor that is exactly 0 in one pass is 0 in
+// the other, which the leave-one-out products rely on.
 __device__ __forceinline__ void becke_s(double mu, double& s, double& ds) {
-  const double q1 = 0.5 * mu * (3.0 - mu * mu);
-  const double q2 = 0.5 * q1 * (3.0 - q1 * q1);
-  const double q3 = 0.5 * q2 * (3.0 - q2 * q2);
-  s = 0.5 * (1.0 - q3);
+  const double q1 = __dmul_rn(__dmul_rn(0.5, mu), __dsub_rn(3.0, __dmul_rn(mu, mu)));
+  const double q2 = __dmul_rn(__dmul_rn(0.5, q1), __dsub_rn(3.0, __dmul_rn(q1, q1)));
+  const double q3 = __dmul_rn(__dmul_rn(0.5, q2), __dsub_rn(3.0, __dmul_rn(q2, q2)));
+  s = __dmul_rn(0.5, __dsub_rn(1.0, q3));
   ds = -0.5 * (1.5 * (1.0 - q2 * q2)) * (1.5 * (1.0 - q1 * q1)) * (1.5 * (1.0 - mu * mu));
 }
 
-// mu_BC at r, with the reference's pair orientation
-__device__ __forceinline__ double becke_mu(const double* A, int b, int c, const double* rv, double& dB, double& dC,
-                                           double& Rbc) {
-  double t[3];
-  for (int k = 0; k < 3; ++k) t[k] = rv[k] - A[3 * b + k];
-  dB = sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
-  for (int k = 0; k < 3; ++k) t[k] = rv[k] - A[3 * c + k];
-  dC = sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
-  for (int k = 0; k < 3; ++k) t[k] = A[3 * b + k] - A[3 * c + k];
-  Rbc = sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
-  return (dB - dC) / Rbc;
-}
-
-// thread per point; per-atom sums in shared memory (3 natm doubles), then global atomics
-__global__ void k_grad_weights(const double* __restrict__ atoms, int natm, const double* __restrict__ px,
-                               const double* __restrict__ py, const double* __restrict__ pz,
-                               const int* __restrict__ owner, int64_t p0, int64_t nvalid,
-                               const double* __restrict__ ef, double* __restrict__ grad) {
-  extern __shared__ double sm[];
-  double* A = sm;              // 3 natm atom coordinates
-  double* G = sm + 3 * natm;   // 3 natm gradient sums
-  for (int i = threadIdx.x; i < 3 * natm; i += blockDim.x) {
-    A[i] = atoms[i];
-    G[i] = 0.0;
-  }
+// Thread per point.  Pass 1 stores, per atom b, the point's distance d_b and
+// the row of P_b = prod_{c != b} s(mu_bc): the product of its nonzero factors,
+// their zero count and the index of a zero factor (scratch [atom][ld]).  Pass
+// 2 gathers, per atom x, the terms of the pairs (x, y) and (y, x) in
+// registers (no scatter):
+//   dmu_xy/dR_x = -u_x/R - mu r_xy/R^2,  dmu_yx/dR_x = u_x/R + mu r_xy/R^2,
+//   kappa_xy = c_x L_xy s'(mu_xy), c_b = ef (delta_bh - W_h) / Z,
+// L_xy the product of row x without its factor y; the point moves with its
+// host h, which collects kappa_xy (u_x - u_y)/R of every pair.  Each atom's sum
+// is reduced over the warp and added to shared memory, then to grad.
+__global__ void k_grad_weights(const double* __restrict__ atoms, const double* __restrict__ dist, int natm,
+                               const double* __restrict__ px, const double* __restrict__ py,
+                               const double* __restrict__ pz, const int* __restrict__ owner, int64_t p0,
+                               int64_t nvalid, int64_t ld, const double* __restrict__ ef, double* __restrict__ sd,
+                               double* __restrict__ spnz, int* __restrict__ snz, double* __restrict__ grad) {
+  extern __shared__ double G[];  // 3 natm sums of the block
+  for (int i = threadIdx.x; i < 3 * natm; i += blockDim.x) G[i] = 0.0;
   __syncthreads();
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p < nvalid && ef[p] != 0.0) {
-    const double rv[3] = {px[p0 + p], py[p0 + p], pz[p0 + p]};
-    const int h = owner[p0 + p];
-    double Z = 0.0, Ph = 0.0;
+  const bool live = p < nvalid && ef[p] != 0.0;
+  double rv[3] = {0, 0, 0}, e = 0.0, Z = 0.0, Wh = 0.0;
+  int h = 0;
+  if (live) {
+    rv[0] = px[p0 + p]; rv[1] = py[p0 + p]; rv[2] = pz[p0 + p];
+    h = owner[p0 + p];
+    e = ef[p];
     for (int b = 0; b < natm; ++b) {
-      double P = 1.0;
+      const double t0 = rv[0] - atoms[3 * b], t1 = rv[1] - atoms[3 * b + 1], t2 = rv[2] - atoms[3 * b + 2];
+      sd[b * ld + p] = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
+    }
+    double Ph = 0.0;
+    for (int b = 0; b < natm; ++b) {
+      const double db = sd[b * ld + p];
+      double pnz = 1.0;
+      int nz = 0, zc = -1;
       for (int c = 0; c < natm; ++c) {
         if (c == b) continue;
-        double dB, dC, R, s, ds;
-        becke_s(becke_mu(A, b, c, rv, dB, dC, R), s, ds);
-        P *= s;
+        double s, ds;
+        becke_s(__ddiv_rn(__dsub_rn(db, sd[c * ld + p]), dist[b * natm + c]), s, ds);
+        if (s == 0.0) { ++nz; zc = c; }
+        else pnz *= s;
       }
+      spnz[b * ld + p] = pnz;
+      snz[b * ld + p] = nz == 0 ? -1 : (nz == 1 ? zc : -2);  // -1: no zero; c: the one zero; -2: several
+      const double P = nz ? 0.0 : pnz;
       Z += P;
       if (b == h) Ph = P;
     }
-    if (Z > 0.0) {
-      const double Wh = Ph / Z;
-      for (int b = 0; b < natm; ++b) {
-        const double cb = ef[p] * ((b == h ? 1.0 : 0.0) - Wh) / Z;
-        // product of the nonzero factors and their zero count: leave-one-out products
-        double pnz = 1.0;
-        int nz = 0;
-        for (int c = 0; c < natm; ++c) {
-          if (c == b) continue;
-          double dB, dC, R, s, ds;
-          becke_s(becke_mu(A, b, c, rv, dB, dC, R), s, ds);
-          if (s == 0.0) ++nz;
-          else pnz *= s;
-        }
-        if (nz > 1) continue;
-        for (int c = 0; c < natm; ++c) {
-          if (c == b) continue;
-          double dB, dC, R, s, ds;
-          const double mu = becke_mu(A, b, c, rv, dB, dC, R);
-          becke_s(mu, s, ds);
-          double L;
-          if (nz == 0) L = pnz / s;
-          else L = (s == 0.0) ? pnz : 0.0;
-          const double kap = cb * L * ds;
-          if (kap == 0.0) continue;
-          for (int k = 0; k < 3; ++k) {
-            const double ub = dB > 0.0 ? (rv[k] - A[3 * b + k]) / dB : 0.0;
-            const double uc = dC > 0.0 ? (rv[k] - A[3 * c + k]) / dC : 0.0;
-            const double rbc = (A[3 * b + k] - A[3 * c + k]) / (R * R);
-            atomicAdd(&G[3 * h + k], kap * (ub - uc) / R);         // the point moves with its host
-            atomicAdd(&G[3 * b + k], kap * (-ub / R - mu * rbc));
-            atomicAdd(&G[3 * c + k], kap * (uc / R + mu * rbc));
-          }
+    if (Z > 0.0) Wh = Ph / Z;
+  }
+  const bool go = live && Z > 0.0;
+  double gh[3] = {0, 0, 0};
+  const int lane = threadIdx.x & 31;
+  for (int x = 0; x < natm; ++x) {
+    double gx[3] = {0, 0, 0};
+    if (go) {
+      const double dx = sd[x * ld + p];
+      const double cx = e * ((x == h ? 1.0 : 0.0) - Wh) / Z;
+      const double pnx = spnz[x * ld + p];
+      const int zx = snz[x * ld + p];
+      double ux[3];
+      for (int k = 0; k < 3; ++k) ux[k] = dx > 0.0 ? (rv[k] - atoms[3 * x + k]) / dx : 0.0;
+      for (int y = 0; y < natm; ++y) {
+        if (y == x) continue;
+        const double R = dist[x * natm + y];
+        const double dy = sd[y * ld + p];
+        const double mu = __ddiv_rn(__dsub_rn(dx, dy), R);
+        double sxy, dsxy, syx, dsyx;
+        becke_s(mu, sxy, dsxy);
+        becke_s(-mu, syx, dsyx);
+        // leave-one-out products of rows x (without y) and y (without x)
+        const double Lxy = zx == -1 ? (sxy != 0.0 ? pnx / sxy : 0.0) : (zx == y ? pnx : 0.0);
+        const int zy = snz[y * ld + p];
+        const double pny = spnz[y * ld + p];
+        const double Lyx = zy == -1 ? (syx != 0.0 ? pny / syx : 0.0) : (zy == x ? pny : 0.0);
+        const double cy = e * ((y == h ? 1.0 : 0.0) - Wh) / Z;
+        const double kxy = cx * Lxy * dsxy, kyx = cy * Lyx * dsyx;
+        if (kxy == 0.0 && kyx == 0.0) continue;
+        const double iR = 1.0 / R, iR2 = iR * iR;
+        for (int k = 0; k < 3; ++k) {
+          const double rxy = atoms[3 * x + k] - atoms[3 * y + k];
+          const double uy = dy > 0.0 ? (rv[k] - atoms[3 * y + k]) / dy : 0.0;
+          gx[k] += (kyx - kxy) * (ux[k] * iR + mu * rxy * iR2);
+          gh[k] += kxy * (ux[k] - uy) * iR;
         }
       }
     }
+    for (int k = 0; k < 3; ++k)
+      for (int off = 16; off > 0; off >>= 1) gx[k] += __shfl_down_sync(0xffffffffu, gx[k], off);
+    if (lane == 0)
+      for (int k = 0; k < 3; ++k)
+        if (gx[k] != 0.0) atomicAdd(&G[3 * x + k], gx[k]);
   }
+  if (go)
+    for (int k = 0; k < 3; ++k) atomicAdd(&G[3 * h + k], gh[k]);
   __syncthreads();
   for (int i = threadIdx.x; i < 3 * natm; i += blockDim.x)
     if (G[i] != 0.0) atomicAdd(grad + i, G[i]);
@@ -432,12 +451,17 @@ void launch_grad_orbital(bool gga, int ispin, int64_t nbas, int64_t ld, int64_t 
                                                              XY, coef, grad);
 }
 
-void launch_grad_weights(const double* atoms, int natm, const double* px, const double* py, const double* pz,
-                         const int* owner, int64_t p0, int64_t nvalid, const double* ef, double* grad, cudaStream_t st) {
-  const size_t smem = sizeof(double) * 6 * natm;
+void launch_grad_weights(const double* atoms, const double* dist, int natm, const double* px, const double* py,
+                         const double* pz, const int* owner, int64_t p0, int64_t nvalid, int64_t ld, const double* ef,
+                         double* scratch, double* grad, cudaStream_t st) {
+  if (nvalid <= 0) return;
+  const size_t smem = sizeof(double) * 3 * natm;
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_grad_weights, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_grad_weights<<<(unsigned)((nvalid + 127) / 128), 128, smem, st>>>(atoms, natm, px, py, pz, owner, p0, nvalid, ef,
-                                                                       grad);
+  double* sd = scratch;
+  double* spnz = scratch + (size_t)natm * ld;
+  int* snz = (int*)(scratch + (size_t)2 * natm * ld);
+  k_grad_weights<<<(unsigned)((nvalid + 127) / 128), 128, smem, st>>>(atoms, dist, natm, px, py, pz, owner, p0,
+                                                                       nvalid, ld, ef, sd, spnz, snz, grad);
 }
 
 }  // namespace pgxc

@@ -39,8 +39,10 @@ void launch_grad_orbital(bool gga, int ispin, int64_t nbas, int64_t ld, int64_t 
                          const int* fatom, const int* owner, const double* basis, int64_t plane, const double* XY,
                          const double* coef, double* grad, cudaStream_t st);
 
-// The weight term sum_g ef_g dW_host(r_g)/dR over the chunk's points.
-void launch_grad_weights(const double* atoms, int natm, const double* px, const double* py, const double* pz,
-                         const int* owner, int64_t p0, int64_t nvalid, const double* ef, double* grad, cudaStream_t st);
+// The weight term sum_g ef_g dW_host(r_g)/dR over the chunk's points; dist is
+// the natm x natm atom distance matrix, scratch holds 2.5 natm ld doubles.
+void launch_grad_weights(const double* atoms, const double* dist, int natm, const double* px, const double* py,
+                         const double* pz, const int* owner, int64_t p0, int64_t nvalid, int64_t ld, const double* ef,
+                         double* scratch, double* grad, cudaStream_t st);
 
 }  // namespace pgxc

@@ -819,11 +819,12 @@ int pgxc_xc_gradient(pgxc_ctx* c, const double* C, const double* occ, int32_t nb
   std::vector<int> fatom((size_t)nbas);
   for (const DevShell& S : c->shells)
     for (int f = 0; f < (2 * S.l + 1) * S.nrad; ++f) fatom[(size_t)S.f0 + f] = S.atom;
-  // chunk of points: 10 basis planes + 4 ispin X/Y planes of nbas x ld, under ~1.5 GB
-  int64_t ld = 4096;
-  while (ld > 128 && (double)(10 + 4 * ispin) * nbas * ld * 8.0 > 1.5e9) ld /= 2;
+  // chunk of points: 10 basis planes + 4 ispin X/Y planes of nbas x ld, under ~4 GB
+  int64_t ld = 65536;
+  while (ld > 128 && (double)(10 + 4 * ispin) * nbas * ld * 8.0 > 4.0e9) ld /= 2;
   const int64_t plane = (int64_t)nbas * ld;
   double *basis = nullptr, *XY = nullptr, *coef = nullptr, *ef = nullptr, *dgrad = nullptr, *de = nullptr;
+  double* wscr = nullptr;
   int* dfatom = nullptr;
   std::vector<void*> mine;
   auto scratch = [&](void** p, size_t bytes) -> int {
@@ -837,6 +838,7 @@ int pgxc_xc_gradient(pgxc_ctx* c, const double* C, const double* occ, int32_t nb
       (st = scratch((void**)&XY, sizeof(double) * 4 * ispin * plane)) ||
       (st = scratch((void**)&coef, sizeof(double) * 4 * ispin * ld)) || (st = scratch((void**)&ef, sizeof(double) * ld)) ||
       (st = scratch((void**)&dgrad, sizeof(double) * 3 * c->natm)) || (st = scratch((void**)&de, sizeof(double))) ||
+      (st = scratch((void**)&wscr, sizeof(double) * ((size_t)5 * c->natm * ld / 2 + 1))) ||
       (st = scratch((void**)&dfatom, sizeof(int) * nbas))) {
     release();
     return st;
@@ -868,7 +870,7 @@ int pgxc_xc_gradient(pgxc_ctx* c, const double* C, const double* occ, int32_t nb
       if (rc) break;
       launch_grad_points(a.xc, gga, ispin, nbas, ld, p0, nv, a.w, c->d_wraw, basis, plane, XY, coef, ef, de, s);
       launch_grad_orbital(gga, ispin, nbas, ld, p0, nv, dfatom, c->d_owner, basis, plane, XY, coef, dgrad, s);
-      launch_grad_weights(a.atoms, c->natm, a.px, a.py, a.pz, c->d_owner, p0, nv, ef, dgrad, s);
+      launch_grad_weights(a.atoms, c->d_dist, c->natm, a.px, a.py, a.pz, c->d_owner, p0, nv, ld, ef, wscr, dgrad, s);
       if (cudaGetLastError() != cudaSuccess) rc = set_err(c, PGXC_ECUDA, "gradient kernel launch failed");
     }
     if (rc) break;
