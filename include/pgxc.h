@@ -105,10 +105,20 @@ extern "C" {
  * spin (keyword "LB94", modules/xc_cntrl.f90:500-506; baerends94_calc,
  * modules/baerends_module.f90:91-134) */
 #define PGXC_XC_LB94 24
+/* The relativistic keywords (exchange with X_LONGTRANS, speed of light
+ * 137.03604): RVWN = relativistic Slater (x phi0(beta)) + VWN5 + the ec_RLDA
+ * correction, an LDA ("RVWN", modules/xc_cntrl.f90:477-488; relxc.f90);
+ * RBP = Slater + VWN5 + relativistic Becke 88 e_x (phi0 - 1 + phi2 G) +
+ * Perdew 86 ("RBP", :545-558); ECMV92 = Slater + relativistic ECMV92
+ * exchange ("ECMV92", :645-650) */
+#define PGXC_XC_RVWN 25
+#define PGXC_XC_RBP 26
+#define PGXC_XC_ECMV92 27
 /* the largest functional id */
-#define PGXC_XC_LAST PGXC_XC_LB94
-/* nonzero for the GGA keywords (all but the three LDAs) */
-#define PGXC_XC_IS_GGA(id) ((id) != PGXC_XC_VWN && (id) != PGXC_XC_XALPHA && (id) != PGXC_XC_PWLDA)
+#define PGXC_XC_LAST PGXC_XC_ECMV92
+/* nonzero for the GGA keywords (all but the four LDAs) */
+#define PGXC_XC_IS_GGA(id) \
+  ((id) != PGXC_XC_VWN && (id) != PGXC_XC_XALPHA && (id) != PGXC_XC_PWLDA && (id) != PGXC_XC_RVWN)
 
 /* ---- precision modes ------------------------------------------------- */
 #define PGXC_PREC_FP64        0  /* FP64 everywhere (FP64 tensor pipe): the drop-in */

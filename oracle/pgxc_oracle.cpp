@@ -140,6 +140,7 @@ struct GgaPar {
   // fractions of Slater, exchange enhancement, LDA and gradient correlation
   // (frac of xc_functionals, xc_func.f90:284-305): 1 but in the hybrids
   double fx_lda = 1.0, fx_g = 1.0, fc_lda = 1.0, fc_g = 1.0;
+  int rel_g = 0;             // relativistic enhancement term: 1 RB88 set, 2 RECMV92 set
 };
 GgaPar gga_par(int xc) {
   const double pi = PI_EXCH;
@@ -166,6 +167,10 @@ GgaPar gga_par(int xc) {
     case PGXC_XC_PBE0: return {0.804, mu_pbe, 0.066725, GX_PBE, GC_PBE, LC_PW92, 0, 0.75, 0.75, 1.0, 1.0};
     // "LB94" (xc_cntrl.f90:500-506): XAlpha + VWN + the baerends94 potential term
     case PGXC_XC_LB94: return {0, 0, 0, GX_NONE, GC_NONE, LC_VWN, 0};
+    // relativistic keywords (xc_cntrl.f90 "RVWN" :477-488, "RBP" :545-558, "ECMV92" :645-650)
+    case PGXC_XC_RVWN: return {0, 0, 0, GX_NONE, GC_NONE, LC_VWN, 0};
+    case PGXC_XC_RBP: return {0, 0, 0, GX_B88, GC_P86, LC_VWN, 0, 1, 1, 1, 1, 1};
+    case PGXC_XC_ECMV92: return {0, 0, 0, GX_ECMV92, GC_NONE, LC_NONE, 0, 1, 1, 1, 1, 2};
     default: return {0.804, mu_pbe, 0.066725, GX_PBE, GC_PBE, LC_PW92, 0};
   }
 }
@@ -231,6 +236,60 @@ D g_ecmv92(D s2) {
   return nomin / denom;
 }
 
+// ---------------------------------------------------------------------------
+// Relativistic exchange factors (exchange.f90, X_LONGTRANS): rbeta :993-1005
+// (beta = (3 pi^2 n)^(1/3)/c, c = 137.03604, 0 below n = 1e-20), phi0
+// :1008-1098 (1 - (3/2) t4^2, t4 = (eta - arcsinh(b)/b)/b or its series below
+// |b| = 1e-4; 0 at b = 0), phi2 :1100-1143 (longitudinal + transverse pade22 in
+// b^2 with the RB88 or RECMV92 sets); the relativistic LDA correlation
+// correction ec_RLDA, relxc.f90:221-283 (0.25 cutoff form).
+// ---------------------------------------------------------------------------
+const double C_LIGHT = 137.03604;
+D rel_beta(D n) {
+  const double pi = 3.14159265358979324;
+  if (n.v >= 1.0e-20) return dpow(3.0 * pi * pi * n, 1.0 / 3.0) / C_LIGHT;
+  return cst(0.0);
+}
+D rel_arcsinh(D x) {  // autodiff2.f90:791-820
+  if (std::fabs(x.v) >= 1.0e-4) return dlog(x + dsqrt(1.0 + x * x));
+  return x - (1.0 / 6.0) * x * x * x + (3.0 / 40.0) * x * x * x * x * x;
+}
+D rel_phi0(D b) {
+  if (b.v == 0.0) return cst(0.0);
+  D t4;
+  if (std::fabs(b.v) > 1.0e-4) {
+    D eta = dsqrt(1.0 + b * b);
+    t4 = (eta - rel_arcsinh(b) / b) / b;
+  } else {
+    D b2 = b * b, b4 = b2 * b2;
+    t4 = (2.0 / 3.0) * b + (-(1.0 / 5.0)) * b * b2 + (3.0 / 28.0) * b * b4;
+  }
+  return 1.0 - 1.5 * t4 * t4;
+}
+D pade22(D x, double a0, double a1, double a2, double b0, double b1, double b2) {
+  return (a0 + x * (a1 + x * a2)) / (b0 + x * (b1 + x * b2));
+}
+D rel_phi2(int set, D b) {
+  D x = b * b;
+  if (set == 2)
+    return pade22(x, 1.0, 2.21259, 0.669152, 1.0, 1.32998, 0.794803) +
+           pade22(x, 0.0, 3.48754, 0.218599, 1.0, 1.15417, 0.015802);
+  return pade22(x, 1.0, 2.20848, 0.668684, 1.0, 1.33075, 0.795105) +
+         pade22(x, 0.0, 3.48638, 0.614753, 1.0, 1.32260, 0.101805);
+}
+D ec_rlda(D n) {
+  const double pi = 3.14159265358979324;
+  if (n.v < 1.0e-7) return cst(0.0);
+  const double a0 = -0.16797, b0 = 0.149530, c0 = -0.007568, d0 = 0.0504295, c1 = -0.007217, c2 = 0.0064572,
+               c3 = -0.005352, d1 = 0.0995769, d2 = 0.110576, d3 = 0.0136740, d4 = 0.0311479;
+  const double AA = -0.2670592864, BB = 0.5321072256;
+  D b = dpow(3.0 * pi * pi * n, 1.0 / 3.0) / C_LIGHT;
+  if (b.v < 0.25) return AA * dipow(b, 3) + BB * dipow(b, 4);
+  D num = c3 * dipow(b, 3) + c2 * dipow(b, 2) + c1 * b + c0;
+  D den = d4 * dipow(b, 4) + d3 * dipow(b, 3) + d2 * dipow(b, 2) + d1 * b + d0;
+  return a0 * b + b0 + num / den;
+}
+
 void x_gga_pbe(const GgaPar& P, double n, double gam, double& F, double& dFdn, double& dFdg) {
   if (P.gx == GX_NONE) return;
   const double pi = PI_EXCH;
@@ -253,6 +312,16 @@ void x_gga_pbe(const GgaPar& P, double n, double gam, double& F, double& dFdn, d
         : P.gx == GX_VT84  ? g_vmt(mu, P.alpha, s2, true)
         : P.gx == GX_ECMV92 ? g_ecmv92(s2)
                            : kappa * mu * s2 / (kappa + mu * s2);
+  if (P.rel_g) {
+    // x_gga with relativity (exchange.f90:418-438): e_x (phi0 - 1 + phi2 G)
+    D bn = rel_beta(var(0, n));
+    D p0 = rel_phi0(bn), p2 = rel_phi2(P.rel_g, bn);
+    const double fac = p0.v - 1.0 + p2.v * G.v;
+    F += ex.v * fac;
+    dFdn += ex.d[0] * fac + ex.v * (p0.d[0] + p2.d[0] * G.v + p2.v * G.d[0] * s2_r);
+    dFdg += ex.v * p2.v * G.d[0] * s2_g;
+    return;
+  }
   F += ex.v * G.v;
   dFdn += ex.d[0] * G.v + ex.v * G.d[0] * s2_r;
   dFdg += ex.v * G.d[0] * s2_g;
@@ -620,13 +689,15 @@ void functional_point(int xc, int ispin, const double* rho, const double* gam,
     fg[0] += a * pg[0]; fg[1] += a * pg[1]; fg[2] += a * pg[2];
   };
   // Slater exchange (exchange_lda, exchange.f90:511-565)
+  // "RVWN": RXAlpha, the Slater term times phi0(beta) (x_lda with X_LONGTRANS, :567-601)
+  auto xlda = [&](D n) { return xc == PGXC_XC_RVWN ? x_lda(n) * rel_phi0(rel_beta(n)) : x_lda(n); };
   clear();
   if (ispin == 1) {
-    D e = x_lda(var(0, rho[0]));
+    D e = xlda(var(0, rho[0]));
     pf += e.v; pr[0] += e.d[0];
   } else {
     for (int s = 0; s < 2; ++s) {
-      D e = x_lda(var(0, 2.0 * rho[s]));
+      D e = xlda(var(0, 2.0 * rho[s]));
       pf += e.v / 2.0; pr[s] += e.d[0];
     }
   }
@@ -647,6 +718,11 @@ void functional_point(int xc, int ispin, const double* rho, const double* gam,
   pf = ec.v; pr[0] = ec.d[0];
   if (ispin == 2) pr[1] = ec.d[1];
   add(P.fc_lda);
+  if (xc == PGXC_XC_RVWN) {  // rel_vwn_calc (relxc.f90:128-160), of the total density
+    D er = ec_rlda(ispin == 1 ? var(0, rho[0]) : var(0, rho[0]) + var(1, rho[1]));
+    f += er.v; fr[0] += er.d[0];
+    if (ispin == 2) fr[1] += er.d[1];
+  }
   if (!PGXC_XC_IS_GGA(xc)) return;
   // GGA exchange enhancement (exchange_gga, exchange.f90:206-292)
   clear();

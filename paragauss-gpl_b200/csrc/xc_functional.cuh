@@ -62,6 +62,12 @@ struct XcConst {
   double fx_lda, fx_g, fc_lda, fc_g;
   int lb94;             // 1: add the LB94 potential correction ("LB94")
   double lb94_two13;    // 2^(1/3)
+  // relativistic exchange (exchange.f90 x_lda / x_gga with X_LONGTRANS):
+  // rel_lda: Slater times phi0(beta) ("RVWN"); rel_g: the enhancement term
+  // e_x (phi0 - 1 + phi2 G) with the Pade set of Becke 88 (1, "RBP") or of
+  // ECMV92 (2, "ECMV92"); rvwn: add ec_RLDA (relxc.f90); rel_c: speed of light
+  int rel_lda, rel_g, rvwn;
+  double rel_c, rel_3pi2;
   // PBE correlation
   double pbe_fi;        // (0.5^(2/3)+0.5^(2/3)) * (1/2^(1/3))
   double pbe_ct;        // pi/(16 (3 pi^2)^(1/3))
@@ -145,6 +151,23 @@ __host__ inline XcConst make_xc_const(int functional = PGXC_XC_PBE) {
   c.fx_lda = c.fx_g = c.fc_lda = c.fc_g = 1.0;
   c.lb94 = f == PGXC_XC_LB94 ? 1 : 0;
   c.lb94_two13 = std::pow(2.0, 1.0 / 3.0);
+  c.rel_c = 137.03604;  // constants.f90 SPEED_OF_LIGHT
+  c.rel_3pi2 = 3.0 * 3.14159265358979324 * 3.14159265358979324;
+  c.rel_lda = f == PGXC_XC_RVWN ? 1 : 0;
+  c.rvwn = f == PGXC_XC_RVWN ? 1 : 0;
+  c.rel_g = f == PGXC_XC_RBP ? 1 : f == PGXC_XC_ECMV92 ? 2 : 0;
+  if (f == PGXC_XC_RVWN) {  // "RVWN": RXAlpha + VWN + rel_vwn_calc (xc_cntrl.f90:477-488)
+    c.lc = LC_VWN;
+    c.cg = CG_NONE;
+  } else if (f == PGXC_XC_RBP) {  // "RBP": XAlpha + VWN + RBecke88 + Perdew (:545-558)
+    c.xg = XG_B88;
+    c.cg = CG_P86;
+    c.lc = LC_VWN;
+  } else if (f == PGXC_XC_ECMV92) {  // "ECMV92": XAlpha + ECMV92 with X_LONGTRANS (:645-650)
+    c.xg = XG_ECMV92;
+    c.cg = CG_NONE;
+    c.lc = LC_NONE;
+  }
   if (c.lb94) {  // "LB94": XAlpha + VWN + baerends94 (a potential term only)
     c.xg = XG_NONE;
     c.cg = CG_NONE;
@@ -204,12 +227,98 @@ __device__ __forceinline__ void pw92_ecu(double rs, double& E, double& dE) {
   dE = -2.0 * a * a1 * Q2 - Q0 * dQ1 / (Q1 * (Q1 + 1.0));
 }
 
-// Slater exchange, closed shell: x_lda with rho > 0 guard, times K.fx_lda.
+// Relativistic beta = (3 pi^2 n)^(1/3) / c (rbeta, exchange.f90:993-1005; 0 below
+// n = 1e-20) and d beta / dn.
+__device__ __forceinline__ void rel_beta(const XcConst& K, double n, double& b, double& db) {
+  if (n >= 1.0e-20) {
+    b = pow(K.rel_3pi2 * n, 1.0 / 3.0) / K.rel_c;
+    db = b / (3.0 * n);
+  } else {
+    b = 0.0;
+    db = 0.0;
+  }
+}
+
+// phi0 for X_LONGTRANS: 1 - (3/2) t4^2, t4 = (eta - arcsinh(b)/b)/b,
+// eta = sqrt(1 + b^2), its series 2b/3 - b^3/5 + 3b^5/28 below |b| = 1e-4, and 0
+// at b = 0 (phi0, exchange.f90:1008-1098); d phi0 / db.
+__device__ __forceinline__ void rel_phi0(double b, double& phi, double& dphi) {
+  if (b == 0.0) {
+    phi = 0.0;
+    dphi = 0.0;
+    return;
+  }
+  double t4, dt4;
+  if (fabs(b) > 1.0e-4) {
+    const double eta = sqrt(1.0 + b * b);
+    const double ash = log(b + eta);  // arcsinh, autodiff2.f90:791-820 (|b| >= 1e-4)
+    t4 = (eta - ash / b) / b;
+    dt4 = -2.0 / (eta * b * b) + 2.0 * ash / (b * b * b);
+  } else {
+    const double b2 = b * b, b4 = b2 * b2;
+    t4 = (2.0 / 3.0) * b + (-(1.0 / 5.0) * b * b2) + (3.0 / 28.0) * b * b4;
+    dt4 = 2.0 / 3.0 - (3.0 / 5.0) * b2 + (15.0 / 28.0) * b4;
+  }
+  phi = 1.0 - 1.5 * t4 * t4;
+  dphi = -3.0 * t4 * dt4;
+}
+
+// phi2 for X_LONGTRANS: the longitudinal plus the transverse 2/2 Pade in b^2,
+// the RB88 set (set 1) or the RECMV92 set (set 2) (phi2 and pade22,
+// exchange.f90:1100-1159); d phi2 / db.
+__device__ __forceinline__ void rel_phi2(int set, double b, double& phi, double& dphi) {
+  const double aL1 = set == 1 ? 2.20848 : 2.21259, aL2 = set == 1 ? 0.668684 : 0.669152;
+  const double bL1 = set == 1 ? 1.33075 : 1.32998, bL2 = set == 1 ? 0.795105 : 0.794803;
+  const double aT1 = set == 1 ? 3.48638 : 3.48754, aT2 = set == 1 ? 0.614753 : 0.218599;
+  const double bT1 = set == 1 ? 1.32260 : 1.15417, bT2 = set == 1 ? 0.101805 : 0.015802;
+  const double x = b * b;
+  const double nL = 1.0 + x * (aL1 + x * aL2), dL = 1.0 + x * (bL1 + x * bL2);
+  const double nT = 0.0 + x * (aT1 + x * aT2), dT = 1.0 + x * (bT1 + x * bT2);
+  phi = nL / dL + nT / dT;
+  const double dnL = aL1 + 2.0 * aL2 * x, ddL = bL1 + 2.0 * bL2 * x;
+  const double dnT = aT1 + 2.0 * aT2 * x, ddT = bT1 + 2.0 * bT2 * x;
+  dphi = ((dnL * dL - nL * ddL) / (dL * dL) + (dnT * dT - nT * ddT) / (dT * dT)) * 2.0 * b;
+}
+
+// Slater exchange, closed shell: x_lda with rho > 0 guard, times phi0(beta)
+// when relativistic (K.rel_lda), times K.fx_lda.
 __device__ __forceinline__ void slater(const XcConst& K, double n, double& f, double& fr) {
   if (n > 0.0) {
     const double c = cbrt(n);
-    f += K.fx_lda * (K.xalpha * n * c);
-    fr += K.fx_lda * ((4.0 / 3.0) * K.xalpha * c);
+    double e = K.xalpha * n * c, de = (4.0 / 3.0) * K.xalpha * c;
+    if (K.rel_lda) {
+      double b, db, ph, dph;
+      rel_beta(K, n, b, db);
+      rel_phi0(b, ph, dph);
+      de = de * ph + e * dph * db;
+      e = e * ph;
+    }
+    f += K.fx_lda * e;
+    fr += K.fx_lda * de;
+  }
+}
+
+// Relativistic LDA correlation correction ec_RLDA(n) and its n derivative
+// (relxc.f90:221-283, the 0.25 cutoff form); 0 below n = 1e-7.  It is added to
+// the energy density as it stands.
+__device__ __forceinline__ void rel_vwn(const XcConst& K, double n, double& e, double& de) {
+  e = 0.0;
+  de = 0.0;
+  if (n < 1.0e-7) return;
+  const double a0 = -0.16797, b0 = 0.149530, c0 = -0.007568, d0 = 0.0504295, c1 = -0.007217, c2 = 0.0064572,
+               c3 = -0.005352, d1 = 0.0995769, d2 = 0.110576, d3 = 0.0136740, d4 = 0.0311479;
+  const double AA = -0.2670592864, BB = 0.5321072256;
+  const double b = pow(K.rel_3pi2 * n, 1.0 / 3.0) / K.rel_c;
+  if (b < 0.25) {
+    e = AA * b * b * b + BB * b * b * b * b;
+    de = (3.0 * AA * b * b + 4.0 * BB * b * b * b) * b / (3.0 * n);
+  } else {
+    const double num = c3 * b * b * b + c2 * b * b + c1 * b + c0;
+    const double den = d4 * b * b * b * b + d3 * b * b * b + d2 * b * b + d1 * b + d0;
+    const double dnum = 3.0 * c3 * b * b + 2.0 * c2 * b + c1;
+    const double dden = 4.0 * d4 * b * b * b + 3.0 * d3 * b * b + 2.0 * d2 * b + d1;
+    e = a0 * b + b0 + num / den;
+    de = (a0 + (den * dnum - num * dden) / (den * den)) * b / (3.0 * n);
   }
 }
 
@@ -239,6 +348,12 @@ __device__ __forceinline__ void xc_vwn(const XcConst& K, double n, double& f, do
   const double ecpara = ap * e;
   f += K.fc_lda * (ecpara * S);
   fr += K.fc_lda * (ecpara - ap * de * X / 6.0);   // dX/dn = -X/(6S)
+  if (K.rvwn) {  // rel_vwn_calc (relxc.f90:128-160)
+    double er, der;
+    rel_vwn(K, n, er, der);
+    f += er;
+    fr += der;
+  }
 }
 
 // GGA exchange enhancement of the closed-shell functional e(n, g): e_x G(s^2),
@@ -339,6 +454,19 @@ __device__ __forceinline__ void pbe_x(const XcConst& K, double n, double g, doub
     const double den = kappa + mu * s2;
     G = kappa * mu * s2 / den;
     Gs = kappa * kappa * mu / (den * den);
+  }
+  if (K.rel_g) {
+    // x_gga with relativity (exchange.f90:418-438): e_x (phi0 - 1 + phi2 G), the
+    // -1 because XAlpha is on
+    double b, db, p0, dp0, p2, dp2;
+    rel_beta(K, n, b, db);
+    rel_phi0(b, p0, dp0);
+    rel_phi2(K.rel_g, b, p2, dp2);
+    const double fac = p0 - 1.0 + p2 * G;
+    f += K.fx_g * (ex * fac);
+    fr += K.fx_g * (exr * fac + ex * ((dp0 + dp2 * G) * db + p2 * Gs * s2r));
+    fg += K.fx_g * (ex * p2 * Gs * s2g);
+    return;
   }
   f += K.fx_g * (ex * G);
   fr += K.fx_g * (exr * G + ex * Gs * s2r);
@@ -903,6 +1031,13 @@ __device__ __forceinline__ void xc_open(const XcConst& K, const double (&rho)[2]
   f += K.fc_lda * ec.v;
   fr[0] += K.fc_lda * ec.d[0];
   fr[1] += K.fc_lda * ec.d[1];
+  if (K.rvwn) {  // rel_vwn_calc: a function of the total density
+    double er, der;
+    rel_vwn(K, rho[0] + rho[1], er, der);
+    f += er;
+    fr[0] += der;
+    fr[1] += der;
+  }
   if constexpr (GGA) xc_open_gga(K, rho, gam, na, nb, ec, f, fr, fg);
 }
 

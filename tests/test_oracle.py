@@ -484,3 +484,39 @@ def test_hcth_published_form(xc):
     # zero gradient: c_0 times each LDA piece
     got0 = O.functionals(xc, 2, np.stack([ra, rb], 1), np.zeros((10, 3)))[0]
     np.testing.assert_allclose(got0, cx[0] * (xs(ra) + xs(rb)) + css[0] * (eaa + ebb) + cab[0] * eab, rtol=1e-11)
+
+
+def test_relativistic_exchange_published_form():
+    """The relativistic keywords against the MacDonald-Vosko form of the
+    relativistic LDA exchange, phi0(b) = 1 - (3/2) [(eta - asinh(b)/b)/b]^2,
+    eta = sqrt(1 + b^2), b = (3 pi^2 n)^(1/3)/c, c = 137.03604, and the Pade
+    corrections phi2 of the GGA term: RVWN - VWN = e_x (phi0 - 1) + ec_RLDA,
+    RBP - BP86 = e_x (phi0 - 1 + (phi2_B88 - 1) G_B88),
+    ECMV92 - NRECMV92 = e_x (phi0 - 1 + (phi2_92 - 1) G_92)."""
+    rng = np.random.default_rng(53)
+    rho = 10 ** rng.uniform(-2, 4, 12)       # up to core densities, where beta matters
+    gam = rho ** (8 / 3) * 10 ** rng.uniform(-4, 0.5, 12)
+    pi = 3.14159265358979324
+    ex = -(3 / 4) * (3 / pi) ** (1 / 3) * rho ** (4 / 3)
+    b = (3 * pi ** 2 * rho) ** (1 / 3) / 137.03604
+    eta = np.sqrt(1 + b * b)
+    phi0 = 1 - 1.5 * ((eta - np.arcsinh(b) / b) / b) ** 2
+    x = b * b
+    pade = lambda a, c: (a[0] + x * (a[1] + x * a[2])) / (c[0] + x * (c[1] + x * c[2]))
+    phi2_88 = pade((1, 2.20848, 0.668684), (1, 1.33075, 0.795105)) + pade((0, 3.48638, 0.614753), (1, 1.32260, 0.101805))
+    phi2_92 = pade((1, 2.21259, 0.669152), (1, 1.32998, 0.794803)) + pade((0, 3.48754, 0.218599), (1, 1.15417, 0.015802))
+    s2 = gam / (4 * (3 * pi ** 2) ** (2 / 3) * rho ** (8 / 3))
+    q = gam / 4
+    g88 = (_b88_published(rho / 2, rho / 2, q, q) - ex) / ex
+    g92 = (0.3402 * s2 + 5.9955 * s2 ** 2) / (1 + 27.5026 * s2 + 5.7728 * s2 ** 2)
+    a0, b0, c0, d0 = -0.16797, 0.149530, -0.007568, 0.0504295
+    c1, c2, c3, d1, d2, d3, d4 = -0.007217, 0.0064572, -0.005352, 0.0995769, 0.110576, 0.0136740, 0.0311479
+    ecr = np.where(b < 0.25, -0.2670592864 * b ** 3 + 0.5321072256 * b ** 4,
+                   a0 * b + b0 + (c3 * b ** 3 + c2 * b ** 2 + c1 * b + c0)
+                   / (d4 * b ** 4 + d3 * b ** 3 + d2 * b ** 2 + d1 * b + d0))
+    ecr = np.where(rho < 1e-7, 0.0, ecr)
+    F = lambda xc, g=None: O.functionals(xc, 1, rho, g)[0]
+    for got, want in ((F("RVWN") - F("VWN"), ex * (phi0 - 1) + ecr),
+                      (F("RBP", gam) - F("BP86", gam), ex * (phi0 - 1 + (phi2_88 - 1) * g88)),
+                      (F("ECMV92", gam) - F("NRECMV92", gam), ex * (phi0 - 1 + (phi2_92 - 1) * g92))):
+        assert np.all(np.abs(got - want) <= 1e-9 * np.abs(want) + 1e-12 * np.abs(ex)), (got, want)
