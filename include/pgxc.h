@@ -114,8 +114,13 @@ extern "C" {
 #define PGXC_XC_RVWN 25
 #define PGXC_XC_RBP 26
 #define PGXC_XC_ECMV92 27
+/* RPW91 = PW92 + relativistic PW91 exchange e_x (phi0 - 1 + phi2 G_PW91)
+ * (no Slater term: the keyword turns XAlpha off) + PW91 correlation H +
+ * phi_c(n) times the H of pw91c_calc ("RPW91", modules/xc_cntrl.f90:626-636;
+ * xc_func.f90:436-446; relxc.f90 rpw91c_calc :162-218) */
+#define PGXC_XC_RPW91 28
 /* the largest functional id */
-#define PGXC_XC_LAST PGXC_XC_ECMV92
+#define PGXC_XC_LAST PGXC_XC_RPW91
 /* nonzero for the GGA keywords (all but the four LDAs) */
 #define PGXC_XC_IS_GGA(id) \
   ((id) != PGXC_XC_VWN && (id) != PGXC_XC_XALPHA && (id) != PGXC_XC_PWLDA && (id) != PGXC_XC_RVWN)

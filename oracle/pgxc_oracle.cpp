@@ -141,6 +141,7 @@ struct GgaPar {
   // (frac of xc_functionals, xc_func.f90:284-305): 1 but in the hybrids
   double fx_lda = 1.0, fx_g = 1.0, fc_lda = 1.0, fc_g = 1.0;
   int rel_g = 0;             // relativistic enhancement term: 1 RB88 set, 2 RECMV92 set
+  int rpw91c = 0;            // "RPW91": phi_c times the H of pw91c_calc added (relxc.f90:162-218)
 };
 GgaPar gga_par(int xc) {
   const double pi = PI_EXCH;
@@ -171,6 +172,9 @@ GgaPar gga_par(int xc) {
     case PGXC_XC_RVWN: return {0, 0, 0, GX_NONE, GC_NONE, LC_VWN, 0};
     case PGXC_XC_RBP: return {0, 0, 0, GX_B88, GC_P86, LC_VWN, 0, 1, 1, 1, 1, 1};
     case PGXC_XC_ECMV92: return {0, 0, 0, GX_ECMV92, GC_NONE, LC_NONE, 0, 1, 1, 1, 1, 2};
+    // "RPW91" (:626-636): pwldac + rperdewwang91x (X_PW91 + X_LONGTRANS, no
+    // XAlpha) + perdewwang91c + rperdewwang91c
+    case PGXC_XC_RPW91: return {0, 0, 0, GX_PW91, GC_PW91, LC_PW92, 0, 0, 1, 1, 1, 1, 1};
     default: return {0.804, mu_pbe, 0.066725, GX_PBE, GC_PBE, LC_PW92, 0};
   }
 }
@@ -489,6 +493,101 @@ D c_pw91(D na, D nb, D gm, D ec) {
 }
 
 // ---------------------------------------------------------------------------
+// The PW91 correlation H0 + H1 of the older routine pw91c_calc
+// (modules/perdew_wang_module.f90:112-490, not revised), which the "RPW91"
+// keyword runs a second time before scaling it (xc_func.f90:436-446).  Its
+// closed-form derivatives are restated as written: n is floored at 1e-50,
+// 1 +- zeta at 1e-25, exp(.) - 1 of A at 1e-50, and dt/dgamma has 1e-50 added
+// to its denominator.  Open shell, dH1/drs lacks the g^3 factor of H1
+// (:365-366).  ec, ecr: the LDA correlation per volume and its density
+// derivatives (pw_ldac).  Returns n H, dF/drho_s, dF/dgamma_* (ispin 1: one
+// of each).
+// ---------------------------------------------------------------------------
+void pw91c_old(int ispin, const double* rho, const double* gam, double ec, const double* ecr, double& f,
+               double* fr, double* fg) {
+  const double pi = 3.141592653589793240, deps = 1.0e-50;
+  const double Cc0 = 0.004235, Cx = -0.001667, al = 0.09, Cx37 = Cx * 3.0 / 7.0;
+  const double a_rg = 23.266, b_rg = 7.389e-3, c_rg = 8.723, d_rg = 0.472, e_rg = 2.568;
+  const double rs_fact = std::pow(3.0 / (4.0 * pi), 1.0 / 3.0);
+  const double h1_fact = (16.0 / pi) * std::pow(3.0 * pi * pi, 1.0 / 3.0);
+  const double bpw = h1_fact * Cc0, h0_fact = bpw * bpw / (2.0 * al), apf = 2.0 * al / bpw;
+  const double t_fact = 1.0 / (2.0 * std::sqrt(std::pow(192.0 / pi, 1.0 / 3.0)));
+  const double e_fact = 100.0 * 4.0 / (pi * std::pow(3.0 * pi * pi, 1.0 / 3.0));
+  const bool open = ispin == 2;
+  double n = open ? rho[0] + rho[1] : rho[0];
+  if (n < deps) n = deps;
+  const double eps = ec / n;
+  const double rt = std::pow(n, 1.0 / 3.0), rs = rs_fact / rt, rs2 = rs * rs;
+  double pa = 1.0, pb = 1.0, za = 0.0, zb = 0.0;
+  if (open) {
+    const double zeta = (rho[0] - rho[1]) / n;
+    pa = std::max(1.0 + zeta, std::sqrt(deps));
+    pb = std::max(1.0 - zeta, std::sqrt(deps));
+    za = pb / n;
+    zb = -pa / n;
+  }
+  const double g = open ? 0.5 * (std::pow(pa, 2.0 / 3.0) + std::pow(pb, 2.0 / 3.0)) : 1.0;
+  const double g2 = g * g, g3 = g2 * g, g4 = g2 * g2;
+  const double gr = std::sqrt(open ? gam[0] + gam[1] + 2.0 * gam[2] : gam[0]);
+  const double t = t_fact * gr / (std::sqrt(rt) * n) / g, t2 = t * t;
+  const double t_g = 0.5 * t_fact / (std::sqrt(rt) * n * gr + deps) / g;
+  const double t_n = -(7.0 / 6.0) * t / n, t_gi = -t / g;
+  const double ex0 = -2.0 * al * eps / (bpw * bpw) / g3;
+  const double V = std::exp(ex0);
+  double Aden = V - 1.0;
+  if (Aden < deps) Aden = deps;
+  const double A = apf / Aden, At2 = A * t2, OA = 1.0 + At2;
+  const double den = (1.0 + (apf + A) * t2 * OA) * (OA + At2 * At2);
+  const double h0 = g3 * h0_fact * std::log(1.0 + apf * (t2 + At2 * t2) / (OA + At2 * At2));
+  const double F0_t = g3 * n * 2.0 * bpw * t * (OA + At2) / den;
+  const double h0_a = -g3 * bpw * t2 * t2 * t2 * A * (2.0 + At2) / den;
+  const double F0_g = F0_t * t_g;
+  // H1 (Rasolt-Geldart Cc(rs))
+  const double ex1 = -g4 * e_fact * t2 / rt, E1 = std::exp(ex1);
+  const double rn = e_rg + a_rg * rs + b_rg * rs2, rd = 1.0 + c_rg * rs + d_rg * rs2 + 10.0 * b_rg * rs2 * rs;
+  const double K1 = h1_fact * (1.0e-3 * rn / rd - Cx - Cc0 - Cx37);
+  const double h1 = g3 * K1 * t2 * E1;
+  const double h1_t = g3 * K1 * E1 * 2.0 * t * (1.0 + ex1);
+  const double rn1 = a_rg + 2.0 * b_rg * rs, rd1 = c_rg + 2.0 * d_rg * rs + 30.0 * b_rg * rs2;
+  const double h_rs = h1_fact * t2 * E1 * 1.0e-3 * (rn1 * rd - rd1 * rn) / (rd * rd);  // no g^3
+  const double rs_n = -rs / (3.0 * n);
+  const double h1_dn = g4 * h1 * t2 * e_fact / (3.0 * n * rt);
+  const double F1_g = n * h1_t * t_g;
+  f = (h0 + h1) * n;
+  if (!open) {
+    const double A_n = (apf * apf / bpw) * V / (Aden * Aden) * (ecr[0] - eps) / n;
+    fr[0] = h0 + n * h0_a * A_n + F0_t * t_n + h1 + n * (h_rs * rs_n + h1_t * t_n + h1_dn);
+    fg[0] = F0_g + F1_g;
+    return;
+  }
+  const double A_gi = 3.0 * (apf / (Aden * Aden)) * V * ex0 * g3 / g4;
+  const double dg = (1.0 / 3.0) * (1.0 / std::pow(pa, 1.0 / 3.0) - 1.0 / std::pow(pb, 1.0 / 3.0));
+  const double h0_t = F0_t / n, h0_gi = 3.0 * g2 / g3 * h0;
+  const double h1_gi = 3.0 * g2 / g3 * h1 + h1 * (4.0 * g3 / g4) * ex1;
+  const double zs[2] = {za, zb};
+  for (int s = 0; s < 2; ++s) {
+    const double A_ns = (apf * apf / (bpw * g3)) * V / (Aden * Aden) * (ecr[s] - eps) / n + A_gi * dg * zs[s];
+    const double h0_ns = h0_gi * dg * zs[s] + h0_a * A_ns + h0_t * (t_n + t_gi * dg * zs[s]);
+    const double h1_ns = h1_t * t_gi * dg * zs[s] + h1_t * t_n + h1_gi * dg * zs[s] + h_rs * rs_n + h1_dn;
+    fr[s] = h0 + n * h0_ns + h1 + n * h1_ns;
+  }
+  fg[0] = fg[1] = F0_g + F1_g;
+  fg[2] = 2.0 * (F0_g + F1_g);
+}
+
+// phi_c(b) = (1 + a1 b^2 + a2 b^4) / (1 + b1 b^2 + b2 b^4), b = (3 pi^2 n)^(1/3)/c,
+// n floored at 1e-50, and its n derivative (rpw91c_calc, relxc.f90:162-218).
+void rpw91_phi(double n, double& phi, double& dphi) {
+  const double a1 = 1.9407, a2 = 0.14435, b1 = 0.28412, b2 = 0.004723, pi = 3.14159265358979324;
+  if (n < 1.0e-50) n = 1.0e-50;
+  const double b = std::pow(3.0 * pi * pi * n, 1.0 / 3.0) / C_LIGHT, bb = b * b;
+  const double num = 1.0 + a1 * bb + a2 * bb * bb, den = 1.0 + b1 * bb + b2 * bb * bb;
+  const double dnum = 2.0 * a1 * b + 4.0 * a2 * bb * b, dden = 2.0 * b1 * b + 4.0 * b2 * bb * b;
+  phi = num / den;
+  dphi = (den * dnum - num * dden) * b / (3.0 * n * den * den);
+}
+
+// ---------------------------------------------------------------------------
 // LYP correlation: lyp_corr (modules/lyp.f90, parameter set 1: a = 0.04918,
 // b = 0.132, c = 0.2533, d = 0.349, e = 3/10 (3 pi^2)^(2/3) as its literal).
 // F is linear in gaa, gbb, gab: returns F with derivatives in (ra, rb) and
@@ -791,6 +890,19 @@ void functional_point(int xc, int ispin, const double* rho, const double* gam,
     pg[0] += c.d[2]; pg[1] += c.d[2]; pg[2] += 2.0 * c.d[2];
   }
   add(P.fc_g);
+  if (P.rpw91c) {
+    // xc_rperdewwang91c (xc_func.f90:436-446): pw91c_calc into a zeroed
+    // contribution, then rpw91c_calc scales it by phi_c and adds to dF/drho
+    // the already scaled F times dphi_c/dn (relxc.f90:190-193, 206-209)
+    const double ecr[2] = {ec.d[0], ispin == 2 ? ec.d[1] : 0.0};
+    double h = 0.0, hr[2] = {0.0, 0.0}, hg[3] = {0.0, 0.0, 0.0}, phi, dphi;
+    pw91c_old(ispin, rho, gam, ec.v, ecr, h, hr, hg);
+    rpw91_phi(ispin == 2 ? rho[0] + rho[1] : rho[0], phi, dphi);
+    const double hs = h * phi;
+    f += hs;
+    for (int s = 0; s < ispin; ++s) fr[s] += hr[s] * phi + hs * dphi;
+    for (int k = 0; k < (ispin == 2 ? 3 : 1); ++k) fg[k] += hg[k] * phi;
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -68,6 +68,8 @@ struct XcConst {
   // ECMV92 (2, "ECMV92"); rvwn: add ec_RLDA (relxc.f90); rel_c: speed of light
   int rel_lda, rel_g, rvwn;
   double rel_c, rel_3pi2;
+  // rpw91c: "RPW91" adds phi_c(n) times the H of pw91c_calc (relxc.f90:162-218)
+  int rpw91c;
   // PBE correlation
   double pbe_fi;        // (0.5^(2/3)+0.5^(2/3)) * (1/2^(1/3))
   double pbe_ct;        // pi/(16 (3 pi^2)^(1/3))
@@ -155,7 +157,8 @@ __host__ inline XcConst make_xc_const(int functional = PGXC_XC_PBE) {
   c.rel_3pi2 = 3.0 * 3.14159265358979324 * 3.14159265358979324;
   c.rel_lda = f == PGXC_XC_RVWN ? 1 : 0;
   c.rvwn = f == PGXC_XC_RVWN ? 1 : 0;
-  c.rel_g = f == PGXC_XC_RBP ? 1 : f == PGXC_XC_ECMV92 ? 2 : 0;
+  c.rel_g = (f == PGXC_XC_RBP || f == PGXC_XC_RPW91) ? 1 : f == PGXC_XC_ECMV92 ? 2 : 0;
+  c.rpw91c = f == PGXC_XC_RPW91 ? 1 : 0;
   if (f == PGXC_XC_RVWN) {  // "RVWN": RXAlpha + VWN + rel_vwn_calc (xc_cntrl.f90:477-488)
     c.lc = LC_VWN;
     c.cg = CG_NONE;
@@ -163,6 +166,11 @@ __host__ inline XcConst make_xc_const(int functional = PGXC_XC_PBE) {
     c.xg = XG_B88;
     c.cg = CG_P86;
     c.lc = LC_VWN;
+  } else if (f == PGXC_XC_RPW91) {  // "RPW91": PW92 + RPW91x (no XAlpha) + PW91c + RPW91c (:626-636)
+    c.xg = XG_PW91;
+    c.cg = CG_PW91;
+    c.lc = LC_PW92;
+    c.fx_lda = 0.0;
   } else if (f == PGXC_XC_ECMV92) {  // "ECMV92": XAlpha + ECMV92 with X_LONGTRANS (:645-650)
     c.xg = XG_ECMV92;
     c.cg = CG_NONE;
@@ -457,7 +465,7 @@ __device__ __forceinline__ void pbe_x(const XcConst& K, double n, double g, doub
   }
   if (K.rel_g) {
     // x_gga with relativity (exchange.f90:418-438): e_x (phi0 - 1 + phi2 G), the
-    // -1 because XAlpha is on
+    // -1 for the XAlpha term (which "RPW91" leaves off all the same)
     double b, db, p0, dp0, p2, dp2;
     rel_beta(K, n, b, db);
     rel_phi0(b, p0, dp0);
@@ -888,6 +896,102 @@ __device__ __forceinline__ void xc_bp86(const XcConst& K, double n, double g, do
   fg += K.fc_g * pg;
 }
 
+// The PW91 correlation of the older pw91c_calc (perdew_wang_module.f90:112-490,
+// not revised) with its closed-form derivatives as written there: n floored at
+// 1e-50, 1 +- zeta at 1e-25, exp(.) - 1 of A at 1e-50, 1e-50 added under
+// dt/dgamma, and (open shell) dH1/drs without the g^3 of H1.  ec, ecr: the LDA
+// correlation per volume and its density derivatives.  f = n H; fr[s], fg[k].
+__device__ __forceinline__ void pw91c_old(bool open, const double* rho, const double* gam, double ec,
+                                          const double* ecr, double& f, double* fr, double* fg) {
+  const double pi = 3.141592653589793240, deps = 1.0e-50;
+  const double Cc0 = 0.004235, Cx = -0.001667, al = 0.09, Cx37 = Cx * 3.0 / 7.0;
+  const double a_rg = 23.266, b_rg = 7.389e-3, c_rg = 8.723, d_rg = 0.472, e_rg = 2.568;
+  const double cr3pi2 = cbrt(3.0 * pi * pi);
+  const double rs_fact = cbrt(3.0 / (4.0 * pi)), h1_fact = (16.0 / pi) * cr3pi2;
+  const double bpw = h1_fact * Cc0, h0_fact = bpw * bpw / (2.0 * al), apf = 2.0 * al / bpw;
+  const double t_fact = 1.0 / (2.0 * sqrt(cbrt(192.0 / pi)));
+  const double e_fact = 100.0 * 4.0 / (pi * cr3pi2);
+  double n = open ? rho[0] + rho[1] : rho[0];
+  if (n < deps) n = deps;
+  const double eps = ec / n;
+  const double rt = cbrt(n), rs = rs_fact / rt, rs2 = rs * rs;
+  double pa = 1.0, pb = 1.0;
+  if (open) {
+    const double zeta = (rho[0] - rho[1]) / n;
+    pa = fmax(1.0 + zeta, 1.0e-25);
+    pb = fmax(1.0 - zeta, 1.0e-25);
+  }
+  const double g = open ? 0.5 * (pow(pa, 2.0 / 3.0) + pow(pb, 2.0 / 3.0)) : 1.0;
+  const double g2 = g * g, g3 = g2 * g, g4 = g2 * g2;
+  const double gr = sqrt(open ? gam[0] + gam[1] + 2.0 * gam[2] : gam[0]);
+  const double srt = sqrt(rt);
+  const double t = t_fact * gr / (srt * n) / g, t2 = t * t;
+  const double t_g = 0.5 * t_fact / (srt * n * gr + deps) / g;
+  const double t_n = -(7.0 / 6.0) * t / n, t_gi = -t / g;
+  const double ex0 = -2.0 * al * eps / (bpw * bpw) / g3;
+  const double V = exp(ex0);
+  const double Aden = fmax(V - 1.0, deps);
+  const double A = apf / Aden, At2 = A * t2, OA = 1.0 + At2;
+  const double den = (1.0 + (apf + A) * t2 * OA) * (OA + At2 * At2);
+  const double h0 = g3 * h0_fact * log(1.0 + apf * (t2 + At2 * t2) / (OA + At2 * At2));
+  const double F0_t = g3 * n * 2.0 * bpw * t * (OA + At2) / den;
+  const double h0_a = -g3 * bpw * t2 * t2 * t2 * A * (2.0 + At2) / den;
+  const double ex1 = -g4 * e_fact * t2 / rt, E1 = exp(ex1);
+  const double rn = e_rg + a_rg * rs + b_rg * rs2, rd = 1.0 + c_rg * rs + d_rg * rs2 + 10.0 * b_rg * rs2 * rs;
+  const double K1 = h1_fact * (1.0e-3 * rn / rd - Cx - Cc0 - Cx37);
+  const double h1 = g3 * K1 * t2 * E1;
+  const double h1_t = g3 * K1 * E1 * 2.0 * t * (1.0 + ex1);
+  const double rn1 = a_rg + 2.0 * b_rg * rs, rd1 = c_rg + 2.0 * d_rg * rs + 30.0 * b_rg * rs2;
+  const double h_rs = h1_fact * t2 * E1 * 1.0e-3 * (rn1 * rd - rd1 * rn) / (rd * rd);
+  const double rs_n = -rs / (3.0 * n);
+  const double h1_dn = g4 * h1 * t2 * e_fact / (3.0 * n * rt);
+  const double Fg = F0_t * t_g + n * h1_t * t_g;
+  const double vA = V / (Aden * Aden);
+  f = (h0 + h1) * n;
+  if (!open) {
+    const double A_n = (apf * apf / bpw) * vA * (ecr[0] - eps) / n;
+    fr[0] = h0 + n * h0_a * A_n + F0_t * t_n + h1 + n * (h_rs * rs_n + h1_t * t_n + h1_dn);
+    fg[0] = Fg;
+    return;
+  }
+  const double A_gi = 3.0 * (apf * vA) * ex0 * g3 / g4;
+  const double dg = (1.0 / 3.0) * (1.0 / cbrt(pa) - 1.0 / cbrt(pb));
+  const double h0_t = F0_t / n, h0_gi = 3.0 * g2 / g3 * h0;
+  const double h1_gi = 3.0 * g2 / g3 * h1 + h1 * (4.0 * g3 / g4) * ex1;
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    const double zs = s == 0 ? pb / n : -pa / n;
+    const double A_ns = (apf * apf / (bpw * g3)) * vA * (ecr[s] - eps) / n + A_gi * dg * zs;
+    const double h0_ns = h0_gi * dg * zs + h0_a * A_ns + h0_t * (t_n + t_gi * dg * zs);
+    const double h1_ns = h1_t * t_gi * dg * zs + h1_t * t_n + h1_gi * dg * zs + h_rs * rs_n + h1_dn;
+    fr[s] = h0 + n * h0_ns + h1 + n * h1_ns;
+  }
+  fg[0] = fg[1] = Fg;
+  fg[2] = 2.0 * Fg;
+}
+
+// "RPW91"'s correction (xc_rperdewwang91c, xc_func.f90:436-446): the H of
+// pw91c_calc times phi_c(b) = (1 + a1 b^2 + a2 b^4) / (1 + b1 b^2 + b2 b^4),
+// b = (3 pi^2 n)^(1/3) / c, n floored at 1e-50; rpw91c_calc scales F first and
+// then adds the scaled F times dphi_c/dn to dF/drho (relxc.f90:162-218).
+__device__ __forceinline__ void rpw91c_add(const XcConst& K, bool open, const double* rho, const double* gam,
+                                           double ec, const double* ecr, double& f, double* fr, double* fg) {
+  double h, hr[2], hg[3];
+  pw91c_old(open, rho, gam, ec, ecr, h, hr, hg);
+  const double a1 = 1.9407, a2 = 0.14435, b1 = 0.28412, b2 = 0.004723;
+  const double n = fmax(open ? rho[0] + rho[1] : rho[0], 1.0e-50);
+  const double b = cbrt(K.rel_3pi2 * n) / K.rel_c, bb = b * b;
+  const double num = 1.0 + a1 * bb + a2 * bb * bb, den = 1.0 + b1 * bb + b2 * bb * bb;
+  const double phi = num / den;
+  const double dphi = (den * (2.0 * a1 * b + 4.0 * a2 * bb * b) - num * (2.0 * b1 * b + 4.0 * b2 * bb * b)) * b /
+                      (3.0 * n * den * den);
+  const double hs = h * phi;
+  f += hs;
+  const int ns = open ? 2 : 1, ng = open ? 3 : 1;
+  for (int s = 0; s < ns; ++s) fr[s] += hr[s] * phi + hs * dphi;
+  for (int k = 0; k < ng; ++k) fg[k] += hg[k] * phi;
+}
+
 // "PW91", "BPW91" (PW92 + PW91 correlation), "BLYP" (LYP) and "B88" (no
 // correlation), closed shell, through the dual numbers in (n, g) or, for
 // LYP, in (rho_a, rho_b).
@@ -912,6 +1016,10 @@ __device__ __forceinline__ void xc_gga_d3(const XcConst& K, double n, double g, 
     f += K.fc_g * c.v;
     fr += K.fc_g * c.d[0];
     fg += K.fc_g * c.d[1];
+    if (K.rpw91c) {
+      const double ecr = ec.d[0];
+      rpw91c_add(K, false, &n, &g, ec.v, &ecr, f, &fr, &fg);
+    }
   } else if (K.cg == CG_LYP) {
     // lyp_C (lyp.f90): ra = rb = n/2, gaa = gbb = gab = g/4; dF/dn is dF/dra
     // and dF/dg is the coefficient of gaa alone, as the reference returns them
@@ -1001,6 +1109,10 @@ __device__ __forceinline__ void xc_open_gga(const XcConst& K, const double (&rho
   fg[0] += a * c.d[2];
   fg[1] += a * c.d[2];
   fg[2] += a * 2.0 * c.d[2];
+  if (K.rpw91c) {
+    const double ecr[2] = {ec.d[0], ec.d[1]};
+    rpw91c_add(K, true, rho, gam, ec.v, ecr, f, fr, fg);
+  }
 }
 
 // Open-shell functional at one point: rho[2] = (rho_a, rho_b), gam[3] =

@@ -9,7 +9,8 @@ from pgxc import abi, cases, lib
 pytestmark = pytest.mark.gpu
 
 GGA_SET = ["PBE", "revPBE", "PBEsol", "BP86", "PW91", "BPW91", "BLYP", "B3LYP", "PBE0", "HCTH", "HCTH407",
-           "VMT", "VT84", "PBEN", "NRECMV92", "LB94", "VWN", "XALPHA", "PWLDA"]
+           "VMT", "VT84", "PBEN", "NRECMV92", "LB94", "VWN", "XALPHA", "PWLDA",
+           "RBP", "RPW91"]
 
 
 @pytest.mark.parametrize("precision,thr,tol", [("fp64", 0.0, 1e-10), ("mixed", 1e-10, 1e-7)], ids=["fp64", "int8"])

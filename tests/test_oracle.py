@@ -24,6 +24,11 @@ GGA_XC = [x for x in ALL_XC if abi.is_gga(x)]
 LYP_XC = ("BLYP", "B3LYP")
 # LB94 adds a potential without an energy: its df/drho is not dE/drho
 POTENTIAL_ONLY = ("LB94",)
+# RPW91's potential is the reference's: the phi_c-scaled PW91 term adds the
+# already scaled F times dphi_c/dn to dF/drho (relxc.f90:190-193), and its
+# open-shell dH1/drs lacks g^3 (perdew_wang_module.f90:365-366); the gamma
+# derivatives are exact.  test_rpw91_published_form pins both.
+RPW91_XC = ("RPW91",)
 
 
 @pytest.mark.parametrize("xc", ALL_XC)
@@ -39,7 +44,7 @@ def test_functional_derivatives_fd(xc):
         return (O.functionals(xc, 1, rho + h, gam)[0] - O.functionals(xc, 1, rho - h, gam)[0]) / (2 * h)
     h = 1e-3 * rho
     num = (4 * central(h / 2) - central(h)) / 3
-    if xc not in POTENTIAL_ONLY:
+    if xc not in POTENTIAL_ONLY + RPW91_XC:
         np.testing.assert_allclose(fr[:, 0], num, rtol=2e-6, atol=1e-12)
     # closed-shell BLYP returns the LYP coefficient of gamma_aa as dF/dgamma,
     # as the reference does: test_lyp_published_form covers it
@@ -84,7 +89,7 @@ def test_open_shell_derivatives_fd(xc):
     f, fr, fg = O.functionals(xc, 2, x[:, :2], x[:, 2:])
     ana = np.concatenate([fr, fg], 1)
     for k in range(5):
-        if xc in POTENTIAL_ONLY and k < 2:
+        if xc in POTENTIAL_ONLY + RPW91_XC and k < 2:
             continue
         h = 1e-4 * np.abs(x[:, k]) if k < 4 else 1e-4 * np.sqrt(gaa * gbb)
         xp, xm = x.copy(), x.copy()
@@ -346,7 +351,7 @@ def test_basis_normalised_and_gradients(small_cases):
         np.testing.assert_allclose(gr[:, d, :], (pp - pm) / (2 * h), rtol=1e-5, atol=1e-8)
 
 
-@pytest.mark.parametrize("xc", [x for x in ALL_XC if x not in LYP_XC + POTENTIAL_ONLY])
+@pytest.mark.parametrize("xc", [x for x in ALL_XC if x not in LYP_XC + POTENTIAL_ONLY + RPW91_XC])
 def test_dE_dC_equals_2_occ_V_C(small_cases, xc):
     if xc in small_cases:
         c = small_cases[xc]
@@ -520,3 +525,45 @@ def test_relativistic_exchange_published_form():
                       (F("RBP", gam) - F("BP86", gam), ex * (phi0 - 1 + (phi2_88 - 1) * g88)),
                       (F("ECMV92", gam) - F("NRECMV92", gam), ex * (phi0 - 1 + (phi2_92 - 1) * g92))):
         assert np.all(np.abs(got - want) <= 1e-9 * np.abs(want) + 1e-12 * np.abs(ex)), (got, want)
+
+
+def test_rpw91_published_form():
+    """RPW91 against its pieces: the relativistic PW91 exchange e_x (phi0 - 1 +
+    phi2_B88 G_PW91) without a Slater term, PW92, the PW91 correlation H and
+    phi_c H, phi_c = (1 + 1.9407 b^2 + 0.14435 b^4) / (1 + 0.28412 b^2 +
+    0.004723 b^4) (xc_cntrl.f90:626-636, relxc.f90:162-218).  H and e_x G_PW91
+    come from the other keywords: H = BPW91 - B88 - (PWLDA - XALPHA), e_x G =
+    PW91 - PWLDA - H, so RPW91 - PW91 = e_x (phi0 - 2) + (phi2 - 1) e_x G +
+    phi_c H (to the 1e-7 by which pw91c_calc's rs constant differs from
+    gga_correlation's 1.91916).  The closed-shell potential is the exact
+    derivative plus H dphi_c/dn (phi_c - 1), as rpw91c_calc writes it."""
+    rng = np.random.default_rng(59)
+    rho = 10 ** rng.uniform(-2, 4, 12)
+    gam = rho ** (8 / 3) * 10 ** rng.uniform(-3, 0.5, 12)
+    pi = 3.14159265358979324
+    ex = -(3 / 4) * (3 / pi) ** (1 / 3) * rho ** (4 / 3)
+    b = (3 * pi ** 2 * rho) ** (1 / 3) / 137.03604
+    eta = np.sqrt(1 + b * b)
+    phi0 = 1 - 1.5 * ((eta - np.arcsinh(b) / b) / b) ** 2
+    x = b * b
+    pade = lambda a, c: (a[0] + x * (a[1] + x * a[2])) / (c[0] + x * (c[1] + x * c[2]))
+    phi2 = pade((1, 2.20848, 0.668684), (1, 1.33075, 0.795105)) + pade((0, 3.48638, 0.614753), (1, 1.32260, 0.101805))
+    num_c, den_c = 1 + 1.9407 * x + 0.14435 * x * x, 1 + 0.28412 * x + 0.004723 * x * x
+    phic = num_c / den_c
+    dphic = ((den_c * (2 * 1.9407 * b + 4 * 0.14435 * b ** 3) - num_c * (2 * 0.28412 * b + 4 * 0.004723 * b ** 3))
+             * b / (3 * rho * den_c ** 2))
+    F = lambda xc, r=rho: O.functionals(xc, 1, r, gam)
+    H = F("BPW91")[0] - F("B88")[0] - (F("PWLDA")[0] - F("XALPHA")[0])
+    exG = F("PW91")[0] - F("PWLDA")[0] - H
+    f, fr, _ = F("RPW91")
+    want = ex * (phi0 - 2) + (phi2 - 1) * exG + phic * H
+    assert np.all(np.abs(f - F("PW91")[0] - want) <= 5e-7 * np.abs(H) + 1e-12 * np.abs(ex))
+
+    def central(h):
+        return (F("RPW91", rho + h)[0] - F("RPW91", rho - h)[0]) / (2 * h)
+    h = 1e-3 * rho
+    exact = (4 * central(h / 2) - central(h)) / 3
+    quirk = H * dphic * (phic - 1)
+    big = np.abs(quirk) > 1e-7 * np.abs(fr[:, 0])  # above the difference quotient's noise
+    assert big.sum() >= 5
+    np.testing.assert_allclose((fr[:, 0] - exact)[big], quirk[big], rtol=2e-2)
