@@ -119,11 +119,17 @@ extern "C" {
  * phi_c(n) times the H of pw91c_calc ("RPW91", modules/xc_cntrl.f90:626-636;
  * xc_func.f90:436-446; relxc.f90 rpw91c_calc :162-218) */
 #define PGXC_XC_RPW91 28
+/* RVWN_ENGEL = relativistic Slater + VWN5 + VWN5 (phic0(beta) - 1), the
+ * Schmid-Engel-Dreizler-Blaha-Schwarz relativistic LDA correlation, an LDA
+ * ("RVWN:Engel" / "RVWN_ENGEL", modules/xc_cntrl.f90:477-498; exchange.f90
+ * correlation_lda :124-157, phic0 :159-204) */
+#define PGXC_XC_RVWN_ENGEL 29
 /* the largest functional id */
-#define PGXC_XC_LAST PGXC_XC_RPW91
-/* nonzero for the GGA keywords (all but the four LDAs) */
+#define PGXC_XC_LAST PGXC_XC_RVWN_ENGEL
+/* nonzero for the GGA keywords (all but the five LDAs) */
 #define PGXC_XC_IS_GGA(id) \
-  ((id) != PGXC_XC_VWN && (id) != PGXC_XC_XALPHA && (id) != PGXC_XC_PWLDA && (id) != PGXC_XC_RVWN)
+  ((id) != PGXC_XC_VWN && (id) != PGXC_XC_XALPHA && (id) != PGXC_XC_PWLDA && (id) != PGXC_XC_RVWN && \
+   (id) != PGXC_XC_RVWN_ENGEL)
 
 /* ---- precision modes ------------------------------------------------- */
 #define PGXC_PREC_FP64        0  /* FP64 everywhere (FP64 tensor pipe): the drop-in */

@@ -170,6 +170,7 @@ GgaPar gga_par(int xc) {
     case PGXC_XC_LB94: return {0, 0, 0, GX_NONE, GC_NONE, LC_VWN, 0};
     // relativistic keywords (xc_cntrl.f90 "RVWN" :477-488, "RBP" :545-558, "ECMV92" :645-650)
     case PGXC_XC_RVWN: return {0, 0, 0, GX_NONE, GC_NONE, LC_VWN, 0};
+    case PGXC_XC_RVWN_ENGEL: return {0, 0, 0, GX_NONE, GC_NONE, LC_VWN, 0};
     case PGXC_XC_RBP: return {0, 0, 0, GX_B88, GC_P86, LC_VWN, 0, 1, 1, 1, 1, 1};
     case PGXC_XC_ECMV92: return {0, 0, 0, GX_ECMV92, GC_NONE, LC_NONE, 0, 1, 1, 1, 1, 2};
     // "RPW91" (:626-636): pwldac + rperdewwang91x (X_PW91 + X_LONGTRANS, no
@@ -292,6 +293,18 @@ D ec_rlda(D n) {
   D num = c3 * dipow(b, 3) + c2 * dipow(b, 2) + c1 * b + c0;
   D den = d4 * dipow(b, 4) + d3 * dipow(b, 3) + d2 * dipow(b, 2) + d1 * b + d0;
   return a0 * b + b0 + num / den;
+}
+
+// phic0(beta) (exchange.f90:159-204, Schmid, Engel, Dreizler, Blaha, Schwarz):
+// the relativistic factor of the LDA correlation of "RVWN:Engel", 1 at beta = 0.
+D engel_phic0(D b) {
+  if (!(b.v > 0.0)) return cst(1.0);
+  const double a1 = -2.44968, a2 = 1.91853, a3 = 0.0718854, b1 = -1.59583, b2 = 1.29176, b3 = 0.364044;
+  const double AA = 0.0621841, BB = AA * std::log(C_LIGHT) + 0.05275877384;
+  D L = dlog(b), b3p = dipow(b, 3), b4p = dipow(b, 4);
+  D num = 1.0 + a1 * b3p * L + a2 * b4p + a3 * dipow(1.0 + b * b, 2) * b4p;
+  D den = 1.0 + b1 * b3p * L + b2 * b4p + b3 * (AA * L + BB) * dipow(b, 7);
+  return num / den;
 }
 
 void x_gga_pbe(const GgaPar& P, double n, double gam, double& F, double& dFdn, double& dFdg) {
@@ -789,7 +802,8 @@ void functional_point(int xc, int ispin, const double* rho, const double* gam,
   };
   // Slater exchange (exchange_lda, exchange.f90:511-565)
   // "RVWN": RXAlpha, the Slater term times phi0(beta) (x_lda with X_LONGTRANS, :567-601)
-  auto xlda = [&](D n) { return xc == PGXC_XC_RVWN ? x_lda(n) * rel_phi0(rel_beta(n)) : x_lda(n); };
+  const bool rel_lda = xc == PGXC_XC_RVWN || xc == PGXC_XC_RVWN_ENGEL;
+  auto xlda = [&](D n) { return rel_lda ? x_lda(n) * rel_phi0(rel_beta(n)) : x_lda(n); };
   clear();
   if (ispin == 1) {
     D e = xlda(var(0, rho[0]));
@@ -817,6 +831,13 @@ void functional_point(int xc, int ispin, const double* rho, const double* gam,
   pf = ec.v; pr[0] = ec.d[0];
   if (ispin == 2) pr[1] = ec.d[1];
   add(P.fc_lda);
+  if (xc == PGXC_XC_RVWN_ENGEL) {
+    // correlation_lda (exchange.f90:124-157): VWN5 (vwn_calc, the same VWN5 as
+    // vwn_ldac) times phic0(beta(n)) - 1, n = the total density
+    D p = engel_phic0(rel_beta(ispin == 1 ? var(0, rho[0]) : var(0, rho[0]) + var(1, rho[1])));
+    f += ec.v * (p.v - 1.0);
+    for (int s = 0; s < ispin; ++s) fr[s] += ec.d[s] * (p.v - 1.0) + ec.v * p.d[s];
+  }
   if (xc == PGXC_XC_RVWN) {  // rel_vwn_calc (relxc.f90:128-160), of the total density
     D er = ec_rlda(ispin == 1 ? var(0, rho[0]) : var(0, rho[0]) + var(1, rho[1]));
     f += er.v; fr[0] += er.d[0];

@@ -65,7 +65,8 @@ struct XcConst {
   // relativistic exchange (exchange.f90 x_lda / x_gga with X_LONGTRANS):
   // rel_lda: Slater times phi0(beta) ("RVWN"); rel_g: the enhancement term
   // e_x (phi0 - 1 + phi2 G) with the Pade set of Becke 88 (1, "RBP") or of
-  // ECMV92 (2, "ECMV92"); rvwn: add ec_RLDA (relxc.f90); rel_c: speed of light
+  // ECMV92 (2, "ECMV92"); rvwn: add ec_RLDA (1, relxc.f90) or VWN5 (phic0 - 1)
+  // (2, "RVWN:Engel", exchange.f90 correlation_lda); rel_c: speed of light
   int rel_lda, rel_g, rvwn;
   double rel_c, rel_3pi2;
   // rpw91c: "RPW91" adds phi_c(n) times the H of pw91c_calc (relxc.f90:162-218)
@@ -155,11 +156,12 @@ __host__ inline XcConst make_xc_const(int functional = PGXC_XC_PBE) {
   c.lb94_two13 = std::pow(2.0, 1.0 / 3.0);
   c.rel_c = 137.03604;  // constants.f90 SPEED_OF_LIGHT
   c.rel_3pi2 = 3.0 * 3.14159265358979324 * 3.14159265358979324;
-  c.rel_lda = f == PGXC_XC_RVWN ? 1 : 0;
-  c.rvwn = f == PGXC_XC_RVWN ? 1 : 0;
+  c.rel_lda = (f == PGXC_XC_RVWN || f == PGXC_XC_RVWN_ENGEL) ? 1 : 0;
+  c.rvwn = f == PGXC_XC_RVWN ? 1 : f == PGXC_XC_RVWN_ENGEL ? 2 : 0;
   c.rel_g = (f == PGXC_XC_RBP || f == PGXC_XC_RPW91) ? 1 : f == PGXC_XC_ECMV92 ? 2 : 0;
   c.rpw91c = f == PGXC_XC_RPW91 ? 1 : 0;
-  if (f == PGXC_XC_RVWN) {  // "RVWN": RXAlpha + VWN + rel_vwn_calc (xc_cntrl.f90:477-488)
+  if (f == PGXC_XC_RVWN || f == PGXC_XC_RVWN_ENGEL) {
+    // "RVWN": RXAlpha + VWN + rel_vwn_calc, "RVWN:Engel": correlation_lda (xc_cntrl.f90:477-498)
     c.lc = LC_VWN;
     c.cg = CG_NONE;
   } else if (f == PGXC_XC_RBP) {  // "RBP": XAlpha + VWN + RBecke88 + Perdew (:545-558)
@@ -306,6 +308,30 @@ __device__ __forceinline__ void slater(const XcConst& K, double n, double& f, do
   }
 }
 
+// phic0(beta) of the relativistic LDA correlation of Schmid, Engel, Dreizler,
+// Blaha and Schwarz (phic0, exchange.f90:159-204): (1 + a1 b^3 ln b + a2 b^4 +
+// a3 (1 + b^2)^2 b^4) / (1 + b1 b^3 ln b + b2 b^4 + b3 (AA ln b + BB) b^7),
+// AA = 0.0621841, BB = AA ln c + 0.05275877384; 1 at beta = 0 (n below 1e-20);
+// and d phic0 / dn.
+__device__ __forceinline__ void engel_phic0(const XcConst& K, double n, double& phi, double& dphi) {
+  double b, db;
+  rel_beta(K, n, b, db);
+  if (!(b > 0.0)) {
+    phi = 1.0;
+    dphi = 0.0;
+    return;
+  }
+  const double a1 = -2.44968, a2 = 1.91853, a3 = 0.0718854, b1 = -1.59583, b2 = 1.29176, b3 = 0.364044;
+  const double AA = 0.0621841, BB = AA * log(K.rel_c) + 0.05275877384;
+  const double bb = b * b, bbb = bb * b, b4 = bb * bb, b6 = b4 * bb, L = log(b), q = 1.0 + bb;
+  const double num = 1.0 + a1 * bbb * L + a2 * b4 + a3 * q * q * b4;
+  const double den = 1.0 + b1 * bbb * L + b2 * b4 + b3 * (AA * L + BB) * b6 * b;
+  const double dnum = a1 * (3.0 * bb * L + bb) + 4.0 * a2 * bbb + a3 * (4.0 * b * q * b4 + 4.0 * q * q * bbb);
+  const double dden = b1 * (3.0 * bb * L + bb) + 4.0 * b2 * bbb + b3 * (AA * b6 + 7.0 * (AA * L + BB) * b6);
+  phi = num / den;
+  dphi = (dnum * den - num * dden) / (den * den) * db;
+}
+
 // Relativistic LDA correlation correction ec_RLDA(n) and its n derivative
 // (relxc.f90:221-283, the 0.25 cutoff form); 0 below n = 1e-7.  It is added to
 // the energy density as it stands.
@@ -356,11 +382,17 @@ __device__ __forceinline__ void xc_vwn(const XcConst& K, double n, double& f, do
   const double ecpara = ap * e;
   f += K.fc_lda * (ecpara * S);
   fr += K.fc_lda * (ecpara - ap * de * X / 6.0);   // dX/dn = -X/(6S)
-  if (K.rvwn) {  // rel_vwn_calc (relxc.f90:128-160)
+  if (K.rvwn == 1) {  // rel_vwn_calc (relxc.f90:128-160)
     double er, der;
     rel_vwn(K, n, er, der);
     f += er;
     fr += der;
+  } else if (K.rvwn == 2) {  // correlation_lda: F (phic0 - 1), F = VWN5 of n
+    double p, dp;
+    engel_phic0(K, n, p, dp);
+    const double F = ecpara * S;
+    f += F * (p - 1.0);
+    fr += (ecpara - ap * de * X / 6.0) * (p - 1.0) + F * dp;
   }
 }
 
@@ -1143,12 +1175,18 @@ __device__ __forceinline__ void xc_open(const XcConst& K, const double (&rho)[2]
   f += K.fc_lda * ec.v;
   fr[0] += K.fc_lda * ec.d[0];
   fr[1] += K.fc_lda * ec.d[1];
-  if (K.rvwn) {  // rel_vwn_calc: a function of the total density
+  if (K.rvwn == 1) {  // rel_vwn_calc: a function of the total density
     double er, der;
     rel_vwn(K, rho[0] + rho[1], er, der);
     f += er;
     fr[0] += der;
     fr[1] += der;
+  } else if (K.rvwn == 2) {  // correlation_lda: VWN5 (phic0(beta(n)) - 1), n = rho_a + rho_b
+    double p, dp;
+    engel_phic0(K, rho[0] + rho[1], p, dp);
+    f += ec.v * (p - 1.0);
+    fr[0] += ec.d[0] * (p - 1.0) + ec.v * dp;
+    fr[1] += ec.d[1] * (p - 1.0) + ec.v * dp;
   }
   if constexpr (GGA) xc_open_gga(K, rho, gam, na, nb, ec, f, fr, fg);
 }

@@ -221,7 +221,8 @@ def test_build_from_density_matrix_open_shell():
                                      ("VT84", 12), ("VMTsol", 13), ("VT84sol", 14), ("HCTH", 15),
                                      ("HCTH120", 16), ("HCTH147", 17), ("HCTH407", 18), ("NRECMV92", 19),
                                      ("PWLDA", 20), ("B3LYP", 21), ("PBE0", 22), ("LB94", 23), ("RVWN", 24),
-                                     ("RBP", 25), ("ECMV92", 26), ("RPW91", 27)])
+                                     ("RBP", 25), ("ECMV92", 26), ("RPW91", 27),
+                                     ("RVWN_ENGEL", 28)])
 def test_gga_keyword_builds(xc, seed, layout, precision, thr, tol):
     """revPBE and PBEsol (the PBE-form keywords with other kappa, mu, beta),
     BP86 (Becke 88 + Perdew 86), PW91, BPW91 (Becke 88 + PW91 correlation),

@@ -496,6 +496,7 @@ def test_relativistic_exchange_published_form():
     relativistic LDA exchange, phi0(b) = 1 - (3/2) [(eta - asinh(b)/b)/b]^2,
     eta = sqrt(1 + b^2), b = (3 pi^2 n)^(1/3)/c, c = 137.03604, and the Pade
     corrections phi2 of the GGA term: RVWN - VWN = e_x (phi0 - 1) + ec_RLDA,
+    RVWN_ENGEL - VWN = e_x (phi0 - 1) + e_c^VWN (phic0 - 1),
     RBP - BP86 = e_x (phi0 - 1 + (phi2_B88 - 1) G_B88),
     ECMV92 - NRECMV92 = e_x (phi0 - 1 + (phi2_92 - 1) G_92)."""
     rng = np.random.default_rng(53)
@@ -520,8 +521,16 @@ def test_relativistic_exchange_published_form():
                    a0 * b + b0 + (c3 * b ** 3 + c2 * b ** 2 + c1 * b + c0)
                    / (d4 * b ** 4 + d3 * b ** 3 + d2 * b ** 2 + d1 * b + d0))
     ecr = np.where(rho < 1e-7, 0.0, ecr)
+    # "RVWN:Engel": VWN5 times phic0 (Schmid, Engel, Dreizler, Blaha, Schwarz)
+    AA = 0.0621841
+    BB = AA * np.log(137.03604) + 0.05275877384
+    L = np.log(b)
+    phic0 = ((1 - 2.44968 * b ** 3 * L + 1.91853 * b ** 4 + 0.0718854 * (1 + b * b) ** 2 * b ** 4)
+             / (1 - 1.59583 * b ** 3 * L + 1.29176 * b ** 4 + 0.364044 * (AA * L + BB) * b ** 7))
     F = lambda xc, g=None: O.functionals(xc, 1, rho, g)[0]
+    vwn_c = F("VWN") - F("XALPHA")
     for got, want in ((F("RVWN") - F("VWN"), ex * (phi0 - 1) + ecr),
+                      (F("RVWN_ENGEL") - F("VWN"), ex * (phi0 - 1) + vwn_c * (phic0 - 1)),
                       (F("RBP", gam) - F("BP86", gam), ex * (phi0 - 1 + (phi2_88 - 1) * g88)),
                       (F("ECMV92", gam) - F("NRECMV92", gam), ex * (phi0 - 1 + (phi2_92 - 1) * g92))):
         assert np.all(np.abs(got - want) <= 1e-9 * np.abs(want) + 1e-12 * np.abs(ex)), (got, want)
