@@ -188,6 +188,21 @@ typedef struct pgxc_grid {
   const int32_t* point_atom;     /* [npts], required when weights_are_raw   */
 } pgxc_grid;
 
+/*
+ * Atom-centred grid built by the library (grid_main_calc without pruning,
+ * modules/grid_module.f90:357-504): atom a gets the Pople radial grid of
+ * nrad[a] points scaled by radius[a] (RADIALGRID, :1246-1301; shells at
+ * r >= 40 bohr dropped) times the Lebedev-McLaren rule with nang points
+ * (INIGRD, :1359-2100; nang = 6, 8, 12, 14, 26, 38, 50, 78, 86, 110, 146,
+ * 194 or 302), not rotated; points ordered atom -> shell -> angular point;
+ * one-centre weights w_ang * w_rad * 4 pi (:425-432).
+ */
+typedef struct pgxc_grid_spec {
+  const int32_t* nrad;           /* [natoms] NRADPTS of each atom            */
+  const double* radius;          /* [natoms] RCUR of each atom, bohr         */
+  int32_t nang;                  /* points of the angular rule               */
+} pgxc_grid_spec;
+
 typedef struct pgxc_options {
   int32_t functional;            /* PGXC_XC_VWN .. PGXC_XC_LAST             */
   int32_t ispin;                 /* 1 or 2; 2 (open shell) needs screen_threshold >= 0,
@@ -241,6 +256,32 @@ void pgxc_default_options(pgxc_options* opt);
 int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas,
                 const pgxc_grid* grid, const pgxc_options* opt,
                 pgxc_ctx** out);
+
+/*
+ * pgxc_create on the grid of a spec, built on the device together with its
+ * Becke weights (grid_main_calc, then mkgrid's Becke step, :3045-3164): for
+ * optimiser or dynamics loops whose per-geometry grid never passes through
+ * host memory.  The context behaves as one created with weights_are_raw = 1
+ * (the nuclear gradient is available).
+ */
+int pgxc_create_on_grid(const pgxc_geometry* geo, const pgxc_basis* bas,
+                        const pgxc_grid_spec* spec, const pgxc_options* opt,
+                        pgxc_ctx** out);
+
+/* Points of the grid of a spec (library extension, no reference counterpart). */
+int pgxc_atomic_grid_size(const pgxc_geometry* geo, const pgxc_grid_spec* spec,
+                          int64_t* npts);
+
+/*
+ * The grid of a spec written to device memory of the current device:
+ * d_grdpts (npts, 4) column-major x, y, z, raw one-centre weight, and
+ * d_point_atom (npts) the host atom of each point, ordered as grid_main_calc
+ * orders AGRID; npts must equal pgxc_atomic_grid_size.  Enqueued on stream
+ * (a cudaStream_t, NULL = legacy default) and synchronised before returning.
+ */
+int pgxc_atomic_grid(const pgxc_geometry* geo, const pgxc_grid_spec* spec,
+                     int64_t npts, double* d_grdpts, int32_t* d_point_atom,
+                     void* stream);
 
 /* Number of orbital basis functions (irrep dimension in C1). */
 int pgxc_nbas(const pgxc_ctx* ctx, int32_t* nbas);
@@ -309,7 +350,8 @@ int pgxc_build_device(pgxc_ctx* ctx, const double* d_C, const double* d_occ,
  * modules/post_scf_module.f90:2569-3318, :3500-5193; density_calc_ph_nl,
  * modules/density_calc_module.f90:2000-3315; becke1, modules/grid_module.f90
  * :2499-2616).  Needs a context created with weights_are_raw (PGXC_ENOTSUP
- * otherwise).  FP64 in every precision mode; C1 only.
+ * otherwise).  FP64 in every precision mode; C1 only: a context with
+ * pgxc_set_symmetry applied returns PGXC_ENOTSUP.
  */
 int pgxc_xc_gradient(pgxc_ctx* ctx, const double* C, const double* occ,
                      int32_t nbas, int32_t nocc, int32_t ispin, double* grad, double* exc);

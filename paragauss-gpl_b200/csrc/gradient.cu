@@ -326,6 +326,18 @@ __device__ __forceinline__ void becke_s(double mu, double& s, double& ds) {
 // L_xy the product of row x without its factor y; the point moves with its
 // host h, which collects kappa_xy (u_x - u_y)/R of every pair.  Each atom's sum
 // is reduced over the warp and added to shared memory, then to grad.
+//
+// Rows whose leave-one-out products are all negligible ("dead" rows) enter
+// pass 2 only through their pairs with live rows.  Every factor is at most 1,
+// so L_xy <= the product of row x's factors with the four atoms nearest to the
+// point, leaving out the smallest of them; where that bound is below 2^-60
+// the row is dead (its P_x is below the same bound and is dropped from Z).
+// Where mu <= -0.994, s rounds to exactly 1 and leaves the row product
+// unchanged.
+constexpr int kGradAlive = 32;  // live rows listed per point; more -> every row is visited
+constexpr double kGradEdge = 0.9941;
+constexpr double kGradTau = 0x1p-60;
+
 __global__ void k_grad_weights(const double* __restrict__ atoms, const double* __restrict__ dist, int natm,
                                const double* __restrict__ px, const double* __restrict__ py,
                                const double* __restrict__ pz, const int* __restrict__ owner, int64_t p0,
@@ -338,28 +350,91 @@ __global__ void k_grad_weights(const double* __restrict__ atoms, const double* _
   const bool live = p < nvalid && ef[p] != 0.0;
   double rv[3] = {0, 0, 0}, e = 0.0, Z = 0.0, Wh = 0.0;
   int h = 0;
+  int alive[kGradAlive];
+  int nalive = 0;  // > kGradAlive: the list overflowed, every row counts as live
   if (live) {
     rv[0] = px[p0 + p]; rv[1] = py[p0 + p]; rv[2] = pz[p0 + p];
     h = owner[p0 + p];
     e = ef[p];
+    int nb[4] = {-1, -1, -1, -1};
+    double nr[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
     for (int b = 0; b < natm; ++b) {
       const double t0 = rv[0] - atoms[3 * b], t1 = rv[1] - atoms[3 * b + 1], t2 = rv[2] - atoms[3 * b + 2];
-      sd[b * ld + p] = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
+      const double r = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
+      sd[b * ld + p] = r;
+      if (r < nr[3]) {
+        int j = 3;
+        for (; j > 0 && nr[j - 1] > r; --j) {
+          nr[j] = nr[j - 1];
+          nb[j] = nb[j - 1];
+        }
+        nr[j] = r;
+        nb[j] = b;
+      }
     }
     double Ph = 0.0;
     for (int b = 0; b < natm; ++b) {
       const double db = sd[b * ld + p];
+      const double* Rb = dist + (int64_t)b * natm;
+      double Q = 1.0, smin = 1.0;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int k = nb[c];
+        if (k < 0 || k == b) continue;
+        const double R = Rb[k], d = __dsub_rn(db, nr[c]);
+        if (d <= -__dmul_rn(kGradEdge, R)) continue;
+        double s, ds;
+        becke_s(__ddiv_rn(d, R), s, ds);
+        Q *= s;
+        smin = fmin(smin, s);
+      }
+      if (smin > 0.0 ? Q / smin < kGradTau : true) {
+        // with smin == 0 the row has a zero factor among the near atoms: its
+        // leave-one-out products are bounded by the product of the other
+        // near factors, recomputed below only if that could matter
+        bool dead = smin > 0.0;
+        if (!dead) {
+          double Qo = 1.0;
+          bool skipped = false;
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            const int k = nb[c];
+            if (k < 0 || k == b) continue;
+            const double R = Rb[k], d = __dsub_rn(db, nr[c]);
+            if (d <= -__dmul_rn(kGradEdge, R)) continue;
+            double s, ds;
+            becke_s(__ddiv_rn(d, R), s, ds);
+            if (s == 0.0 && !skipped) {
+              skipped = true;
+              continue;
+            }
+            Qo *= s;
+          }
+          dead = Qo < kGradTau;
+        }
+        if (dead) {
+          spnz[b * ld + p] = 0.0;
+          snz[b * ld + p] = -2;
+          continue;
+        }
+      }
       double pnz = 1.0;
       int nz = 0, zc = -1;
       for (int c = 0; c < natm; ++c) {
         if (c == b) continue;
+        const double R = Rb[c], d = __dsub_rn(db, sd[c * ld + p]);
+        if (d <= -__dmul_rn(kGradEdge, R)) continue;  // s == 1 exactly
         double s, ds;
-        becke_s(__ddiv_rn(__dsub_rn(db, sd[c * ld + p]), dist[b * natm + c]), s, ds);
+        becke_s(__ddiv_rn(d, R), s, ds);
         if (s == 0.0) { ++nz; zc = c; }
         else pnz *= s;
       }
       spnz[b * ld + p] = pnz;
       snz[b * ld + p] = nz == 0 ? -1 : (nz == 1 ? zc : -2);  // -1: no zero; c: the one zero; -2: several
+      if (nz < 2) {
+        if (nalive < kGradAlive) alive[nalive] = b;
+        ++nalive;
+      }
       const double P = nz ? 0.0 : pnz;
       Z += P;
       if (b == h) Ph = P;
@@ -367,8 +442,34 @@ __global__ void k_grad_weights(const double* __restrict__ atoms, const double* _
     if (Z > 0.0) Wh = Ph / Z;
   }
   const bool go = live && Z > 0.0;
+  const bool listed = nalive <= kGradAlive;
   double gh[3] = {0, 0, 0};
   const int lane = threadIdx.x & 31;
+  // terms of the pair (x, y): adds to gx (atom x) and gh (the host)
+  auto pair_terms = [&](int x, int y, double dx, double cx, double pnx, int zx, const double (&ux)[3],
+                        double (&gx)[3]) {
+    const double R = dist[x * natm + y];
+    const double dy = sd[y * ld + p];
+    const double mu = __ddiv_rn(__dsub_rn(dx, dy), R);
+    double sxy, dsxy, syx, dsyx;
+    becke_s(mu, sxy, dsxy);
+    becke_s(-mu, syx, dsyx);
+    // leave-one-out products of rows x (without y) and y (without x)
+    const double Lxy = zx == -1 ? (sxy != 0.0 ? pnx / sxy : 0.0) : (zx == y ? pnx : 0.0);
+    const int zy = snz[y * ld + p];
+    const double pny = spnz[y * ld + p];
+    const double Lyx = zy == -1 ? (syx != 0.0 ? pny / syx : 0.0) : (zy == x ? pny : 0.0);
+    const double cy = e * ((y == h ? 1.0 : 0.0) - Wh) / Z;
+    const double kxy = cx * Lxy * dsxy, kyx = cy * Lyx * dsyx;
+    if (kxy == 0.0 && kyx == 0.0) return;
+    const double iR = 1.0 / R, iR2 = iR * iR;
+    for (int k = 0; k < 3; ++k) {
+      const double rxy = atoms[3 * x + k] - atoms[3 * y + k];
+      const double uy = dy > 0.0 ? (rv[k] - atoms[3 * y + k]) / dy : 0.0;
+      gx[k] += (kyx - kxy) * (ux[k] * iR + mu * rxy * iR2);
+      gh[k] += kxy * (ux[k] - uy) * iR;
+    }
+  };
   for (int x = 0; x < natm; ++x) {
     double gx[3] = {0, 0, 0};
     if (go) {
@@ -378,29 +479,11 @@ __global__ void k_grad_weights(const double* __restrict__ atoms, const double* _
       const int zx = snz[x * ld + p];
       double ux[3];
       for (int k = 0; k < 3; ++k) ux[k] = dx > 0.0 ? (rv[k] - atoms[3 * x + k]) / dx : 0.0;
-      for (int y = 0; y < natm; ++y) {
-        if (y == x) continue;
-        const double R = dist[x * natm + y];
-        const double dy = sd[y * ld + p];
-        const double mu = __ddiv_rn(__dsub_rn(dx, dy), R);
-        double sxy, dsxy, syx, dsyx;
-        becke_s(mu, sxy, dsxy);
-        becke_s(-mu, syx, dsyx);
-        // leave-one-out products of rows x (without y) and y (without x)
-        const double Lxy = zx == -1 ? (sxy != 0.0 ? pnx / sxy : 0.0) : (zx == y ? pnx : 0.0);
-        const int zy = snz[y * ld + p];
-        const double pny = spnz[y * ld + p];
-        const double Lyx = zy == -1 ? (syx != 0.0 ? pny / syx : 0.0) : (zy == x ? pny : 0.0);
-        const double cy = e * ((y == h ? 1.0 : 0.0) - Wh) / Z;
-        const double kxy = cx * Lxy * dsxy, kyx = cy * Lyx * dsyx;
-        if (kxy == 0.0 && kyx == 0.0) continue;
-        const double iR = 1.0 / R, iR2 = iR * iR;
-        for (int k = 0; k < 3; ++k) {
-          const double rxy = atoms[3 * x + k] - atoms[3 * y + k];
-          const double uy = dy > 0.0 ? (rv[k] - atoms[3 * y + k]) / dy : 0.0;
-          gx[k] += (kyx - kxy) * (ux[k] * iR + mu * rxy * iR2);
-          gh[k] += kxy * (ux[k] - uy) * iR;
-        }
+      if (zx != -2 || !listed) {
+        for (int y = 0; y < natm; ++y)
+          if (y != x) pair_terms(x, y, dx, cx, pnx, zx, ux, gx);
+      } else {  // dead row x: only the pairs with live rows y contribute
+        for (int j = 0; j < nalive; ++j) pair_terms(x, alive[j], dx, cx, pnx, zx, ux, gx);
       }
     }
     for (int k = 0; k < 3; ++k)

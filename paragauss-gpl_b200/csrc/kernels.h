@@ -82,8 +82,10 @@ void launch_pack(const BuildArgs& a, int64_t nbas, int ispin, int spin, double* 
 // point-wise functional and Becke weights (standalone entry points)
 void launch_xc_points(int functional, int ispin, int64_t n, const double* rho, const double* gam, double* f,
                       double* fr, double* fg, cudaStream_t st);
-void launch_becke(const double* atoms, double* dist, int natm, const double* px, const double* py, const double* pz,
-                  const int* owner, int64_t n, double* w, cudaStream_t st);
+// Becke partition weights of n points (atom-atom distances into dist, natm^2);
+// returns the launch status
+cudaError_t launch_becke(const double* atoms, double* dist, int natm, const double* px, const double* py,
+                         const double* pz, const int* owner, int64_t n, double* w, cudaStream_t st);
 // message returned by pgxc_last_error(NULL)
 void set_global_error(const std::string& msg);
 

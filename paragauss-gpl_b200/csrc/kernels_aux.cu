@@ -14,14 +14,30 @@ namespace pgxc {
 // The reference accumulates P_i *= s_ik, P_k *= s_ki over pairs k < i.  For a
 // fixed atom a this multiplies P_a by s_ak for the other atoms in ascending
 // order, and s_ki = (1 - p3(mu_ki))/2 because p3 is odd (exactly, in floating
-// point).  So each P_a is formed here independently as that same ordered
-// product, giving the reference's rounding.  Once a product reaches exactly 0
-// (s rounds to 0 when |mu| is close to 1) the remaining factors cannot change
-// it and are skipped: the skip is exact.
+// point).  So each P_i is formed here independently as that same ordered
+// product, with the reference's rounding, and w = P_a / sum_i P_i with the sum
+// in ascending i.
+//
+// Cost: natm^2 pair evaluations per point in the reference.  Two shortcuts
+// bring it near natm:
+//  * screening: every factor is at most 1, so P_i <= Q_i, the product of its
+//    factors with the four atoms nearest to the point.  Where Q_i < 2^-70 the
+//    atom's P_i is dropped from the sum (and w = 0 if it is the host atom).
+//    The dropped terms total at most natm 2^-70, far below the rounding of the
+//    sum (which is at least the host cell's P, of order 0.1..1), so the
+//    weights agree with the full ordered products to within an ulp, and in
+//    almost every point bit for bit;
+//  * exact skips: where mu <= -0.994 the rounded p3(mu) is -1 or -1 + 2^-53
+//    and s = (1 - p3)/2 rounds to exactly 1, so the factor leaves P unchanged
+//    and is not evaluated (for x in [0.994, 1] the second iterate of p is
+//    1 - e with e < 2^-27, and the third rounds to 1 or 1 - 2^-53).
+// The point-atom distances are kept in shared memory as floats (for up to
+// kBeckeCacheAtoms atoms) for the skip test, which allows for their rounding;
+// the factors themselves use exact FP64 distances.
 // ---------------------------------------------------------------------------
 // Arithmetic is written with explicit round-to-nearest intrinsics: no FMA
-// contraction, so every weight is bit-identical to the reference's IEEE
-// double arithmetic (which has no fused operations on its path).
+// contraction, so the factors round as the reference's IEEE double arithmetic
+// (which has no fused operations on its path).
 __device__ __forceinline__ double dist3(double ax, double ay, double az, double bx, double by, double bz) {
   const double dx = __dsub_rn(ax, bx), dy = __dsub_rn(ay, by), dz = __dsub_rn(az, bz);
   return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
@@ -36,46 +52,111 @@ __global__ void k_atom_dist(const double* __restrict__ atoms, int natm, double* 
                     atoms[3 * hi + 2]);
 }
 
-__global__ void __launch_bounds__(128) k_becke(const double* __restrict__ atoms, const double* __restrict__ dist,
-                                               int natm, const double* __restrict__ px, const double* __restrict__ py,
-                                               const double* __restrict__ pz, const int* __restrict__ owner,
-                                               int64_t n, double* __restrict__ w) {
-  extern __shared__ double sa[];  // natm * 3 coordinates
-  for (int i = threadIdx.x; i < 3 * natm; i += blockDim.x) sa[i] = atoms[i];
-  __syncthreads();
+namespace {
+
+constexpr int kBeckeThreads = 128;
+constexpr int kBeckeCacheAtoms = 128;       // float distance cache in shared memory up to this many atoms
+constexpr double kBeckeEdge = 0.9941;      // d <= -kBeckeEdge R_ik => mu <= -0.994 after rounding
+constexpr double kBeckeTau = 0x1p-70;      // P_i bound below which an atom's term is dropped
+
+// s(mu_ik) of the reference for d = r_i - r_k and R = |R_i - R_k|.  The
+// reference's pair orientation, mu = (r_i - r_k)/dst(k,i) for k < i and
+// -(r_k - r_i)/dst(i,k) for k > i, is the same rounded value: IEEE
+// subtraction and division are exactly antisymmetric.  mu0(mu, 0) =
+// p(p(p(mu))), p(q) = q (3 - q^2) / 2; the halvings are multiplications by
+// 0.5, which round exactly as the divisions by 2 do.
+__device__ __forceinline__ double becke_s(double d, double R) {
+  double q = __ddiv_rn(d, R);
+#pragma unroll
+  for (int it = 0; it < 3; ++it) q = __dmul_rn(__dmul_rn(q, __dsub_rn(3.0, __dmul_rn(q, q))), 0.5);
+  return __dmul_rn(__dsub_rn(1.0, q), 0.5);
+}
+
+template <bool kCache>
+__global__ void __launch_bounds__(kBeckeThreads) k_becke(const double* __restrict__ atoms,
+                                                         const double* __restrict__ dist, int natm,
+                                                         const double* __restrict__ px, const double* __restrict__ py,
+                                                         const double* __restrict__ pz,
+                                                         const int* __restrict__ owner, int64_t n,
+                                                         double* __restrict__ w) {
+  extern __shared__ float srf[];  // kCache: r[k][thread] as float
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   const double x = px[p], y = py[p], z = pz[p];
   const int a = owner[p];
+  auto r_of = [&](int k) {
+    return dist3(__ldg(atoms + 3 * k), __ldg(atoms + 3 * k + 1), __ldg(atoms + 3 * k + 2), x, y, z);
+  };
+  // the four atoms nearest to the point (sorted) and their exact distances
+  int nb[4] = {-1, -1, -1, -1};
+  double nr[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
+  for (int k = 0; k < natm; ++k) {
+    const double r = r_of(k);
+    if (kCache) srf[k * kBeckeThreads + threadIdx.x] = (float)r;
+    if (r < nr[3]) {
+      int j = 3;
+      for (; j > 0 && nr[j - 1] > r; --j) {
+        nr[j] = nr[j - 1];
+        nb[j] = nb[j - 1];
+      }
+      nr[j] = r;
+      nb[j] = k;
+    }
+  }
   double sum = 0.0, pa = 0.0;
   for (int i = 0; i < natm; ++i) {
-    const double ri = dist3(sa[3 * i], sa[3 * i + 1], sa[3 * i + 2], x, y, z);
-    double P = 1.0;
-    for (int k = 0; k < natm && P != 0.0; ++k) {
-      if (k == i) continue;
-      const double rk = dist3(sa[3 * k], sa[3 * k + 1], sa[3 * k + 2], x, y, z);
-      // the reference's pair orientation: mu = (r_i - r_k)/dst(k,i) for k < i
-      double mu;
-      if (k < i) mu = __ddiv_rn(__dsub_rn(ri, rk), __ldg(dist + k * natm + i));
-      else mu = -__ddiv_rn(__dsub_rn(rk, ri), __ldg(dist + i * natm + k));
-      // mu0(mu, 0) = p(p(p(mu))), p(q) = q (3 - q^2) / 2; the halvings are
-      // multiplications by 0.5, which round exactly as the divisions by 2 do
-      double q = mu;
+    const double ri = r_of(i);
+    const double* Ri = dist + (int64_t)i * natm;
+    // screening bound from the nearest atoms
+    double Q = 1.0;
 #pragma unroll
-      for (int it = 0; it < 3; ++it) q = __dmul_rn(__dmul_rn(q, __dsub_rn(3.0, __dmul_rn(q, q))), 0.5);
-      P = __dmul_rn(P, __dmul_rn(__dsub_rn(1.0, q), 0.5));
+    for (int c = 0; c < 4; ++c) {
+      const int k = nb[c];
+      if (k < 0 || k == i) continue;
+      const double R = __ldg(Ri + k);
+      const double d = __dsub_rn(ri, nr[c]);
+      if (d > -__dmul_rn(kBeckeEdge, R)) Q *= becke_s(d, R);
     }
-    sum = __dadd_rn(sum, P);
+    if (Q < kBeckeTau) continue;
+    // the ordered product, factors that are exactly 1 skipped
+    double P = 1.0;
+    for (int k = 0; k < natm; ++k) {
+      if (k == i) continue;
+      const double R = __ldg(Ri + k);
+      const double edge = __dmul_rn(kBeckeEdge, R);
+      if (kCache) {
+        // the float distance is within 2^-24 r of the exact one
+        const double rf = (double)srf[k * kBeckeThreads + threadIdx.x];
+        if (ri - rf <= -(edge + 1.2e-7 * rf)) continue;
+      }
+      const double d = __dsub_rn(ri, r_of(k));
+      if (d <= -edge) continue;
+      P = __dmul_rn(P, becke_s(d, R));
+      if (P == 0.0) break;
+    }
+    if (P != 0.0) sum = __dadd_rn(sum, P);  // zeros leave the ascending sum unchanged
     if (i == a) pa = P;
   }
   w[p] = __ddiv_rn(pa, sum);
 }
 
-void launch_becke(const double* atoms, double* dist, int natm, const double* px, const double* py, const double* pz,
-                  const int* owner, int64_t n, double* w, cudaStream_t st) {
+}  // namespace
+
+cudaError_t launch_becke(const double* atoms, double* dist, int natm, const double* px, const double* py,
+                         const double* pz, const int* owner, int64_t n, double* w, cudaStream_t st) {
   k_atom_dist<<<(natm * natm + 255) / 256, 256, 0, st>>>(atoms, natm, dist);
-  const size_t smem = (size_t)(3 * natm) * sizeof(double);
-  k_becke<<<(unsigned)((n + 127) / 128), 128, smem, st>>>(atoms, dist, natm, px, py, pz, owner, n, w);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || n == 0) return e;
+  const unsigned nb = (unsigned)((n + kBeckeThreads - 1) / kBeckeThreads);
+  if (natm <= kBeckeCacheAtoms) {
+    const int smem = natm * kBeckeThreads * (int)sizeof(float);
+    e = cudaFuncSetAttribute(k_becke<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    k_becke<true><<<nb, kBeckeThreads, smem, st>>>(atoms, dist, natm, px, py, pz, owner, n, w);
+  } else {
+    k_becke<false><<<nb, kBeckeThreads, 0, st>>>(atoms, dist, natm, px, py, pz, owner, n, w);
+  }
+  return cudaGetLastError();
 }
 
 __global__ void k_scale_inplace(double* __restrict__ x, const double* __restrict__ s, int64_t n) {

@@ -30,13 +30,38 @@ constexpr int kMaxAtoms = PGXC_NOALLOC_MAX_ATOMS;
 // Scratch: atom-atom distance matrix, row-major natoms x natoms (2 MiB).
 static __device__ __align__(256) double g_becke_dist[kMaxAtoms * kMaxAtoms];
 
-// Device address of g_becke_dist per device ordinal, resolved once.  In host
-// code the name g_becke_dist is only a host-side shadow symbol, not a device
-// address, so the address must come from cudaGetSymbolAddress on a context of
-// that device.
+// Device address of g_becke_dist per device ordinal, resolved once per CUDA
+// context.  In host code the name g_becke_dist is only a host-side shadow
+// symbol, not a device address, so the address must come from
+// cudaGetSymbolAddress on a context of that device.  The cache remembers the
+// context it was resolved in: after cudaDeviceReset, or when the caller makes
+// another context current on the same ordinal, the address is resolved again
+// instead of reusing one that belongs to a destroyed or different context.
 constexpr int kMaxDevices = 64;
-double* g_dist_addr[kMaxDevices] = {};
+struct SymbolSlot {
+  void* ctx = nullptr;
+  double* addr = nullptr;
+};
+SymbolSlot g_dist_addr[kMaxDevices];
 std::mutex g_mu;
+
+// The calling thread's current CUDA context (CUcontext as an opaque pointer),
+// through the driver entry point the runtime exposes, so that the library does
+// not link libcuda itself.  nullptr when the entry point is unavailable.
+void* current_context() {
+  using CtxGetCurrent = int (*)(void**);  // CUresult cuCtxGetCurrent(CUcontext*)
+  static CtxGetCurrent fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      return (CtxGetCurrent) nullptr;
+    return reinterpret_cast<CtxGetCurrent>(f);
+  }();
+  void* ctx = nullptr;
+  if (!fn || fn(&ctx) != 0) return nullptr;
+  return ctx;
+}
 
 // The message is read back with pgxc_last_error(NULL).
 int fail(int code, const std::string& msg) {
@@ -62,22 +87,24 @@ extern "C" int pgxc_becke_weights_noalloc(int32_t natoms, const double* d_coords
   if (dev < 0 || dev >= kMaxDevices) return fail(PGXC_ENOTSUP, "device ordinal beyond the supported range");
   double* dist = nullptr;
   {
-    // one-time set-up on this device (the current device)
+    // set-up on this device (the current device), once per context
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_dist_addr[dev]) {
+    void* ctx = current_context();
+    SymbolSlot& slot = g_dist_addr[dev];
+    if (!slot.addr || !ctx || slot.ctx != ctx) {
       void* p = nullptr;
       e = cudaGetSymbolAddress(&p, g_becke_dist);
       if (e != cudaSuccess || !p)
         return fail(PGXC_ECUDA, std::string("cudaGetSymbolAddress(g_becke_dist): ") + cudaGetErrorString(e));
-      g_dist_addr[dev] = static_cast<double*>(p);
+      slot.addr = static_cast<double*>(p);
+      slot.ctx = ctx;
     }
-    dist = g_dist_addr[dev];
+    dist = slot.addr;
   }
   // d_pts is (npts, 3) column-major; the kernels write every entry they read
   // of the scratch (distance matrix) before reading it.
-  pgxc::launch_becke(d_coords, dist, natoms, d_pts, d_pts + npts, d_pts + 2 * npts, d_point_atom, npts, d_w_out,
-                     static_cast<cudaStream_t>(stream));
-  e = cudaGetLastError();
+  e = pgxc::launch_becke(d_coords, dist, natoms, d_pts, d_pts + npts, d_pts + 2 * npts, d_point_atom, npts, d_w_out,
+                         static_cast<cudaStream_t>(stream));
   if (e != cudaSuccess) return fail(PGXC_ECUDA, std::string("Becke kernels: ") + cudaGetErrorString(e));
   return PGXC_OK;
 }

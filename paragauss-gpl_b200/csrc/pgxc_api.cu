@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include "gradient.h"
+#include "grid.h"
 #include "kernels.h"
 #include "mixed.h"
 #include "pgxc_common.cuh"
@@ -255,8 +256,61 @@ static int validate_basis(pgxc_ctx* c, const pgxc_geometry* geo, const pgxc_basi
   return PGXC_OK;
 }
 
-int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid* grid, const pgxc_options* opt,
-                pgxc_ctx** out) {
+namespace {
+
+// Grid of a spec: shells kept per atom (r < 40 bohr) and the first point of each atom.
+int spec_layout(pgxc_ctx* c, const pgxc_geometry* geo, const pgxc_grid_spec* spec, std::vector<int64_t>& off,
+                std::vector<double>& ang) {
+  if (!geo || geo->natoms <= 0 || !geo->coords) return set_err(c, PGXC_EINVAL, "bad geometry");
+  if (!spec || !spec->nrad || !spec->radius) return set_err(c, PGXC_EINVAL, "grid spec needs nrad and radius");
+  if (lebedev_rule(spec->nang, ang) != 0)
+    return set_err(c, PGXC_EINVAL, "no Lebedev-McLaren rule with " + std::to_string(spec->nang) +
+                                       " points (6, 8, 12, 14, 26, 38, 50, 78, 86, 110, 146, 194, 302)");
+  off.assign((size_t)geo->natoms + 1, 0);
+  for (int a = 0; a < geo->natoms; ++a) {
+    if (spec->nrad[a] <= 0 || !(spec->radius[a] > 0.0) || !std::isfinite(spec->radius[a]))
+      return set_err(c, PGXC_EINVAL, "grid spec: nrad and radius must be positive");
+    off[(size_t)a + 1] = off[(size_t)a] + radial_shells(spec->nrad[a], spec->radius[a]) * spec->nang;
+  }
+  return PGXC_OK;
+}
+
+// The spec's grid into device arrays gx, gy, gz, gw (SoA, n points) and owner.
+int spec_generate(pgxc_ctx* c, const pgxc_geometry* geo, const pgxc_grid_spec* spec, const std::vector<int64_t>& off,
+                  const std::vector<double>& ang, double* gx, double* gy, double* gz, double* gw, int* owner,
+                  cudaStream_t st) {
+  const int natm = geo->natoms;
+  const int64_t n = off.back();
+  double *datoms = nullptr, *drc = nullptr, *dang = nullptr;
+  int64_t* doff = nullptr;
+  int* dnr = nullptr;
+  cudaError_t e = cudaMalloc(&datoms, sizeof(double) * 3 * natm);
+  if (e == cudaSuccess) e = cudaMalloc(&drc, sizeof(double) * natm);
+  if (e == cudaSuccess) e = cudaMalloc(&dang, sizeof(double) * ang.size());
+  if (e == cudaSuccess) e = cudaMalloc(&doff, sizeof(int64_t) * off.size());
+  if (e == cudaSuccess) e = cudaMalloc(&dnr, sizeof(int) * natm);
+  const bool oom = e == cudaErrorMemoryAllocation;
+  if (e == cudaSuccess) e = cudaMemcpy(datoms, geo->coords, sizeof(double) * 3 * natm, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(drc, spec->radius, sizeof(double) * natm, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dang, ang.data(), sizeof(double) * ang.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(doff, off.data(), sizeof(int64_t) * off.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dnr, spec->nrad, sizeof(int) * natm, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = launch_atomic_grid(natm, datoms, doff, drc, dnr, dang, spec->nang, n, gx, gy, gz, gw, owner, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(datoms);
+  cudaFree(drc);
+  cudaFree(dang);
+  cudaFree(doff);
+  cudaFree(dnr);
+  if (e != cudaSuccess)
+    return set_err(c, oom ? PGXC_ENOMEM : PGXC_ECUDA, std::string("atomic grid: ") + cudaGetErrorString(e));
+  return PGXC_OK;
+}
+
+// pgxc_create with either a host grid or a grid spec (exactly one non-NULL)
+int create_impl(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid* grid, const pgxc_grid_spec* spec,
+                const pgxc_options* opt, pgxc_ctx** out) {
   if (!out) return set_err(nullptr, PGXC_EINVAL, "out is NULL");
   *out = nullptr;
   pgxc_ctx* c = new (std::nothrow) pgxc_ctx();
@@ -278,17 +332,28 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
     return fail(set_err(c, PGXC_ENOTSUP, "open-shell (ispin=2) builds need the screened layout (screen_threshold >= 0)"));
   if (o.precision != PGXC_PREC_FP64 && o.precision != PGXC_PREC_MIXED_INT8)
     return fail(set_err(c, PGXC_EINVAL, "unknown precision mode"));
-  if (!grid || grid->npts <= 0 || !grid->grdpts) return fail(set_err(c, PGXC_EINVAL, "empty grid"));
-  if (grid->weights_are_raw && !grid->point_atom)
-    return fail(set_err(c, PGXC_EINVAL, "raw weights need point_atom"));
+  std::vector<int64_t> spec_off;
+  std::vector<double> spec_ang;
+  if (spec) {
+    int sst = spec_layout(c, geo, spec, spec_off, spec_ang);
+    if (sst) return fail(sst);
+    if (spec_off.back() <= 0) return fail(set_err(c, PGXC_EINVAL, "empty grid"));
+  } else {
+    if (!grid || grid->npts <= 0 || !grid->grdpts) return fail(set_err(c, PGXC_EINVAL, "empty grid"));
+    if (grid->weights_are_raw && !grid->point_atom)
+      return fail(set_err(c, PGXC_EINVAL, "raw weights need point_atom"));
+  }
   int64_t nexp_tot, ncon_tot;
   int st = validate_basis(c, geo, bas, c->shells, c->nbas, c->lmax, nexp_tot, ncon_tot);
   if (st) return fail(st);
-  if (!all_finite(grid->grdpts, 4 * grid->npts)) return fail(set_err(c, PGXC_ENONFINITE, "non-finite grid input"));
-  if (grid->weights_are_raw)
-    for (int64_t i = 0; i < grid->npts; ++i)
-      if (grid->point_atom[i] < 0 || grid->point_atom[i] >= geo->natoms)
-        return fail(set_err(c, PGXC_EINVAL, "point_atom out of range"));
+  if (!spec) {
+    if (!all_finite(grid->grdpts, 4 * grid->npts)) return fail(set_err(c, PGXC_ENONFINITE, "non-finite grid input"));
+    if (grid->weights_are_raw)
+      for (int64_t i = 0; i < grid->npts; ++i)
+        if (grid->point_atom[i] < 0 || grid->point_atom[i] >= geo->natoms)
+          return fail(set_err(c, PGXC_EINVAL, "point_atom out of range"));
+  }
+  const bool raw_weights = spec || grid->weights_are_raw;
   st = check_device(c, o.device);
   if (st) return fail(st);
   if (cudaSetDevice(c->device) != cudaSuccess) return fail(set_err(c, PGXC_ECUDA, "cudaSetDevice failed"));
@@ -296,7 +361,7 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
   for (auto& e : c->ev) CUDA_TRY(c, cudaEventCreate(&e));
   for (auto& e : c->kev) CUDA_TRY(c, cudaEventCreate(&e));
   c->natm = geo->natoms;
-  c->npts = grid->npts;
+  c->npts = spec ? spec_off.back() : grid->npts;
   BuildArgs& a = c->a;
   a.nshells = (int)c->shells.size();
   a.xc = make_xc_const(o.functional);
@@ -385,25 +450,31 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
   const int64_t n = c->npts;
   double* dgrid;
   if ((st = dalloc(c, &dgrid, 4 * (size_t)n))) return fail(st);
-  CUDA_TRY(c, cudaMemcpy(dgrid, grid->grdpts, 4 * sizeof(double) * n, cudaMemcpyHostToDevice));
+  if (!spec) CUDA_TRY(c, cudaMemcpy(dgrid, grid->grdpts, 4 * sizeof(double) * n, cudaMemcpyHostToDevice));
   a.px = dgrid;
   a.py = dgrid + n;
   a.pz = dgrid + 2 * n;
   a.w = dgrid + 3 * n;
-  if (grid->weights_are_raw) {
+  if (raw_weights) {
     // w <- w_raw * Becke partition weight of the host atom (mkgrid :3135-3137)
     int* downer;
     double* dbecke;
     if ((st = dalloc(c, &downer, n)) || (st = dalloc(c, &dbecke, n)) ||
         (st = dalloc(c, &c->d_dist, (size_t)c->natm * c->natm)))
       return fail(st);
-    CUDA_TRY(c, cudaMemcpy(downer, grid->point_atom, sizeof(int) * n, cudaMemcpyHostToDevice));
+    if (spec) {
+      // the grid itself is built on the device (grid_main_calc)
+      if ((st = spec_generate(c, geo, spec, spec_off, spec_ang, dgrid, dgrid + n, dgrid + 2 * n, dgrid + 3 * n, downer,
+                              c->stream)))
+        return fail(st);
+    } else {
+      CUDA_TRY(c, cudaMemcpy(downer, grid->point_atom, sizeof(int) * n, cudaMemcpyHostToDevice));
+    }
     // the raw weights and hosts stay for the nuclear gradient (pgxc_xc_gradient)
     if ((st = dalloc(c, &c->d_wraw, n))) return fail(st);
     CUDA_TRY(c, cudaMemcpy(c->d_wraw, dgrid + 3 * n, sizeof(double) * n, cudaMemcpyDeviceToDevice));
     c->d_owner = downer;
-    launch_becke(datoms, c->d_dist, c->natm, a.px, a.py, a.pz, downer, n, dbecke, c->stream);
-    CUDA_TRY(c, cudaGetLastError());
+    CUDA_TRY(c, launch_becke(datoms, c->d_dist, c->natm, a.px, a.py, a.pz, downer, n, dbecke, c->stream));
     launch_scale_inplace(dgrid + 3 * n, dbecke, n, c->stream);
     CUDA_TRY(c, cudaStreamSynchronize(c->stream));
   }
@@ -422,7 +493,6 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
     in.atoms = geo->coords;
     in.natm = c->natm;
     in.nbas = c->nbas;
-    in.grdpts = grid->grdpts;
     in.npts = n;
     in.exps = bas->exponents;
     in.norms = bas->norms;
@@ -512,6 +582,44 @@ int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
   *out = c;
   return PGXC_OK;
 }
+
+}  // namespace
+
+int pgxc_create(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid* grid, const pgxc_options* opt,
+                pgxc_ctx** out) {
+  return create_impl(geo, bas, grid, nullptr, opt, out);
+}
+
+int pgxc_create_on_grid(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid_spec* spec,
+                        const pgxc_options* opt, pgxc_ctx** out) {
+  if (!spec) return set_err(nullptr, PGXC_EINVAL, "spec is NULL");
+  return create_impl(geo, bas, nullptr, spec, opt, out);
+}
+
+int pgxc_atomic_grid_size(const pgxc_geometry* geo, const pgxc_grid_spec* spec, int64_t* npts) {
+  if (!npts) return set_err(nullptr, PGXC_EINVAL, "npts is NULL");
+  std::vector<int64_t> off;
+  std::vector<double> ang;
+  int st = spec_layout(nullptr, geo, spec, off, ang);
+  if (st) return st;
+  *npts = off.back();
+  return PGXC_OK;
+}
+
+int pgxc_atomic_grid(const pgxc_geometry* geo, const pgxc_grid_spec* spec, int64_t npts, double* d_grdpts,
+                     int32_t* d_point_atom, void* stream) {
+  std::vector<int64_t> off;
+  std::vector<double> ang;
+  int st = spec_layout(nullptr, geo, spec, off, ang);
+  if (st) return st;
+  if (npts != off.back())
+    return set_err(nullptr, PGXC_EINVAL, "npts must be " + std::to_string(off.back()) + " (pgxc_atomic_grid_size)");
+  if (!d_grdpts || !d_point_atom) return set_err(nullptr, PGXC_EINVAL, "NULL output");
+  if ((st = check_device(nullptr, -1))) return st;
+  return spec_generate(nullptr, geo, spec, off, ang, d_grdpts, d_grdpts + npts, d_grdpts + 2 * npts,
+                       d_grdpts + 3 * npts, d_point_atom, static_cast<cudaStream_t>(stream));
+}
+
 
 // Ensure C / occ buffers for nocc orbitals.
 static int ensure_occ(pgxc_ctx* c, int nocc) {
@@ -795,6 +903,9 @@ int pgxc_xc_gradient(pgxc_ctx* c, const double* C, const double* occ, int32_t nb
   if (!c->d_owner)
     return set_err(c, PGXC_ENOTSUP, "the XC gradient needs a grid created with raw weights and point_atom "
                                     "(the grid moves with its atoms)");
+  if (c->sym)
+    return set_err(c, PGXC_ENOTSUP, "the XC gradient is C1 only: a context with pgxc_set_symmetry applied may hold "
+                                    "a symmetry-reduced grid, whose per-atom gradient is not the full one");
   if (!all_finite(C, (int64_t)nbas * nocc * ispin) || !all_finite(occ, (int64_t)nocc * ispin))
     return set_err(c, PGXC_ENONFINITE, "non-finite C or occ");
   CUDA_TRY(c, cudaSetDevice(c->device));
@@ -1448,23 +1559,25 @@ int pgxc_becke_weights(const pgxc_geometry* geo, int64_t npts, const double* pts
   int st = check_device(nullptr, -1);
   if (st) return st;
   const int natm = geo->natoms;
-  double *d, *datoms, *ddist;
-  int* downer;
-  if (cudaMalloc(&d, sizeof(double) * 4 * npts) != cudaSuccess) return set_err(nullptr, PGXC_ENOMEM, "cudaMalloc");
-  cudaMalloc(&datoms, sizeof(double) * 3 * natm);
-  cudaMalloc(&ddist, sizeof(double) * natm * natm);
-  cudaMalloc(&downer, sizeof(int) * npts);
-  cudaMemcpy(d, pts, sizeof(double) * 3 * npts, cudaMemcpyHostToDevice);
-  cudaMemcpy(datoms, geo->coords, sizeof(double) * 3 * natm, cudaMemcpyHostToDevice);
-  cudaMemcpy(downer, point_atom, sizeof(int) * npts, cudaMemcpyHostToDevice);
-  launch_becke(datoms, ddist, natm, d, d + npts, d + 2 * npts, downer, npts, d + 3 * npts, 0);
-  cudaError_t e = cudaDeviceSynchronize();
-  if (e == cudaSuccess) cudaMemcpy(w_out, d + 3 * npts, sizeof(double) * npts, cudaMemcpyDeviceToHost);
+  double *d = nullptr, *datoms = nullptr, *ddist = nullptr;
+  int* downer = nullptr;
+  cudaError_t e = cudaMalloc(&d, sizeof(double) * 4 * npts);
+  if (e == cudaSuccess) e = cudaMalloc(&datoms, sizeof(double) * 3 * natm);
+  if (e == cudaSuccess) e = cudaMalloc(&ddist, sizeof(double) * natm * natm);
+  if (e == cudaSuccess) e = cudaMalloc(&downer, sizeof(int) * npts);
+  const bool oom = e == cudaErrorMemoryAllocation;
+  if (e == cudaSuccess) e = cudaMemcpy(d, pts, sizeof(double) * 3 * npts, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(datoms, geo->coords, sizeof(double) * 3 * natm, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(downer, point_atom, sizeof(int) * npts, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = launch_becke(datoms, ddist, natm, d, d + npts, d + 2 * npts, downer, npts, d + 3 * npts, 0);
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e == cudaSuccess) e = cudaMemcpy(w_out, d + 3 * npts, sizeof(double) * npts, cudaMemcpyDeviceToHost);
   cudaFree(d);
   cudaFree(datoms);
   cudaFree(ddist);
   cudaFree(downer);
-  if (e != cudaSuccess) return set_err(nullptr, PGXC_ECUDA, cudaGetErrorString(e));
+  if (e != cudaSuccess)
+    return set_err(nullptr, oom ? PGXC_ENOMEM : PGXC_ECUDA, std::string("Becke weights: ") + cudaGetErrorString(e));
   return PGXC_OK;
 }
 

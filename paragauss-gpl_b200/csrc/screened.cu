@@ -28,6 +28,7 @@
 
 #include "basis.cuh"
 #include "dgemm.cuh"
+#include "grid.h"
 #include "kernels.h"
 #include "screened.h"
 #include "screened_mixed.h"
@@ -392,41 +393,6 @@ __global__ void k_spack(const double* __restrict__ V, int64_t nbas, bool sym2, i
 // ---------------------------------------------------------------------------
 namespace {
 
-uint64_t spread3(uint64_t v) {  // 21 bits -> every third bit
-  v &= 0x1fffff;
-  v = (v | v << 32) & 0x1f00000000ffffull;
-  v = (v | v << 16) & 0x1f0000ff0000ffull;
-  v = (v | v << 8) & 0x100f00f00f00f00full;
-  v = (v | v << 4) & 0x10c30c30c30c30c3ull;
-  v = (v | v << 2) & 0x1249249249249249ull;
-  return v;
-}
-
-// Morton order of the grid points (ties by index: deterministic)
-std::vector<int64_t> morton_order(const double* g, int64_t n) {
-  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-  for (int d = 0; d < 3; ++d)
-    for (int64_t i = 0; i < n; ++i) {
-      lo[d] = std::min(lo[d], g[d * n + i]);
-      hi[d] = std::max(hi[d], g[d * n + i]);
-    }
-  std::vector<std::pair<uint64_t, int64_t>> key((size_t)n);
-  for (int64_t i = 0; i < n; ++i) {
-    uint64_t k = 0;
-    for (int d = 0; d < 3; ++d) {
-      const double span = hi[d] - lo[d];
-      const double u = span > 0 ? (g[d * n + i] - lo[d]) / span : 0.0;
-      const uint64_t q = (uint64_t)std::min(2097151.0, std::max(0.0, u * 2097151.0));
-      k |= spread3(q) << d;
-    }
-    key[(size_t)i] = {k, i};
-  }
-  std::sort(key.begin(), key.end());
-  std::vector<int64_t> perm((size_t)n);
-  for (int64_t i = 0; i < n; ++i) perm[(size_t)i] = key[(size_t)i].second;
-  return perm;
-}
-
 // Squared radius beyond which radial function rr of shell S is dropped.
 double listing_r2(const DevShell& S, int rr, const double* exps, const double* norms, const double* contr,
                   double threshold, double sa_fac) {
@@ -525,19 +491,18 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
   const int64_t ntiles = (n + 127) / 128;
   sp->ntiles = ntiles;
   {
-    std::vector<int64_t> perm = morton_order(in.grdpts, n);
-    perm.resize((size_t)ntiles * 128, -1);
+    // Morton order of the points, on the device (ties by point index)
+    const int64_t nq = ntiles * 128;
     int64_t* dperm;
-    SP_TRY(cudaMalloc(&dperm, sizeof(int64_t) * perm.size()), "cudaMalloc");
-    const size_t nq = perm.size();
-    cudaError_t e = cudaMemcpy(dperm, perm.data(), sizeof(int64_t) * nq, cudaMemcpyHostToDevice);
+    SP_TRY(cudaMalloc(&dperm, sizeof(int64_t) * nq), "cudaMalloc");
+    cudaError_t e = morton_perm_device(a.px, a.py, a.pz, n, nq, dperm, st);
     if (e == cudaSuccess) e = sp_alloc(sp, &sp->qx, 4 * nq);
     if (e == cudaSuccess) {
       sp->qy = sp->qx + nq;
       sp->qz = sp->qx + 2 * nq;
       sp->qw = sp->qx + 3 * nq;
-      k_gather_points<<<(unsigned)((nq + 255) / 256), 256, 0, st>>>(dperm, (int64_t)nq, a.px, a.py, a.pz, a.w,
-                                                                   sp->qx, sp->qy, sp->qz, sp->qw);
+      k_gather_points<<<(unsigned)((nq + 255) / 256), 256, 0, st>>>(dperm, nq, a.px, a.py, a.pz, a.w, sp->qx,
+                                                                   sp->qy, sp->qz, sp->qw);
       e = cudaStreamSynchronize(st);
     }
     cudaFree(dperm);

@@ -37,7 +37,6 @@ struct ScreenInput {
   const double* atoms;        // host, 3 x natm
   int natm;
   int64_t nbas;
-  const double* grdpts;       // host, npts x 4 column-major (x, y, z, w)
   int64_t npts;
   const double* exps;         // host
   const double* norms;        // host

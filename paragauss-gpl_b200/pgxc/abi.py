@@ -96,6 +96,25 @@ class Grid(ct.Structure):
     ]
 
 
+class GridSpec(ct.Structure):
+    _fields_ = [
+        ("nrad", _i32p),
+        ("radius", _f64p),
+        ("nang", ct.c_int32),
+    ]
+
+
+class MarshalledSpec:
+    """pgxc_grid_spec of a case built on an atomic grid: its nrad, nang and the
+    Pople radius of each element (pgxc/grid.py)."""
+
+    def __init__(self, case):
+        from . import grid as G
+        self.nrad = np.full(len(case.coords), int(case.meta["nrad"]), dtype=np.int32)
+        self.radius = np.array([G.POPLE_RADIUS[int(z)] for z in case.Z], dtype=np.float64)
+        self.spec = GridSpec(i32p(self.nrad), f64p(self.radius), int(case.meta["nang"]))
+
+
 class Options(ct.Structure):
     _fields_ = [
         ("functional", ct.c_int32),

@@ -2,14 +2,16 @@
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libpgxc.so")
 SOURCES = ["pgxc_api.cu", "kernels_fp64.cu", "kernels_aux.cu", "mixed.cu", "noalloc.cu", "screened.cu",
-           "screened_mixed.cu", "symmetry.cu", "gradient.cu"]
+           "screened_mixed.cu", "symmetry.cu", "gradient.cu", "grid.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
-              "-Xcompiler", "-fPIC", "-shared"]
+              "-Xcompiler", "-fPIC"]
+OBJDIR = os.path.join(PKG, "_build")
 
 
 def nvcc():
@@ -31,9 +33,23 @@ def needs_build():
 
 
 def build(force=False, verbose=False):
+    """Compile every source to an object (in parallel), then link the library."""
     if not force and not needs_build():
         return LIB
-    cmd = [nvcc()] + NVCC_FLAGS + [os.path.join(CSRC, s) for s in SOURCES] + ["-lcublas", "-o", LIB]
+    os.makedirs(OBJDIR, exist_ok=True)
+    cc = nvcc()
+
+    def compile_one(src):
+        obj = os.path.join(OBJDIR, os.path.splitext(src)[0] + ".o")
+        cmd = [cc] + NVCC_FLAGS + ["-c", os.path.join(CSRC, src), "-o", obj]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True, cwd=CSRC)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 4)) as ex:
+        objs = list(ex.map(compile_one, SOURCES))
+    cmd = [cc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared"] + objs + ["-lcublas", "-o", LIB]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True, cwd=CSRC)

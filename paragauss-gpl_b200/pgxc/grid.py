@@ -5,17 +5,16 @@ RADIALGRID builds it (modules/grid_module.f90:1246-1301):
     r_i = R (i/(N+1-i))^2,  w_i = 2 R^3 (N+1) i^5 / (N+1-i)^7,
 points with r >= 40 bohr are cut from the outside in.
 
-Angular part: ParaGauss uses Lebedev-McLaren tables (INIGRD, :1359-2100).
-Those tables are published data that this project does not reproduce; the
-angular rule here is a Gauss-Legendre (cos theta) x uniform (phi) product
-rule of similar size and exactness (degree 2*n_theta-1).  The grid is an
-input of the XC build (grdpts), so the choice does not affect parity: the
-oracle and the GPU integrate the identical points and weights.
+Angular part: the Lebedev-McLaren rules of INIGRD (:1359-2100), restated in
+pgxc/lebedev.py, unrotated (the orientation the reference uses when weight
+gradients are on, angular_grid :1339-1341).
 
 One-centre weights are w_ang * w_rad * 4 pi (grid_main_calc, :425-432);
 points are ordered atom -> radial shell -> angular point, as AGRID is.
 """
 import numpy as np
+
+from . import lebedev
 
 # Radii (bohr) of Gill, Johnson & Pople, Chem. Phys. Lett. 209, 506 (1993),
 # the "Pople radius" option of ParaGauss's GRIDATOM namelist.
@@ -23,41 +22,42 @@ POPLE_RADIUS = {1: 1.0000, 6: 1.2308, 7: 1.0256, 8: 0.8791}
 
 RAD_LIMIT = 40.0
 
-# angular rules standing in for the Lebedev sizes named by the workloads
-ANGULAR_RULES = {194: (10, 20), 302: (12, 25), 110: (8, 14), 50: (5, 10)}
 
 
 def radial_grid(nrad, radius):
-    """RADIALGRID: returns (r, w) with the r >= 40 cut applied."""
-    rhn = nrad + 1
+    """RADIALGRID: returns (r, w) with the r >= 40 cut applied.
+
+    The integer powers of the reference, (I/RHNI)**2, RCUR**3, (I/RHNI)**5 and
+    RHNI**2, are written as products evaluated left to right, the same
+    operations the device grid builder rounds, so both give identical points.
+    """
+    rhn = nrad + 1.0
     i_top = nrad
     for i in range(nrad, 0, -1):
-        r = radius * (i / (rhn - i)) ** 2
+        t = i / (rhn - i)
         i_top = i
-        if r < RAD_LIMIT:
+        if radius * (t * t) < RAD_LIMIT:
             break
+    else:
+        i_top = 0
     i = np.arange(1, i_top + 1, dtype=np.float64)
     rhni = rhn - i
-    r = radius * (i / rhni) ** 2
-    w = 2 * radius ** 3 * rhn * (i / rhni) ** 5 / rhni ** 2
+    t = i / rhni
+    t2 = t * t
+    r = radius * t2
+    r3 = radius * radius * radius
+    w = 2.0 * r3 * rhn * (t2 * t2 * t) / (rhni * rhni)
     return r, w
 
 
-def angular_grid(n_theta, n_phi):
-    """Product rule on the unit sphere; weights sum to 1."""
-    x, wx = np.polynomial.legendre.leggauss(n_theta)
-    phi = (np.arange(n_phi) + 0.5) * (2 * np.pi / n_phi)
-    ct_, ph = np.meshgrid(x, phi, indexing="ij")
-    st = np.sqrt(1 - ct_ ** 2)
-    pts = np.stack([st * np.cos(ph), st * np.sin(ph), ct_], axis=-1).reshape(-1, 3)
-    w = np.repeat(wx / 2.0, n_phi) / n_phi
-    return pts, w
+def angular_grid(nang):
+    """INIGRD: the Lebedev-McLaren rule with nang points; weights sum to 1."""
+    return lebedev.rule(nang)
 
 
 def atomic_grids(coords, Z, nrad, nang):
     """grid_main_calc without pruning (NPART=1): returns xyz, raw w, host atom."""
-    nt, nph = ANGULAR_RULES[nang]
-    apts, aw = angular_grid(nt, nph)
+    apts, aw = angular_grid(nang)
     xs, ws, owner = [], [], []
     for a, (c, z) in enumerate(zip(coords, Z)):
         r, wr = radial_grid(nrad, POPLE_RADIUS[int(z)])

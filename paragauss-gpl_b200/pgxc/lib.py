@@ -32,6 +32,9 @@ def lib():
     vp = ct.c_void_p
     L.pgxc_default_options.argtypes = [P(abi.Options)]
     L.pgxc_create.argtypes = [P(abi.Geometry), P(abi.Basis), P(abi.Grid), P(abi.Options), P(vp)]
+    L.pgxc_create_on_grid.argtypes = [P(abi.Geometry), P(abi.Basis), P(abi.GridSpec), P(abi.Options), P(vp)]
+    L.pgxc_atomic_grid_size.argtypes = [P(abi.Geometry), P(abi.GridSpec), P(ct.c_int64)]
+    L.pgxc_atomic_grid.argtypes = [P(abi.Geometry), P(abi.GridSpec), ct.c_int64, vp, vp, vp]
     L.pgxc_nbas.argtypes = [vp, P(ct.c_int32)]
     L.pgxc_screen_stats.argtypes = [vp, P(ct.c_int64), P(ct.c_int64), P(ct.c_int64), P(ct.c_double)]
     L.pgxc_build.argtypes = [vp, abi._f64p, abi._f64p, ct.c_int32, ct.c_int32, ct.c_int32, abi._f64p, ct.c_int64,
@@ -76,7 +79,9 @@ class Context:
     """One geometry: pgxc_create ... pgxc_destroy."""
 
     def __init__(self, case, precision="fp64", weighted=True, device=-1, max_chunk_points=0,
-                 screen_threshold=0.0, batch_points=128, keep_orbitals=False):
+                 screen_threshold=0.0, batch_points=128, keep_orbitals=False, on_grid=False):
+        """on_grid: build the case's atomic grid and its Becke weights on the
+        device (pgxc_create_on_grid) instead of passing the host grid."""
         L = lib()
         self.case = case
         self._m = abi.Marshalled(case, weighted=weighted)
@@ -92,8 +97,13 @@ class Context:
         o.keep_orbitals = int(bool(keep_orbitals))
         self.opt = o
         h = ct.c_void_p()
-        st = L.pgxc_create(ct.byref(self._m.geometry), ct.byref(self._m.basis), ct.byref(self._m.grid),
-                           ct.byref(o), ct.byref(h))
+        if on_grid:
+            self._spec = abi.MarshalledSpec(case)
+            st = L.pgxc_create_on_grid(ct.byref(self._m.geometry), ct.byref(self._m.basis),
+                                       ct.byref(self._spec.spec), ct.byref(o), ct.byref(h))
+        else:
+            st = L.pgxc_create(ct.byref(self._m.geometry), ct.byref(self._m.basis), ct.byref(self._m.grid),
+                               ct.byref(o), ct.byref(h))
         _check(st)
         self.h = h
         nb = ct.c_int32()

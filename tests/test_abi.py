@@ -110,3 +110,17 @@ def test_no_device_fails_loudly(case):
 def test_strerror():
     for s in range(0, -8, -1):
         assert lib.lib().pgxc_strerror(s)
+
+
+def test_grid_spec_size_matches_the_host_grid():
+    """pgxc_atomic_grid_size needs no device: shells with r < 40 bohr times the rule."""
+    import ctypes as ct
+    for c in (cases.config(1), cases.small_case(functional="PBE", seed=31, natoms=5, nrad=30, nang=302)):
+        m = abi.Marshalled(c, weighted=False)
+        sp = abi.MarshalledSpec(c)
+        n = ct.c_int64()
+        assert lib.lib().pgxc_atomic_grid_size(ct.byref(m.geometry), ct.byref(sp.spec), ct.byref(n)) == 0
+        assert n.value == c.npts
+    sp.spec.nang = 100
+    assert lib.lib().pgxc_atomic_grid_size(ct.byref(m.geometry), ct.byref(sp.spec), ct.byref(n)) == abi.PGXC_EINVAL
+    assert ct.sizeof(abi.GridSpec) == 24

@@ -70,15 +70,33 @@ def test_device_becke_matches_oracle():
     np.testing.assert_allclose(w_gpu, w_ref, rtol=0, atol=2e-16)
 
 
-def test_device_becke_many_atoms_bit_identical():
-    """72 atoms, 25,200 points: the device weights are the oracle's bit for bit."""
+def _becke_agreement(c):
+    w_gpu = lib.becke_weights(c)
+    w_ref = O.becke(c)
+    dw = np.abs(w_gpu - w_ref)
+    # terms the device drops are below 2^-70 of a point's sum: within 2e-16,
+    # and bit for bit at nearly every point
+    assert float(dw.max()) <= 2e-16, float(dw.max())
+    assert np.mean(w_gpu == w_ref) > 0.999, float(np.mean(w_gpu == w_ref))
+
+
+def test_device_becke_many_atoms_matches_oracle():
+    """72 atoms, 50-point rule: the device weights are the oracle's to 2e-16."""
     rng = np.random.default_rng(21)
     els, xyz = cases.random_cluster(rng, [("C", 36), ("H", 36)], 13.0, 1.1)
     c = cases.build_case("becke72", els, xyz, seed=21, exp_range=(0.1, 100.0), nrad=8, nang=50,
                          functional="VWN", nocc=1, orthonormalise=False)
-    w_gpu = lib.becke_weights(c)
-    w_ref = O.becke(c)
-    assert np.array_equal(w_gpu, w_ref), float(np.max(np.abs(w_gpu - w_ref)))
+    _becke_agreement(c)
+
+
+def test_device_becke_uncached_many_atoms_matches_oracle():
+    """140 atoms: beyond the shared-memory distance cache the point-atom
+    distances are recomputed; the weights still match the oracle to 2e-16."""
+    rng = np.random.default_rng(23)
+    els, xyz = cases.random_cluster(rng, [("C", 70), ("H", 70)], 17.0, 1.1)
+    c = cases.build_case("becke140", els, xyz, seed=23, exp_range=(0.1, 100.0), nrad=3, nang=50,
+                         functional="VWN", nocc=1, orthonormalise=False)
+    _becke_agreement(c)
 
 
 @LAYOUTS
