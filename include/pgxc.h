@@ -484,13 +484,14 @@ int pgxc_becke_weights(const pgxc_geometry* geo, int64_t npts,
  * Same result as pgxc_becke_weights, but every argument is device memory:
  *   d_coords (natoms*3), d_pts (npts,3) column-major, d_point_atom (npts),
  *   d_w_out (npts).
- * The only scratch, the natoms x natoms distance matrix, lives in a fixed
- * device array inside the library (PGXC_NOALLOC_MAX_ATOMS^2 doubles, 2 MiB,
- * present on every GPU that loads the library until the process exits);
- * natoms above PGXC_NOALLOC_MAX_ATOMS is rejected with PGXC_EINVAL.  It makes
- * no cudaMalloc/cudaFree call.  The first call on a device looks up the
- * array's device address (cudaGetSymbolAddress); make that first call before
- * any stream capture.  Work is queued on `stream` (a cudaStream_t, NULL for
+ * The only scratch, the natoms x natoms matrices of atom-atom distances and
+ * of their reciprocals, lives in a fixed device array inside the library
+ * (2 PGXC_NOALLOC_MAX_ATOMS^2 doubles, 4 MiB, present on every GPU that loads
+ * the library until the process exits); natoms above PGXC_NOALLOC_MAX_ATOMS
+ * is rejected with PGXC_EINVAL.  It makes no cudaMalloc/cudaFree call.  The
+ * first call on a device (and again after the caller makes a different CUDA
+ * context current on it) looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture.  Work is queued on `stream` (a cudaStream_t, NULL for
  * the legacy default stream) and the call returns without waiting: the
  * weights are valid once that stream is synchronised.  All calls on a device
  * share the scratch array, which keeps the last call's contents (each call

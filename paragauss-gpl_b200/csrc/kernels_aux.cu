@@ -18,46 +18,58 @@ namespace pgxc {
 // product, with the reference's rounding, and w = P_a / sum_i P_i with the sum
 // in ascending i.
 //
-// Cost: natm^2 pair evaluations per point in the reference.  Two shortcuts
-// bring it near natm:
-//  * screening: every factor is at most 1, so P_i <= Q_i, the product of its
-//    factors with the four atoms nearest to the point.  Where Q_i < 2^-70 the
-//    atom's P_i is dropped from the sum (and w = 0 if it is the host atom).
-//    The dropped terms total at most natm 2^-70, far below the rounding of the
-//    sum (which is at least the host cell's P, of order 0.1..1), so the
-//    weights agree with the full ordered products to within an ulp, and in
-//    almost every point bit for bit;
-//  * exact skips: where mu <= -0.994 the rounded p3(mu) is -1 or -1 + 2^-53
-//    and s = (1 - p3)/2 rounds to exactly 1, so the factor leaves P unchanged
-//    and is not evaluated (for x in [0.994, 1] the second iterate of p is
+// Cost: natm^2 pair evaluations per point in the reference.  The kernel drops
+// the terms that cannot matter at double precision:
+//  * the nearest atom's P_near is formed first (exactly); sum_i P_i >= P_near;
+//  * every factor is at most 1, so an atom whose product (or the product of
+//    its factors with the four atoms nearest to the point) falls below
+//    tau = 2^-56 P_near / natm contributes less than 2^-56 of the sum in
+//    total: it is dropped (and w = 0 if it is the host atom).  The weights
+//    then agree with the full ordered products to within 2^-56 relative (a
+//    quarter of an ulp of the sum), and bit for bit at nearly every point;
+//  * where mu <= -0.994 the rounded p3(mu) is -1 or -1 + 2^-53 and
+//    s = (1 - p3)/2 rounds to exactly 1, so the factor leaves P unchanged and
+//    is not evaluated (for x in [0.994, 1] the second iterate of p is
 //    1 - e with e < 2^-27, and the third rounds to 1 or 1 - 2^-53).
-// The point-atom distances are kept in shared memory as floats (for up to
-// kBeckeCacheAtoms atoms) for the skip test, which allows for their rounding;
-// the factors themselves use exact FP64 distances.
+// mu = d / R is the correctly rounded quotient by Markstein's method
+// (P. W. Markstein, IBM J. Res. Dev. 34 (1990) 111): with y = RN(1/R),
+// q = RN(d y), r = d - R q (exact with one FMA), mu = RN(q + r y).
+// The point-atom distances are kept in shared memory (exact) for up to
+// kBeckeCacheAtoms atoms and recomputed beyond.
 // ---------------------------------------------------------------------------
 // Arithmetic is written with explicit round-to-nearest intrinsics: no FMA
-// contraction, so the factors round as the reference's IEEE double arithmetic
-// (which has no fused operations on its path).
+// contraction where the reference has none, so the factors round as the
+// reference's IEEE double arithmetic.
 __device__ __forceinline__ double dist3(double ax, double ay, double az, double bx, double by, double bz) {
   const double dx = __dsub_rn(ax, bx), dy = __dsub_rn(ay, by), dz = __dsub_rn(az, bz);
   return __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)));
 }
 
-__global__ void k_atom_dist(const double* __restrict__ atoms, int natm, double* __restrict__ dist) {
+// dist[i][j] = |R_i - R_j|; rdist[i][j] = RN(1 / dist[i][j]) (0 on the diagonal)
+__global__ void k_atom_dist(const double* __restrict__ atoms, int natm, double* __restrict__ dist,
+                            double* __restrict__ rdist) {
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= natm * natm) return;
   const int i = idx / natm, j = idx % natm;
   const int lo = i < j ? i : j, hi = i < j ? j : i;  // dst(lo,hi) computed once, mirrored
-  dist[idx] = dist3(atoms[3 * lo], atoms[3 * lo + 1], atoms[3 * lo + 2], atoms[3 * hi], atoms[3 * hi + 1],
-                    atoms[3 * hi + 2]);
+  const double d = dist3(atoms[3 * lo], atoms[3 * lo + 1], atoms[3 * lo + 2], atoms[3 * hi], atoms[3 * hi + 1],
+                         atoms[3 * hi + 2]);
+  dist[idx] = d;
+  if (rdist) rdist[idx] = i == j ? 0.0 : __drcp_rn(d);
 }
 
 namespace {
 
 constexpr int kBeckeThreads = 128;
-constexpr int kBeckeCacheAtoms = 128;       // float distance cache in shared memory up to this many atoms
+constexpr int kBeckeCacheAtoms = 64;       // exact distance cache in shared memory up to this many atoms
 constexpr double kBeckeEdge = 0.9941;      // d <= -kBeckeEdge R_ik => mu <= -0.994 after rounding
-constexpr double kBeckeTau = 0x1p-70;      // P_i bound below which an atom's term is dropped
+
+// d / R correctly rounded, y = RN(1 / R) (Markstein)
+__device__ __forceinline__ double div_rn(double d, double R, double y) {
+  const double q = __dmul_rn(d, y);
+  const double r = __fma_rn(-q, R, d);
+  return __fma_rn(r, y, q);
+}
 
 // s(mu_ik) of the reference for d = r_i - r_k and R = |R_i - R_k|.  The
 // reference's pair orientation, mu = (r_i - r_k)/dst(k,i) for k < i and
@@ -65,8 +77,8 @@ constexpr double kBeckeTau = 0x1p-70;      // P_i bound below which an atom's te
 // subtraction and division are exactly antisymmetric.  mu0(mu, 0) =
 // p(p(p(mu))), p(q) = q (3 - q^2) / 2; the halvings are multiplications by
 // 0.5, which round exactly as the divisions by 2 do.
-__device__ __forceinline__ double becke_s(double d, double R) {
-  double q = __ddiv_rn(d, R);
+__device__ __forceinline__ double becke_s(double d, double R, double y) {
+  double q = div_rn(d, R, y);
 #pragma unroll
   for (int it = 0; it < 3; ++it) q = __dmul_rn(__dmul_rn(q, __dsub_rn(3.0, __dmul_rn(q, q))), 0.5);
   return __dmul_rn(__dsub_rn(1.0, q), 0.5);
@@ -74,25 +86,27 @@ __device__ __forceinline__ double becke_s(double d, double R) {
 
 template <bool kCache>
 __global__ void __launch_bounds__(kBeckeThreads) k_becke(const double* __restrict__ atoms,
-                                                         const double* __restrict__ dist, int natm,
+                                                         const double* __restrict__ dist,
+                                                         const double* __restrict__ rdist, int natm,
                                                          const double* __restrict__ px, const double* __restrict__ py,
                                                          const double* __restrict__ pz,
                                                          const int* __restrict__ owner, int64_t n,
                                                          double* __restrict__ w) {
-  extern __shared__ float srf[];  // kCache: r[k][thread] as float
+  extern __shared__ double sr[];  // kCache: r[k][thread]
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   const double x = px[p], y = py[p], z = pz[p];
   const int a = owner[p];
   auto r_of = [&](int k) {
+    if (kCache) return sr[k * kBeckeThreads + threadIdx.x];
     return dist3(__ldg(atoms + 3 * k), __ldg(atoms + 3 * k + 1), __ldg(atoms + 3 * k + 2), x, y, z);
   };
-  // the four atoms nearest to the point (sorted) and their exact distances
+  // the four atoms nearest to the point (sorted) and their distances
   int nb[4] = {-1, -1, -1, -1};
   double nr[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
   for (int k = 0; k < natm; ++k) {
-    const double r = r_of(k);
-    if (kCache) srf[k * kBeckeThreads + threadIdx.x] = (float)r;
+    const double r = dist3(__ldg(atoms + 3 * k), __ldg(atoms + 3 * k + 1), __ldg(atoms + 3 * k + 2), x, y, z);
+    if (kCache) sr[k * kBeckeThreads + threadIdx.x] = r;
     if (r < nr[3]) {
       int j = 3;
       for (; j > 0 && nr[j - 1] > r; --j) {
@@ -103,36 +117,45 @@ __global__ void __launch_bounds__(kBeckeThreads) k_becke(const double* __restric
       nb[j] = k;
     }
   }
-  double sum = 0.0, pa = 0.0;
-  for (int i = 0; i < natm; ++i) {
-    const double ri = r_of(i);
+  // P_i as the ordered product, factors that are exactly 1 skipped; 0 once
+  // the partial product is below tau (the factors left are at most 1)
+  auto ordered = [&](int i, double ri, double tau) {
     const double* Ri = dist + (int64_t)i * natm;
-    // screening bound from the nearest atoms
-    double Q = 1.0;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-      const int k = nb[c];
-      if (k < 0 || k == i) continue;
-      const double R = __ldg(Ri + k);
-      const double d = __dsub_rn(ri, nr[c]);
-      if (d > -__dmul_rn(kBeckeEdge, R)) Q *= becke_s(d, R);
-    }
-    if (Q < kBeckeTau) continue;
-    // the ordered product, factors that are exactly 1 skipped
+    const double* Yi = rdist + (int64_t)i * natm;
     double P = 1.0;
     for (int k = 0; k < natm; ++k) {
       if (k == i) continue;
       const double R = __ldg(Ri + k);
-      const double edge = __dmul_rn(kBeckeEdge, R);
-      if (kCache) {
-        // the float distance is within 2^-24 r of the exact one
-        const double rf = (double)srf[k * kBeckeThreads + threadIdx.x];
-        if (ri - rf <= -(edge + 1.2e-7 * rf)) continue;
-      }
       const double d = __dsub_rn(ri, r_of(k));
-      if (d <= -edge) continue;
-      P = __dmul_rn(P, becke_s(d, R));
-      if (P == 0.0) break;
+      if (d <= -__dmul_rn(kBeckeEdge, R)) continue;
+      P = __dmul_rn(P, becke_s(d, R, __ldg(Yi + k)));
+      if (P < tau) return 0.0;
+    }
+    return P;
+  };
+  const int i0 = nb[0];
+  const double P0 = ordered(i0, nr[0], 0.0);
+  const double tau = fmax(0x1p-56 * P0 / natm, 0x1p-1000);
+  double sum = 0.0, pa = 0.0;
+  for (int i = 0; i < natm; ++i) {
+    double P;
+    if (i == i0) {
+      P = P0;
+    } else {
+      const double ri = r_of(i);
+      const double* Ri = dist + (int64_t)i * natm;
+      const double* Yi = rdist + (int64_t)i * natm;
+      // bound from the nearest atoms
+      double Q = 1.0;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int k = nb[c];
+        if (k < 0 || k == i) continue;
+        const double R = __ldg(Ri + k);
+        const double d = __dsub_rn(ri, nr[c]);
+        if (d > -__dmul_rn(kBeckeEdge, R)) Q *= becke_s(d, R, __ldg(Yi + k));
+      }
+      P = Q < tau ? 0.0 : ordered(i, ri, tau);
     }
     if (P != 0.0) sum = __dadd_rn(sum, P);  // zeros leave the ascending sum unchanged
     if (i == a) pa = P;
@@ -144,17 +167,19 @@ __global__ void __launch_bounds__(kBeckeThreads) k_becke(const double* __restric
 
 cudaError_t launch_becke(const double* atoms, double* dist, int natm, const double* px, const double* py,
                          const double* pz, const int* owner, int64_t n, double* w, cudaStream_t st) {
-  k_atom_dist<<<(natm * natm + 255) / 256, 256, 0, st>>>(atoms, natm, dist);
+  // dist holds 2 natm^2 doubles: the distances, then their reciprocals
+  double* rdist = dist + (int64_t)natm * natm;
+  k_atom_dist<<<(natm * natm + 255) / 256, 256, 0, st>>>(atoms, natm, dist, rdist);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || n == 0) return e;
   const unsigned nb = (unsigned)((n + kBeckeThreads - 1) / kBeckeThreads);
   if (natm <= kBeckeCacheAtoms) {
-    const int smem = natm * kBeckeThreads * (int)sizeof(float);
+    const int smem = natm * kBeckeThreads * (int)sizeof(double);
     e = cudaFuncSetAttribute(k_becke<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    k_becke<true><<<nb, kBeckeThreads, smem, st>>>(atoms, dist, natm, px, py, pz, owner, n, w);
+    k_becke<true><<<nb, kBeckeThreads, smem, st>>>(atoms, dist, rdist, natm, px, py, pz, owner, n, w);
   } else {
-    k_becke<false><<<nb, kBeckeThreads, 0, st>>>(atoms, dist, natm, px, py, pz, owner, n, w);
+    k_becke<false><<<nb, kBeckeThreads, 0, st>>>(atoms, dist, rdist, natm, px, py, pz, owner, n, w);
   }
   return cudaGetLastError();
 }

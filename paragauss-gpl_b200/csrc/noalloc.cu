@@ -6,7 +6,8 @@
 // come from its own OpenACC / CUDA Fortran data regions or memory pool, or a
 // process that has reserved the whole device for its own allocator.  For them
 // pgxc_becke_weights_noalloc takes device pointers for every input and output
-// and keeps its only scratch, the distance matrix, in the fixed array below.
+// and keeps its only scratch, the atom-atom distance and reciprocal-distance
+// matrices, in the fixed array below.
 //
 // The array is a file-scope __device__ object: it exists on every GPU that
 // loads this library, from module load until process exit, and is shared by
@@ -27,8 +28,9 @@ namespace {
 // Largest geometry the allocation-free entry point accepts.
 constexpr int kMaxAtoms = PGXC_NOALLOC_MAX_ATOMS;
 
-// Scratch: atom-atom distance matrix, row-major natoms x natoms (2 MiB).
-static __device__ __align__(256) double g_becke_dist[kMaxAtoms * kMaxAtoms];
+// Scratch: atom-atom distances and their reciprocals, two row-major
+// natoms x natoms matrices (4 MiB at the limit).
+static __device__ __align__(256) double g_becke_dist[2 * kMaxAtoms * kMaxAtoms];
 
 // Device address of g_becke_dist per device ordinal, resolved once per CUDA
 // context.  In host code the name g_becke_dist is only a host-side shadow

@@ -460,7 +460,7 @@ int create_impl(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
     int* downer;
     double* dbecke;
     if ((st = dalloc(c, &downer, n)) || (st = dalloc(c, &dbecke, n)) ||
-        (st = dalloc(c, &c->d_dist, (size_t)c->natm * c->natm)))
+        (st = dalloc(c, &c->d_dist, 2 * (size_t)c->natm * c->natm)))
       return fail(st);
     if (spec) {
       // the grid itself is built on the device (grid_main_calc)
@@ -1563,7 +1563,7 @@ int pgxc_becke_weights(const pgxc_geometry* geo, int64_t npts, const double* pts
   int* downer = nullptr;
   cudaError_t e = cudaMalloc(&d, sizeof(double) * 4 * npts);
   if (e == cudaSuccess) e = cudaMalloc(&datoms, sizeof(double) * 3 * natm);
-  if (e == cudaSuccess) e = cudaMalloc(&ddist, sizeof(double) * natm * natm);
+  if (e == cudaSuccess) e = cudaMalloc(&ddist, 2 * sizeof(double) * natm * natm);
   if (e == cudaSuccess) e = cudaMalloc(&downer, sizeof(int) * npts);
   const bool oom = e == cudaErrorMemoryAllocation;
   if (e == cudaSuccess) e = cudaMemcpy(d, pts, sizeof(double) * 3 * npts, cudaMemcpyHostToDevice);
