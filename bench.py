@@ -203,17 +203,19 @@ def fp64_comparison(torch, case, sub, local, args):
     dham = torch.zeros(case.xc_length, dtype=torch.float64, device="cuda")
     dsum = torch.zeros(2, dtype=torch.float64, device="cuda")
 
+    tm = {}
+
     def step():
         dham.zero_()
         dsum.zero_()
-        ctx.build_device(dC.data_ptr(), docc.data_ptr(), dham.data_ptr(), dsum.data_ptr())
+        tm.update(ctx.build_device(dC.data_ptr(), docc.data_ptr(), dham.data_ptr(), dsum.data_ptr()))
 
     for _ in range(2):
         step()
     steps = max(1, min(args.steps, 3))
     ms = cuda_timer(torch, step, steps) / steps
     out = {"ham": dham.cpu().numpy(), "exc": float(dsum[0]), "nel": float(dsum[1]), "ms": ms,
-           "value": case.npts / (ms * 1e-3)}
+           "value": case.npts / (ms * 1e-3), "timings": dict(tm)}
     ctx.close()
     # the unscreened build costs 4 N nbas^2 flop: time it only where that is seconds
     if args.screen >= 0 and 4.0 * case.npts * case.nbas ** 2 < 2e14:
@@ -224,6 +226,95 @@ def fp64_comparison(torch, case, sub, local, args):
         ctx.close()
     del dC, docc, dham, dsum
     torch.cuda.empty_cache()
+    return out
+
+
+def becke_leg(torch, case):
+    """Becke partition weights of the workload's grid on the device (the
+    allocation-free entry: device inputs, events around the kernels)."""
+    import ctypes as ct
+    from pgxc import lib
+    natm = len(case.coords)
+    if natm > 512:
+        return None
+    L = lib.lib()
+    L.pgxc_becke_weights_noalloc.argtypes = [ct.c_int32, ct.c_void_p, ct.c_int64, ct.c_void_p, ct.c_void_p,
+                                             ct.c_void_p, ct.c_void_p]
+    coords = torch.from_numpy(np.ascontiguousarray(case.coords)).cuda()
+    pts = torch.from_numpy(np.ascontiguousarray(case.grid_xyz.T).reshape(-1).copy()).cuda()
+    own = torch.from_numpy(case.point_atom.astype(np.int32)).cuda()
+    w = torch.zeros(case.npts, dtype=torch.float64, device="cuda")
+
+    def run():
+        st = L.pgxc_becke_weights_noalloc(natm, coords.data_ptr(), case.npts, pts.data_ptr(), own.data_ptr(),
+                                          w.data_ptr(), None)
+        if st != 0:
+            raise RuntimeError(L.pgxc_last_error(None))
+
+    run()
+    ms = cuda_timer(torch, run, 3) / 3
+    pairs = case.npts * natm * (natm - 1) / 2
+    byts = case.npts * (3 * 8 + 4 + 8)  # point coordinates and host atom in, weight out
+    return {"ms": ms, "points_per_s": case.npts / (ms * 1e-3), "pair_evals_per_s": pairs / (ms * 1e-3),
+            "achieved_gbs": byts / (ms * 1e-3) / 1e9,
+            "note": "FP64-ALU bound (natm^2/2 pair terms per point in the reference form); GB/s is secondary"}
+
+
+def kernel_table(case, screen, tm, prec, mp, tpeak, args):
+    """Per-kernel algorithmic work, measured time and roofline fraction of one
+    build (library CUDA events around each kernel)."""
+    from pgxc import abi
+    gga = abi.is_gga(case.functional)
+    arrays = 4 if gga else 1
+    hbm = mp["hbm_gbs"]
+    out = {}
+    if screen is not None:
+        nslots, sum_n2, ntl = screen["nslots"], screen["sum_n2"], screen["ntiles"]
+        npts_t = 128.0 * ntl
+        flops_x = 2.0 * 128 * sum_n2
+        flops_v = flops_x if gga else 0.5 * flops_x
+        # density: phi (+ grad phi) of every slot read once, rho (+ grad rho) written once
+        bytes_x = 8.0 * arrays * 128 * (nslots + ntl)
+        # potential: phi (+ grad phi) of every slot read once, A (+ B) per point
+        bytes_v = 8.0 * arrays * 128 * nslots + 8.0 * arrays * npts_t
+        bytes_b = 8.0 * arrays * 128 * nslots  # basis: phi (+ grad phi) written
+    else:
+        flops_x = 2.0 * case.npts * case.nbas ** 2
+        flops_v = flops_x if gga else 0.5 * flops_x
+        bytes_x = 8.0 * arrays * case.npts * (case.nbas + 1)
+        bytes_v = 8.0 * arrays * case.npts * (case.nbas + 1)
+        bytes_b = 8.0 * arrays * case.npts * case.nbas
+    mixed = prec != "fp64"
+    issued = OZAKI_PAIRS if mixed else 1
+    names = {"density": "k_sm_density" if mixed else ("k_sdensity" if screen is not None else "k_density"),
+             "potential": "k_sm_vpot" if mixed else ("k_svpot" if screen is not None else "k_vpot")}
+    if mixed and screen is not None:
+        # the potential contraction reads the digits of phi and Z (5 B each per slot-point)
+        bytes_v = 10.0 * 128 * nslots
+    for key, ms, byts, fl in (("density", tm["xgemm_ms"], bytes_x, flops_x),
+                              ("potential", tm["vgemm_ms"], bytes_v, flops_v)):
+        gbs = byts / (ms * 1e-3) / 1e9
+        tf = fl / (ms * 1e-3) / 1e12
+        out[names[key]] = {"ms": ms, "algorithmic_bytes": byts, "achieved_gbs": gbs, "hbm_frac": gbs / hbm,
+                           "algorithmic_tflops": tf, "issued_tops": tf * issued, "tensor_frac": tf * issued / tpeak}
+    if mixed and screen is not None:
+        # Z = A phi (+ B . grad phi) and the digits of Z and phi: the rest of the potential phase
+        zms = tm["potential_ms"] - tm["vgemm_ms"]
+        zb = 8.0 * arrays * 128 * nslots + 8.0 * arrays * npts_t + 10.0 * 128 * nslots
+        out["k_sm_zquant"] = {"ms": zms, "algorithmic_bytes": zb, "achieved_gbs": zb / (zms * 1e-3) / 1e9,
+                              "hbm_frac": zb / (zms * 1e-3) / 1e9 / hbm,
+                              "note": "phase time less the contraction kernel (includes the packing kernel)"}
+    fb = 72.0 if gga else 32.0
+    fms = tm["functional_ms"]
+    out["k_functional"] = {"ms": fms, "algorithmic_bytes": fb * case.npts,
+                           "achieved_gbs": fb * case.npts / (fms * 1e-3) / 1e9,
+                           "hbm_frac": fb * case.npts / (fms * 1e-3) / 1e9 / hbm,
+                           "note": "phase time: the functional kernel and its block-sum reduction"}
+    bms = tm["basis_ms"]
+    out["k_basis_items"] = {"ms": bms, "algorithmic_bytes": bytes_b, "achieved_gbs": bytes_b / (bms * 1e-3) / 1e9,
+                            "hbm_frac": bytes_b / (bms * 1e-3) / 1e9 / hbm,
+                            "note": "phase time: one launch per angular momentum and the padding kernel; "
+                                    "FP64 ALU + exp bound with the stores of phi (and grad phi)"}
     return out
 
 
@@ -550,47 +641,46 @@ def main():
     h2d = (nb * nocc + nocc) * 8
     d2h = (case.xc_length + 2) * 8
 
-    # roofline of the density kernel (the largest kernel of the build), per
-    # launch from the library's CUDA events around it
-    from pgxc import abi
-    gga = abi.is_gga(case.functional)
-    arrays = 4 if gga else 1
-    if screen is not None:
-        nlisted, sum_n2, ntl = screen["nlisted"], screen["sum_n2"], screen["ntiles"]
-        kflops = 2.0 * 128 * sum_n2                       # X = phi_sig P_sig, 2 B n_b^2 per tile
-        kbytes = 8.0 * arrays * 128 * (nlisted + ntl)     # phi (+ grad phi) of every listed pair, rho (+ grad rho)
-    else:
-        kflops = 2.0 * case.npts * case.nbas ** 2
-        kbytes = 8.0 * arrays * case.npts * (case.nbas + 1)
-    kms = last_tm["xgemm_ms"]
+    # roofline of the dominant kernel of the build (the larger of the two
+    # contraction kernels; per launch from the library's CUDA events around it)
     roof = None
+    kernels = None
     if rank == 0:
         mp = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-        achieved = kbytes / (kms * 1e-3) / 1e9
-        tflops = kflops / (kms * 1e-3) / 1e12
+        dgemm_peak = fp64_peak_tflops(torch)
         if prec == "fp64":
-            tpeak = fp64_peak_tflops(torch)
+            tpeak = dgemm_peak
             tsrc = "cuBLAS DGEMM 8192^3 measured in this run (FP64 tensor pipe)"
-            tissued = tflops
         else:
             tpeak = mp["bf16_tflops"] * INT8_PER_BF16
             tsrc = "INT8 dense rate taken as 2 x MEASURED_PEAKS.json bf16_tflops (burst), of measured"
-            tissued = tflops * OZAKI_PAIRS
+        kernels = kernel_table(case, screen, last_tm, prec, mp, tpeak, args)
+        single = [k for k in kernels if k in ("k_sm_density", "k_sm_vpot", "k_sm_zquant", "k_sdensity", "k_svpot",
+                                              "k_density", "k_vpot")]
+        dom = max(single, key=lambda k: kernels[k]["ms"])
+        kd = kernels[dom]
         traffic = None
         tf = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tf):
-            traffic = json.load(open(tf)).get(f"{case.name}:{prec}:{args.screen:g}")
-        roof = {"bound": "hbm", "kernel": "density: X = phi_sig P_sig with fused rho, grad rho "
-                                          + ("(k_sm_density, tcgen05 kind::i8)" if prec != "fp64" else
-                                             "(k_sdensity, DMMA)" if screen is not None else "(k_density, DMMA)"),
-                "achieved": achieved, "peak": mp["hbm_gbs"], "unit": "GB/s", "frac": achieved / mp["hbm_gbs"],
-                "traffic": traffic, "peak_source": "MEASURED_PEAKS.json hbm_gbs, of measured",
-                "algorithmic_bytes": kbytes, "kernel_ms_per_build": kms,
-                "tensor": {"algorithmic_tflops": tflops, "issued_tflops_or_tops": tissued, "peak": tpeak,
-                           "frac_issued": tissued / tpeak, "peak_source": tsrc,
-                           "flops_per_build": kflops},
+            traffic = json.load(open(tf)).get(f"{case.name}:{prec}:{args.screen:g}:{dom}")
+        roof = {"bound": "hbm", "kernel": dom, "achieved": kd["achieved_gbs"], "peak": mp["hbm_gbs"], "unit": "GB/s",
+                "frac": kd["hbm_frac"], "traffic": traffic,
+                "peak_source": "MEASURED_PEAKS.json hbm_gbs, of measured",
+                "algorithmic_bytes": kd["algorithmic_bytes"], "kernel_ms_per_build": kd["ms"],
+                "tensor": None if "tensor_frac" not in kd else {
+                    "algorithmic_tflops": kd["algorithmic_tflops"], "issued_tflops_or_tops": kd["issued_tops"],
+                    "peak": tpeak, "frac_issued": kd["tensor_frac"], "peak_source": tsrc},
                 "phase_ms": {k: last_tm[k] for k in ("basis_ms", "density_ms", "functional_ms", "potential_ms",
                                                      "xgemm_ms", "vgemm_ms")}}
+        if fp64_leg is not None:
+            k64 = kernel_table(case, screen, fp64_leg["timings"], "fp64", mp, dgemm_peak, args)
+            kernels["fp64_build"] = {k: v for k, v in k64.items() if k in ("k_sdensity", "k_svpot", "k_density",
+                                                                          "k_vpot")}
+            kernels["fp64_build"]["fp64_tensor_peak_tflops"] = dgemm_peak
+            kernels["fp64_build"]["note"] = ("FP64 DMMA contractions of the drop-in build: algorithmic TFLOP/s "
+                                             "against cuBLAS DGEMM measured in this run")
+        if world == 1 and not args.profile:
+            kernels["k_becke"] = becke_leg(torch, case)
 
     out = None
     if rank == 0:
@@ -609,6 +699,8 @@ def main():
                        "l2": "no flush: each build streams several GB of basis/Z data (inputs larger than L2)"},
             "xc_builds_per_s": 1e3 / per_step, "E_xc": exc, "N_el": nel,
             "vs_fp64": None if fp64_leg is None else {
+                "fp64_phase_ms": {k: fp64_leg["timings"][k] for k in ("basis_ms", "density_ms", "functional_ms",
+                                                                      "potential_ms")},
                 "fp64_value": fp64_leg["value"], "fp64_ms_per_step": fp64_leg["ms"],
                 "speedup": fp64_leg["ms"] / per_step,
                 "dE_xc": exc - fp64_leg["exc"], "dN_el": nel - fp64_leg["nel"],
@@ -617,6 +709,7 @@ def main():
                 "note": "FP64 GPU build, same screening, same GPU, this run (matches the FP64 oracle to 1e-10); "
                         "fp64_dense: the unscreened FP64 build"},
             "roofline": roof,
+            "kernels": kernels,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": ms_e / args.steps},
             "gpu_launches": int(last_tm["kernel_launches"]) * args.steps,

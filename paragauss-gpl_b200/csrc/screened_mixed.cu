@@ -12,11 +12,11 @@
 //                    warps, two TMEM accumulator sets (MMA of slot block j+1
 //                    overlaps the epilogue of block j); fused FP64 epilogue
 //                    rho += X phi, grad rho += 2 X grad phi
-//   k_sm_vpot        Z = A phi (+ B . grad phi) in FP64 and the digits of phi
+//   k_sm_zquant      Z = A phi (+ B . grad phi) in FP64 and the digits of phi
 //                    (slice-interleaved per 8 slots: one copy per A block) and
-//                    of Z (slices one after another), one scale per (tile,
-//                    slot), formed by producer warps of the same kernel; then
-//                    H[S_t, S_t] += Z_t^T phi_t computed as phi_t Z_t^T (TMEM
+//                    of Z (slices one after another), one scale per
+//                    (tile, slot)                                       (A, B of V)
+//   k_sm_vpot        H[S_t, S_t] += Z_t^T phi_t computed as phi_t Z_t^T (TMEM
 //                    lane = column j of H), 128 x 48 slot blocks, K = the
 //                    tile's 128 points; scaled in FP64 and scatter-added
 //                    into the full matrix with atomics that run along rows
@@ -452,85 +452,48 @@ __global__ void __launch_bounds__(kDensThreads, 1)
   if (warp == 0) tc::tmem_dealloc(tbase, 512);
 }
 
+// ---------------------------------------------------------------------------
+// Z and the V operand digits: warp per slot, lane = 4 consecutive points
+// ---------------------------------------------------------------------------
 __device__ __forceinline__ double warp_max(double v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
 
-// Generic-proxy global writes -> visible to later bulk copies (async proxy).
-__device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
-
-// ---------------------------------------------------------------------------
-// H[S_t, S_t] += Z_t^T phi_t with Z = A phi (+ B . grad phi) formed in the same
-// kernel, scatter-added into V with FP64 atomics (LDA: fn_i <= fn_j only, H is
-// symmetric; GGA: the whole square, V = H + H^T when packing, the ham + ham^T
-// of modules/xc_hamiltonian.f90:1559-1566; Z is orbs_help of :1479-1482).
-//
-// Roles (persistent CTA, one per SM, tiles c, c + G, ...):
-//   warps 10-15  Z producers: per tile, Z = A phi (+ B . grad phi) in FP64 from
-//                the basis values, then the INT8 digits of phi and of Z with one
-//                scale per (tile, slot) (the largest |.| over the tile's 128
-//                points), written to this CTA's tile region of tF / tZ / fs / zs
-//                (global, read back from L2 by the bulk copies); up to two
-//                tiles ahead of the epilogue;
-//   warp 9       bulk copies: the phi block of each 128-slot block J once, the Z
-//                block of each (J, I) pair per K step (32 points);
-//   warp 8       MMA issuer: D = phi_J Z_I^T (TMEM lane = column j of H), 128 x
-//                48 slot blocks, K = the tile's 128 points in 4 steps;
-//   warps 0-7    epilogue: scaled FP64 atomics along rows of V.
-// ---------------------------------------------------------------------------
-constexpr int kVStages = 8;
-constexpr int kZWarps = 6;
-constexpr int kZThreads = kZWarps * 32;
-struct VSmem {
-  alignas(1024) int8_t a[2][4][kOpA];      // phi digits of a 128-slot block, all 4 K steps, double-buffered
-  alignas(1024) int8_t b[kVStages][kOpB];  // Z digits of a 48-slot block, one K step
-  uint64_t a_full[2], a_empty[2];
-  uint64_t full[kVStages];
-  uint64_t empty[kVStages];
-  uint64_t acc_full[2];
-  uint64_t acc_empty[2];
-  uint64_t tready[2];  // a tile's digits and scales are written (producers -> copier, epilogue)
-  uint64_t sfree[2];   // the epilogue is done with a tile (-> producers, two tiles later)
-  uint32_t tslot;
-};
-constexpr int kVThreads = tc::kWholeSmThreads;  // warps 0-7 epilogue, 8 MMA, 9 copies, 10-15 Z producers
-
-// LDA keeps j >= i: the last 48-slot row block I of column block J
-__device__ __forceinline__ int last_I(int J, int nI, bool all) { return all ? nI : min(nI, (kM * J + kM - 1) / kN + 1); }
-
-// Z producers, one tile: lane = 4 consecutive points, warp w takes the slot
-// pairs (i, i + kZWarps), i = w, w + 2 kZWarps, ...
 template <bool GGA>
-__device__ __forceinline__ void produce_z_tile(int zw, int lane, int64_t sb, int n, int64_t pbase,
-                                               const double* __restrict__ phi, const double* __restrict__ gx,
-                                               const double* __restrict__ gy, const double* __restrict__ gz,
-                                               const double* __restrict__ A, const double* __restrict__ Bx,
-                                               const double* __restrict__ By, const double* __restrict__ Bz,
-                                               int8_t* __restrict__ tZ, int8_t* __restrict__ tF,
-                                               double* __restrict__ zs, double* __restrict__ fs) {
-  // A and B of the lane's four points, for every slot of the tile (written
-  // by the functional kernel before this launch: read-only here)
-  const int q0 = lane * 4;
-  double ca[4], cb[3][4];
-#pragma unroll
-  for (int u = 0; u < 4; ++u) {
-    ca[u] = __ldg(A + pbase + q0 + u);
+__global__ void __launch_bounds__(256, 3) k_sm_zquant(const int64_t* __restrict__ tso, int64_t t0, int64_t s0,
+                                                   const double* __restrict__ phi, const double* __restrict__ gx,
+                                                   const double* __restrict__ gy, const double* __restrict__ gz,
+                                                   const double* __restrict__ A, const double* __restrict__ Bx,
+                                                   const double* __restrict__ By, const double* __restrict__ Bz,
+                                                   int8_t* __restrict__ tZ, int8_t* __restrict__ tF,
+                                                   double* __restrict__ zs, double* __restrict__ fs) {
+  __shared__ double sA[128], sB[3][128];
+  const int64_t t = t0 + blockIdx.x;
+  const int64_t sb = tso[t] - s0;
+  const int n = (int)(tso[t + 1] - tso[t]);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  if (tid < 128) {
+    const int64_t p = (int64_t)blockIdx.x * 128 + tid;
+    sA[tid] = A[p];
     if (GGA) {
-      cb[0][u] = __ldg(Bx + pbase + q0 + u);
-      cb[1][u] = __ldg(By + pbase + q0 + u);
-      cb[2][u] = __ldg(Bz + pbase + q0 + u);
+      sB[0][tid] = Bx[p];
+      sB[1][tid] = By[p];
+      sB[2][tid] = Bz[p];
     }
   }
+  __syncthreads();
   const int p0 = lane * 4;
   const int kstep = lane >> 3, kin = (lane & 7) * 4;
   const int64_t tile_off = sb * kDigBytesPerSlot;
-  for (int i0 = zw; i0 < n; i0 += 2 * kZWarps) {
+  // two adjacent slots per warp and iteration: the loads of both are in
+  // flight together, and their digit rows fill whole 32-byte sectors
+  for (int i0 = 2 * warp; i0 < n; i0 += 16) {
     double f[2][4], z[2][4];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const int i = i0 + kZWarps * h;
+      const int i = i0 + h;
       const int64_t o = (sb + min(i, n - 1)) * 128 + p0;
       const double2 a = *reinterpret_cast<const double2*>(phi + o);
       const double2 b = *reinterpret_cast<const double2*>(phi + o + 2);
@@ -541,19 +504,19 @@ __device__ __forceinline__ void produce_z_tile(int zw, int lane, int64_t sb, int
           const double* g = c == 0 ? gx : (c == 1 ? gy : gz);
           const double2 ga = *reinterpret_cast<const double2*>(g + o);
           const double2 gb = *reinterpret_cast<const double2*>(g + o + 2);
-          z[h][0] = (c == 0 ? 0.0 : z[h][0]) + cb[c][0] * ga.x;
-          z[h][1] = (c == 0 ? 0.0 : z[h][1]) + cb[c][1] * ga.y;
-          z[h][2] = (c == 0 ? 0.0 : z[h][2]) + cb[c][2] * gb.x;
-          z[h][3] = (c == 0 ? 0.0 : z[h][3]) + cb[c][3] * gb.y;
+          z[h][0] = (c == 0 ? 0.0 : z[h][0]) + sB[c][p0] * ga.x;
+          z[h][1] = (c == 0 ? 0.0 : z[h][1]) + sB[c][p0 + 1] * ga.y;
+          z[h][2] = (c == 0 ? 0.0 : z[h][2]) + sB[c][p0 + 2] * gb.x;
+          z[h][3] = (c == 0 ? 0.0 : z[h][3]) + sB[c][p0 + 3] * gb.y;
         }
       }
     }
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      const int i = i0 + kZWarps * h;
+      const int i = i0 + h;
       if (i >= n) break;
 #pragma unroll
-      for (int u = 0; u < 4; ++u) z[h][u] = GGA ? z[h][u] + ca[u] * f[h][u] : ca[u] * f[h][u];
+      for (int u = 0; u < 4; ++u) z[h][u] = GGA ? z[h][u] + sA[p0 + u] * f[h][u] : sA[p0 + u] * f[h][u];
       const double mz = warp_max(fmax(fmax(fabs(z[h][0]), fabs(z[h][1])), fmax(fabs(z[h][2]), fabs(z[h][3]))));
       const double mf = warp_max(fmax(fmax(fabs(f[h][0]), fabs(f[h][1])), fmax(fabs(f[h][2]), fabs(f[h][3]))));
       const int ez = scale_exp(mz), ef = scale_exp(mf);
@@ -580,13 +543,38 @@ __device__ __forceinline__ void produce_z_tile(int zw, int lane, int64_t sb, int
   }
 }
 
+// ---------------------------------------------------------------------------
+// H[S_t, S_t] += Z_t^T phi_t, scatter-added into V with FP64 atomics (LDA:
+// fn_i <= fn_j only, H is symmetric; GGA: the whole square, V = H + H^T when
+// packing, the ham + ham^T of modules/xc_hamiltonian.f90:1559-1566).
+// Computed as D = phi_J Z_I^T: the 128 TMEM lanes are columns j of H, so the
+// 32 atomics of a warp instruction run along one row of V (consecutive
+// functions, few sectors).  Pairs of 128-slot blocks J (A, phi) and 48-slot
+// blocks I (B, Z); K = the tile's 128 points in 4 steps; each A block is one
+// copy of whole 8-slot groups and stays resident for its 48-slot blocks.
+// Persistent like k_sm_density.
+// ---------------------------------------------------------------------------
+constexpr int kVStages = 8;
+struct VSmem {
+  alignas(1024) int8_t a[2][4][kOpA];      // phi digits of a 128-slot block, all 4 K steps, double-buffered
+  alignas(1024) int8_t b[kVStages][kOpB];  // Z digits of a 48-slot block, one K step
+  uint64_t a_full[2], a_empty[2];
+  uint64_t full[kVStages];
+  uint64_t empty[kVStages];
+  uint64_t acc_full[2];
+  uint64_t acc_empty[2];
+  uint32_t tslot;
+};
+constexpr int kVThreads = tc::kWholeSmThreads;  // warps 0-7 epilogue, 8 MMA, 9 producer, 10-15 idle
+
+// LDA keeps j >= i: the last 48-slot row block I of column block J
+__device__ __forceinline__ int last_I(int J, int nI, bool all) { return all ? nI : min(nI, (kM * J + kM - 1) / kN + 1); }
+
 template <bool GGA>
 __global__ void __launch_bounds__(kVThreads, 1)
     k_sm_vpot(const int64_t* __restrict__ tso, const int* __restrict__ slot_fn, int64_t t0, int64_t nt, int64_t s0,
-              const double* __restrict__ phi, const double* __restrict__ gx, const double* __restrict__ gy,
-              const double* __restrict__ gz, const double* __restrict__ A, const double* __restrict__ Bx,
-              const double* __restrict__ By, const double* __restrict__ Bz, int8_t* __restrict__ tF,
-              int8_t* __restrict__ tZ, double* fs, double* zs, double* __restrict__ V, int64_t ldv, int* err) {
+              const int8_t* __restrict__ tF, const int8_t* __restrict__ tZ, const double* __restrict__ fs,
+              const double* __restrict__ zs, double* __restrict__ V, int64_t ldv, int* err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   VSmem& S = *reinterpret_cast<VSmem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -595,8 +583,6 @@ __global__ void __launch_bounds__(kVThreads, 1)
     for (int q = 0; q < 2; ++q) {
       tc::mbar_init(&S.a_full[q], 1);
       tc::mbar_init(&S.a_empty[q], 1);
-      tc::mbar_init(&S.tready[q], kZThreads);
-      tc::mbar_init(&S.sfree[q], 256);
     }
     for (int s = 0; s < kVStages; ++s) {
       tc::mbar_init(&S.full[s], 1);
@@ -613,30 +599,10 @@ __global__ void __launch_bounds__(kVThreads, 1)
   tc::fence_after_sync();
   const uint32_t tbase = S.tslot;
   bool ok = true;
-  if (warp >= 10) {  // Z producers
-    const int zw = warp - 10;
-    int lt = 0;
-    for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x, ++lt) {
-      // at most two tiles ahead of the epilogue (tready / sfree are double-buffered)
-      if (lt >= 2 && !tc::mbar_wait(&S.sfree[lt & 1], ((lt >> 1) - 1) & 1)) {
-        ok = false;
-        break;
-      }
-      const int64_t sb = tso[t0 + ti] - s0;
-      const int n = (int)(tso[t0 + ti + 1] - tso[t0 + ti]);
-      produce_z_tile<GGA>(zw, lane, sb, n, ti * 128, phi, gx, gy, gz, A, Bx, By, Bz, tZ, tF, zs, fs);
-      fence_proxy_async_global();
-      tc::mbar_arrive(&S.tready[lt & 1]);
-    }
-    if (!ok) atomicExch(err, 1);
-  } else if (warp == 9) {
-    if (lane == 0) {  // copies: the phi block of each J once, the Z block of each (J, I) pair per K step
-      int it = 0, ia = 0, lt = 0;
-      for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x, ++lt) {
-        if (!tc::mbar_wait(&S.tready[lt & 1], (lt >> 1) & 1)) {
-          ok = false;
-          break;
-        }
+  if (warp == 9) {
+    if (lane == 0) {  // producer: the phi block of each J once, the Z block of each (J, I) pair per K step
+      int it = 0, ia = 0;
+      for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
         const int64_t sb = tso[t0 + ti] - s0;
         const int n = (int)(tso[t0 + ti + 1] - tso[t0 + ti]);
         const int nJ = (n + kM - 1) / kM, nI = (n + kN - 1) / kN;
@@ -705,31 +671,28 @@ __global__ void __launch_bounds__(kVThreads, 1)
       }
       if (!ok) atomicExch(err, 1);
     }
+  } else if (warp >= 10) {
+    // idle: the CTA holds the whole SM
   } else {  // epilogue: column j = 128 J + 32 (warp & 3) + lane of H, rows 24 (warp >> 2) .. of each 48-slot block
     const int half = warp >> 2;
     const uint32_t trow = tbase + ((uint32_t)((warp & 3) * 32) << 16);
-    int pp = 0, lt = 0;
-    for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x, ++lt) {
+    int pp = 0;
+    for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
       const int64_t sg = tso[t0 + ti];
       const int64_t sb = sg - s0;
       const int n = (int)(tso[t0 + ti + 1] - sg);
       const int nJ = (n + kM - 1) / kM, nI = (n + kN - 1) / kN;
       const int* sfn = slot_fn + sg;
-      // the tile's scales are written by the producers of this CTA (plain loads, not the read-only path)
-      if (!tc::mbar_wait(&S.tready[lt & 1], (lt >> 1) & 1)) {
-        ok = false;
-        break;
-      }
       for (int J = 0; J < nJ && ok; ++J) {
         const int j = J * kM + (warp & 3) * 32 + lane;
         const int fj = j < n ? __ldg(sfn + j) : -1;
-        const double fsj = j < n ? fs[sb + j] : 0.0;
+        const double fsj = j < n ? __ldg(fs + sb + j) : 0.0;
         for (int I = 0; I < last_I(J, nI, GGA); ++I, ++pp) {
           const int b = pp & 1;
           // row i of lane (< 24) of this warp's 24: its function and scale, broadcast below
           const int il = I * kN + half * 24 + lane;
           const int fil = (lane < 24 && il < n) ? __ldg(sfn + il) : -1;
-          const double zsl = (lane < 24 && il < n) ? zs[sb + il] : 0.0;
+          const double zsl = (lane < 24 && il < n) ? __ldg(zs + sb + il) : 0.0;
           if (!tc::mbar_wait_warp(&S.acc_full[b], (pp >> 1) & 1)) {
             ok = false;
             break;
@@ -747,7 +710,6 @@ __global__ void __launch_bounds__(kVThreads, 1)
           }
         }
       }
-      tc::mbar_arrive(&S.sfree[lt & 1]);
     }
     if (!ok) atomicExch(err, 1);
   }
@@ -876,17 +838,22 @@ int screen_mixed_potential(ScreenMixed* m, const int64_t* tso, const int* slot_f
                            double* V, int64_t ldv, cudaStream_t st, cudaEvent_t k0, cudaEvent_t k1) {
   (void)slot_tile;
   (void)ns;
+  if (m->gga)
+    k_sm_zquant<true><<<(unsigned)nt, 256, 0, st>>>(tso, t0, s0, phi, gx, gy, gz, A, Bx, By, Bz, m->tZ, m->tF,
+                                                    m->zs, m->fs);
+  else
+    k_sm_zquant<false><<<(unsigned)nt, 256, 0, st>>>(tso, t0, s0, phi, nullptr, nullptr, nullptr, A, nullptr,
+                                                     nullptr, nullptr, m->tZ, m->tF, m->zs, m->fs);
   if (k0) cudaEventRecord(k0, st);
   const unsigned grid = (unsigned)std::min<int64_t>(nt, m->nsm);
   if (m->gga)
-    k_sm_vpot<true><<<grid, kVThreads, tc::kWholeSmSmem, st>>>(tso, slot_fn, t0, nt, s0, phi, gx, gy, gz, A, Bx, By,
-                                                               Bz, m->tF, m->tZ, m->fs, m->zs, V, ldv, m->err);
+    k_sm_vpot<true><<<grid, kVThreads, tc::kWholeSmSmem, st>>>(tso, slot_fn, t0, nt, s0, m->tF, m->tZ, m->fs, m->zs, V, ldv,
+                                                   m->err);
   else
-    k_sm_vpot<false><<<grid, kVThreads, tc::kWholeSmSmem, st>>>(tso, slot_fn, t0, nt, s0, phi, nullptr, nullptr,
-                                                                nullptr, A, nullptr, nullptr, nullptr, m->tF, m->tZ,
-                                                                m->fs, m->zs, V, ldv, m->err);
+    k_sm_vpot<false><<<grid, kVThreads, tc::kWholeSmSmem, st>>>(tso, slot_fn, t0, nt, s0, m->tF, m->tZ, m->fs, m->zs, V, ldv,
+                                                    m->err);
   if (k1) cudaEventRecord(k1, st);
-  return 1;
+  return 2;
 }
 
 int screen_mixed_error_flag(ScreenMixed* m, cudaStream_t st, int* flag) {
