@@ -164,29 +164,30 @@ def algorithmic_flops(case):
     return x, v
 
 
-def cpu_baseline(case, weights, seconds):
+def cpu_baseline(case, weights, seconds, threads=0):
     """Oracle port on host cores over a bounded sample of the workload: whole
-    builds (or a contiguous prefix of the grid) repeated to ~`seconds`."""
+    builds (or a contiguous prefix of the grid) repeated to ~`seconds`;
+    threads = 0: all host threads."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     c = case
     c.grid_w = weights
-    threads = O.max_threads()
-    pilot = min(c.npts, 65536)
-    O.xc_build(c, pt_range=(0, min(c.npts, 4096)))  # thread start-up
+    threads = threads or O.max_threads()
+    pilot = min(c.npts, 65536 if threads > 1 else 8192)
+    O.xc_build(c, pt_range=(0, min(c.npts, 4096)), nthreads=threads)  # thread start-up
     t = time.perf_counter()
-    O.xc_build(c, pt_range=(0, pilot))
+    O.xc_build(c, pt_range=(0, pilot), nthreads=threads)
     rate = pilot / max(time.perf_counter() - t, 1e-6)
     n = int(min(c.npts, max(pilot, rate * seconds)))
     n = max(128, n // 128 * 128)
     reps = max(1, int(round(seconds / (n / rate))))
     t = time.perf_counter()
     for _ in range(reps):
-        O.xc_build(c, pt_range=(0, n))
+        O.xc_build(c, pt_range=(0, n), nthreads=threads)
     dt = time.perf_counter() - t
     what = "the whole grid" if n == c.npts else f"the first {n} of {c.npts} grid points"
     return {"value": reps * n / dt, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{reps} build(s) over {what} (128-point batches), {threads} OpenMP threads, "
+            "sample": f"{reps} build(s) over {what} (128-point batches), {threads} OpenMP thread(s), "
                       f"OpenBLAS DGEMM; FP64 oracle restating the reference CPU path",
             "seconds": dt}
 
@@ -382,9 +383,14 @@ def run_batch(args):
     import torch
     from pgxc import cases, lib
 
+    from pgxc import tune
     torch.cuda.set_device(0)
     mols = cases.molecule_set()
     npts = sum(m.npts for m in mols)
+    # chunk sizes from the committed tuning table (pgxc/tune.py): the set's
+    # chunk of concatenated tiles, and the FP64 contexts' own chunks
+    table = tune.load()
+    set_chunk = args.max_chunk_points or tune.choose_set(mols, table)
     chunk = args.max_chunk_points or 32768
 
     def operands():
@@ -419,14 +425,16 @@ def run_batch(args):
     del ctx64
     torch.cuda.empty_cache()
 
-    ctxs = [lib.Context(m, precision="mixed", weighted=False, max_chunk_points=chunk, screen_threshold=args.screen)
+    # the contexts' own chunk buffers (used by the one-by-one builds) stay small; the set has its own
+    ctxs = [lib.Context(m, precision="mixed", weighted=False, max_chunk_points=4096, screen_threshold=args.screen)
             for m in mols]
     ops = operands()
     ms_seq = one_by_one(ctxs, ops, max(1, min(args.steps, 2)))
     dC, docc, dham, dsum = ops
     batch = lib.Batch(ctxs, [t.data_ptr() for t in dC], [t.data_ptr() for t in docc], [t.data_ptr() for t in dham],
-                      [t.data_ptr() for t in dsum])
+                      [t.data_ptr() for t in dsum], max_chunk_points=set_chunk)
     gstats = batch.stats()
+    batch_is_set = batch.is_set()
     for _ in range(max(args.warmup, 3)):
         batch.run()
     torch.cuda.synchronize()
@@ -471,8 +479,14 @@ def run_batch(args):
                                f"{max(m.nbas for m in mols)} functions, {npts} grid pts in total, VWN and PBE "
                                f"alternating", "precision": "mixed",
                    "screening": f"per 128-point tile, threshold {args.screen:g}",
-                   "batching": f"one context per molecule (chunks of at most {chunk} points), all device builds "
-                               f"captured as the parallel branches of one CUDA graph, one replay per step",
+                   "batching": f"one context per molecule; the INT8 builds of all molecules run as one set: "
+                               f"per chunk of their concatenated 128-point tiles ("
+                               f"{'at most ' + str(set_chunk) + ' points' if set_chunk else 'sized from free memory'}"
+                               f", from the tuning table) one launch of each kernel walking tiles of many "
+                               f"molecules, captured with the per-molecule P preparation in one CUDA graph, "
+                               f"one replay per step",
+                   "tuning": {"key": tune.set_key(npts), "max_chunk_points": set_chunk,
+                              "table": "paragauss-gpl_b200/pgxc/tune_b200.json" if table else None},
                    "l2": "no flush: each step streams several GB of basis data (inputs larger than L2)"},
         "molecules_per_s": len(mols) / (ms * 1e-3),
         "one_by_one": {"mixed_ms_per_set": ms_seq, "fp64_ms_per_set": ms64,
@@ -488,6 +502,7 @@ def run_batch(args):
         "e2e": {"value": npts / (ms_e * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": ms_e},
         "gpu_launches": gstats["kernel_nodes"] * args.steps, "graph_nodes": gstats["nodes"], "clocks": clocks,
+        "set": batch_is_set,
     }
     print(json.dumps(out), flush=True)
 
@@ -726,6 +741,7 @@ def main():
             out["xc_gradient"] = gradient_leg(torch, sub, local)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(case, weights, args.cpu_seconds)
+        out["cpu_baseline_1thread"] = cpu_baseline(case, weights, min(args.cpu_seconds, 6.0), threads=1)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:

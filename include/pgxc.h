@@ -394,6 +394,24 @@ typedef struct pgxc_symmetry {
 /* Attach (or replace) the symmetry adaptation of a context. */
 int pgxc_set_symmetry(pgxc_ctx* ctx, const pgxc_symmetry* sym);
 
+/*
+ * Pseudo-2D irreps of the attached symmetry adaptation (xc_pseudo2d_sym,
+ * modules/xc_hamiltonian.f90:2637-2779, called by xc_build after the grid
+ * sums): in such an irrep the functions of every (unique atom, l) block come
+ * in two halves A and B (n_exponents x n_independent/2 functions each, A
+ * first), and because the grid is not totally symmetric the built matrix is
+ * made to satisfy H(X_A, Y_A) = H(X_B, Y_B) (their mean) and H(X_A, Y_B) =
+ * -H(X_B, Y_A) (half their difference) for every pair of blocks X >= Y.
+ * pgxc_build_sym applies it to its result (before accumulating into
+ * ham_xc_arr) for the irreps with nblocks[i] > 0.
+ *   nblocks[n_irrep] : blocks of each irrep (0: not pseudo-2D)
+ *   first[sum]       : first function of each block within its irrep
+ *                      (0-based, ascending: orbitalprojection_ob - 1)
+ *   half[sum]        : functions in each block's first half
+ * NULL nblocks removes it.  Needs pgxc_set_symmetry first.
+ */
+int pgxc_set_pseudo2d(pgxc_ctx* ctx, const int32_t* nblocks, const int32_t* first, const int32_t* half);
+
 /* ispin * sum_i dims_i (dims_i + 1) / 2: the ham_xc_arr length of pgxc_build_sym. */
 int pgxc_sym_xc_length(const pgxc_ctx* ctx, int64_t* xc_length);
 
@@ -432,10 +450,25 @@ int pgxc_build_sym(pgxc_ctx* ctx, const double* const* C, const double* const* o
  * context) and d_exc_nel[i] ({E_xc, N_el}) are overwritten by every run.
  * pgxc_batch_run synchronises and returns the graph's device time in *ms
  * (may be NULL).  No counterpart in the reference (one system per process).
+ *
+ * When every context is a screened INT8 closed-shell one (no symmetry
+ * adaptation, no keep_orbitals) the contexts run as one set: per chunk of
+ * their concatenated 128-point tiles (all contexts' grid batches in one work
+ * queue) the graph holds one launch of each kernel, whose persistent blocks
+ * walk tiles of many contexts (each tile's density matrix and V_xc through a
+ * per-tile context table); only the per-context density-matrix preparation
+ * stays one branch per context.  pgxc_batch_create_chunked sets the set's
+ * chunk in points (0: sized from free device memory, the choice of
+ * pgxc_batch_create).
  */
 typedef struct pgxc_batch pgxc_batch;
 int pgxc_batch_create(pgxc_ctx* const* ctx, int32_t n, const double* const* d_C, const double* const* d_occ,
                       const int32_t* nocc, double* const* d_ham, double* const* d_exc_nel, pgxc_batch** out);
+int pgxc_batch_create_chunked(pgxc_ctx* const* ctx, int32_t n, const double* const* d_C,
+                              const double* const* d_occ, const int32_t* nocc, double* const* d_ham,
+                              double* const* d_exc_nel, int64_t max_chunk_points, pgxc_batch** out);
+/* Whether a batch runs as one set (1) or as per-context graph branches (0). */
+int pgxc_batch_is_set(const pgxc_batch* batch, int32_t* is_set);
 int pgxc_batch_run(pgxc_batch* batch, double* ms);
 /* Nodes of the batch's CUDA graph: kernel launches and all nodes. */
 int pgxc_batch_stats(const pgxc_batch* batch, int64_t* kernel_nodes, int64_t* nodes);

@@ -178,3 +178,78 @@ def unpack(ham, nbas, ispin=1, s=0):
     V[kk, jj] = vals
     V[jj, kk] = vals
     return V
+
+
+def pseudo2d_sym(ham, ispin, dims, nblocks, first, half):
+    """xc_pseudo2d_sym (modules/xc_hamiltonian.f90:2637-2779) on a copy of the
+    packed matrix of pgxc_build_sym's layout, with the reference's own 1-based
+    packed positions and loop order.  Block b of irrep i: first function
+    first[b] (0-based within the irrep: orbitalprojection_ob - ob - 1), the
+    half size half[b] = n_exp * n_independent / 2.  Pure Python: small cases."""
+    h = np.array(ham, dtype=np.float64, copy=True)
+    offset = 0  # 0-based start of the irrep's packed block (times ispin)
+    b0 = 0
+    for i, dim in enumerate(dims):
+        nb = int(nblocks[i])
+        blk = [(int(first[b0 + b]) + 1, int(half[b0 + b])) for b in range(nb)]  # 1-based first function
+        for x in range(nb):
+            px, m1 = blk[x]
+            for y in range(x + 1):
+                py, m2 = blk[y]
+                if x == y:
+                    for s in range(ispin):
+                        # diagonal blocks: A x A and B x B (:2686-2704)
+                        c1 = (px * (px - 1)) // 2 + py
+                        c2 = m2 + py + ((px + m1) * (px + m1 - 1)) // 2
+                        stride = px * ispin - ispin
+                        c1 = (c1 - 1) * ispin + s + 1 + offset
+                        c2 = (c2 - 1) * ispin + s + 1 + offset
+                        for im1 in range(1, m1 + 1):
+                            for im2 in range(1, im1 + 1):
+                                h[c1 - 1] = 0.5 * (h[c1 - 1] + h[c2 - 1])
+                                h[c2 - 1] = h[c1 - 1]
+                                c1 += ispin
+                                c2 += ispin
+                            c1 += stride
+                            c2 += stride + m1 * ispin
+                        # off diagonals: B x A (:2706-2721)
+                        for i1 in range(1, m1 + 1):
+                            c4 = ((px + m1 + i1 - 1) * (px + m1 + i1 - 2)) // 2 + py + i1 - 1
+                            c4 = (c4 - 1) * ispin + s + 1 + offset
+                            c3 = c4
+                            st = (px + m1 + i1 - 1) * ispin
+                            for i2 in range(i1, m1 + 1):
+                                h[c4 - 1] = 0.5 * (h[c4 - 1] - h[c3 - 1])
+                                h[c3 - 1] = -h[c4 - 1]
+                                c4 += ispin
+                                c3 += st
+                                st += ispin
+                else:
+                    for s in range(ispin):
+                        stride = (px - m2 + 1) * ispin - ispin
+                        c1 = ((px * (px - 1)) // 2) + py
+                        c2 = m2 + py + ((px + m1) * (px + m1 - 1)) // 2
+                        c3 = ((px * (px - 1)) // 2) + py + m2
+                        c4 = py + ((px + m1) * (px + m1 - 1)) // 2
+                        c1 = (c1 - 1) * ispin + s + 1 + offset
+                        c2 = (c2 - 1) * ispin + s + 1 + offset
+                        c3 = (c3 - 1) * ispin + s + 1 + offset
+                        c4 = (c4 - 1) * ispin + s + 1 + offset
+                        for _ in range(m1):
+                            for _ in range(m2):
+                                h[c1 - 1] = 0.5 * (h[c1 - 1] + h[c2 - 1])
+                                h[c2 - 1] = h[c1 - 1]
+                                h[c3 - 1] = 0.5 * (h[c3 - 1] - h[c4 - 1])
+                                h[c4 - 1] = -h[c3 - 1]
+                                c1 += ispin
+                                c2 += ispin
+                                c3 += ispin
+                                c4 += ispin
+                            c1 += stride
+                            c2 += stride + m1 * ispin
+                            c3 += stride
+                            c4 += stride + m1 * ispin
+                            stride += ispin
+        offset += dim * (dim + 1) // 2 * ispin
+        b0 += nb
+    return h

@@ -6,6 +6,7 @@
 #include <cmath>
 
 #include "basis.cuh"
+#include "dgemm.cuh"
 #include "gradient.h"
 #include "xc_functional.cuh"
 
@@ -499,6 +500,33 @@ __global__ void k_grad_weights(const double* __restrict__ atoms, const double* _
     if (G[i] != 0.0) atomicAdd(grad + i, G[i]);
 }
 
+// X (component 0) or Y_j (components 1..3) = (d_j Phi) P on the FP64 tensor
+// pipe (DMMA): C[f][p] = sum_g A[g][p] P[g][f] for f < nbas, with the 64 x 64
+// tile engine of dgemm.cuh (A: basis component rows of ld points, P: ldc x
+// ldc, zero past nbas).  K runs to nbas rounded up to 16: the rows read past
+// nbas belong to the next basis plane and meet P's zero rows.
+__global__ void __launch_bounds__(kGemmThreads) k_grad_xy(const double* __restrict__ A, int64_t ld,
+                                                         const double* __restrict__ P, int64_t ldc, int64_t nbas,
+                                                         int64_t kend, double* __restrict__ C) {
+  extern __shared__ double smem[];
+  const int64_t m0 = (int64_t)blockIdx.x * 64, n0 = (int64_t)blockIdx.y * 64;
+  Acc acc;
+  acc.zero();
+  gemm_tile<false, false>(acc, A, ld, m0, P, ldc, n0, 0, kend, smem);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wm0 = (warp >> 1) * 32, wn0 = (warp & 1) * 32;
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const int64_t p = m0 + wm0 + i * 8 + (lane >> 2);
+        const int64_t f = n0 + wn0 + j * 8 + 2 * (lane & 3) + e;
+        if (f < nbas) C[f * ld + p] = acc.v[i][j][e];
+      }
+}
+
 template <int L>
 void launch_hess_l(const BuildArgs& a, int64_t p0, int64_t nvalid, int64_t ld, int64_t plane, double* out,
                    cudaStream_t st) {
@@ -532,6 +560,14 @@ void launch_grad_orbital(bool gga, int ispin, int64_t nbas, int64_t ld, int64_t 
   k_grad_fn<<<grid, 256, 0, st>>>(gga, ispin, nbas, ld, nvalid, fatom, basis, plane, XY, coef, grad);
   k_grad_host<<<(unsigned)((ld + 127) / 128), 128, 0, st>>>(gga, ispin, nbas, ld, p0, nvalid, owner, basis, plane,
                                                              XY, coef, grad);
+}
+
+void launch_grad_xy(const double* basis_j, int64_t ld, const double* P, int64_t ldc, int64_t nbas, double* out,
+                    cudaStream_t st) {
+  constexpr int smem = gemm_smem_bytes<false, false>();
+  cudaFuncSetAttribute(k_grad_xy, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  const dim3 grid((unsigned)(ld / 64), (unsigned)((nbas + 63) / 64));
+  k_grad_xy<<<grid, kGemmThreads, smem, st>>>(basis_j, ld, P, ldc, nbas, round_up(nbas, 16), out);
 }
 
 void launch_grad_weights(const double* atoms, const double* dist, int natm, const double* px, const double* py,

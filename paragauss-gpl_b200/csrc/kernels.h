@@ -72,6 +72,8 @@ void launch_basis_points_f64(const BuildArgs& a, const double* px, const double*
 void launch_pmat_f64(const BuildArgs& a, int64_t kpad, cudaStream_t st);
 void launch_density_f64(const BuildArgs& a, bool gga, cudaStream_t st);
 void launch_functional_f64(const BuildArgs& a, int64_t p0, int64_t nvalid, bool gga, cudaStream_t st);
+// the functional on ntiles whole 128-point tiles, one partial pair per tile (no reduction)
+void launch_functional_tiles(const BuildArgs& a, int64_t p0, int64_t ntiles, bool gga, cudaStream_t st);
 // open shell: pa / pb = 8 point columns of ld per spin (rho, grad rho, A, B)
 void launch_functional2_f64(const XcConst& K, const double* w, double* pa, double* pb, int64_t ld, int64_t p0,
                             int64_t nvalid, bool gga, double* partial, double* acc, cudaStream_t st);

@@ -34,8 +34,6 @@ namespace pgxc {
 // mu = d / R is the correctly rounded quotient by Markstein's method
 // (P. W. Markstein, IBM J. Res. Dev. 34 (1990) 111): with y = RN(1/R),
 // q = RN(d y), r = d - R q (exact with one FMA), mu = RN(q + r y).
-// The point-atom distances are kept in shared memory (exact) for up to
-// kBeckeCacheAtoms atoms and recomputed beyond.
 // ---------------------------------------------------------------------------
 // Arithmetic is written with explicit round-to-nearest intrinsics: no FMA
 // contraction where the reference has none, so the factors round as the
@@ -61,7 +59,6 @@ __global__ void k_atom_dist(const double* __restrict__ atoms, int natm, double* 
 namespace {
 
 constexpr int kBeckeThreads = 128;
-constexpr int kBeckeCacheAtoms = 64;       // exact distance cache in shared memory up to this many atoms
 constexpr double kBeckeEdge = 0.9941;      // d <= -kBeckeEdge R_ik => mu <= -0.994 after rounding
 
 // d / R correctly rounded, y = RN(1 / R) (Markstein)
@@ -84,29 +81,27 @@ __device__ __forceinline__ double becke_s(double d, double R, double y) {
   return __dmul_rn(__dsub_rn(1.0, q), 0.5);
 }
 
-template <bool kCache>
-__global__ void __launch_bounds__(kBeckeThreads) k_becke(const double* __restrict__ atoms,
-                                                         const double* __restrict__ dist,
-                                                         const double* __restrict__ rdist, int natm,
-                                                         const double* __restrict__ px, const double* __restrict__ py,
-                                                         const double* __restrict__ pz,
-                                                         const int* __restrict__ owner, int64_t n,
-                                                         double* __restrict__ w) {
-  extern __shared__ double sr[];  // kCache: r[k][thread]
+// Thread per point (geometries of more than kBeckeWarpAtoms atoms).
+__global__ void __launch_bounds__(kBeckeThreads) k_becke_thread(const double* __restrict__ atoms,
+                                                                const double* __restrict__ dist,
+                                                                const double* __restrict__ rdist, int natm,
+                                                                const double* __restrict__ px,
+                                                                const double* __restrict__ py,
+                                                                const double* __restrict__ pz,
+                                                                const int* __restrict__ owner, int64_t n,
+                                                                double* __restrict__ w) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   const double x = px[p], y = py[p], z = pz[p];
   const int a = owner[p];
   auto r_of = [&](int k) {
-    if (kCache) return sr[k * kBeckeThreads + threadIdx.x];
     return dist3(__ldg(atoms + 3 * k), __ldg(atoms + 3 * k + 1), __ldg(atoms + 3 * k + 2), x, y, z);
   };
   // the four atoms nearest to the point (sorted) and their distances
   int nb[4] = {-1, -1, -1, -1};
   double nr[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
   for (int k = 0; k < natm; ++k) {
-    const double r = dist3(__ldg(atoms + 3 * k), __ldg(atoms + 3 * k + 1), __ldg(atoms + 3 * k + 2), x, y, z);
-    if (kCache) sr[k * kBeckeThreads + threadIdx.x] = r;
+    const double r = r_of(k);
     if (r < nr[3]) {
       int j = 3;
       for (; j > 0 && nr[j - 1] > r; --j) {
@@ -163,6 +158,164 @@ __global__ void __launch_bounds__(kBeckeThreads) k_becke(const double* __restric
   w[p] = __ddiv_rn(pa, sum);
 }
 
+// The same weights with the surviving (point, atom) products spread over the
+// lanes of a warp (for up to kBeckeWarpAtoms atoms).  Thread per point, each
+// lane first finds its point's nearest atoms, the nearest atom's P, tau and a
+// bitmask of the atoms whose bound Q_i reaches tau; the warp then computes the
+// ordered products of all its points' surviving atoms 32 at a time (lane l
+// takes the l-th pending pair, whatever point it belongs to), and each
+// product is handed back to its point's lane in ascending atom order, so
+// every point's sum is formed in the reference's order.  Thread-per-point
+// loops over the atoms diverge wherever the lanes' points keep different
+// atoms; here every lane of a round has a product to form.
+constexpr int kBeckeWarpAtoms = 256;
+constexpr int kMaskWords = kBeckeWarpAtoms / 32;
+
+__global__ void __launch_bounds__(kBeckeThreads) k_becke_warp(const double* __restrict__ atoms,
+                                                              const double* __restrict__ dist,
+                                                              const double* __restrict__ rdist, int natm,
+                                                              const double* __restrict__ px,
+                                                              const double* __restrict__ py,
+                                                              const double* __restrict__ pz,
+                                                              const int* __restrict__ owner, int64_t n,
+                                                              double* __restrict__ w) {
+  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const bool live = p < n;  // every lane takes part in the warp's rounds
+  double x = 0.0, y = 0.0, z = 0.0;
+  int a = -1;
+  if (live) {
+    x = px[p];
+    y = py[p];
+    z = pz[p];
+    a = owner[p];
+  }
+  // P_i of the point at (qx, qy, qz): the ordered product, exactly-1 factors
+  // skipped, 0 once below tau
+  auto ordered = [&](int i, double qx, double qy, double qz, double tau) {
+    const double ri = dist3(__ldg(atoms + 3 * i), __ldg(atoms + 3 * i + 1), __ldg(atoms + 3 * i + 2), qx, qy, qz);
+    const double* Ri = dist + (int64_t)i * natm;
+    const double* Yi = rdist + (int64_t)i * natm;
+    double P = 1.0;
+    for (int k = 0; k < natm; ++k) {
+      if (k == i) continue;
+      const double R = __ldg(Ri + k);
+      const double d = __dsub_rn(ri, dist3(__ldg(atoms + 3 * k), __ldg(atoms + 3 * k + 1), __ldg(atoms + 3 * k + 2),
+                                           qx, qy, qz));
+      if (d <= -__dmul_rn(kBeckeEdge, R)) continue;
+      P = __dmul_rn(P, becke_s(d, R, __ldg(Yi + k)));
+      if (P < tau) return 0.0;
+    }
+    return P;
+  };
+  int nb[4] = {-1, -1, -1, -1};
+  double nr[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
+  unsigned mask[kMaskWords] = {};
+  int cnt = 0;
+  double P0 = 0.0, tau = 0.0;
+  int i0 = -1;
+  if (live) {
+    for (int k = 0; k < natm; ++k) {
+      const double r = dist3(__ldg(atoms + 3 * k), __ldg(atoms + 3 * k + 1), __ldg(atoms + 3 * k + 2), x, y, z);
+      if (r < nr[3]) {
+        int j = 3;
+        for (; j > 0 && nr[j - 1] > r; --j) {
+          nr[j] = nr[j - 1];
+          nb[j] = nb[j - 1];
+        }
+        nr[j] = r;
+        nb[j] = k;
+      }
+    }
+    i0 = nb[0];
+    P0 = ordered(i0, x, y, z, 0.0);
+    tau = fmax(0x1p-56 * P0 / natm, 0x1p-1000);
+    for (int i = 0; i < natm; ++i) {
+      if (i == i0) continue;
+      const double ri = dist3(__ldg(atoms + 3 * i), __ldg(atoms + 3 * i + 1), __ldg(atoms + 3 * i + 2), x, y, z);
+      const double* Ri = dist + (int64_t)i * natm;
+      const double* Yi = rdist + (int64_t)i * natm;
+      double Q = 1.0;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int k = nb[c];
+        if (k < 0 || k == i) continue;
+        const double R = __ldg(Ri + k);
+        const double d = __dsub_rn(ri, nr[c]);
+        if (d > -__dmul_rn(kBeckeEdge, R)) Q *= becke_s(d, R, __ldg(Yi + k));
+      }
+      if (Q >= tau) {
+        mask[i >> 5] |= 1u << (i & 31);
+        ++cnt;
+      }
+    }
+  }
+  // the warp's pending pairs: lane l's are positions off .. off + cnt - 1, ascending atom
+  int off = cnt;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, off, d);
+    if (lane >= d) off += v;
+  }
+  const int total = __shfl_sync(0xffffffffu, off, 31);
+  off -= cnt;
+  double sum = 0.0, pa = 0.0;
+  bool p0_added = false;
+  auto add = [&](int i, double P) {  // this lane's point: the next product in ascending atom order
+    if (!p0_added && i > i0) {
+      if (P0 != 0.0) sum = __dadd_rn(sum, P0);
+      if (a == i0) pa = P0;
+      p0_added = true;
+    }
+    if (P != 0.0) sum = __dadd_rn(sum, P);
+    if (i == a) pa = P;
+  };
+  for (int base = 0; base < total; base += 32) {
+    const int q = base + lane;
+    // owner lane of position q: the largest l with off_l <= q
+    int ol = 0;
+#pragma unroll
+    for (int st = 16; st > 0; st >>= 1) {
+      const int cand = ol + st;
+      const int oc = __shfl_sync(0xffffffffu, off, cand & 31);
+      if (cand < 32 && oc <= q) ol = cand;
+    }
+    const int j = q - __shfl_sync(0xffffffffu, off, ol);  // rank of the pair among the owner's
+    unsigned m[kMaskWords];
+#pragma unroll
+    for (int u = 0; u < kMaskWords; ++u) m[u] = __shfl_sync(0xffffffffu, mask[u], ol);
+    const double qx = __shfl_sync(0xffffffffu, x, ol), qy = __shfl_sync(0xffffffffu, y, ol),
+                 qz = __shfl_sync(0xffffffffu, z, ol), qt = __shfl_sync(0xffffffffu, tau, ol);
+    int pi = -1;
+    double P = 0.0;
+    if (q < total) {
+      int r = j;
+      for (int u = 0; u < kMaskWords; ++u) {
+        const int c = __popc(m[u]);
+        if (r < c) {
+          pi = 32 * u + (int)__fns(m[u], 0, r + 1);
+          break;
+        }
+        r -= c;
+      }
+      P = ordered(pi, qx, qy, qz, qt);
+    }
+    // hand the round's products to their points' lanes, in position order
+    for (int t = 0; t < 32; ++t) {
+      const int tl = __shfl_sync(0xffffffffu, ol, t), ti = __shfl_sync(0xffffffffu, pi, t);
+      const double tp = __shfl_sync(0xffffffffu, P, t);
+      if (base + t < total && tl == lane) add(ti, tp);
+    }
+  }
+  if (live) {
+    if (!p0_added) {
+      if (P0 != 0.0) sum = __dadd_rn(sum, P0);
+      if (a == i0) pa = P0;
+    }
+    w[p] = __ddiv_rn(pa, sum);
+  }
+}
+
 }  // namespace
 
 cudaError_t launch_becke(const double* atoms, double* dist, int natm, const double* px, const double* py,
@@ -173,14 +326,10 @@ cudaError_t launch_becke(const double* atoms, double* dist, int natm, const doub
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess || n == 0) return e;
   const unsigned nb = (unsigned)((n + kBeckeThreads - 1) / kBeckeThreads);
-  if (natm <= kBeckeCacheAtoms) {
-    const int smem = natm * kBeckeThreads * (int)sizeof(double);
-    e = cudaFuncSetAttribute(k_becke<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    if (e != cudaSuccess) return e;
-    k_becke<true><<<nb, kBeckeThreads, smem, st>>>(atoms, dist, rdist, natm, px, py, pz, owner, n, w);
-  } else {
-    k_becke<false><<<nb, kBeckeThreads, 0, st>>>(atoms, dist, rdist, natm, px, py, pz, owner, n, w);
-  }
+  if (natm <= kBeckeWarpAtoms)
+    k_becke_warp<<<nb, kBeckeThreads, 0, st>>>(atoms, dist, rdist, natm, px, py, pz, owner, n, w);
+  else
+    k_becke_thread<<<nb, kBeckeThreads, 0, st>>>(atoms, dist, rdist, natm, px, py, pz, owner, n, w);
   return cudaGetLastError();
 }
 

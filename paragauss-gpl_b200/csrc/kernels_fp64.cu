@@ -222,12 +222,12 @@ __global__ void __launch_bounds__(256) k_functional(XcConst K, int64_t p0, int64
     }
     q = r * wt;
   }
-  // fixed-order block reduction (deterministic)
+  // fixed-order block reduction (deterministic; blockDim a power of two <= 256)
   __shared__ double se[256], sq[256];
   se[threadIdx.x] = e;
   sq[threadIdx.x] = q;
   __syncthreads();
-  for (int s = 128; s > 0; s >>= 1) {
+  for (int s = blockDim.x >> 1; s > 0; s >>= 1) {
     if (threadIdx.x < s) {
       se[threadIdx.x] += se[threadIdx.x + s];
       sq[threadIdx.x] += sq[threadIdx.x + s];
@@ -345,6 +345,18 @@ void launch_functional_f64(const BuildArgs& a, int64_t p0, int64_t nvalid, bool 
     k_functional<false><<<nb, 256, 0, st>>>(a.xc, p0, nvalid, a.ldp, a.w, a.rho, nullptr, nullptr, nullptr, a.A, nullptr,
                                             nullptr, nullptr, a.partial);
   k_sum_partials<<<1, 256, 0, st>>>(a.partial, (int)nb, a.acc);
+}
+
+// One block per 128-point tile of a set's chunk: partial[2 t], partial[2 t + 1]
+// = the tile's sums of w f and w rho (reduced per context by the caller).
+void launch_functional_tiles(const BuildArgs& a, int64_t p0, int64_t ntiles, bool gga, cudaStream_t st) {
+  const int64_t n = ntiles * 128;
+  if (gga)
+    k_functional<true><<<(unsigned)ntiles, 128, 0, st>>>(a.xc, p0, n, n, a.w, a.rho, a.grx, a.gry, a.grz, a.A, a.Bx,
+                                                         a.By, a.Bz, a.partial);
+  else
+    k_functional<false><<<(unsigned)ntiles, 128, 0, st>>>(a.xc, p0, n, n, a.w, a.rho, nullptr, nullptr, nullptr, a.A,
+                                                          nullptr, nullptr, nullptr, a.partial);
 }
 
 // ---------------------------------------------------------------------------

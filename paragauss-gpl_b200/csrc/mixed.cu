@@ -159,10 +159,11 @@ __global__ void __launch_bounds__(128) k_oz_quant_pts(const double* __restrict__
 
 // rows = functions (blocks of ROWS), K = points: element (f, p) = a[f][p], per-function scale
 template <int ROWS>
-__global__ void __launch_bounds__(ROWS) k_oz_quant_fn(const double* __restrict__ a, int64_t ldp,
-                                                      const int* __restrict__ e_fn, int nks,
-                                                      int8_t* __restrict__ out) {
+__global__ void __launch_bounds__(kBlock4(ROWS)) k_oz_quant_fn(const double* __restrict__ a, int64_t ldp,
+                                                               const int* __restrict__ e_fn, int nks,
+                                                               int8_t* __restrict__ out) {
   const int fb = blockIdx.x, kb = blockIdx.y, t = threadIdx.x;
+  if (t >= ROWS) return;
   const int64_t f = (int64_t)fb * ROWS + t;
   const int e = e_fn[f];
   const double2* src = reinterpret_cast<const double2*>(a + f * ldp + (int64_t)kb * 32);
@@ -187,10 +188,11 @@ __global__ void __launch_bounds__(ROWS) k_oz_quant_fn(const double* __restrict__
 }
 
 // density B: rows = nu (blocks of 96), K = mu, element P[mu][nu] = P[nu][mu], per-row scale
-__global__ void __launch_bounds__(kRowsB) k_oz_quant_P(const double* __restrict__ P, int64_t ldk,
-                                                       const int* __restrict__ e_P, int nks,
-                                                       int8_t* __restrict__ out) {
+__global__ void __launch_bounds__(kBlock4(kRowsB)) k_oz_quant_P(const double* __restrict__ P, int64_t ldk,
+                                                                const int* __restrict__ e_P, int nks,
+                                                                int8_t* __restrict__ out) {
   const int nb = blockIdx.x, kb = blockIdx.y, t = threadIdx.x;
+  if (t >= kRowsB) return;
   const int64_t nu = (int64_t)nb * kRowsB + t;
   const int e = e_P[nu];
   int8_t* dst = out + ((int64_t)nb * nks + kb) * kOpB;
@@ -647,7 +649,7 @@ int mixed_prepare(MixedState* m, const BuildArgs& a, int nocc, cudaStream_t st) 
   k_oz_pmat<<<g2, b2, 0, st>>>(a.C, a.occ, a.ldc, kpad, m->nbas, m->ldk, m->P);
   k_oz_rowexp_P<<<(unsigned)m->ldk, 256, 0, st>>>(m->P, m->ldk, m->e_P);
   const int nks = (int)(m->ldk / kKStep);
-  k_oz_quant_P<<<dim3((unsigned)(m->ldk / kRowsB), (unsigned)nks), kRowsB, 0, st>>>(m->P, m->ldk, m->e_P, nks,
+  k_oz_quant_P<<<dim3((unsigned)(m->ldk / kRowsB), (unsigned)nks), kBlock4(kRowsB), 0, st>>>(m->P, m->ldk, m->e_P, nks,
                                                                                   m->tB1);
   cudaMemsetAsync(m->vpart, 0, sizeof(double) * m->nsplit * m->ntiles * kRowsA * kRowsB, st);
   return 3;
@@ -666,7 +668,7 @@ int mixed_prepare_P(MixedState* m, const double* P, int64_t ldc, cudaStream_t st
   k_oz_copy_P<<<g2, b2, 0, st>>>(P, ldc, m->nbas, m->ldk, m->P);
   k_oz_rowexp_P<<<(unsigned)m->ldk, 256, 0, st>>>(m->P, m->ldk, m->e_P);
   const int nks = (int)(m->ldk / kKStep);
-  k_oz_quant_P<<<dim3((unsigned)(m->ldk / kRowsB), (unsigned)nks), kRowsB, 0, st>>>(m->P, m->ldk, m->e_P, nks,
+  k_oz_quant_P<<<dim3((unsigned)(m->ldk / kRowsB), (unsigned)nks), kBlock4(kRowsB), 0, st>>>(m->P, m->ldk, m->e_P, nks,
                                                                                   m->tB1);
   cudaMemsetAsync(m->vpart, 0, sizeof(double) * m->nsplit * m->ntiles * kRowsA * kRowsB, st);
   return 3;
@@ -707,8 +709,8 @@ int mixed_potential(MixedState* m, const BuildArgs& a, bool gga, cudaStream_t st
   k_oz_fexp<<<ne, 256, 0, st>>>(m->zmax, m->ldk, m->e_Z);
   k_oz_fexp<<<ne, 256, 0, st>>>(m->fmax, m->ldk, m->e_fn);
   const int nks = (int)(m->ldp / kKStep);
-  k_oz_quant_fn<kRowsA><<<dim3((unsigned)m->nta, (unsigned)nks), kRowsA, 0, st>>>(m->Z, m->ldp, m->e_Z, nks, m->tZ);
-  k_oz_quant_fn<kRowsB><<<dim3((unsigned)m->ntb, (unsigned)nks), kRowsB, 0, st>>>(m->phi, m->ldp, m->e_fn, nks,
+  k_oz_quant_fn<kRowsA><<<dim3((unsigned)m->nta, (unsigned)nks), kBlock4(kRowsA), 0, st>>>(m->Z, m->ldp, m->e_Z, nks, m->tZ);
+  k_oz_quant_fn<kRowsB><<<dim3((unsigned)m->ntb, (unsigned)nks), kBlock4(kRowsB), 0, st>>>(m->phi, m->ldp, m->e_fn, nks,
                                                                                  m->tP2);
   cudaEventRecord(k0, st);
   const int smem = tc::kWholeSmSmem;  // >= sizeof(OzSmem) + 1024 (base alignment)

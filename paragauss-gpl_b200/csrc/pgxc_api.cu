@@ -12,7 +12,6 @@
 #include <string>
 #include <vector>
 
-#include <cublas_v2.h>
 #include <cuda_runtime.h>
 
 #include "gradient.h"
@@ -39,6 +38,10 @@ struct SymPlan {
   int64_t* d_cofs = nullptr;       // [ispin * n_irrep]
   int* d_nocc = nullptr;           // [n_irrep]
   int64_t* d_col0 = nullptr;       // [nip]
+  // pseudo-2D irreps (pgxc_set_pseudo2d)
+  Pseudo2dPair* d_p2 = nullptr;
+  int64_t* d_p2first = nullptr;
+  int64_t p2_pairs = 0, p2_quads = 0;
 };
 
 struct pgxc_ctx {
@@ -73,7 +76,6 @@ struct pgxc_ctx {
   int eacc_cap = 0;
   int* d_owner = nullptr;       // host atom of each point (raw-weight grids)
   double* d_wraw = nullptr;     // the raw weights of those grids
-  cublasHandle_t cublas = nullptr;
 };
 
 namespace {
@@ -178,7 +180,6 @@ void pgxc_destroy(pgxc_ctx* c) {
   if (c->mixed) mixed_destroy(c->mixed);
   if (c->screen) screen_destroy(c->screen);
   delete c->sym;
-  if (c->cublas) cublasDestroy(c->cublas);
   for (void* p : c->allocs) cudaFree(p);
   if (c->h_ham) cudaFreeHost(c->h_ham);
   if (c->h_acc) cudaFreeHost(c->h_acc);
@@ -912,10 +913,6 @@ int pgxc_xc_gradient(pgxc_ctx* c, const double* C, const double* occ, int32_t nb
   if ((st = ensure_occ(c, nocc))) return st;
   BuildArgs& a = c->a;
   cudaStream_t s = c->stream;
-  if (!c->cublas) {
-    if (cublasCreate(&c->cublas) != CUBLAS_STATUS_SUCCESS) return set_err(c, PGXC_ECUDA, "cublasCreate failed");
-  }
-  if (cublasSetStream(c->cublas, s) != CUBLAS_STATUS_SUCCESS) return set_err(c, PGXC_ECUDA, "cublasSetStream failed");
   const int64_t kpad = round_up(std::max(nocc, 1), 16);
   if ((st = upload_orbitals(c, C, occ, nbas, nocc, kpad, cudaMemcpyHostToDevice))) return st;
   launch_pmat_f64(a, kpad, s);
@@ -963,7 +960,6 @@ int pgxc_xc_gradient(pgxc_ctx* c, const double* C, const double* occ, int32_t nb
       rc = set_err(c, PGXC_ECUDA, "gradient set-up copies failed");
       break;
     }
-    const double one = 1.0, zero = 0.0;
     for (int64_t p0 = 0; p0 < c->npts && rc == PGXC_OK; p0 += ld) {
       const int64_t nv = std::min<int64_t>(ld, c->npts - p0);
       launch_basis_hess(a, p0, nv, ld, plane, basis, s);
@@ -971,11 +967,7 @@ int pgxc_xc_gradient(pgxc_ctx* c, const double* C, const double* occ, int32_t nb
         const double* P = sp ? c->P2 : a.P;
         for (int j = 0; j < (gga ? 4 : 1); ++j) {
           // X (j = 0) or Y_j = (d_j Phi) P: (ld x nbas) = (ld x nbas)(nbas x nbas), P symmetric
-          if (cublasDgemm(c->cublas, CUBLAS_OP_N, CUBLAS_OP_N, (int)ld, (int)nbas, (int)nbas, &one, basis + j * plane,
-                          (int)ld, P, (int)a.ldc, &zero, XY + (4 * sp + j) * plane, (int)ld) != CUBLAS_STATUS_SUCCESS) {
-            rc = set_err(c, PGXC_ECUDA, "cublasDgemm failed");
-            break;
-          }
+          launch_grad_xy(basis + j * plane, ld, P, a.ldc, nbas, XY + (4 * sp + j) * plane, s);
         }
       }
       if (rc) break;
@@ -1202,6 +1194,56 @@ int pgxc_sym_xc_length(const pgxc_ctx* c, int64_t* xc_length) {
   return PGXC_OK;
 }
 
+int pgxc_set_pseudo2d(pgxc_ctx* c, const int32_t* nblocks, const int32_t* first, const int32_t* half) {
+  if (!c) return set_err(nullptr, PGXC_EINVAL, "ctx is NULL");
+  SymPlan* P = c->sym;
+  if (!P) return set_err(c, PGXC_EINVAL, "pgxc_set_pseudo2d needs pgxc_set_symmetry first");
+  P->p2_pairs = P->p2_quads = 0;
+  if (!nblocks) return PGXC_OK;
+  const int n = P->dev.n_irrep;
+  std::vector<Pseudo2dPair> pairs;
+  std::vector<int64_t> qfirst(1, 0);
+  int64_t b0 = 0;
+  for (int i = 0; i < n; ++i) {
+    const int nb = nblocks[i];
+    if (nb < 0) return set_err(c, PGXC_EINVAL, "pseudo2d: negative block count");
+    if (nb > 0 && (!first || !half)) return set_err(c, PGXC_EINVAL, "pseudo2d: first and half are required");
+    for (int b = 0; b < nb; ++b) {
+      const int64_t f = first[b0 + b], h = half[b0 + b];
+      const int64_t next = b + 1 < nb ? first[b0 + b + 1] : P->dims[(size_t)i];
+      if (f < 0 || h < 0 || f + 2 * h > next || (b + 1 < nb && next < f))
+        return set_err(c, PGXC_EINVAL, "pseudo2d: blocks must be ascending, disjoint and inside the irrep");
+    }
+    // block pairs X >= Y in block order (the reference's unique-atom / l loops)
+    for (int bx = 0; bx < nb; ++bx)
+      for (int by = 0; by <= bx; ++by) {
+        Pseudo2dPair q;
+        q.pk = P->pkofs[(size_t)i];
+        q.px = first[b0 + bx];
+        q.hx = half[b0 + bx];
+        q.py = first[b0 + by];
+        q.hy = half[b0 + by];
+        q.same = bx == by;
+        const int64_t nq = q.same ? q.hx * (q.hx + 1) / 2 : q.hx * q.hy;
+        if (nq == 0) continue;
+        pairs.push_back(q);
+        qfirst.push_back(qfirst.back() + nq);
+      }
+    b0 += nb;
+  }
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  int st;
+  if ((st = dalloc(c, &P->d_p2, std::max<size_t>(pairs.size(), 1))) ||
+      (st = dalloc(c, &P->d_p2first, qfirst.size())))
+    return st;
+  if (!pairs.empty())
+    CUDA_TRY(c, cudaMemcpy(P->d_p2, pairs.data(), sizeof(Pseudo2dPair) * pairs.size(), cudaMemcpyHostToDevice));
+  CUDA_TRY(c, cudaMemcpy(P->d_p2first, qfirst.data(), sizeof(int64_t) * qfirst.size(), cudaMemcpyHostToDevice));
+  P->p2_pairs = (int64_t)pairs.size();
+  P->p2_quads = qfirst.back();
+  return PGXC_OK;
+}
+
 int pgxc_build_sym(pgxc_ctx* c, const double* const* C, const double* const* occ, const int32_t* nocc, int32_t ispin,
                    double* ham, int64_t xc_length, double* exc, double* nel, pgxc_timings* tm) {
   if (!c) return set_err(nullptr, PGXC_EINVAL, "ctx is NULL");
@@ -1279,6 +1321,7 @@ int pgxc_build_sym(pgxc_ctx* c, const double* const* C, const double* const* occ
   cudaEvent_t e0 = c->ev[5], e1 = c->ev[6];
   CUDA_TRY(c, cudaEventRecord(e0, s));
   launch_sym_potential(P->dev, P->max_dim, ispin, c->d_ham, P->d_ham, s);
+  launch_pseudo2d(P->d_p2, P->d_p2first, P->p2_pairs, P->p2_quads, ispin, P->d_ham, s);
   CUDA_TRY(c, cudaGetLastError());
   std::vector<double> hH((size_t)xc_length);
   if (xc_length > 0)
@@ -1339,8 +1382,25 @@ static int enqueue_screened_build(pgxc_ctx* c, const double* d_C, const double* 
   return PGXC_OK;
 }
 
+// A set member's share of a batch step (capturable): its orbitals uploaded,
+// P formed and turned into digits, its accumulators zeroed.  The set's
+// launches then build every member at once.
+static int enqueue_set_member(pgxc_ctx* c, const double* d_C, const double* d_occ, int32_t nocc) {
+  BuildArgs& a = c->a;
+  cudaStream_t s = c->stream;
+  const int64_t kpad = round_up(std::max(nocc, 1), 16);
+  int st = upload_orbitals(c, d_C, d_occ, (int32_t)c->nbas, nocc, kpad, cudaMemcpyDeviceToDevice);
+  if (st) return st;
+  CUDA_TRY(c, cudaMemsetAsync(a.acc, 0, 4 * sizeof(double), s));
+  launch_pmat_f64(a, kpad, s);
+  CUDA_TRY(c, cudaGetLastError());
+  if (screen_set_prepare_member(c->screen, a.P, a.ldc, s)) return set_err(c, PGXC_ECUDA, "set member preparation");
+  return PGXC_OK;
+}
+
 struct pgxc_batch {
   std::vector<pgxc_ctx*> ctx;
+  ScreenSet* set = nullptr;  // the contexts' builds as one sequence of launches over all their tiles
   int device = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
@@ -1353,6 +1413,7 @@ void pgxc_batch_destroy(pgxc_batch* b) {
   if (!b) return;
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->set) screen_set_destroy(b->set);
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   for (cudaEvent_t e : b->join)
@@ -1365,6 +1426,18 @@ void pgxc_batch_destroy(pgxc_batch* b) {
 
 int pgxc_batch_create(pgxc_ctx* const* ctx, int32_t n, const double* const* d_C, const double* const* d_occ,
                       const int32_t* nocc, double* const* d_ham, double* const* d_exc_nel, pgxc_batch** out) {
+  return pgxc_batch_create_chunked(ctx, n, d_C, d_occ, nocc, d_ham, d_exc_nel, 0, out);
+}
+
+int pgxc_batch_is_set(const pgxc_batch* b, int32_t* is_set) {
+  if (!b || !is_set) return set_err(nullptr, PGXC_EINVAL, "NULL argument");
+  *is_set = b->set != nullptr;
+  return PGXC_OK;
+}
+
+int pgxc_batch_create_chunked(pgxc_ctx* const* ctx, int32_t n, const double* const* d_C,
+                              const double* const* d_occ, const int32_t* nocc, double* const* d_ham,
+                              double* const* d_exc_nel, int64_t max_chunk_points, pgxc_batch** out) {
   if (!out) return set_err(nullptr, PGXC_EINVAL, "out is NULL");
   *out = nullptr;
   if (!ctx || n <= 0 || !d_C || !d_occ || !nocc || !d_ham || !d_exc_nel)
@@ -1400,6 +1473,20 @@ int pgxc_batch_create(pgxc_ctx* const* ctx, int32_t n, const double* const* d_C,
   if (ce == cudaSuccess) ce = cudaEventCreate(&b->t1);
   for (int32_t i = 0; i < n && ce == cudaSuccess; ++i) ce = cudaEventCreateWithFlags(&b->join[(size_t)i], cudaEventDisableTiming);
   if (ce != cudaSuccess) return fail(PGXC_ECUDA, std::string("batch: ") + cudaGetErrorString(ce));
+  // Contexts that all use the screened INT8 closed-shell layout run as one
+  // set: per chunk of their concatenated tiles one launch per kernel.
+  bool as_set = true;
+  for (int32_t i = 0; i < n && as_set; ++i)
+    as_set = ctx[i]->opt.precision == PGXC_PREC_MIXED_INT8 && !ctx[i]->sym && ctx[i]->a.sa.identity &&
+             screen_set_eligible(ctx[i]->screen);
+  if (as_set) {
+    std::vector<SetMember> mem;
+    for (int32_t i = 0; i < n; ++i)
+      mem.push_back({ctx[i]->screen, &ctx[i]->a, ctx[i]->opt.functional, d_ham[i], d_exc_nel[i]});
+    std::string e;
+    if (int st = screen_set_create(&b->set, mem, std::max<int64_t>(max_chunk_points, 0), b->stream, e))
+      return fail(st, "batch: " + e);
+  }
   // fork from the batch stream into every context's stream, join back
   ce = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed);
   if (ce != cudaSuccess) return fail(PGXC_ECUDA, std::string("batch: begin capture: ") + cudaGetErrorString(ce));
@@ -1410,12 +1497,17 @@ int pgxc_batch_create(pgxc_ctx* const* ctx, int32_t n, const double* const* d_C,
     pgxc_ctx* c = ctx[i];
     ce = cudaStreamWaitEvent(c->stream, b->fork, 0);
     if (ce != cudaSuccess) break;
-    if ((st = enqueue_screened_build(c, d_C[i], d_occ[i], nocc[i], d_ham[i], d_exc_nel[i]))) {
+    if ((st = b->set ? enqueue_set_member(c, d_C[i], d_occ[i], nocc[i])
+                     : enqueue_screened_build(c, d_C[i], d_occ[i], nocc[i], d_ham[i], d_exc_nel[i]))) {
       msg = "batch: context " + std::to_string(i) + ": " + c->err;
       break;
     }
     ce = cudaEventRecord(b->join[(size_t)i], c->stream);
     if (ce == cudaSuccess) ce = cudaStreamWaitEvent(b->stream, b->join[(size_t)i], 0);
+  }
+  if (b->set && st == PGXC_OK && ce == cudaSuccess) {
+    std::string e;
+    if ((st = screen_set_run(b->set, b->stream, e))) msg = "batch: " + e;
   }
   cudaGraph_t g = nullptr;
   const cudaError_t ce_end = cudaStreamEndCapture(b->stream, &g);  // always ends the capture
@@ -1443,6 +1535,12 @@ int pgxc_batch_run(pgxc_batch* b, double* ms) {
     float f = 0;
     CUDA_TRY(nullptr, cudaEventElapsedTime(&f, b->t0, b->t1));
     *ms = f;
+  }
+  if (b->set) {
+    int flag = 0;
+    if (screen_set_error_flag(b->set, b->stream, &flag) != PGXC_OK)
+      return set_err(nullptr, PGXC_ECUDA, "batch: error-flag read failed");
+    if (flag) return set_err(nullptr, PGXC_ETIMEOUT, "batch: a bounded tensor-core pipeline wait ran out");
   }
   for (size_t i = 0; i < b->ctx.size(); ++i) {
     int flag = 0;

@@ -43,6 +43,13 @@ constexpr int kTile = 64;
 
 inline int64_t round_up(int64_t x, int64_t m) { return (x + m - 1) / m * m; }
 
+// Thread count of a block rounded up to whole groups of four warps.  Every
+// kernel of the library launches such blocks: a tensor-core CTA placed on an
+// SM beside other CTAs then starts on a warp slot that is a multiple of four,
+// so that its warp w sits in sub-partition w % 4, whose TMEM lanes
+// 32 (w % 4) .. 32 (w % 4) + 31 its tcgen05.ld addresses.
+__host__ __device__ constexpr int kBlock4(int threads) { return (threads + 127) / 128 * 128; }
+
 // Raise, never lower, a kernel's dynamic shared-memory limit.  The limit
 // belongs to the function, shared by every context of the process: a
 // context whose tiles list fewer functions must not undercut the launches of

@@ -32,46 +32,9 @@
 #include "kernels.h"
 #include "screened.h"
 #include "screened_mixed.h"
+#include "screened_plan.h"
 
 namespace pgxc {
-
-constexpr int kSlotAlign = 32;   // slots per tile are padded to this (INT8 K step)
-constexpr int64_t kSlack = 128;  // zero rows after the last slot of a chunk
-constexpr int kBasisBlocksPerSM = 16;  // blocks of the basis kernels per SM (each walks a range of items)
-
-struct ScreenPlan {
-  int64_t ntiles = 0, nslots = 0, nlisted = 0;
-  double sum_n2 = 0.0;
-  int max_n = 0;
-  bool gga = false;
-  int ispin = 1;
-  int64_t nbas = 0;
-  bool keep = false;         // basis values (and INT8 point digits) of all slots stay resident
-  bool basis_ready = false;  // ... and a completed build has filled them
-  // device, whole grid
-  double *qx = nullptr, *qy = nullptr, *qz = nullptr, *qw = nullptr;  // Morton-ordered points [ntiles*128]
-  int64_t* tso = nullptr;   // [ntiles+1] first slot of each tile
-  int* slot_fn = nullptr;   // [nslots] function of each slot, -1 for padding
-  int* slot_tile = nullptr; // [nslots]
-  int* listed = nullptr;    // [ntiles] listed (not padding) slots of each tile
-  int64_t* b_off = nullptr;  // [ntiles+1] first density B stage of each tile (INT8 path)
-  BasisItem* items[kMaxL + 1] = {};
-  // host copies of the partition
-  std::vector<int64_t> h_tso;
-  std::vector<int64_t> chunk_t0;                   // chunk c covers tiles [chunk_t0[c], chunk_t0[c+1])
-  std::vector<int64_t> item_off[kMaxL + 1];        // items of chunk c: [item_off[L][c], item_off[L][c+1])
-  int64_t chunk_slots = 0, chunk_tiles = 0;        // buffer capacities
-  // device, per chunk
-  double *phi = nullptr, *gx = nullptr, *gy = nullptr, *gz = nullptr, *Z = nullptr;
-  double* pt = nullptr;      // 8 point arrays of chunk_tiles*128 per spin
-  double* partial = nullptr;
-  double* V = nullptr;       // [ispin][nbas][nbas]
-  unsigned long long* pmax = nullptr;  // [chunk_tiles*128] largest |phi| per point (INT8 path)
-  ScreenMixed* mixed = nullptr;
-  cudaEvent_t ev[12] = {};
-  int nsm = 148;
-  std::vector<void*> allocs;
-};
 
 namespace {
 
@@ -474,6 +437,11 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
   sp->nbas = in.nbas;
   sp->keep = in.keep_basis;
   const std::vector<DevShell>& shells = *in.shells;
+  for (const DevShell& S : shells) {
+    sp->n_exps = std::max<int64_t>(sp->n_exps, S.exp_off + S.nexp);
+    sp->n_contr = std::max<int64_t>(sp->n_contr, S.con_off + (int64_t)S.nexp * S.ncontr);
+    if (S.seg) sp->n_rng = std::max<int64_t>(sp->n_rng, S.rad_off + S.ncontr);
+  }
   for (const DevShell& S : shells)
     if (S.nrad > 64) {
       err = "screened build: a shell has more than 64 radial functions";
@@ -588,7 +556,10 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
     slot_tile.resize(slot_fn.size(), (int)t);
     tso[(size_t)t + 1] = (int64_t)slot_fn.size();
   }
-  for (int l = 0; l <= kMaxL; ++l) tile_items[l][(size_t)ntiles] = (int64_t)items[l].size();
+  for (int l = 0; l <= kMaxL; ++l) {
+    tile_items[l][(size_t)ntiles] = (int64_t)items[l].size();
+    sp->tile_item[l] = tile_items[l];
+  }
   sp->nslots = (int64_t)slot_fn.size();
   sp->h_tso = tso;
   // --- chunks -------------------------------------------------------------------
@@ -935,5 +906,453 @@ int screen_error_flag(ScreenPlan* sp, cudaStream_t st, int* flag) {
   if (!sp->mixed) return PGXC_OK;
   return screen_mixed_error_flag(sp->mixed, st, flag);
 }
+
+
+// ---------------------------------------------------------------------------
+// Sets of contexts (screened.h): one launch per kernel over many contexts'
+// tiles.
+// ---------------------------------------------------------------------------
+namespace {
+
+// per context: where its E_xc / N_el accumulators, V and outputs live
+struct SetOutDev {
+  double* acc;        // {E, cE, N, cN}
+  const double* V;    // [nbas][nbas]
+  int64_t nbas;
+  int gga;
+  double* ham;        // packed out
+  double* exc_nel;    // {E, N} out
+};
+
+// one segment of a chunk: tiles [t0, t0 + n) (chunk-relative) of context m
+struct SetSeg {
+  int64_t t0, n;
+  int m;
+  int pad_;
+};
+
+__global__ void k_set_adjust_items(BasisItem* __restrict__ it, int64_t n, int64_t dtile, int64_t dslot, int dexp,
+                                   int dcon, int drng) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  it[i].tile += (int)dtile;
+  it[i].slot += dslot;
+  it[i].exp_off += dexp;
+  it[i].con_off += dcon;
+  it[i].rad_off += drng;
+}
+
+// Per segment (block): the fixed-order sum of its tiles' partials, Kahan-added
+// into its context's acc.
+__global__ void k_set_sum(const double* __restrict__ partial, const SetSeg* __restrict__ seg,
+                          const SetOutDev* __restrict__ out) {
+  const SetSeg g = seg[blockIdx.x];
+  __shared__ double se[128], sq[128];
+  double e = 0.0, q = 0.0;
+  for (int64_t i = threadIdx.x; i < g.n; i += blockDim.x) {
+    e += partial[2 * (g.t0 + i)];
+    q += partial[2 * (g.t0 + i) + 1];
+  }
+  se[threadIdx.x] = e;
+  sq[threadIdx.x] = q;
+  __syncthreads();
+  for (int s = 64; s > 0; s >>= 1) {
+    if (threadIdx.x < s) {
+      se[threadIdx.x] += se[threadIdx.x + s];
+      sq[threadIdx.x] += sq[threadIdx.x + s];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double* acc = out[g.m].acc;
+    const double vals[2] = {se[0], sq[0]};
+    for (int k = 0; k < 2; ++k) {
+      const double y = vals[k] - acc[2 * k + 1];
+      const double t = acc[2 * k] + y;
+      acc[2 * k + 1] = (t - acc[2 * k]) - y;
+      acc[2 * k] = t;
+    }
+  }
+}
+
+// Block per context: the packed triangle (tristore order; GGA: H + H^T) and
+// {E_xc, N_el}.
+__global__ void k_set_pack(const SetOutDev* __restrict__ out) {
+  const SetOutDev o = out[blockIdx.x];
+  const int64_t len = o.nbas * (o.nbas + 1) / 2;
+  for (int64_t idx = threadIdx.x; idx < len; idx += blockDim.x) {
+    int64_t j = (int64_t)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
+    while (j * (j + 1) / 2 > idx) --j;
+    while ((j + 1) * (j + 2) / 2 <= idx) ++j;
+    const int64_t k = idx - j * (j + 1) / 2;
+    double v = o.V[k * o.nbas + j];
+    if (o.gga) v += o.V[j * o.nbas + k];
+    o.ham[idx] = v;
+  }
+  if (threadIdx.x == 0) {
+    o.exc_nel[0] = o.acc[0];
+    o.exc_nel[1] = o.acc[2];
+  }
+}
+
+}  // namespace
+
+struct ScreenSet {
+  struct Group {
+    XcConst xc;
+    bool gga;
+  };
+  struct Chunk {
+    int64_t t0, t1, s0;
+    int64_t i0[kMaxL + 1], i1[kMaxL + 1];
+    int group;
+    int64_t seg0, nseg;
+  };
+  std::vector<SetMember> mem;
+  std::vector<Group> groups;
+  std::vector<Chunk> chunks;
+  int64_t ntiles = 0, nslots = 0, chunk_slots = 0, chunk_tiles = 0;
+  int max_n = 0;
+  DevSA sa;
+  // merged plan (device)
+  double *qx = nullptr, *qy = nullptr, *qz = nullptr, *qw = nullptr;
+  int64_t* tso = nullptr;
+  int* slot_fn = nullptr;
+  int* listed = nullptr;
+  int* tile_mol = nullptr;
+  BasisItem* items[kMaxL + 1] = {};
+  double *exps = nullptr, *norms = nullptr, *contr = nullptr;
+  int2* rng = nullptr;
+  SetMolDev* mols = nullptr;
+  SetOutDev* outs = nullptr;
+  SetSeg* segs = nullptr;
+  int64_t* b_off = nullptr;
+  // chunk buffers
+  double *phi = nullptr, *gx = nullptr, *gy = nullptr, *gz = nullptr;
+  double* pt = nullptr;
+  double* partial = nullptr;
+  unsigned long long* pmax = nullptr;
+  ScreenMixed* mixed = nullptr;
+  int nsm = 148;
+  int64_t launches = 0;
+  std::vector<void*> allocs;
+};
+
+void screen_set_destroy(ScreenSet* s) {
+  if (!s) return;
+  if (s->mixed) screen_mixed_destroy(s->mixed);
+  for (void* p : s->allocs) cudaFree(p);
+  delete s;
+}
+
+void screen_set_stats(const ScreenSet* s, int64_t* ntiles, int64_t* nchunks, int64_t* launches) {
+  if (ntiles) *ntiles = s->ntiles;
+  if (nchunks) *nchunks = (int64_t)s->chunks.size();
+  if (launches) *launches = s->launches;
+}
+
+int screen_set_create(ScreenSet** out, const std::vector<SetMember>& members, int64_t max_chunk_points,
+                      cudaStream_t st, std::string& err) {
+  *out = nullptr;
+  ScreenSet* S = new ScreenSet();
+  auto fail = [&](int code, const std::string& m) {
+    err = "set: " + m;
+    screen_set_destroy(S);
+    return code;
+  };
+#define SS_TRY(call, what)                                                                         \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess)                                                                         \
+      return fail(e_ == cudaErrorMemoryAllocation ? PGXC_ENOMEM : PGXC_ECUDA,                       \
+                  std::string(what) + ": " + cudaGetErrorString(e_));                              \
+  } while (0)
+  auto alloc = [&](auto** p, size_t n) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(**p));
+    if (e == cudaSuccess) {
+      S->allocs.push_back(q);
+      *p = static_cast<std::remove_reference_t<decltype(*p)>>(q);
+    }
+    return e;
+  };
+  if (members.empty()) return fail(PGXC_EINVAL, "no contexts");
+  // members grouped by functional (stable): a chunk holds one functional
+  std::vector<int> order(members.size());
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int x, int y) { return members[(size_t)x].functional < members[(size_t)y].functional; });
+  for (int i : order) S->mem.push_back(members[(size_t)i]);
+  S->sa = S->mem[0].a->sa;
+  for (const SetMember& m : S->mem) {
+    const ScreenPlan* sp = m.sp;
+    if (!sp->mixed || sp->ispin != 1 || sp->keep)
+      return fail(PGXC_ENOTSUP, "every context must be a screened INT8 closed-shell one without keep_orbitals");
+    if (!m.a->sa.identity) return fail(PGXC_ENOTSUP, "contexts with a symmetry adaptation table");
+  }
+  std::vector<int> mgroup(S->mem.size());
+  for (size_t i = 0; i < S->mem.size(); ++i) {
+    if (i == 0 || S->mem[i].functional != S->mem[i - 1].functional)
+      S->groups.push_back({S->mem[i].a->xc, S->mem[i].sp->gga});
+    mgroup[i] = (int)S->groups.size() - 1;
+  }
+  {
+    int dev = 0;
+    SS_TRY(cudaGetDevice(&dev), "cudaGetDevice");
+    SS_TRY(cudaDeviceGetAttribute(&S->nsm, cudaDevAttrMultiProcessorCount, dev), "cudaDeviceGetAttribute");
+  }
+  // --- merged plan -----------------------------------------------------------
+  const size_t nm = S->mem.size();
+  std::vector<int64_t> toff(nm + 1, 0), soff(nm + 1, 0), eoff(nm + 1, 0), coff(nm + 1, 0), roff(nm + 1, 0);
+  std::vector<int64_t> ioff[kMaxL + 1];
+  for (int l = 0; l <= kMaxL; ++l) ioff[l].assign(nm + 1, 0);
+  for (size_t i = 0; i < nm; ++i) {
+    const ScreenPlan* sp = S->mem[i].sp;
+    toff[i + 1] = toff[i] + sp->ntiles;
+    soff[i + 1] = soff[i] + sp->nslots;
+    eoff[i + 1] = eoff[i] + sp->n_exps;
+    coff[i + 1] = coff[i] + sp->n_contr;
+    roff[i + 1] = roff[i] + sp->n_rng;
+    for (int l = 0; l <= kMaxL; ++l) ioff[l][i + 1] = ioff[l][i] + sp->item_off[l].back();
+    S->max_n = std::max(S->max_n, sp->max_n);
+  }
+  S->ntiles = toff[nm];
+  S->nslots = soff[nm];
+  const int64_t T = S->ntiles;
+  SS_TRY(alloc(&S->qx, 4 * (size_t)T * 128), "cudaMalloc");
+  S->qy = S->qx + T * 128;
+  S->qz = S->qx + 2 * T * 128;
+  S->qw = S->qx + 3 * T * 128;
+  SS_TRY(alloc(&S->tso, (size_t)T + 1), "cudaMalloc");
+  SS_TRY(alloc(&S->slot_fn, (size_t)S->nslots), "cudaMalloc");
+  SS_TRY(alloc(&S->listed, (size_t)T), "cudaMalloc");
+  SS_TRY(alloc(&S->tile_mol, (size_t)T), "cudaMalloc");
+  SS_TRY(alloc(&S->exps, (size_t)eoff[nm]), "cudaMalloc");
+  SS_TRY(alloc(&S->norms, (size_t)eoff[nm]), "cudaMalloc");
+  SS_TRY(alloc(&S->contr, (size_t)coff[nm]), "cudaMalloc");
+  SS_TRY(alloc(&S->rng, (size_t)roff[nm]), "cudaMalloc");
+  for (int l = 0; l <= kMaxL; ++l) SS_TRY(alloc(&S->items[l], (size_t)ioff[l][nm]), "cudaMalloc");
+  std::vector<int64_t> h_tso((size_t)T + 1, 0);
+  std::vector<int> h_tile_mol((size_t)T);
+  std::vector<SetMolDev> h_mols(nm);
+  std::vector<SetOutDev> h_outs(nm);
+  for (size_t i = 0; i < nm; ++i) {
+    const ScreenPlan* sp = S->mem[i].sp;
+    const BuildArgs* a = S->mem[i].a;
+    const int64_t nt = sp->ntiles, t0 = toff[i];
+    for (int c = 0; c < 4; ++c) {
+      const double* src = c == 0 ? sp->qx : (c == 1 ? sp->qy : (c == 2 ? sp->qz : sp->qw));
+      SS_TRY(cudaMemcpyAsync(S->qx + c * T * 128 + t0 * 128, src, sizeof(double) * nt * 128,
+                             cudaMemcpyDeviceToDevice, st), "copy");
+    }
+    SS_TRY(cudaMemcpyAsync(S->slot_fn + soff[i], sp->slot_fn, sizeof(int) * sp->nslots, cudaMemcpyDeviceToDevice, st),
+           "copy");
+    SS_TRY(cudaMemcpyAsync(S->listed + t0, sp->listed, sizeof(int) * nt, cudaMemcpyDeviceToDevice, st), "copy");
+    SS_TRY(cudaMemcpyAsync(S->exps + eoff[i], a->exps, sizeof(double) * sp->n_exps, cudaMemcpyDeviceToDevice, st),
+           "copy");
+    SS_TRY(cudaMemcpyAsync(S->norms + eoff[i], a->norms, sizeof(double) * sp->n_exps, cudaMemcpyDeviceToDevice, st),
+           "copy");
+    if (sp->n_contr)
+      SS_TRY(cudaMemcpyAsync(S->contr + coff[i], a->contr, sizeof(double) * sp->n_contr, cudaMemcpyDeviceToDevice,
+                             st), "copy");
+    if (sp->n_rng)
+      SS_TRY(cudaMemcpyAsync(S->rng + roff[i], a->rng, sizeof(int2) * sp->n_rng, cudaMemcpyDeviceToDevice, st),
+             "copy");
+    for (int l = 0; l <= kMaxL; ++l) {
+      const int64_t ni = ioff[l][i + 1] - ioff[l][i];
+      if (!ni) continue;
+      BasisItem* dst = S->items[l] + ioff[l][i];
+      SS_TRY(cudaMemcpyAsync(dst, sp->items[l], sizeof(BasisItem) * ni, cudaMemcpyDeviceToDevice, st), "copy");
+      k_set_adjust_items<<<(unsigned)((ni + 255) / 256), 256, 0, st>>>(dst, ni, t0, soff[i], (int)eoff[i],
+                                                                      (int)coff[i], (int)roff[i]);
+    }
+    for (int64_t t = 0; t <= nt; ++t) h_tso[(size_t)(t0 + t)] = sp->h_tso[(size_t)t] + soff[i];
+    for (int64_t t = 0; t < nt; ++t) h_tile_mol[(size_t)(t0 + t)] = (int)i;
+    const unsigned long long* P8;
+    const int* eP;
+    screen_mixed_p8(sp->mixed, 0, &P8, &eP);
+    h_mols[i] = {P8, eP, sp->nbas, sp->V, sp->nbas};
+    h_outs[i] = {a->acc, sp->V, sp->nbas, sp->gga ? 1 : 0, S->mem[i].d_ham, S->mem[i].d_exc_nel};
+  }
+  SS_TRY(cudaGetLastError(), "item offsets");
+  SS_TRY(cudaMemcpyAsync(S->tso, h_tso.data(), sizeof(int64_t) * h_tso.size(), cudaMemcpyHostToDevice, st), "copy");
+  SS_TRY(cudaMemcpyAsync(S->tile_mol, h_tile_mol.data(), sizeof(int) * h_tile_mol.size(), cudaMemcpyHostToDevice, st),
+         "copy");
+  SS_TRY(alloc(&S->mols, nm), "cudaMalloc");
+  SS_TRY(alloc(&S->outs, nm), "cudaMalloc");
+  SS_TRY(cudaMemcpyAsync(S->mols, h_mols.data(), sizeof(SetMolDev) * nm, cudaMemcpyHostToDevice, st), "copy");
+  SS_TRY(cudaMemcpyAsync(S->outs, h_outs.data(), sizeof(SetOutDev) * nm, cudaMemcpyHostToDevice, st), "copy");
+  // --- chunks: runs of whole tiles of one functional group --------------------
+  size_t freeb = 0, totb = 0;
+  SS_TRY(cudaMemGetInfo(&freeb, &totb), "cudaMemGetInfo");
+  const bool any_gga = std::any_of(S->groups.begin(), S->groups.end(), [](const ScreenSet::Group& g) { return g.gga; });
+  const int64_t per_slot = 128 * 8 * (any_gga ? 4 : 1) + screen_mixed_bytes_per_slot();
+  const int64_t per_tile = 128 * 8 * 8 + screen_mixed_bytes_per_tile() + 128 * 8 + 16;
+  int64_t budget_slots = std::max<int64_t>((int64_t)(0.40 * (double)freeb) / per_slot, S->max_n);
+  int64_t budget_tiles = std::max<int64_t>(1, (int64_t)(0.05 * (double)freeb) / per_tile);
+  if (max_chunk_points > 0) budget_tiles = std::min(budget_tiles, std::max<int64_t>(1, max_chunk_points / 128));
+  budget_tiles = std::min<int64_t>(budget_tiles, 1 << 16);
+  std::vector<int64_t> boff((size_t)T + 1, 0);
+  for (int64_t t = 0; t < T; ++t)
+    boff[(size_t)t + 1] = boff[(size_t)t] + screen_mixed_bstages(h_tso[(size_t)t + 1] - h_tso[(size_t)t]);
+  const int64_t budget_b = std::max<int64_t>((int64_t)(0.20 * (double)freeb) / screen_mixed_bytes_per_bstage(),
+                                             screen_mixed_bstages(S->max_n));
+  std::vector<SetSeg> h_segs;
+  int64_t chunk_b = 0;
+  {
+    int64_t t0 = 0;
+    auto close_chunk = [&](int64_t t1) {
+      ScreenSet::Chunk c{};
+      c.t0 = t0;
+      c.t1 = t1;
+      c.s0 = h_tso[(size_t)t0];
+      c.group = mgroup[(size_t)h_tile_mol[(size_t)t0]];
+      // item ranges: items are ordered by tile within and across contexts
+      for (int l = 0; l <= kMaxL; ++l) {
+        auto first_item = [&](int64_t t) {
+          if (t >= T) return ioff[l][nm];
+          const int m = h_tile_mol[(size_t)t];
+          // the context's items before its tile t - toff[m]
+          return ioff[l][(size_t)m] + S->mem[(size_t)m].sp->tile_item[l][(size_t)(t - toff[(size_t)m])];
+        };
+        c.i0[l] = first_item(t0);
+        c.i1[l] = first_item(t1);
+      }
+      c.seg0 = (int64_t)h_segs.size();
+      for (int64_t t = t0; t < t1;) {
+        const int m = h_tile_mol[(size_t)t];
+        const int64_t te = std::min(t1, toff[(size_t)m + 1]);
+        h_segs.push_back({t - t0, te - t, m, 0});
+        t = te;
+      }
+      c.nseg = (int64_t)h_segs.size() - c.seg0;
+      S->chunks.push_back(c);
+      S->chunk_tiles = std::max(S->chunk_tiles, t1 - t0);
+      S->chunk_slots = std::max(S->chunk_slots, h_tso[(size_t)t1] - h_tso[(size_t)t0]);
+      chunk_b = std::max(chunk_b, boff[(size_t)t1] - boff[(size_t)t0]);
+      t0 = t1;
+    };
+    for (int64_t t = 0; t < T; ++t) {
+      if (t == t0) continue;
+      const bool new_group = mgroup[(size_t)h_tile_mol[(size_t)t]] != mgroup[(size_t)h_tile_mol[(size_t)t0]];
+      const bool full = h_tso[(size_t)t + 1] - h_tso[(size_t)t0] > budget_slots || t + 1 - t0 > budget_tiles ||
+                        boff[(size_t)t + 1] - boff[(size_t)t0] > budget_b;
+      if (new_group || full) close_chunk(t);
+    }
+    close_chunk(T);
+  }
+  SS_TRY(alloc(&S->segs, h_segs.size()), "cudaMalloc");
+  SS_TRY(cudaMemcpyAsync(S->segs, h_segs.data(), sizeof(SetSeg) * h_segs.size(), cudaMemcpyHostToDevice, st), "copy");
+  SS_TRY(alloc(&S->b_off, boff.size()), "cudaMalloc");
+  SS_TRY(cudaMemcpyAsync(S->b_off, boff.data(), sizeof(int64_t) * boff.size(), cudaMemcpyHostToDevice, st), "copy");
+  // --- chunk buffers -----------------------------------------------------------
+  const size_t rows = (size_t)(S->chunk_slots + kSlack) * 128;
+  SS_TRY(alloc(&S->phi, rows), "cudaMalloc (phi)");
+  SS_TRY(cudaMemsetAsync(S->phi, 0, sizeof(double) * rows, st), "memset");
+  if (any_gga) {
+    SS_TRY(alloc(&S->gx, rows), "cudaMalloc (grad phi)");
+    SS_TRY(alloc(&S->gy, rows), "cudaMalloc (grad phi)");
+    SS_TRY(alloc(&S->gz, rows), "cudaMalloc (grad phi)");
+    SS_TRY(cudaMemsetAsync(S->gx, 0, sizeof(double) * rows, st), "memset");
+    SS_TRY(cudaMemsetAsync(S->gy, 0, sizeof(double) * rows, st), "memset");
+    SS_TRY(cudaMemsetAsync(S->gz, 0, sizeof(double) * rows, st), "memset");
+  }
+  SS_TRY(alloc(&S->pt, 8 * (size_t)S->chunk_tiles * 128), "cudaMalloc");
+  SS_TRY(alloc(&S->partial, 2 * (size_t)S->chunk_tiles), "cudaMalloc");
+  SS_TRY(alloc(&S->pmax, (size_t)S->chunk_tiles * 128), "cudaMalloc");
+  SS_TRY(cudaStreamSynchronize(st), "set-up");
+  ScreenMixedInput mi;
+  mi.nbas = 1;  // the members' own density-matrix digits are used
+  mi.ldc = 1;
+  mi.gga = any_gga;
+  mi.nspin = 1;
+  mi.chunk_slots = S->chunk_slots + kSlack;
+  mi.chunk_tiles = S->chunk_tiles;
+  mi.max_n = S->max_n;
+  mi.chunk_bstages = chunk_b;
+  mi.b_off = S->b_off;
+  std::string e2;
+  if (int st2 = screen_mixed_create(&S->mixed, mi, e2)) return fail(st2, e2);
+#undef SS_TRY
+  *out = S;
+  return PGXC_OK;
+}
+
+int screen_set_run(ScreenSet* S, cudaStream_t st, std::string& err) {
+  const int64_t cp = S->chunk_tiles * 128;
+  int64_t launches = 0;
+  for (const ScreenSet::Chunk& c : S->chunks) {
+    const ScreenSet::Group& g = S->groups[(size_t)c.group];
+    const bool gga = g.gga;
+    const int64_t t0 = c.t0, nt = c.t1 - c.t0, s0 = c.s0;
+    double* gxc = gga ? S->gx : nullptr;
+    double* gyc = gga ? S->gy : nullptr;
+    double* gzc = gga ? S->gz : nullptr;
+    cudaMemsetAsync(S->pmax, 0, sizeof(unsigned long long) * nt * 128, st);
+    auto launch_l = [&](auto Lc) {
+      constexpr int L = decltype(Lc)::value;
+      const int64_t i0 = c.i0[L], n = c.i1[L] - c.i0[L];
+      if (n <= 0) return;
+      const unsigned nb = (unsigned)std::min<int64_t>(n, (int64_t)S->nsm * kBasisBlocksPerSM);
+      if (gga)
+        k_basis_items<L, true><<<nb, 128, 0, st>>>(S->items[L] + i0, n, S->exps, S->norms, S->contr, S->rng, S->sa,
+                                                   S->qx, S->qy, S->qz, s0, t0, S->phi, gxc, gyc, gzc, S->pmax);
+      else
+        k_basis_items<L, false><<<nb, 128, 0, st>>>(S->items[L] + i0, n, S->exps, S->norms, S->contr, S->rng, S->sa,
+                                                    S->qx, S->qy, S->qz, s0, t0, S->phi, nullptr, nullptr, nullptr,
+                                                    S->pmax);
+      ++launches;
+    };
+    launch_l(std::integral_constant<int, 0>());
+    launch_l(std::integral_constant<int, 1>());
+    launch_l(std::integral_constant<int, 2>());
+    launch_l(std::integral_constant<int, 3>());
+    if (gga) k_pad_zero<true><<<(unsigned)nt, 128, 0, st>>>(S->tso, S->listed, t0, s0, S->phi, gxc, gyc, gzc);
+    else k_pad_zero<false><<<(unsigned)nt, 128, 0, st>>>(S->tso, S->listed, t0, s0, S->phi, nullptr, nullptr, nullptr);
+    ++launches;
+    screen_mixed_set_gga(S->mixed, gga);
+    launches += screen_mixed_basis(S->mixed, S->tso, S->slot_fn, t0, nt, s0, S->phi, S->pmax, 0, 0, st, S->tile_mol,
+                                   S->mols);
+    double* q = S->pt;
+    BuildArgs b{};
+    b.xc = g.xc;
+    b.w = S->qw;
+    b.rho = q;
+    b.grx = q + cp;
+    b.gry = q + 2 * cp;
+    b.grz = q + 3 * cp;
+    b.A = q + 4 * cp;
+    b.Bx = q + 5 * cp;
+    b.By = q + 6 * cp;
+    b.Bz = q + 7 * cp;
+    b.partial = S->partial;
+    launches += screen_mixed_density(S->mixed, S->tso, S->slot_fn, t0, nt, s0, S->phi, gxc, gyc, gzc, b.rho, b.grx,
+                                     b.gry, b.grz, 0, 0, st);
+    launch_functional_tiles(b, t0 * 128, nt, gga, st);
+    k_set_sum<<<(unsigned)c.nseg, 128, 0, st>>>(S->partial, S->segs + c.seg0, S->outs);
+    launches += 2;
+    launches += screen_mixed_potential(S->mixed, S->tso, S->slot_fn, nullptr, t0, nt, s0, 0, S->phi, gxc, gyc, gzc, b.A,
+                                       b.Bx, b.By, b.Bz, nullptr, 0, st, nullptr, nullptr, S->tile_mol, S->mols);
+  }
+  k_set_pack<<<(unsigned)S->mem.size(), 256, 0, st>>>(S->outs);
+  ++launches;
+  S->launches = launches;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    err = std::string("set build: ") + cudaGetErrorString(e);
+    return PGXC_ECUDA;
+  }
+  return PGXC_OK;
+}
+
+int screen_set_error_flag(ScreenSet* S, cudaStream_t st, int* flag) { return screen_mixed_error_flag(S->mixed, st, flag); }
+
+int screen_set_prepare_member(ScreenPlan* sp, const double* P, int64_t ldc, cudaStream_t st) {
+  if (cudaMemsetAsync(sp->V, 0, sizeof(double) * sp->nbas * sp->nbas, st) != cudaSuccess) return PGXC_ECUDA;
+  screen_mixed_prepare(sp->mixed, P, ldc, 0, st);
+  return cudaGetLastError() == cudaSuccess ? PGXC_OK : PGXC_ECUDA;
+}
+
+bool screen_set_eligible(const ScreenPlan* sp) { return sp->mixed && sp->ispin == 1 && !sp->keep; }
 
 }  // namespace pgxc

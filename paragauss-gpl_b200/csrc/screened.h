@@ -72,6 +72,41 @@ struct ScreenExtra {
 int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_t st, double* ham, ScreenTimes* t,
                std::string& err, const ScreenExtra* extra = nullptr);
 int screen_error_flag(ScreenPlan* sp, cudaStream_t st, int* flag);
+
+// ---------------------------------------------------------------------------
+// Sets: the screened INT8 builds of many contexts (closed shell, identity
+// symmetry adaptation) run as one sequence of launches over the tiles of all
+// of them: per chunk of the concatenated tile queue one basis launch per
+// angular momentum, one gather, one density contraction, one functional,
+// one Z quantization and one potential contraction, each walking tiles of
+// many contexts (their density-matrix digits and potential matrices through
+// a per-tile context table), and one packing launch for all contexts.
+// Contexts are grouped by functional (a chunk holds one functional).
+// ---------------------------------------------------------------------------
+struct ScreenSet;
+struct SetMember {
+  ScreenPlan* sp;
+  const BuildArgs* a;    // the context's arguments (basis tables, functional, acc)
+  int functional;        // PGXC_XC_* id
+  double* d_ham;         // packed matrix out (overwritten)
+  double* d_exc_nel;     // {E_xc, N_el} out (overwritten)
+};
+// max_chunk_points: 0 -> sized from free device memory
+int screen_set_create(ScreenSet** out, const std::vector<SetMember>& members, int64_t max_chunk_points,
+                      cudaStream_t st, std::string& err);
+void screen_set_destroy(ScreenSet* s);
+// Enqueue the set's build on st (capturable: no synchronisation, events or
+// host reads).  Each member's density-matrix digits (screen_mixed_prepare),
+// potential accumulator (zeroed) and acc (zeroed) must be ready on st.
+int screen_set_run(ScreenSet* s, cudaStream_t st, std::string& err);
+int screen_set_error_flag(ScreenSet* s, cudaStream_t st, int* flag);
+// A member's per-build preparation on st: its potential accumulator zeroed
+// and its density matrix P (leading dimension ldc) in digit form.
+int screen_set_prepare_member(ScreenPlan* sp, const double* P, int64_t ldc, cudaStream_t st);
+// whether a context's plan can join a set (screened INT8, closed shell, basis not kept)
+bool screen_set_eligible(const ScreenPlan* sp);
+// tiles, chunks and launches of one run
+void screen_set_stats(const ScreenSet* s, int64_t* ntiles, int64_t* nchunks, int64_t* launches);
 // Plan statistics: tiles, total slots (padded), listed functions, sum of n_t^2.
 void screen_stats(const ScreenPlan* sp, int64_t* ntiles, int64_t* nslots, int64_t* nlisted, double* sum_n2,
                   int64_t* nchunks);

@@ -168,14 +168,22 @@ __device__ __forceinline__ unsigned long long gather_slice(const unsigned long l
 // tile's slots are zero.  One block per tile, thread = (row, 8 K values).
 // ---------------------------------------------------------------------------
 constexpr int kGatherSplit = 4;  // blocks per tile: block y takes the slot blocks j = y, y + 4, ...
-__global__ void __launch_bounds__(192) k_sm_gather_B(const int64_t* __restrict__ tso,
+__global__ void __launch_bounds__(kBlock4(192)) k_sm_gather_B(const int64_t* __restrict__ tso,
                                                     const int* __restrict__ slot_fn,
                                                     const int64_t* __restrict__ b_off, int64_t t0, int64_t s0,
                                                     const unsigned long long* __restrict__ P8,
                                                     const int* __restrict__ e_P, int64_t nbas,
-                                                    int8_t* __restrict__ tB, double* __restrict__ ps) {
+                                                    int8_t* __restrict__ tB, double* __restrict__ ps,
+                                                    const int* __restrict__ tile_mol,
+                                                    const SetMolDev* __restrict__ mols) {
   extern __shared__ int sfn[];
   const int64_t t = t0 + blockIdx.x;
+  if (tile_mol) {  // a set: this tile's context
+    const SetMolDev& M = mols[tile_mol[t]];
+    P8 = M.P8;
+    e_P = M.e_P;
+    nbas = M.nbas;
+  }
   const int64_t sg = tso[t];
   const int n = (int)(tso[t + 1] - sg);
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -184,6 +192,7 @@ __global__ void __launch_bounds__(192) k_sm_gather_B(const int64_t* __restrict__
     if (blockIdx.y == 0) ps[sg - s0 + i] = f >= 0 ? pow2(e_P[f]) : 0.0;  // P's row scale for the density epilogue
   }
   __syncthreads();
+  if (threadIdx.x >= 192) return;  // thread = (row of 48, group of 8 K values)
   const int nK = n / 32, nN = (n + kN - 1) / kN;
   const int r = threadIdx.x >> 2, grp = threadIdx.x & 3;
   int8_t* out = tB + (b_off[t] - b_off[t0]) * kOpB;
@@ -570,11 +579,12 @@ constexpr int kVThreads = tc::kWholeSmThreads;  // warps 0-7 epilogue, 8 MMA, 9 
 // LDA keeps j >= i: the last 48-slot row block I of column block J
 __device__ __forceinline__ int last_I(int J, int nI, bool all) { return all ? nI : min(nI, (kM * J + kM - 1) / kN + 1); }
 
-template <bool GGA>
+template <bool GGA, bool SET>
 __global__ void __launch_bounds__(kVThreads, 1)
     k_sm_vpot(const int64_t* __restrict__ tso, const int* __restrict__ slot_fn, int64_t t0, int64_t nt, int64_t s0,
               const int8_t* __restrict__ tF, const int8_t* __restrict__ tZ, const double* __restrict__ fs,
-              const double* __restrict__ zs, double* __restrict__ V, int64_t ldv, int* err) {
+              const double* __restrict__ zs, double* __restrict__ V, int64_t ldv, int* err,
+              const int* __restrict__ tile_mol, const SetMolDev* __restrict__ mols) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   VSmem& S = *reinterpret_cast<VSmem*>(smem_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -683,6 +693,13 @@ __global__ void __launch_bounds__(kVThreads, 1)
       const int n = (int)(tso[t0 + ti + 1] - sg);
       const int nJ = (n + kM - 1) / kM, nI = (n + kN - 1) / kN;
       const int* sfn = slot_fn + sg;
+      double* Vt = V;  // this tile's potential matrix (a set: its context's)
+      int64_t ldt = ldv;
+      if (SET) {
+        const SetMolDev& M = mols[tile_mol[t0 + ti]];
+        Vt = M.V;
+        ldt = M.ldv;
+      }
       for (int J = 0; J < nJ && ok; ++J) {
         const int j = J * kM + (warp & 3) * 32 + lane;
         const int fj = j < n ? __ldg(sfn + j) : -1;
@@ -706,7 +723,7 @@ __global__ void __launch_bounds__(kVThreads, 1)
           for (int c = 0; c < 24; ++c) {
             const int fi = __shfl_sync(0xffffffffu, fil, c);
             const double zsc = __shfl_sync(0xffffffffu, zsl, c);
-            if (fj >= 0 && fi >= 0 && (GGA || fj >= fi)) atomicAdd(V + (int64_t)fi * ldv + fj, x[c] * (fsj * zsc));
+            if (fj >= 0 && fi >= 0 && (GGA || fj >= fi)) atomicAdd(Vt + (int64_t)fi * ldt + fj, x[c] * (fsj * zsc));
           }
         }
       }
@@ -767,8 +784,10 @@ int screen_mixed_create(ScreenMixed** out, const ScreenMixedInput& in, std::stri
   raise_smem_limit(k_sm_gather_B, 4 * in.max_n);
   cudaFuncSetAttribute(k_sm_density<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm);
   cudaFuncSetAttribute(k_sm_density<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm);
-  cudaFuncSetAttribute(k_sm_vpot<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kWholeSmSmem);
-  e = cudaFuncSetAttribute(k_sm_vpot<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kWholeSmSmem);
+  cudaFuncSetAttribute(k_sm_vpot<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kWholeSmSmem);
+  cudaFuncSetAttribute(k_sm_vpot<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kWholeSmSmem);
+  cudaFuncSetAttribute(k_sm_vpot<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kWholeSmSmem);
+  e = cudaFuncSetAttribute(k_sm_vpot<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kWholeSmSmem);
   int dev = 0;
   if (e == cudaSuccess) e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&m->nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -796,16 +815,19 @@ int screen_mixed_prepare(ScreenMixed* m, const double* P, int64_t ldc, int spin,
 }
 
 int screen_mixed_basis(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
-                       const double* phi, const unsigned long long* pmax, int64_t so, int64_t to, cudaStream_t st) {
+                       const double* phi, const unsigned long long* pmax, int64_t so, int64_t to, cudaStream_t st,
+                       const int* tile_mol, const SetMolDev* mols) {
   k_sm_quant_pts<<<(unsigned)nt, 128, 0, st>>>(tso, t0, s0, phi, pmax, m->e_pt + to * 128,
                                               m->tA + so * kDigBytesPerSlot);
-  return 1 + screen_mixed_gather(m, tso, slot_fn, t0, nt, s0, 0, st);
+  return 1 + screen_mixed_gather(m, tso, slot_fn, t0, nt, s0, 0, st, tile_mol, mols);
 }
 
+void screen_mixed_set_gga(ScreenMixed* m, bool gga) { m->gga = gga; }
+
 int screen_mixed_gather(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
-                        int spin, cudaStream_t st) {
-  k_sm_gather_B<<<dim3((unsigned)nt, kGatherSplit), 192, 4 * m->max_n, st>>>(
-      tso, slot_fn, m->b_off, t0, s0, m->P8[spin], m->e_P[spin], m->nbas, m->tB, m->ps);
+                        int spin, cudaStream_t st, const int* tile_mol, const SetMolDev* mols) {
+  k_sm_gather_B<<<dim3((unsigned)nt, kGatherSplit), kBlock4(192), 4 * m->max_n, st>>>(
+      tso, slot_fn, m->b_off, t0, s0, m->P8[spin], m->e_P[spin], m->nbas, m->tB, m->ps, tile_mol, mols);
   return 1;
 }
 
@@ -835,7 +857,8 @@ int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn,
 int screen_mixed_potential(ScreenMixed* m, const int64_t* tso, const int* slot_fn, const int* slot_tile, int64_t t0,
                            int64_t nt, int64_t s0, int64_t ns, const double* phi, const double* gx, const double* gy,
                            const double* gz, const double* A, const double* Bx, const double* By, const double* Bz,
-                           double* V, int64_t ldv, cudaStream_t st, cudaEvent_t k0, cudaEvent_t k1) {
+                           double* V, int64_t ldv, cudaStream_t st, cudaEvent_t k0, cudaEvent_t k1,
+                           const int* tile_mol, const SetMolDev* mols) {
   (void)slot_tile;
   (void)ns;
   if (m->gga)
@@ -846,14 +869,24 @@ int screen_mixed_potential(ScreenMixed* m, const int64_t* tso, const int* slot_f
                                                      nullptr, nullptr, m->tZ, m->tF, m->zs, m->fs);
   if (k0) cudaEventRecord(k0, st);
   const unsigned grid = (unsigned)std::min<int64_t>(nt, m->nsm);
-  if (m->gga)
-    k_sm_vpot<true><<<grid, kVThreads, tc::kWholeSmSmem, st>>>(tso, slot_fn, t0, nt, s0, m->tF, m->tZ, m->fs, m->zs, V, ldv,
-                                                   m->err);
-  else
-    k_sm_vpot<false><<<grid, kVThreads, tc::kWholeSmSmem, st>>>(tso, slot_fn, t0, nt, s0, m->tF, m->tZ, m->fs, m->zs, V, ldv,
-                                                    m->err);
+  auto launch = [&](auto kern) {
+    kern<<<grid, kVThreads, tc::kWholeSmSmem, st>>>(tso, slot_fn, t0, nt, s0, m->tF, m->tZ, m->fs, m->zs, V, ldv, m->err,
+                                                   tile_mol, mols);
+  };
+  if (m->gga) {
+    if (tile_mol) launch(k_sm_vpot<true, true>);
+    else launch(k_sm_vpot<true, false>);
+  } else {
+    if (tile_mol) launch(k_sm_vpot<false, true>);
+    else launch(k_sm_vpot<false, false>);
+  }
   if (k1) cudaEventRecord(k1, st);
   return 2;
+}
+
+void screen_mixed_p8(ScreenMixed* m, int spin, const unsigned long long** P8, const int** e_P) {
+  *P8 = m->P8[spin];
+  *e_P = m->e_P[spin];
 }
 
 int screen_mixed_error_flag(ScreenMixed* m, cudaStream_t st, int* flag) {

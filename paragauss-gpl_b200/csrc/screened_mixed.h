@@ -13,6 +13,17 @@ namespace pgxc {
 
 struct ScreenMixed;
 
+// One context of a multi-context set (screened.cu, screen_set_*): the
+// tensor-core kernels take the density-matrix digits and the potential
+// matrix of each tile's context from this table.
+struct SetMolDev {
+  const unsigned long long* P8;  // digits of P, [nbas][nbas]
+  const int* e_P;                // row scales of P
+  int64_t nbas;
+  double* V;                     // potential accumulator, [nbas][ldv]
+  int64_t ldv;
+};
+
 struct ScreenMixedInput {
   int64_t nbas = 0, ldc = 0;
   bool gga = false;
@@ -41,19 +52,27 @@ int screen_mixed_prepare(ScreenMixed* m, const double* P, int64_t ldc, int spin,
 // chunk) and the gathered digits of P[S_t, S_t] of every tile (spin 0)
 // so / to: the chunk's first slot / tile in the resident digit arrays (0 when they are per chunk)
 int screen_mixed_basis(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
-                       const double* phi, const unsigned long long* pmax, int64_t so, int64_t to, cudaStream_t st);
-// the gathered digits of P_spin[S_t, S_t] of every tile (replaces the previous spin's)
+                       const double* phi, const unsigned long long* pmax, int64_t so, int64_t to, cudaStream_t st,
+                       const int* tile_mol = nullptr, const SetMolDev* mols = nullptr);
+// the functional kind of the following launches (a set's chunks alternate)
+void screen_mixed_set_gga(ScreenMixed* m, bool gga);
+// the gathered digits of P_spin[S_t, S_t] of every tile (replaces the previous spin's);
+// with tile_mol, tile t's digits come from mols[tile_mol[t]] instead
 int screen_mixed_gather(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
-                        int spin, cudaStream_t st);
+                        int spin, cudaStream_t st, const int* tile_mol = nullptr, const SetMolDev* mols = nullptr);
 int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
                          const double* phi, const double* gx, const double* gy, const double* gz, double* rho,
                          double* grx, double* gry, double* grz, int64_t so, int64_t to, cudaStream_t st);
 // Z digits (per-slot scales), then H[S_t, S_t] += Z_t^T phi_t scatter-added into V;
 // records k0 / k1 around the contraction kernel
+// (with tile_mol: into mols[tile_mol[t]].V of each tile t instead of V)
 int screen_mixed_potential(ScreenMixed* m, const int64_t* tso, const int* slot_fn, const int* slot_tile, int64_t t0,
                            int64_t nt, int64_t s0, int64_t ns, const double* phi, const double* gx, const double* gy,
                            const double* gz, const double* A, const double* Bx, const double* By, const double* Bz,
-                           double* V, int64_t ldv, cudaStream_t st, cudaEvent_t k0, cudaEvent_t k1);
+                           double* V, int64_t ldv, cudaStream_t st, cudaEvent_t k0, cudaEvent_t k1,
+                           const int* tile_mol = nullptr, const SetMolDev* mols = nullptr);
+// the digits of P_spin and their row scales (read by a set's gather)
+void screen_mixed_p8(ScreenMixed* m, int spin, const unsigned long long** P8, const int** e_P);
 // copies the device error flag (a bounded wait ran out) to *flag and clears it
 int screen_mixed_error_flag(ScreenMixed* m, cudaStream_t st, int* flag);
 

@@ -64,12 +64,70 @@ __global__ void k_sym_potential(SymDev S, int ispin, const double* __restrict__ 
   }
 }
 
+// One thread per element quadruple of a pseudo-2D irrep's packed matrix.
+// Pair q: blocks X (first function px, half hx) >= Y (py, hy) of one irrep
+// (packed offset pk); element (r, c) of the pair's A x A part, r < hx, c < hy
+// (X == Y: c <= r).  The reference's loops (xc_pseudo2d_sym,
+// modules/xc_hamiltonian.f90:2637-2779) touch every element of a quadruple
+// once, so the quadruples are independent.
+__device__ __forceinline__ int64_t pk1(int64_t j, int64_t k) { return j * (j + 1) / 2 + k; }  // k <= j, 0-based
+
+__global__ void k_pseudo2d(const Pseudo2dPair* __restrict__ pairs, const int64_t* __restrict__ first,
+                           int64_t npairs_total, int ispin, double* __restrict__ ham) {
+  // first[q] = the pair's first quadruple; quadruples of pair q: [first[q], first[q + 1])
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < first[npairs_total];
+       e += (int64_t)gridDim.x * blockDim.x) {
+    int64_t lo = 0, hi = npairs_total;  // the pair holding quadruple e
+    while (hi - lo > 1) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (first[mid] <= e) lo = mid;
+      else hi = mid;
+    }
+    const Pseudo2dPair P = pairs[lo];
+    const int64_t t = e - first[lo];
+    int64_t r, c;
+    if (P.same) {  // t enumerates (r, c), c <= r
+      r = (int64_t)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+      while (r * (r + 1) / 2 > t) --r;
+      while ((r + 1) * (r + 2) / 2 <= t) ++r;
+      c = t - r * (r + 1) / 2;
+    } else {
+      r = t / P.hy;
+      c = t - r * P.hy;
+    }
+    for (int s = 0; s < ispin; ++s) {
+      auto at = [&](int64_t j, int64_t k) -> double& { return ham[s + ispin * (P.pk + pk1(j, k))]; };
+      if (P.same) {
+        // A x A and B x B (r >= c): their mean into both
+        double& aa = at(P.px + r, P.px + c);
+        double& bb = at(P.px + P.hx + r, P.px + P.hx + c);
+        aa = 0.5 * (aa + bb);
+        bb = aa;
+        // B x A: H(B_c, A_r) = (H(B_c, A_r) - H(B_r, A_c)) / 2, H(B_r, A_c) = -H(B_c, A_r)
+        double& x4 = at(P.px + P.hx + c, P.px + r);
+        double& x3 = at(P.px + P.hx + r, P.px + c);
+        x4 = 0.5 * (x4 - x3);
+        x3 = -x4;
+      } else {
+        double& aa = at(P.px + r, P.py + c);
+        double& bb = at(P.px + P.hx + r, P.py + P.hy + c);
+        aa = 0.5 * (aa + bb);
+        bb = aa;
+        double& ab = at(P.px + r, P.py + P.hy + c);
+        double& ba = at(P.px + P.hx + r, P.py + c);
+        ab = 0.5 * (ab - ba);
+        ba = -ab;
+      }
+    }
+  }
+}
+
 }  // namespace
 
 void launch_sym_orbitals(const SymDev& S, const double* Csa, const int64_t* cofs, const int* nocc,
                          const int64_t* col0, int nocc_max, double* C, int64_t ldc, cudaStream_t st) {
   if (S.ngroups == 0 || nocc_max == 0) return;
-  const int threads = nocc_max >= 128 ? 128 : ((nocc_max + 31) / 32) * 32;
+  const int threads = 128;  // whole groups of four warps (kBlock4); threads past nocc idle
   k_sym_orbitals<<<S.ngroups, threads, 0, st>>>(S, Csa, cofs, nocc, col0, C, ldc);
 }
 
@@ -79,6 +137,17 @@ void launch_sym_potential(const SymDev& S, int max_dim, int ispin, const double*
   if (np_max == 0 || S.n_irrep == 0) return;
   const dim3 grid((unsigned)((np_max + 255) / 256), (unsigned)S.n_irrep);
   k_sym_potential<<<grid, 256, 0, st>>>(S, ispin, V, ham_sym);
+}
+
+}  // namespace pgxc
+
+namespace pgxc {
+
+void launch_pseudo2d(const Pseudo2dPair* pairs, const int64_t* first, int64_t npairs, int64_t nquads, int ispin,
+                     double* ham, cudaStream_t st) {
+  if (npairs == 0 || nquads == 0) return;
+  const unsigned nb = (unsigned)std::min<int64_t>((nquads + 255) / 256, 148 * 16);
+  k_pseudo2d<<<nb, 256, 0, st>>>(pairs, first, npairs, ispin, ham);
 }
 
 }  // namespace pgxc

@@ -48,4 +48,19 @@ void launch_sym_orbitals(const SymDev& S, const double* Csa, const int64_t* cofs
 void launch_sym_potential(const SymDev& S, int max_dim, int ispin, const double* V, double* ham_sym,
                           cudaStream_t st);
 
+// Pseudo-2D irreps (xc_pseudo2d_sym, modules/xc_hamiltonian.f90:2637-2779):
+// the functions of every (unique atom, l) block of such an irrep come in two
+// halves A, B; the matrix is made to satisfy H(X_A, Y_A) = H(X_B, Y_B) and
+// H(X_A, Y_B) = -H(X_B, Y_A) for every pair of blocks X >= Y.  One entry per
+// block pair: X's first function px and half hx, Y's py, hy (0-based within
+// the irrep), the irrep's packed offset pk, same = (X == Y).
+struct Pseudo2dPair {
+  int64_t pk;
+  int64_t px, hx, py, hy;
+  int64_t same;
+};
+// first[q]: quadruples before pair q (first[npairs] = nquads)
+void launch_pseudo2d(const Pseudo2dPair* pairs, const int64_t* first, int64_t npairs, int64_t nquads, int ispin,
+                     double* ham, cudaStream_t st);
+
 }  // namespace pgxc

@@ -49,7 +49,7 @@ def build(force=False, verbose=False):
 
     with ThreadPoolExecutor(max_workers=min(len(SOURCES), os.cpu_count() or 4)) as ex:
         objs = list(ex.map(compile_one, SOURCES))
-    cmd = [cc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared"] + objs + ["-lcublas", "-o", LIB]
+    cmd = [cc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared"] + objs + ["-o", LIB]
     if verbose:
         print(" ".join(cmd), file=sys.stderr)
     subprocess.run(cmd, check=True, cwd=CSRC)

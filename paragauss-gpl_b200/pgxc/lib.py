@@ -54,6 +54,9 @@ def lib():
     L.pgxc_strerror.restype = ct.c_char_p
     L.pgxc_destroy.argtypes = [vp]
     L.pgxc_batch_create.argtypes = [P(vp), ct.c_int32, P(vp), P(vp), P(ct.c_int32), P(vp), P(vp), P(vp)]
+    L.pgxc_batch_create_chunked.argtypes = [P(vp), ct.c_int32, P(vp), P(vp), P(ct.c_int32), P(vp), P(vp),
+                                            ct.c_int64, P(vp)]
+    L.pgxc_batch_is_set.argtypes = [vp, P(ct.c_int32)]
     L.pgxc_batch_run.argtypes = [vp, P(ct.c_double)]
     L.pgxc_batch_destroy.argtypes = [vp]
     L.pgxc_batch_stats.argtypes = [vp, P(ct.c_int64), P(ct.c_int64)]
@@ -62,6 +65,7 @@ def lib():
     L.pgxc_xc_energies.argtypes = [vp, abi._f64p, abi._f64p, ct.c_int32, ct.c_int32, ct.c_int32, ct.c_int32,
                                    abi._i32p, abi._f64p, P(ct.c_double)]
     L.pgxc_set_symmetry.argtypes = [vp, P(abi.Symmetry)]
+    L.pgxc_set_pseudo2d.argtypes = [vp, abi._i32p, abi._i32p, abi._i32p]
     L.pgxc_sym_xc_length.argtypes = [vp, P(ct.c_int64)]
     L.pgxc_build_sym.argtypes = [vp, P(abi._f64p), P(abi._f64p), abi._i32p, ct.c_int32, abi._f64p, ct.c_int64,
                                  P(ct.c_double), P(ct.c_double), P(abi.Timings)]
@@ -160,6 +164,15 @@ class Context:
         _check(lib().pgxc_sym_xc_length(self.h, ct.byref(n)), self.h)
         self.sym_xc_length = n.value
 
+    def set_pseudo2d(self, nblocks, first=(), half=()):
+        """Pseudo-2D irreps (pgxc_set_pseudo2d): per irrep its (atom, l) blocks'
+        first functions and half sizes; None removes it."""
+        if nblocks is None:
+            _check(lib().pgxc_set_pseudo2d(self.h, None, None, None), self.h)
+            return
+        self._p2 = [np.ascontiguousarray(x, dtype=np.int32) for x in (nblocks, first, half)]
+        _check(lib().pgxc_set_pseudo2d(self.h, *[abi.i32p(x) for x in self._p2]), self.h)
+
     def build_sym(self, Cs, occs, ham=None, timings=False):
         """Symmetry-adapted build from per-irrep C (dims, nocc, ispin) and occ
         (nocc, ispin); returns (ham_xc_arr, exc, nel[, timings])."""
@@ -245,7 +258,8 @@ class Batch:
     pointers (ints): C and occ in the pgxc_build_device layout, the packed V
     and {E_xc, N_el} outputs (overwritten by every run)."""
 
-    def __init__(self, contexts, d_C, d_occ, d_ham, d_exc_nel):
+    def __init__(self, contexts, d_C, d_occ, d_ham, d_exc_nel, max_chunk_points=0):
+        """max_chunk_points: the chunk of a set of INT8 contexts (0: from free memory)."""
         n = len(contexts)
         arr = lambda xs: (ct.c_void_p * n)(*[ct.c_void_p(int(x)) for x in xs])
         self.contexts = list(contexts)  # kept alive while the batch exists
@@ -253,8 +267,15 @@ class Batch:
                       (ct.c_int32 * n)(*[c.case.nocc for c in contexts]), arr(d_ham), arr(d_exc_nel))
         h = ct.c_void_p()
         a = self._args
-        _check(lib().pgxc_batch_create(a[0], n, a[1], a[2], a[3], a[4], a[5], ct.byref(h)))
+        _check(lib().pgxc_batch_create_chunked(a[0], n, a[1], a[2], a[3], a[4], a[5], int(max_chunk_points),
+                                               ct.byref(h)))
         self.h = h
+
+    def is_set(self):
+        """Whether the batch runs as one set (one launch per kernel over all contexts' tiles)."""
+        v = ct.c_int32()
+        _check(lib().pgxc_batch_is_set(self.h, ct.byref(v)))
+        return bool(v.value)
 
     def run(self):
         """One replay of every build; returns its device time in ms."""

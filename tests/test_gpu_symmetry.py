@@ -92,3 +92,44 @@ def test_reduced_grid_build_matches_full_grid_oracle(precision, thr, tol):
         ham, e, n = ctx.build_sym(Cs, occs)
     assert abs(e - re) < tol and abs(n - rn) < tol
     assert float(np.max(np.abs(ham - ref))) < tol
+
+
+@pytest.mark.parametrize("ispin", [1, 2])
+def test_pseudo2d_symmetrisation_on_the_device(ispin):
+    """pgxc_set_pseudo2d: the built matrix equals the oracle's restatement of
+    xc_pseudo2d_sym applied to the build without it (bit for bit: the same
+    halvings of sums and differences)."""
+    case, ad, Cs, occs = Y.symmetric_case("C3v", functional="PBE", ispin=ispin)
+    dims = list(ad.dims)
+    i = int(np.argmax(dims))              # declare blocks in the largest irrep
+    d = dims[i]
+    first, half, pos = [], [], 0
+    for h in (2, 3, 1):
+        if pos + 2 * h > d:
+            break
+        first.append(pos)
+        half.append(h)
+        pos += 2 * h + 1
+    nblocks = [0] * len(dims)
+    nblocks[i] = len(first)
+    with lib.Context(case, screen_threshold=0.0) as ctx:
+        ctx.set_symmetry(ad)
+        h0, e0, n0 = ctx.build_sym(Cs, occs)
+        ctx.set_pseudo2d(nblocks, first, half)
+        h1, e1, n1 = ctx.build_sym(Cs, occs)
+        ctx.set_pseudo2d(None)
+        h2, _, _ = ctx.build_sym(Cs, occs)
+    want = O.pseudo2d_sym(h0, ispin, dims, nblocks, first, half)
+    np.testing.assert_allclose(h1, want, rtol=0, atol=1e-14)
+    assert not np.allclose(h1, h0)
+    np.testing.assert_allclose(h2, h0, rtol=0, atol=1e-14)
+    assert e1 == e0 and n1 == n0
+
+
+def test_pseudo2d_rejects_bad_blocks():
+    case, ad, Cs, occs = Y.symmetric_case("C2v", functional="VWN")
+    with lib.Context(case, screen_threshold=0.0) as ctx:
+        ctx.set_symmetry(ad)
+        d = ad.dims[0]
+        with pytest.raises(lib.PgxcError):
+            ctx.set_pseudo2d([1] + [0] * (len(ad.dims) - 1), [0], [d])   # 2 * half > dims
