@@ -364,14 +364,16 @@ def gradient_leg(torch, sub, local):
     try:
         ctx.xc_gradient()
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        g, e = ctx.xc_gradient()
-        ms = (time.perf_counter() - t0) * 1e3
+        times = []
+        for _ in range(2):
+            t0 = time.perf_counter()
+            g, e = ctx.xc_gradient()
+            times.append((time.perf_counter() - t0) * 1e3)
     finally:
         ctx.close()
-    return {"ms": ms, "E_xc": e, "max_abs_component": float(abs(g).max()), "sum_over_atoms": float(abs(g.sum(0)).max()),
+    return {"ms": min(times), "ms_calls": times, "E_xc": e, "max_abs_component": float(abs(g).max()), "sum_over_atoms": float(abs(g.sum(0)).max()),
             "note": "dE_xc/dR of every atom with the grid moving with its atoms and the Becke weights differentiated; "
-                    "host wall clock around one synchronous call (inputs from host memory)"}
+                    "host wall clock around one synchronous call (inputs from host memory), the faster of two calls"}
 
 
 # ---------------------------------------------------------------------------
@@ -425,11 +427,19 @@ def run_batch(args):
     del ctx64
     torch.cuda.empty_cache()
 
-    # the contexts' own chunk buffers (used by the one-by-one builds) stay small; the set has its own
+    # INT8, one molecule after another, with the same per-context chunks as the FP64 path
+    ctx8 = [lib.Context(m, precision="mixed", weighted=False, max_chunk_points=chunk, screen_threshold=args.screen)
+            for m in mols]
+    ms_seq = one_by_one(ctx8, ops64, max(1, min(args.steps, 2)))
+    for c in ctx8:
+        c.close()
+    del ctx8, ops64
+    torch.cuda.empty_cache()
+
+    # the set: the contexts' own chunk buffers stay small (the set does not use them); the set has its own
     ctxs = [lib.Context(m, precision="mixed", weighted=False, max_chunk_points=4096, screen_threshold=args.screen)
             for m in mols]
     ops = operands()
-    ms_seq = one_by_one(ctxs, ops, max(1, min(args.steps, 2)))
     dC, docc, dham, dsum = ops
     batch = lib.Batch(ctxs, [t.data_ptr() for t in dC], [t.data_ptr() for t in docc], [t.data_ptr() for t in dham],
                       [t.data_ptr() for t in dsum], max_chunk_points=set_chunk)

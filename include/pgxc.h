@@ -350,8 +350,8 @@ int pgxc_build_device(pgxc_ctx* ctx, const double* d_C, const double* d_occ,
  * modules/post_scf_module.f90:2569-3318, :3500-5193; density_calc_ph_nl,
  * modules/density_calc_module.f90:2000-3315; becke1, modules/grid_module.f90
  * :2499-2616).  Needs a context created with weights_are_raw (PGXC_ENOTSUP
- * otherwise).  FP64 in every precision mode; C1 only: a context with
- * pgxc_set_symmetry applied returns PGXC_ENOTSUP.
+ * otherwise).  FP64 in every precision mode.  A context with
+ * pgxc_set_symmetry applied takes pgxc_xc_gradient_sym (PGXC_EINVAL here).
  */
 int pgxc_xc_gradient(pgxc_ctx* ctx, const double* C, const double* occ,
                      int32_t nbas, int32_t nocc, int32_t ispin, double* grad, double* exc);
@@ -435,6 +435,22 @@ int pgxc_build_sym(pgxc_ctx* ctx, const double* const* C, const double* const* o
                    const int32_t* nocc, int32_t ispin,
                    double* ham_xc_arr, int64_t xc_length,
                    double* exc, double* nel, pgxc_timings* timings);
+
+/*
+ * The XC nuclear gradient of a symmetry-adapted context (pgxc_set_symmetry),
+ * with the irreps' orbitals as pgxc_build_sym takes them.  grad (natoms x 3,
+ * the context's atoms in their C1 order) and *exc are ADDED into, as
+ * pgxc_xc_gradient.  The orbitals are expanded into the C1 basis and the C1
+ * gradient runs on the context's grid.  On the symmetry-reduced grid of the
+ * reference (the points of one equal atom per unique atom, weights times
+ * n_equal_atoms, point_atom that atom) the result is the reference's grad_xc
+ * before post_scf_average_gradient (modules/post_scf_module.f90:1953-1982),
+ * which the caller applies as before; on the full grid it is the gradient
+ * itself.  Replaces the gradient accumulation of post_scf_calc_xc_en_and_gr_nl
+ * (modules/post_scf_module.f90:2940-3013) for symmetric molecules.
+ */
+int pgxc_xc_gradient_sym(pgxc_ctx* ctx, const double* const* C, const double* const* occ,
+                         const int32_t* nocc, int32_t ispin, double* grad, double* exc);
 
 /*
  * Batched builds of many small systems (a set of molecules, each with its own

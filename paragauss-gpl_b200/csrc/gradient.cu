@@ -305,45 +305,52 @@ __global__ void k_grad_host(bool gga, int ispin, int64_t nbas, int64_t ld, int64
   for (int k = 0; k < 3; ++k) atomicAdd(grad + 3 * h + k, t[k]);
 }
 
-// Becke cell function s(mu) = (1 - p(p(p(mu)))) / 2, p(q) = q (3 - q^2) / 2, and ds/dmu
-// Written with round-to-nearest intrinsics (no FMA contraction), so that
-// every call site rounds alike: a factor that is exactly 0 in one pass is 0 in
-// the other, which the leave-one-out products rely on.
-__device__ __forceinline__ void becke_s(double mu, double& s, double& ds) {
-  const double q1 = __dmul_rn(__dmul_rn(0.5, mu), __dsub_rn(3.0, __dmul_rn(mu, mu)));
-  const double q2 = __dmul_rn(__dmul_rn(0.5, q1), __dsub_rn(3.0, __dmul_rn(q1, q1)));
-  const double q3 = __dmul_rn(__dmul_rn(0.5, q2), __dsub_rn(3.0, __dmul_rn(q2, q2)));
-  s = __dmul_rn(0.5, __dsub_rn(1.0, q3));
-  ds = -0.5 * (1.5 * (1.0 - q2 * q2)) * (1.5 * (1.0 - q1 * q1)) * (1.5 * (1.0 - mu * mu));
-}
-
-// Thread per point.  Pass 1 stores, per atom b, the point's distance d_b and
-// the row of P_b = prod_{c != b} s(mu_bc): the product of its nonzero factors,
-// their zero count and the index of a zero factor (scratch [atom][ld]).  Pass
-// 2 gathers, per atom x, the terms of the pairs (x, y) and (y, x) in
-// registers (no scatter):
+// Thread per point.  Pass 1 stores, per atom b, the point's distance d_b,
+// its reciprocal and the row of P_b = prod_{c != b} s(mu_bc): the product of
+// its nonzero factors, their zero count and the index of a zero factor
+// (scratch [atom][ld]).  Pass 2 gathers, per atom x, the terms of the pairs
+// (x, y) and (y, x) in registers (no scatter):
 //   dmu_xy/dR_x = -u_x/R - mu r_xy/R^2,  dmu_yx/dR_x = u_x/R + mu r_xy/R^2,
 //   kappa_xy = c_x L_xy s'(mu_xy), c_b = ef (delta_bh - W_h) / Z,
 // L_xy the product of row x without its factor y; the point moves with its
 // host h, which collects kappa_xy (u_x - u_y)/R of every pair.  Each atom's sum
 // is reduced over the warp and added to shared memory, then to grad.
 //
-// Rows whose leave-one-out products are all negligible ("dead" rows) enter
-// pass 2 only through their pairs with live rows.  Every factor is at most 1,
+// Rows whose leave-one-out products are all negligible ("dead" rows) take
+// part only through their pairs with live rows.  Every factor is at most 1,
 // so L_xy <= the product of row x's factors with the four atoms nearest to the
 // point, leaving out the smallest of them; where that bound is below 2^-60
 // the row is dead (its P_x is below the same bound and is dropped from Z).
+// Both loops of pass 2 run over all atoms in the same order on every lane of
+// a warp; a pair is skipped when, for every lane, both its rows are dead.
 // Where mu <= -0.994, s rounds to exactly 1 and leaves the row product
 // unchanged.
-constexpr int kGradAlive = 32;  // live rows listed per point; more -> every row is visited
+//
+// mu_bc = (d_b - d_c) RN(1/R_bc): pass 1 and pass 2 form it alike, and
+// mu_cb = -mu_bc exactly, so s(mu_cb) = (1 + p3(mu_bc))/2 with the same
+// bits as pass 1's factor (p3 is odd in floating point too): a factor that is
+// exactly 0 in one pass is 0 in the other.
 constexpr double kGradEdge = 0.9941;
 constexpr double kGradTau = 0x1p-60;
 
-__global__ void k_grad_weights(const double* __restrict__ atoms, const double* __restrict__ dist, int natm,
-                               const double* __restrict__ px, const double* __restrict__ py,
-                               const double* __restrict__ pz, const int* __restrict__ owner, int64_t p0,
-                               int64_t nvalid, int64_t ld, const double* __restrict__ ef, double* __restrict__ sd,
-                               double* __restrict__ spnz, int* __restrict__ snz, double* __restrict__ grad) {
+// p3(mu) and ds/dmu (even in mu)
+__device__ __forceinline__ void becke_p3(double mu, double& q3, double& ds) {
+  const double q1 = __dmul_rn(__dmul_rn(0.5, mu), __dsub_rn(3.0, __dmul_rn(mu, mu)));
+  const double q2 = __dmul_rn(__dmul_rn(0.5, q1), __dsub_rn(3.0, __dmul_rn(q1, q1)));
+  q3 = __dmul_rn(__dmul_rn(0.5, q2), __dsub_rn(3.0, __dmul_rn(q2, q2)));
+  ds = -0.5 * (1.5 * (1.0 - q2 * q2)) * (1.5 * (1.0 - q1 * q1)) * (1.5 * (1.0 - mu * mu));
+}
+
+template <bool MASK>
+__global__ void __launch_bounds__(128) k_grad_weights(const double* __restrict__ atoms,
+                                                      const double* __restrict__ dist,
+                                                      const double* __restrict__ rdist, int natm,
+                                                      const double* __restrict__ px, const double* __restrict__ py,
+                                                      const double* __restrict__ pz, const int* __restrict__ owner,
+                                                      int64_t p0, int64_t nvalid, int64_t ld,
+                                                      const double* __restrict__ ef, double* __restrict__ sd,
+                                                      double* __restrict__ sinv, double* __restrict__ spnz,
+                                                      int* __restrict__ snz, double* __restrict__ grad) {
   extern __shared__ double G[];  // 3 natm sums of the block
   for (int i = threadIdx.x; i < 3 * natm; i += blockDim.x) G[i] = 0.0;
   __syncthreads();
@@ -351,8 +358,7 @@ __global__ void k_grad_weights(const double* __restrict__ atoms, const double* _
   const bool live = p < nvalid && ef[p] != 0.0;
   double rv[3] = {0, 0, 0}, e = 0.0, Z = 0.0, Wh = 0.0;
   int h = 0;
-  int alive[kGradAlive];
-  int nalive = 0;  // > kGradAlive: the list overflowed, every row counts as live
+  uint64_t live_lo = 0, live_hi = 0;  // live rows of the point (atoms < 128; MASK)
   if (live) {
     rv[0] = px[p0 + p]; rv[1] = py[p0 + p]; rv[2] = pz[p0 + p];
     h = owner[p0 + p];
@@ -363,6 +369,7 @@ __global__ void k_grad_weights(const double* __restrict__ atoms, const double* _
       const double t0 = rv[0] - atoms[3 * b], t1 = rv[1] - atoms[3 * b + 1], t2 = rv[2] - atoms[3 * b + 2];
       const double r = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
       sd[b * ld + p] = r;
+      sinv[b * ld + p] = r > 0.0 ? 1.0 / r : 0.0;
       if (r < nr[3]) {
         int j = 3;
         for (; j > 0 && nr[j - 1] > r; --j) {
@@ -377,65 +384,53 @@ __global__ void k_grad_weights(const double* __restrict__ atoms, const double* _
     for (int b = 0; b < natm; ++b) {
       const double db = sd[b * ld + p];
       const double* Rb = dist + (int64_t)b * natm;
+      const double* Yb = rdist + (int64_t)b * natm;
+      // bound: the near factors' product with its smallest factor left out
       double Q = 1.0, smin = 1.0;
+      int nzero = 0;
 #pragma unroll
       for (int c = 0; c < 4; ++c) {
         const int k = nb[c];
         if (k < 0 || k == b) continue;
         const double R = Rb[k], d = __dsub_rn(db, nr[c]);
         if (d <= -__dmul_rn(kGradEdge, R)) continue;
-        double s, ds;
-        becke_s(__ddiv_rn(d, R), s, ds);
-        Q *= s;
-        smin = fmin(smin, s);
+        double q3, ds;
+        becke_p3(__dmul_rn(d, Yb[k]), q3, ds);
+        const double sv = __dmul_rn(0.5, __dsub_rn(1.0, q3));
+        if (sv == 0.0) ++nzero;
+        else Q *= sv;
+        smin = fmin(smin, sv);
       }
-      if (smin > 0.0 ? Q / smin < kGradTau : true) {
-        // with smin == 0 the row has a zero factor among the near atoms: its
-        // leave-one-out products are bounded by the product of the other
-        // near factors, recomputed below only if that could matter
-        bool dead = smin > 0.0;
-        if (!dead) {
-          double Qo = 1.0;
-          bool skipped = false;
-#pragma unroll
-          for (int c = 0; c < 4; ++c) {
-            const int k = nb[c];
-            if (k < 0 || k == b) continue;
-            const double R = Rb[k], d = __dsub_rn(db, nr[c]);
-            if (d <= -__dmul_rn(kGradEdge, R)) continue;
-            double s, ds;
-            becke_s(__ddiv_rn(d, R), s, ds);
-            if (s == 0.0 && !skipped) {
-              skipped = true;
-              continue;
-            }
-            Qo *= s;
-          }
-          dead = Qo < kGradTau;
-        }
-        if (dead) {
-          spnz[b * ld + p] = 0.0;
-          snz[b * ld + p] = -2;
-          continue;
-        }
+      // with no zero factor the bound is Q / smin; with one, Q (the others); with more, 0
+      const double bound = nzero == 0 ? (smin > 0.0 ? Q / smin : 0.0) : (nzero == 1 ? Q : 0.0);
+      if (bound < kGradTau) {
+        spnz[b * ld + p] = 0.0;
+        snz[b * ld + p] = -2;
+        continue;
       }
-      double pnz = 1.0;
+      double pnz = 1.0, fmin_row = 1.0;
       int nz = 0, zc = -1;
       for (int c = 0; c < natm; ++c) {
         if (c == b) continue;
         const double R = Rb[c], d = __dsub_rn(db, sd[c * ld + p]);
         if (d <= -__dmul_rn(kGradEdge, R)) continue;  // s == 1 exactly
-        double s, ds;
-        becke_s(__ddiv_rn(d, R), s, ds);
-        if (s == 0.0) { ++nz; zc = c; }
-        else pnz *= s;
+        double q3, ds;
+        becke_p3(__dmul_rn(d, Yb[c]), q3, ds);
+        const double sv = __dmul_rn(0.5, __dsub_rn(1.0, q3));
+        if (sv == 0.0) { ++nz; zc = c; }
+        else { pnz *= sv; fmin_row = fmin(fmin_row, sv); }
+      }
+      // the largest leave-one-out product of the whole row decides: below tau the row is dead
+      const double lmax = nz == 0 ? pnz / fmin_row : (nz == 1 ? pnz : 0.0);
+      if (lmax < kGradTau) {
+        spnz[b * ld + p] = 0.0;
+        snz[b * ld + p] = -2;
+        continue;
       }
       spnz[b * ld + p] = pnz;
-      snz[b * ld + p] = nz == 0 ? -1 : (nz == 1 ? zc : -2);  // -1: no zero; c: the one zero; -2: several
-      if (nz < 2) {
-        if (nalive < kGradAlive) alive[nalive] = b;
-        ++nalive;
-      }
+      snz[b * ld + p] = nz == 0 ? -1 : zc;  // -1: no zero; c: the one zero; -2: dead
+      if (b < 64) live_lo |= 1ull << b;
+      else if (b < 128) live_hi |= 1ull << (b - 64);
       const double P = nz ? 0.0 : pnz;
       Z += P;
       if (b == h) Ph = P;
@@ -443,48 +438,59 @@ __global__ void k_grad_weights(const double* __restrict__ atoms, const double* _
     if (Z > 0.0) Wh = Ph / Z;
   }
   const bool go = live && Z > 0.0;
-  const bool listed = nalive <= kGradAlive;
+  const double iZ = go ? 1.0 / Z : 0.0;
   double gh[3] = {0, 0, 0};
   const int lane = threadIdx.x & 31;
-  // terms of the pair (x, y): adds to gx (atom x) and gh (the host)
-  auto pair_terms = [&](int x, int y, double dx, double cx, double pnx, int zx, const double (&ux)[3],
-                        double (&gx)[3]) {
-    const double R = dist[x * natm + y];
-    const double dy = sd[y * ld + p];
-    const double mu = __ddiv_rn(__dsub_rn(dx, dy), R);
-    double sxy, dsxy, syx, dsyx;
-    becke_s(mu, sxy, dsxy);
-    becke_s(-mu, syx, dsyx);
-    // leave-one-out products of rows x (without y) and y (without x)
-    const double Lxy = zx == -1 ? (sxy != 0.0 ? pnx / sxy : 0.0) : (zx == y ? pnx : 0.0);
-    const int zy = snz[y * ld + p];
-    const double pny = spnz[y * ld + p];
-    const double Lyx = zy == -1 ? (syx != 0.0 ? pny / syx : 0.0) : (zy == x ? pny : 0.0);
-    const double cy = e * ((y == h ? 1.0 : 0.0) - Wh) / Z;
-    const double kxy = cx * Lxy * dsxy, kyx = cy * Lyx * dsyx;
-    if (kxy == 0.0 && kyx == 0.0) return;
-    const double iR = 1.0 / R, iR2 = iR * iR;
-    for (int k = 0; k < 3; ++k) {
-      const double rxy = atoms[3 * x + k] - atoms[3 * y + k];
-      const double uy = dy > 0.0 ? (rv[k] - atoms[3 * y + k]) / dy : 0.0;
-      gx[k] += (kyx - kxy) * (ux[k] * iR + mu * rxy * iR2);
-      gh[k] += kxy * (ux[k] - uy) * iR;
-    }
-  };
   for (int x = 0; x < natm; ++x) {
     double gx[3] = {0, 0, 0};
+    int zx = -2;
+    double dx = 0.0, cx = 0.0, pnx = 0.0, ux[3] = {0, 0, 0};
     if (go) {
-      const double dx = sd[x * ld + p];
-      const double cx = e * ((x == h ? 1.0 : 0.0) - Wh) / Z;
-      const double pnx = spnz[x * ld + p];
-      const int zx = snz[x * ld + p];
-      double ux[3];
-      for (int k = 0; k < 3; ++k) ux[k] = dx > 0.0 ? (rv[k] - atoms[3 * x + k]) / dx : 0.0;
-      if (zx != -2 || !listed) {
-        for (int y = 0; y < natm; ++y)
-          if (y != x) pair_terms(x, y, dx, cx, pnx, zx, ux, gx);
-      } else {  // dead row x: only the pairs with live rows y contribute
-        for (int j = 0; j < nalive; ++j) pair_terms(x, alive[j], dx, cx, pnx, zx, ux, gx);
+      dx = sd[x * ld + p];
+      cx = e * ((x == h ? 1.0 : 0.0) - Wh) * iZ;
+      const double ix = sinv[x * ld + p];
+      for (int k = 0; k < 3; ++k) ux[k] = (rv[k] - atoms[3 * x + k]) * ix;
+      if (!MASK || ((x < 64 ? live_lo >> x : live_hi >> (x - 64)) & 1ull)) {
+        zx = snz[x * ld + p];
+        pnx = spnz[x * ld + p];
+      }
+    }
+    const bool lx = zx != -2;
+    const double* Yx = rdist + (int64_t)x * natm;
+    for (int y = 0; y < natm; ++y) {
+      if (y == x) continue;
+      int zy = -2;
+      bool ly;
+      if (MASK) {
+        ly = ((y < 64 ? live_lo >> y : live_hi >> (y - 64)) & 1ull) != 0;
+      } else {
+        zy = go ? snz[y * ld + p] : -2;
+        ly = zy != -2;
+      }
+      const bool need = go && (lx || ly);
+      if (!__any_sync(0xffffffffu, need)) continue;
+      if (!need) continue;
+      if (MASK && ly) zy = snz[y * ld + p];
+      const double iR = Yx[y];
+      const double dy = sd[y * ld + p];
+      const double mu = __dmul_rn(__dsub_rn(dx, dy), iR);
+      double q3, ds;
+      becke_p3(mu, q3, ds);
+      const double sxy = __dmul_rn(0.5, __dsub_rn(1.0, q3)), syx = __dmul_rn(0.5, __dadd_rn(1.0, q3));
+      // leave-one-out products of rows x (without y) and y (without x)
+      const double Lxy = zx == -1 ? (sxy != 0.0 ? pnx / sxy : 0.0) : (zx == y ? pnx : 0.0);
+      const double pny = spnz[y * ld + p];
+      const double Lyx = zy == -1 ? (syx != 0.0 ? pny / syx : 0.0) : (zy == x ? pny : 0.0);
+      const double cy = e * ((y == h ? 1.0 : 0.0) - Wh) * iZ;
+      const double kxy = cx * Lxy * ds, kyx = cy * Lyx * ds;
+      if (kxy == 0.0 && kyx == 0.0) continue;
+      const double iy = sinv[y * ld + p];
+      const double mr = mu * iR * iR;
+      for (int k = 0; k < 3; ++k) {
+        const double rxy = atoms[3 * x + k] - atoms[3 * y + k];
+        const double uy = (rv[k] - atoms[3 * y + k]) * iy;
+        gx[k] += (kyx - kxy) * (ux[k] * iR + mr * rxy);
+        gh[k] += kxy * (ux[k] - uy) * iR;
       }
     }
     for (int k = 0; k < 3; ++k)
@@ -575,12 +581,22 @@ void launch_grad_weights(const double* atoms, const double* dist, int natm, cons
                          double* scratch, double* grad, cudaStream_t st) {
   if (nvalid <= 0) return;
   const size_t smem = sizeof(double) * 3 * natm;
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_grad_weights, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (smem > 48 * 1024) {
+    cudaFuncSetAttribute(k_grad_weights<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_grad_weights<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  }
+  const double* rdist = dist + (size_t)natm * natm;
   double* sd = scratch;
-  double* spnz = scratch + (size_t)natm * ld;
-  int* snz = (int*)(scratch + (size_t)2 * natm * ld);
-  k_grad_weights<<<(unsigned)((nvalid + 127) / 128), 128, smem, st>>>(atoms, dist, natm, px, py, pz, owner, p0,
-                                                                       nvalid, ld, ef, sd, spnz, snz, grad);
+  double* sinv = scratch + (size_t)natm * ld;
+  double* spnz = scratch + (size_t)2 * natm * ld;
+  int* snz = (int*)(scratch + (size_t)3 * natm * ld);
+  const unsigned nb = (unsigned)((nvalid + 127) / 128);
+  if (natm <= 128)
+    k_grad_weights<true><<<nb, 128, smem, st>>>(atoms, dist, rdist, natm, px, py, pz, owner, p0, nvalid, ld, ef, sd,
+                                                sinv, spnz, snz, grad);
+  else
+    k_grad_weights<false><<<nb, 128, smem, st>>>(atoms, dist, rdist, natm, px, py, pz, owner, p0, nvalid, ld, ef, sd,
+                                                 sinv, spnz, snz, grad);
 }
 
 }  // namespace pgxc

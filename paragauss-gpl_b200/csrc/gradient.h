@@ -44,7 +44,8 @@ void launch_grad_orbital(bool gga, int ispin, int64_t nbas, int64_t ld, int64_t 
                          const double* coef, double* grad, cudaStream_t st);
 
 // The weight term sum_g ef_g dW_host(r_g)/dR over the chunk's points; dist is
-// the natm x natm atom distance matrix, scratch holds 2.5 natm ld doubles.
+// the natm x natm atom distance matrix followed by its reciprocals (the
+// table of launch_becke); scratch holds 3.5 natm ld doubles.
 void launch_grad_weights(const double* atoms, const double* dist, int natm, const double* px, const double* py,
                          const double* pz, const int* owner, int64_t p0, int64_t nvalid, int64_t ld, const double* ef,
                          double* scratch, double* grad, cudaStream_t st);

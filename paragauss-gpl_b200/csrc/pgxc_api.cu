@@ -73,6 +73,8 @@ struct pgxc_ctx {
   ScreenPlan* screen = nullptr; // screened (tile-sparse) build, when screen_threshold >= 0
   SymPlan* sym = nullptr;       // symmetry adaptation, when set
   double* d_eacc = nullptr;     // {E, cE, N, cN} per functional of pgxc_xc_energies
+  void* grad_scr = nullptr;     // scratch of pgxc_xc_gradient, kept across calls (grows only)
+  size_t grad_scr_bytes = 0;
   int eacc_cap = 0;
   int* d_owner = nullptr;       // host atom of each point (raw-weight grids)
   double* d_wraw = nullptr;     // the raw weights of those grids
@@ -181,6 +183,7 @@ void pgxc_destroy(pgxc_ctx* c) {
   if (c->screen) screen_destroy(c->screen);
   delete c->sym;
   for (void* p : c->allocs) cudaFree(p);
+  if (c->grad_scr) cudaFree(c->grad_scr);
   if (c->h_ham) cudaFreeHost(c->h_ham);
   if (c->h_acc) cudaFreeHost(c->h_acc);
   for (auto& e : c->ev)
@@ -891,30 +894,14 @@ int pgxc_build_device(pgxc_ctx* c, const double* d_C, const double* d_occ, int32
 
 // ---------------------------------------------------------------------------
 // Post-SCF XC nuclear gradient (gradient.h): per chunk of points the basis
-// values with Hessians, X = Phi P and Y_j = d_j Phi P (library DGEMMs), the
+// values with Hessians, X = Phi P and Y_j = d_j Phi P (DMMA), the
 // functional's coefficients per point, the orbital terms and the Becke weight
 // term.  FP64, every layout; needs the raw grid (weights_are_raw, point_atom).
+// The orbitals (kpad padded columns) are in the context's C1 buffers.
 // ---------------------------------------------------------------------------
-int pgxc_xc_gradient(pgxc_ctx* c, const double* C, const double* occ, int32_t nbas, int32_t nocc, int32_t ispin,
-                     double* grad, double* exc) {
-  if (!c) return set_err(nullptr, PGXC_EINVAL, "ctx is NULL");
-  int st = check_build_args(c, nbas, nocc, ispin, (int64_t)ispin * nbas * (nbas + 1) / 2);
-  if (st) return st;
-  if (!grad || (nocc > 0 && (!C || !occ))) return set_err(c, PGXC_EINVAL, "NULL output/input");
-  if (!c->d_owner)
-    return set_err(c, PGXC_ENOTSUP, "the XC gradient needs a grid created with raw weights and point_atom "
-                                    "(the grid moves with its atoms)");
-  if (c->sym)
-    return set_err(c, PGXC_ENOTSUP, "the XC gradient is C1 only: a context with pgxc_set_symmetry applied may hold "
-                                    "a symmetry-reduced grid, whose per-atom gradient is not the full one");
-  if (!all_finite(C, (int64_t)nbas * nocc * ispin) || !all_finite(occ, (int64_t)nocc * ispin))
-    return set_err(c, PGXC_ENONFINITE, "non-finite C or occ");
-  CUDA_TRY(c, cudaSetDevice(c->device));
-  if ((st = ensure_occ(c, nocc))) return st;
+static int gradient_core(pgxc_ctx* c, int32_t nbas, int32_t ispin, int64_t kpad, double* grad, double* exc) {
   BuildArgs& a = c->a;
   cudaStream_t s = c->stream;
-  const int64_t kpad = round_up(std::max(nocc, 1), 16);
-  if ((st = upload_orbitals(c, C, occ, nbas, nocc, kpad, cudaMemcpyHostToDevice))) return st;
   launch_pmat_f64(a, kpad, s);
   if (ispin == 2) {
     BuildArgs b = a;
@@ -931,26 +918,38 @@ int pgxc_xc_gradient(pgxc_ctx* c, const double* C, const double* occ, int32_t nb
   int64_t ld = 65536;
   while (ld > 128 && (double)(10 + 4 * ispin) * nbas * ld * 8.0 > 4.0e9) ld /= 2;
   const int64_t plane = (int64_t)nbas * ld;
-  double *basis = nullptr, *XY = nullptr, *coef = nullptr, *ef = nullptr, *dgrad = nullptr, *de = nullptr;
-  double* wscr = nullptr;
-  int* dfatom = nullptr;
-  std::vector<void*> mine;
-  auto scratch = [&](void** p, size_t bytes) -> int {
-    cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 8));
-    if (e != cudaSuccess) return set_err(c, PGXC_ENOMEM, std::string("gradient scratch: ") + cudaGetErrorString(e));
-    mine.push_back(*p);
-    return PGXC_OK;
-  };
-  auto release = [&]() { for (void* p : mine) cudaFree(p); };
-  if ((st = scratch((void**)&basis, sizeof(double) * 10 * plane)) ||
-      (st = scratch((void**)&XY, sizeof(double) * 4 * ispin * plane)) ||
-      (st = scratch((void**)&coef, sizeof(double) * 4 * ispin * ld)) || (st = scratch((void**)&ef, sizeof(double) * ld)) ||
-      (st = scratch((void**)&dgrad, sizeof(double) * 3 * c->natm)) || (st = scratch((void**)&de, sizeof(double))) ||
-      (st = scratch((void**)&wscr, sizeof(double) * ((size_t)5 * c->natm * ld / 2 + 1))) ||
-      (st = scratch((void**)&dfatom, sizeof(int) * nbas))) {
-    release();
-    return st;
+  // one scratch buffer, carved in 256-byte aligned pieces and kept in the
+  // context for the next call (allocation and release of several GB per call
+  // would cost more than the gradient's kernels)
+  const size_t sizes[8] = {sizeof(double) * 10 * plane,         sizeof(double) * 4 * ispin * plane,
+                           sizeof(double) * 4 * ispin * ld,      sizeof(double) * ld,
+                           sizeof(double) * 3 * c->natm,         sizeof(double),
+                           sizeof(double) * ((size_t)7 * c->natm * ld / 2 + 1), sizeof(int) * (size_t)nbas};
+  size_t offs[8], total = 0;
+  for (int i = 0; i < 8; ++i) {
+    offs[i] = total;
+    total += (sizes[i] + 255) / 256 * 256;
   }
+  if (total > c->grad_scr_bytes) {
+    if (c->grad_scr) cudaFree(c->grad_scr);
+    c->grad_scr = nullptr;
+    c->grad_scr_bytes = 0;
+    cudaError_t e = cudaMalloc(&c->grad_scr, total);
+    if (e != cudaSuccess) {
+      c->grad_scr = nullptr;
+      return set_err(c, PGXC_ENOMEM, std::string("gradient scratch: ") + cudaGetErrorString(e));
+    }
+    c->grad_scr_bytes = total;
+  }
+  char* base = (char*)c->grad_scr;
+  double* basis = (double*)(base + offs[0]);
+  double* XY = (double*)(base + offs[1]);
+  double* coef = (double*)(base + offs[2]);
+  double* ef = (double*)(base + offs[3]);
+  double* dgrad = (double*)(base + offs[4]);
+  double* de = (double*)(base + offs[5]);
+  double* wscr = (double*)(base + offs[6]);
+  int* dfatom = (int*)(base + offs[7]);
   const bool gga = PGXC_XC_IS_GGA(c->opt.functional);
   int rc = PGXC_OK;
   do {
@@ -995,8 +994,34 @@ int pgxc_xc_gradient(pgxc_ctx* c, const double* C, const double* occ, int32_t nb
     if (exc) *exc += he;
   } while (false);
   cudaStreamSynchronize(s);
-  release();
   return rc;
+}
+
+static int gradient_checks(pgxc_ctx* c, double* grad) {
+  if (!grad) return set_err(c, PGXC_EINVAL, "NULL output");
+  if (!c->d_owner)
+    return set_err(c, PGXC_ENOTSUP, "the XC gradient needs a grid created with raw weights and point_atom "
+                                    "(the grid moves with its atoms)");
+  return PGXC_OK;
+}
+
+int pgxc_xc_gradient(pgxc_ctx* c, const double* C, const double* occ, int32_t nbas, int32_t nocc, int32_t ispin,
+                     double* grad, double* exc) {
+  if (!c) return set_err(nullptr, PGXC_EINVAL, "ctx is NULL");
+  int st = check_build_args(c, nbas, nocc, ispin, (int64_t)ispin * nbas * (nbas + 1) / 2);
+  if (st) return st;
+  if ((st = gradient_checks(c, grad))) return st;
+  if (nocc > 0 && (!C || !occ)) return set_err(c, PGXC_EINVAL, "NULL input");
+  if (c->sym)
+    return set_err(c, PGXC_EINVAL, "a context with pgxc_set_symmetry applied takes the irreps' orbitals: "
+                                   "pgxc_xc_gradient_sym");
+  if (!all_finite(C, (int64_t)nbas * nocc * ispin) || !all_finite(occ, (int64_t)nocc * ispin))
+    return set_err(c, PGXC_ENONFINITE, "non-finite C or occ");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  if ((st = ensure_occ(c, nocc))) return st;
+  const int64_t kpad = round_up(std::max(nocc, 1), 16);
+  if ((st = upload_orbitals(c, C, occ, nbas, nocc, kpad, cudaMemcpyHostToDevice))) return st;
+  return gradient_core(c, nbas, ispin, kpad, grad, exc);
 }
 
 // ---------------------------------------------------------------------------
@@ -1244,15 +1269,12 @@ int pgxc_set_pseudo2d(pgxc_ctx* c, const int32_t* nblocks, const int32_t* first,
   return PGXC_OK;
 }
 
-int pgxc_build_sym(pgxc_ctx* c, const double* const* C, const double* const* occ, const int32_t* nocc, int32_t ispin,
-                   double* ham, int64_t xc_length, double* exc, double* nel, pgxc_timings* tm) {
-  if (!c) return set_err(nullptr, PGXC_EINVAL, "ctx is NULL");
+// The irreps' orbitals expanded into the C1 orbital buffers of the context
+// (k_sym_orbitals): columns U_ip C_i with occupations occ_i / partners_i per
+// (irrep, partner), both spins; *ntot_out = the number of C1 orbitals.
+static int sym_expand(pgxc_ctx* c, const double* const* C, const double* const* occ, const int32_t* nocc,
+                      int32_t ispin, int64_t* ntot_out) {
   SymPlan* P = c->sym;
-  if (!P) return set_err(c, PGXC_EINVAL, "pgxc_build_sym needs pgxc_set_symmetry first");
-  if (ispin != c->opt.ispin) return set_err(c, PGXC_EINVAL, "ispin does not match the context");
-  if (xc_length != (int64_t)ispin * P->len)
-    return set_err(c, PGXC_EINVAL, "xc_length must be ispin * sum_i dims_i (dims_i + 1) / 2");
-  if (!ham || !exc || !nel || !nocc || !C || !occ) return set_err(c, PGXC_EINVAL, "NULL output/input");
   const int n = P->dev.n_irrep;
   int64_t ntot = 0, csa = 0;
   int nocc_max = 0;
@@ -1299,7 +1321,6 @@ int pgxc_build_sym(pgxc_ctx* c, const double* const* C, const double* const* occ
     }
   BuildArgs& a = c->a;
   cudaStream_t s = c->stream;
-  CUDA_TRY(c, cudaEventRecord(c->ev[0], s));
   if (csa > 0) CUDA_TRY(c, cudaMemcpyAsync(P->d_Csa, hC.data(), sizeof(double) * csa, cudaMemcpyHostToDevice, s));
   CUDA_TRY(c, cudaMemcpyAsync(P->d_cofs, cofs.data(), sizeof(int64_t) * cofs.size(), cudaMemcpyHostToDevice, s));
   CUDA_TRY(c, cudaMemcpyAsync(P->d_nocc, hnocc.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
@@ -1312,6 +1333,48 @@ int pgxc_build_sym(pgxc_ctx* c, const double* const* C, const double* const* occ
     launch_sym_orbitals(P->dev, P->d_Csa, P->d_cofs + (size_t)sp * n, P->d_nocc, P->d_col0, nocc_max, dC, a.ldc, s);
   }
   CUDA_TRY(c, cudaGetLastError());
+  // the host staging vectors must outlive the asynchronous copies
+  CUDA_TRY(c, cudaStreamSynchronize(s));
+  *ntot_out = ntot;
+  return PGXC_OK;
+}
+
+// The XC gradient of a symmetry-adapted context: the irreps' orbitals are
+// expanded into C1 orbitals (the density is then the C1 one) and the C1
+// gradient runs on the context's grid.  On a symmetry-reduced grid (the
+// unique atoms' points, weights times n_equal_atoms, point_atom the first
+// equal atom) this is the reference's grad_xc before post_scf_average_gradient.
+int pgxc_xc_gradient_sym(pgxc_ctx* c, const double* const* C, const double* const* occ, const int32_t* nocc,
+                         int32_t ispin, double* grad, double* exc) {
+  if (!c) return set_err(nullptr, PGXC_EINVAL, "ctx is NULL");
+  if (!c->sym) return set_err(c, PGXC_EINVAL, "pgxc_xc_gradient_sym needs pgxc_set_symmetry first");
+  if (ispin != c->opt.ispin) return set_err(c, PGXC_EINVAL, "ispin does not match the context");
+  if (!nocc || !C || !occ) return set_err(c, PGXC_EINVAL, "NULL input");
+  int st = gradient_checks(c, grad);
+  if (st) return st;
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  int64_t ntot = 0;
+  if ((st = sym_expand(c, C, occ, nocc, ispin, &ntot))) return st;
+  const int64_t kpad = round_up(std::max<int64_t>(ntot, 1), 16);
+  return gradient_core(c, (int32_t)c->nbas, ispin, kpad, grad, exc);
+}
+
+int pgxc_build_sym(pgxc_ctx* c, const double* const* C, const double* const* occ, const int32_t* nocc, int32_t ispin,
+                   double* ham, int64_t xc_length, double* exc, double* nel, pgxc_timings* tm) {
+  if (!c) return set_err(nullptr, PGXC_EINVAL, "ctx is NULL");
+  SymPlan* P = c->sym;
+  if (!P) return set_err(c, PGXC_EINVAL, "pgxc_build_sym needs pgxc_set_symmetry first");
+  if (ispin != c->opt.ispin) return set_err(c, PGXC_EINVAL, "ispin does not match the context");
+  if (xc_length != (int64_t)ispin * P->len)
+    return set_err(c, PGXC_EINVAL, "xc_length must be ispin * sum_i dims_i (dims_i + 1) / 2");
+  if (!ham || !exc || !nel || !nocc || !C || !occ) return set_err(c, PGXC_EINVAL, "NULL output/input");
+  CUDA_TRY(c, cudaSetDevice(c->device));
+  BuildArgs& a = c->a;
+  cudaStream_t s = c->stream;
+  CUDA_TRY(c, cudaEventRecord(c->ev[0], s));
+  int64_t ntot = 0;
+  int st;
+  if ((st = sym_expand(c, C, occ, nocc, ispin, &ntot))) return st;
   CUDA_TRY(c, cudaEventRecord(c->ev[1], s));
   CUDA_TRY(c, cudaEventSynchronize(c->ev[1]));
   float h2d = 0;

@@ -69,6 +69,8 @@ def lib():
     L.pgxc_sym_xc_length.argtypes = [vp, P(ct.c_int64)]
     L.pgxc_build_sym.argtypes = [vp, P(abi._f64p), P(abi._f64p), abi._i32p, ct.c_int32, abi._f64p, ct.c_int64,
                                  P(ct.c_double), P(ct.c_double), P(abi.Timings)]
+    L.pgxc_xc_gradient_sym.argtypes = [vp, P(abi._f64p), P(abi._f64p), abi._i32p, ct.c_int32, abi._f64p,
+                                       P(ct.c_double)]
     _LIB = L
     return L
 
@@ -188,6 +190,16 @@ class Context:
         if timings:
             return ham, exc.value, nel.value, tm.as_dict()
         return ham, exc.value, nel.value
+
+    def xc_gradient_sym(self, Cs, occs):
+        """XC nuclear gradient of a symmetry-adapted context from per-irrep C
+        and occ (as build_sym); returns (grad (natoms, 3), E_xc)."""
+        o = abi.IrrepOrbitals(Cs, occs)
+        g = np.zeros(3 * len(self.case.coords))
+        e = ct.c_double(0.0)
+        _check(lib().pgxc_xc_gradient_sym(self.h, o.pC, o.pocc, abi.i32p(o.nocc), self.case.ispin, abi.f64p(g),
+                                          ct.byref(e)), self.h)
+        return g.reshape(-1, 3), e.value
 
     def build_density(self, P, ham=None):
         """Build from density matrices P (ispin, nbas, nbas); returns (ham_xc_arr, exc, nel)."""

@@ -133,3 +133,65 @@ def test_pseudo2d_rejects_bad_blocks():
         d = ad.dims[0]
         with pytest.raises(lib.PgxcError):
             ctx.set_pseudo2d([1] + [0] * (len(ad.dims) - 1), [0], [d])   # 2 * half > dims
+
+
+@pytest.mark.parametrize("precision,thr", [("fp64", -1.0), ("fp64", 0.0), ("mixed", 1e-10)],
+                         ids=["fp64-dense", "fp64-screened", "int8-screened"])
+@pytest.mark.parametrize("group,xc,ispin", [("C2v", "PBE", 1), ("C3v", "BLYP", 1), ("C2v", "VWN", 2)])
+def test_symmetric_gradient_matches_c1_oracle(group, xc, ispin, precision, thr):
+    """pgxc_xc_gradient_sym against the oracle's C1 gradient of the same
+    density (the irreps' orbitals expanded with U), full raw grid; 1e-10 of
+    the largest component."""
+    if ispin == 2 and thr < 0:
+        pytest.skip("open shell needs the screened layout")
+    case, ad, Cs, occs = Y.symmetric_case(group, functional=xc, ispin=ispin)
+    C, occ = Y.c1_orbitals(ad, Cs, occs)
+    c1 = Y.cases.Case(**{**case.__dict__})
+    c1.C, c1.occ, c1.nocc = C, occ, C.shape[1]
+    ref, re = O.xc_gradient(c1)
+    with lib.Context(case, precision=precision, weighted=False, screen_threshold=thr) as ctx:
+        ctx.set_symmetry(ad)
+        g, e = ctx.xc_gradient_sym(Cs, occs)
+        with pytest.raises(lib.PgxcError):
+            ctx.xc_gradient(C, occ)   # a symmetric context takes the irreps' orbitals
+    scale = float(np.max(np.abs(ref)))
+    assert abs(e - re) < 1e-10 * max(1.0, abs(re))
+    assert float(np.max(np.abs(g - ref))) < 1e-10 * max(scale, 1.0), float(np.max(np.abs(g - ref)))
+
+
+def test_symmetric_gradient_on_reduced_grid_averages_to_full():
+    """On the reference's symmetry-reduced grid the device gradient is
+    grad_xc before post_scf_average_gradient: averaged over the group it
+    equals the device gradient on the full grid, and the oracle's."""
+    from test_symmetry import average_gradient, reduced_raw_grid
+    case, ad, Cs, occs = Y.symmetric_case("C2v", functional="PBE")
+    ops, _ = Y.c2v()
+    red = reduced_raw_grid(case, {0: 1, 1: 2, 3: 2})
+    with lib.Context(case, precision="fp64", weighted=False, screen_threshold=0.0) as ctx:
+        ctx.set_symmetry(ad)
+        g_full, e_full = ctx.xc_gradient_sym(Cs, occs)
+    with lib.Context(red, precision="fp64", weighted=False, screen_threshold=0.0) as ctx:
+        ctx.set_symmetry(ad)
+        g_red, e_red = ctx.xc_gradient_sym(Cs, occs)
+    C, occ = Y.c1_orbitals(ad, Cs, occs)
+    c1 = Y.cases.Case(**{**case.__dict__})
+    c1.C, c1.occ, c1.nocc = C, occ, C.shape[1]
+    ref, _ = O.xc_gradient(c1)
+    assert abs(e_red - e_full) < 1e-10 * abs(e_full)
+    np.testing.assert_allclose(average_gradient(case.coords, ops, g_red), g_full, rtol=0, atol=1e-10)
+    np.testing.assert_allclose(g_full, ref, rtol=0, atol=1e-10)
+
+
+def test_symmetric_gradient_argument_errors():
+    case, ad, Cs, occs = Y.symmetric_case("C2v", functional="VWN")
+    with lib.Context(case, precision="fp64", weighted=False, screen_threshold=0.0) as ctx:
+        with pytest.raises(lib.PgxcError):
+            ctx.xc_gradient_sym(Cs, occs)     # no symmetry set
+        ctx.set_symmetry(ad)
+        with pytest.raises(lib.PgxcError):
+            ctx.xc_gradient_sym(Cs[:-1] + [np.full_like(Cs[-1], np.nan)], occs)
+    O.weight_case(case)
+    with lib.Context(case, precision="fp64", screen_threshold=0.0) as ctx:   # Becke-weighted grid: no gradient
+        ctx.set_symmetry(ad)
+        with pytest.raises(lib.PgxcError):
+            ctx.xc_gradient_sym(Cs, occs)

@@ -101,3 +101,51 @@ def test_symmetry_reduced_grid_equals_full_grid():
     assert len(red.grid_w) < len(full.grid_w)
     assert abs(e1 - e2) < 1e-10 * abs(e1) and abs(n1 - n2) < 1e-10 * n1
     np.testing.assert_allclose(h2, h1, rtol=0, atol=1e-11)
+
+
+def reduced_raw_grid(case, unique):
+    """The reference's symmetry-reduced raw grid: the grids of one atom per
+    class of equal atoms ({atom: n_equal_atoms}), raw weights times
+    n_equal_atoms, each point moving with that atom."""
+    keep = np.isin(case.point_atom, list(unique))
+    red = Y.cases.Case(**{**case.__dict__})
+    red.grid_xyz = case.grid_xyz[keep]
+    red.point_atom = case.point_atom[keep]
+    red.grid_wraw = case.grid_wraw[keep] * np.array([unique[int(a)] for a in red.point_atom])
+    red.grid_w = None
+    return red
+
+
+def average_gradient(coords, ops, g):
+    """post_scf_average_gradient (modules/post_scf_module.f90:1953-1982): the
+    projection of a per-atom gradient on the totally symmetric displacements,
+    (1/|G|) sum_R D(R) g with D(R) moving atom a's vector, rotated, to the
+    atom at R R_a."""
+    out = np.zeros_like(g)
+    for R in ops:
+        moved = coords @ R.T
+        perm = [int(np.argmin(np.linalg.norm(coords - m, axis=1))) for m in moved]
+        for a, b in enumerate(perm):
+            out[b] += R @ g[a]
+    return out / len(ops)
+
+
+def test_reduced_grid_gradient_averages_to_full_grid_gradient():
+    """The reference's symmetric XC gradient: the gradient of the reduced grid
+    (every atom's derivative, points moving with their unique atom) averaged
+    over the group equals the gradient on the full grid, whose atomic grids
+    (Lebedev rules, invariant under the sign changes of x, y, z) are the
+    group's images of the reduced ones.  Oracle only, C1 orbitals of the
+    symmetric density."""
+    case, ad, Cs, occs = Y.symmetric_case("C2v", functional="PBE")
+    C, occ = Y.c1_orbitals(ad, Cs, occs)
+    case.C, case.occ, case.nocc = C, occ, C.shape[1]
+    ops, _ = Y.c2v()
+    g_full, e_full = O.xc_gradient(case)
+    red = reduced_raw_grid(case, {0: 1, 1: 2, 3: 2})
+    g_red, e_red = O.xc_gradient(red)
+    assert len(red.grid_wraw) < len(case.grid_wraw)
+    assert abs(e_red - e_full) < 1e-10 * abs(e_full)
+    assert np.max(np.abs(average_gradient(case.coords, ops, g_full) - g_full)) < 1e-10
+    assert np.max(np.abs(g_red - g_full)) > 1e-6   # the reduced grid alone is not symmetric
+    np.testing.assert_allclose(average_gradient(case.coords, ops, g_red), g_full, rtol=0, atol=1e-10)
