@@ -124,9 +124,20 @@ extern "C" {
  * ("RVWN:Engel" / "RVWN_ENGEL", modules/xc_cntrl.f90:477-498; exchange.f90
  * correlation_lda :124-157, phic0 :159-204) */
 #define PGXC_XC_RVWN_ENGEL 29
+/* TPSS = TPSS exchange (tpss_X, modules/tpss.f90, TPSS_key) + TPSS
+ * correlation (tpss_mgga_C, modules/tpss_mgga_module.f90), a meta-GGA: the
+ * builds also form the kinetic-energy density tau = 1/2 sum occ |grad phi|^2
+ * (density_calc_nl, modules/density_calc_module.f90:1540-1551) and the
+ * potential's tau term 1/2 w df/dtau grad phi_i . grad phi_j
+ * (modules/xc_hamiltonian.f90:1448-1454, :1534-1555); keyword "TPSS",
+ * modules/xc_cntrl.f90:845-850; xc_func.f90:679-697.  Screened layout only
+ * (screen_threshold >= 0). */
+#define PGXC_XC_TPSS 30
 /* the largest functional id */
-#define PGXC_XC_LAST PGXC_XC_RVWN_ENGEL
-/* nonzero for the GGA keywords (all but the five LDAs) */
+#define PGXC_XC_LAST PGXC_XC_TPSS
+/* nonzero for the meta-GGA keywords (density and potential with tau) */
+#define PGXC_XC_IS_MGGA(id) ((id) == PGXC_XC_TPSS)
+/* nonzero for the GGA keywords (all but the five LDAs; the meta-GGAs too) */
 #define PGXC_XC_IS_GGA(id) \
   ((id) != PGXC_XC_VWN && (id) != PGXC_XC_XALPHA && (id) != PGXC_XC_PWLDA && (id) != PGXC_XC_RVWN && \
    (id) != PGXC_XC_RVWN_ENGEL)

@@ -44,6 +44,8 @@ def lib():
     L.oracle_orbitals.argtypes = [P(abi.Geometry), P(abi.Basis), ct.c_int64, abi._f64p, abi._f64p, abi._f64p]
     L.oracle_functionals.argtypes = [ct.c_int32, ct.c_int32, ct.c_int64, abi._f64p, abi._f64p, abi._f64p,
                                      abi._f64p, abi._f64p]
+    L.oracle_functionals_mgga.argtypes = [ct.c_int32, ct.c_int32, ct.c_int64, abi._f64p, abi._f64p, abi._f64p,
+                                          abi._f64p, abi._f64p, abi._f64p, abi._f64p]
     L.oracle_becke.argtypes = [P(abi.Geometry), ct.c_int64, abi._f64p, abi._i32p, abi._f64p, ct.c_int32]
     L.oracle_xc_build.argtypes = [P(abi.Geometry), P(abi.Basis), P(abi.Grid), ct.c_int32, ct.c_int32,
                                   abi._f64p, abi._f64p, ct.c_int32, ct.c_int32, abi._f64p, ct.c_int64,
@@ -96,6 +98,22 @@ def functionals(xc, ispin, rho, gam=None):
                                   abi.f64p(fg))
     assert st == 0, st
     return f, fr.reshape(ispin, n).T, fg.reshape(ng, n).T
+
+
+def functionals_mgga(xc, ispin, rho, gam, tau):
+    """A meta-GGA: rho (n, ispin), gam (n, 2ispin-1), tau (n, ispin) ->
+    f (n), fr (n, ispin), fg (n, 2ispin-1), ft (n, ispin)."""
+    xcid = abi.XC_IDS[xc] if isinstance(xc, str) else xc
+    rho = np.asarray(rho, dtype=np.float64).reshape(len(rho), -1)
+    n = rho.shape[0]
+    ng = 2 * ispin - 1
+    col = lambda a, k: np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(n, k).T).reshape(-1)
+    r, g, t = col(rho, ispin), col(gam, ng), col(tau, ispin)
+    f, fr, fg, ft = np.zeros(n), np.zeros(n * ispin), np.zeros(n * ng), np.zeros(n * ispin)
+    st = lib().oracle_functionals_mgga(xcid, ispin, n, abi.f64p(r), abi.f64p(g), abi.f64p(t), abi.f64p(f),
+                                       abi.f64p(fr), abi.f64p(fg), abi.f64p(ft))
+    assert st == 0, st
+    return f, fr.reshape(ispin, n).T, fg.reshape(ng, n).T, ft.reshape(ispin, n).T
 
 
 def becke(case, nthreads=0):

@@ -30,6 +30,7 @@
 #endif
 
 #include "../include/pgxc.h"
+#include "mgga_oracle.h"
 
 namespace {
 
@@ -1306,6 +1307,7 @@ int oracle_orbitals(const pgxc_geometry* geo, const pgxc_basis* bas, int64_t npt
 int oracle_functionals(int32_t xc, int32_t ispin, int64_t n, const double* rho, const double* gam,
                        double* f, double* fr, double* fg) {
   if (xc < PGXC_XC_VWN || xc > PGXC_XC_LAST || (ispin != 1 && ispin != 2)) return PGXC_EINVAL;
+  if (PGXC_XC_IS_MGGA(xc)) return PGXC_EINVAL;  // needs tau: oracle_functionals_mgga
   const int ng = 2 * ispin - 1;
   for (int64_t i = 0; i < n; ++i) {
     double r[2] = {rho[i], ispin == 2 ? rho[i + n] : 0.0};
@@ -1318,6 +1320,30 @@ int oracle_functionals(int32_t xc, int32_t ispin, int64_t n, const double* rho, 
     for (int s = 0; s < ispin; ++s) fr[i + n * s] = Fr[s];
     if (fg && PGXC_XC_IS_GGA(xc))
       for (int c = 0; c < ng; ++c) fg[i + n * c] = Fg[c];
+  }
+  return PGXC_OK;
+}
+
+// A meta-GGA on n points: rho (n, ispin), gam (n, 2 ispin - 1), tau (n, ispin)
+// column-major; f, fr, fg, ft in the same layouts (xc_functionals with tau,
+// xc_func.f90:187, :679-697).
+int oracle_functionals_mgga(int32_t xc, int32_t ispin, int64_t n, const double* rho, const double* gam,
+                            const double* tau, double* f, double* fr, double* fg, double* ft) {
+  if (!PGXC_XC_IS_MGGA(xc) || (ispin != 1 && ispin != 2)) return PGXC_EINVAL;
+  const int ng = 2 * ispin - 1;
+  for (int64_t i = 0; i < n; ++i) {
+    double r[2] = {rho[i], ispin == 2 ? rho[i + n] : 0.0};
+    double g[3] = {0, 0, 0};
+    for (int c = 0; c < ng; ++c) g[c] = gam[i + n * c];
+    double t[2] = {tau[i], ispin == 2 ? tau[i + n] : 0.0};
+    double F, Fr[2], Fg[3], Ft[2];
+    mgga::tpss_point(ispin, r, g, t, F, Fr, Fg, Ft);
+    f[i] = F;
+    for (int s = 0; s < ispin; ++s) {
+      fr[i + n * s] = Fr[s];
+      ft[i + n * s] = Ft[s];
+    }
+    for (int c = 0; c < ng; ++c) fg[i + n * c] = Fg[c];
   }
   return PGXC_OK;
 }
@@ -1399,6 +1425,7 @@ int oracle_xc_build(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_
   const double* gz = gy + npts;
   const double* gw = gz + npts;
   const bool gga = PGXC_XC_IS_GGA(xc);
+  const bool mgga = PGXC_XC_IS_MGGA(xc);
   const int64_t nbatch = (pt_hi - pt_lo + vla - 1) / vla;
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);
@@ -1423,6 +1450,7 @@ int oracle_xc_build(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_
     if (gga) W.graphi.assign((size_t)vla * 3 * std::max(nocc, 1), 0.0);
     W.help.assign((size_t)vla * nb, 0.0);
     std::vector<double> rho(2 * vla), grarho(6 * vla), gam(3 * vla), fxc(vla), fr(2 * vla), fg(3 * vla);
+    std::vector<double> tau(2 * vla), ft(2 * vla);
 #ifdef _OPENMP
 #pragma omp for schedule(dynamic, 4)
 #endif
@@ -1434,6 +1462,7 @@ int oracle_xc_build(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_
       // density_calc_nl (density_calc_module.f90:1447-1576)
       std::fill(rho.begin(), rho.end(), 0.0);
       std::fill(grarho.begin(), grarho.end(), 0.0);
+      std::fill(tau.begin(), tau.end(), 0.0);
       for (int s = 0; s < ispin; ++s) {
         if (nocc == 0) break;
         const double* Cs = C + (size_t)s * nb * nocc;
@@ -1448,6 +1477,11 @@ int oracle_xc_build(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_
             const double* gj = W.graphi.data() + (size_t)j * 3 * vl;
             for (int c = 0; c < 3; ++c)
               for (int i = 0; i < vl; ++i) grarho[i + vla * (c + 3 * s)] += 2 * pj[i] * gj[c * vl + i] * o;
+            // tau = 1/2 sum_i occ |grad phi_i|^2 (density_calc_module.f90:1540-1551)
+            if (mgga)
+              for (int i = 0; i < vl; ++i)
+                tau[i + vla * s] += (gj[i] * gj[i] + gj[vl + i] * gj[vl + i] + gj[2 * vl + i] * gj[2 * vl + i]) *
+                                    0.5 * o;
           }
         }
       }
@@ -1472,11 +1506,17 @@ int oracle_xc_build(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_
       for (int i = 0; i < vl; ++i) {
         double r[2] = {rho[i], ispin == 2 ? rho[i + vla] : 0.0};
         double g[3] = {gam[i], gam[i + vla], gam[i + 2 * vla]};
-        double F, Fr[2], Fg[3];
-        functional_point(xc, ispin, r, g, F, Fr, Fg);
+        double F, Fr[2], Fg[3], Ft[2] = {0.0, 0.0};
+        if (mgga) {
+          double t[2] = {tau[i], ispin == 2 ? tau[i + vla] : 0.0};
+          mgga::tpss_point(ispin, r, g, t, F, Fr, Fg, Ft);
+        } else {
+          functional_point(xc, ispin, r, g, F, Fr, Fg);
+        }
         fxc[i] = F;
         fr[i] = Fr[0]; fr[i + vla] = Fr[1];
         fg[i] = Fg[0]; fg[i + vla] = Fg[1]; fg[i + 2 * vla] = Fg[2];
+        ft[i] = Ft[0]; ft[i + vla] = Ft[1];
       }
       // exc_int (:949 / :1423)
       for (int i = 0; i < vl; ++i) W.exc += fxc[i] * gw[lo + i];
@@ -1513,6 +1553,19 @@ int oracle_xc_build(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_
         }
         // ham = orbs_help^T * phi (DGEMM 't','n', :1009 / :1528)
         dgemm('t', 'n', nb, nb, vl, 1.0, W.help.data(), vl, W.phi.data(), vl, 1.0, ham, nb);
+        if (mgga) {
+          // tau term (:1448-1454, :1534-1555): per direction, orbs_help = C_SCAL
+          // grad_c phi with C_SCAL = w df/dtau, ham += 1/4 orbs_help^T grad_c phi
+          for (int c = 0; c < 3; ++c) {
+            for (int64_t f = 0; f < nb; ++f) {
+              const double* q = W.grads.data() + (size_t)f * 3 * vl + (size_t)c * vl;
+              double* h = W.help.data() + (size_t)f * vl;
+              for (int i = 0; i < vl; ++i) h[i] = ft[i + vla * s] * gw[lo + i] * q[i];
+            }
+            dgemm('t', 'n', nb, nb, vl, 0.25, W.help.data(), vl, W.grads.data() + (size_t)c * vl, 3 * vl, 1.0, ham,
+                  nb);
+          }
+        }
       }
     }
   }

@@ -918,13 +918,20 @@ static int gradient_core(pgxc_ctx* c, int32_t nbas, int32_t ispin, int64_t kpad,
   int64_t ld = 65536;
   while (ld > 128 && (double)(10 + 4 * ispin) * nbas * ld * 8.0 > 4.0e9) ld /= 2;
   const int64_t plane = (int64_t)nbas * ld;
+  // The weight term needs only each point's w_raw f (ef, kept for the whole
+  // grid: whole chunks of ld, which k_grad_points fills to the end) and runs after the chunk loop in launches of ldw points, as many as
+  // its per-(atom, point) scratch of 3.5 natm ldw doubles allows under ~2 GB:
+  // far more blocks than one basis chunk would give (its per-point loops over
+  // atom pairs are long, and a few blocks per SM leave it latency-bound).
+  int64_t ldw = round_up(c->npts, 128);
+  while (ldw > 128 && 28.0 * c->natm * ldw > 2.0e9) ldw = round_up(ldw / 2, 128);
   // one scratch buffer, carved in 256-byte aligned pieces and kept in the
   // context for the next call (allocation and release of several GB per call
   // would cost more than the gradient's kernels)
   const size_t sizes[8] = {sizeof(double) * 10 * plane,         sizeof(double) * 4 * ispin * plane,
-                           sizeof(double) * 4 * ispin * ld,      sizeof(double) * ld,
+                           sizeof(double) * 4 * ispin * ld,      sizeof(double) * (size_t)round_up(c->npts, ld),
                            sizeof(double) * 3 * c->natm,         sizeof(double),
-                           sizeof(double) * ((size_t)7 * c->natm * ld / 2 + 1), sizeof(int) * (size_t)nbas};
+                           sizeof(double) * ((size_t)7 * c->natm * ldw / 2 + 1), sizeof(int) * (size_t)nbas};
   size_t offs[8], total = 0;
   for (int i = 0; i < 8; ++i) {
     offs[i] = total;
@@ -970,11 +977,17 @@ static int gradient_core(pgxc_ctx* c, int32_t nbas, int32_t ispin, int64_t kpad,
         }
       }
       if (rc) break;
-      launch_grad_points(a.xc, gga, ispin, nbas, ld, p0, nv, a.w, c->d_wraw, basis, plane, XY, coef, ef, de, s);
+      launch_grad_points(a.xc, gga, ispin, nbas, ld, p0, nv, a.w, c->d_wraw, basis, plane, XY, coef, ef + p0, de, s);
       launch_grad_orbital(gga, ispin, nbas, ld, p0, nv, dfatom, c->d_owner, basis, plane, XY, coef, dgrad, s);
-      launch_grad_weights(a.atoms, c->d_dist, c->natm, a.px, a.py, a.pz, c->d_owner, p0, nv, ld, ef, wscr, dgrad, s);
       if (cudaGetLastError() != cudaSuccess) rc = set_err(c, PGXC_ECUDA, "gradient kernel launch failed");
     }
+    if (rc) break;
+    for (int64_t p0 = 0; p0 < c->npts; p0 += ldw) {
+      const int64_t nv = std::min<int64_t>(ldw, c->npts - p0);
+      launch_grad_weights(a.atoms, c->d_dist, c->natm, a.px, a.py, a.pz, c->d_owner, p0, nv, ldw, ef + p0, wscr,
+                          dgrad, s);
+    }
+    if (cudaGetLastError() != cudaSuccess) rc = set_err(c, PGXC_ECUDA, "gradient kernel launch failed");
     if (rc) break;
     std::vector<double> hg((size_t)3 * c->natm);
     double he = 0.0;

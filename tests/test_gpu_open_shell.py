@@ -60,7 +60,7 @@ def _oracle_noise(xc, rho, gam, rf, rfr, rfg, trials=6):
     return nf, nr, ng
 
 
-@pytest.mark.parametrize("xc", list(abi.XC_IDS))
+@pytest.mark.parametrize("xc", list(abi.GGA_LDA_XC))
 def test_point_functionals_open_shell(xc):
     rho, gam = _spin_points(600, 5)
     f, fr, fg = lib.xc_functionals(xc, rho, gam if abi.is_gga(xc) else None)

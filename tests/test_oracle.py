@@ -17,7 +17,7 @@ RHO = np.array([1e-12, 1e-6, 1e-3, 0.05, 0.7, 3.0, 120.0])
 GAM = np.array([1e-20, 1e-9, 1e-5, 0.02, 0.9, 10.0, 5e4])
 
 
-ALL_XC = list(abi.XC_IDS)
+ALL_XC = list(abi.GGA_LDA_XC)
 GGA_XC = [x for x in ALL_XC if abi.is_gga(x)]
 # closed shell, LYP returns the coefficient of gamma_aa as dF/dgamma (lyp.f90):
 # not the gamma derivative of its energy
