@@ -526,6 +526,16 @@ int pgxc_xc_functionals(int32_t functional, int32_t ispin, int64_t n,
                         double* f, double* fr, double* fg);
 
 /*
+ * The same for a meta-GGA (PGXC_XC_IS_MGGA), which also takes the kinetic
+ * energy density: xc_functionals with tau (modules/xc_func.f90:187, :679-697).
+ *   tau : (n, ispin); ft : (n, ispin) = df/dtau
+ * pgxc_xc_functionals rejects the meta-GGA ids (PGXC_EINVAL).
+ */
+int pgxc_xc_functionals_mgga(int32_t functional, int32_t ispin, int64_t n, const double* rho,
+                             const double* gam, const double* tau, double* f, double* fr,
+                             double* fg, double* ft);
+
+/*
  * Becke partition weights on the device; replaces atomicweight2/becke0
  * (modules/grid_module.f90:2264-2497, autodiff/becke_step_func.f90:84-124)
  * with art = 0 (WEIGHT_GRADS default, :371-372).

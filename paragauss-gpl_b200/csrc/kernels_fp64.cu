@@ -328,6 +328,10 @@ __global__ void __launch_bounds__(256) k_functional2(XcConst K, int64_t p0, int6
   }
 }
 
+void launch_sum_partials(const double* partial, int nblocks, double* acc, cudaStream_t st) {
+  k_sum_partials<<<1, 256, 0, st>>>(partial, nblocks, acc);
+}
+
 void launch_functional2_f64(const XcConst& K, const double* w, double* pa, double* pb, int64_t ld, int64_t p0,
                             int64_t nvalid, bool gga, double* partial, double* acc, cudaStream_t st) {
   const unsigned nb = (unsigned)((ld + 255) / 256);

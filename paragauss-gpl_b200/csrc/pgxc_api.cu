@@ -334,6 +334,8 @@ int create_impl(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
   if (o.ispin != 1 && o.ispin != 2) return fail(set_err(c, PGXC_EINVAL, "ispin must be 1 or 2"));
   if (o.ispin == 2 && !(o.screen_threshold >= 0.0))
     return fail(set_err(c, PGXC_ENOTSUP, "open-shell (ispin=2) builds need the screened layout (screen_threshold >= 0)"));
+  if (PGXC_XC_IS_MGGA(o.functional) && !(o.screen_threshold >= 0.0))
+    return fail(set_err(c, PGXC_ENOTSUP, "meta-GGA builds need the screened layout (screen_threshold >= 0)"));
   if (o.precision != PGXC_PREC_FP64 && o.precision != PGXC_PREC_MIXED_INT8)
     return fail(set_err(c, PGXC_EINVAL, "unknown precision mode"));
   std::vector<int64_t> spec_off;
@@ -506,6 +508,7 @@ int create_impl(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
     in.ispin = o.ispin;
     in.precision = o.precision;
     in.keep_basis = o.keep_orbitals != 0;
+    in.mgga = PGXC_XC_IS_MGGA(o.functional);
     in.max_chunk_points = o.max_chunk_points;
     std::string e;
     st = screen_create(&c->screen, in, a, c->stream, e);
@@ -1012,6 +1015,8 @@ static int gradient_core(pgxc_ctx* c, int32_t nbas, int32_t ispin, int64_t kpad,
 
 static int gradient_checks(pgxc_ctx* c, double* grad) {
   if (!grad) return set_err(c, PGXC_EINVAL, "NULL output");
+  if (PGXC_XC_IS_MGGA(c->opt.functional))
+    return set_err(c, PGXC_ENOTSUP, "the XC gradient of a meta-GGA is not supported");
   if (!c->d_owner)
     return set_err(c, PGXC_ENOTSUP, "the XC gradient needs a grid created with raw weights and point_atom "
                                     "(the grid moves with its atoms)");
@@ -1056,6 +1061,7 @@ int pgxc_xc_energies(pgxc_ctx* c, const double* C, const double* occ, int32_t nb
   for (int i = 0; i < n; ++i) {
     const int f = functionals[i];
     if (f < PGXC_XC_VWN || f > PGXC_XC_LAST) return set_err(c, PGXC_EINVAL, "functional id out of range");
+    if (PGXC_XC_IS_MGGA(f)) return set_err(c, PGXC_ENOTSUP, "pgxc_xc_energies: meta-GGA energies are not supported");
     if (PGXC_XC_IS_GGA(f) && !gga)
       return set_err(c, PGXC_EINVAL, "a GGA energy needs a context created with a GGA functional (no grad rho)");
     xcs[i] = make_xc_const(f);
@@ -1693,9 +1699,40 @@ int pgxc_orbital_calculate(pgxc_ctx* c, int64_t npts, const double* pts, double*
   return st;
 }
 
+int pgxc_xc_functionals_mgga(int32_t functional, int32_t ispin, int64_t n, const double* rho, const double* gam,
+                             const double* tau, double* f, double* fr, double* fg, double* ft) {
+  if (!PGXC_XC_IS_MGGA(functional)) return set_err(nullptr, PGXC_EINVAL, "not a meta-GGA functional id");
+  if (ispin != 1 && ispin != 2) return set_err(nullptr, PGXC_EINVAL, "ispin must be 1 or 2");
+  if (n < 0 || !rho || !gam || !tau || !f || !fr || !fg || !ft) return set_err(nullptr, PGXC_EINVAL, "bad arguments");
+  if (n == 0) return PGXC_OK;
+  int st = check_device(nullptr, -1);
+  if (st) return st;
+  const int64_t ng = 2 * ispin - 1;
+  const int64_t cols = 2 * (2 * ispin + ng) + 1;  // in: rho, gam, tau; out: f, fr, fg, ft
+  double* d;
+  if (cudaMalloc(&d, sizeof(double) * cols * n) != cudaSuccess) return set_err(nullptr, PGXC_ENOMEM, "cudaMalloc");
+  double *drho = d, *dgam = drho + ispin * n, *dtau = dgam + ng * n, *df = dtau + ispin * n, *dfr = df + n,
+         *dfg = dfr + ispin * n, *dft = dfg + ng * n;
+  cudaError_t e = cudaMemcpy(drho, rho, sizeof(double) * ispin * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dgam, gam, sizeof(double) * ng * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dtau, tau, sizeof(double) * ispin * n, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    launch_xc_points_mgga(ispin, n, drho, dgam, dtau, df, dfr, dfg, dft, 0);
+    e = cudaDeviceSynchronize();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(f, df, sizeof(double) * n, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(fr, dfr, sizeof(double) * ispin * n, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(fg, dfg, sizeof(double) * ng * n, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(ft, dft, sizeof(double) * ispin * n, cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return set_err(nullptr, PGXC_ECUDA, cudaGetErrorString(e));
+  return PGXC_OK;
+}
+
 int pgxc_xc_functionals(int32_t functional, int32_t ispin, int64_t n, const double* rho, const double* gam, double* f,
                         double* fr, double* fg) {
   if (functional < PGXC_XC_VWN || functional > PGXC_XC_LAST) return set_err(nullptr, PGXC_EINVAL, "functional");
+  if (PGXC_XC_IS_MGGA(functional)) return set_err(nullptr, PGXC_EINVAL, "a meta-GGA needs tau: pgxc_xc_functionals_mgga");
   if (ispin != 1 && ispin != 2) return set_err(nullptr, PGXC_EINVAL, "ispin must be 1 or 2");
   if (n < 0 || !rho || !f || !fr) return set_err(nullptr, PGXC_EINVAL, "bad arguments");
   const bool gga = PGXC_XC_IS_GGA(functional);

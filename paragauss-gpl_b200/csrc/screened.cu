@@ -433,6 +433,7 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
   *out = nullptr;
   ScreenPlan* sp = new ScreenPlan();
   sp->gga = in.gga;
+  sp->mgga = in.mgga;
   sp->ispin = in.ispin;
   sp->nbas = in.nbas;
   sp->keep = in.keep_basis;
@@ -652,6 +653,11 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
   }
   const int64_t cp = sp->chunk_tiles * 128;
   SP_TRY(sp_alloc(sp, &sp->pt, 8 * (size_t)in.ispin * cp), "cudaMalloc");
+  SP_TRY(cudaMemset(sp->pt, 0, sizeof(double) * 8 * in.ispin * cp), "memset");
+  if (in.mgga) {
+    SP_TRY(sp_alloc(sp, &sp->tq, 4 * (size_t)in.ispin * cp), "cudaMalloc");
+    SP_TRY(cudaMemset(sp->tq, 0, sizeof(double) * 4 * in.ispin * cp), "memset");
+  }
   SP_TRY(sp_alloc(sp, &sp->partial, 2 * (size_t)((cp + 255) / 256) + 2), "cudaMalloc");
   SP_TRY(sp_alloc(sp, &sp->V, (size_t)in.ispin * in.nbas * in.nbas), "cudaMalloc (V)");
   if (mixed) {
@@ -794,10 +800,25 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
         }
         ++T.launches;
       }
+      if (sp->mgga) {
+        // 2 tau_j = sum_nu (d_j phi P)_nu d_j phi_nu: the density contraction with d_j phi in the
+        // place of phi (FP64 DMMA in every precision mode)
+        const int smem = gemm_smem_bytes<false, false>() + (int)sizeof(int) * sp->max_n;
+        raise_smem_limit(k_sdensity<false>, smem);
+        const double* gj[3] = {gxc, gyc, gzc};
+        for (int j = 0; j < 3; ++j) {
+          k_sdensity<false><<<dim3((unsigned)nt, 2), kGemmThreads, smem, st>>>(
+              gj[j], nullptr, nullptr, nullptr, sp->tso, t0, s0, sp->slot_fn, P[s], a.ldc,
+              sp->tq + (4 * s + j) * cp, nullptr, nullptr, nullptr);
+          ++T.launches;
+        }
+      }
     }
     if (timed) SR_TRY(cudaEventRecord(ev[5], st));
     // K2
-    if (ispin == 1) {
+    if (sp->mgga) {
+      launch_functional_mgga(ispin, sp->qw, sp->pt, sp->tq, cp, t0 * 128, npt, sp->partial, a.acc, st);
+    } else if (ispin == 1) {
       BuildArgs bf = b[0];
       bf.w = sp->qw;
       launch_functional_f64(bf, t0 * 128, npt, gga, st);
@@ -836,6 +857,22 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
         }
         if (timed) SR_TRY(cudaEventRecord(k1, st));
         T.launches += 2;
+      }
+      if (sp->mgga) {
+        // tau term: per direction Z = C d_j phi and H += Z^T d_j phi over the whole square of
+        // each tile (k_spack then forms H + H^T), FP64 DMMA in every precision mode
+        const unsigned nbk = (unsigned)std::max<int64_t>(1, std::min<int64_t>((ns * 128 + 255) / 256, 148 * 32));
+        const int smem = gemm_smem_bytes<true, true>() + (int)sizeof(int) * sp->max_n;
+        raise_smem_limit(k_svpot<true>, smem);
+        const double* gj[3] = {gxc, gyc, gzc};
+        const double* Cs = sp->tq + (4 * s + 3) * cp;
+        for (int j = 0; j < 3; ++j) {
+          k_szbuild<false><<<nbk, 256, 0, st>>>(ns, sp->slot_tile + s0, t0, gj[j], nullptr, nullptr, nullptr, Cs,
+                                                nullptr, nullptr, nullptr, sp->Z);
+          k_svpot<true><<<dim3((unsigned)nt, 4), kGemmThreads, smem, st>>>(gj[j], sp->Z, sp->tso, t0, s0,
+                                                                            sp->slot_fn, Vs, sp->nbas);
+          T.launches += 2;
+        }
       }
     }
     // further functionals on the same density (after K4, whose A and B they overwrite)
@@ -1353,6 +1390,6 @@ int screen_set_prepare_member(ScreenPlan* sp, const double* P, int64_t ldc, cuda
   return cudaGetLastError() == cudaSuccess ? PGXC_OK : PGXC_ECUDA;
 }
 
-bool screen_set_eligible(const ScreenPlan* sp) { return sp->mixed && sp->ispin == 1 && !sp->keep; }
+bool screen_set_eligible(const ScreenPlan* sp) { return sp->mixed && sp->ispin == 1 && !sp->keep && !sp->mgga; }
 
 }  // namespace pgxc

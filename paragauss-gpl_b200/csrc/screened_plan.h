@@ -43,6 +43,8 @@ struct ScreenPlan {
   // device, per chunk
   double *phi = nullptr, *gx = nullptr, *gy = nullptr, *gz = nullptr, *Z = nullptr;
   double* pt = nullptr;      // 8 point arrays of chunk_tiles*128 per spin
+  bool mgga = false;
+  double* tq = nullptr;      // meta-GGA: 4 point arrays per spin (2 tau_x, 2 tau_y, 2 tau_z, C)
   double* partial = nullptr;
   double* V = nullptr;       // [ispin][nbas][nbas]
   unsigned long long* pmax = nullptr;  // [chunk_tiles*128] largest |phi| per point (INT8 path)

@@ -8,7 +8,7 @@ PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "libpgxc.so")
 SOURCES = ["pgxc_api.cu", "kernels_fp64.cu", "kernels_aux.cu", "mixed.cu", "noalloc.cu", "screened.cu",
-           "screened_mixed.cu", "symmetry.cu", "gradient.cu", "grid.cu"]
+           "screened_mixed.cu", "symmetry.cu", "gradient.cu", "grid.cu", "mgga.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
               "-Xcompiler", "-fPIC"]
 OBJDIR = os.path.join(PKG, "_build")

@@ -45,6 +45,8 @@ def lib():
                                      P(ct.c_double), P(abi.Timings)]
     L.pgxc_grid_weights.argtypes = [vp, abi._f64p, ct.c_int64]
     L.pgxc_orbital_calculate.argtypes = [vp, ct.c_int64, abi._f64p, abi._f64p, abi._f64p]
+    L.pgxc_xc_functionals_mgga.argtypes = [ct.c_int32, ct.c_int32, ct.c_int64, abi._f64p, abi._f64p, abi._f64p,
+                                           abi._f64p, abi._f64p, abi._f64p, abi._f64p]
     L.pgxc_xc_functionals.argtypes = [ct.c_int32, ct.c_int32, ct.c_int64, abi._f64p, abi._f64p, abi._f64p,
                                       abi._f64p, abi._f64p]
     L.pgxc_becke_weights.argtypes = [P(abi.Geometry), ct.c_int64, abi._f64p, abi._i32p, abi._f64p]
@@ -340,3 +342,20 @@ def becke_weights(case):
     w = np.zeros(case.npts)
     _check(lib().pgxc_becke_weights(ct.byref(m.geometry), case.npts, abi.f64p(pts), abi.i32p(owner), abi.f64p(w)))
     return w
+
+
+def xc_functionals_mgga(xc, rho, gam, tau):
+    """Meta-GGA point functional on the device: rho, gam, tau as the oracle's
+    functionals_mgga ((n, ispin), (n, 2 ispin - 1), (n, ispin)) -> f (n,),
+    fr (n, ispin), fg (n, 2 ispin - 1), ft (n, ispin)."""
+    rho = np.asarray(rho, dtype=np.float64)
+    n = rho.shape[0]
+    rho = rho.reshape(n, -1)
+    ispin = rho.shape[1]
+    ng = 2 * ispin - 1
+    col = lambda a, k: np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(n, k).T).reshape(-1)
+    r, g, t = col(rho, ispin), col(gam, ng), col(tau, ispin)
+    f, fr, fg, ft = np.zeros(n), np.zeros(n * ispin), np.zeros(n * ng), np.zeros(n * ispin)
+    _check(lib().pgxc_xc_functionals_mgga(abi.XC_IDS[xc], ispin, n, abi.f64p(r), abi.f64p(g), abi.f64p(t),
+                                          abi.f64p(f), abi.f64p(fr), abi.f64p(fg), abi.f64p(ft)))
+    return f, fr.reshape(ispin, n).T, fg.reshape(ng, n).T, ft.reshape(ispin, n).T

@@ -1,0 +1,105 @@
+"""TPSS (meta-GGA) on the device against the oracle: the point functional
+with tau, and whole builds with the kinetic-energy density in the density
+step and the tau term in the potential (screened layout, FP64 and INT8,
+closed and open shell).  Bars 1e-10 (FP64) and 1e-7 (INT8) as for the other
+keywords."""
+import numpy as np
+import pytest
+
+import oracle as O
+from pgxc import cases, lib
+
+pytestmark = pytest.mark.gpu
+
+CT = 0.3 * (3 * np.pi ** 2) ** (2.0 / 3.0)
+
+
+def _points(rng, n, ispin):
+    rho = 10.0 ** rng.uniform(-10, 3, size=(n, ispin))
+    s = 10.0 ** rng.uniform(-3, 1, size=(n, ispin))
+    kf = (3 * np.pi ** 2 * rho * ispin) ** (1 / 3)
+    gs = (2 * kf * s * rho) ** 2 / ispin
+    tau = np.maximum(gs / (8 * rho), CT * (ispin * rho) ** (5 / 3) / ispin) * 10.0 ** rng.uniform(0, 1, size=(n, ispin))
+    if ispin == 2:
+        gab = np.sqrt(gs[:, 0] * gs[:, 1]) * rng.uniform(-1, 1, size=n)
+        gs = np.column_stack([gs[:, 0], gs[:, 1], gab])
+        rho[:8, 1] = 0.0   # one spin empty
+        gs[:8, 1:] = 0.0
+        tau[:8, 1] = 0.0
+    rho[0] = 0.0
+    return rho, gs, tau
+
+
+@pytest.mark.parametrize("ispin", [1, 2])
+def test_tpss_points_match_oracle(ispin):
+    rng = np.random.default_rng(20 + ispin)
+    rho, gam, tau = _points(rng, 400, ispin)
+    f, fr, fg, ft = lib.xc_functionals_mgga("TPSS", rho, gam, tau)
+    rf, rfr, rfg, rft = O.functionals_mgga("TPSS", ispin, rho, gam, tau)
+    # relative to the size of the Slater term at each point (the pieces have mixed signs)
+    n = rho.sum(1)
+    sl = 0.75 * (3 / np.pi) ** (1 / 3) * n ** (4 / 3)
+    assert np.all(np.abs(f - rf) <= 1e-11 * (np.abs(rf) + sl) + 1e-300)
+    for a, b in ((fr, rfr), (fg, rfg), (ft, rft)):
+        assert np.all(np.abs(a - b) <= 1e-9 * np.abs(b) + 1e-11 * np.max(np.abs(b), axis=0, keepdims=True) + 1e-300)
+
+
+def _build(c, **kw):
+    with lib.Context(c, **kw) as ctx:
+        return ctx.build()
+
+
+BUILDS = pytest.mark.parametrize("precision,thr,tol", [("fp64", 0.0, 1e-10), ("fp64", 1e-10, 1e-10),
+                                                       ("mixed", 1e-10, 1e-7)],
+                                 ids=["fp64-exact", "fp64-screened", "int8-screened"])
+
+
+@BUILDS
+@pytest.mark.parametrize("seed,lmax", [(41, 2), (42, 3)])
+def test_tpss_build_matches_oracle(seed, lmax, precision, thr, tol):
+    c = cases.small_case(functional="TPSS", seed=seed, lmax=lmax)
+    O.weight_case(c)
+    ref, re, rn = O.xc_build(c)
+    ham, e, n = _build(c, precision=precision, screen_threshold=thr, max_chunk_points=1024)
+    print(f"TPSS {precision} {thr}: |dE|={abs(e - re):.2e} |dN|={abs(n - rn):.2e} max|dV|={np.max(np.abs(ham - ref)):.2e}")
+    assert abs(e - re) < tol and abs(n - rn) < tol
+    assert float(np.max(np.abs(ham - ref))) < tol
+
+
+@BUILDS
+def test_tpss_open_shell_build_matches_oracle(precision, thr, tol):
+    c = cases.small_case(functional="TPSS", seed=43, natoms=5, nocc=7, ispin=2)
+    O.weight_case(c)
+    ref, re, rn = O.xc_build(c)
+    ham, e, n = _build(c, precision=precision, screen_threshold=thr, max_chunk_points=1024)
+    assert abs(e - re) < tol and abs(n - rn) < tol
+    assert float(np.max(np.abs(ham - ref))) < tol
+
+
+def test_tpss_equal_spins_reproduce_closed_shell():
+    c = cases.small_case(functional="TPSS", seed=44)
+    O.weight_case(c)
+    h1, e1, n1 = _build(c, screen_threshold=0.0)
+    c.ispin = 2
+    c.C = np.concatenate([c.C, c.C], axis=2)
+    c.occ = np.ones((c.nocc, 2))
+    h2, e2, n2 = _build(c, screen_threshold=0.0)
+    assert abs(e1 - e2) < 1e-11 and abs(n1 - n2) < 1e-11
+    np.testing.assert_allclose(h2[0::2], h1, atol=1e-11)
+    np.testing.assert_allclose(h2[1::2], h1, atol=1e-11)
+
+
+def test_tpss_rejections():
+    c = cases.small_case(functional="TPSS", seed=45)
+    O.weight_case(c)
+    with pytest.raises(lib.PgxcError):
+        lib.Context(c, screen_threshold=-1.0)          # dense layout: no tau path
+    with pytest.raises(lib.PgxcError):
+        lib.xc_functionals("TPSS", np.ones(3), np.ones(3))   # needs tau
+    with lib.Context(c, screen_threshold=0.0) as ctx:
+        with pytest.raises(lib.PgxcError):
+            ctx.xc_energies(["TPSS"])
+    d = cases.small_case(functional="TPSS", seed=46)
+    with lib.Context(d, weighted=False, screen_threshold=0.0) as ctx:
+        with pytest.raises(lib.PgxcError):
+            ctx.xc_gradient()
