@@ -133,10 +133,25 @@ extern "C" {
  * modules/xc_cntrl.f90:845-850; xc_func.f90:679-697.  Screened layout only
  * (screen_threshold >= 0). */
 #define PGXC_XC_TPSS 30
+/* M06L = M06-L exchange (m06_X, parameter set 1: e_x^LSDA F_PBE f(w) plus the
+ * VSXC-form term) + M06-L correlation (m06_C: the VSXC-form same- and
+ * opposite-spin terms plus the B97-form series), modules/m06.f90; keyword
+ * "M06L", modules/xc_cntrl.f90:885-890; xc_func.f90:647-661.  A meta-GGA. */
+#define PGXC_XC_M06L 31
+/* M06 = the grid part of the hybrid M06 (m06_X and m06_C with parameter set
+ * 2; the 0.27 exact exchange is not a grid term), keyword "M06",
+ * modules/xc_cntrl.f90:892-898; xc_func.f90:663-677.  A meta-GGA. */
+#define PGXC_XC_M06 32
+/* VSXC = vsxc_X + vsxc_C (Van Voorhis-Scuseria, parameter set 0),
+ * modules/vsxc_mgga_module.f90; keyword "VSXC" / "VS98",
+ * modules/xc_cntrl.f90:952-957; xc_func.f90:776-790.  A meta-GGA.  The
+ * closed-shell derivatives are the reference's: half those of the
+ * open-shell form at equal spins (vsxc_X, vsxc_C). */
+#define PGXC_XC_VSXC 33
 /* the largest functional id */
-#define PGXC_XC_LAST PGXC_XC_TPSS
+#define PGXC_XC_LAST PGXC_XC_VSXC
 /* nonzero for the meta-GGA keywords (density and potential with tau) */
-#define PGXC_XC_IS_MGGA(id) ((id) == PGXC_XC_TPSS)
+#define PGXC_XC_IS_MGGA(id) ((id) >= PGXC_XC_TPSS && (id) <= PGXC_XC_VSXC)
 /* nonzero for the GGA keywords (all but the five LDAs; the meta-GGAs too) */
 #define PGXC_XC_IS_GGA(id) \
   ((id) != PGXC_XC_VWN && (id) != PGXC_XC_XALPHA && (id) != PGXC_XC_PWLDA && (id) != PGXC_XC_RVWN && \

@@ -268,25 +268,183 @@ DN<N> tpss_c(const DN<N>& ra, const DN<N>& rb, const DN<N>& gaa, const DN<N>& gb
   return sumrho * etp;
 }
 
-// TPSS at one point: f and its derivatives in the reference's layout
-// (ispin 1: rho, gamma, tau of the total density; ispin 2: rho_a, rho_b;
-// gamma_aa, gamma_bb, gamma_ab; tau_a, tau_b).
-inline void tpss_point(int ispin, const double* rho, const double* gam, const double* tau, double& f, double* fr,
-                       double* fg, double* ft) {
+// ---------------------------------------------------------------------------
+// VSXC and the Minnesota M06 family: modules/vsxc_mgga_module.f90 (vsxc_X
+// :90-173, vsxc_C :177-260, vsxc_exchange :264-425, vsxc_correlation
+// :429-722, eX_lsda :726-762, Dsic_term :766-850, gvt4_term :854-975) and
+// modules/m06.f90 (m06_X :85-156, m06_C :160-231, m06_exchange :235-563 with
+// pbeef and kedef, m06_correlation :567-821, bmk_term :825-906).  Parameter
+// set 0 is VSXC, 1 M06-L, 2 M06 (the grid part of the hybrid).
+// ---------------------------------------------------------------------------
+const double VS_DTOL = 1.0e-30;
+const double VS_CF = 9.11559974469119;
+
+// gvt4_term's h(x^2, z) = d0/g + (d1 x^2 + d2 z)/g^2 + (d3 x^4 + d4 x^2 z + d5 z^2)/g^3, g = 1 + alpha (x^2 + z)
+template <int N>
+DN<N> gvt4(double alpha, const double* d, const DN<N>& x2, const DN<N>& z) {
+  const DN<N> g = 1.0 + alpha * (x2 + z);
+  const DN<N> g2 = g * g;
+  return d[0] / g + (d[1] * x2 + d[2] * z) / g2 + (d[3] * x2 * x2 + d[4] * x2 * z + d[5] * z * z) / (g2 * g);
+}
+// x_s^2 = gamma_ss / rho_s^(8/3) and z_s = 2 tau_s / rho_s^(5/3) - CF; zero below 1e-30
+template <int N>
+DN<N> vs_x2(const DN<N>& r, const DN<N>& g) {
+  return r.v >= VS_DTOL ? g / dpow(r, 8.0 / 3.0) : cst<N>(0.0);
+}
+template <int N>
+DN<N> vs_z(const DN<N>& r, const DN<N>& t) {
+  return r.v >= VS_DTOL ? 2.0 * t / dpow(r, 5.0 / 3.0) - VS_CF : cst<N>(0.0);
+}
+// Dsic_term: 1 - x^2 / (4 (z + CF)) where rho and tau are above 1e-30, clipped at 0
+template <int N>
+DN<N> vs_dsic(const DN<N>& r, const DN<N>& g, const DN<N>& t) {
+  if (!(r.v >= VS_DTOL && t.v >= VS_DTOL)) return cst<N>(0.0);
+  const DN<N> x2 = g / dpow(r, 8.0 / 3.0);
+  const DN<N> z = 2.0 * t / dpow(r, 5.0 / 3.0) - VS_CF;
+  const DN<N> D = 1.0 - x2 / (4.0 * (z + VS_CF));
+  return D.v < 0.0 ? cst<N>(0.0) : D;
+}
+// eX_lsda of the vsxc module
+template <int N>
+DN<N> vs_ex(const DN<N>& r) {
+  return r.v >= VS_DTOL ? -0.930525736349100 * dpow(r, 4.0 / 3.0) : cst<N>(0.0);
+}
+
+inline const double* vsxc_dx(int set) {  // get_pars_vsxc_exchange
+  static const double p[3][6] = {
+      {1.05324147599106640E+00, 3.82234242542822070E-03, -6.71698348131996321E-03, 2.53030938105796706E-05,
+       1.37850244210630278E-04, -3.84172286736070984E-04},
+      {6.012244E-01, 4.748822E-03, -8.635108E-03, -9.308062E-06, 4.482811E-05, 0.0},
+      {1.422057E-01, 7.370319E-04, -1.601373E-02, 0.0, 0.0, 0.0}};
+  return p[set];
+}
+inline const double* vsxc_dc(int set, int term) {  // get_pars_vsxc_correlation: term 1 same spin, 2 opposite
+  static const double p[3][2][6] = {
+      {{3.270912E-01, -3.228915E-02, -2.942406E-02, 2.134222E-03, -5.451559E-03, 1.577575E-02},
+       {7.035010E-01, 7.694574E-03, 5.152765E-02, 3.394308E-05, -1.269420E-03, 1.296118E-03}},
+      {{4.650534E-01, 1.617589E-01, 1.833657E-01, 4.692100E-04, -4.990573E-03, 0.0},
+       {3.957626E-01, -5.614546E-01, 1.403963E-02, 9.831442E-04, -3.577176E-03, 0.0}},
+      {{4.905945E-01, -1.437348E-01, 2.357824E-01, 1.871015E-03, -3.788963E-03, 0.0},
+       {-2.741539E+00, -6.720113E-01, -7.932688E-02, 1.918681E-03, -2.032902E-03, 0.0}}};
+  return p[set][term - 1];
+}
+
+// vsxc_exchange of one spin: e_x^LSDA h(x_s^2, z_s), alpha = 0.00186726
+template <int N>
+DN<N> vsxc_x_spin(int set, const DN<N>& r, const DN<N>& g, const DN<N>& t) {
+  return vs_ex(r) * gvt4(0.00186726, vsxc_dx(set), vs_x2(r, g), vs_z(r, t));
+}
+
+// vsxc_correlation (spin-resolved input): same-spin terms e_s h_ss D_s and the
+// opposite-spin term (e_c(a, b) - e_c(a, 0) - e_c(0, b)) h_os with summed
+// x^2 and z.  A spin density below 1e-30 has no derivatives (the reference
+// masks its derivative terms there).
+template <int N>
+DN<N> vsxc_c(int set, DN<N> ra, DN<N> rb, const DN<N>& gaa, const DN<N>& gbb, const DN<N>& ta, const DN<N>& tb) {
+  if (!(ra.v >= VS_DTOL)) ra = cst<N>(ra.v);
+  if (!(rb.v >= VS_DTOL)) rb = cst<N>(rb.v);
+  const DN<N> zero = cst<N>(0.0);
+  const DN<N> ea = pw92_c_lda(ra, zero), eb = pw92_c_lda(zero, rb);
+  const DN<N> eo = pw92_c_lda(ra, rb) - ea - eb;
+  DN<N> F = zero;
+  if (ra.v >= VS_DTOL) F = F + ea * gvt4(0.00515088, vsxc_dc(set, 1), vs_x2(ra, gaa), vs_z(ra, ta)) * vs_dsic(ra, gaa, ta);
+  if (rb.v >= VS_DTOL) F = F + eb * gvt4(0.00515088, vsxc_dc(set, 1), vs_x2(rb, gbb), vs_z(rb, tb)) * vs_dsic(rb, gbb, tb);
+  if ((ra + rb).v >= VS_DTOL)
+    F = F + eo * gvt4(0.00304966, vsxc_dc(set, 2), vs_x2(ra, gaa) + vs_x2(rb, gbb), vs_z(ra, ta) + vs_z(rb, tb));
+  return F;
+}
+
+inline const double* m06_a(int set) {  // get_pars_m06_exchange, a(0:11)
+  static const double p[2][12] = {
+      {3.987756E-01, 2.548219E-01, 3.923994E-01, -2.103655E+00, -6.302147E+00, 1.097615E+01, 3.097273E+01,
+       -2.318489E+01, -5.673480E+01, 2.160364E+01, 3.421814E+01, -9.049762E+00},
+      {5.877943E-01, -1.371776E-01, 2.682367E-01, -2.515898E+00, -2.978892E+00, 8.710679E+00, 1.688195E+01,
+       -4.489724E+00, -3.299983E+01, -1.449050E+01, 2.043747E+01, 1.256504E+01}};
+  return p[set - 1];
+}
+inline const double* m06_c(int set, int term) {  // get_pars_m06_correlation
+  static const double p[2][2][5] = {
+      {{5.349466E-01, 5.396620E-01, -3.161217E+01, 5.149592E+01, -2.919613E+01},
+       {6.042374E-01, 1.776783E+02, -2.513252E+02, 7.635173E+01, -1.255699E+01}},
+      {{5.094055E-01, -1.491085E+00, 1.723922E+01, -3.859018E+01, 2.845044E+01},
+       {3.741539E+00, 2.187098E+02, -4.531252E+02, 2.936479E+02, -6.287470E+01}}};
+  return p[set - 1][term - 1];
+}
+
+// m06_exchange of one spin: e_x^LSDA F_PBE(x^2) f(w) (pbeef, kedef) plus vsxc_exchange of the set
+template <int N>
+DN<N> m06_x_spin(int set, const DN<N>& r, const DN<N>& g, const DN<N>& t) {
+  const double pbec2 = 4.49267E-3, pbec1 = 3.612108584108E-03, CT = 4.55779987234560;
+  const DN<N> x2 = vs_x2(r, g);
+  const DN<N> pf = 1.0 + pbec1 * x2 / (1.0 + pbec2 * x2);
+  DN<N> w = cst<N>(0.0);
+  if (r.v >= VS_DTOL && t.v >= VS_DTOL) {
+    const DN<N> tu = CT * dpow(r, 5.0 / 3.0);
+    w = (tu - t) / (tu + t);
+  }
+  const double* a = m06_a(set);
+  DN<N> k = cst<N>(a[11]);
+  for (int j = 10; j >= 0; --j) k = k * w + a[j];
+  return vs_ex(r) * pf * k + vsxc_x_spin(set, r, g, t);
+}
+
+// bmk_term: c0 + c1 v + ... + c4 v^4, v = beta x^2 / (1 + beta x^2)
+template <int N>
+DN<N> bmk(double beta, const double* c, const DN<N>& x2) {
+  const DN<N> v = beta * x2 / (1.0 + beta * x2);
+  return c[0] + (c[1] + (c[2] + (c[3] + c[4] * v) * v) * v) * v;
+}
+
+// m06_correlation: vsxc_correlation of the set plus the B97-type terms
+template <int N>
+DN<N> m06_cor(int set, const DN<N>& ra, const DN<N>& rb, const DN<N>& gaa, const DN<N>& gbb, const DN<N>& ta,
+              const DN<N>& tb) {
+  const DN<N> zero = cst<N>(0.0);
+  const DN<N> ea = pw92_c_lda(ra, zero), eb = pw92_c_lda(zero, rb);
+  const DN<N> eo = pw92_c_lda(ra, rb) - ea - eb;
+  const DN<N> xa = vs_x2(ra, gaa), xb = vs_x2(rb, gbb);
+  DN<N> F = vsxc_c(set, ra, rb, gaa, gbb, ta, tb);
+  F = F + ea * bmk(0.06, m06_c(set, 1), xa) * vs_dsic(ra, gaa, ta);
+  F = F + eb * bmk(0.06, m06_c(set, 1), xb) * vs_dsic(rb, gbb, tb);
+  return F + eo * bmk(0.0031, m06_c(set, 2), xa + xb);
+}
+
+// VSXC / M06-L / M06 of the spin-resolved quantities (gamma_ab is not used)
+template <int N>
+DN<N> vs_family(int set, const DN<N>& ra, const DN<N>& rb, const DN<N>& gaa, const DN<N>& gbb, const DN<N>& ta,
+                const DN<N>& tb) {
+  if (set == 0) return vsxc_x_spin(0, ra, gaa, ta) + vsxc_x_spin(0, rb, gbb, tb) + vsxc_c(0, ra, rb, gaa, gbb, ta, tb);
+  return m06_x_spin(set, ra, gaa, ta) + m06_x_spin(set, rb, gbb, tb) + m06_cor(set, ra, rb, gaa, gbb, ta, tb);
+}
+
+// A meta-GGA at one point (set: -1 TPSS, 0 VSXC, 1 M06-L, 2 M06): f and its
+// derivatives in the reference's layout (ispin 1: rho, gamma, tau of the
+// total density; ispin 2: rho_a, rho_b; gamma_aa, gamma_bb, gamma_ab; tau_a,
+// tau_b).  The closed shell is the open form at rho/2, gamma/4, tau/2, as
+// the reference's wrappers evaluate it; its derivatives are the chain rule of
+// that (tpss_X, m06_X, m06_C), except that vsxc_X and vsxc_C scale the
+// spin-a derivatives by 0.5, 0.25, 0.5 (vsxc_mgga_module.f90:127-131,
+// :213-217), half the chain rule, which is restated as it is.
+inline void mgga_point(int set, int ispin, const double* rho, const double* gam, const double* tau, double& f,
+                       double* fr, double* fg, double* ft) {
   if (ispin == 1) {
     const DN<3> r = var<3>(0, rho[0]), g = var<3>(1, gam[0]), t = var<3>(2, tau[0]);
     const DN<3> hr = 0.5 * r, qg = 0.25 * g, ht = 0.5 * t;
-    const DN<3> F = 2.0 * tpss_x_spin(hr, qg, ht) + tpss_c(hr, hr, qg, qg, qg, ht, ht, true);
+    const DN<3> F = set < 0 ? 2.0 * tpss_x_spin(hr, qg, ht) + tpss_c(hr, hr, qg, qg, qg, ht, ht, true)
+                            : vs_family(set, hr, hr, qg, qg, ht, ht);
+    const double h = set == 0 ? 0.5 : 1.0;
     f = F.v;
-    fr[0] = F.d[0];
-    fg[0] = F.d[1];
-    ft[0] = F.d[2];
+    fr[0] = h * F.d[0];
+    fg[0] = h * F.d[1];
+    ft[0] = h * F.d[2];
     return;
   }
   const DN<7> ra = var<7>(0, rho[0]), rb = var<7>(1, rho[1]);
   const DN<7> gaa = var<7>(2, gam[0]), gbb = var<7>(3, gam[1]), gab = var<7>(4, gam[2]);
   const DN<7> ta = var<7>(5, tau[0]), tb = var<7>(6, tau[1]);
-  const DN<7> F = tpss_x_spin(ra, gaa, ta) + tpss_x_spin(rb, gbb, tb) + tpss_c(ra, rb, gaa, gbb, gab, ta, tb, false);
+  const DN<7> F = set < 0 ? tpss_x_spin(ra, gaa, ta) + tpss_x_spin(rb, gbb, tb) +
+                                tpss_c(ra, rb, gaa, gbb, gab, ta, tb, false)
+                          : vs_family(set, ra, rb, gaa, gbb, ta, tb);
   f = F.v;
   fr[0] = F.d[0];
   fr[1] = F.d[1];

@@ -32,6 +32,11 @@
 #include "../include/pgxc.h"
 #include "mgga_oracle.h"
 
+// parameter set of mgga::mgga_point for a meta-GGA keyword
+static int mgga_set(int xc) {
+  return xc == PGXC_XC_TPSS ? -1 : xc == PGXC_XC_VSXC ? 0 : xc == PGXC_XC_M06L ? 1 : 2;
+}
+
 namespace {
 
 // ---------------------------------------------------------------------------
@@ -1337,7 +1342,7 @@ int oracle_functionals_mgga(int32_t xc, int32_t ispin, int64_t n, const double* 
     for (int c = 0; c < ng; ++c) g[c] = gam[i + n * c];
     double t[2] = {tau[i], ispin == 2 ? tau[i + n] : 0.0};
     double F, Fr[2], Fg[3], Ft[2];
-    mgga::tpss_point(ispin, r, g, t, F, Fr, Fg, Ft);
+    mgga::mgga_point(mgga_set(xc), ispin, r, g, t, F, Fr, Fg, Ft);
     f[i] = F;
     for (int s = 0; s < ispin; ++s) {
       fr[i + n * s] = Fr[s];
@@ -1509,7 +1514,7 @@ int oracle_xc_build(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_
         double F, Fr[2], Fg[3], Ft[2] = {0.0, 0.0};
         if (mgga) {
           double t[2] = {tau[i], ispin == 2 ? tau[i + vla] : 0.0};
-          mgga::tpss_point(ispin, r, g, t, F, Fr, Fg, Ft);
+          mgga::mgga_point(mgga_set(xc), ispin, r, g, t, F, Fr, Fg, Ft);
         } else {
           functional_point(xc, ispin, r, g, F, Fr, Fg);
         }

@@ -79,12 +79,12 @@ void launch_functional2_f64(const XcConst& K, const double* w, double* pa, doubl
                             int64_t nvalid, bool gga, double* partial, double* acc, cudaStream_t st);
 // Fixed-order sum of nblocks {w f, w rho} block partials, Kahan-added into acc[4].
 void launch_sum_partials(const double* partial, int nblocks, double* acc, cudaStream_t st);
-// The meta-GGA (TPSS) functional step of the screened build (mgga.cu): pt as
+// The meta-GGA functional step of the screened build (mgga.cu): pt as
 // the screened point arrays (8 planes of ld per spin: rho, grad rho, A, B),
 // tq 4 planes of ld per spin (the three 2 tau_j contractions, then C).
-void launch_xc_points_mgga(int ispin, int64_t n, const double* rho, const double* gam, const double* tau, double* f,
+void launch_xc_points_mgga(int functional, int ispin, int64_t n, const double* rho, const double* gam, const double* tau, double* f,
                            double* fr, double* fg, double* ft, cudaStream_t st);
-void launch_functional_mgga(int ispin, const double* w, double* pt, double* tq, int64_t ld, int64_t p0,
+void launch_functional_mgga(int functional, int ispin, const double* w, double* pt, double* tq, int64_t ld, int64_t p0,
                             int64_t nvalid, double* partial, double* acc, cudaStream_t st);
 void launch_zbuild_f64(const BuildArgs& a, bool gga, cudaStream_t st);
 void launch_vpot_f64(const BuildArgs& a, bool gga, cudaStream_t st);

@@ -1,4 +1,5 @@
-// mgga.cu -- the meta-GGA functional step of the screened builds.
+// mgga.cu -- the meta-GGA functional step of the screened builds (TPSS,
+// M06-L, M06, VSXC).
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -17,7 +18,7 @@ namespace {
 // grad phi_i . grad phi_j as calc_xcks_nl (xc_hamiltonian.f90:1448-1454,
 // :1534-1555).  Partials of w f and w rho as k_functional.
 template <int ISPIN>
-__global__ void __launch_bounds__(256) k_functional_mgga(int64_t p0, int64_t nvalid, int64_t n,
+__global__ void __launch_bounds__(256) k_functional_mgga(int functional, int64_t p0, int64_t nvalid, int64_t n,
                                                          const double* __restrict__ w, double* __restrict__ pt,
                                                          double* __restrict__ tq, int64_t ld,
                                                          double* __restrict__ partial) {
@@ -38,7 +39,7 @@ __global__ void __launch_bounds__(256) k_functional_mgga(int64_t p0, int64_t nva
     if (ISPIN == 1) {
       const double gam = g[0][0] * g[0][0] + g[0][1] * g[0][1] + g[0][2] * g[0][2];
       double f, fr, fg, ft;
-      mgga::tpss_closed(rho[0], gam, tau[0], f, fr, fg, ft);
+      mgga::mgga_closed(functional, rho[0], gam, tau[0], f, fr, fg, ft);
       pt[4 * ld + p] = 0.5 * fr * wt;
       const double bb = wt * 2.0 * fg;
 #pragma unroll
@@ -55,7 +56,7 @@ __global__ void __launch_bounds__(256) k_functional_mgga(int64_t p0, int64_t nva
         gam[2] += g[0][c] * g[1][c];
       }
       double f, fr[2], fg[3], ft[2];
-      mgga::tpss_open(rho, gam, tau, f, fr, fg, ft);
+      mgga::mgga_open(functional, rho, gam, tau, f, fr, fg, ft);
 #pragma unroll
       for (int s = 0; s < 2; ++s) {
         double* a = pt + 8 * s * ld;
@@ -88,14 +89,14 @@ __global__ void __launch_bounds__(256) k_functional_mgga(int64_t p0, int64_t nva
 // The meta-GGA at n points, column-major: rho (ispin), gam (2 ispin - 1),
 // tau (ispin) -> f, fr (ispin), fg (2 ispin - 1), ft (ispin).
 template <int ISPIN>
-__global__ void k_xc_points_mgga(int64_t n, const double* __restrict__ rho, const double* __restrict__ gam,
+__global__ void k_xc_points_mgga(int functional, int64_t n, const double* __restrict__ rho, const double* __restrict__ gam,
                                  const double* __restrict__ tau, double* __restrict__ f, double* __restrict__ fr,
                                  double* __restrict__ fg, double* __restrict__ ft) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= n) return;
   if (ISPIN == 1) {
     double F, Fr, Fg, Ft;
-    mgga::tpss_closed(rho[p], gam[p], tau[p], F, Fr, Fg, Ft);
+    mgga::mgga_closed(functional, rho[p], gam[p], tau[p], F, Fr, Fg, Ft);
     f[p] = F;
     fr[p] = Fr;
     fg[p] = Fg;
@@ -104,7 +105,7 @@ __global__ void k_xc_points_mgga(int64_t n, const double* __restrict__ rho, cons
     const double r[2] = {rho[p], rho[p + n]}, g[3] = {gam[p], gam[p + n], gam[p + 2 * n]},
                  t[2] = {tau[p], tau[p + n]};
     double F, Fr[2], Fg[3], Ft[2];
-    mgga::tpss_open(r, g, t, F, Fr, Fg, Ft);
+    mgga::mgga_open(functional, r, g, t, F, Fr, Fg, Ft);
     f[p] = F;
     for (int s = 0; s < 2; ++s) {
       fr[p + s * n] = Fr[s];
@@ -116,18 +117,18 @@ __global__ void k_xc_points_mgga(int64_t n, const double* __restrict__ rho, cons
 
 }  // namespace
 
-void launch_xc_points_mgga(int ispin, int64_t n, const double* rho, const double* gam, const double* tau, double* f,
+void launch_xc_points_mgga(int functional, int ispin, int64_t n, const double* rho, const double* gam, const double* tau, double* f,
                            double* fr, double* fg, double* ft, cudaStream_t st) {
   const unsigned nb = (unsigned)((n + 127) / 128);
-  if (ispin == 1) k_xc_points_mgga<1><<<nb, 128, 0, st>>>(n, rho, gam, tau, f, fr, fg, ft);
-  else k_xc_points_mgga<2><<<nb, 128, 0, st>>>(n, rho, gam, tau, f, fr, fg, ft);
+  if (ispin == 1) k_xc_points_mgga<1><<<nb, 128, 0, st>>>(functional, n, rho, gam, tau, f, fr, fg, ft);
+  else k_xc_points_mgga<2><<<nb, 128, 0, st>>>(functional, n, rho, gam, tau, f, fr, fg, ft);
 }
 
-void launch_functional_mgga(int ispin, const double* w, double* pt, double* tq, int64_t ld, int64_t p0,
+void launch_functional_mgga(int functional, int ispin, const double* w, double* pt, double* tq, int64_t ld, int64_t p0,
                             int64_t nvalid, double* partial, double* acc, cudaStream_t st) {
   const unsigned nb = (unsigned)((ld + 255) / 256);
-  if (ispin == 1) k_functional_mgga<1><<<nb, 256, 0, st>>>(p0, nvalid, ld, w, pt, tq, ld, partial);
-  else k_functional_mgga<2><<<nb, 256, 0, st>>>(p0, nvalid, ld, w, pt, tq, ld, partial);
+  if (ispin == 1) k_functional_mgga<1><<<nb, 256, 0, st>>>(functional, p0, nvalid, ld, w, pt, tq, ld, partial);
+  else k_functional_mgga<2><<<nb, 256, 0, st>>>(functional, p0, nvalid, ld, w, pt, tq, ld, partial);
   launch_sum_partials(partial, (int)nb, acc, st);
 }
 

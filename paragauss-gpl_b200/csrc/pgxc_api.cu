@@ -509,6 +509,7 @@ int create_impl(const pgxc_geometry* geo, const pgxc_basis* bas, const pgxc_grid
     in.precision = o.precision;
     in.keep_basis = o.keep_orbitals != 0;
     in.mgga = PGXC_XC_IS_MGGA(o.functional);
+    in.functional = o.functional;
     in.max_chunk_points = o.max_chunk_points;
     std::string e;
     st = screen_create(&c->screen, in, a, c->stream, e);
@@ -1717,7 +1718,7 @@ int pgxc_xc_functionals_mgga(int32_t functional, int32_t ispin, int64_t n, const
   if (e == cudaSuccess) e = cudaMemcpy(dgam, gam, sizeof(double) * ng * n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(dtau, tau, sizeof(double) * ispin * n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess) {
-    launch_xc_points_mgga(ispin, n, drho, dgam, dtau, df, dfr, dfg, dft, 0);
+    launch_xc_points_mgga(functional, ispin, n, drho, dgam, dtau, df, dfr, dfg, dft, 0);
     e = cudaDeviceSynchronize();
   }
   if (e == cudaSuccess) e = cudaMemcpy(f, df, sizeof(double) * n, cudaMemcpyDeviceToHost);

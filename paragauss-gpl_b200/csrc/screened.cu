@@ -434,6 +434,7 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
   ScreenPlan* sp = new ScreenPlan();
   sp->gga = in.gga;
   sp->mgga = in.mgga;
+  sp->functional = in.functional;
   sp->ispin = in.ispin;
   sp->nbas = in.nbas;
   sp->keep = in.keep_basis;
@@ -817,7 +818,8 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
     if (timed) SR_TRY(cudaEventRecord(ev[5], st));
     // K2
     if (sp->mgga) {
-      launch_functional_mgga(ispin, sp->qw, sp->pt, sp->tq, cp, t0 * 128, npt, sp->partial, a.acc, st);
+      launch_functional_mgga(sp->functional, ispin, sp->qw, sp->pt, sp->tq, cp, t0 * 128, npt, sp->partial, a.acc,
+                             st);
     } else if (ispin == 1) {
       BuildArgs bf = b[0];
       bf.w = sp->qw;

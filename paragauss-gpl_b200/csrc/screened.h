@@ -48,6 +48,7 @@ struct ScreenInput {
   int64_t max_chunk_points;   // 0: sized from free device memory
   bool keep_basis = false;    // basis values of the whole grid stay resident across builds
   bool mgga = false;          // meta-GGA: tau in the density, its term in the potential (FP64 DMMA)
+  int functional = 0;         // PGXC_XC_*
 };
 
 int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, cudaStream_t st, std::string& err);

@@ -44,6 +44,7 @@ struct ScreenPlan {
   double *phi = nullptr, *gx = nullptr, *gy = nullptr, *gz = nullptr, *Z = nullptr;
   double* pt = nullptr;      // 8 point arrays of chunk_tiles*128 per spin
   bool mgga = false;
+  int functional = 0;        // PGXC_XC_* (the meta-GGA step selects its functional by id)
   double* tq = nullptr;      // meta-GGA: 4 point arrays per spin (2 tau_x, 2 tau_y, 2 tau_z, C)
   double* partial = nullptr;
   double* V = nullptr;       // [ispin][nbas][nbas]

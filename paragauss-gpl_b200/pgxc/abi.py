@@ -46,15 +46,19 @@ XC_ECMV92 = 27
 XC_RPW91 = 28
 XC_RVWN_ENGEL = 29
 XC_TPSS = 30
+XC_M06L = 31
+XC_M06 = 32
+XC_VSXC = 33
 XC_IDS = {"VWN": XC_VWN, "PBE": XC_PBE, "revPBE": XC_REVPBE, "PBEsol": XC_PBESOL, "BP86": XC_BP86,
           "PW91": XC_PW91, "BPW91": XC_BPW91, "BLYP": XC_BLYP, "XALPHA": XC_XALPHA, "B88": XC_B88,
           "PBEN": XC_PBEN, "VMT": XC_VMT, "VT84": XC_VT84, "VMTsol": XC_VMTSOL, "VT84sol": XC_VT84SOL,
           "HCTH": XC_HCTH, "HCTH120": XC_HCTH120, "HCTH147": XC_HCTH147, "HCTH407": XC_HCTH407,
           "NRECMV92": XC_NRECMV92, "PWLDA": XC_PWLDA, "B3LYP": XC_B3LYP, "PBE0": XC_PBE0,
           "LB94": XC_LB94, "RVWN": XC_RVWN, "RBP": XC_RBP, "ECMV92": XC_ECMV92,
-          "RPW91": XC_RPW91, "RVWN_ENGEL": XC_RVWN_ENGEL, "TPSS": XC_TPSS}
+          "RPW91": XC_RPW91, "RVWN_ENGEL": XC_RVWN_ENGEL, "TPSS": XC_TPSS,
+          "M06L": XC_M06L, "M06": XC_M06, "VSXC": XC_VSXC}
 LDA_XC = ("VWN", "XALPHA", "PWLDA", "RVWN", "RVWN_ENGEL")
-MGGA_XC = ("TPSS",)
+MGGA_XC = ("TPSS", "M06L", "M06", "VSXC")
 # the keywords without tau (the point-functional API and every layout)
 GGA_LDA_XC = tuple(k for k in XC_IDS if k not in MGGA_XC)
 

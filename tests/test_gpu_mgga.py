@@ -1,4 +1,4 @@
-"""TPSS (meta-GGA) on the device against the oracle: the point functional
+"""The meta-GGAs (TPSS, M06-L, M06, VSXC) on the device against the oracle: the point functional
 with tau, and whole builds with the kinetic-energy density in the density
 step and the tau term in the potential (screened layout, FP64 and INT8,
 closed and open shell).  Bars 1e-10 (FP64) and 1e-7 (INT8) as for the other
@@ -30,18 +30,33 @@ def _points(rng, n, ispin):
     return rho, gs, tau
 
 
+MGGA = ["TPSS", "M06L", "M06", "VSXC"]
+
+
+@pytest.mark.parametrize("xc", MGGA)
 @pytest.mark.parametrize("ispin", [1, 2])
-def test_tpss_points_match_oracle(ispin):
+def test_mgga_points_match_oracle(xc, ispin):
     rng = np.random.default_rng(20 + ispin)
     rho, gam, tau = _points(rng, 400, ispin)
-    f, fr, fg, ft = lib.xc_functionals_mgga("TPSS", rho, gam, tau)
-    rf, rfr, rfg, rft = O.functionals_mgga("TPSS", ispin, rho, gam, tau)
+    f, fr, fg, ft = lib.xc_functionals_mgga(xc, rho, gam, tau)
+    rf, rfr, rfg, rft = O.functionals_mgga(xc, ispin, rho, gam, tau)
     # relative to the size of the Slater term at each point (the pieces have mixed signs)
     n = rho.sum(1)
     sl = 0.75 * (3 / np.pi) ** (1 / 3) * n ** (4 / 3)
     assert np.all(np.abs(f - rf) <= 1e-11 * (np.abs(rf) + sl) + 1e-300)
+    # The derivatives at 1e-9.  Where one spin density is below 1e-6 of the
+    # other, the opposite-spin energy of VSXC and M06, e_c(a, b) - e_c(a, 0) -
+    # e_c(0, b), is a difference of nearly equal terms: ulp-level differences
+    # between the device's and the host's pow/log grow by the ratio of the
+    # densities (host-compiled device code agrees with the oracle to 1e-12
+    # there), so those points get 1e-6.
+    rel = np.full(rho.shape[0], 1e-9)
+    if ispin == 2:
+        lop = np.min(rho, axis=1) < 1e-6 * np.max(rho, axis=1)
+        rel[lop] = 1e-6
     for a, b in ((fr, rfr), (fg, rfg), (ft, rft)):
-        assert np.all(np.abs(a - b) <= 1e-9 * np.abs(b) + 1e-11 * np.max(np.abs(b), axis=0, keepdims=True) + 1e-300)
+        tol = rel[:, None] * np.abs(b) + 1e-11 * np.max(np.abs(b), axis=0, keepdims=True) + 1e-300
+        assert np.all(np.abs(a - b) <= tol), float(np.max(np.abs(a - b) / tol))
 
 
 def _build(c, **kw):
@@ -55,20 +70,22 @@ BUILDS = pytest.mark.parametrize("precision,thr,tol", [("fp64", 0.0, 1e-10), ("f
 
 
 @BUILDS
-@pytest.mark.parametrize("seed,lmax", [(41, 2), (42, 3)])
-def test_tpss_build_matches_oracle(seed, lmax, precision, thr, tol):
-    c = cases.small_case(functional="TPSS", seed=seed, lmax=lmax)
+@pytest.mark.parametrize("xc,seed,lmax", [("TPSS", 41, 2), ("TPSS", 42, 3), ("M06L", 47, 2), ("M06", 48, 3),
+                                          ("VSXC", 49, 2)])
+def test_mgga_build_matches_oracle(xc, seed, lmax, precision, thr, tol):
+    c = cases.small_case(functional=xc, seed=seed, lmax=lmax)
     O.weight_case(c)
     ref, re, rn = O.xc_build(c)
     ham, e, n = _build(c, precision=precision, screen_threshold=thr, max_chunk_points=1024)
-    print(f"TPSS {precision} {thr}: |dE|={abs(e - re):.2e} |dN|={abs(n - rn):.2e} max|dV|={np.max(np.abs(ham - ref)):.2e}")
+    print(f"{xc} {precision} {thr}: |dE|={abs(e - re):.2e} |dN|={abs(n - rn):.2e} max|dV|={np.max(np.abs(ham - ref)):.2e}")
     assert abs(e - re) < tol and abs(n - rn) < tol
     assert float(np.max(np.abs(ham - ref))) < tol
 
 
 @BUILDS
-def test_tpss_open_shell_build_matches_oracle(precision, thr, tol):
-    c = cases.small_case(functional="TPSS", seed=43, natoms=5, nocc=7, ispin=2)
+@pytest.mark.parametrize("xc", MGGA)
+def test_mgga_open_shell_build_matches_oracle(xc, precision, thr, tol):
+    c = cases.small_case(functional=xc, seed=43, natoms=5, nocc=7, ispin=2)
     O.weight_case(c)
     ref, re, rn = O.xc_build(c)
     ham, e, n = _build(c, precision=precision, screen_threshold=thr, max_chunk_points=1024)
