@@ -1643,6 +1643,7 @@ int oracle_xc_build_sym(const pgxc_geometry* geo, const pgxc_basis* bas, const p
   const double* gz = gy + npts;
   const double* gw = gz + npts;
   const bool gga = PGXC_XC_IS_GGA(xc);
+  const bool mgga = PGXC_XC_IS_MGGA(xc);
   const int64_t nbatch = (npts + vla - 1) / vla;
   int dmax = 1, omax = 1;
   for (int i = 0; i < nirr; ++i) {
@@ -1673,7 +1674,7 @@ int oracle_xc_build_sym(const pgxc_geometry* geo, const pgxc_basis* bas, const p
     W.graphi.assign((size_t)vla * 3 * omax, 0.0);
     W.help.assign((size_t)vla * dmax, 0.0);
     std::vector<double> rho(2 * vla), grarho(6 * vla), gam(3 * vla), fxc(vla), fr(2 * vla), fg(3 * vla);
-    std::vector<double> Asc(2 * vla), Bv(6 * vla);
+    std::vector<double> Asc(2 * vla), Bv(6 * vla), tau(2 * vla), ft(2 * vla);
 #ifdef _OPENMP
 #pragma omp for schedule(dynamic, 4)
 #endif
@@ -1684,6 +1685,7 @@ int oracle_xc_build_sym(const pgxc_geometry* geo, const pgxc_basis* bas, const p
                  W.rad1, W.prim0, W.prim1);
       std::fill(rho.begin(), rho.end(), 0.0);
       std::fill(grarho.begin(), grarho.end(), 0.0);
+      std::fill(tau.begin(), tau.end(), 0.0);
       // density_calc_nl over irreps and partners
       for (int i = 0; i < nirr; ++i) {
         const int d = sym->dims[i], no = nocc[i], np = sym->partners[i];
@@ -1704,6 +1706,11 @@ int oracle_xc_build_sym(const pgxc_geometry* geo, const pgxc_basis* bas, const p
                 const double* gj = W.graphi.data() + (size_t)j * 3 * vl;
                 for (int c = 0; c < 3; ++c)
                   for (int k = 0; k < vl; ++k) grarho[k + vla * (c + 3 * s)] += 2 * pj[k] * gj[c * vl + k] * o;
+                // tau = 1/2 sum occ/partners |grad phi|^2 (density_calc_module.f90:1540-1551)
+                if (mgga)
+                  for (int k = 0; k < vl; ++k)
+                    tau[k + vla * s] += (gj[k] * gj[k] + gj[vl + k] * gj[vl + k] + gj[2 * vl + k] * gj[2 * vl + k]) *
+                                        0.5 * o;
               }
             }
           }
@@ -1727,11 +1734,17 @@ int oracle_xc_build_sym(const pgxc_geometry* geo, const pgxc_basis* bas, const p
       for (int k = 0; k < vl; ++k) {
         double r[2] = {rho[k], ispin == 2 ? rho[k + vla] : 0.0};
         double g[3] = {gam[k], gam[k + vla], gam[k + 2 * vla]};
-        double F, Fr[2], Fg[3];
-        functional_point(xc, ispin, r, g, F, Fr, Fg);
+        double F, Fr[2], Fg[3], Ft[2] = {0.0, 0.0};
+        if (mgga) {
+          double t[2] = {tau[k], ispin == 2 ? tau[k + vla] : 0.0};
+          mgga::mgga_point(mgga_set(xc), ispin, r, g, t, F, Fr, Fg, Ft);
+        } else {
+          functional_point(xc, ispin, r, g, F, Fr, Fg);
+        }
         fxc[k] = F;
         fr[k] = Fr[0]; fr[k + vla] = Fr[1];
         fg[k] = Fg[0]; fg[k + vla] = Fg[1]; fg[k + 2 * vla] = Fg[2];
+        ft[k] = Ft[0]; ft[k + vla] = Ft[1];
         W.exc += F * gw[lo + k];
       }
       // A and B per spin (:1429-1446), or w dfdrho (:955-957)
@@ -1763,6 +1776,16 @@ int oracle_xc_build_sym(const pgxc_geometry* geo, const pgxc_basis* bas, const p
               }
             double* ham = W.ham.data() + (size_t)s * hlen + hofs[i];
             dgemm('t', 'n', d, d, vl, 1.0 / np, W.help.data(), vl, sp.data(), vl, 1.0, ham, d);
+            if (mgga) {
+              // tau term per direction (xc_hamiltonian.f90:1534-1555): 1/4 (C grad_c phi)^T grad_c phi / partners
+              for (int c = 0; c < 3; ++c) {
+                for (int ff = 0; ff < d; ++ff)
+                  for (int k = 0; k < vl; ++k)
+                    W.help[(size_t)ff * vl + k] = ft[k + vla * s] * gw[lo + k] * sg[(size_t)ff * 3 * vl + c * vl + k];
+                dgemm('t', 'n', d, d, vl, 0.25 / np, W.help.data(), vl, sg.data() + (size_t)c * vl, 3 * vl, 1.0, ham,
+                      d);
+              }
+            }
           }
         }
       }

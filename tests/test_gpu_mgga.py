@@ -120,3 +120,32 @@ def test_tpss_rejections():
     with lib.Context(d, weighted=False, screen_threshold=0.0) as ctx:
         with pytest.raises(lib.PgxcError):
             ctx.xc_gradient()
+
+
+@pytest.mark.parametrize("xc", ["TPSS", "M06L"])
+def test_mgga_symmetric_build_matches_oracle(xc):
+    """A meta-GGA through pgxc_build_sym (C2v): the C1 build of the expanded
+    orbitals, tau included, projected per irrep."""
+    from pgxc import symmetry as Y
+    case, ad, Cs, occs = Y.symmetric_case("C2v", functional=xc)
+    O.weight_case(case)
+    ref, re, rn = O.xc_build_sym(case, ad, Cs, occs)
+    with lib.Context(case, precision="fp64", screen_threshold=0.0) as ctx:
+        ctx.set_symmetry(ad)
+        ham, e, n = ctx.build_sym(Cs, occs)
+    assert abs(e - re) < 1e-10 and abs(n - rn) < 1e-10
+    assert float(np.max(np.abs(ham - ref))) < 1e-10
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_mgga_keep_orbitals_repeats_the_build(precision):
+    """With the basis values kept across builds, a second TPSS build (tau
+    contractions on the kept gradients) equals the first."""
+    c = cases.small_case(functional="TPSS", seed=51)
+    O.weight_case(c)
+    thr = 0.0 if precision == "fp64" else 1e-10
+    with lib.Context(c, precision=precision, screen_threshold=thr, keep_orbitals=True) as ctx:
+        h1, e1, n1 = ctx.build()
+        h2, e2, n2 = ctx.build()
+    assert e1 == e2 and n1 == n2
+    np.testing.assert_allclose(h2, h1, rtol=0, atol=1e-12)

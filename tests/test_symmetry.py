@@ -149,3 +149,20 @@ def test_reduced_grid_gradient_averages_to_full_grid_gradient():
     assert np.max(np.abs(average_gradient(case.coords, ops, g_full) - g_full)) < 1e-10
     assert np.max(np.abs(g_red - g_full)) > 1e-6   # the reduced grid alone is not symmetric
     np.testing.assert_allclose(average_gradient(case.coords, ops, g_red), g_full, rtol=0, atol=1e-10)
+
+
+@pytest.mark.parametrize("xc", ["TPSS", "M06L", "VSXC"])
+def test_symmetric_mgga_build_matches_projected_c1_build(xc):
+    """The oracle's irrep and partner loops with tau (occ / partners per
+    partner, the tau term per irrep) against the C1 build of the expanded
+    orbitals projected with U."""
+    case, ad, Cs, occs = Y.symmetric_case("C2v", functional=xc)
+    O.weight_case(case)
+    h1, e1, n1 = O.xc_build_sym(case, ad, Cs, occs)
+    C, occ = Y.c1_orbitals(ad, Cs, occs)
+    c1 = Y.cases.Case(**{**case.__dict__})
+    c1.C, c1.occ, c1.nocc = C, occ, C.shape[1]
+    hc, ec, nc = O.xc_build(c1)
+    hp = Y.project(ad, O.unpack(hc, c1.nbas)[None])
+    assert abs(e1 - ec) < 1e-12 and abs(n1 - nc) < 1e-12
+    np.testing.assert_allclose(h1, hp, rtol=0, atol=1e-12)
