@@ -239,70 +239,83 @@ __global__ void k_grad_points(XcConst K, bool gga, int ispin, int64_t nbas, int6
   atomicAdd(exc, wp * f);
 }
 
-// q^s_mu,k(p) for one function and point, summed over spins
-__device__ __forceinline__ void q_terms(bool gga, int ispin, int64_t f, int64_t p, int64_t ld, int64_t plane,
-                                        const double* __restrict__ B, const double* __restrict__ XY,
-                                        const double* __restrict__ coef, double* q) {
-  const int64_t o = f * ld + p;
-  double d[3], H[6];
-  for (int c = 0; c < 3; ++c) d[c] = B[(1 + c) * plane + o];
-  if (gga)
-    for (int k = 0; k < 6; ++k) H[k] = B[(4 + k) * plane + o];
-  q[0] = q[1] = q[2] = 0.0;
-  for (int s = 0; s < ispin; ++s) {
-    const double X = XY[(4 * s) * plane + o];
-    const double a = coef[(4 * s) * ld + p];
-    for (int k = 0; k < 3; ++k) q[k] += 2.0 * a * d[k] * X;
-    if (!gga) continue;
-    double Yj[3], b[3];
-    for (int j = 0; j < 3; ++j) {
-      Yj[j] = XY[(4 * s + 1 + j) * plane + o];
-      b[j] = coef[(4 * s + 1 + j) * ld + p];
+// The orbital terms in one pass: q^s_mu,k(p) is formed once per function and
+// point.  Block = 256 points x kGradFB functions: each thread takes one point
+// and loops over the block's functions; -q goes to atom(mu) through a warp
+// reduction and the block's shared sums, +q to the point's host through the
+// thread's running sum, reduced over the warp when all its points share a
+// host (the usual case: the raw grid is atom by atom) and the block's shared
+// per-atom sums.
+constexpr int kGradFB = 32;
+
+__global__ void __launch_bounds__(256) k_grad_orb(bool gga, int ispin, int64_t nbas, int64_t ld, int64_t p0,
+                                                  int64_t nvalid, int natm, const int* __restrict__ fatom,
+                                                  const int* __restrict__ owner, const double* __restrict__ B,
+                                                  int64_t plane, const double* __restrict__ XY,
+                                                  const double* __restrict__ coef, double* __restrict__ grad) {
+  extern __shared__ double sh[];  // [kGradFB][3] function sums, then [natm][3] host sums
+  double* gq = sh;
+  double* gh = sh + 3 * kGradFB;
+  for (int i = threadIdx.x; i < 3 * (kGradFB + natm); i += blockDim.x) sh[i] = 0.0;
+  __syncthreads();
+  const int64_t p = (int64_t)blockIdx.y * blockDim.x + threadIdx.x;
+  const bool live = p < nvalid;
+  const int lane = threadIdx.x & 31;
+  const int64_t f0 = (int64_t)blockIdx.x * kGradFB, f1 = min(nbas, f0 + kGradFB);
+  // the point's coefficients, once for all its functions
+  double a[2] = {0, 0}, b[2][3] = {{0, 0, 0}, {0, 0, 0}};
+  if (live)
+    for (int sp = 0; sp < ispin; ++sp) {
+      a[sp] = coef[(4 * sp) * ld + p];
+      if (gga)
+        for (int j = 0; j < 3; ++j) b[sp][j] = coef[(4 * sp + 1 + j) * ld + p];
+    }
+  double t[3] = {0, 0, 0};
+  for (int64_t f = f0; f < f1; ++f) {
+    double q[3] = {0, 0, 0};
+    if (live) {
+      const int64_t o = f * ld + p;
+      double d[3], H[6];
+      for (int c = 0; c < 3; ++c) d[c] = B[(1 + c) * plane + o];
+      if (gga)
+        for (int k = 0; k < 6; ++k) H[k] = B[(4 + k) * plane + o];
+      for (int sp = 0; sp < ispin; ++sp) {
+        const double X = XY[(4 * sp) * plane + o];
+        for (int k = 0; k < 3; ++k) q[k] += 2.0 * a[sp] * d[k] * X;
+        if (!gga) continue;
+        double Yj[3];
+        for (int j = 0; j < 3; ++j) Yj[j] = XY[(4 * sp + 1 + j) * plane + o];
+        for (int k = 0; k < 3; ++k) {
+          double u = 0.0;
+          for (int j = 0; j < 3; ++j) u += b[sp][j] * (H[hidx(k, j)] * X + d[k] * Yj[j]);
+          q[k] += 2.0 * u;
+        }
+      }
     }
     for (int k = 0; k < 3; ++k) {
-      double t = 0.0;
-      for (int j = 0; j < 3; ++j) t += b[j] * (H[hidx(k, j)] * X + d[k] * Yj[j]);
-      q[k] += 2.0 * t;
+      t[k] += q[k];
+      double v = q[k];
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+      if (lane == 0 && v != 0.0) atomicAdd(&gq[3 * (f - f0) + k], v);
     }
   }
-}
-
-// grid = (nbas, ld / 256): -sum over the block's points of q_mu into atom(mu)
-__global__ void k_grad_fn(bool gga, int ispin, int64_t nbas, int64_t ld, int64_t nvalid, const int* __restrict__ fatom,
-                          const double* __restrict__ B, int64_t plane, const double* __restrict__ XY,
-                          const double* __restrict__ coef, double* __restrict__ grad) {
-  __shared__ double red[3][8];
-  const int64_t f = blockIdx.x;
-  const int64_t p = (int64_t)blockIdx.y * blockDim.x + threadIdx.x;
-  double q[3] = {0, 0, 0};
-  if (p < nvalid) q_terms(gga, ispin, f, p, ld, plane, B, XY, coef, q);
-  for (int k = 0; k < 3; ++k)
-    for (int off = 16; off > 0; off >>= 1) q[k] += __shfl_down_sync(0xffffffffu, q[k], off);
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (lane == 0)
-    for (int k = 0; k < 3; ++k) red[k][warp] = q[k];
+  // host sums: one shared atomic per warp when its points share a host
+  const int h = live ? owner[p0 + p] : -1;
+  const int h0 = __shfl_sync(0xffffffffu, h, 0);
+  if (__all_sync(0xffffffffu, h == h0) && h0 >= 0) {
+    for (int k = 0; k < 3; ++k) {
+      double v = t[k];
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+      if (lane == 0) atomicAdd(&gh[3 * h0 + k], v);
+    }
+  } else if (live) {
+    for (int k = 0; k < 3; ++k) atomicAdd(&gh[3 * h + k], t[k]);
+  }
   __syncthreads();
-  if (threadIdx.x < 3) {
-    double s = 0.0;
-    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += red[threadIdx.x][i];
-    atomicAdd(grad + 3 * fatom[f] + threadIdx.x, -s);
-  }
-}
-
-// thread per point: +sum over functions of q into the point's host atom
-__global__ void k_grad_host(bool gga, int ispin, int64_t nbas, int64_t ld, int64_t p0, int64_t nvalid,
-                            const int* __restrict__ owner, const double* __restrict__ B, int64_t plane,
-                            const double* __restrict__ XY, const double* __restrict__ coef, double* __restrict__ grad) {
-  const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= nvalid) return;
-  double t[3] = {0, 0, 0};
-  for (int64_t f = 0; f < nbas; ++f) {
-    double q[3];
-    q_terms(gga, ispin, f, p, ld, plane, B, XY, coef, q);
-    for (int k = 0; k < 3; ++k) t[k] += q[k];
-  }
-  const int h = owner[p0 + p];
-  for (int k = 0; k < 3; ++k) atomicAdd(grad + 3 * h + k, t[k]);
+  for (int i = threadIdx.x; i < 3 * (int)(f1 - f0); i += blockDim.x)
+    if (gq[i] != 0.0) atomicAdd(grad + 3 * fatom[f0 + i / 3] + i % 3, -gq[i]);
+  for (int i = threadIdx.x; i < 3 * natm; i += blockDim.x)
+    if (gh[i] != 0.0) atomicAdd(grad + i, gh[i]);
 }
 
 // Thread per point.  Pass 1 stores, per atom b, the point's distance d_b,
@@ -559,13 +572,14 @@ void launch_grad_points(const XcConst& K, bool gga, int ispin, int64_t nbas, int
                                                                plane, XY, coef, ef, exc);
 }
 
-void launch_grad_orbital(bool gga, int ispin, int64_t nbas, int64_t ld, int64_t p0, int64_t nvalid,
+void launch_grad_orbital(bool gga, int ispin, int64_t nbas, int64_t ld, int64_t p0, int64_t nvalid, int natm,
                          const int* fatom, const int* owner, const double* basis, int64_t plane, const double* XY,
                          const double* coef, double* grad, cudaStream_t st) {
-  dim3 grid((unsigned)nbas, (unsigned)((ld + 255) / 256));
-  k_grad_fn<<<grid, 256, 0, st>>>(gga, ispin, nbas, ld, nvalid, fatom, basis, plane, XY, coef, grad);
-  k_grad_host<<<(unsigned)((ld + 127) / 128), 128, 0, st>>>(gga, ispin, nbas, ld, p0, nvalid, owner, basis, plane,
-                                                             XY, coef, grad);
+  const size_t smem = sizeof(double) * 3 * (kGradFB + natm);
+  if (smem > 48 * 1024) cudaFuncSetAttribute(k_grad_orb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  dim3 grid((unsigned)((nbas + kGradFB - 1) / kGradFB), (unsigned)((ld + 255) / 256));
+  k_grad_orb<<<grid, 256, smem, st>>>(gga, ispin, nbas, ld, p0, nvalid, natm, fatom, owner, basis, plane, XY, coef,
+                                      grad);
 }
 
 void launch_grad_xy(const double* basis_j, int64_t ld, const double* P, int64_t ldc, int64_t nbas, double* out,

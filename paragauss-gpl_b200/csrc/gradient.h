@@ -39,7 +39,7 @@ void launch_grad_points(const XcConst& K, bool gga, int ispin, int64_t nbas, int
                         double* coef, double* ef, double* exc, cudaStream_t st);
 
 // The orbital terms: -sum_g q to atom(mu) (fatom[mu]) and +sum_mu q to host(g).
-void launch_grad_orbital(bool gga, int ispin, int64_t nbas, int64_t ld, int64_t p0, int64_t nvalid,
+void launch_grad_orbital(bool gga, int ispin, int64_t nbas, int64_t ld, int64_t p0, int64_t nvalid, int natm,
                          const int* fatom, const int* owner, const double* basis, int64_t plane, const double* XY,
                          const double* coef, double* grad, cudaStream_t st);
 

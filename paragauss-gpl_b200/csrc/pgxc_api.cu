@@ -982,7 +982,8 @@ static int gradient_core(pgxc_ctx* c, int32_t nbas, int32_t ispin, int64_t kpad,
       }
       if (rc) break;
       launch_grad_points(a.xc, gga, ispin, nbas, ld, p0, nv, a.w, c->d_wraw, basis, plane, XY, coef, ef + p0, de, s);
-      launch_grad_orbital(gga, ispin, nbas, ld, p0, nv, dfatom, c->d_owner, basis, plane, XY, coef, dgrad, s);
+      launch_grad_orbital(gga, ispin, nbas, ld, p0, nv, c->natm, dfatom, c->d_owner, basis, plane, XY, coef, dgrad,
+                          s);
       if (cudaGetLastError() != cudaSuccess) rc = set_err(c, PGXC_ECUDA, "gradient kernel launch failed");
     }
     if (rc) break;
