@@ -269,23 +269,26 @@ def kernel_table(case, screen, tm, prec, mp, tpeak, args):
     arrays = 4 if gga else 1
     hbm = mp["hbm_gbs"]
     out = {}
+    mixed = prec != "fp64"
+    # bytes of one basis value and its gradient: phi in FP64; grad phi in FP32 in
+    # the screened INT8 build, FP64 otherwise
+    eb = 8.0 + ((12.0 if (mixed and screen is not None) else 24.0) if gga else 0.0)
     if screen is not None:
         nslots, sum_n2, ntl = screen["nslots"], screen["sum_n2"], screen["ntiles"]
         npts_t = 128.0 * ntl
         flops_x = 2.0 * 128 * sum_n2
         flops_v = flops_x if gga else 0.5 * flops_x
         # density: phi (+ grad phi) of every slot read once, rho (+ grad rho) written once
-        bytes_x = 8.0 * arrays * 128 * (nslots + ntl)
+        bytes_x = eb * 128 * nslots + 8.0 * arrays * 128 * ntl
         # potential: phi (+ grad phi) of every slot read once, A (+ B) per point
-        bytes_v = 8.0 * arrays * 128 * nslots + 8.0 * arrays * npts_t
-        bytes_b = 8.0 * arrays * 128 * nslots  # basis: phi (+ grad phi) written
+        bytes_v = eb * 128 * nslots + 8.0 * arrays * npts_t
+        bytes_b = eb * 128 * nslots  # basis: phi (+ grad phi) written
     else:
         flops_x = 2.0 * case.npts * case.nbas ** 2
         flops_v = flops_x if gga else 0.5 * flops_x
         bytes_x = 8.0 * arrays * case.npts * (case.nbas + 1)
         bytes_v = 8.0 * arrays * case.npts * (case.nbas + 1)
         bytes_b = 8.0 * arrays * case.npts * case.nbas
-    mixed = prec != "fp64"
     issued = OZAKI_PAIRS if mixed else 1
     names = {"density": "k_sm_density" if mixed else ("k_sdensity" if screen is not None else "k_density"),
              "potential": "k_sm_vpot" if mixed else ("k_svpot" if screen is not None else "k_vpot")}
@@ -301,7 +304,7 @@ def kernel_table(case, screen, tm, prec, mp, tpeak, args):
     if mixed and screen is not None:
         # Z = A phi (+ B . grad phi) and the digits of Z and phi: the rest of the potential phase
         zms = tm["potential_ms"] - tm["vgemm_ms"]
-        zb = 8.0 * arrays * 128 * nslots + 8.0 * arrays * npts_t + 10.0 * 128 * nslots
+        zb = eb * 128 * nslots + 8.0 * arrays * npts_t + 10.0 * 128 * nslots
         out["k_sm_zquant"] = {"ms": zms, "algorithmic_bytes": zb, "achieved_gbs": zb / (zms * 1e-3) / 1e9,
                               "hbm_frac": zb / (zms * 1e-3) / 1e9 / hbm,
                               "note": "phase time less the contraction kernel (includes the packing kernel)"}

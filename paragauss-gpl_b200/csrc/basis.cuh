@@ -322,15 +322,17 @@ __device__ __forceinline__ unsigned long long item_u64(unsigned w, int k) {
   return ((unsigned long long)hi << 32) | lo;
 }
 
-template <int L, bool GRAD>
+// GT: the element type of the gradient planes (double; float in the INT8
+// build, whose potential and density gradient tolerate 24-bit gradients).
+template <int L, bool GRAD, typename GT = double>
 __global__ void __launch_bounds__(128) k_basis_items(const BasisItem* __restrict__ items, int64_t nitems,
                                                      const double* __restrict__ exps, const double* __restrict__ norms,
                                                      const double* __restrict__ contr,
                                                      const int2* __restrict__ rng, DevSA sa,
                                                      const double* __restrict__ qx, const double* __restrict__ qy,
                                                      const double* __restrict__ qz, int64_t s0, int64_t t0,
-                                                     double* __restrict__ phi, double* __restrict__ gx,
-                                                     double* __restrict__ gy, double* __restrict__ gz,
+                                                     double* __restrict__ phi, GT* __restrict__ gx,
+                                                     GT* __restrict__ gy, GT* __restrict__ gz,
                                                      unsigned long long* __restrict__ pmax) {
   const int lane = threadIdx.x & 31;
   const int64_t per = (nitems + gridDim.x - 1) / gridDim.x;
@@ -408,9 +410,9 @@ __global__ void __launch_bounds__(128) k_basis_items(const BasisItem* __restrict
         vmax = fmax(vmax, fabs(Ys[k] * Rv));
         if (GRAD) {
           const double h = Ys[k] * dRv;
-          gx[o] = x * h + dYs[0][k] * Rv;
-          gy[o] = y * h + dYs[1][k] * Rv;
-          gz[o] = z * h + dYs[2][k] * Rv;
+          gx[o] = (GT)(x * h + dYs[0][k] * Rv);
+          gy[o] = (GT)(y * h + dYs[1][k] * Rv);
+          gz[o] = (GT)(z * h + dYs[2][k] * Rv);
         }
       };
       if (seg) {

@@ -94,19 +94,19 @@ __global__ void __launch_bounds__(128) k_tile_atom_d2(const double* __restrict__
 // ---------------------------------------------------------------------------
 // Zero the padding slots of each tile (the slots after its listed
 // functions: tso[t] + listed[t] .. tso[t+1]).  grid = chunk tiles.
-template <bool GGA>
+template <bool GGA, typename GT = double>
 __global__ void __launch_bounds__(128) k_pad_zero(const int64_t* __restrict__ tso, const int* __restrict__ listed,
                                                   int64_t t0, int64_t s0, double* __restrict__ phi,
-                                                  double* __restrict__ gx, double* __restrict__ gy,
-                                                  double* __restrict__ gz) {
+                                                  GT* __restrict__ gx, GT* __restrict__ gy,
+                                                  GT* __restrict__ gz) {
   const int64_t t = t0 + blockIdx.x;
   const int64_t r0 = tso[t] - s0 + listed[t], r1 = tso[t + 1] - s0;
   for (int64_t e = r0 * 128 + threadIdx.x; e < r1 * 128; e += 128) {
     phi[e] = 0.0;
     if (GGA) {
-      gx[e] = 0.0;
-      gy[e] = 0.0;
-      gz[e] = 0.0;
+      gx[e] = (GT)0;
+      gy[e] = (GT)0;
+      gz[e] = (GT)0;
     }
   }
 }
@@ -435,6 +435,12 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
   sp->gga = in.gga;
   sp->mgga = in.mgga;
   sp->functional = in.functional;
+  // The INT8 build keeps grad phi in FP32 (phi stays FP64): its density
+  // gradient and potential then move 12 fewer bytes per basis value, within
+  // the mixed-mode bars (measured on CH60-PBE: |dE_xc| 9.7e-8 Eh, max |dV_xc|
+  // 3.1e-8 against the FP64 build; FP32 phi too would give 1.1e-6 Eh).  The
+  // meta-GGA tau contractions run on the FP64 kernels and keep FP64 gradients.
+  sp->gf32 = in.precision != PGXC_PREC_FP64 && in.gga && !in.mgga;
   sp->ispin = in.ispin;
   sp->nbas = in.nbas;
   sp->keep = in.keep_basis;
@@ -570,7 +576,8 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
   SP_TRY(cudaMemGetInfo(&freeb, &totb), "cudaMemGetInfo");
   if (sp->keep) {
     // resident basis values and point digits of every slot: phi (+ grad phi), INT8 digits
-    const double need = (double)(sp->nslots + kSlack) * 128 * (8.0 * (in.gga ? 4 : 1) + (mixed ? 5.0 : 0.0));
+    const double gb = in.gga ? 3.0 * (sp->gf32 ? 4.0 : 8.0) : 0.0;
+    const double need = (double)(sp->nslots + kSlack) * 128 * (8.0 + gb + (mixed ? 5.0 : 0.0));
     if (need > 0.6 * (double)freeb) {
       err = "screened build: the basis values of the whole grid (" + std::to_string((int64_t)(need / 1e9)) +
             " GB) do not fit beside the build's buffers; create the context without keep_orbitals";
@@ -579,7 +586,7 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
     }
     freeb -= (size_t)need;
   }
-  const int64_t per_slot = 128 * 8 * (in.gga ? 5 : 2) + (mixed ? screen_mixed_bytes_per_slot() : 0);
+  const int64_t per_slot = 128 * (16 + (in.gga ? 3 * (sp->gf32 ? 4 : 8) : 0)) + (mixed ? screen_mixed_bytes_per_slot() : 0);
   const int64_t per_tile = 128 * 8 * 8 * in.ispin + (mixed ? screen_mixed_bytes_per_tile() : 0);
   int64_t budget_slots = (int64_t)(0.45 * (double)freeb) / per_slot;
   budget_slots = std::max<int64_t>(budget_slots, sp->max_n);
@@ -644,7 +651,14 @@ int screen_create(ScreenPlan** out, const ScreenInput& in, const BuildArgs& a, c
   SP_TRY(sp_alloc(sp, &sp->Z, rows), "cudaMalloc (Z)");
   SP_TRY(cudaMemset(sp->phi, 0, sizeof(double) * brows), "memset");
   SP_TRY(cudaMemset(sp->Z, 0, sizeof(double) * rows), "memset");
-  if (in.gga) {
+  if (in.gga && sp->gf32) {
+    SP_TRY(sp_alloc(sp, &sp->fx, brows), "cudaMalloc (grad phi)");
+    SP_TRY(sp_alloc(sp, &sp->fy, brows), "cudaMalloc (grad phi)");
+    SP_TRY(sp_alloc(sp, &sp->fz, brows), "cudaMalloc (grad phi)");
+    SP_TRY(cudaMemset(sp->fx, 0, sizeof(float) * brows), "memset");
+    SP_TRY(cudaMemset(sp->fy, 0, sizeof(float) * brows), "memset");
+    SP_TRY(cudaMemset(sp->fz, 0, sizeof(float) * brows), "memset");
+  } else if (in.gga) {
     SP_TRY(sp_alloc(sp, &sp->gx, brows), "cudaMalloc (grad phi)");
     SP_TRY(sp_alloc(sp, &sp->gy, brows), "cudaMalloc (grad phi)");
     SP_TRY(sp_alloc(sp, &sp->gz, brows), "cudaMalloc (grad phi)");
@@ -743,9 +757,13 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
     // this chunk's rows of the basis arrays (resident: the chunk's place among all slots)
     const int64_t so = sp->keep ? s0 : 0, to = sp->keep ? t0 : 0;
     double* phi = sp->phi + so * 128;
-    double* gxc = gga ? sp->gx + so * 128 : nullptr;
-    double* gyc = gga ? sp->gy + so * 128 : nullptr;
-    double* gzc = gga ? sp->gz + so * 128 : nullptr;
+    const bool gf = sp->gf32;
+    double* gxc = gga && !gf ? sp->gx + so * 128 : nullptr;
+    double* gyc = gga && !gf ? sp->gy + so * 128 : nullptr;
+    double* gzc = gga && !gf ? sp->gz + so * 128 : nullptr;
+    float* fxc = gga && gf ? sp->fx + so * 128 : nullptr;
+    float* fyc = gga && gf ? sp->fy + so * 128 : nullptr;
+    float* fzc = gga && gf ? sp->fz + so * 128 : nullptr;
     if (timed) SR_TRY(cudaEventRecord(ev[2], st));
     // K1
     if (!eval_basis) {
@@ -758,21 +776,28 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
         if (i1 <= i0) return;
         // persistent-style blocks, each walking a contiguous range of items
         const unsigned nb = (unsigned)std::min<int64_t>(i1 - i0, (int64_t)sp->nsm * kBasisBlocksPerSM);
-        if (gga)
+        if (gga && gf)
+          k_basis_items<L, true, float><<<nb, 128, 0, st>>>(sp->items[L] + i0, i1 - i0, a.exps, a.norms, a.contr,
+                                                            a.rng, a.sa, sp->qx, sp->qy, sp->qz, s0, t0, phi, fxc, fyc,
+                                                            fzc, sp->pmax);
+        else if (gga)
           k_basis_items<L, true><<<nb, 128, 0, st>>>(sp->items[L] + i0, i1 - i0, a.exps, a.norms, a.contr, a.rng,
                                                      a.sa, sp->qx, sp->qy, sp->qz, s0, t0, phi, gxc, gyc, gzc, sp->pmax);
         else
-          k_basis_items<L, false><<<nb, 128, 0, st>>>(sp->items[L] + i0, i1 - i0, a.exps, a.norms, a.contr, a.rng,
-                                                      a.sa, sp->qx, sp->qy, sp->qz, s0, t0, phi, nullptr,
-                                                      nullptr, nullptr, sp->pmax);
+          k_basis_items<L, false, double><<<nb, 128, 0, st>>>(sp->items[L] + i0, i1 - i0, a.exps, a.norms, a.contr,
+                                                              a.rng, a.sa, sp->qx, sp->qy, sp->qz, s0, t0, phi,
+                                                              (double*)nullptr, (double*)nullptr, (double*)nullptr,
+                                                              sp->pmax);
         ++T.launches;
       };
       launch_l(std::integral_constant<int, 0>());
       launch_l(std::integral_constant<int, 1>());
       launch_l(std::integral_constant<int, 2>());
       launch_l(std::integral_constant<int, 3>());
-      if (gga) k_pad_zero<true><<<(unsigned)nt, 128, 0, st>>>(sp->tso, sp->listed, t0, s0, phi, gxc, gyc, gzc);
-      else k_pad_zero<false><<<(unsigned)nt, 128, 0, st>>>(sp->tso, sp->listed, t0, s0, phi, nullptr, nullptr, nullptr);
+      if (gga && gf) k_pad_zero<true, float><<<(unsigned)nt, 128, 0, st>>>(sp->tso, sp->listed, t0, s0, phi, fxc, fyc, fzc);
+      else if (gga) k_pad_zero<true><<<(unsigned)nt, 128, 0, st>>>(sp->tso, sp->listed, t0, s0, phi, gxc, gyc, gzc);
+      else k_pad_zero<false, double><<<(unsigned)nt, 128, 0, st>>>(sp->tso, sp->listed, t0, s0, phi, (double*)nullptr,
+                                                                   (double*)nullptr, (double*)nullptr);
       ++T.launches;
       if (sp->mixed)
         T.launches += screen_mixed_basis(sp->mixed, sp->tso, sp->slot_fn, t0, nt, s0, phi, sp->pmax, so, to, st);
@@ -783,8 +808,12 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
     for (int s = 0; s < ispin; ++s) {
       if (sp->mixed) {
         if (s > 0) T.launches += screen_mixed_gather(sp->mixed, sp->tso, sp->slot_fn, t0, nt, s0, s, st);
-        T.launches += screen_mixed_density(sp->mixed, sp->tso, sp->slot_fn, t0, nt, s0, phi, gxc, gyc, gzc,
-                                           b[s].rho, b[s].grx, b[s].gry, b[s].grz, so, to, st);
+        if (gf)
+          T.launches += screen_mixed_density(sp->mixed, sp->tso, sp->slot_fn, t0, nt, s0, phi, fxc, fyc, fzc,
+                                             b[s].rho, b[s].grx, b[s].gry, b[s].grz, so, to, st);
+        else
+          T.launches += screen_mixed_density(sp->mixed, sp->tso, sp->slot_fn, t0, nt, s0, phi, gxc, gyc, gzc,
+                                             b[s].rho, b[s].grx, b[s].gry, b[s].grz, so, to, st);
       } else {
         const int smem = gemm_smem_bytes<false, false>() + (int)sizeof(int) * sp->max_n;
         dim3 grid((unsigned)nt, 2);
@@ -834,9 +863,14 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
       double* Vs = sp->V + s * nb2;
       cudaEvent_t k0 = timed ? ev[7 + 3 * s] : nullptr, k1 = timed ? ev[8 + 3 * s] : nullptr;
       if (sp->mixed) {
-        T.launches += screen_mixed_potential(sp->mixed, sp->tso, sp->slot_fn, sp->slot_tile, t0, nt, s0, ns, phi,
-                                             gxc, gyc, gzc, b[s].A, b[s].Bx, b[s].By, b[s].Bz, Vs, sp->nbas,
-                                             st, k0, k1);
+        if (gf)
+          T.launches += screen_mixed_potential(sp->mixed, sp->tso, sp->slot_fn, sp->slot_tile, t0, nt, s0, ns, phi,
+                                               fxc, fyc, fzc, b[s].A, b[s].Bx, b[s].By, b[s].Bz, Vs, sp->nbas,
+                                               st, k0, k1);
+        else
+          T.launches += screen_mixed_potential(sp->mixed, sp->tso, sp->slot_fn, sp->slot_tile, t0, nt, s0, ns, phi,
+                                               gxc, gyc, gzc, b[s].A, b[s].Bx, b[s].By, b[s].Bz, Vs, sp->nbas,
+                                               st, k0, k1);
       } else {
         const unsigned nbk = (unsigned)std::max<int64_t>(1, std::min<int64_t>((ns * 128 + 255) / 256, 148 * 32));
         if (gga)
@@ -1067,7 +1101,8 @@ struct ScreenSet {
   SetSeg* segs = nullptr;
   int64_t* b_off = nullptr;
   // chunk buffers
-  double *phi = nullptr, *gx = nullptr, *gy = nullptr, *gz = nullptr;
+  double* phi = nullptr;
+  float *gx = nullptr, *gy = nullptr, *gz = nullptr;  // grad phi in 32 bits (the INT8 build's)
   double* pt = nullptr;
   double* partial = nullptr;
   unsigned long long* pmax = nullptr;
@@ -1225,7 +1260,7 @@ int screen_set_create(ScreenSet** out, const std::vector<SetMember>& members, in
   size_t freeb = 0, totb = 0;
   SS_TRY(cudaMemGetInfo(&freeb, &totb), "cudaMemGetInfo");
   const bool any_gga = std::any_of(S->groups.begin(), S->groups.end(), [](const ScreenSet::Group& g) { return g.gga; });
-  const int64_t per_slot = 128 * 8 * (any_gga ? 4 : 1) + screen_mixed_bytes_per_slot();
+  const int64_t per_slot = 128 * (8 + (any_gga ? 12 : 0)) + screen_mixed_bytes_per_slot();
   const int64_t per_tile = 128 * 8 * 8 + screen_mixed_bytes_per_tile() + 128 * 8 + 16;
   int64_t budget_slots = std::max<int64_t>((int64_t)(0.40 * (double)freeb) / per_slot, S->max_n);
   int64_t budget_tiles = std::max<int64_t>(1, (int64_t)(0.05 * (double)freeb) / per_tile);
@@ -1292,9 +1327,9 @@ int screen_set_create(ScreenSet** out, const std::vector<SetMember>& members, in
     SS_TRY(alloc(&S->gx, rows), "cudaMalloc (grad phi)");
     SS_TRY(alloc(&S->gy, rows), "cudaMalloc (grad phi)");
     SS_TRY(alloc(&S->gz, rows), "cudaMalloc (grad phi)");
-    SS_TRY(cudaMemsetAsync(S->gx, 0, sizeof(double) * rows, st), "memset");
-    SS_TRY(cudaMemsetAsync(S->gy, 0, sizeof(double) * rows, st), "memset");
-    SS_TRY(cudaMemsetAsync(S->gz, 0, sizeof(double) * rows, st), "memset");
+    SS_TRY(cudaMemsetAsync(S->gx, 0, sizeof(float) * rows, st), "memset");
+    SS_TRY(cudaMemsetAsync(S->gy, 0, sizeof(float) * rows, st), "memset");
+    SS_TRY(cudaMemsetAsync(S->gz, 0, sizeof(float) * rows, st), "memset");
   }
   SS_TRY(alloc(&S->pt, 8 * (size_t)S->chunk_tiles * 128), "cudaMalloc");
   SS_TRY(alloc(&S->partial, 2 * (size_t)S->chunk_tiles), "cudaMalloc");
@@ -1324,9 +1359,9 @@ int screen_set_run(ScreenSet* S, cudaStream_t st, std::string& err) {
     const ScreenSet::Group& g = S->groups[(size_t)c.group];
     const bool gga = g.gga;
     const int64_t t0 = c.t0, nt = c.t1 - c.t0, s0 = c.s0;
-    double* gxc = gga ? S->gx : nullptr;
-    double* gyc = gga ? S->gy : nullptr;
-    double* gzc = gga ? S->gz : nullptr;
+    float* gxc = gga ? S->gx : nullptr;
+    float* gyc = gga ? S->gy : nullptr;
+    float* gzc = gga ? S->gz : nullptr;
     cudaMemsetAsync(S->pmax, 0, sizeof(unsigned long long) * nt * 128, st);
     auto launch_l = [&](auto Lc) {
       constexpr int L = decltype(Lc)::value;
@@ -1334,20 +1369,22 @@ int screen_set_run(ScreenSet* S, cudaStream_t st, std::string& err) {
       if (n <= 0) return;
       const unsigned nb = (unsigned)std::min<int64_t>(n, (int64_t)S->nsm * kBasisBlocksPerSM);
       if (gga)
-        k_basis_items<L, true><<<nb, 128, 0, st>>>(S->items[L] + i0, n, S->exps, S->norms, S->contr, S->rng, S->sa,
-                                                   S->qx, S->qy, S->qz, s0, t0, S->phi, gxc, gyc, gzc, S->pmax);
+        k_basis_items<L, true, float><<<nb, 128, 0, st>>>(S->items[L] + i0, n, S->exps, S->norms, S->contr, S->rng,
+                                                          S->sa, S->qx, S->qy, S->qz, s0, t0, S->phi, gxc, gyc, gzc,
+                                                          S->pmax);
       else
-        k_basis_items<L, false><<<nb, 128, 0, st>>>(S->items[L] + i0, n, S->exps, S->norms, S->contr, S->rng, S->sa,
-                                                    S->qx, S->qy, S->qz, s0, t0, S->phi, nullptr, nullptr, nullptr,
-                                                    S->pmax);
+        k_basis_items<L, false, float><<<nb, 128, 0, st>>>(S->items[L] + i0, n, S->exps, S->norms, S->contr, S->rng,
+                                                           S->sa, S->qx, S->qy, S->qz, s0, t0, S->phi, (float*)nullptr,
+                                                           (float*)nullptr, (float*)nullptr, S->pmax);
       ++launches;
     };
     launch_l(std::integral_constant<int, 0>());
     launch_l(std::integral_constant<int, 1>());
     launch_l(std::integral_constant<int, 2>());
     launch_l(std::integral_constant<int, 3>());
-    if (gga) k_pad_zero<true><<<(unsigned)nt, 128, 0, st>>>(S->tso, S->listed, t0, s0, S->phi, gxc, gyc, gzc);
-    else k_pad_zero<false><<<(unsigned)nt, 128, 0, st>>>(S->tso, S->listed, t0, s0, S->phi, nullptr, nullptr, nullptr);
+    if (gga) k_pad_zero<true, float><<<(unsigned)nt, 128, 0, st>>>(S->tso, S->listed, t0, s0, S->phi, gxc, gyc, gzc);
+    else k_pad_zero<false, float><<<(unsigned)nt, 128, 0, st>>>(S->tso, S->listed, t0, s0, S->phi, (float*)nullptr,
+                                                                (float*)nullptr, (float*)nullptr);
     ++launches;
     screen_mixed_set_gga(S->mixed, gga);
     launches += screen_mixed_basis(S->mixed, S->tso, S->slot_fn, t0, nt, s0, S->phi, S->pmax, 0, 0, st, S->tile_mol,

@@ -276,13 +276,15 @@ __device__ __forceinline__ void read_acc24(uint32_t taddr, int half, double (&x)
 // size); the copy / MMA / epilogue pipeline runs on across tile boundaries.
 // rho and grad rho are accumulated with atomics (the two column halves of a
 // point and nothing else), so they must be zero on entry.
-template <bool GGA>
+// GT: element type of the grad phi planes (staged beside phi in the same
+// ring entry: phi in doubles, then the three gradient blocks in GT).
+template <bool GGA, typename GT>
 __global__ void __launch_bounds__(kDensThreads, 1)
     k_sm_density(const int64_t* __restrict__ tso, const int* __restrict__ slot_fn, int64_t t0, int64_t nt,
                  int64_t s0, const int8_t* __restrict__ tA, const int* __restrict__ e_pt,
                  const int8_t* __restrict__ tB, const int64_t* __restrict__ b_off, const double* __restrict__ ps,
-                 const double* __restrict__ phi, const double* __restrict__ gx, const double* __restrict__ gy,
-                 const double* __restrict__ gz, double* __restrict__ rho, double* __restrict__ grx,
+                 const double* __restrict__ phi, const GT* __restrict__ gx, const GT* __restrict__ gy,
+                 const GT* __restrict__ gz, double* __restrict__ rho, double* __restrict__ grx,
                  double* __restrict__ gry, double* __restrict__ grz, int* err) {
   extern __shared__ __align__(1024) uint8_t smem_raw[];
   DensSmem& S = *reinterpret_cast<DensSmem*>(smem_raw);
@@ -330,13 +332,15 @@ __global__ void __launch_bounds__(kDensThreads, 1)
                 continue;
               }
               const uint32_t bytes = (uint32_t)nc * 128 * sizeof(double);
+              const uint32_t gbytes = (uint32_t)nc * 128 * sizeof(GT);
               const int64_t off = (sb + c0) * 128;
-              tc::mbar_expect_tx(&S.e_full[r], (GGA ? 4 : 1) * bytes);
+              tc::mbar_expect_tx(&S.e_full[r], bytes + (GGA ? 3 * gbytes : 0));
               tc::bulk_g2s(S.e[r], phi + off, bytes, &S.e_full[r]);
               if (GGA) {
-                tc::bulk_g2s(S.e[r] + kECols * 128, gx + off, bytes, &S.e_full[r]);
-                tc::bulk_g2s(S.e[r] + 2 * kECols * 128, gy + off, bytes, &S.e_full[r]);
-                tc::bulk_g2s(S.e[r] + 3 * kECols * 128, gz + off, bytes, &S.e_full[r]);
+                GT* eg = reinterpret_cast<GT*>(S.e[r] + kECols * 128);
+                tc::bulk_g2s(eg, gx + off, gbytes, &S.e_full[r]);
+                tc::bulk_g2s(eg + kECols * 128, gy + off, gbytes, &S.e_full[r]);
+                tc::bulk_g2s(eg + 2 * kECols * 128, gz + off, gbytes, &S.e_full[r]);
               }
             }
         }
@@ -430,15 +434,16 @@ __global__ void __launch_bounds__(kDensThreads, 1)
           }
           const int c0 = j * kN + half * 24 + u * kECols;
           const double* eb = S.e[r];
+          const GT* eg = reinterpret_cast<const GT*>(eb + kECols * 128);
 #pragma unroll
           for (int v = 0; v < kECols; ++v) {
             const double X = x[u * kECols + v] * (rs * __shfl_sync(0xffffffffu, psl, u * kECols + v));
             if (c0 + v < n) {
               r_acc += X * eb[v * 128 + row];
               if (GGA) {
-                g_acc[0] += X * eb[(kECols + v) * 128 + row];
-                g_acc[1] += X * eb[(2 * kECols + v) * 128 + row];
-                g_acc[2] += X * eb[(3 * kECols + v) * 128 + row];
+                g_acc[0] += X * (double)eg[v * 128 + row];
+                g_acc[1] += X * (double)eg[(kECols + v) * 128 + row];
+                g_acc[2] += X * (double)eg[(2 * kECols + v) * 128 + row];
               }
             }
           }
@@ -470,10 +475,10 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
-template <bool GGA>
+template <bool GGA, typename GT>
 __global__ void __launch_bounds__(256, 3) k_sm_zquant(const int64_t* __restrict__ tso, int64_t t0, int64_t s0,
-                                                   const double* __restrict__ phi, const double* __restrict__ gx,
-                                                   const double* __restrict__ gy, const double* __restrict__ gz,
+                                                   const double* __restrict__ phi, const GT* __restrict__ gx,
+                                                   const GT* __restrict__ gy, const GT* __restrict__ gz,
                                                    const double* __restrict__ A, const double* __restrict__ Bx,
                                                    const double* __restrict__ By, const double* __restrict__ Bz,
                                                    int8_t* __restrict__ tZ, int8_t* __restrict__ tF,
@@ -510,13 +515,18 @@ __global__ void __launch_bounds__(256, 3) k_sm_zquant(const int64_t* __restrict_
       if (GGA) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          const double* g = c == 0 ? gx : (c == 1 ? gy : gz);
-          const double2 ga = *reinterpret_cast<const double2*>(g + o);
-          const double2 gb = *reinterpret_cast<const double2*>(g + o + 2);
-          z[h][0] = (c == 0 ? 0.0 : z[h][0]) + sB[c][p0] * ga.x;
-          z[h][1] = (c == 0 ? 0.0 : z[h][1]) + sB[c][p0 + 1] * ga.y;
-          z[h][2] = (c == 0 ? 0.0 : z[h][2]) + sB[c][p0 + 2] * gb.x;
-          z[h][3] = (c == 0 ? 0.0 : z[h][3]) + sB[c][p0 + 3] * gb.y;
+          const GT* g = c == 0 ? gx : (c == 1 ? gy : gz);
+          double gv[4];
+          if constexpr (sizeof(GT) == 4) {
+            const float4 q = *reinterpret_cast<const float4*>(g + o);
+            gv[0] = q.x; gv[1] = q.y; gv[2] = q.z; gv[3] = q.w;
+          } else {
+            const double2 ga = *reinterpret_cast<const double2*>(g + o);
+            const double2 gb = *reinterpret_cast<const double2*>(g + o + 2);
+            gv[0] = ga.x; gv[1] = ga.y; gv[2] = gb.x; gv[3] = gb.y;
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) z[h][u] = (c == 0 ? 0.0 : z[h][u]) + sB[c][p0 + u] * gv[u];
         }
       }
     }
@@ -782,8 +792,10 @@ int screen_mixed_create(ScreenMixed** out, const ScreenMixedInput& in, std::stri
   static_assert(sizeof(DensSmem) <= tc::kWholeSmSmem && sizeof(VSmem) <= tc::kWholeSmSmem, "smem");
   const int dsm = tc::kWholeSmSmem;
   raise_smem_limit(k_sm_gather_B, 4 * in.max_n);
-  cudaFuncSetAttribute(k_sm_density<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm);
-  cudaFuncSetAttribute(k_sm_density<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm);
+  cudaFuncSetAttribute(k_sm_density<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm);
+  cudaFuncSetAttribute(k_sm_density<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm);
+  cudaFuncSetAttribute(k_sm_density<true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm);
+  cudaFuncSetAttribute(k_sm_density<false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm);
   cudaFuncSetAttribute(k_sm_vpot<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kWholeSmSmem);
   cudaFuncSetAttribute(k_sm_vpot<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kWholeSmSmem);
   cudaFuncSetAttribute(k_sm_vpot<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc::kWholeSmSmem);
@@ -831,9 +843,12 @@ int screen_mixed_gather(ScreenMixed* m, const int64_t* tso, const int* slot_fn, 
   return 1;
 }
 
-int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
-                         const double* phi, const double* gx, const double* gy, const double* gz, double* rho,
-                         double* grx, double* gry, double* grz, int64_t so, int64_t to, cudaStream_t st) {
+namespace {
+
+template <typename GT>
+int mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
+                  const double* phi, const GT* gx, const GT* gy, const GT* gz, double* rho, double* grx, double* gry,
+                  double* grz, int64_t so, int64_t to, cudaStream_t st) {
   const int8_t* tA = m->tA + so * kDigBytesPerSlot;
   const int* e_pt = m->e_pt + to * 128;
   cudaMemsetAsync(rho, 0, sizeof(double) * nt * 128, st);
@@ -845,28 +860,26 @@ int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn,
   const unsigned grid = (unsigned)std::min<int64_t>(nt, m->nsm);
   const int smem = tc::kWholeSmSmem;
   if (m->gga)
-    k_sm_density<true><<<grid, kDensThreads, smem, st>>>(tso, slot_fn, t0, nt, s0, tA, e_pt, m->tB, m->b_off,
-                                                         m->ps, phi, gx, gy, gz, rho, grx, gry, grz, m->err);
+    k_sm_density<true, GT><<<grid, kDensThreads, smem, st>>>(tso, slot_fn, t0, nt, s0, tA, e_pt, m->tB, m->b_off,
+                                                             m->ps, phi, gx, gy, gz, rho, grx, gry, grz, m->err);
   else
-    k_sm_density<false><<<grid, kDensThreads, smem, st>>>(tso, slot_fn, t0, nt, s0, tA, e_pt, m->tB, m->b_off,
-                                                          m->ps, phi, nullptr, nullptr, nullptr, rho, nullptr,
-                                                          nullptr, nullptr, m->err);
+    k_sm_density<false, GT><<<grid, kDensThreads, smem, st>>>(tso, slot_fn, t0, nt, s0, tA, e_pt, m->tB, m->b_off,
+                                                              m->ps, phi, nullptr, nullptr, nullptr, rho, nullptr,
+                                                              nullptr, nullptr, m->err);
   return 1;
 }
 
-int screen_mixed_potential(ScreenMixed* m, const int64_t* tso, const int* slot_fn, const int* slot_tile, int64_t t0,
-                           int64_t nt, int64_t s0, int64_t ns, const double* phi, const double* gx, const double* gy,
-                           const double* gz, const double* A, const double* Bx, const double* By, const double* Bz,
-                           double* V, int64_t ldv, cudaStream_t st, cudaEvent_t k0, cudaEvent_t k1,
-                           const int* tile_mol, const SetMolDev* mols) {
-  (void)slot_tile;
-  (void)ns;
+template <typename GT>
+int mixed_potential(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
+                    const double* phi, const GT* gx, const GT* gy, const GT* gz, const double* A, const double* Bx,
+                    const double* By, const double* Bz, double* V, int64_t ldv, cudaStream_t st, cudaEvent_t k0,
+                    cudaEvent_t k1, const int* tile_mol, const SetMolDev* mols) {
   if (m->gga)
-    k_sm_zquant<true><<<(unsigned)nt, 256, 0, st>>>(tso, t0, s0, phi, gx, gy, gz, A, Bx, By, Bz, m->tZ, m->tF,
-                                                    m->zs, m->fs);
+    k_sm_zquant<true, GT><<<(unsigned)nt, 256, 0, st>>>(tso, t0, s0, phi, gx, gy, gz, A, Bx, By, Bz, m->tZ, m->tF,
+                                                        m->zs, m->fs);
   else
-    k_sm_zquant<false><<<(unsigned)nt, 256, 0, st>>>(tso, t0, s0, phi, nullptr, nullptr, nullptr, A, nullptr,
-                                                     nullptr, nullptr, m->tZ, m->tF, m->zs, m->fs);
+    k_sm_zquant<false, GT><<<(unsigned)nt, 256, 0, st>>>(tso, t0, s0, phi, nullptr, nullptr, nullptr, A, nullptr,
+                                                         nullptr, nullptr, m->tZ, m->tF, m->zs, m->fs);
   if (k0) cudaEventRecord(k0, st);
   const unsigned grid = (unsigned)std::min<int64_t>(nt, m->nsm);
   auto launch = [&](auto kern) {
@@ -882,6 +895,40 @@ int screen_mixed_potential(ScreenMixed* m, const int64_t* tso, const int* slot_f
   }
   if (k1) cudaEventRecord(k1, st);
   return 2;
+}
+
+}  // namespace
+
+int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
+                         const double* phi, const double* gx, const double* gy, const double* gz, double* rho,
+                         double* grx, double* gry, double* grz, int64_t so, int64_t to, cudaStream_t st) {
+  return mixed_density<double>(m, tso, slot_fn, t0, nt, s0, phi, gx, gy, gz, rho, grx, gry, grz, so, to, st);
+}
+int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
+                         const double* phi, const float* gx, const float* gy, const float* gz, double* rho,
+                         double* grx, double* gry, double* grz, int64_t so, int64_t to, cudaStream_t st) {
+  return mixed_density<float>(m, tso, slot_fn, t0, nt, s0, phi, gx, gy, gz, rho, grx, gry, grz, so, to, st);
+}
+
+int screen_mixed_potential(ScreenMixed* m, const int64_t* tso, const int* slot_fn, const int* slot_tile, int64_t t0,
+                           int64_t nt, int64_t s0, int64_t ns, const double* phi, const double* gx, const double* gy,
+                           const double* gz, const double* A, const double* Bx, const double* By, const double* Bz,
+                           double* V, int64_t ldv, cudaStream_t st, cudaEvent_t k0, cudaEvent_t k1,
+                           const int* tile_mol, const SetMolDev* mols) {
+  (void)slot_tile;
+  (void)ns;
+  return mixed_potential<double>(m, tso, slot_fn, t0, nt, s0, phi, gx, gy, gz, A, Bx, By, Bz, V, ldv, st, k0, k1,
+                                 tile_mol, mols);
+}
+int screen_mixed_potential(ScreenMixed* m, const int64_t* tso, const int* slot_fn, const int* slot_tile, int64_t t0,
+                           int64_t nt, int64_t s0, int64_t ns, const double* phi, const float* gx, const float* gy,
+                           const float* gz, const double* A, const double* Bx, const double* By, const double* Bz,
+                           double* V, int64_t ldv, cudaStream_t st, cudaEvent_t k0, cudaEvent_t k1,
+                           const int* tile_mol, const SetMolDev* mols) {
+  (void)slot_tile;
+  (void)ns;
+  return mixed_potential<float>(m, tso, slot_fn, t0, nt, s0, phi, gx, gy, gz, A, Bx, By, Bz, V, ldv, st, k0, k1,
+                                tile_mol, mols);
 }
 
 void screen_mixed_p8(ScreenMixed* m, int spin, const unsigned long long** P8, const int** e_P) {

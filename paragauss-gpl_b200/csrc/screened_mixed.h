@@ -63,12 +63,22 @@ int screen_mixed_gather(ScreenMixed* m, const int64_t* tso, const int* slot_fn, 
 int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
                          const double* phi, const double* gx, const double* gy, const double* gz, double* rho,
                          double* grx, double* gry, double* grz, int64_t so, int64_t to, cudaStream_t st);
+// the same with 32-bit gradient planes (the INT8 build's basis values: phi in
+// FP64, grad phi in FP32)
+int screen_mixed_density(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int64_t t0, int64_t nt, int64_t s0,
+                         const double* phi, const float* gx, const float* gy, const float* gz, double* rho,
+                         double* grx, double* gry, double* grz, int64_t so, int64_t to, cudaStream_t st);
 // Z digits (per-slot scales), then H[S_t, S_t] += Z_t^T phi_t scatter-added into V;
 // records k0 / k1 around the contraction kernel
 // (with tile_mol: into mols[tile_mol[t]].V of each tile t instead of V)
 int screen_mixed_potential(ScreenMixed* m, const int64_t* tso, const int* slot_fn, const int* slot_tile, int64_t t0,
                            int64_t nt, int64_t s0, int64_t ns, const double* phi, const double* gx, const double* gy,
                            const double* gz, const double* A, const double* Bx, const double* By, const double* Bz,
+                           double* V, int64_t ldv, cudaStream_t st, cudaEvent_t k0, cudaEvent_t k1,
+                           const int* tile_mol = nullptr, const SetMolDev* mols = nullptr);
+int screen_mixed_potential(ScreenMixed* m, const int64_t* tso, const int* slot_fn, const int* slot_tile, int64_t t0,
+                           int64_t nt, int64_t s0, int64_t ns, const double* phi, const float* gx, const float* gy,
+                           const float* gz, const double* A, const double* Bx, const double* By, const double* Bz,
                            double* V, int64_t ldv, cudaStream_t st, cudaEvent_t k0, cudaEvent_t k1,
                            const int* tile_mol = nullptr, const SetMolDev* mols = nullptr);
 // the digits of P_spin and their row scales (read by a set's gather)

@@ -42,6 +42,9 @@ struct ScreenPlan {
   int64_t chunk_slots = 0, chunk_tiles = 0;        // buffer capacities
   // device, per chunk
   double *phi = nullptr, *gx = nullptr, *gy = nullptr, *gz = nullptr, *Z = nullptr;
+  // INT8 build (not a meta-GGA): grad phi in 32-bit planes instead of gx/gy/gz
+  bool gf32 = false;
+  float *fx = nullptr, *fy = nullptr, *fz = nullptr;
   double* pt = nullptr;      // 8 point arrays of chunk_tiles*128 per spin
   bool mgga = false;
   int functional = 0;        // PGXC_XC_* (the meta-GGA step selects its functional by id)
