@@ -475,8 +475,11 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
+// slots per warp and loop iteration of k_sm_zquant (two with FP64 gradients,
+// four with FP32 ones: the same bytes in flight per warp)
+constexpr int kZSlots = 4;
 template <bool GGA, typename GT>
-__global__ void __launch_bounds__(256, 3) k_sm_zquant(const int64_t* __restrict__ tso, int64_t t0, int64_t s0,
+__global__ void __launch_bounds__(256, 2) k_sm_zquant(const int64_t* __restrict__ tso, int64_t t0, int64_t s0,
                                                    const double* __restrict__ phi, const GT* __restrict__ gx,
                                                    const GT* __restrict__ gy, const GT* __restrict__ gz,
                                                    const double* __restrict__ A, const double* __restrict__ Bx,
@@ -501,12 +504,12 @@ __global__ void __launch_bounds__(256, 3) k_sm_zquant(const int64_t* __restrict_
   const int p0 = lane * 4;
   const int kstep = lane >> 3, kin = (lane & 7) * 4;
   const int64_t tile_off = sb * kDigBytesPerSlot;
-  // two adjacent slots per warp and iteration: the loads of both are in
-  // flight together, and their digit rows fill whole 32-byte sectors
-  for (int i0 = 2 * warp; i0 < n; i0 += 16) {
-    double f[2][4], z[2][4];
+  // kZSlots adjacent slots per warp and iteration: their loads are in flight
+  // together, and their digit rows fill whole 32-byte sectors
+  for (int i0 = kZSlots * warp; i0 < n; i0 += 8 * kZSlots) {
+    double f[kZSlots][4], z[kZSlots][4];
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < kZSlots; ++h) {
       const int i = i0 + h;
       const int64_t o = (sb + min(i, n - 1)) * 128 + p0;
       const double2 a = *reinterpret_cast<const double2*>(phi + o);
@@ -531,7 +534,7 @@ __global__ void __launch_bounds__(256, 3) k_sm_zquant(const int64_t* __restrict_
       }
     }
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
+    for (int h = 0; h < kZSlots; ++h) {
       const int i = i0 + h;
       if (i >= n) break;
 #pragma unroll
