@@ -346,11 +346,13 @@ __global__ void __launch_bounds__(256) k_grad_orb(bool gga, int ispin, int64_t n
 constexpr double kGradEdge = 0.9941;
 constexpr double kGradTau = 0x1p-60;
 
-// p3(mu) and ds/dmu (even in mu)
+// p3(mu) and ds/dmu (even in mu).  Each step RN(RN(q / 2) RN(3 - RN(q q)))
+// is formed as RN(q RN(1.5 - RN(q q) / 2)) (one FMA inside): halving is exact
+// and commutes with rounding for these normal operands, so the bits agree.
 __device__ __forceinline__ void becke_p3(double mu, double& q3, double& ds) {
-  const double q1 = __dmul_rn(__dmul_rn(0.5, mu), __dsub_rn(3.0, __dmul_rn(mu, mu)));
-  const double q2 = __dmul_rn(__dmul_rn(0.5, q1), __dsub_rn(3.0, __dmul_rn(q1, q1)));
-  q3 = __dmul_rn(__dmul_rn(0.5, q2), __dsub_rn(3.0, __dmul_rn(q2, q2)));
+  const double q1 = __dmul_rn(mu, __fma_rn(-0.5, __dmul_rn(mu, mu), 1.5));
+  const double q2 = __dmul_rn(q1, __fma_rn(-0.5, __dmul_rn(q1, q1), 1.5));
+  q3 = __dmul_rn(q2, __fma_rn(-0.5, __dmul_rn(q2, q2), 1.5));
   ds = -0.5 * (1.5 * (1.0 - q2 * q2)) * (1.5 * (1.0 - q1 * q1)) * (1.5 * (1.0 - mu * mu));
 }
 

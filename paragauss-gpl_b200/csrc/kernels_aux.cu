@@ -72,13 +72,45 @@ __device__ __forceinline__ double div_rn(double d, double R, double y) {
 // reference's pair orientation, mu = (r_i - r_k)/dst(k,i) for k < i and
 // -(r_k - r_i)/dst(i,k) for k > i, is the same rounded value: IEEE
 // subtraction and division are exactly antisymmetric.  mu0(mu, 0) =
-// p(p(p(mu))), p(q) = q (3 - q^2) / 2; the halvings are multiplications by
-// 0.5, which round exactly as the divisions by 2 do.
+// p(p(p(mu))), p(q) = q (3 - q^2) / 2, s = (1 - q) / 2.  Halving is exact
+// and commutes with rounding (no operand here is subnormal: |mu| is at least
+// an ulp of a distance over a distance), so the reference's
+// RN(RN(q RN(3 - RN(q q))) / 2) is RN(q RN(1.5 - RN(q q) / 2)), the inner
+// step one FMA, and RN(1 - q) / 2 is the FMA RN(0.5 - q / 2): the same
+// bits in 13 operations instead of 17.
 __device__ __forceinline__ double becke_s(double d, double R, double y) {
   double q = div_rn(d, R, y);
 #pragma unroll
-  for (int it = 0; it < 3; ++it) q = __dmul_rn(__dmul_rn(q, __dsub_rn(3.0, __dmul_rn(q, q))), 0.5);
-  return __dmul_rn(__dsub_rn(1.0, q), 0.5);
+  for (int it = 0; it < 3; ++it) q = __dmul_rn(q, __fma_rn(-0.5, __dmul_rn(q, q), 1.5));
+  return __fma_rn(-0.5, q, 0.5);
+}
+
+// P_i = the ordered product over k != i of s(mu_ik) for the point whose
+// distance to atom k is rk(k) (ri = rk(i)); 0 once the partial product is
+// below tau.  Four factors are formed independently per step (their FP64
+// chains overlap) and multiplied into P in ascending k; a factor that is
+// skipped (k = i, or exactly 1) enters as 1.0, which leaves P bit for bit
+// unchanged.  Every factor lies in [0, 1], so P never rises: testing tau once
+// per step returns 0 exactly where the test after every factor would.
+template <class RK>
+__device__ __forceinline__ double becke_product(int i, double ri, int natm, const double* __restrict__ Ri,
+                                                const double* __restrict__ Yi, double tau, RK rk) {
+  double P = 1.0;
+  for (int k0 = 0; k0 < natm; k0 += 4) {
+    double f[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int k = min(k0 + u, natm - 1);
+      const double R = __ldg(Ri + k);
+      const double d = __dsub_rn(ri, rk(k));
+      const bool use = k0 + u < natm && k != i && d > -__dmul_rn(kBeckeEdge, R);
+      f[u] = use ? becke_s(d, R, __ldg(Yi + k)) : 1.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) P = __dmul_rn(P, f[u]);
+    if (P < tau) return 0.0;
+  }
+  return P;
 }
 
 // Thread per point (geometries of more than kBeckeWarpAtoms atoms).
@@ -115,18 +147,7 @@ __global__ void __launch_bounds__(kBeckeThreads) k_becke_thread(const double* __
   // P_i as the ordered product, factors that are exactly 1 skipped; 0 once
   // the partial product is below tau (the factors left are at most 1)
   auto ordered = [&](int i, double ri, double tau) {
-    const double* Ri = dist + (int64_t)i * natm;
-    const double* Yi = rdist + (int64_t)i * natm;
-    double P = 1.0;
-    for (int k = 0; k < natm; ++k) {
-      if (k == i) continue;
-      const double R = __ldg(Ri + k);
-      const double d = __dsub_rn(ri, r_of(k));
-      if (d <= -__dmul_rn(kBeckeEdge, R)) continue;
-      P = __dmul_rn(P, becke_s(d, R, __ldg(Yi + k)));
-      if (P < tau) return 0.0;
-    }
-    return P;
+    return becke_product(i, ri, natm, dist + (int64_t)i * natm, rdist + (int64_t)i * natm, tau, r_of);
   };
   const int i0 = nb[0];
   const double P0 = ordered(i0, nr[0], 0.0);
@@ -168,8 +189,16 @@ __global__ void __launch_bounds__(kBeckeThreads) k_becke_thread(const double* __
 // every point's sum is formed in the reference's order.  Thread-per-point
 // loops over the atoms diverge wherever the lanes' points keep different
 // atoms; here every lane of a round has a product to form.
+//
+// A round's 32 pairs belong to few points (2.8 on average at 60 atoms), and
+// each ordered product needs the point's distance to every atom.  The warp
+// therefore first writes the distances of the round's first kTabPts points to
+// all atoms into a shared table (the same correctly rounded dist3 values) and
+// the products read them there; a lane whose point is not in the table (a
+// round of more than kTabPts points) computes its distances itself.
 constexpr int kBeckeWarpAtoms = 256;
 constexpr int kMaskWords = kBeckeWarpAtoms / 32;
+constexpr int kTabPts = 4;
 
 __global__ void __launch_bounds__(kBeckeThreads) k_becke_warp(const double* __restrict__ atoms,
                                                               const double* __restrict__ dist,
@@ -179,8 +208,10 @@ __global__ void __launch_bounds__(kBeckeThreads) k_becke_warp(const double* __re
                                                               const double* __restrict__ pz,
                                                               const int* __restrict__ owner, int64_t n,
                                                               double* __restrict__ w) {
+  extern __shared__ double becke_tab[];  // per warp: kTabPts x natm point-atom distances
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
+  double* tab = becke_tab + (threadIdx.x >> 5) * kTabPts * natm;
   const bool live = p < n;  // every lane takes part in the warp's rounds
   double x = 0.0, y = 0.0, z = 0.0;
   int a = -1;
@@ -193,20 +224,15 @@ __global__ void __launch_bounds__(kBeckeThreads) k_becke_warp(const double* __re
   // P_i of the point at (qx, qy, qz): the ordered product, exactly-1 factors
   // skipped, 0 once below tau
   auto ordered = [&](int i, double qx, double qy, double qz, double tau) {
-    const double ri = dist3(__ldg(atoms + 3 * i), __ldg(atoms + 3 * i + 1), __ldg(atoms + 3 * i + 2), qx, qy, qz);
-    const double* Ri = dist + (int64_t)i * natm;
-    const double* Yi = rdist + (int64_t)i * natm;
-    double P = 1.0;
-    for (int k = 0; k < natm; ++k) {
-      if (k == i) continue;
-      const double R = __ldg(Ri + k);
-      const double d = __dsub_rn(ri, dist3(__ldg(atoms + 3 * k), __ldg(atoms + 3 * k + 1), __ldg(atoms + 3 * k + 2),
-                                           qx, qy, qz));
-      if (d <= -__dmul_rn(kBeckeEdge, R)) continue;
-      P = __dmul_rn(P, becke_s(d, R, __ldg(Yi + k)));
-      if (P < tau) return 0.0;
-    }
-    return P;
+    auto rk = [&](int k) {
+      return dist3(__ldg(atoms + 3 * k), __ldg(atoms + 3 * k + 1), __ldg(atoms + 3 * k + 2), qx, qy, qz);
+    };
+    return becke_product(i, rk(i), natm, dist + (int64_t)i * natm, rdist + (int64_t)i * natm, tau, rk);
+  };
+  // the same product with the point's distances to the atoms read from rt
+  auto ordered_tab = [&](int i, const double* rt, double tau) {
+    return becke_product(i, rt[i], natm, dist + (int64_t)i * natm, rdist + (int64_t)i * natm, tau,
+                         [&](int k) { return rt[k]; });
   };
   int nb[4] = {-1, -1, -1, -1};
   double nr[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
@@ -286,6 +312,21 @@ __global__ void __launch_bounds__(kBeckeThreads) k_becke_warp(const double* __re
     for (int u = 0; u < kMaskWords; ++u) m[u] = __shfl_sync(0xffffffffu, mask[u], ol);
     const double qx = __shfl_sync(0xffffffffu, x, ol), qy = __shfl_sync(0xffffffffu, y, ol),
                  qz = __shfl_sync(0xffffffffu, z, ol), qt = __shfl_sync(0xffffffffu, tau, ol);
+    // the round's points in lane order (owners ascend with the position);
+    // jd = this lane's point among them
+    const int olp = __shfl_up_sync(0xffffffffu, ol, 1);
+    const unsigned fm = __ballot_sync(0xffffffffu, q < total && (lane == 0 || olp != ol));
+    const int jd = __popc(fm & ((2u << lane) - 1u)) - 1;
+    const int md = min(__popc(fm), kTabPts);
+    __syncwarp();  // the previous round's reads of the table are done
+    for (int jt = 0; jt < md; ++jt) {
+      const int src = __shfl_sync(0xffffffffu, ol, (int)__fns(fm, 0, jt + 1));
+      const double tx = __shfl_sync(0xffffffffu, x, src), ty = __shfl_sync(0xffffffffu, y, src),
+                   tz = __shfl_sync(0xffffffffu, z, src);
+      for (int k = lane; k < natm; k += 32)
+        tab[jt * natm + k] = dist3(__ldg(atoms + 3 * k), __ldg(atoms + 3 * k + 1), __ldg(atoms + 3 * k + 2), tx, ty, tz);
+    }
+    __syncwarp();
     int pi = -1;
     double P = 0.0;
     if (q < total) {
@@ -298,7 +339,7 @@ __global__ void __launch_bounds__(kBeckeThreads) k_becke_warp(const double* __re
         }
         r -= c;
       }
-      P = ordered(pi, qx, qy, qz, qt);
+      P = jd < kTabPts ? ordered_tab(pi, tab + jd * natm, qt) : ordered(pi, qx, qy, qz, qt);
     }
     // hand the round's products to their points' lanes, in position order
     for (int t = 0; t < 32; ++t) {
@@ -327,7 +368,8 @@ cudaError_t launch_becke(const double* atoms, double* dist, int natm, const doub
   if (e != cudaSuccess || n == 0) return e;
   const unsigned nb = (unsigned)((n + kBeckeThreads - 1) / kBeckeThreads);
   if (natm <= kBeckeWarpAtoms)
-    k_becke_warp<<<nb, kBeckeThreads, 0, st>>>(atoms, dist, rdist, natm, px, py, pz, owner, n, w);
+    k_becke_warp<<<nb, kBeckeThreads, (kBeckeThreads / 32) * kTabPts * natm * sizeof(double), st>>>(
+        atoms, dist, rdist, natm, px, py, pz, owner, n, w);
   else
     k_becke_thread<<<nb, kBeckeThreads, 0, st>>>(atoms, dist, rdist, natm, px, py, pz, owner, n, w);
   return cudaGetLastError();

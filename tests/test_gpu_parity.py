@@ -89,9 +89,9 @@ def test_device_becke_many_atoms_matches_oracle():
     _becke_agreement(c)
 
 
-def test_device_becke_uncached_many_atoms_matches_oracle():
-    """140 atoms: beyond the shared-memory distance cache the point-atom
-    distances are recomputed; the weights still match the oracle to 2e-16."""
+def test_device_becke_140_atoms_matches_oracle():
+    """140 atoms (a five-word survivor mask per point, a 140-entry distance
+    table per round point): the weights still match the oracle to 2e-16."""
     rng = np.random.default_rng(23)
     els, xyz = cases.random_cluster(rng, [("C", 70), ("H", 70)], 17.0, 1.1)
     c = cases.build_case("becke140", els, xyz, seed=23, exp_range=(0.1, 100.0), nrad=3, nang=50,
