@@ -92,14 +92,15 @@ __device__ __forceinline__ double becke_s(double d, double R, double y) {
 // skipped (k = i, or exactly 1) enters as 1.0, which leaves P bit for bit
 // unchanged.  Every factor lies in [0, 1], so P never rises: testing tau once
 // per step returns 0 exactly where the test after every factor would.
+constexpr int kBeckeStep = 4;
 template <class RK>
 __device__ __forceinline__ double becke_product(int i, double ri, int natm, const double* __restrict__ Ri,
                                                 const double* __restrict__ Yi, double tau, RK rk) {
   double P = 1.0;
-  for (int k0 = 0; k0 < natm; k0 += 4) {
-    double f[4];
+  for (int k0 = 0; k0 < natm; k0 += kBeckeStep) {
+    double f[kBeckeStep];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
+    for (int u = 0; u < kBeckeStep; ++u) {
       const int k = min(k0 + u, natm - 1);
       const double R = __ldg(Ri + k);
       const double d = __dsub_rn(ri, rk(k));
@@ -107,7 +108,7 @@ __device__ __forceinline__ double becke_product(int i, double ri, int natm, cons
       f[u] = use ? becke_s(d, R, __ldg(Yi + k)) : 1.0;
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u) P = __dmul_rn(P, f[u]);
+    for (int u = 0; u < kBeckeStep; ++u) P = __dmul_rn(P, f[u]);
     if (P < tau) return 0.0;
   }
   return P;
