@@ -475,93 +475,188 @@ __device__ __forceinline__ double warp_max(double v) {
   return v;
 }
 
-// slots per warp and loop iteration of k_sm_zquant (two with FP64 gradients,
-// four with FP32 ones: the same bytes in flight per warp)
-constexpr int kZSlots = 4;
+// Persistent, one CTA per SM.  Warp kZWarps (one thread) streams the chunk's
+// phi and grad phi rows through a ring of stages of kZStage slots by bulk
+// copies, and each tile's A and B into a double buffer; warps 0 .. kZWarps-1
+// take one slot of every stage each (lane = 4 consecutive points), form
+// Z = A phi (+ B . grad phi) in FP64, the scales and the digits, and store
+// them.  The copies of
+// the next stages are in flight while a stage is converted, so the reads run
+// at the HBM rate instead of one load latency per slot group.
+constexpr int kZWarps = 16;                          // consumer warps, one slot of each stage each
+constexpr int kZStage = kZWarps;                     // slots per ring stage
+constexpr int kZThreads = kBlock4((kZWarps + 1) * 32);  // + the producer warp; the rest idle
 template <bool GGA, typename GT>
-__global__ void __launch_bounds__(256, 2) k_sm_zquant(const int64_t* __restrict__ tso, int64_t t0, int64_t s0,
-                                                   const double* __restrict__ phi, const GT* __restrict__ gx,
-                                                   const GT* __restrict__ gy, const GT* __restrict__ gz,
-                                                   const double* __restrict__ A, const double* __restrict__ Bx,
-                                                   const double* __restrict__ By, const double* __restrict__ Bz,
-                                                   int8_t* __restrict__ tZ, int8_t* __restrict__ tF,
-                                                   double* __restrict__ zs, double* __restrict__ fs) {
-  __shared__ double sA[128], sB[3][128];
-  const int64_t t = t0 + blockIdx.x;
-  const int64_t sb = tso[t] - s0;
-  const int n = (int)(tso[t + 1] - tso[t]);
+struct ZLayout {
+  static constexpr int kRing = (GGA && sizeof(GT) == 8) ? 3 : 4;
+  static constexpr int kF = kZStage * 128 * 8;                        // phi of a stage
+  static constexpr int kG = GGA ? kZStage * 128 * (int)sizeof(GT) : 0;  // one gradient plane of a stage
+  static constexpr int kStage = kF + 3 * kG;
+  static constexpr int kAB = 4 * 128 * 8;  // A, Bx, By, Bz of a tile
+  static constexpr int kBar = kRing * kStage + 2 * kAB;
+  static constexpr int kBytes = kBar + (2 * kRing + 4) * 8;
+};
+
+template <bool GGA, typename GT>
+__global__ void __launch_bounds__(kZThreads, 1) k_sm_zquant(const int64_t* __restrict__ tso, int64_t t0, int64_t nt,
+                                                            int64_t s0, const double* __restrict__ phi,
+                                                            const GT* __restrict__ gx, const GT* __restrict__ gy,
+                                                            const GT* __restrict__ gz, const double* __restrict__ A,
+                                                            const double* __restrict__ Bx,
+                                                            const double* __restrict__ By,
+                                                            const double* __restrict__ Bz, int8_t* __restrict__ tZ,
+                                                            int8_t* __restrict__ tF, double* __restrict__ zs,
+                                                            double* __restrict__ fs, int* err) {
+  using L = ZLayout<GGA, GT>;
+  extern __shared__ __align__(128) uint8_t zsm[];
+  uint64_t* full = reinterpret_cast<uint64_t*>(zsm + L::kBar);
+  uint64_t* empty = full + L::kRing;
+  uint64_t* ab_full = empty + L::kRing;
+  uint64_t* ab_empty = ab_full + 2;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  if (tid < 128) {
-    const int64_t p = (int64_t)blockIdx.x * 128 + tid;
-    sA[tid] = A[p];
-    if (GGA) {
-      sB[0][tid] = Bx[p];
-      sB[1][tid] = By[p];
-      sB[2][tid] = Bz[p];
+  if (tid == 0) {
+    for (int r = 0; r < L::kRing; ++r) {
+      tc::mbar_init(&full[r], 1);
+      tc::mbar_init(&empty[r], kZWarps);
     }
+    for (int b = 0; b < 2; ++b) {
+      tc::mbar_init(&ab_full[b], 1);
+      tc::mbar_init(&ab_empty[b], kZWarps);
+    }
+    tc::mbar_fence_init();
   }
   __syncthreads();
-  const int p0 = lane * 4;
-  const int kstep = lane >> 3, kin = (lane & 7) * 4;
-  const int64_t tile_off = sb * kDigBytesPerSlot;
-  // kZSlots adjacent slots per warp and iteration: their loads are in flight
-  // together, and their digit rows fill whole 32-byte sectors
-  for (int i0 = kZSlots * warp; i0 < n; i0 += 8 * kZSlots) {
-    double f[kZSlots][4], z[kZSlots][4];
-#pragma unroll
-    for (int h = 0; h < kZSlots; ++h) {
-      const int i = i0 + h;
-      const int64_t o = (sb + min(i, n - 1)) * 128 + p0;
-      const double2 a = *reinterpret_cast<const double2*>(phi + o);
-      const double2 b = *reinterpret_cast<const double2*>(phi + o + 2);
-      f[h][0] = a.x; f[h][1] = a.y; f[h][2] = b.x; f[h][3] = b.y;
-      if (GGA) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const GT* g = c == 0 ? gx : (c == 1 ? gy : gz);
-          double gv[4];
-          if constexpr (sizeof(GT) == 4) {
-            const float4 q = *reinterpret_cast<const float4*>(g + o);
-            gv[0] = q.x; gv[1] = q.y; gv[2] = q.z; gv[3] = q.w;
-          } else {
-            const double2 ga = *reinterpret_cast<const double2*>(g + o);
-            const double2 gb = *reinterpret_cast<const double2*>(g + o + 2);
-            gv[0] = ga.x; gv[1] = ga.y; gv[2] = gb.x; gv[3] = gb.y;
+  bool ok = true;
+  if (warp == kZWarps) {
+    if (lane == 0) {  // producer
+      int it = 0, tt = 0;
+      for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x, ++tt) {
+        const int64_t sb = tso[t0 + ti] - s0;
+        const int n = (int)(tso[t0 + ti + 1] - tso[t0 + ti]);
+        const int b = tt & 1;
+        if (tt >= 2 && !tc::mbar_wait(&ab_empty[b], ((tt >> 1) - 1) & 1)) {
+          ok = false;
+          break;
+        }
+        double* ab = reinterpret_cast<double*>(zsm + L::kRing * L::kStage + b * L::kAB);
+        tc::mbar_expect_tx(&ab_full[b], (GGA ? 4 : 1) * 1024);
+        tc::bulk_g2s(ab, A + ti * 128, 1024, &ab_full[b]);
+        if (GGA) {
+          tc::bulk_g2s(ab + 128, Bx + ti * 128, 1024, &ab_full[b]);
+          tc::bulk_g2s(ab + 256, By + ti * 128, 1024, &ab_full[b]);
+          tc::bulk_g2s(ab + 384, Bz + ti * 128, 1024, &ab_full[b]);
+        }
+        for (int i0 = 0; i0 < n; i0 += kZStage, ++it) {
+          const int r = it % L::kRing;
+          if (it >= L::kRing && !tc::mbar_wait(&empty[r], ((it / L::kRing) - 1) & 1)) {
+            ok = false;
+            break;
           }
-#pragma unroll
-          for (int u = 0; u < 4; ++u) z[h][u] = (c == 0 ? 0.0 : z[h][u]) + sB[c][p0 + u] * gv[u];
+          const int ns = min(kZStage, n - i0);
+          const int64_t o = (sb + i0) * 128;
+          uint8_t* st = zsm + r * L::kStage;
+          const uint32_t fb = (uint32_t)ns * 128 * 8, gb = (uint32_t)ns * 128 * sizeof(GT);
+          tc::mbar_expect_tx(&full[r], fb + (GGA ? 3 * gb : 0));
+          tc::bulk_g2s(st, phi + o, fb, &full[r]);
+          if (GGA) {
+            tc::bulk_g2s(st + L::kF, gx + o, gb, &full[r]);
+            tc::bulk_g2s(st + L::kF + L::kG, gy + o, gb, &full[r]);
+            tc::bulk_g2s(st + L::kF + 2 * L::kG, gz + o, gb, &full[r]);
+          }
         }
       }
+      if (!ok) atomicExch(err, 1);
+      // the copies still in flight land before the CTA exits
+      for (int j = max(0, it - L::kRing); j < it; ++j) tc::mbar_wait(&full[j % L::kRing], (j / L::kRing) & 1);
+      for (int j = max(0, tt - 2); j < tt; ++j) tc::mbar_wait(&ab_full[j & 1], (j >> 1) & 1);
     }
-#pragma unroll
-    for (int h = 0; h < kZSlots; ++h) {
-      const int i = i0 + h;
-      if (i >= n) break;
-#pragma unroll
-      for (int u = 0; u < 4; ++u) z[h][u] = GGA ? z[h][u] + sA[p0 + u] * f[h][u] : sA[p0 + u] * f[h][u];
-      const double mz = warp_max(fmax(fmax(fabs(z[h][0]), fabs(z[h][1])), fmax(fabs(z[h][2]), fabs(z[h][3]))));
-      const double mf = warp_max(fmax(fmax(fabs(f[h][0]), fabs(f[h][1])), fmax(fabs(f[h][2]), fabs(f[h][3]))));
-      const int ez = scale_exp(mz), ef = scale_exp(mf);
-      if (lane == 0) {
-        zs[sb + i] = pow2(ez);
-        fs[sb + i] = pow2(ef + kCombShift);
+  } else if (warp < kZWarps) {
+    const int p0 = lane * 4;
+    const int kstep = lane >> 3, kin = (lane & 7) * 4;
+    int it = 0, tt = 0;
+    for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x, ++tt) {
+      const int64_t sb = tso[t0 + ti] - s0;
+      const int n = (int)(tso[t0 + ti + 1] - tso[t0 + ti]);
+      const int b = tt & 1;
+      if (!tc::mbar_wait(&ab_full[b], (tt >> 1) & 1)) {
+        ok = false;
+        break;
       }
-      long long qz[4], qf[4];
+      const double* ab = reinterpret_cast<const double*>(zsm + L::kRing * L::kStage + b * L::kAB);
+      double a[4], bv[3][4];
 #pragma unroll
       for (int u = 0; u < 4; ++u) {
-        qz[u] = oz_int(z[h][u], ez);
-        qf[u] = oz_int(f[h][u], ef);
+        a[u] = ab[p0 + u];
+        if (GGA) {
+          bv[0][u] = ab[128 + p0 + u];
+          bv[1][u] = ab[256 + p0 + u];
+          bv[2][u] = ab[384 + p0 + u];
+        }
       }
-      uint32_t wz[kSlices], wf[kSlices];
-      oz_pack4(qz, wz);
-      oz_pack4(qf, wf);
-      const int64_t kb = tile_off + (int64_t)kstep * n * (32 * kSlices);
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&ab_empty[b]);
+      const int64_t tile_off = sb * kDigBytesPerSlot;
+      for (int i0 = 0; i0 < n && ok; i0 += kZStage, ++it) {
+        const int r = it % L::kRing;
+        if (!tc::mbar_wait(&full[r], (it / L::kRing) & 1)) {
+          ok = false;
+          break;
+        }
+        const uint8_t* st = zsm + r * L::kStage;
+        const double* fst = reinterpret_cast<const double*>(st);
+        if (i0 + warp < n) {
+          const int q = warp, i = i0 + q;
+          double f[4], z[4];
+          const double2 fa = *reinterpret_cast<const double2*>(fst + q * 128 + p0);
+          const double2 fb = *reinterpret_cast<const double2*>(fst + q * 128 + p0 + 2);
+          f[0] = fa.x; f[1] = fa.y; f[2] = fb.x; f[3] = fb.y;
+          if (GGA) {
 #pragma unroll
-      for (int sl = 0; sl < kSlices; ++sl) {
-        *reinterpret_cast<uint32_t*>(tF + kb + ilv_off(i, kin, sl)) = wf[sl];
-        *reinterpret_cast<uint32_t*>(tZ + kb + (int64_t)sl * n * 32 + blk_off(i, kin)) = wz[sl];
+            for (int c = 0; c < 3; ++c) {
+              const GT* g = reinterpret_cast<const GT*>(st + L::kF + c * L::kG) + q * 128 + p0;
+              double gv[4];
+              if constexpr (sizeof(GT) == 4) {
+                const float4 w4 = *reinterpret_cast<const float4*>(g);
+                gv[0] = w4.x; gv[1] = w4.y; gv[2] = w4.z; gv[3] = w4.w;
+              } else {
+                const double2 ga = *reinterpret_cast<const double2*>(g);
+                const double2 gb2 = *reinterpret_cast<const double2*>(g + 2);
+                gv[0] = ga.x; gv[1] = ga.y; gv[2] = gb2.x; gv[3] = gb2.y;
+              }
+#pragma unroll
+              for (int u = 0; u < 4; ++u) z[u] = (c == 0 ? 0.0 : z[u]) + bv[c][u] * gv[u];
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) z[u] = GGA ? z[u] + a[u] * f[u] : a[u] * f[u];
+          const double mz = warp_max(fmax(fmax(fabs(z[0]), fabs(z[1])), fmax(fabs(z[2]), fabs(z[3]))));
+          const double mf = warp_max(fmax(fmax(fabs(f[0]), fabs(f[1])), fmax(fabs(f[2]), fabs(f[3]))));
+          const int ez = scale_exp(mz), ef = scale_exp(mf);
+          if (lane == 0) {
+            zs[sb + i] = pow2(ez);
+            fs[sb + i] = pow2(ef + kCombShift);
+          }
+          long long qz[4], qf[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            qz[u] = oz_int(z[u], ez);
+            qf[u] = oz_int(f[u], ef);
+          }
+          uint32_t wz[kSlices], wf[kSlices];
+          oz_pack4(qz, wz);
+          oz_pack4(qf, wf);
+          const int64_t kb = tile_off + (int64_t)kstep * n * (32 * kSlices);
+#pragma unroll
+          for (int sl = 0; sl < kSlices; ++sl) {
+            *reinterpret_cast<uint32_t*>(tF + kb + ilv_off(i, kin, sl)) = wf[sl];
+            *reinterpret_cast<uint32_t*>(tZ + kb + (int64_t)sl * n * 32 + blk_off(i, kin)) = wz[sl];
+          }
+        }
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&empty[r]);
       }
     }
+    if (!ok) atomicExch(err, 1);
   }
 }
 
@@ -793,8 +888,18 @@ int screen_mixed_create(ScreenMixed** out, const ScreenMixedInput& in, std::stri
     return e == cudaErrorMemoryAllocation ? PGXC_ENOMEM : PGXC_ECUDA;
   }
   static_assert(sizeof(DensSmem) <= tc::kWholeSmSmem && sizeof(VSmem) <= tc::kWholeSmSmem, "smem");
+  static_assert(ZLayout<true, double>::kBytes <= tc::kWholeSmSmem && ZLayout<true, float>::kBytes <= tc::kWholeSmSmem,
+                "smem");
   const int dsm = tc::kWholeSmSmem;
   raise_smem_limit(k_sm_gather_B, 4 * in.max_n);
+  cudaFuncSetAttribute(k_sm_zquant<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       ZLayout<true, double>::kBytes);
+  cudaFuncSetAttribute(k_sm_zquant<true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       ZLayout<true, float>::kBytes);
+  cudaFuncSetAttribute(k_sm_zquant<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       ZLayout<false, double>::kBytes);
+  cudaFuncSetAttribute(k_sm_zquant<false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       ZLayout<false, float>::kBytes);
   cudaFuncSetAttribute(k_sm_density<true, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm);
   cudaFuncSetAttribute(k_sm_density<false, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm);
   cudaFuncSetAttribute(k_sm_density<true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, dsm);
@@ -877,12 +982,14 @@ int mixed_potential(ScreenMixed* m, const int64_t* tso, const int* slot_fn, int6
                     const double* phi, const GT* gx, const GT* gy, const GT* gz, const double* A, const double* Bx,
                     const double* By, const double* Bz, double* V, int64_t ldv, cudaStream_t st, cudaEvent_t k0,
                     cudaEvent_t k1, const int* tile_mol, const SetMolDev* mols) {
+  const unsigned zgrid = (unsigned)std::min<int64_t>(nt, m->nsm);
   if (m->gga)
-    k_sm_zquant<true, GT><<<(unsigned)nt, 256, 0, st>>>(tso, t0, s0, phi, gx, gy, gz, A, Bx, By, Bz, m->tZ, m->tF,
-                                                        m->zs, m->fs);
+    k_sm_zquant<true, GT><<<zgrid, kZThreads, ZLayout<true, GT>::kBytes, st>>>(
+        tso, t0, nt, s0, phi, gx, gy, gz, A, Bx, By, Bz, m->tZ, m->tF, m->zs, m->fs, m->err);
   else
-    k_sm_zquant<false, GT><<<(unsigned)nt, 256, 0, st>>>(tso, t0, s0, phi, nullptr, nullptr, nullptr, A, nullptr,
-                                                         nullptr, nullptr, m->tZ, m->tF, m->zs, m->fs);
+    k_sm_zquant<false, GT><<<zgrid, kZThreads, ZLayout<false, GT>::kBytes, st>>>(
+        tso, t0, nt, s0, phi, nullptr, nullptr, nullptr, A, nullptr, nullptr, nullptr, m->tZ, m->tF, m->zs, m->fs,
+        m->err);
   if (k0) cudaEventRecord(k0, st);
   const unsigned grid = (unsigned)std::min<int64_t>(nt, m->nsm);
   auto launch = [&](auto kern) {
