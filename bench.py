@@ -691,9 +691,17 @@ def main():
         tf = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tf):
             traffic = json.load(open(tf)).get(f"{case.name}:{prec}:{args.screen:g}:{dom}")
-        roof = {"bound": "hbm", "kernel": dom, "achieved": kd["achieved_gbs"], "peak": mp["hbm_gbs"], "unit": "GB/s",
-                "frac": kd["hbm_frac"], "traffic": traffic,
-                "peak_source": "MEASURED_PEAKS.json hbm_gbs, of measured",
+        # the roof the kernel is nearest to: DRAM for the streaming kernels, the
+        # tensor pipe (INT8 ops issued, or FP64 DMMA) for a contraction whose
+        # operand bytes are small beside its MMA work
+        tensor_bound = kd.get("tensor_frac", 0.0) > kd["hbm_frac"]
+        roof = {"bound": "tensor" if tensor_bound else "hbm", "kernel": dom,
+                "achieved": kd["issued_tops"] if tensor_bound else kd["achieved_gbs"],
+                "peak": tpeak if tensor_bound else mp["hbm_gbs"],
+                "unit": ("TOP/s" if prec != "fp64" else "TFLOP/s") if tensor_bound else "GB/s",
+                "frac": kd["tensor_frac"] if tensor_bound else kd["hbm_frac"], "traffic": traffic,
+                "hbm": {"achieved": kd["achieved_gbs"], "peak": mp["hbm_gbs"], "unit": "GB/s", "frac": kd["hbm_frac"]},
+                "peak_source": tsrc if tensor_bound else "MEASURED_PEAKS.json hbm_gbs, of measured",
                 "algorithmic_bytes": kd["algorithmic_bytes"], "kernel_ms_per_build": kd["ms"],
                 "tensor": None if "tensor_frac" not in kd else {
                     "algorithmic_tflops": kd["algorithmic_tflops"], "issued_tflops_or_tops": kd["issued_tops"],

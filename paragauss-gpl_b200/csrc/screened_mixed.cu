@@ -682,7 +682,10 @@ struct VSmem {
   uint64_t acc_empty[2];
   uint32_t tslot;
 };
-constexpr int kVThreads = tc::kWholeSmThreads;  // warps 0-7 epilogue, 8 MMA, 9 producer, 10-15 idle
+// warps 0-7 and 10-13 epilogue (three per TMEM lane quarter, 16 columns of
+// each 48-slot block each), 8 MMA, 9 producer, 14-15 idle
+constexpr int kVThreads = tc::kWholeSmThreads;
+constexpr int kVEpiWarps = 12;
 
 // LDA keeps j >= i: the last 48-slot row block I of column block J
 __device__ __forceinline__ int last_I(int J, int nI, bool all) { return all ? nI : min(nI, (kM * J + kM - 1) / kN + 1); }
@@ -708,7 +711,7 @@ __global__ void __launch_bounds__(kVThreads, 1)
     }
     for (int b = 0; b < 2; ++b) {
       tc::mbar_init(&S.acc_full[b], 1);
-      tc::mbar_init(&S.acc_empty[b], 256);
+      tc::mbar_init(&S.acc_empty[b], 32 * kVEpiWarps);
     }
     tc::mbar_fence_init();
   }
@@ -789,10 +792,10 @@ __global__ void __launch_bounds__(kVThreads, 1)
       }
       if (!ok) atomicExch(err, 1);
     }
-  } else if (warp >= 10) {
+  } else if (warp >= 14) {
     // idle: the CTA holds the whole SM
-  } else {  // epilogue: column j = 128 J + 32 (warp & 3) + lane of H, rows 24 (warp >> 2) .. of each 48-slot block
-    const int half = warp >> 2;
+  } else {  // epilogue: column j = 128 J + 32 (warp & 3) + lane of H, rows 16 third .. +15 of each 48-slot block
+    const int third = warp < 8 ? (warp >> 2) : 2;
     const uint32_t trow = tbase + ((uint32_t)((warp & 3) * 32) << 16);
     int pp = 0;
     for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
@@ -814,21 +817,21 @@ __global__ void __launch_bounds__(kVThreads, 1)
         const double fsj = j < n ? __ldg(fs + sb + j) : 0.0;
         for (int I = 0; I < last_I(J, nI, GGA); ++I, ++pp) {
           const int b = pp & 1;
-          // row i of lane (< 24) of this warp's 24: its function and scale, broadcast below
-          const int il = I * kN + half * 24 + lane;
-          const int fil = (lane < 24 && il < n) ? __ldg(sfn + il) : -1;
-          const double zsl = (lane < 24 && il < n) ? __ldg(zs + sb + il) : 0.0;
+          // row i of lane (< 16) of this warp's 16: its function and scale, broadcast below
+          const int il = I * kN + third * 16 + lane;
+          const int fil = (lane < 16 && il < n) ? __ldg(sfn + il) : -1;
+          const double zsl = (lane < 16 && il < n) ? __ldg(zs + sb + il) : 0.0;
           if (!tc::mbar_wait_warp(&S.acc_full[b], (pp >> 1) & 1)) {
             ok = false;
             break;
           }
           tc::fence_after_sync();
-          double x[24];
-          read_acc24(trow + b * kAccCols, half, x);
+          double x[16];
+          acc_cols<16>(trow + b * kAccCols + third * 16, x);
           tc::fence_before_sync();
           tc::mbar_arrive(&S.acc_empty[b]);
 #pragma unroll
-          for (int c = 0; c < 24; ++c) {
+          for (int c = 0; c < 16; ++c) {
             const int fi = __shfl_sync(0xffffffffu, fil, c);
             const double zsc = __shfl_sync(0xffffffffu, zsl, c);
             if (fj >= 0 && fi >= 0 && (GGA || fj >= fi)) atomicAdd(Vt + (int64_t)fi * ldt + fj, x[c] * (fsj * zsc));
