@@ -254,7 +254,8 @@ __device__ __forceinline__ void acc_cols(uint32_t taddr, double* x) {
 #pragma unroll
   for (int g = 0; g < kGroups; ++g) {
     if constexpr (W == 16) tc::tmem_ld16u(taddr + g * kN, r[g]);
-    else tc::tmem_ld8(taddr + g * kN, r[g]);
+    else if constexpr (W == 8) tc::tmem_ld8(taddr + g * kN, r[g]);
+    else tc::tmem_ld4(taddr + g * kN, r[g]);
   }
   tc::tmem_ld_wait();
 #pragma unroll
@@ -682,10 +683,10 @@ struct VSmem {
   uint64_t acc_empty[2];
   uint32_t tslot;
 };
-// warps 0-7 and 10-13 epilogue (three per TMEM lane quarter, 16 columns of
-// each 48-slot block each), 8 MMA, 9 producer, 14-15 idle
-constexpr int kVThreads = tc::kWholeSmThreads;
-constexpr int kVEpiWarps = 12;
+// warps 0-15 epilogue (four per TMEM lane quarter, 12 columns of each 48-slot
+// block each), 16 MMA, 17 producer, 18-19 idle
+constexpr int kVEpiWarps = 16;
+constexpr int kVThreads = (kVEpiWarps + 4) * 32;
 
 // LDA keeps j >= i: the last 48-slot row block I of column block J
 __device__ __forceinline__ int last_I(int J, int nI, bool all) { return all ? nI : min(nI, (kM * J + kM - 1) / kN + 1); }
@@ -720,7 +721,7 @@ __global__ void __launch_bounds__(kVThreads, 1)
   tc::fence_after_sync();
   const uint32_t tbase = S.tslot;
   bool ok = true;
-  if (warp == 9) {
+  if (warp == kVEpiWarps + 1) {
     if (lane == 0) {  // producer: the phi block of each J once, the Z block of each (J, I) pair per K step
       int it = 0, ia = 0;
       for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
@@ -755,7 +756,7 @@ __global__ void __launch_bounds__(kVThreads, 1)
       }
       if (!ok) atomicExch(err, 1);
     }
-  } else if (warp == 8) {
+  } else if (warp == kVEpiWarps) {
     if (lane == 0) {  // MMA issuer
       int it = 0, pp = 0, ia = 0;
       for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
@@ -792,10 +793,10 @@ __global__ void __launch_bounds__(kVThreads, 1)
       }
       if (!ok) atomicExch(err, 1);
     }
-  } else if (warp >= 14) {
+  } else if (warp > kVEpiWarps + 1) {
     // idle: the CTA holds the whole SM
-  } else {  // epilogue: column j = 128 J + 32 (warp & 3) + lane of H, rows 16 third .. +15 of each 48-slot block
-    const int third = warp < 8 ? (warp >> 2) : 2;
+  } else {  // epilogue: column j = 128 J + 32 (warp & 3) + lane of H, rows 12 part .. +11 of each 48-slot block
+    const int part = warp >> 2;
     const uint32_t trow = tbase + ((uint32_t)((warp & 3) * 32) << 16);
     int pp = 0;
     for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
@@ -817,21 +818,22 @@ __global__ void __launch_bounds__(kVThreads, 1)
         const double fsj = j < n ? __ldg(fs + sb + j) : 0.0;
         for (int I = 0; I < last_I(J, nI, GGA); ++I, ++pp) {
           const int b = pp & 1;
-          // row i of lane (< 16) of this warp's 16: its function and scale, broadcast below
-          const int il = I * kN + third * 16 + lane;
-          const int fil = (lane < 16 && il < n) ? __ldg(sfn + il) : -1;
-          const double zsl = (lane < 16 && il < n) ? __ldg(zs + sb + il) : 0.0;
+          // row i of lane (< 12) of this warp's 12: its function and scale, broadcast below
+          const int il = I * kN + part * 12 + lane;
+          const int fil = (lane < 12 && il < n) ? __ldg(sfn + il) : -1;
+          const double zsl = (lane < 12 && il < n) ? __ldg(zs + sb + il) : 0.0;
           if (!tc::mbar_wait_warp(&S.acc_full[b], (pp >> 1) & 1)) {
             ok = false;
             break;
           }
           tc::fence_after_sync();
-          double x[16];
-          acc_cols<16>(trow + b * kAccCols + third * 16, x);
+          double x[12];
+          acc_cols<8>(trow + b * kAccCols + part * 12, x);
+          acc_cols<4>(trow + b * kAccCols + part * 12 + 8, x + 8);
           tc::fence_before_sync();
           tc::mbar_arrive(&S.acc_empty[b]);
 #pragma unroll
-          for (int c = 0; c < 16; ++c) {
+          for (int c = 0; c < 12; ++c) {
             const int fi = __shfl_sync(0xffffffffu, fil, c);
             const double zsc = __shfl_sync(0xffffffffu, zsl, c);
             if (fj >= 0 && fi >= 0 && (GGA || fj >= fi)) atomicAdd(Vt + (int64_t)fi * ldt + fj, x[c] * (fsj * zsc));
