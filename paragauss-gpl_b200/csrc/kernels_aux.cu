@@ -191,15 +191,24 @@ __global__ void __launch_bounds__(kBeckeThreads) k_becke_thread(const double* __
 // loops over the atoms diverge wherever the lanes' points keep different
 // atoms; here every lane of a round has a product to form.
 //
+// The survivor bitmasks live in shared memory, word u of lane l at
+// [u][l] of the warp's block (ceil(natm / 32) words per point).
+//
 // A round's 32 pairs belong to few points (2.8 on average at 60 atoms), and
-// each ordered product needs the point's distance to every atom.  The warp
-// therefore first writes the distances of the round's first kTabPts points to
-// all atoms into a shared table (the same correctly rounded dist3 values) and
-// the products read them there; a lane whose point is not in the table (a
-// round of more than kTabPts points) computes its distances itself.
-constexpr int kBeckeWarpAtoms = 256;
-constexpr int kMaskWords = kBeckeWarpAtoms / 32;
+// each ordered product needs the point's distance to every atom.  Up to
+// kTabAtoms atoms the warp therefore first writes the distances of the
+// round's first kTabPts points to all atoms into a shared table (the same
+// correctly rounded dist3 values) and the products read them there; a lane
+// whose point is not in the table (a round of more than kTabPts points), and
+// every lane beyond kTabAtoms atoms, computes its distances itself.
+constexpr int kBeckeWarpAtoms = 1024;
+constexpr int kTabAtoms = 256;
 constexpr int kTabPts = 4;
+
+// dynamic shared memory of one warp: the masks, then the distance table
+__host__ __device__ constexpr int becke_warp_smem(int natm) {
+  return 128 * ((natm + 31) / 32) + (natm <= kTabAtoms ? kTabPts * natm * 8 : 0);
+}
 
 __global__ void __launch_bounds__(kBeckeThreads) k_becke_warp(const double* __restrict__ atoms,
                                                               const double* __restrict__ dist,
@@ -209,10 +218,14 @@ __global__ void __launch_bounds__(kBeckeThreads) k_becke_warp(const double* __re
                                                               const double* __restrict__ pz,
                                                               const int* __restrict__ owner, int64_t n,
                                                               double* __restrict__ w) {
-  extern __shared__ double becke_tab[];  // per warp: kTabPts x natm point-atom distances
+  extern __shared__ double becke_sm[];
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
-  double* tab = becke_tab + (threadIdx.x >> 5) * kTabPts * natm;
+  const int mw = (natm + 31) / 32;
+  unsigned* wmask = reinterpret_cast<unsigned*>(reinterpret_cast<char*>(becke_sm) +
+                                                (threadIdx.x >> 5) * becke_warp_smem(natm));
+  double* tab = reinterpret_cast<double*>(wmask + 32 * mw);  // natm <= kTabAtoms only
+  const bool use_tab = natm <= kTabAtoms;
   const bool live = p < n;  // every lane takes part in the warp's rounds
   double x = 0.0, y = 0.0, z = 0.0;
   int a = -1;
@@ -237,7 +250,6 @@ __global__ void __launch_bounds__(kBeckeThreads) k_becke_warp(const double* __re
   };
   int nb[4] = {-1, -1, -1, -1};
   double nr[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
-  unsigned mask[kMaskWords] = {};
   int cnt = 0;
   double P0 = 0.0, tau = 0.0;
   int i0 = -1;
@@ -257,7 +269,12 @@ __global__ void __launch_bounds__(kBeckeThreads) k_becke_warp(const double* __re
     i0 = nb[0];
     P0 = ordered(i0, x, y, z, 0.0);
     tau = fmax(0x1p-56 * P0 / natm, 0x1p-1000);
+    unsigned word = 0;
     for (int i = 0; i < natm; ++i) {
+      if ((i & 31) == 0 && i > 0) {
+        wmask[32 * ((i >> 5) - 1) + lane] = word;
+        word = 0;
+      }
       if (i == i0) continue;
       const double ri = dist3(__ldg(atoms + 3 * i), __ldg(atoms + 3 * i + 1), __ldg(atoms + 3 * i + 2), x, y, z);
       const double* Ri = dist + (int64_t)i * natm;
@@ -272,11 +289,15 @@ __global__ void __launch_bounds__(kBeckeThreads) k_becke_warp(const double* __re
         if (d > -__dmul_rn(kBeckeEdge, R)) Q *= becke_s(d, R, __ldg(Yi + k));
       }
       if (Q >= tau) {
-        mask[i >> 5] |= 1u << (i & 31);
+        word |= 1u << (i & 31);
         ++cnt;
       }
     }
+    wmask[32 * (mw - 1) + lane] = word;
+  } else {
+    for (int u = 0; u < mw; ++u) wmask[32 * u + lane] = 0u;
   }
+  __syncwarp();
   // the warp's pending pairs: lane l's are positions off .. off + cnt - 1, ascending atom
   int off = cnt;
 #pragma unroll
@@ -308,9 +329,6 @@ __global__ void __launch_bounds__(kBeckeThreads) k_becke_warp(const double* __re
       if (cand < 32 && oc <= q) ol = cand;
     }
     const int j = q - __shfl_sync(0xffffffffu, off, ol);  // rank of the pair among the owner's
-    unsigned m[kMaskWords];
-#pragma unroll
-    for (int u = 0; u < kMaskWords; ++u) m[u] = __shfl_sync(0xffffffffu, mask[u], ol);
     const double qx = __shfl_sync(0xffffffffu, x, ol), qy = __shfl_sync(0xffffffffu, y, ol),
                  qz = __shfl_sync(0xffffffffu, z, ol), qt = __shfl_sync(0xffffffffu, tau, ol);
     // the round's points in lane order (owners ascend with the position);
@@ -318,7 +336,7 @@ __global__ void __launch_bounds__(kBeckeThreads) k_becke_warp(const double* __re
     const int olp = __shfl_up_sync(0xffffffffu, ol, 1);
     const unsigned fm = __ballot_sync(0xffffffffu, q < total && (lane == 0 || olp != ol));
     const int jd = __popc(fm & ((2u << lane) - 1u)) - 1;
-    const int md = min(__popc(fm), kTabPts);
+    const int md = use_tab ? min(__popc(fm), kTabPts) : 0;
     __syncwarp();  // the previous round's reads of the table are done
     for (int jt = 0; jt < md; ++jt) {
       const int src = __shfl_sync(0xffffffffu, ol, (int)__fns(fm, 0, jt + 1));
@@ -332,15 +350,16 @@ __global__ void __launch_bounds__(kBeckeThreads) k_becke_warp(const double* __re
     double P = 0.0;
     if (q < total) {
       int r = j;
-      for (int u = 0; u < kMaskWords; ++u) {
-        const int c = __popc(m[u]);
+      for (int u = 0; u < mw; ++u) {
+        const unsigned mu = wmask[32 * u + ol];
+        const int c = __popc(mu);
         if (r < c) {
-          pi = 32 * u + (int)__fns(m[u], 0, r + 1);
+          pi = 32 * u + (int)__fns(mu, 0, r + 1);
           break;
         }
         r -= c;
       }
-      P = jd < kTabPts ? ordered_tab(pi, tab + jd * natm, qt) : ordered(pi, qx, qy, qz, qt);
+      P = jd < md ? ordered_tab(pi, tab + jd * natm, qt) : ordered(pi, qx, qy, qz, qt);
     }
     // hand the round's products to their points' lanes, in position order
     for (int t = 0; t < 32; ++t) {
@@ -369,7 +388,7 @@ cudaError_t launch_becke(const double* atoms, double* dist, int natm, const doub
   if (e != cudaSuccess || n == 0) return e;
   const unsigned nb = (unsigned)((n + kBeckeThreads - 1) / kBeckeThreads);
   if (natm <= kBeckeWarpAtoms)
-    k_becke_warp<<<nb, kBeckeThreads, (kBeckeThreads / 32) * kTabPts * natm * sizeof(double), st>>>(
+    k_becke_warp<<<nb, kBeckeThreads, (kBeckeThreads / 32) * becke_warp_smem(natm), st>>>(
         atoms, dist, rdist, natm, px, py, pz, owner, n, w);
   else
     k_becke_thread<<<nb, kBeckeThreads, 0, st>>>(atoms, dist, rdist, natm, px, py, pz, owner, n, w);

@@ -99,6 +99,17 @@ def test_device_becke_140_atoms_matches_oracle():
     _becke_agreement(c)
 
 
+def test_device_becke_300_atoms_matches_oracle():
+    """300 atoms: beyond the distance table (every lane forms its own
+    distances) with ten-word survivor masks; the weights still match the
+    oracle to 2e-16."""
+    rng = np.random.default_rng(29)
+    els, xyz = cases.random_cluster(rng, [("C", 150), ("H", 150)], 23.0, 1.1)
+    c = cases.build_case("becke300", els, xyz, seed=29, exp_range=(0.1, 100.0), nrad=2, nang=26,
+                         functional="VWN", nocc=1, orthonormalise=False)
+    _becke_agreement(c)
+
+
 @LAYOUTS
 def test_raw_weight_grid_is_becke_scaled_on_device(thr):
     c = cases.small_case(functional="PBE", seed=9)
