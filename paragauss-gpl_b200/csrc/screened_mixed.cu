@@ -225,11 +225,14 @@ __global__ void __launch_bounds__(kBlock4(192)) k_sm_gather_B(const int64_t* __r
 // ---------------------------------------------------------------------------
 // X = phi_t P[S_t, S_t] with fused rho / grad rho
 // ---------------------------------------------------------------------------
-// epilogue operands: phi (and grad phi) of 6 slots x 128 points per buffer
-constexpr int kECols = 6;
-constexpr int kERing = 4;
-constexpr int kEGroups = 24 / kECols;  // staged groups per column half of a slot block
-constexpr int kEBuf = 4 * kECols * 128;  // doubles
+// epilogue operands: phi (and grad phi) of 4 slots x 128 points per buffer;
+// the 12 epilogue warps take the three 16-column thirds of each 48-slot
+// block, and each third has two ring buffers
+constexpr int kECols = 4;
+constexpr int kEThirds = 3;
+constexpr int kERing = 2 * kEThirds;
+constexpr int kEGroups = kN / kEThirds / kECols;  // staged groups per column third of a slot block
+constexpr int kEBuf = 4 * kECols * 128;           // doubles
 struct DensSmem {
   alignas(1024) int8_t a[kDStages][kOpA];
   alignas(1024) int8_t b[kDStages][kOpB];
@@ -242,12 +245,14 @@ struct DensSmem {
   uint64_t e_empty[kERing];
   uint32_t tslot;
 };
-// warps 0-7 epilogue, 8 MMA, 9 operand copies, 10 epilogue-operand copies
-constexpr int kDensThreads = tc::kWholeSmThreads;  // warps 11-15 idle
+// warps 0-7 and 11-14 epilogue (three per TMEM lane quarter), 8 MMA, 9 operand
+// copies, 10 epilogue-operand copies, 15 idle
+constexpr int kDensThreads = tc::kWholeSmThreads;
+constexpr int kDensEpiWarps = 12;
 
-// TMEM -> the 24 combined FP64 values of column half `half` of one
-// accumulator set (columns 24 half .. 24 half + 23 of each group; taddr is the
-// set's first column at this warp's lane quarter): 16 columns, then 8.
+// TMEM -> the W combined FP64 values of W consecutive columns of one
+// accumulator set (taddr: the first of them in group 0, at this warp's lane
+// quarter; the five digit groups are kN columns apart).
 template <int W>
 __device__ __forceinline__ void acc_cols(uint32_t taddr, double* x) {
   uint32_t r[kGroups][W];
@@ -268,11 +273,6 @@ __device__ __forceinline__ void acc_cols(uint32_t taddr, double* x) {
     x[c] = oz_combine(v);
   }
 }
-__device__ __forceinline__ void read_acc24(uint32_t taddr, int half, double (&x)[24]) {
-  acc_cols<16>(taddr + half * 24, x);
-  acc_cols<8>(taddr + half * 24 + 16, x + 16);
-}
-
 // Persistent: CTA c takes the chunk's tiles c, c + G, c + 2G, ... (G = grid
 // size); the copy / MMA / epilogue pipeline runs on across tile boundaries.
 // rho and grad rho are accumulated with atomics (the two column halves of a
@@ -298,11 +298,11 @@ __global__ void __launch_bounds__(kDensThreads, 1)
     }
     for (int b = 0; b < 2; ++b) {
       tc::mbar_init(&S.acc_full[b], 1);
-      tc::mbar_init(&S.acc_empty[b], 256);
+      tc::mbar_init(&S.acc_empty[b], 32 * kDensEpiWarps);
     }
     for (int r = 0; r < kERing; ++r) {
       tc::mbar_init(&S.e_full[r], 1);
-      tc::mbar_init(&S.e_empty[r], 128);
+      tc::mbar_init(&S.e_empty[r], 128);  // the four warps of one column third
     }
     tc::mbar_fence_init();
   }
@@ -312,7 +312,7 @@ __global__ void __launch_bounds__(kDensThreads, 1)
   const uint32_t tbase = S.tslot;
   bool ok = true;
   if (warp == 10) {
-    if (lane == 0) {  // epilogue operands: per slot block j, half h, group u: kECols slots of phi (grad phi)
+    if (lane == 0) {  // epilogue operands: per slot block j, group u, third h: kECols slots of phi (grad phi)
       int e = 0;
       for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
         const int64_t sb = tso[t0 + ti] - s0;
@@ -320,13 +320,13 @@ __global__ void __launch_bounds__(kDensThreads, 1)
         const int nN = (n + kN - 1) / kN;
         for (int j = 0; j < nN && ok; ++j) {
           for (int u = 0; u < kEGroups && ok; ++u)
-            for (int h = 0; h < 2; ++h, ++e) {
+            for (int h = 0; h < kEThirds; ++h, ++e) {
               const int r = e % kERing;
               if (e >= kERing && !tc::mbar_wait(&S.e_empty[r], ((e / kERing) - 1) & 1)) {
                 ok = false;
                 break;
               }
-              const int c0 = j * kN + h * 24 + u * kECols;
+              const int c0 = j * kN + h * (kN / kEThirds) + u * kECols;
               const int nc = max(0, min(kECols, n - c0));
               if (nc == 0) {
                 tc::mbar_arrive(&S.e_full[r]);
@@ -399,10 +399,10 @@ __global__ void __launch_bounds__(kDensThreads, 1)
       }
       if (!ok) atomicExch(err, 1);
     }
-  } else if (warp >= 11) {
+  } else if (warp >= 15) {
     // idle: the CTA holds the whole SM
-  } else {  // epilogue: point row = 32 (warp & 3) + lane, columns 24 (warp >> 2) .. +24 of each slot block
-    const int row = (warp & 3) * 32 + lane, half = warp >> 2;
+  } else {  // epilogue: point row = 32 (warp & 3) + lane, columns 16 third .. +15 of each slot block
+    const int row = (warp & 3) * 32 + lane, third = warp < 8 ? (warp >> 2) : 2;
     const uint32_t trow = tbase + ((uint32_t)((warp & 3) * 32) << 16);
     int jj = 0;
     for (int64_t ti = blockIdx.x; ti < nt && ok; ti += gridDim.x) {
@@ -414,26 +414,26 @@ __global__ void __launch_bounds__(kDensThreads, 1)
       double r_acc = 0.0, g_acc[3] = {0.0, 0.0, 0.0};
       for (int j = 0; j < nN && ok; ++j, ++jj) {
         const int b = jj & 1;
-        // the P row scale of column lane (< 24) of this warp's half, broadcast below
-        const int cl = j * kN + half * 24 + lane;
-        const double psl = (lane < 24 && cl < n) ? __ldg(ps + sb + cl) : 0.0;
+        // the P row scale of column lane (< 16) of this warp's third, broadcast below
+        const int cl = j * kN + third * 16 + lane;
+        const double psl = (lane < 16 && cl < n) ? __ldg(ps + sb + cl) : 0.0;
         if (!tc::mbar_wait_warp(&S.acc_full[b], (jj >> 1) & 1)) {
           ok = false;
           break;
         }
         tc::fence_after_sync();
-        double x[24];
-        read_acc24(trow + b * kAccCols, half, x);
+        double x[16];
+        acc_cols<16>(trow + b * kAccCols + third * 16, x);
         tc::fence_before_sync();
         tc::mbar_arrive(&S.acc_empty[b]);
 #pragma unroll
         for (int u = 0; u < kEGroups; ++u) {
-          const int e = (jj * kEGroups + u) * 2 + half, r = e % kERing;
+          const int e = (jj * kEGroups + u) * kEThirds + third, r = e % kERing;
           if (!tc::mbar_wait(&S.e_full[r], (e / kERing) & 1)) {
             ok = false;
             break;
           }
-          const int c0 = j * kN + half * 24 + u * kECols;
+          const int c0 = j * kN + third * 16 + u * kECols;
           const double* eb = S.e[r];
           const GT* eg = reinterpret_cast<const GT*>(eb + kECols * 128);
 #pragma unroll
