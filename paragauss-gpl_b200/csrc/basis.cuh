@@ -324,8 +324,10 @@ __device__ __forceinline__ unsigned long long item_u64(unsigned w, int k) {
 
 // GT: the element type of the gradient planes (double; float in the INT8
 // build, whose potential and density gradient tolerate 24-bit gradients).
+// f shells: at most 128 registers (four blocks per SM; 164 registers and
+// three blocks without the bound, the slower form for the 500-atom grid).
 template <int L, bool GRAD, typename GT = double>
-__global__ void __launch_bounds__(128) k_basis_items(const BasisItem* __restrict__ items, int64_t nitems,
+__global__ void __launch_bounds__(128, L >= 3 ? 4 : 1) k_basis_items(const BasisItem* __restrict__ items, int64_t nitems,
                                                      const double* __restrict__ exps, const double* __restrict__ norms,
                                                      const double* __restrict__ contr,
                                                      const int2* __restrict__ rng, DevSA sa,
