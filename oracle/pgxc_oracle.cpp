@@ -1840,7 +1840,8 @@ int oracle_xc_gradient(const pgxc_geometry* geo, const pgxc_basis* bas, const pg
   const double* gz = gy + npts;
   const double* wr = gz + npts;
   const int* host = grid->point_atom;
-  const bool gga = PGXC_XC_IS_GGA(xc);
+  const bool mgga = PGXC_XC_IS_MGGA(xc);
+  const bool gga = PGXC_XC_IS_GGA(xc) || mgga;
   std::vector<int> fatom((size_t)nb);
   for (const Shell& S : B.shells)
     for (int f = 0; f < (2 * S.l + 1) * S.nrad; ++f) fatom[(size_t)S.f0 + f] = S.atom;
@@ -1910,7 +1911,7 @@ int oracle_xc_gradient(const pgxc_geometry* geo, const pgxc_basis* bas, const pg
     const double Wh = W_of(-1).v;
     const double w = wr[p] * Wh;
     // density from the occupied orbitals (density_calc_nl), and X' = P phi, Y'_j = P d_j phi
-    double rho[2] = {0, 0}, grr[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    double rho[2] = {0, 0}, grr[2][3] = {{0, 0, 0}, {0, 0, 0}}, tau[2] = {0, 0};
     std::vector<double> Xs((size_t)ispin * nb, 0.0), Yj((size_t)ispin * 3 * nb, 0.0);
     for (int s = 0; s < ispin; ++s) {
       const double* Cs = C + (size_t)s * nb * nocc;
@@ -1924,6 +1925,7 @@ int oracle_xc_gradient(const pgxc_geometry* geo, const pgxc_basis* bas, const pg
         const double o = occ[j + (size_t)nocc * s];
         rho[s] += o * psi * psi;
         for (int c = 0; c < 3; ++c) grr[s][c] += 2.0 * o * psi * dpsi[c];
+        tau[s] += 0.5 * o * (dpsi[0] * dpsi[0] + dpsi[1] * dpsi[1] + dpsi[2] * dpsi[2]);
         for (int64_t f = 0; f < nb; ++f) {
           const double cf = o * Cs[f + (size_t)nb * j];
           Xs[(size_t)s * nb + f] += cf * psi;
@@ -1936,12 +1938,16 @@ int oracle_xc_gradient(const pgxc_geometry* geo, const pgxc_basis* bas, const pg
       gam[0] += grr[0][c] * grr[0][c];
       if (ispin == 2) { gam[1] += grr[1][c] * grr[1][c]; gam[2] += grr[0][c] * grr[1][c]; }
     }
-    double F, Fr[2], Fg[3];
-    functional_point(xc, ispin, rho, gam, F, Fr, Fg);
+    double F, Fr[2], Fg[3], Ft[2] = {0, 0};
+    if (mgga) mgga::mgga_point(mgga_set(xc), ispin, rho, gam, tau, F, Fr, Fg, Ft);
+    else functional_point(xc, ispin, rho, gam, F, Fr, Fg);
     E += w * F;
-    double a[2], b[2][3];
+    // meta-GGAs: tau_s = 1/2 sum_j d_j phi P_s d_j phi moves with the functions
+    // through d_k d_j phi (nuc_grad_tau of modules/post_scf_module.f90)
+    double a[2], b[2][3], ct[2];
     for (int s = 0; s < ispin; ++s) {
       a[s] = w * Fr[s];
+      ct[s] = w * Ft[s];
       for (int c = 0; c < 3; ++c)
         b[s][c] = !gga ? 0.0 : (ispin == 1 ? w * 2.0 * Fg[0] * grr[0][c]
                                            : w * (2.0 * Fg[s] * grr[s][c] + Fg[2] * grr[1 - s][c]));
@@ -1956,6 +1962,8 @@ int oracle_xc_gradient(const pgxc_geometry* geo, const pgxc_basis* bas, const pg
           for (int j = 0; j < 3; ++j)
             t += b[s][j] * (val[10 * f + 4 + hx(k, j)] * X + val[10 * f + 1 + k] * Yj[((size_t)s * 3 + j) * nb + f]);
           q[k] += 2.0 * t;
+          if (mgga)
+            for (int j = 0; j < 3; ++j) q[k] += ct[s] * val[10 * f + 4 + hx(k, j)] * Yj[((size_t)s * 3 + j) * nb + f];
         }
       }
       for (int k = 0; k < 3; ++k) {

@@ -9,6 +9,7 @@
 #include "dgemm.cuh"
 #include "gradient.h"
 #include "xc_functional.cuh"
+#include "xc_mgga.cuh"
 
 namespace pgxc {
 
@@ -191,19 +192,24 @@ __device__ __forceinline__ int hidx(int c, int d) {
   return a == 0 ? b : (a == 1 ? 2 + b : 5);
 }
 
-__global__ void k_grad_points(XcConst K, bool gga, int ispin, int64_t nbas, int64_t ld, int64_t p0, int64_t nvalid,
-                              const double* __restrict__ w, const double* __restrict__ wraw,
+// coef planes per spin: a, b_x, b_y, b_z, c (c = w df/dtau, meta-GGAs)
+constexpr int kCoefPlanes = 5;
+
+__global__ void k_grad_points(XcConst K, int functional, bool gga, int ispin, int64_t nbas, int64_t ld, int64_t p0,
+                              int64_t nvalid, const double* __restrict__ w, const double* __restrict__ wraw,
                               const double* __restrict__ B, int64_t plane, const double* __restrict__ XY,
                               double* __restrict__ coef, double* __restrict__ ef, double* __restrict__ exc) {
   const int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= ld) return;
   if (p >= nvalid) {
     for (int s = 0; s < ispin; ++s)
-      for (int c = 0; c < 4; ++c) coef[(4 * s + c) * ld + p] = 0.0;
+      for (int c = 0; c < kCoefPlanes; ++c) coef[(kCoefPlanes * s + c) * ld + p] = 0.0;
     ef[p] = 0.0;
     return;
   }
-  double rho[2] = {0, 0}, gr[2][3] = {{0, 0, 0}, {0, 0, 0}};
+  const bool mgga = PGXC_XC_IS_MGGA(functional);
+  // rho_s, grad rho_s and (meta-GGAs) tau_s = 1/2 sum_j d_j phi P_s d_j phi = 1/2 sum_j,f d_j phi_f Y_j,f
+  double rho[2] = {0, 0}, gr[2][3] = {{0, 0, 0}, {0, 0, 0}}, tau[2] = {0, 0};
   for (int s = 0; s < ispin; ++s) {
     const double* X = XY + (4 * s) * plane;
     for (int64_t f = 0; f < nbas; ++f) {
@@ -211,28 +217,34 @@ __global__ void k_grad_points(XcConst K, bool gga, int ispin, int64_t nbas, int6
       rho[s] += B[f * ld + p] * xv;
       if (gga)
         for (int c = 0; c < 3; ++c) gr[s][c] += 2.0 * B[(1 + c) * plane + f * ld + p] * xv;
+      if (mgga)
+        for (int c = 0; c < 3; ++c) tau[s] += 0.5 * B[(1 + c) * plane + f * ld + p] * X[(1 + c) * plane + f * ld + p];
     }
   }
   const double wp = w[p0 + p];
-  double f = 0.0, fr[2] = {0, 0}, fg[3] = {0, 0, 0};
+  double f = 0.0, fr[2] = {0, 0}, fg[3] = {0, 0, 0}, ft[2] = {0, 0};
   if (ispin == 1) {
     const double g = gr[0][0] * gr[0][0] + gr[0][1] * gr[0][1] + gr[0][2] * gr[0][2];
-    if (gga) xc_gga(K, rho[0], g, f, fr[0], fg[0]);
+    if (mgga) mgga::mgga_closed(functional, rho[0], g, tau[0], f, fr[0], fg[0], ft[0]);
+    else if (gga) xc_gga(K, rho[0], g, f, fr[0], fg[0]);
     else xc_vwn(K, rho[0], f, fr[0]);
     coef[p] = wp * fr[0];
     for (int c = 0; c < 3; ++c) coef[(1 + c) * ld + p] = gga ? wp * 2.0 * fg[0] * gr[0][c] : 0.0;
+    coef[4 * ld + p] = wp * ft[0];
   } else {
     const double r2[2] = {rho[0], rho[1]};
     const double g3[3] = {gr[0][0] * gr[0][0] + gr[0][1] * gr[0][1] + gr[0][2] * gr[0][2],
                           gr[1][0] * gr[1][0] + gr[1][1] * gr[1][1] + gr[1][2] * gr[1][2],
                           gr[0][0] * gr[1][0] + gr[0][1] * gr[1][1] + gr[0][2] * gr[1][2]};
     double fr2[2], fg3[3];
-    if (gga) xc_open<true>(K, r2, g3, f, fr2, fg3);
+    if (mgga) mgga::mgga_open(functional, r2, g3, tau, f, fr2, fg3, ft);
+    else if (gga) xc_open<true>(K, r2, g3, f, fr2, fg3);
     else xc_open<false>(K, r2, g3, f, fr2, fg3);
     for (int s = 0; s < 2; ++s) {
-      coef[(4 * s) * ld + p] = wp * fr2[s];
+      coef[(kCoefPlanes * s) * ld + p] = wp * fr2[s];
       for (int c = 0; c < 3; ++c)
-        coef[(4 * s + 1 + c) * ld + p] = gga ? wp * (2.0 * fg3[s] * gr[s][c] + fg3[2] * gr[1 - s][c]) : 0.0;
+        coef[(kCoefPlanes * s + 1 + c) * ld + p] = gga ? wp * (2.0 * fg3[s] * gr[s][c] + fg3[2] * gr[1 - s][c]) : 0.0;
+      coef[(kCoefPlanes * s + 4) * ld + p] = wp * ft[s];
     }
   }
   ef[p] = wraw[p0 + p] * f;
@@ -248,7 +260,7 @@ __global__ void k_grad_points(XcConst K, bool gga, int ispin, int64_t nbas, int6
 // per-atom sums.
 constexpr int kGradFB = 32;
 
-__global__ void __launch_bounds__(256) k_grad_orb(bool gga, int ispin, int64_t nbas, int64_t ld, int64_t p0,
+__global__ void __launch_bounds__(256) k_grad_orb(bool gga, bool mgga, int ispin, int64_t nbas, int64_t ld, int64_t p0,
                                                   int64_t nvalid, int natm, const int* __restrict__ fatom,
                                                   const int* __restrict__ owner, const double* __restrict__ B,
                                                   int64_t plane, const double* __restrict__ XY,
@@ -263,12 +275,13 @@ __global__ void __launch_bounds__(256) k_grad_orb(bool gga, int ispin, int64_t n
   const int lane = threadIdx.x & 31;
   const int64_t f0 = (int64_t)blockIdx.x * kGradFB, f1 = min(nbas, f0 + kGradFB);
   // the point's coefficients, once for all its functions
-  double a[2] = {0, 0}, b[2][3] = {{0, 0, 0}, {0, 0, 0}};
+  double a[2] = {0, 0}, b[2][3] = {{0, 0, 0}, {0, 0, 0}}, ct[2] = {0, 0};
   if (live)
     for (int sp = 0; sp < ispin; ++sp) {
-      a[sp] = coef[(4 * sp) * ld + p];
+      a[sp] = coef[(kCoefPlanes * sp) * ld + p];
       if (gga)
-        for (int j = 0; j < 3; ++j) b[sp][j] = coef[(4 * sp + 1 + j) * ld + p];
+        for (int j = 0; j < 3; ++j) b[sp][j] = coef[(kCoefPlanes * sp + 1 + j) * ld + p];
+      if (mgga) ct[sp] = coef[(kCoefPlanes * sp + 4) * ld + p];
     }
   double t[3] = {0, 0, 0};
   for (int64_t f = f0; f < f1; ++f) {
@@ -289,6 +302,9 @@ __global__ void __launch_bounds__(256) k_grad_orb(bool gga, int ispin, int64_t n
           double u = 0.0;
           for (int j = 0; j < 3; ++j) u += b[sp][j] * (H[hidx(k, j)] * X + d[k] * Yj[j]);
           q[k] += 2.0 * u;
+          // meta-GGAs: tau moves with the functions through d_k d_j phi
+          if (mgga)
+            for (int j = 0; j < 3; ++j) q[k] += ct[sp] * H[hidx(k, j)] * Yj[j];
         }
       }
     }
@@ -567,21 +583,21 @@ void launch_basis_hess(const BuildArgs& a, int64_t p0, int64_t nvalid, int64_t l
   launch_hess_l<3>(a, p0, nvalid, ld, plane, out, st);
 }
 
-void launch_grad_points(const XcConst& K, bool gga, int ispin, int64_t nbas, int64_t ld, int64_t p0, int64_t nvalid,
-                        const double* w, const double* wraw, const double* basis, int64_t plane, const double* XY,
-                        double* coef, double* ef, double* exc, cudaStream_t st) {
-  k_grad_points<<<(unsigned)((ld + 127) / 128), 128, 0, st>>>(K, gga, ispin, nbas, ld, p0, nvalid, w, wraw, basis,
-                                                               plane, XY, coef, ef, exc);
+void launch_grad_points(const XcConst& K, int functional, bool gga, int ispin, int64_t nbas, int64_t ld, int64_t p0,
+                        int64_t nvalid, const double* w, const double* wraw, const double* basis, int64_t plane,
+                        const double* XY, double* coef, double* ef, double* exc, cudaStream_t st) {
+  k_grad_points<<<(unsigned)((ld + 127) / 128), 128, 0, st>>>(K, functional, gga, ispin, nbas, ld, p0, nvalid, w,
+                                                               wraw, basis, plane, XY, coef, ef, exc);
 }
 
-void launch_grad_orbital(bool gga, int ispin, int64_t nbas, int64_t ld, int64_t p0, int64_t nvalid, int natm,
-                         const int* fatom, const int* owner, const double* basis, int64_t plane, const double* XY,
-                         const double* coef, double* grad, cudaStream_t st) {
+void launch_grad_orbital(bool gga, bool mgga, int ispin, int64_t nbas, int64_t ld, int64_t p0, int64_t nvalid,
+                         int natm, const int* fatom, const int* owner, const double* basis, int64_t plane,
+                         const double* XY, const double* coef, double* grad, cudaStream_t st) {
   const size_t smem = sizeof(double) * 3 * (kGradFB + natm);
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_grad_orb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   dim3 grid((unsigned)((nbas + kGradFB - 1) / kGradFB), (unsigned)((ld + 255) / 256));
-  k_grad_orb<<<grid, 256, smem, st>>>(gga, ispin, nbas, ld, p0, nvalid, natm, fatom, owner, basis, plane, XY, coef,
-                                      grad);
+  k_grad_orb<<<grid, 256, smem, st>>>(gga, mgga, ispin, nbas, ld, p0, nvalid, natm, fatom, owner, basis, plane, XY,
+                                      coef, grad);
 }
 
 void launch_grad_xy(const double* basis_j, int64_t ld, const double* P, int64_t ldc, int64_t nbas, double* out,

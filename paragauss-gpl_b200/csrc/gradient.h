@@ -27,21 +27,22 @@ namespace pgxc {
 void launch_basis_hess(const BuildArgs& a, int64_t p0, int64_t nvalid, int64_t ld, int64_t plane, double* out,
                        cudaStream_t st);
 
-// Per point of the chunk: rho_s, grad rho_s from X, Y and the basis values,
-// the functional, and the coefficients a_s, b_s (coef[(4 s + c) ld + p]) and
+// Per point of the chunk: rho_s, grad rho_s (and for meta-GGAs tau_s) from X,
+// Y and the basis values, the functional, and the coefficients a_s, b_s, c_s
+// (coef[(5 s + c) ld + p]; c_s = w df/dtau_s, 0 below meta-GGAs) and
 // ef = w_raw f; E_xc = sum w f is added into *exc.
 // out[f][p] = sum_g basis_j[g][p] P[g][f], f < nbas, p < ld (ld a multiple of
 // 64; basis_j followed by at least 15 more rows of ld; P ldc x ldc, zero past nbas)
 void launch_grad_xy(const double* basis_j, int64_t ld, const double* P, int64_t ldc, int64_t nbas, double* out,
                     cudaStream_t st);
-void launch_grad_points(const XcConst& K, bool gga, int ispin, int64_t nbas, int64_t ld, int64_t p0, int64_t nvalid,
-                        const double* w, const double* wraw, const double* basis, int64_t plane, const double* XY,
-                        double* coef, double* ef, double* exc, cudaStream_t st);
+void launch_grad_points(const XcConst& K, int functional, bool gga, int ispin, int64_t nbas, int64_t ld, int64_t p0,
+                        int64_t nvalid, const double* w, const double* wraw, const double* basis, int64_t plane,
+                        const double* XY, double* coef, double* ef, double* exc, cudaStream_t st);
 
 // The orbital terms: -sum_g q to atom(mu) (fatom[mu]) and +sum_mu q to host(g).
-void launch_grad_orbital(bool gga, int ispin, int64_t nbas, int64_t ld, int64_t p0, int64_t nvalid, int natm,
-                         const int* fatom, const int* owner, const double* basis, int64_t plane, const double* XY,
-                         const double* coef, double* grad, cudaStream_t st);
+void launch_grad_orbital(bool gga, bool mgga, int ispin, int64_t nbas, int64_t ld, int64_t p0, int64_t nvalid,
+                         int natm, const int* fatom, const int* owner, const double* basis, int64_t plane,
+                         const double* XY, const double* coef, double* grad, cudaStream_t st);
 
 // The weight term sum_g ef_g dW_host(r_g)/dR over the chunk's points; dist is
 // the natm x natm atom distance matrix followed by its reciprocals (the

@@ -933,7 +933,7 @@ static int gradient_core(pgxc_ctx* c, int32_t nbas, int32_t ispin, int64_t kpad,
   // context for the next call (allocation and release of several GB per call
   // would cost more than the gradient's kernels)
   const size_t sizes[8] = {sizeof(double) * 10 * plane,         sizeof(double) * 4 * ispin * plane,
-                           sizeof(double) * 4 * ispin * ld,      sizeof(double) * (size_t)round_up(c->npts, ld),
+                           sizeof(double) * 5 * ispin * ld,      sizeof(double) * (size_t)round_up(c->npts, ld),
                            sizeof(double) * 3 * c->natm,         sizeof(double),
                            sizeof(double) * ((size_t)7 * c->natm * ldw / 2 + 1), sizeof(int) * (size_t)nbas};
   size_t offs[8], total = 0;
@@ -961,7 +961,8 @@ static int gradient_core(pgxc_ctx* c, int32_t nbas, int32_t ispin, int64_t kpad,
   double* de = (double*)(base + offs[5]);
   double* wscr = (double*)(base + offs[6]);
   int* dfatom = (int*)(base + offs[7]);
-  const bool gga = PGXC_XC_IS_GGA(c->opt.functional);
+  const bool mgga = PGXC_XC_IS_MGGA(c->opt.functional);
+  const bool gga = PGXC_XC_IS_GGA(c->opt.functional) || mgga;
   int rc = PGXC_OK;
   do {
     if (cudaMemcpyAsync(dfatom, fatom.data(), sizeof(int) * nbas, cudaMemcpyHostToDevice, s) != cudaSuccess ||
@@ -981,9 +982,10 @@ static int gradient_core(pgxc_ctx* c, int32_t nbas, int32_t ispin, int64_t kpad,
         }
       }
       if (rc) break;
-      launch_grad_points(a.xc, gga, ispin, nbas, ld, p0, nv, a.w, c->d_wraw, basis, plane, XY, coef, ef + p0, de, s);
-      launch_grad_orbital(gga, ispin, nbas, ld, p0, nv, c->natm, dfatom, c->d_owner, basis, plane, XY, coef, dgrad,
-                          s);
+      launch_grad_points(a.xc, c->opt.functional, gga, ispin, nbas, ld, p0, nv, a.w, c->d_wraw, basis, plane, XY,
+                         coef, ef + p0, de, s);
+      launch_grad_orbital(gga, mgga, ispin, nbas, ld, p0, nv, c->natm, dfatom, c->d_owner, basis, plane, XY, coef,
+                          dgrad, s);
       if (cudaGetLastError() != cudaSuccess) rc = set_err(c, PGXC_ECUDA, "gradient kernel launch failed");
     }
     if (rc) break;
@@ -1017,8 +1019,6 @@ static int gradient_core(pgxc_ctx* c, int32_t nbas, int32_t ispin, int64_t kpad,
 
 static int gradient_checks(pgxc_ctx* c, double* grad) {
   if (!grad) return set_err(c, PGXC_EINVAL, "NULL output");
-  if (PGXC_XC_IS_MGGA(c->opt.functional))
-    return set_err(c, PGXC_ENOTSUP, "the XC gradient of a meta-GGA is not supported");
   if (!c->d_owner)
     return set_err(c, PGXC_ENOTSUP, "the XC gradient needs a grid created with raw weights and point_atom "
                                     "(the grid moves with its atoms)");

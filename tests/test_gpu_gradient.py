@@ -1,6 +1,6 @@
 """Post-SCF XC nuclear gradient on the device (pgxc_xc_gradient) against the
 oracle's independent restatement (itself checked against finite differences
-in tests/test_gradient.py); every layout, both spins, LDA and GGA."""
+in tests/test_gradient.py); every layout, both spins, LDA, GGA and meta-GGA."""
 import numpy as np
 import pytest
 
@@ -19,6 +19,23 @@ def test_gradient_matches_oracle(xc, ispin, lmax, layout):
     if ispin == 2 and thr < 0:
         pytest.skip("the dense layout is closed shell")
     case = cases.small_case(functional=xc, seed=62, natoms=4, nocc=5, ispin=ispin, lmax=lmax)
+    ref, re = O.xc_gradient(case)
+    with lib.Context(case, weighted=False, precision=precision, screen_threshold=thr) as ctx:
+        g, e = ctx.xc_gradient()
+    scale = max(1.0, float(np.max(np.abs(ref))))
+    assert abs(e - re) < 1e-10 * max(1.0, abs(re))
+    np.testing.assert_allclose(g, ref, rtol=0, atol=1e-10 * scale)
+    np.testing.assert_allclose(g.sum(0), 0.0, atol=1e-9 * scale)
+
+
+@pytest.mark.parametrize("layout", [("fp64", 0.0), ("mixed", 1e-10)], ids=["screened", "int8-screened"])
+@pytest.mark.parametrize("xc,ispin", [("TPSS", 1), ("TPSS", 2), ("M06L", 2), ("VSXC", 1)])
+def test_mgga_gradient_matches_oracle(xc, ispin, layout):
+    """Meta-GGAs: tau and df/dtau per point, and the tau terms (d_k d_j phi Y_j)
+    in the orbital sums; the oracle's form is checked against finite
+    differences in tests/test_gradient.py."""
+    precision, thr = layout
+    case = cases.small_case(functional=xc, seed=64, natoms=4, nocc=5, ispin=ispin, lmax=2)
     ref, re = O.xc_gradient(case)
     with lib.Context(case, weighted=False, precision=precision, screen_threshold=thr) as ctx:
         g, e = ctx.xc_gradient()

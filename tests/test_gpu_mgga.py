@@ -116,10 +116,6 @@ def test_tpss_rejections():
     with lib.Context(c, screen_threshold=0.0) as ctx:
         with pytest.raises(lib.PgxcError):
             ctx.xc_energies(["TPSS"])
-    d = cases.small_case(functional="TPSS", seed=46)
-    with lib.Context(d, weighted=False, screen_threshold=0.0) as ctx:
-        with pytest.raises(lib.PgxcError):
-            ctx.xc_gradient()
 
 
 @pytest.mark.parametrize("xc", ["TPSS", "M06L"])

@@ -24,9 +24,12 @@ def _displaced(case, atom, k, h):
     return c
 
 
-@pytest.mark.parametrize("xc,ispin", [("VWN", 1), ("PBE", 1), ("BLYP", 2), ("PBE", 2), ("PW91", 2)])
+@pytest.mark.parametrize("xc,ispin", [("VWN", 1), ("PBE", 1), ("BLYP", 2), ("PBE", 2), ("PW91", 2),
+                                     ("TPSS", 1), ("TPSS", 2), ("M06L", 2), ("VSXC", 2)])
 def test_gradient_matches_finite_differences(xc, ispin):
-    """(closed-shell LYP is left out: its df/dgamma is not the derivative of its energy)"""
+    """(closed-shell LYP is left out: its df/dgamma is not the derivative of its energy; the same
+    holds for the closed-shell derivatives of the VSXC family, which the meta-GGA cases therefore
+    take open shell; the meta-GGAs add the terms of tau moving with the functions)"""
     case = cases.small_case(functional=xc, seed=61, natoms=3, nocc=4, ispin=ispin, nrad=14, lmax=2)
     g, e = O.xc_gradient(case)
     assert abs(e - _energy(case)) < 1e-11
