@@ -389,8 +389,12 @@ int pgxc_xc_gradient(pgxc_ctx* ctx, const double* C, const double* occ,
  * and density pass, then one functional pass per entry of functionals[n];
  * exc[i] is overwritten with the energy of functionals[i], *nel (may be NULL)
  * with the integrated charge.  Needs a screened context (PGXC_ENOTSUP
- * otherwise); a GGA functional needs a context created with a GGA
- * functional (its density gradients).  No potential is built.
+ * otherwise); a GGA functional needs a context created with a GGA or
+ * meta-GGA functional (its density gradients).  A meta-GGA (TPSS, M06L, M06,
+ * VSXC) also needs tau = 1/2 sum_i occ_i |grad psi_i|^2, which the pass forms
+ * (as the reference's post-SCF pass does) in a meta-GGA context or in a GGA
+ * context of the FP64 build; in an INT8 GGA context (FP32 gradient planes)
+ * it returns PGXC_ENOTSUP.  No potential is built.
  */
 int pgxc_xc_energies(pgxc_ctx* ctx, const double* C, const double* occ,
                      int32_t nbas, int32_t nocc, int32_t ispin,

@@ -1057,17 +1057,24 @@ int pgxc_xc_energies(pgxc_ctx* c, const double* C, const double* occ, int32_t nb
   if (st) return st;
   if (!c->screen) return set_err(c, PGXC_ENOTSUP, "pgxc_xc_energies needs a screened context (screen_threshold >= 0)");
   if (n < 1 || !functionals || !exc || (nocc > 0 && (!C || !occ))) return set_err(c, PGXC_EINVAL, "NULL or empty input");
-  const bool gga = PGXC_XC_IS_GGA(c->opt.functional);
+  // grad rho (and the gradient planes) exist in GGA and meta-GGA contexts
+  const bool gga = PGXC_XC_IS_GGA(c->opt.functional) || PGXC_XC_IS_MGGA(c->opt.functional);
   std::vector<XcConst> xcs((size_t)n);
   std::vector<int> ggas((size_t)n);
+  bool tau = false;
   for (int i = 0; i < n; ++i) {
     const int f = functionals[i];
     if (f < PGXC_XC_VWN || f > PGXC_XC_LAST) return set_err(c, PGXC_EINVAL, "functional id out of range");
-    if (PGXC_XC_IS_MGGA(f)) return set_err(c, PGXC_ENOTSUP, "pgxc_xc_energies: meta-GGA energies are not supported");
-    if (PGXC_XC_IS_GGA(f) && !gga)
+    const bool fg = PGXC_XC_IS_GGA(f) || PGXC_XC_IS_MGGA(f);
+    if (fg && !gga)
       return set_err(c, PGXC_EINVAL, "a GGA energy needs a context created with a GGA functional (no grad rho)");
-    xcs[i] = make_xc_const(f);
+    tau = tau || PGXC_XC_IS_MGGA(f);
+    if (!PGXC_XC_IS_MGGA(f)) xcs[i] = make_xc_const(f);
     ggas[i] = PGXC_XC_IS_GGA(f) ? 1 : 0;
+  }
+  if (tau) {  // meta-GGAs: the kinetic-energy density of the same orbitals
+    std::string e;
+    if ((st = screen_enable_tau(c->screen, e))) return set_err(c, st, e);
   }
   if (!all_finite(C, (int64_t)nbas * nocc * ispin) || !all_finite(occ, (int64_t)nocc * ispin))
     return set_err(c, PGXC_ENONFINITE, "non-finite C or occ");
@@ -1095,9 +1102,11 @@ int pgxc_xc_energies(pgxc_ctx* c, const double* C, const double* occ, int32_t nb
   ScreenExtra x;
   x.xc = xcs.data();
   x.gga = ggas.data();
+  x.fid = functionals;
   x.n = n;
   x.acc = d_acc;
   x.potential = false;
+  x.tau = tau;
   std::string e;
   if ((st = screen_run(c->screen, a, c->P2, s, c->d_ham, nullptr, e, &x))) return set_err(c, st, e);
   std::vector<double> h((size_t)4 * n);

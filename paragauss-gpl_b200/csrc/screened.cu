@@ -830,7 +830,7 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
         }
         ++T.launches;
       }
-      if (sp->mgga) {
+      if (sp->mgga || (extra && extra->tau)) {
         // 2 tau_j = sum_nu (d_j phi P)_nu d_j phi_nu: the density contraction with d_j phi in the
         // place of phi (FP64 DMMA in every precision mode)
         const int smem = gemm_smem_bytes<false, false>() + (int)sizeof(int) * sp->max_n;
@@ -913,7 +913,10 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
     }
     // further functionals on the same density (after K4, whose A and B they overwrite)
     for (int i = 0; extra && i < extra->n; ++i) {
-      if (ispin == 1) {
+      if (extra->fid && PGXC_XC_IS_MGGA(extra->fid[i])) {
+        launch_functional_mgga(extra->fid[i], ispin, sp->qw, sp->pt, sp->tq, cp, t0 * 128, npt, sp->partial,
+                               extra->acc + 4 * i, st);
+      } else if (ispin == 1) {
         BuildArgs bx = b[0];
         bx.w = sp->qw;
         bx.xc = extra->xc[i];
@@ -971,6 +974,21 @@ int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_
 #undef SR_TRY
   if (sp->keep) sp->basis_ready = true;  // a completed build has filled the resident basis values
   *tm = T;
+  return PGXC_OK;
+}
+
+int screen_enable_tau(ScreenPlan* sp, std::string& err) {
+  if (sp->tq) return PGXC_OK;
+  if (!sp->gga || sp->gf32) {
+    err = "meta-GGA energies need the FP64 gradient planes of a GGA (or a meta-GGA) context";
+    return PGXC_ENOTSUP;
+  }
+  const int64_t cp = sp->chunk_tiles * 128;
+  if (sp_alloc(sp, &sp->tq, 4 * (size_t)sp->ispin * cp) != cudaSuccess ||
+      cudaMemset(sp->tq, 0, sizeof(double) * 4 * sp->ispin * cp) != cudaSuccess) {
+    err = "meta-GGA energies: the tau buffer";
+    return PGXC_ENOMEM;
+  }
   return PGXC_OK;
 }
 

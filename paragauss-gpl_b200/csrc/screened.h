@@ -67,13 +67,19 @@ void screen_destroy(ScreenPlan* sp);
 struct ScreenExtra {
   const XcConst* xc = nullptr;   // host array of n
   const int* gga = nullptr;      // host flags of n
+  const int* fid = nullptr;      // host PGXC_XC_* ids of n (the meta-GGAs are evaluated by id)
   int n = 0;
   double* acc = nullptr;         // device, 4 n
   bool potential = true;
+  bool tau = false;              // form tau (some functional is a meta-GGA; screen_enable_tau first)
 };
 int screen_run(ScreenPlan* sp, const BuildArgs& a, const double* Pb, cudaStream_t st, double* ham, ScreenTimes* t,
                std::string& err, const ScreenExtra* extra = nullptr);
 int screen_error_flag(ScreenPlan* sp, cudaStream_t st, int* flag);
+// The kinetic-energy density for meta-GGA energies on the density of a plan
+// that does not form it in its builds: its buffer, allocated once.  Needs FP64
+// gradient planes (a GGA plan of the FP64 build); PGXC_ENOTSUP otherwise.
+int screen_enable_tau(ScreenPlan* sp, std::string& err);
 
 // ---------------------------------------------------------------------------
 // Sets: the screened INT8 builds of many contexts (closed shell, identity

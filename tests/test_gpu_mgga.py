@@ -113,9 +113,6 @@ def test_tpss_rejections():
         lib.Context(c, screen_threshold=-1.0)          # dense layout: no tau path
     with pytest.raises(lib.PgxcError):
         lib.xc_functionals("TPSS", np.ones(3), np.ones(3))   # needs tau
-    with lib.Context(c, screen_threshold=0.0) as ctx:
-        with pytest.raises(lib.PgxcError):
-            ctx.xc_energies(["TPSS"])
 
 
 @pytest.mark.parametrize("xc", ["TPSS", "M06L"])
