@@ -22,7 +22,7 @@ namespace pgxc {
 // the terms that cannot matter at double precision:
 //  * the nearest atom's P_near is formed first (exactly); sum_i P_i >= P_near;
 //  * every factor is at most 1, so an atom whose product (or the product of
-//    its factors with the four atoms nearest to the point) falls below
+//    its factors with the eight atoms nearest to the point) falls below
 //    tau = 2^-56 P_near / natm contributes less than 2^-56 of the sum in
 //    total: it is dropped (and w = 0 if it is the host atom).  The weights
 //    then agree with the full ordered products to within 2^-56 relative (a
@@ -114,6 +114,44 @@ __device__ __forceinline__ double becke_product(int i, double ri, int natm, cons
   return P;
 }
 
+// The kNear atoms nearest to the point, kept sorted by distance (ties in
+// ascending atom order): insert atom k at distance r.
+constexpr int kNear = 8;
+__device__ __forceinline__ void near_insert(int (&nb)[kNear], double (&nr)[kNear], int k, double r) {
+  if (!(r < nr[kNear - 1])) return;
+  int kk = k;
+  double rr = r;
+#pragma unroll
+  for (int c = 0; c < kNear; ++c) {  // one pass of swaps keeps the array sorted
+    if (rr < nr[c]) {
+      const double tr = nr[c];
+      const int tk = nb[c];
+      nr[c] = rr;
+      nb[c] = kk;
+      rr = tr;
+      kk = tk;
+    }
+  }
+}
+// Whether P_i can reach tau: every factor is at most 1, so P_i is at most the
+// product of its factors with the nearest atoms; they are multiplied nearest
+// first, which brings a far atom's bound below tau after a factor or two.
+__device__ __forceinline__ bool near_bound(int i, double ri, const int (&nb)[kNear], const double (&nr)[kNear],
+                                           const double* __restrict__ Ri, const double* __restrict__ Yi,
+                                           double tau) {
+  double Q = 1.0;
+#pragma unroll
+  for (int c = 0; c < kNear; ++c) {
+    const int k = nb[c];
+    if (k < 0 || k == i) continue;
+    const double R = __ldg(Ri + k);
+    const double d = __dsub_rn(ri, nr[c]);
+    if (d > -__dmul_rn(kBeckeEdge, R)) Q *= becke_s(d, R, __ldg(Yi + k));
+    if (Q < tau) return false;
+  }
+  return true;
+}
+
 // Thread per point (geometries of more than kBeckeWarpAtoms atoms).
 __global__ void __launch_bounds__(kBeckeThreads) k_becke_thread(const double* __restrict__ atoms,
                                                                 const double* __restrict__ dist,
@@ -130,21 +168,15 @@ __global__ void __launch_bounds__(kBeckeThreads) k_becke_thread(const double* __
   auto r_of = [&](int k) {
     return dist3(__ldg(atoms + 3 * k), __ldg(atoms + 3 * k + 1), __ldg(atoms + 3 * k + 2), x, y, z);
   };
-  // the four atoms nearest to the point (sorted) and their distances
-  int nb[4] = {-1, -1, -1, -1};
-  double nr[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
-  for (int k = 0; k < natm; ++k) {
-    const double r = r_of(k);
-    if (r < nr[3]) {
-      int j = 3;
-      for (; j > 0 && nr[j - 1] > r; --j) {
-        nr[j] = nr[j - 1];
-        nb[j] = nb[j - 1];
-      }
-      nr[j] = r;
-      nb[j] = k;
-    }
+  // the kNear atoms nearest to the point (sorted) and their distances
+  int nb[kNear];
+  double nr[kNear];
+#pragma unroll
+  for (int c = 0; c < kNear; ++c) {
+    nb[c] = -1;
+    nr[c] = INFINITY;
   }
+  for (int k = 0; k < natm; ++k) near_insert(nb, nr, k, r_of(k));
   // P_i as the ordered product, factors that are exactly 1 skipped; 0 once
   // the partial product is below tau (the factors left are at most 1)
   auto ordered = [&](int i, double ri, double tau) {
@@ -160,19 +192,9 @@ __global__ void __launch_bounds__(kBeckeThreads) k_becke_thread(const double* __
       P = P0;
     } else {
       const double ri = r_of(i);
-      const double* Ri = dist + (int64_t)i * natm;
-      const double* Yi = rdist + (int64_t)i * natm;
       // bound from the nearest atoms
-      double Q = 1.0;
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const int k = nb[c];
-        if (k < 0 || k == i) continue;
-        const double R = __ldg(Ri + k);
-        const double d = __dsub_rn(ri, nr[c]);
-        if (d > -__dmul_rn(kBeckeEdge, R)) Q *= becke_s(d, R, __ldg(Yi + k));
-      }
-      P = Q < tau ? 0.0 : ordered(i, ri, tau);
+      P = near_bound(i, ri, nb, nr, dist + (int64_t)i * natm, rdist + (int64_t)i * natm, tau) ? ordered(i, ri, tau)
+                                                                                             : 0.0;
     }
     if (P != 0.0) sum = __dadd_rn(sum, P);  // zeros leave the ascending sum unchanged
     if (i == a) pa = P;
@@ -248,23 +270,20 @@ __global__ void __launch_bounds__(kBeckeThreads) k_becke_warp(const double* __re
     return becke_product(i, rt[i], natm, dist + (int64_t)i * natm, rdist + (int64_t)i * natm, tau,
                          [&](int k) { return rt[k]; });
   };
-  int nb[4] = {-1, -1, -1, -1};
-  double nr[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
+  int nb[kNear];
+  double nr[kNear];
+#pragma unroll
+  for (int c = 0; c < kNear; ++c) {
+    nb[c] = -1;
+    nr[c] = INFINITY;
+  }
   int cnt = 0;
   double P0 = 0.0, tau = 0.0;
   int i0 = -1;
   if (live) {
     for (int k = 0; k < natm; ++k) {
       const double r = dist3(__ldg(atoms + 3 * k), __ldg(atoms + 3 * k + 1), __ldg(atoms + 3 * k + 2), x, y, z);
-      if (r < nr[3]) {
-        int j = 3;
-        for (; j > 0 && nr[j - 1] > r; --j) {
-          nr[j] = nr[j - 1];
-          nb[j] = nb[j - 1];
-        }
-        nr[j] = r;
-        nb[j] = k;
-      }
+      near_insert(nb, nr, k, r);
     }
     i0 = nb[0];
     P0 = ordered(i0, x, y, z, 0.0);
@@ -277,18 +296,7 @@ __global__ void __launch_bounds__(kBeckeThreads) k_becke_warp(const double* __re
       }
       if (i == i0) continue;
       const double ri = dist3(__ldg(atoms + 3 * i), __ldg(atoms + 3 * i + 1), __ldg(atoms + 3 * i + 2), x, y, z);
-      const double* Ri = dist + (int64_t)i * natm;
-      const double* Yi = rdist + (int64_t)i * natm;
-      double Q = 1.0;
-#pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const int k = nb[c];
-        if (k < 0 || k == i) continue;
-        const double R = __ldg(Ri + k);
-        const double d = __dsub_rn(ri, nr[c]);
-        if (d > -__dmul_rn(kBeckeEdge, R)) Q *= becke_s(d, R, __ldg(Yi + k));
-      }
-      if (Q >= tau) {
+      if (near_bound(i, ri, nb, nr, dist + (int64_t)i * natm, rdist + (int64_t)i * natm, tau)) {
         word |= 1u << (i & 31);
         ++cnt;
       }
