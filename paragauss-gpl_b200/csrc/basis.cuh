@@ -324,10 +324,17 @@ __device__ __forceinline__ unsigned long long item_u64(unsigned w, int k) {
 
 // GT: the element type of the gradient planes (double; float in the INT8
 // build, whose potential and density gradient tolerate 24-bit gradients).
-// f shells: at most 128 registers (four blocks per SM; 164 registers and
-// three blocks without the bound, the slower form for the 500-atom grid).
+// Blocks per SM: with gradients 6, 5, 4, 4 for l = 0..3 (at most 80, 96, 128
+// and 128 registers), without them 8, 8, 8, 7.  Without a bound the f-shell
+// kernel took 164 registers and ran three blocks per SM, the slower form for
+// the 500-atom grid; a bound of one block lets the compiler take 144-188
+// registers for l <= 2, which cost the 60-atom build 0.6 ms.
+template <int L, bool GRAD>
+constexpr int basis_blocks() {
+  return GRAD ? (L == 0 ? 6 : (L == 1 ? 5 : 4)) : (L <= 2 ? 8 : 7);
+}
 template <int L, bool GRAD, typename GT = double>
-__global__ void __launch_bounds__(128, L >= 3 ? 4 : 1) k_basis_items(const BasisItem* __restrict__ items, int64_t nitems,
+__global__ void __launch_bounds__(128, (basis_blocks<L, GRAD>())) k_basis_items(const BasisItem* __restrict__ items, int64_t nitems,
                                                      const double* __restrict__ exps, const double* __restrict__ norms,
                                                      const double* __restrict__ contr,
                                                      const int2* __restrict__ rng, DevSA sa,
