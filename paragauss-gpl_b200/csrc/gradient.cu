@@ -347,7 +347,7 @@ __global__ void __launch_bounds__(256) k_grad_orb(bool gga, bool mgga, int ispin
 //
 // Rows whose leave-one-out products are all negligible ("dead" rows) take
 // part only through their pairs with live rows.  Every factor is at most 1,
-// so L_xy <= the product of row x's factors with the four atoms nearest to the
+// so L_xy <= the product of row x's factors with the eight atoms nearest to the
 // point, leaving out the smallest of them; where that bound is below 2^-60
 // the row is dead (its P_x is below the same bound and is dropped from Z).
 // Both loops of pass 2 run over all atoms in the same order on every lane of
@@ -361,6 +361,7 @@ __global__ void __launch_bounds__(256) k_grad_orb(bool gga, bool mgga, int ispin
 // exactly 0 in one pass is 0 in the other.
 constexpr double kGradEdge = 0.9941;
 constexpr double kGradTau = 0x1p-60;
+constexpr int kGradNear = 8;  // atoms nearest to the point in the dead-row bound
 
 // p3(mu) and ds/dmu (even in mu).  Each step RN(RN(q / 2) RN(3 - RN(q q)))
 // is formed as RN(q RN(1.5 - RN(q q) / 2)) (one FMA inside): halving is exact
@@ -394,21 +395,32 @@ __global__ void __launch_bounds__(128) k_grad_weights(const double* __restrict__
     rv[0] = px[p0 + p]; rv[1] = py[p0 + p]; rv[2] = pz[p0 + p];
     h = owner[p0 + p];
     e = ef[p];
-    int nb[4] = {-1, -1, -1, -1};
-    double nr[4] = {INFINITY, INFINITY, INFINITY, INFINITY};
+    int nb[kGradNear];
+    double nr[kGradNear];
+#pragma unroll
+    for (int c = 0; c < kGradNear; ++c) {
+      nb[c] = -1;
+      nr[c] = INFINITY;
+    }
     for (int b = 0; b < natm; ++b) {
       const double t0 = rv[0] - atoms[3 * b], t1 = rv[1] - atoms[3 * b + 1], t2 = rv[2] - atoms[3 * b + 2];
       const double r = sqrt(t0 * t0 + t1 * t1 + t2 * t2);
       sd[b * ld + p] = r;
       sinv[b * ld + p] = r > 0.0 ? 1.0 / r : 0.0;
-      if (r < nr[3]) {
-        int j = 3;
-        for (; j > 0 && nr[j - 1] > r; --j) {
-          nr[j] = nr[j - 1];
-          nb[j] = nb[j - 1];
+      if (r < nr[kGradNear - 1]) {  // keep the kGradNear nearest sorted (ties in ascending atom order)
+        int kk = b;
+        double rr = r;
+#pragma unroll
+        for (int c = 0; c < kGradNear; ++c) {
+          if (rr < nr[c]) {
+            const double tr = nr[c];
+            const int tk = nb[c];
+            nr[c] = rr;
+            nb[c] = kk;
+            rr = tr;
+            kk = tk;
+          }
         }
-        nr[j] = r;
-        nb[j] = b;
       }
     }
     double Ph = 0.0;
@@ -416,11 +428,14 @@ __global__ void __launch_bounds__(128) k_grad_weights(const double* __restrict__
       const double db = sd[b * ld + p];
       const double* Rb = dist + (int64_t)b * natm;
       const double* Yb = rdist + (int64_t)b * natm;
-      // bound: the near factors' product with its smallest factor left out
-      double Q = 1.0, smin = 1.0;
+      // bound: the near factors' product with its smallest factor left out (with
+      // no zero factor Q / smin; with one, Q, the others; with more, 0).  Taking
+      // in a further factor never raises it, so the nearest atoms come first and
+      // the loop stops once it is below tau.
+      double Q = 1.0, smin = 1.0, bound = 1.0;
       int nzero = 0;
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
+      for (int c = 0; c < kGradNear; ++c) {
         const int k = nb[c];
         if (k < 0 || k == b) continue;
         const double R = Rb[k], d = __dsub_rn(db, nr[c]);
@@ -431,9 +446,9 @@ __global__ void __launch_bounds__(128) k_grad_weights(const double* __restrict__
         if (sv == 0.0) ++nzero;
         else Q *= sv;
         smin = fmin(smin, sv);
+        bound = nzero == 0 ? (smin > 0.0 ? Q / smin : 0.0) : (nzero == 1 ? Q : 0.0);
+        if (bound < kGradTau) break;
       }
-      // with no zero factor the bound is Q / smin; with one, Q (the others); with more, 0
-      const double bound = nzero == 0 ? (smin > 0.0 ? Q / smin : 0.0) : (nzero == 1 ? Q : 0.0);
       if (bound < kGradTau) {
         spnz[b * ld + p] = 0.0;
         snz[b * ld + p] = -2;
