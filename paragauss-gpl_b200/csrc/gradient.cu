@@ -258,6 +258,21 @@ __global__ void k_grad_points(XcConst K, int functional, bool gga, int ispin, in
 // thread's running sum, reduced over the warp when all its points share a
 // host (the usual case: the raw grid is atom by atom) and the block's shared
 // per-atom sums.
+// GGAs (not meta-GGAs): the Y_j enter the orbital terms only as
+// sum_j b_j Y_j = W P with W = sum_j b_j d_j phi, one product instead of
+// three.  W[f][p] for f < nbas, and zero rows nbas .. kpad - 1 (read by the
+// product's K loop, which meets P's zero rows there).
+__global__ void k_grad_w(int64_t nbas, int64_t kpad, int64_t ld, const double* __restrict__ B, int64_t plane,
+                         const double* __restrict__ cb, double* __restrict__ W) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kpad * ld) return;
+  const int64_t f = i / ld, p = i - f * ld;
+  double w = 0.0;
+  if (f < nbas)
+    for (int j = 0; j < 3; ++j) w += cb[j * ld + p] * B[(1 + j) * plane + i];
+  W[i] = w;
+}
+
 constexpr int kGradFB = 32;
 
 __global__ void __launch_bounds__(256) k_grad_orb(bool gga, bool mgga, int ispin, int64_t nbas, int64_t ld, int64_t p0,
@@ -296,6 +311,15 @@ __global__ void __launch_bounds__(256) k_grad_orb(bool gga, bool mgga, int ispin
         const double X = XY[(4 * sp) * plane + o];
         for (int k = 0; k < 3; ++k) q[k] += 2.0 * a[sp] * d[k] * X;
         if (!gga) continue;
+        if (!mgga) {  // sum_j b_j Y_j = (sum_j b_j d_j phi) P = V, plane 2 of the spin
+          const double V = XY[(4 * sp + 2) * plane + o];
+          for (int k = 0; k < 3; ++k) {
+            double u = d[k] * V;
+            for (int j = 0; j < 3; ++j) u += b[sp][j] * H[hidx(k, j)] * X;
+            q[k] += 2.0 * u;
+          }
+          continue;
+        }
         double Yj[3];
         for (int j = 0; j < 3; ++j) Yj[j] = XY[(4 * sp + 1 + j) * plane + o];
         for (int k = 0; k < 3; ++k) {
@@ -613,6 +637,12 @@ void launch_grad_orbital(bool gga, bool mgga, int ispin, int64_t nbas, int64_t l
   dim3 grid((unsigned)((nbas + kGradFB - 1) / kGradFB), (unsigned)((ld + 255) / 256));
   k_grad_orb<<<grid, 256, smem, st>>>(gga, mgga, ispin, nbas, ld, p0, nvalid, natm, fatom, owner, basis, plane, XY,
                                       coef, grad);
+}
+
+void launch_grad_w(int64_t nbas, int64_t ld, const double* basis, int64_t plane, const double* coef_b, double* W,
+                   cudaStream_t st) {
+  const int64_t n = round_up(nbas, 16) * ld;
+  k_grad_w<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(nbas, round_up(nbas, 16), ld, basis, plane, coef_b, W);
 }
 
 void launch_grad_xy(const double* basis_j, int64_t ld, const double* P, int64_t ldc, int64_t nbas, double* out,

@@ -39,6 +39,12 @@ void launch_grad_points(const XcConst& K, int functional, bool gga, int ispin, i
                         int64_t nvalid, const double* w, const double* wraw, const double* basis, int64_t plane,
                         const double* XY, double* coef, double* ef, double* exc, cudaStream_t st);
 
+// GGAs (not meta-GGAs): W = sum_j b_j d_j phi of the chunk (coef_b: the three
+// b planes of one spin), rows nbas .. round_up(nbas, 16) - 1 zero; the orbital
+// terms then take V = W P (plane 2 of the spin) in place of the three Y_j.
+void launch_grad_w(int64_t nbas, int64_t ld, const double* basis, int64_t plane, const double* coef_b, double* W,
+                   cudaStream_t st);
+
 // The orbital terms: -sum_g q to atom(mu) (fatom[mu]) and +sum_mu q to host(g).
 void launch_grad_orbital(bool gga, bool mgga, int ispin, int64_t nbas, int64_t ld, int64_t p0, int64_t nvalid,
                          int natm, const int* fatom, const int* owner, const double* basis, int64_t plane,

@@ -976,14 +976,20 @@ static int gradient_core(pgxc_ctx* c, int32_t nbas, int32_t ispin, int64_t kpad,
       launch_basis_hess(a, p0, nv, ld, plane, basis, s);
       for (int sp = 0; sp < ispin; ++sp) {
         const double* P = sp ? c->P2 : a.P;
-        for (int j = 0; j < (gga ? 4 : 1); ++j) {
-          // X (j = 0) or Y_j = (d_j Phi) P: (ld x nbas) = (ld x nbas)(nbas x nbas), P symmetric
+        // X (j = 0) or Y_j = (d_j Phi) P: (ld x nbas) = (ld x nbas)(nbas x nbas), P symmetric; the
+        // Y_j only for meta-GGAs (tau and its terms), GGAs take V = W P after the coefficients
+        for (int j = 0; j < (mgga ? 4 : 1); ++j)
           launch_grad_xy(basis + j * plane, ld, P, a.ldc, nbas, XY + (4 * sp + j) * plane, s);
-        }
       }
       if (rc) break;
       launch_grad_points(a.xc, c->opt.functional, gga, ispin, nbas, ld, p0, nv, a.w, c->d_wraw, basis, plane, XY,
                          coef, ef + p0, de, s);
+      if (gga && !mgga)
+        for (int sp = 0; sp < ispin; ++sp) {
+          double* W = XY + (4 * sp + 1) * plane;
+          launch_grad_w(nbas, ld, basis, plane, coef + (5 * sp + 1) * ld, W, s);
+          launch_grad_xy(W, ld, sp ? c->P2 : a.P, a.ldc, nbas, XY + (4 * sp + 2) * plane, s);
+        }
       launch_grad_orbital(gga, mgga, ispin, nbas, ld, p0, nv, c->natm, dfatom, c->d_owner, basis, plane, XY, coef,
                           dgrad, s);
       if (cudaGetLastError() != cudaSuccess) rc = set_err(c, PGXC_ECUDA, "gradient kernel launch failed");
