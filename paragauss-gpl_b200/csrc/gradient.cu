@@ -511,6 +511,15 @@ __global__ void __launch_bounds__(128) k_grad_weights(const double* __restrict__
   const double iZ = go ? 1.0 / Z : 0.0;
   double gh[3] = {0, 0, 0};
   const int lane = threadIdx.x & 31;
+  // rows live on some lane of the warp (MASK)
+  uint64_t ulo = 0, uhi = 0;
+  if (MASK) {
+    const uint64_t mlo = go ? live_lo : 0ull, mhi = go ? live_hi : 0ull;
+    ulo = ((uint64_t)__reduce_or_sync(0xffffffffu, (unsigned)(mlo >> 32)) << 32) |
+          __reduce_or_sync(0xffffffffu, (unsigned)mlo);
+    uhi = ((uint64_t)__reduce_or_sync(0xffffffffu, (unsigned)(mhi >> 32)) << 32) |
+          __reduce_or_sync(0xffffffffu, (unsigned)mhi);
+  }
   for (int x = 0; x < natm; ++x) {
     double gx[3] = {0, 0, 0};
     int zx = -2;
@@ -527,7 +536,23 @@ __global__ void __launch_bounds__(128) k_grad_weights(const double* __restrict__
     }
     const bool lx = zx != -2;
     const double* Yx = rdist + (int64_t)x * natm;
+    // a row x dead on every lane pairs only with rows live on some lane: walk
+    // those (the same y in the same order as the full loop takes them)
+    const bool xall = MASK && !__any_sync(0xffffffffu, lx);
+    uint64_t ylo = xall ? ulo : ~0ull, yhi = xall ? uhi : ~0ull;
     for (int y = 0; y < natm; ++y) {
+      if (MASK && xall) {
+        if (ylo) {
+          y = __ffsll((long long)ylo) - 1;
+          ylo &= ylo - 1;
+        } else if (yhi) {
+          y = 64 + __ffsll((long long)yhi) - 1;
+          yhi &= yhi - 1;
+        } else {
+          break;
+        }
+        if (y >= natm) break;
+      }
       if (y == x) continue;
       int zy = -2;
       bool ly;
