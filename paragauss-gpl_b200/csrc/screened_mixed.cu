@@ -470,10 +470,16 @@ __global__ void __launch_bounds__(kDensThreads, 1)
 // ---------------------------------------------------------------------------
 // Z and the V operand digits: warp per slot, lane = 4 consecutive points
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ double warp_max(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
+// scale_exp of the largest of the warp's values v >= 0, from exponent fields
+// alone: the high word of a non-negative double orders like the value, so the
+// warp's largest high word holds the largest exponent field, and for a normal
+// maximum field - 1022 is scale_exp's ilogb + 1.  A maximum of 0 (or one
+// below the normal range, which no digit can resolve) gives 0.  One integer
+// reduction in place of five double shuffles and maxima.
+__device__ __forceinline__ int warp_scale_exp(double v) {
+  const unsigned m = __reduce_max_sync(0xffffffffu, (unsigned)((unsigned long long)__double_as_longlong(v) >> 32));
+  const int field = (int)(m >> 20);
+  return field == 0 ? 0 : field - 1022;
 }
 
 // Persistent, one CTA per SM.  Warp kZWarps (one thread) streams the chunk's
@@ -630,9 +636,8 @@ __global__ void __launch_bounds__(kZThreads, 1) k_sm_zquant(const int64_t* __res
           }
 #pragma unroll
           for (int u = 0; u < 4; ++u) z[u] = GGA ? z[u] + a[u] * f[u] : a[u] * f[u];
-          const double mz = warp_max(fmax(fmax(fabs(z[0]), fabs(z[1])), fmax(fabs(z[2]), fabs(z[3]))));
-          const double mf = warp_max(fmax(fmax(fabs(f[0]), fabs(f[1])), fmax(fabs(f[2]), fabs(f[3]))));
-          const int ez = scale_exp(mz), ef = scale_exp(mf);
+          const int ez = warp_scale_exp(fmax(fmax(fabs(z[0]), fabs(z[1])), fmax(fabs(z[2]), fabs(z[3]))));
+          const int ef = warp_scale_exp(fmax(fmax(fabs(f[0]), fabs(f[1])), fmax(fabs(f[2]), fabs(f[3]))));
           if (lane == 0) {
             zs[sb + i] = pow2(ez);
             fs[sb + i] = pow2(ef + kCombShift);
